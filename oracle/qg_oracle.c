@@ -1,0 +1,313 @@
+/*
+ * qg_oracle.c -- CPU oracle for the SU(2)/SU(3) checkerboard link sweep.
+ *
+ * TEST INFRASTRUCTURE ONLY.  A plain-C restatement of the QCDGPU reference
+ * (vadimdi/QCDGPU, SU(N)/) used by tests/ to check the CUDA product path.
+ * The product never links or loads this file.  Each routine names the
+ * reference file:line it restates.
+ */
+#include <math.h>
+#include <stdint.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include "qg_oracle.h"
+
+#define PASTE_(a, b) a##b
+#define PASTE(a, b) PASTE_(a, b)
+
+/* ======================================================= RANLUX + seeding */
+#define RL_ICONS  2147483563
+#define RL_ITWO24 16777216
+#define RL_TWOM24 0.000000059604644775390625f
+#define RL_TWOM12 0.000244140625f
+
+int ol_sizeof_ranlux(void) { return (int)sizeof(ol_ranlux); }
+
+/* PRNG::initialize -> RL_initialize_CPU -> RL_initialize seeding order
+ * (random/random.cpp:228-235, 462-465, 508): srand(series); first rand()
+ * (mod 2^31-1) seeds instance 0, the next instances-1 rand() calls seed the
+ * other instances.  Uses the C library's own srand/rand, as the reference. */
+void ol_glibc_seeds(uint32_t randseries, int instances, uint32_t *seeds)
+{
+    srand(randseries);
+    int jseed = rand() % 2147483647;
+    seeds[0] = (uint32_t)jseed;
+    for (int i = 1; i < instances; i++) seeds[i] = (uint32_t)rand();
+}
+
+/* RL_initialize_CPU (random/random.cpp:504-522) and ranlux_init
+ * (random/prngcl_ranlux.cl:97-157): 24 seeds from the 40014/53668 LCG. */
+void ol_ranlux_init(ol_ranlux *st, int32_t jseed, int nskip)
+{
+    int32_t j = jseed;
+    for (int i = 0; i < 24; i++) {
+        int32_t k = j / 53668;
+        j = 40014 * (j - k * 53668) - k * 12211;
+        if (j < 0) j += RL_ICONS;
+        st->seeds[i] = ((float)(j % RL_ITWO24)) * RL_TWOM24;
+    }
+    st->i24 = 23; st->j24 = 9; st->in24 = 0; st->nskip = nskip;
+    st->carry = (st->seeds[23] == 0) ? RL_TWOM24 : 0.0f;
+}
+
+/* RL_produce_one_CPU (random/random.cpp:523-574): subtract-with-borrow with
+ * luxury skip every 24 outputs; outputs below 2^-12 get 24 more bits. */
+float ol_ranlux_next(ol_ranlux *st)
+{
+    float uni;
+    if (st->in24 == 0) {
+        st->in24 = 24;
+        for (int isk = 0; isk < st->nskip; isk++) {
+            uni = st->seeds[st->j24] - st->seeds[st->i24] - st->carry;
+            if (uni < 0.0f) { uni += 1.0f; st->carry = RL_TWOM24; } else st->carry = 0.0f;
+            st->seeds[st->i24] = uni;
+            if (st->i24 == 0) st->i24 = 24;
+            if (st->j24 == 0) st->j24 = 24;
+            st->i24--; st->j24--;
+        }
+    }
+    uni = st->seeds[st->j24] - st->seeds[st->i24] - st->carry;
+    if (uni < 0.0f) { uni += 1.0f; st->carry = RL_TWOM24; } else st->carry = 0.0f;
+    st->seeds[st->i24] = uni;
+    if (st->i24 == 0) st->i24 = 24;
+    if (st->j24 == 0) st->j24 = 24;
+    st->i24--; st->j24--;
+    if (uni < RL_TWOM12) {
+        uni = uni + RL_TWOM24 * st->seeds[st->j24];
+        if (uni == 0.0f) uni = RL_TWOM24 * RL_TWOM24;
+    }
+    st->in24--;
+    return uni;
+}
+
+void ol_ranlux_states(const uint32_t *seeds, int instances, int nskip, ol_ranlux *states)
+{
+    for (int i = 0; i < instances; i++) ol_ranlux_init(&states[i], (int32_t)seeds[i], nskip);
+}
+
+/* ranlux kernel (random/prngcl_ranlux.cl:533-563): instance i writes its
+ * s-th float4 (four consecutive outputs) to prns[s*instances + i]. */
+void ol_ranlux_batch(ol_ranlux *states, int instances, int samples, float *prns)
+{
+    for (int i = 0; i < instances; i++)
+        for (int s = 0; s < samples; s++) {
+            float *o = prns + ((size_t)s * instances + i) * 4;
+            o[0] = ol_ranlux_next(&states[i]);
+            o[1] = ol_ranlux_next(&states[i]);
+            o[2] = ol_ranlux_next(&states[i]);
+            o[3] = ol_ranlux_next(&states[i]);
+        }
+}
+
+/* ======================================================= Philox4x32-10 */
+/* Counter-based generator of Salmon, Moraes, Dror, Shaw, "Parallel random
+ * numbers: as easy as 1, 2, 3" (SC'11): 10 rounds of two 32x32->64
+ * multiplies with Weyl-sequence key bumps.                                */
+void ol_philox4x32(const uint32_t ctr[4], const uint32_t key[2], uint32_t out[4])
+{
+    uint32_t c0 = ctr[0], c1 = ctr[1], c2 = ctr[2], c3 = ctr[3];
+    uint32_t k0 = key[0], k1 = key[1];
+    for (int r = 0; r < 10; r++) {
+        uint64_t p0 = (uint64_t)0xD2511F53u * c0;
+        uint64_t p1 = (uint64_t)0xCD9E8D57u * c2;
+        uint32_t hi0 = (uint32_t)(p0 >> 32), lo0 = (uint32_t)p0;
+        uint32_t hi1 = (uint32_t)(p1 >> 32), lo1 = (uint32_t)p1;
+        c0 = hi1 ^ c1 ^ k0;
+        c1 = lo1;
+        c2 = hi0 ^ c3 ^ k1;
+        c3 = lo0;
+        k0 += 0x9E3779B9u;
+        k1 += 0xBB67AE85u;
+    }
+    out[0] = c0; out[1] = c1; out[2] = c2; out[3] = c3;
+}
+
+/* fast-mode PRN quad: counter (thread, k, phase lo, phase hi); each 32-bit
+ * word becomes ((w>>8)|1) * 2^-24, an odd multiple of 2^-24 in (0,1). */
+void ol_philox_prn(const ol_prn *src, uint32_t thread, uint32_t k, float out[4])
+{
+    uint32_t ctr[4] = { thread, k, (uint32_t)src->phase, (uint32_t)(src->phase >> 32) };
+    uint32_t key[2] = { src->key0, src->key1 }, w[4];
+    ol_philox4x32(ctr, key, w);
+    for (int i = 0; i < 4; i++) out[i] = (float)((w[i] >> 8) | 1u) * RL_TWOM24;
+}
+
+/* ======================================================= geometry */
+typedef struct { int x, y, z, t; } crd;
+
+static inline int sites_of(const ol_cfg *c) { return c->n[0] * c->n[1] * c->n[2] * c->n[3]; }
+static inline int has_twist(const ol_cfg *c) { return !(c->phi == 0.0 && c->omega == 0.0); }
+
+/* lattice_gid_to_coords / lattice_coords_to_gid, sun_common.cl:41-66 */
+static inline void gid2c(const ol_cfg *c, unsigned g, crd *o)
+{
+    unsigned n2 = c->n[1], n2n3 = c->n[1] * c->n[2], n2n3n4 = n2n3 * c->n[3];
+    o->x = g / n2n3n4; g -= o->x * n2n3n4;
+    o->t = g / n2n3;   g -= o->t * n2n3;
+    o->z = g / n2;     o->y = g - o->z * n2;
+}
+static inline unsigned c2gid(const ol_cfg *c, crd o)
+{
+    return o.y + o.z * c->n[1] + o.t * c->n[1] * c->n[2] + o.x * c->n[1] * c->n[2] * c->n[3];
+}
+/* lattice_neighbours_gid(_minus), sun_common.cl:455-513 (periodic) */
+static inline crd nb_plus(const ol_cfg *c, crd o, int d)
+{
+    switch (d) {
+    case 0: if (++o.x >= c->n[0]) o.x = 0; break;
+    case 1: if (++o.y >= c->n[1]) o.y = 0; break;
+    case 2: if (++o.z >= c->n[2]) o.z = 0; break;
+    default: if (++o.t >= c->n[3]) o.t = 0; break;
+    }
+    return o;
+}
+static inline crd nb_minus(const ol_cfg *c, crd o, int d)
+{
+    switch (d) {
+    case 0: if (o.x <= 0) o.x = c->n[0]; o.x--; break;
+    case 1: if (o.y <= 0) o.y = c->n[1]; o.y--; break;
+    case 2: if (o.z <= 0) o.z = c->n[2]; o.z--; break;
+    default: if (o.t <= 0) o.t = c->n[3]; o.t--; break;
+    }
+    return o;
+}
+/* lattice_even_gid / lattice_odd_gid, sun_common.cl:351-381 */
+static inline unsigned even_gid(const ol_cfg *c, unsigned t)
+{
+    crd o; unsigned g = 2 * t; gid2c(c, g, &o);
+    return g + ((o.x + o.y + o.z + o.t) & 1);
+}
+static inline unsigned odd_gid(const ol_cfg *c, unsigned t)
+{
+    crd o; unsigned g = 2 * t + 1; gid2c(c, g, &o);
+    return g - (((o.x + o.y + o.z + o.t) & 1) ^ 1);
+}
+
+/* ======================================================= FP64 3x3 helpers */
+typedef struct { double re, im; } cdd;
+typedef struct { cdd m[3][3]; } cd3;
+
+static void cd_mul(const cd3 *a, const cd3 *b, cd3 *o, int N)
+{
+    cd3 r;
+    memset(&r, 0, sizeof(r));
+    for (int i = 0; i < N; i++)
+        for (int j = 0; j < N; j++) {
+            double re = 0, im = 0;
+            for (int k = 0; k < N; k++) {
+                re += a->m[i][k].re * b->m[k][j].re - a->m[i][k].im * b->m[k][j].im;
+                im += a->m[i][k].re * b->m[k][j].im + a->m[i][k].im * b->m[k][j].re;
+            }
+            r.m[i][j].re = re; r.m[i][j].im = im;
+        }
+    *o = r;
+}
+static void cd_herm(const cd3 *a, cd3 *o, int N)
+{
+    cd3 r;
+    memset(&r, 0, sizeof(r));
+    for (int i = 0; i < N; i++)
+        for (int j = 0; j < N; j++) { r.m[i][j].re = a->m[j][i].re; r.m[i][j].im = -a->m[j][i].im; }
+    *o = r;
+}
+static double cd_retr(const cd3 *a, int N)
+{
+    double s = 0;
+    for (int i = 0; i < N; i++) s += a->m[i][i].re;
+    return s;
+}
+
+/* ======================================================= precision bodies */
+#define REAL double
+#define SFX _d
+#define IS_F 0
+#include "qg_oracle_impl.h"
+#undef REAL
+#undef SFX
+#undef IS_F
+
+#define REAL float
+#define SFX _f
+#define IS_F 1
+#include "qg_oracle_impl.h"
+#undef REAL
+#undef SFX
+#undef IS_F
+
+/* ======================================================= public API */
+#define DISPATCH(call_f, call_d) do { if (c->precision == 0) { call_f; } else { call_d; } } while (0)
+
+void ol_init_cold(const ol_cfg *c, void *t) { DISPATCH(init_cold_f(c, (float *)t), init_cold_d(c, (double *)t)); }
+void ol_init_gid(const ol_cfg *c, void *t)  { DISPATCH(init_gid_f(c, (float *)t), init_gid_d(c, (double *)t)); }
+void ol_init_hot_dir(const ol_cfg *c, void *t, int dir, const float *prns)
+{
+    DISPATCH(init_hot_dir_f(c, (float *)t, dir, prns), init_hot_dir_d(c, (double *)t, dir, prns));
+}
+void ol_phase_hb(const ol_cfg *c, void *t, int parity, int dir, const ol_prn *src)
+{
+    DISPATCH(phase_f(c, (float *)t, parity, dir, src, 0), phase_d(c, (double *)t, parity, dir, src, 0));
+}
+void ol_phase_or(const ol_cfg *c, void *t, int parity, int dir)
+{
+    ol_prn none;
+    memset(&none, 0, sizeof(none));
+    DISPATCH(phase_f(c, (float *)t, parity, dir, &none, 1), phase_d(c, (double *)t, parity, dir, &none, 1));
+}
+void ol_gramschmidt(const ol_cfg *c, void *t) { DISPATCH(gramschmidt_f(c, (float *)t), gramschmidt_d(c, (double *)t)); }
+
+/* FP64 reunitarisation of the stored links (new: REUNIT in double for FP32
+ * links); same Gram-Schmidt steps as lattice_GramSchmidt3 in double. */
+void ol_gramschmidt_fp64(const ol_cfg *c, void *t)
+{
+    if (c->precision != 0) { gramschmidt_d(c, (double *)t); return; }
+    int V = sites_of(c);
+    float *tf = (float *)t;
+    for (int g = 0; g < V; g++)
+        for (int mu = 0; mu < 4; mu++) {
+            if (c->group == 3) {
+                g3_f a = load3_notwist_f(c, tf, g, mu);
+                g3_d b;
+                b.uv1.x = a.uv1.x; b.uv1.y = a.uv1.y; b.uv1.z = a.uv1.z; b.uv1.w = a.uv1.w;
+                b.uv2.x = a.uv2.x; b.uv2.y = a.uv2.y; b.uv2.z = a.uv2.z; b.uv2.w = a.uv2.w;
+                b.uv3.x = a.uv3.x; b.uv3.y = a.uv3.y; b.uv3.z = a.uv3.z; b.uv3.w = a.uv3.w;
+                b = gs3_d(b);
+                a.uv1.x = (float)b.uv1.x; a.uv1.y = (float)b.uv1.y; a.uv1.z = (float)b.uv1.z; a.uv1.w = (float)b.uv1.w;
+                a.uv2.x = (float)b.uv2.x; a.uv2.y = (float)b.uv2.y; a.uv2.z = (float)b.uv2.z; a.uv2.w = (float)b.uv2.w;
+                a.uv3.x = (float)b.uv3.x; a.uv3.y = (float)b.uv3.y; a.uv3.z = (float)b.uv3.z; a.uv3.w = (float)b.uv3.w;
+                store3_f(c, tf, g, mu, a);
+            } else {
+                r4_f m = ld4_f(tf, c->rowsize, g, mu);
+                double x = m.x, y = m.y, z = m.z, w = m.w;
+                double det = sqrt(x * x + y * y + z * z + w * w);
+                m.x = (float)(x / det); m.y = (float)(y / det); m.z = (float)(z / det); m.w = (float)(w / det);
+                st4_f(tf, c->rowsize, g, mu, m);
+            }
+        }
+}
+
+void ol_plaquette(const ol_cfg *c, const void *t, double out[2])
+{
+    DISPATCH(plaquette_f(c, (const float *)t, out, NULL), plaquette_d(c, (const double *)t, out, NULL));
+}
+void ol_action(const ol_cfg *c, const void *t, double out[2])
+{
+    double p[2];
+    DISPATCH(plaquette_f(c, (const float *)t, p, out), plaquette_d(c, (const double *)t, p, out));
+}
+void ol_polyakov(const ol_cfg *c, const void *t, double out[4])
+{
+    DISPATCH(polyakov_f(c, (const float *)t, out), polyakov_d(c, (const double *)t, out));
+}
+double ol_wilson(const ol_cfg *c, const void *t, int R, int T)
+{
+    double r;
+    DISPATCH(r = wilson_f(c, (const float *)t, R, T), r = wilson_d(c, (const double *)t, R, T));
+    return r;
+}
+double ol_local_action_link(const ol_cfg *c, const void *t, int gid, int dir)
+{
+    double r;
+    DISPATCH(r = local_action_f(c, (const float *)t, gid, dir), r = local_action_d(c, (const double *)t, gid, dir));
+    return r;
+}

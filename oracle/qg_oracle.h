@@ -1,0 +1,84 @@
+/*
+ * qg_oracle.h -- CPU oracle for the SU(2)/SU(3) checkerboard link sweep.
+ *
+ * TEST INFRASTRUCTURE ONLY.  This is a plain-C restatement of the QCDGPU
+ * reference algorithm (vadimdi/QCDGPU, OpenCL kernels under SU(N)/suncl and
+ * SU(N)/random).  It exists to check the CUDA product path; nothing in the
+ * product may link, load or call it.  Only tests/, __graft_entry__.smoke()
+ * and the cpu_baseline leg of bench.py use it.
+ *
+ * Link tables handed to this oracle use the reference's storage layout
+ * (SU(N)/suncl/su3_matrix_memory.cl:43-176, su2_matrix_memory.cl:56-143):
+ * SoA planes of 4-vectors, element (site, plane) at (site + plane*rowsize)*4,
+ * SU(3) planes dir, dir+4, dir+8 = (Re u11,Re u12,Re u13,Re u23),
+ * (Im u11,Im u12,Im u13,Im u23), (Re u21,Re u22,Im u21,Im u22);
+ * SU(2) plane dir = (Re u11, Re u12, Im u11, Im u12).
+ * Site index gid = y + N2*z + N2N3*t + N2N3N4*x (SU(N)/suncl/sun_common.cl:41-66).
+ */
+#ifndef QG_ORACLE_H
+#define QG_ORACLE_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct ol_cfg {
+    int group;          /* 2 or 3                                        */
+    int n[4];           /* N1..N4 = x, y, z, t extents                   */
+    int precision;      /* 0: float links/arithmetic, 1: double          */
+    int rowsize;        /* ROWSIZE  (V aligned)                          */
+    int prngstep;       /* PRNGSTEP (V/2 aligned)                        */
+    int nhit;           /* NHIT                                          */
+    int nhitpar;        /* NHITPar                                       */
+    double beta;        /* BETA; kernels see (Real)(BETA/N)              */
+    double phi, omega;  /* twisted boundary parameters (0,0 = periodic)  */
+    int gid_mode;       /* INTS=2 deterministic update formulas          */
+} ol_cfg;
+
+/* PRN source for the heatbath: 0 = reference-layout float4 buffer read at
+ * GID + k*PRNGSTEP; 1 = Philox4x32-10 counter stream (fast mode).          */
+typedef struct ol_prn {
+    int mode;
+    const float *prns;        /* mode 0: float4 buffer                      */
+    uint32_t key0, key1;      /* mode 1: Philox key                         */
+    uint64_t phase;           /* mode 1: phase counter                      */
+} ol_prn;
+
+/* ---- PRNG: glibc seeding + RANLUX (random/random.cpp, prngcl_ranlux.cl) */
+typedef struct ol_ranlux {
+    float seeds[24];
+    int i24, j24, in24, nskip;
+    float carry;
+} ol_ranlux;
+
+void  ol_glibc_seeds(uint32_t randseries, int instances, uint32_t *seeds);
+void  ol_ranlux_init(ol_ranlux *st, int32_t jseed, int nskip);
+float ol_ranlux_next(ol_ranlux *st);
+void  ol_ranlux_states(const uint32_t *seeds, int instances, int nskip, ol_ranlux *states);
+void  ol_ranlux_batch(ol_ranlux *states, int instances, int samples, float *prns);
+int   ol_sizeof_ranlux(void);
+
+/* ---- Philox4x32-10 (Salmon et al., SC'11) */
+void  ol_philox4x32(const uint32_t ctr[4], const uint32_t key[2], uint32_t out[4]);
+void  ol_philox_prn(const ol_prn *src, uint32_t thread, uint32_t k, float out[4]);
+
+/* ---- lattice kernels (table in reference layout, Real = float|double) */
+void ol_init_cold(const ol_cfg *c, void *table);
+void ol_init_gid(const ol_cfg *c, void *table);
+void ol_init_hot_dir(const ol_cfg *c, void *table, int dir, const float *prns);
+void ol_phase_hb(const ol_cfg *c, void *table, int parity, int dir, const ol_prn *src);
+void ol_phase_or(const ol_cfg *c, void *table, int parity, int dir);
+void ol_gramschmidt(const ol_cfg *c, void *table);        /* Real precision  */
+void ol_gramschmidt_fp64(const ol_cfg *c, void *table);   /* FP64 arithmetic */
+void ol_plaquette(const ol_cfg *c, const void *table, double out[2]);
+void ol_action(const ol_cfg *c, const void *table, double out[2]);
+void ol_polyakov(const ol_cfg *c, const void *table, double out[4]);
+double ol_wilson(const ol_cfg *c, const void *table, int R, int T);
+double ol_local_action_link(const ol_cfg *c, const void *table, int gid, int dir);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,870 @@
+/*
+ * qg_oracle_impl.h -- precision-generic body of the CPU oracle.
+ *
+ * TEST INFRASTRUCTURE ONLY (see qg_oracle.h).  Included twice by qg_oracle.c,
+ * once with REAL=float (SFX=_f, IS_F=1) and once with REAL=double (SFX=_d).
+ * REAL plays the role of the reference's hgpu_float (SU(N)/kernel/complex.h:69-91);
+ * where the reference's float kernels promote to double through a double
+ * literal (cl_khr_fp64 is enabled, SU(N)/suncl/model.cl:40-44) this file
+ * promotes explicitly with (double).
+ */
+
+#define R4  PASTE(r4,  SFX)
+#define CX  PASTE(cx,  SFX)
+#define G3  PASTE(g3,  SFX)
+#define S3  PASTE(s3,  SFX)
+#define G2  PASTE(g2,  SFX)
+#define S2  PASTE(s2,  SFX)
+#define FN(n) PASTE(n, SFX)
+
+#if IS_F
+#define RPI   3.141592653589793f
+#define RPI2  6.283185307179586f
+#define RSIN  sinf
+#define RCOS  cosf
+#define RSQRT sqrtf
+#else
+#define RPI   3.1415926535897932384626433832795
+#define RPI2  6.2831853071795864769252867665590
+#define RSIN  sin
+#define RCOS  cos
+#define RSQRT sqrt
+#endif
+
+typedef struct { REAL x, y, z, w; } R4;
+typedef struct { REAL re, im; } CX;
+typedef struct { R4 uv1, uv2, uv3; } G3;              /* 12-real compressed SU(3) */
+typedef struct { CX u1, u2, u3, v1, v2, v3, w1, w2, w3; } S3;
+typedef struct { R4 uv1; } G2;                        /* 4-real SU(2)             */
+typedef struct { CX u1, u2, v1, v2; } S2;
+
+/* ------------------------------------------------------------------ memory */
+/* lattice_table_3 / lattice_store_3: SU(N)/suncl/su3_matrix_memory.cl:43-176 */
+static R4 FN(ld4)(const REAL *tab, int rowsize, unsigned site, int plane)
+{
+    const REAL *p = tab + ((size_t)site + (size_t)plane * rowsize) * 4;
+    R4 r = { p[0], p[1], p[2], p[3] };
+    return r;
+}
+static void FN(st4)(REAL *tab, int rowsize, unsigned site, int plane, R4 v)
+{
+    REAL *p = tab + ((size_t)site + (size_t)plane * rowsize) * 4;
+    p[0] = v.x; p[1] = v.y; p[2] = v.z; p[3] = v.w;
+}
+
+/* twisted boundary: Y links at x = N1-1 (su3_matrix_memory.cl:57-97) */
+static G3 FN(twist3)(const ol_cfg *c, G3 m)
+{
+    REAL phi = (REAL)c->phi, omega = (REAL)c->omega;
+    REAL p = (phi + omega) / 2, q = (omega - phi) / 2;
+    REAL cp = RCOS(p), sp = RSIN(p), cq = RCOS(q), sq = RSIN(q);
+    R4 a = m.uv1, b = m.uv2, d = m.uv3;
+    G3 r;
+    r.uv1.x = a.x * cp - b.x * sp;  r.uv2.x = b.x * cp + a.x * sp;
+    r.uv1.y = a.y * cp - b.y * sp;  r.uv2.y = b.y * cp + a.y * sp;
+    r.uv1.z = a.z * cp - b.z * sp;  r.uv2.z = b.z * cp + a.z * sp;
+    r.uv1.w = a.w * cq - b.w * sq;  r.uv2.w = b.w * cq + a.w * sq;
+    r.uv3.x = d.x * cq - d.z * sq;  r.uv3.y = d.y * cq - d.w * sq;
+    r.uv3.z = d.z * cq + d.x * sq;  r.uv3.w = d.w * cq + d.y * sq;
+    return r;
+}
+
+static G3 FN(load3)(const ol_cfg *c, const REAL *tab, const crd *co, unsigned site, int dir)
+{
+    G3 m;
+    m.uv1 = FN(ld4)(tab, c->rowsize, site, dir);
+    m.uv2 = FN(ld4)(tab, c->rowsize, site, dir + 4);
+    m.uv3 = FN(ld4)(tab, c->rowsize, site, dir + 8);
+    if (dir == 1 && has_twist(c) && co->x == c->n[0] - 1) m = FN(twist3)(c, m);
+    return m;
+}
+static G3 FN(load3_notwist)(const ol_cfg *c, const REAL *tab, unsigned site, int dir)
+{
+    G3 m;
+    m.uv1 = FN(ld4)(tab, c->rowsize, site, dir);
+    m.uv2 = FN(ld4)(tab, c->rowsize, site, dir + 4);
+    m.uv3 = FN(ld4)(tab, c->rowsize, site, dir + 8);
+    return m;
+}
+static void FN(store3)(const ol_cfg *c, REAL *tab, unsigned site, int dir, G3 m)
+{
+    FN(st4)(tab, c->rowsize, site, dir, m.uv1);
+    FN(st4)(tab, c->rowsize, site, dir + 4, m.uv2);
+    FN(st4)(tab, c->rowsize, site, dir + 8, m.uv3);
+}
+
+/* SU(2): su2_matrix_memory.cl:56-143 */
+static R4 FN(times2)(R4 u, R4 v);
+static G2 FN(load2)(const ol_cfg *c, const REAL *tab, const crd *co, unsigned site, int dir)
+{
+    G2 m;
+    m.uv1 = FN(ld4)(tab, c->rowsize, site, dir);
+    if (dir == 1 && has_twist(c) && co->x == c->n[0] - 1) {
+        REAL phi = (REAL)c->phi;
+        R4 om;
+        om.x = RCOS(phi / 2); om.z = RSIN(phi / 2); om.y = 0; om.w = 0;
+        m.uv1 = FN(times2)(om, m.uv1);
+    }
+    return m;
+}
+static void FN(store2)(const ol_cfg *c, REAL *tab, unsigned site, int dir, G2 m)
+{
+    FN(st4)(tab, c->rowsize, site, dir, m.uv1);
+}
+
+/* --------------------------------------------------------------- algebra */
+/* complex helpers: every product written as (a.re*b.re - a.im*b.im) etc.   */
+static inline CX FN(cmul)(CX a, CX b) { CX r; r.re = a.re * b.re - a.im * b.im; r.im = a.re * b.im + a.im * b.re; return r; }
+static inline CX FN(cconj)(CX a) { a.im = -a.im; return a; }
+
+/* row3 = conj(row1 x row2): lattice_reconstruct3, SU(N)/suncl/su3cl.cl:137-165 */
+static S3 FN(rec3)(G3 a)
+{
+    S3 b;
+    b.u1.re = a.uv1.x; b.u1.im = a.uv2.x;
+    b.u2.re = a.uv1.y; b.u2.im = a.uv2.y;
+    b.u3.re = a.uv1.z; b.u3.im = a.uv2.z;
+    b.v1.re = a.uv3.x; b.v1.im = a.uv3.z;
+    b.v2.re = a.uv3.y; b.v2.im = a.uv3.w;
+    b.v3.re = a.uv1.w; b.v3.im = a.uv2.w;
+    b.w1.re =  b.u2.re * b.v3.re - b.u2.im * b.v3.im - b.u3.re * b.v2.re + b.u3.im * b.v2.im;
+    b.w1.im = -b.u2.re * b.v3.im - b.u2.im * b.v3.re + b.u3.re * b.v2.im + b.u3.im * b.v2.re;
+    b.w2.re =  b.u3.re * b.v1.re - b.u3.im * b.v1.im - b.u1.re * b.v3.re + b.u1.im * b.v3.im;
+    b.w2.im = -b.u3.re * b.v1.im - b.u3.im * b.v1.re + b.u1.re * b.v3.im + b.u1.im * b.v3.re;
+    b.w3.re =  b.u1.re * b.v2.re - b.u1.im * b.v2.im - b.u2.re * b.v1.re + b.u2.im * b.v1.im;
+    b.w3.im = -b.u1.re * b.v2.im - b.u1.im * b.v2.re + b.u2.re * b.v1.im + b.u2.im * b.v1.re;
+    return b;
+}
+
+static G3 FN(compress3)(const S3 *s)
+{
+    G3 g;
+    g.uv1.x = s->u1.re; g.uv1.y = s->u2.re; g.uv1.z = s->u3.re; g.uv1.w = s->v3.re;
+    g.uv2.x = s->u1.im; g.uv2.y = s->u2.im; g.uv2.z = s->u3.im; g.uv2.w = s->v3.im;
+    g.uv3.x = s->v1.re; g.uv3.y = s->v2.re; g.uv3.z = s->v1.im; g.uv3.w = s->v2.im;
+    return g;
+}
+
+/* one entry of a 3x3 complex product: sum_k a_k b_k in the order k=1,2,3 */
+static inline CX FN(dot3)(CX a1, CX a2, CX a3, CX b1, CX b2, CX b3)
+{
+    CX r;
+    r.re = a1.re * b1.re - a1.im * b1.im + a2.re * b2.re - a2.im * b2.im + a3.re * b3.re - a3.im * b3.im;
+    r.im = a1.re * b1.im + a1.im * b1.re + a2.re * b2.im + a2.im * b2.re + a3.re * b3.im + a3.im * b3.re;
+    return r;
+}
+
+/* full 3x3 product: matrix_times_su3, su3cl.cl:101-135 */
+static S3 FN(mul3)(const S3 *u, const S3 *v)
+{
+    S3 t;
+    t.u1 = FN(dot3)(u->u1, u->u2, u->u3, v->u1, v->v1, v->w1);
+    t.u2 = FN(dot3)(u->u1, u->u2, u->u3, v->u2, v->v2, v->w2);
+    t.u3 = FN(dot3)(u->u1, u->u2, u->u3, v->u3, v->v3, v->w3);
+    t.v1 = FN(dot3)(u->v1, u->v2, u->v3, v->u1, v->v1, v->w1);
+    t.v2 = FN(dot3)(u->v1, u->v2, u->v3, v->u2, v->v2, v->w2);
+    t.v3 = FN(dot3)(u->v1, u->v2, u->v3, v->u3, v->v3, v->w3);
+    t.w1 = FN(dot3)(u->w1, u->w2, u->w3, v->u1, v->v1, v->w1);
+    t.w2 = FN(dot3)(u->w1, u->w2, u->w3, v->u2, v->v2, v->w2);
+    t.w3 = FN(dot3)(u->w1, u->w2, u->w3, v->u3, v->v3, v->w3);
+    return t;
+}
+
+/* compressed x compressed -> compressed (rows 1,2 of the product):
+ * matrix_times3, su3cl.cl:51-99 */
+static G3 FN(times3)(G3 a, G3 b)
+{
+    S3 u = FN(rec3)(a), v = FN(rec3)(b), t;
+    t.u1 = FN(dot3)(u.u1, u.u2, u.u3, v.u1, v.v1, v.w1);
+    t.u2 = FN(dot3)(u.u1, u.u2, u.u3, v.u2, v.v2, v.w2);
+    t.u3 = FN(dot3)(u.u1, u.u2, u.u3, v.u3, v.v3, v.w3);
+    t.v1 = FN(dot3)(u.v1, u.v2, u.v3, v.u1, v.v1, v.w1);
+    t.v2 = FN(dot3)(u.v1, u.v2, u.v3, v.u2, v.v2, v.w2);
+    t.v3 = FN(dot3)(u.v1, u.v2, u.v3, v.u3, v.v3, v.w3);
+    return FN(compress3)(&t);
+}
+
+/* compressed hermitian conjugate: matrix_hermitian3, su3_update_cl.cl:86-110 */
+static G3 FN(herm3)(G3 a)
+{
+    S3 u = FN(rec3)(a), h;
+    h.u1 = FN(cconj)(u.u1); h.u2 = FN(cconj)(u.v1); h.u3 = FN(cconj)(u.w1);
+    h.v1 = FN(cconj)(u.u2); h.v2 = FN(cconj)(u.v2); h.v3 = FN(cconj)(u.w2);
+    h.w1 = FN(cconj)(u.u3); h.w2 = FN(cconj)(u.v3); h.w3 = FN(cconj)(u.w3);
+    return FN(compress3)(&h);
+}
+
+static S3 FN(add3)(const S3 *a, const S3 *b)
+{
+    S3 r;
+    const REAL *pa = (const REAL *)a, *pb = (const REAL *)b;
+    REAL *pr = (REAL *)&r;
+    for (int i = 0; i < 18; i++) pr[i] = pa[i] + pb[i];
+    return r;
+}
+
+/* staple pieces, su3_update_cl.cl:293-338 */
+static S3 FN(staple_fwd3)(G3 u1, G3 u2, G3 u3)     /* u1 u2^+ u3^+ */
+{
+    G3 m2 = FN(times3)(u1, FN(herm3)(u2));
+    return FN(rec3)(FN(times3)(m2, FN(herm3)(u3)));
+}
+static S3 FN(staple_bwd3)(G3 u1, G3 u2, G3 u3)     /* u1^+ u2^+ u3 */
+{
+    G3 m3 = FN(times3)(FN(herm3)(u1), FN(herm3)(u2));
+    return FN(rec3)(FN(times3)(m3, u3));
+}
+
+/* lattice_GramSchmidt3, su3_update_cl.cl:228-291 (in REAL precision) */
+static G3 FN(gs3)(G3 m)
+{
+    R4 t1 = m.uv1, t2 = m.uv2, t3 = m.uv3;
+    REAL nu = RSQRT((t1.x * t1.x + t2.x * t2.x) + (t1.y * t1.y + t2.y * t2.y) + (t1.z * t1.z + t2.z * t2.z));
+    REAL ur[3] = { t1.x / nu, t1.y / nu, t1.z / nu };
+    REAL ui[3] = { t2.x / nu, t2.y / nu, t2.z / nu };
+    REAL vr[3] = { t3.x, t3.y, t1.w };
+    REAL vi[3] = { t3.z, t3.w, t2.w };
+    /* sc = sum_k v_k * conj(u_k) */
+    REAL sr = (ur[0] * vr[0] + ui[0] * vi[0]) + (ur[1] * vr[1] + ui[1] * vi[1]) + (ur[2] * vr[2] + ui[2] * vi[2]);
+    REAL si = (ur[0] * vi[0] - ui[0] * vr[0]) + (ur[1] * vi[1] - ui[1] * vr[1]) + (ur[2] * vi[2] - ui[2] * vr[2]);
+    REAL nr[3], ni[3];
+    for (int k = 0; k < 3; k++) {
+        nr[k] = vr[k] - ur[k] * sr + ui[k] * si;
+        ni[k] = vi[k] - ur[k] * si - ui[k] * sr;
+    }
+    REAL nv = RSQRT((nr[0] * nr[0] + ni[0] * ni[0]) + (nr[1] * nr[1] + ni[1] * ni[1]) + (nr[2] * nr[2] + ni[2] * ni[2]));
+    G3 r;
+    r.uv1.x = ur[0]; r.uv1.y = ur[1]; r.uv1.z = ur[2]; r.uv1.w = nr[2] / nv;
+    r.uv2.x = ui[0]; r.uv2.y = ui[1]; r.uv2.z = ui[2]; r.uv2.w = ni[2] / nv;
+    r.uv3.x = nr[0] / nv; r.uv3.y = nr[1] / nv; r.uv3.z = ni[0] / nv; r.uv3.w = ni[1] / nv;
+    return r;
+}
+
+/* SU(2) algebra, gpu_su_2 layout (x=Re u11, y=Re u12, z=Im u11, w=Im u12):
+ * matrix_times2, su2_matrix_memory.cl:41-53 / su3_update_cl.cl:150-162 */
+static R4 FN(times2)(R4 u, R4 v)
+{
+    R4 a;
+    a.x = u.x * v.x - u.y * v.y - u.z * v.z - u.w * v.w;
+    a.z = u.x * v.z + u.z * v.x + u.y * v.w - u.w * v.y;
+    a.y = u.x * v.y + u.y * v.x + u.w * v.z - u.z * v.w;
+    a.w = u.x * v.w + u.w * v.x + u.z * v.y - u.y * v.z;
+    return a;
+}
+static R4 FN(herm2)(R4 u) { R4 r = { u.x, -u.y, -u.z, -u.w }; return r; }
+static S2 FN(rec2)(R4 a)
+{
+    S2 b;
+    b.u1.re = a.x;  b.u1.im = a.z;  b.u2.re = a.y;  b.u2.im = a.w;
+    b.v1.re = -a.y; b.v1.im = a.w;  b.v2.re = a.x;  b.v2.im = -a.z;
+    return b;
+}
+/* full 2x2 complex product: matrix_times_su2, su2cl.cl:43-60 */
+static S2 FN(mul2)(const S2 *u, const S2 *v)
+{
+    S2 t;
+    t.u1 = FN(cmul)(u->u1, v->u1); { CX q = FN(cmul)(u->u2, v->v1); t.u1.re += q.re; t.u1.im += q.im; }
+    t.u2 = FN(cmul)(u->u1, v->u2); { CX q = FN(cmul)(u->u2, v->v2); t.u2.re += q.re; t.u2.im += q.im; }
+    t.v1 = FN(cmul)(u->v1, v->u1); { CX q = FN(cmul)(u->v2, v->v1); t.v1.re += q.re; t.v1.im += q.im; }
+    t.v2 = FN(cmul)(u->v1, v->u2); { CX q = FN(cmul)(u->v2, v->v2); t.v2.re += q.re; t.v2.im += q.im; }
+    return t;
+}
+static S2 FN(add2)(S2 a, S2 b)
+{
+    S2 r;
+    r.u1.re = a.u1.re + b.u1.re; r.u1.im = a.u1.im + b.u1.im;
+    r.u2.re = a.u2.re + b.u2.re; r.u2.im = a.u2.im + b.u2.im;
+    r.v1.re = a.v1.re + b.v1.re; r.v1.im = a.v1.im + b.v1.im;
+    r.v2.re = a.v2.re + b.v2.re; r.v2.im = a.v2.im + b.v2.im;
+    return r;
+}
+/* staple pieces for SU(2): su2_update_cl.cl:158-203 */
+static S2 FN(staple_fwd2)(R4 u1, R4 u2, R4 u3)
+{
+    return FN(rec2)(FN(times2)(FN(times2)(u1, FN(herm2)(u2)), FN(herm2)(u3)));
+}
+static S2 FN(staple_bwd2)(R4 u1, R4 u2, R4 u3)
+{
+    return FN(rec2)(FN(times2)(FN(times2)(FN(herm2)(u1), FN(herm2)(u2)), u3));
+}
+
+/* ------------------------------------------------------------- PRN source */
+typedef struct {
+    const ol_prn *src;
+    const ol_cfg *cfg;
+    uint32_t thread;      /* GID of the phase kernel thread            */
+    uint32_t k;           /* PRN quads consumed so far (indprng step)  */
+    double gidval;        /* INTS=2: float(gindex)                     */
+} FN(prnctx);
+
+static void FN(prn_next)(FN(prnctx) *p, REAL r[4])
+{
+    float q[4];
+    if (p->src->mode == 0) {
+        size_t idx = (size_t)p->thread + (size_t)p->k * (size_t)p->cfg->prngstep;
+        const float *s = p->src->prns + idx * 4;
+        q[0] = s[0]; q[1] = s[1]; q[2] = s[2]; q[3] = s[3];
+    } else {
+        ol_philox_prn(p->src, p->thread, p->k, q);
+    }
+    p->k++;
+    r[0] = (REAL)q[0]; r[1] = (REAL)q[1]; r[2] = (REAL)q[2]; r[3] = (REAL)q[3];
+}
+
+/* --------------------------------------------------------------- heatbath */
+/* Kennedy-Pendleton step on the SU(2) block a (su_2 form).  Returns 1 when a
+ * try was accepted and a is overwritten with c*aH; on rejection the SU(3)
+ * caller wants the identity and one extra PRN skip (su3_update_cl.cl:665-668).
+ * su3_update_cl.cl:568-669 (SU(3) path) / su2_update_cl.cl:434-531 (SU(2)). */
+static int FN(kp_step)(S2 *a, REAL beta, FN(prnctx) *p, int su3_path)
+{
+    const ol_cfg *c = p->cfg;
+    R4 aH, cc, d;
+    REAL det, bdet, cosrnd, delta = 0, rnd[4];
+    int flag = 0;
+    if (su3_path) {
+        aH.x =  (a->u1.re + a->v2.re);
+        aH.z = -(a->u1.im - a->v2.im);
+        aH.y = -(a->u2.re - a->v1.re);
+        aH.w = -(a->u2.im + a->v1.im);
+        det = RSQRT(aH.x * aH.x + aH.y * aH.y + aH.z * aH.z + aH.w * aH.w);
+        aH.x /= det; aH.z /= det; aH.y /= det; aH.w /= det;
+    } else {
+        REAL Mx = a->u1.re + a->v2.re, My = a->u1.im - a->v2.im;
+        REAL Mz = a->u2.re - a->v1.re, Mw = a->u2.im + a->v1.im;
+        det = RSQRT(Mx * Mx + My * My + Mz * Mz + Mw * Mw);
+        aH.x = Mx / det; aH.z = -My / det; aH.y = -Mz / det; aH.w = -Mw / det;
+    }
+    bdet = beta * det;
+    for (int i = 0; i < c->nhit && !flag; i++) {
+        if (c->gid_mode) {
+            double g = p->gidval, V = (double)sites_of(c);
+            rnd[0] = (REAL)fabs(sin((0.005 * (1 + c->nhit) + 270.0 / V) * g));
+            rnd[1] = (REAL)fabs(cos((0.005 * (1 + c->nhit) +  60.0 / V) * g));
+            rnd[2] = (REAL)fabs(sin((0.005 * (1 + c->nhit) - 150.0 / V) * g));
+            rnd[3] = (REAL)fabs(cos((0.005 * (1 + c->nhit) - 380.0 / V) * g));
+        } else {
+            FN(prn_next)(p, rnd);
+        }
+        cosrnd = RCOS(RPI2 * rnd[1]);
+        delta = (REAL)(-(log(1.0 - (double)rnd[0]) + (double)(cosrnd * cosrnd) * log(1.0 - (double)rnd[2])) / (double)bdet);
+        if ((double)(rnd[3] * rnd[3]) <= (1.0 - 0.5 * (double)delta)) flag = 1;
+        if (c->gid_mode) { delta = cosrnd * cosrnd / bdet; flag = 1; }
+    }
+    if (flag) {
+        if (c->gid_mode) {
+            double g = p->gidval, V = (double)sites_of(c);
+            rnd[0] = (REAL)fabs(cos((0.08 - 270.0 / V) * g));
+            rnd[1] = (REAL)fabs(sin((0.08 -  60.0 / V) * g));
+            rnd[2] = (REAL)fabs(cos((0.08 + 150.0 / V) * g));
+            rnd[3] = (REAL)fabs(sin((0.08 + 380.0 / V) * g));
+        } else {
+            FN(prn_next)(p, rnd);
+        }
+        REAL cosal = (REAL)(1.0 - (double)delta);
+        REAL costh = (REAL)(2.0 * (double)rnd[0] - 1.0);
+        REAL sinth = (REAL)sqrt(1.0 - (double)(costh * costh));
+        REAL sinal = (REAL)sqrt(1.0 - (double)(cosal * cosal));
+        REAL phi = RPI2 * rnd[1];
+        REAL sinphi = RSIN(phi), cosphi = RCOS(phi);
+        cc.x = cosal;
+        cc.z = sinal * costh;
+        cc.y = sinal * sinth * sinphi;
+        cc.w = sinal * sinth * cosphi;
+        d = FN(times2)(cc, aH);
+        *a = FN(rec2)(d);
+        return 1;
+    }
+    if (su3_path) {
+        a->u1.re = 1; a->u1.im = 0; a->u2.re = 0; a->u2.im = 0;
+        a->v1.re = 0; a->v1.im = 0; a->v2.re = 1; a->v2.im = 0;
+        if (!c->gid_mode) p->k++;
+    }
+    return 0;
+}
+
+/* Microcanonical reflection of the SU(2) block (overrelaxation; absent in
+ * the reference, Creutz PRD 36 (1987) 515, Brown-Woch PRL 58 (1987) 2394):
+ * with aH the normalised hermitian projection used by the heatbath, the
+ * subgroup element aH*aH leaves Re Tr(V W) unchanged and is an involution. */
+static void FN(or_step)(S2 *a)
+{
+    R4 aH;
+    aH.x =  (a->u1.re + a->v2.re);
+    aH.z = -(a->u1.im - a->v2.im);
+    aH.y = -(a->u2.re - a->v1.re);
+    aH.w = -(a->u2.im + a->v1.im);
+    REAL det = RSQRT(aH.x * aH.x + aH.y * aH.y + aH.z * aH.z + aH.w * aH.w);
+    aH.x /= det; aH.z /= det; aH.y /= det; aH.w /= det;
+    *a = FN(rec2)(FN(times2)(aH, aH));
+}
+
+/* Cabibbo-Marinari over the three SU(2) subgroups; lattice_heatbath3,
+ * su3_update_cl.cl:672-779.  kind 0 = heatbath, 1 = overrelaxation. */
+static G3 FN(cm3)(const S3 *staple, G3 m0, REAL beta, FN(prnctx) *p, int nhitpar, int kind)
+{
+    G3 reslt = m0, Vg, m1, m2, m3 = m0;
+    S3 U0 = FN(rec3)(m0), x0;
+    S2 r0;
+    R4 z = { 0, 0, 0, 0 };
+    for (int j = 0; j < nhitpar; j++) {
+        /* subgroup (1,2) */
+        x0 = FN(mul3)(&U0, staple);
+        r0.u1 = x0.u1; r0.u2 = x0.u2; r0.v1 = x0.v1; r0.v2 = x0.v2;
+        if (kind == 0) FN(kp_step)(&r0, beta, p, 1); else FN(or_step)(&r0);
+        Vg.uv1 = z; Vg.uv2 = z;
+        Vg.uv1.x = r0.u1.re; Vg.uv1.y = r0.u2.re;
+        Vg.uv2.x = r0.u1.im; Vg.uv2.y = r0.u2.im;
+        Vg.uv3.x = r0.v1.re; Vg.uv3.y = r0.v2.re; Vg.uv3.z = r0.v1.im; Vg.uv3.w = r0.v2.im;
+        m1 = FN(times3)(Vg, m3);
+        U0 = FN(rec3)(m1);
+        /* subgroup (1,3) */
+        x0 = FN(mul3)(&U0, staple);
+        r0.u1 = x0.u1; r0.u2 = x0.u3; r0.v1 = x0.w1; r0.v2 = x0.w3;
+        if (kind == 0) FN(kp_step)(&r0, beta, p, 1); else FN(or_step)(&r0);
+        Vg.uv1 = z; Vg.uv2 = z; Vg.uv3 = z;
+        Vg.uv1.x = r0.u1.re; Vg.uv1.z = r0.u2.re;
+        Vg.uv2.x = r0.u1.im; Vg.uv2.z = r0.u2.im;
+        Vg.uv3.y = 1;
+        m2 = FN(times3)(Vg, m1);
+        U0 = FN(rec3)(m2);
+        /* subgroup (2,3) */
+        x0 = FN(mul3)(&U0, staple);
+        r0.u1 = x0.v2; r0.u2 = x0.v3; r0.v1 = x0.w2; r0.v2 = x0.w3;
+        if (kind == 0) FN(kp_step)(&r0, beta, p, 1); else FN(or_step)(&r0);
+        Vg.uv1 = z; Vg.uv2 = z; Vg.uv3 = z;
+        Vg.uv1.x = 1; Vg.uv1.w = r0.u2.re;
+        Vg.uv2.w = r0.u2.im;
+        Vg.uv3.y = r0.u1.re; Vg.uv3.w = r0.u1.im;
+        m3 = FN(times3)(Vg, m2);
+        reslt = FN(gs3)(m3);
+        U0 = FN(rec3)(reslt);
+    }
+    return reslt;
+}
+
+/* --------------------------------------------------------------- staples */
+/* lattice_staple_3, su3_update_cl.cl:341-565: for direction mu the three
+ * other directions are visited in the reference's fixed order and summed
+ * pairwise as written there (forward+backward per plane, running sum). */
+static const int FN(nu_order)[4][3] = { {1, 2, 3}, {0, 2, 3}, {1, 0, 3}, {1, 2, 0} };
+
+static S3 FN(staple3)(const ol_cfg *c, const REAL *tab, unsigned g, int mu)
+{
+    crd co, cp, cn, cm, cmp;
+    gid2c(c, g, &co);
+    cp = nb_plus(c, co, mu);
+    S3 st, s2;
+    for (int i = 0; i < 3; i++) {
+        int nu = FN(nu_order)[mu][i];
+        cn = nb_plus(c, co, nu);
+        cm = nb_minus(c, co, nu);
+        cmp = nb_plus(c, cm, mu);
+        G3 a = FN(load3)(c, tab, &cp, c2gid(c, cp), nu);
+        G3 b = FN(load3)(c, tab, &cn, c2gid(c, cn), mu);
+        G3 d = FN(load3)(c, tab, &co, g, nu);
+        S3 fw = FN(staple_fwd3)(a, b, d);
+        a = FN(load3)(c, tab, &cmp, c2gid(c, cmp), nu);
+        b = FN(load3)(c, tab, &cm, c2gid(c, cm), mu);
+        d = FN(load3)(c, tab, &cm, c2gid(c, cm), nu);
+        S3 bw = FN(staple_bwd3)(a, b, d);
+        if (i == 0) {
+            st = FN(add3)(&fw, &bw);                   /* staple  = f0 + b0    */
+        } else {
+            s2 = FN(add3)(&st, &fw);                   /* staple2 = st + f_i   */
+            st = FN(add3)(&bw, &s2);                   /* staple  = b_i + s2   */
+        }
+    }
+    return st;
+}
+
+static S2 FN(staple2)(const ol_cfg *c, const REAL *tab, unsigned g, int mu)
+{
+    crd co, cp, cn, cm, cmp;
+    gid2c(c, g, &co);
+    cp = nb_plus(c, co, mu);
+    S2 st, s2;
+    for (int i = 0; i < 3; i++) {
+        int nu = FN(nu_order)[mu][i];
+        cn = nb_plus(c, co, nu);
+        cm = nb_minus(c, co, nu);
+        cmp = nb_plus(c, cm, mu);
+        R4 a = FN(load2)(c, tab, &cp, c2gid(c, cp), nu).uv1;
+        R4 b = FN(load2)(c, tab, &cn, c2gid(c, cn), mu).uv1;
+        R4 d = FN(load2)(c, tab, &co, g, nu).uv1;
+        S2 fw = FN(staple_fwd2)(a, b, d);
+        a = FN(load2)(c, tab, &cmp, c2gid(c, cmp), nu).uv1;
+        b = FN(load2)(c, tab, &cm, c2gid(c, cm), mu).uv1;
+        d = FN(load2)(c, tab, &cm, c2gid(c, cm), nu).uv1;
+        S2 bw = FN(staple_bwd2)(a, b, d);
+        if (i == 0) {
+            st = FN(add2)(fw, bw);
+        } else {
+            s2 = FN(add2)(st, fw);
+            st = FN(add2)(bw, s2);
+        }
+    }
+    return st;
+}
+
+/* ----------------------------------------------------------- phase kernel */
+/* update_{even,odd}_{X,Y,Z,T}, SU(N)/suncl/suncl.cl:399-975 */
+static void FN(phase)(const ol_cfg *c, REAL *tab, int parity, int mu, const ol_prn *src, int kind)
+{
+    unsigned half = (unsigned)(sites_of(c) / 2);
+    REAL beta = (REAL)(c->beta / c->group);
+    for (unsigned t = 0; t < half; t++) {
+        unsigned g = parity ? odd_gid(c, t) : even_gid(c, t);
+        crd co;
+        gid2c(c, g, &co);
+        FN(prnctx) p;
+        p.src = src; p.cfg = c; p.thread = t; p.k = 0; p.gidval = (double)(float)g;
+        if (c->group == 3) {
+            G3 m0 = FN(load3)(c, tab, &co, g, mu);
+            S3 st = FN(staple3)(c, tab, g, mu);
+            G3 mU = FN(cm3)(&st, m0, beta, &p, c->nhitpar, kind);
+            FN(store3)(c, tab, g, mu, mU);
+        } else {
+            G2 m0 = FN(load2)(c, tab, &co, g, mu);
+            S2 st = FN(staple2)(c, tab, g, mu);
+            if (kind == 0) {
+                S2 a = st;
+                if (FN(kp_step)(&a, beta, &p, 0)) {
+                    G2 r; r.uv1.x = a.u1.re; r.uv1.y = a.u2.re; r.uv1.z = a.u1.im; r.uv1.w = a.u2.im;
+                    FN(store2)(c, tab, g, mu, r);
+                } else {
+                    FN(store2)(c, tab, g, mu, m0);
+                }
+            } else {
+                /* U -> aH U^+ aH with aH = normalised (staple projection)^+ */
+                R4 aH;
+                REAL Mx = st.u1.re + st.v2.re, My = st.u1.im - st.v2.im;
+                REAL Mz = st.u2.re - st.v1.re, Mw = st.u2.im + st.v1.im;
+                REAL det = RSQRT(Mx * Mx + My * My + Mz * Mz + Mw * Mw);
+                aH.x = Mx / det; aH.z = -My / det; aH.y = -Mz / det; aH.w = -Mw / det;
+                G2 r;
+                r.uv1 = FN(times2)(FN(times2)(aH, FN(herm2)(m0.uv1)), aH);
+                FN(store2)(c, tab, g, mu, r);
+            }
+        }
+    }
+}
+
+/* --------------------------------------------------------- initialisation */
+static void FN(init_cold)(const ol_cfg *c, REAL *tab)
+{
+    int V = sites_of(c);
+    for (int g = 0; g < V; g++)
+        for (int mu = 0; mu < 4; mu++) {
+            if (c->group == 3) {
+                G3 m; R4 z = { 0, 0, 0, 0 };
+                m.uv1 = z; m.uv2 = z; m.uv3 = z; m.uv1.x = 1; m.uv3.y = 1;
+                FN(store3)(c, tab, g, mu, m);
+            } else {
+                G2 m; m.uv1.x = 1; m.uv1.y = 0; m.uv1.z = 0; m.uv1.w = 0;
+                FN(store2)(c, tab, g, mu, m);
+            }
+        }
+}
+
+/* lattice_init_gid, suncl.cl:190-347 (sin/cos in double, GS in REAL) */
+static void FN(init_gid)(const ol_cfg *c, REAL *tab)
+{
+    int V = sites_of(c);
+    double s = (double)V;
+    for (int g = 0; g < V; g++) {
+        double gd = (double)g;
+        for (int mu = 0; mu < 4; mu++) {
+            static const double off[4] = { 0.001, 0.002, 0.003, 0.004 };
+            double o = off[mu];
+            if (c->group == 3) {
+                double f1  = sin((o + 10.0 / s) * gd) / 2.0;
+                double f2  = cos((o - 10.0 / s) * gd) / 3.0;
+                double f3  = sin((o - 18.0 / s) * gd) / 4.0;
+                double f4  = cos((o + 12.0 / s) * gd) / 4.0;
+                double f5  = sin((o - 12.0 / s) * gd) / 3.0;
+                double f6  = cos((o - 15.0 / s) * gd) / 2.0;
+                double f7  = sin((o + 15.0 / s) * gd) / 3.0;
+                double f8  = cos((o - 11.0 / s) * gd) / 4.0;
+                double f9  = sin((o - 11.0 / s) * gd) / 3.0;
+                double f10 = cos((o + 16.0 / s) * gd) / 2.0;
+                double f11 = sin((o - 16.0 / s) * gd) / 3.0;
+                double f12 = cos((o - 18.0 / s) * gd) / 2.0;
+                G3 m;
+                m.uv1.x = (REAL)f1; m.uv1.y = (REAL)f3; m.uv1.z = (REAL)f5; m.uv1.w = (REAL)f11;
+                m.uv2.x = (REAL)f2; m.uv2.y = (REAL)f4; m.uv2.z = (REAL)f6; m.uv2.w = (REAL)f12;
+                m.uv3.x = (REAL)f7; m.uv3.y = (REAL)f9; m.uv3.z = (REAL)f8; m.uv3.w = (REAL)f10;
+                FN(store3)(c, tab, g, mu, FN(gs3)(m));
+            } else {
+                double f1 = sin((o + 10.0 / s) * gd) / 2.0;
+                double f2 = cos((o - 10.0 / s) * gd) / 3.0;
+                double f3 = sin((o - 18.0 / s) * gd) / 4.0;
+                double f4 = sqrt(1.0 - f1 * f1 - f2 * f2 - f3 * f3);
+                G2 m;
+                m.uv1.x = (REAL)f1; m.uv1.y = (REAL)f3; m.uv1.z = (REAL)f4; m.uv1.w = (REAL)f2;
+                FN(store2)(c, tab, g, mu, m);
+            }
+        }
+    }
+}
+
+/* lattice_random3 / lattice_random2 (su3_update_cl.cl:165-225,
+ * su2_update_cl.cl:110-146): NOT Haar; alpha uniform in [0,pi]. */
+static R4 FN(rnd_r4)(const float *prns, size_t idx)
+{
+    R4 r = { (REAL)prns[idx * 4], (REAL)prns[idx * 4 + 1], (REAL)prns[idx * 4 + 2], (REAL)prns[idx * 4 + 3] };
+    return r;
+}
+static void FN(init_hot_dir)(const ol_cfg *c, REAL *tab, int mu, const float *prns)
+{
+    int V = sites_of(c);
+    for (int g = 0; g < V; g++) {
+        if (c->group == 3) {
+            R4 r1 = FN(rnd_r4)(prns, (size_t)g);
+            R4 r2 = FN(rnd_r4)(prns, (size_t)g + c->rowsize);
+            R4 r3 = FN(rnd_r4)(prns, (size_t)g + 2 * (size_t)c->rowsize);
+            REAL a0[4], a1[4], a2[4], a3[4];
+            REAL R1[4] = { r1.x, r1.y, r1.z, r1.w }, R2[4] = { r2.x, r2.y, r2.z, r2.w }, R3[4] = { r3.x, r3.y, r3.z, r3.w };
+            for (int k = 0; k < 4; k++) {
+                REAL alpha = RPI * R1[k], phi = RPI2 * R2[k];
+#if IS_F
+                REAL costh = 2.0f * R3[k] - 1.0f;
+                REAL sinth = sqrtf(1.0f - costh * costh);
+#else
+                REAL costh = 2.0 * R3[k] - 1.0;
+                REAL sinth = sqrt(1.0 - costh * costh);
+#endif
+                REAL sinal = RSIN(alpha);
+                a0[k] = RCOS(alpha);
+                REAL sinph = RSIN(phi), cosph = RCOS(phi);
+                REAL t1 = sinal * sinth;
+                a1[k] = t1 * cosph;
+                a2[k] = t1 * sinph;
+                a3[k] = sinal * costh;
+            }
+            /* product of three embedded SU(2) rotations, written out as in
+             * su3_update_cl.cl:209-220 (components .x,.y,.z of a0..a3) */
+            G3 m;
+#define X 0
+#define Y 1
+#define Z 2
+            m.uv1.x = a0[X] * a0[Y] - a3[X] * a3[Y];
+            m.uv2.x = a0[Y] * a3[X] + a0[X] * a3[Y];
+            m.uv1.y = -a0[X] * a1[Y] * a1[Z] + a0[Z] * a2[X] - a0[X] * a2[Y] * a2[Z] - a1[Z] * a2[Y] * a3[X] + a1[Y] * a2[Z] * a3[X] - a1[X] * a3[Z];
+            m.uv2.y = a0[Z] * a1[X] + a0[X] * a1[Z] * a2[Y] - a0[X] * a1[Y] * a2[Z] - a1[Y] * a1[Z] * a3[X] - a2[Y] * a2[Z] * a3[X] + a2[X] * a3[Z];
+            m.uv1.z = -a1[X] * a1[Z] + a0[X] * a0[Z] * a2[Y] + a2[X] * a2[Z] - a0[Z] * a1[Y] * a3[X] + a0[X] * a1[Y] * a3[Z] + a2[Y] * a3[X] * a3[Z];
+            m.uv2.z = a0[X] * a0[Z] * a1[Y] + a1[Z] * a2[X] + a1[X] * a2[Z] + a0[Z] * a2[Y] * a3[X] - a0[X] * a2[Y] * a3[Z] + a1[Y] * a3[X] * a3[Z];
+            m.uv1.w = -a0[Z] * a1[X] * a1[Y] - a0[Z] * a2[X] * a2[Y] + a0[X] * a2[Z] + a1[Z] * a3[X] - a1[Y] * a2[X] * a3[Z] + a1[X] * a2[Y] * a3[Z];
+            m.uv2.w = a0[X] * a1[Z] - a0[Z] * a1[Y] * a2[X] + a0[Z] * a1[X] * a2[Y] - a2[Z] * a3[X] + a1[X] * a1[Y] * a3[Z] + a2[X] * a2[Y] * a3[Z];
+            m.uv3.x = -a0[Y] * a2[X] - a1[X] * a3[Y];
+            m.uv3.z = a0[Y] * a1[X] - a2[X] * a3[Y];
+            m.uv3.y = a0[X] * a0[Z] + a1[Y] * a1[Z] * a2[X] - a1[X] * a1[Z] * a2[Y] + a1[X] * a1[Y] * a2[Z] + a2[X] * a2[Y] * a2[Z] + a3[X] * a3[Z];
+            m.uv3.w = -a1[X] * a1[Y] * a1[Z] - a1[Z] * a2[X] * a2[Y] + a1[Y] * a2[X] * a2[Z] - a1[X] * a2[Y] * a2[Z] - a0[Z] * a3[X] + a0[X] * a3[Z];
+#undef X
+#undef Y
+#undef Z
+            FN(store3)(c, tab, g, mu, m);
+        } else {
+            R4 r = FN(rnd_r4)(prns, (size_t)g);
+            REAL alpha = RPI * r.x, phi = RPI2 * r.y;
+#if IS_F
+            REAL costh = 2.0f * r.z - 1.0f;
+            REAL sinth = sqrtf(1.0f - costh * costh);
+#else
+            REAL costh = 2.0 * r.z - 1.0;
+            REAL sinth = sqrt(1.0 - costh * costh);
+#endif
+            REAL sinal = RSIN(alpha), a0 = RCOS(alpha);
+            REAL sinph = RSIN(phi), cosph = RCOS(phi);
+            REAL t1 = sinal * sinth;
+            G2 m;
+            m.uv1.x = a0; m.uv1.y = t1 * sinph; m.uv1.z = sinal * costh; m.uv1.w = t1 * cosph;
+            FN(store2)(c, tab, g, mu, m);
+        }
+    }
+}
+
+/* lattice_GramSchmidt kernel, suncl.cl:350-396 (REAL precision) */
+static void FN(gramschmidt)(const ol_cfg *c, REAL *tab)
+{
+    int V = sites_of(c);
+    for (int g = 0; g < V; g++)
+        for (int mu = 0; mu < 4; mu++) {
+            if (c->group == 3) {
+                FN(store3)(c, tab, g, mu, FN(gs3)(FN(load3_notwist)(c, tab, g, mu)));
+            } else {
+                R4 m = FN(ld4)(tab, c->rowsize, g, mu);
+                REAL det = RSQRT(m.x * m.x + m.y * m.y + m.z * m.z + m.w * m.w);
+                m.x /= det; m.y /= det; m.z /= det; m.w /= det;
+                FN(st4)(tab, c->rowsize, g, mu, m);
+            }
+        }
+}
+
+/* ------------------------------------------------------------ measurement */
+/* lattice_reconstruct3_double + FP64 products (su3_measurements_cl.cl:292-548) */
+static void FN(to_d3)(G3 a, cd3 *b)
+{
+    g3_d ad;
+    ad.uv1.x = (double)a.uv1.x; ad.uv1.y = (double)a.uv1.y; ad.uv1.z = (double)a.uv1.z; ad.uv1.w = (double)a.uv1.w;
+    ad.uv2.x = (double)a.uv2.x; ad.uv2.y = (double)a.uv2.y; ad.uv2.z = (double)a.uv2.z; ad.uv2.w = (double)a.uv2.w;
+    ad.uv3.x = (double)a.uv3.x; ad.uv3.y = (double)a.uv3.y; ad.uv3.z = (double)a.uv3.z; ad.uv3.w = (double)a.uv3.w;
+    s3_d s = rec3_d(ad);
+    memcpy(b, &s, sizeof(s));
+}
+static void FN(to_d2)(R4 a, cd3 *b)
+{
+    /* SU(2) embedded in the 2x2 block of a 3x3 with zero third row/column */
+    memset(b, 0, sizeof(*b));
+    b->m[0][0].re = (double)a.x;  b->m[0][0].im = (double)a.z;
+    b->m[0][1].re = (double)a.y;  b->m[0][1].im = (double)a.w;
+    b->m[1][0].re = -(double)a.y; b->m[1][0].im = (double)a.w;
+    b->m[1][1].re = (double)a.x;  b->m[1][1].im = -(double)a.z;
+}
+static void FN(load_d)(const ol_cfg *c, const REAL *tab, const crd *co, int mu, cd3 *out)
+{
+    unsigned g = c2gid(c, *co);
+    if (c->group == 3) FN(to_d3)(FN(load3)(c, tab, co, g, mu), out);
+    else FN(to_d2)(FN(load2)(c, tab, co, g, mu).uv1, out);
+}
+
+static void FN(plaquette)(const ol_cfg *c, const REAL *tab, double out[2], double *act_out)
+{
+    int V = sites_of(c);
+    double sp = 0, tp = 0, as = 0, at = 0;
+    REAL bet = (REAL)(c->beta / c->group);
+    for (int g = 0; g < V; g++) {
+        crd co; gid2c(c, g, &co);
+        double rs = 0, rt = 0;
+        /* planes in the reference order: xy, xz, xt, yz, yt, zt (sun_measurements_cl.cl:1240-1305) */
+        static const int pl[6][2] = { {0, 1}, {0, 2}, {0, 3}, {1, 2}, {1, 3}, {2, 3} };
+        for (int q = 0; q < 6; q++) {
+            int m = pl[q][0], n = pl[q][1];
+            crd cm = nb_plus(c, co, m), cn = nb_plus(c, co, n);
+            cd3 a, b, d, e, w1, w2, w3;
+            FN(load_d)(c, tab, &co, m, &a);
+            FN(load_d)(c, tab, &cm, n, &b);
+            FN(load_d)(c, tab, &cn, m, &d);
+            FN(load_d)(c, tab, &co, n, &e);
+            int N = c->group;
+            cd_mul(&a, &b, &w1, N);
+            cd_herm(&d, &w2, N);
+            cd_mul(&w1, &w2, &w3, N);
+            cd_herm(&e, &w2, N);
+            cd_mul(&w3, &w2, &w1, N);
+            double tr = cd_retr(&w1, N);
+            if (n == 3) rt += tr; else rs += tr;
+        }
+        sp += rs; tp += rt;
+        as += (double)bet * (3.0 * c->group - rs);
+        at += (double)bet * (3.0 * c->group - rt);
+    }
+    out[0] = sp; out[1] = tp;
+    if (act_out) { act_out[0] = as; act_out[1] = at; }
+}
+
+/* lattice_polyakov, polyakov.cl:54-140: ordered product of N4 T-links in
+ * REAL precision, Re/Im trace to double. */
+static void FN(polyakov)(const ol_cfg *c, const REAL *tab, double out[4])
+{
+    double re = 0, im = 0, p2 = 0, p4 = 0;
+    for (int x = 0; x < c->n[0]; x++)
+        for (int z = 0; z < c->n[2]; z++)
+            for (int y = 0; y < c->n[1]; y++) {
+                crd co = { x, y, z, 0 };
+                double pr, pi;
+                if (c->group == 3) {
+                    S3 v0 = FN(rec3)(FN(load3)(c, tab, &co, c2gid(c, co), 3));
+                    for (int i = 1; i < c->n[3]; i++) {
+                        co = nb_plus(c, co, 3);
+                        S3 v1 = FN(rec3)(FN(load3)(c, tab, &co, c2gid(c, co), 3));
+                        v0 = FN(mul3)(&v0, &v1);
+                    }
+                    pr = (double)v0.u1.re + (double)v0.v2.re + (double)v0.w3.re;
+                    pi = (double)v0.u1.im + (double)v0.v2.im + (double)v0.w3.im;
+                } else {
+                    S2 v0 = FN(rec2)(FN(load2)(c, tab, &co, c2gid(c, co), 3).uv1);
+                    for (int i = 1; i < c->n[3]; i++) {
+                        co = nb_plus(c, co, 3);
+                        S2 v1 = FN(rec2)(FN(load2)(c, tab, &co, c2gid(c, co), 3).uv1);
+                        v0 = FN(mul2)(&v0, &v1);
+                    }
+                    pr = (double)v0.u1.re + (double)v0.v2.re;
+                    pi = (double)v0.u1.im + (double)v0.v2.im;
+                }
+                re += pr; im += pi;
+                double q2 = pr * pr + pi * pi;
+                p2 += q2; p4 += q2 * q2;
+            }
+    out[0] = re; out[1] = im; out[2] = p2; out[3] = p4;
+}
+
+/* lattice_measurement_wilson, wilson_loop.cl:55-454: for every site and
+ * i in {x,y,z}, Re Tr of the R x T loop (R along i, T along t), FP64. */
+static double FN(wilson)(const ol_cfg *c, const REAL *tab, int R, int T)
+{
+    int V = sites_of(c), N = c->group;
+    double sum = 0;
+    for (int g = 0; g < V; g++) {
+        crd c1; gid2c(c, g, &c1);
+        cd3 m1, m2, m3, m4, m5, w;
+        crd co = c1;
+        FN(load_d)(c, tab, &co, 3, &m1);
+        for (int k = 1; k < T; k++) { co = nb_plus(c, co, 3); FN(load_d)(c, tab, &co, 3, &m5); cd_mul(&m1, &m5, &w, N); m1 = w; }
+        crd c2 = nb_plus(c, co, 3);                 /* x + T t^ */
+        for (int i = 0; i < 3; i++) {
+            crd a = c1, b = c2;
+            FN(load_d)(c, tab, &a, i, &m4);
+            FN(load_d)(c, tab, &b, i, &m2);
+            for (int k = 1; k < R; k++) {
+                a = nb_plus(c, a, i); b = nb_plus(c, b, i);
+                FN(load_d)(c, tab, &a, i, &m5); cd_mul(&m4, &m5, &w, N); m4 = w;
+                FN(load_d)(c, tab, &b, i, &m5); cd_mul(&m2, &m5, &w, N); m2 = w;
+            }
+            crd c4 = nb_plus(c, a, i);             /* x + R i^ */
+            FN(load_d)(c, tab, &c4, 3, &m3);
+            for (int k = 1; k < T; k++) { c4 = nb_plus(c, c4, 3); FN(load_d)(c, tab, &c4, 3, &m5); cd_mul(&m3, &m5, &w, N); m3 = w; }
+            cd3 h, w1, w3;
+            cd_mul(&m1, &m2, &w1, N);
+            cd_herm(&m3, &h, N);
+            cd_mul(&w1, &h, &w3, N);
+            cd_herm(&m4, &h, N);
+            cd_mul(&w3, &h, &w1, N);
+            sum += cd_retr(&w1, N);
+        }
+    }
+    return sum;
+}
+
+/* local Wilson action of one link (used by property tests of OR) */
+static double FN(local_action)(const ol_cfg *c, const REAL *tab, unsigned g, int mu)
+{
+    crd co; gid2c(c, g, &co);
+    double s = 0;
+    if (c->group == 3) {
+        S3 st = FN(staple3)(c, tab, g, mu);
+        S3 u = FN(rec3)(FN(load3)(c, tab, &co, g, mu));
+        S3 p = FN(mul3)(&u, &st);
+        s = (double)p.u1.re + (double)p.v2.re + (double)p.w3.re;
+    } else {
+        S2 st = FN(staple2)(c, tab, g, mu);
+        S2 u = FN(rec2)(FN(load2)(c, tab, &co, g, mu).uv1);
+        /* Re Tr(u * st) */
+        s = (double)(u.u1.re * st.u1.re - u.u1.im * st.u1.im + u.u2.re * st.v1.re - u.u2.im * st.v1.im)
+          + (double)(u.v1.re * st.u2.re - u.v1.im * st.u2.im + u.v2.re * st.v2.re - u.v2.im * st.v2.im);
+    }
+    return s;
+}
+
+#undef R4
+#undef CX
+#undef G3
+#undef S3
+#undef G2
+#undef S2
+#undef FN
+#undef RPI
+#undef RPI2
+#undef RSIN
+#undef RCOS
+#undef RSQRT

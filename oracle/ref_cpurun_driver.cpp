@@ -1,0 +1,92 @@
+// Test and baseline infrastructure only.  Drives the reference's own
+// sequential CPU path (SU(N)/suncpp, the -D CPU_RUN build of vadimdi/QCDGPU)
+// through its templates: modelCPU<su_n> (suncpp/sunh.h), lattice_update_odd /
+// lattice_update_even (suncpp/Update/sun_update.h:80-119) and plqConf
+// (suncpp/Measurements/Plq.h:47-95), in the sweep order of
+// suncpp/suncpp.h:143-167.  Compiled from the reference sources where they
+// lie; nothing of it is copied into this repository.
+//
+// Usage:
+//   ref_cpurun plaq  <group> <L1> <L2> <L3> <L4> <beta> <ints> <randseries> <sweeps>
+//       prints "sweep spat temp total" per sweep with %.17g (sweep 0 = start)
+//   ref_cpurun bench <group> <L1> <L2> <L3> <L4> <beta> <randseries> <warm> <timed>
+//       cold start, <warm> untimed sweeps, then times <timed> sweeps and
+//       prints "link_updates_per_s <value> seconds <t>"
+#include <chrono>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+
+#include "QCDGPU.h"
+
+template <typename su_n>
+static void sweep(modelCPU<su_n> *lat, PRNG_CL::PRNG *prng)
+{
+    lattice_update_odd(lat, X, prng);
+    lattice_update_odd(lat, Y, prng);
+    lattice_update_odd(lat, Z, prng);
+    lattice_update_odd(lat, T, prng);
+    lattice_update_even(lat, X, prng);
+    lattice_update_even(lat, Y, prng);
+    lattice_update_even(lat, Z, prng);
+    lattice_update_even(lat, T, prng);
+}
+
+template <typename su_n>
+static int run(int mode, int group, int *L, double beta, int ints, int series, int a, int b)
+{
+    modelCPU<su_n> *lat = new modelCPU<su_n>;
+    lat->lattice_ndCPU = 4;
+    lat->lattice_size = (int *)calloc(4, sizeof(int));
+    for (int i = 0; i < 4; i++) lat->lattice_size[i] = L[i];
+    lat->ints = ints;
+    lat->nhit = 10;
+    lat->beta = beta;
+    lat->lattice_group = group;
+    lat->lattice_sitesCPU = L[0] * L[1] * L[2] * L[3];
+    PRNG_CL::PRNG *prng = new PRNG_CL::PRNG;
+    prng->PRNG_generator = PRNG_CL::PRNG::PRNG_generator_RANLUX3;
+    prng->PRNG_randseries = series;
+    prng->PRNG_precision = PRNG_CL::PRNG::PRNG_precision_single;
+    prng->initialize_CPU();
+    lat->create_latticeCPU();
+    lat->lattice_initializeCPU();
+    if (mode == 0) {
+        for (int s = 0; s <= a; s++) {
+            if (s > 0) sweep(lat, prng);
+            hgpu_double tot;
+            hgpu_complex p = plqConf(lat, &tot);
+            printf("%d %.17g %.17g %.17g\n", s, (double)p.re, (double)p.im, (double)tot);
+        }
+    } else {
+        for (int s = 0; s < a; s++) sweep(lat, prng);
+        auto t0 = std::chrono::steady_clock::now();
+        for (int s = 0; s < b; s++) sweep(lat, prng);
+        auto t1 = std::chrono::steady_clock::now();
+        double sec = std::chrono::duration<double>(t1 - t0).count();
+        double lu = 4.0 * lat->lattice_sitesCPU * b / sec;
+        hgpu_double tot;
+        plqConf(lat, &tot);
+        printf("link_updates_per_s %.6e seconds %.6f plaquette %.10f\n", lu, sec, (double)tot);
+    }
+    lat->delete_latticeCPU();
+    free(lat->lattice_size);
+    delete lat;
+    delete prng;
+    return 0;
+}
+
+int main(int argc, char **argv)
+{
+    if (argc < 11) { fprintf(stderr, "see source for usage\n"); return 2; }
+    int mode = strcmp(argv[1], "plaq") == 0 ? 0 : 1;
+    int group = atoi(argv[2]);
+    int L[4] = { atoi(argv[3]), atoi(argv[4]), atoi(argv[5]), atoi(argv[6]) };
+    double beta = atof(argv[7]);
+    if (mode == 0)
+        return group == 3 ? run<su_3>(0, 3, L, beta, atoi(argv[8]), atoi(argv[9]), atoi(argv[10]), 0)
+                          : run<su_2>(0, 2, L, beta, atoi(argv[8]), atoi(argv[9]), atoi(argv[10]), 0);
+    if (argc < 11) return 2;
+    return group == 3 ? run<su_3>(1, 3, L, beta, 1, atoi(argv[8]), atoi(argv[9]), atoi(argv[10]))
+                      : run<su_2>(1, 2, L, beta, 1, atoi(argv[8]), atoi(argv[9]), atoi(argv[10]));
+}

@@ -1,0 +1,182 @@
+"""ctypes binding of the CPU oracle (oracle/qg_oracle.c) for the tests.
+
+Test infrastructure only: the oracle is the checker the CUDA path is compared
+against, never part of the product.
+"""
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+ORACLE_DIR = os.path.join(ROOT, "oracle")
+LIB_PATH = os.path.join(ORACLE_DIR, "_build", "liboracle.so")
+REF_DIR = os.path.join(ORACLE_DIR, "_ref")
+
+
+class Cfg(ctypes.Structure):
+    _fields_ = [
+        ("group", ctypes.c_int),
+        ("n", ctypes.c_int * 4),
+        ("precision", ctypes.c_int),
+        ("rowsize", ctypes.c_int),
+        ("prngstep", ctypes.c_int),
+        ("nhit", ctypes.c_int),
+        ("nhitpar", ctypes.c_int),
+        ("beta", ctypes.c_double),
+        ("phi", ctypes.c_double),
+        ("omega", ctypes.c_double),
+        ("gid_mode", ctypes.c_int),
+    ]
+
+
+class Prn(ctypes.Structure):
+    _fields_ = [
+        ("mode", ctypes.c_int),
+        ("prns", ctypes.c_void_p),
+        ("key0", ctypes.c_uint32),
+        ("key1", ctypes.c_uint32),
+        ("phase", ctypes.c_uint64),
+    ]
+
+
+def _load():
+    src = [os.path.join(ORACLE_DIR, f) for f in ("qg_oracle.c", "qg_oracle_impl.h", "qg_oracle.h")]
+    if not os.path.exists(LIB_PATH) or any(os.path.getmtime(s) > os.path.getmtime(LIB_PATH) for s in src):
+        subprocess.check_call(["make", "-s", "-C", ORACLE_DIR])
+    lib = ctypes.CDLL(LIB_PATH)
+    P = ctypes.POINTER
+    lib.ol_glibc_seeds.argtypes = [ctypes.c_uint32, ctypes.c_int, P(ctypes.c_uint32)]
+    lib.ol_ranlux_init.argtypes = [ctypes.c_void_p, ctypes.c_int32, ctypes.c_int]
+    lib.ol_ranlux_next.argtypes = [ctypes.c_void_p]
+    lib.ol_ranlux_next.restype = ctypes.c_float
+    lib.ol_ranlux_states.argtypes = [P(ctypes.c_uint32), ctypes.c_int, ctypes.c_int, ctypes.c_void_p]
+    lib.ol_ranlux_batch.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_void_p]
+    lib.ol_sizeof_ranlux.restype = ctypes.c_int
+    lib.ol_philox4x32.argtypes = [P(ctypes.c_uint32), P(ctypes.c_uint32), P(ctypes.c_uint32)]
+    lib.ol_philox_prn.argtypes = [P(Prn), ctypes.c_uint32, ctypes.c_uint32, P(ctypes.c_float)]
+    for name in ("ol_init_cold", "ol_init_gid", "ol_gramschmidt", "ol_gramschmidt_fp64"):
+        getattr(lib, name).argtypes = [P(Cfg), ctypes.c_void_p]
+    lib.ol_init_hot_dir.argtypes = [P(Cfg), ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p]
+    lib.ol_phase_hb.argtypes = [P(Cfg), ctypes.c_void_p, ctypes.c_int, ctypes.c_int, P(Prn)]
+    lib.ol_phase_or.argtypes = [P(Cfg), ctypes.c_void_p, ctypes.c_int, ctypes.c_int]
+    lib.ol_plaquette.argtypes = [P(Cfg), ctypes.c_void_p, P(ctypes.c_double)]
+    lib.ol_action.argtypes = [P(Cfg), ctypes.c_void_p, P(ctypes.c_double)]
+    lib.ol_polyakov.argtypes = [P(Cfg), ctypes.c_void_p, P(ctypes.c_double)]
+    lib.ol_wilson.argtypes = [P(Cfg), ctypes.c_void_p, ctypes.c_int, ctypes.c_int]
+    lib.ol_wilson.restype = ctypes.c_double
+    lib.ol_local_action_link.argtypes = [P(Cfg), ctypes.c_void_p, ctypes.c_int, ctypes.c_int]
+    lib.ol_local_action_link.restype = ctypes.c_double
+    return lib
+
+
+lib = _load()
+
+
+def align(n, a):
+    return ((n + a - 1) // a) * a
+
+
+def make_cfg(group=3, dims=(4, 4, 4, 4), precision=1, beta=6.0, nhit=10, nhitpar=1,
+             row_align=64, gid_mode=False, phi=0.0, omega=0.0):
+    c = Cfg()
+    c.group = group
+    for i in range(4):
+        c.n[i] = dims[i]
+    V = dims[0] * dims[1] * dims[2] * dims[3]
+    c.precision = precision
+    c.rowsize = align(V, row_align)
+    c.prngstep = align(V // 2, row_align)
+    c.nhit = nhit
+    c.nhitpar = nhitpar
+    c.beta = beta
+    c.phi = phi
+    c.omega = omega
+    c.gid_mode = 1 if gid_mode else 0
+    return c
+
+
+def volume(c):
+    return c.n[0] * c.n[1] * c.n[2] * c.n[3]
+
+
+def new_table(c):
+    planes = 12 if c.group == 3 else 4
+    dt = np.float32 if c.precision == 0 else np.float64
+    return np.zeros(planes * c.rowsize * 4, dtype=dt)
+
+
+def vp(a):
+    return a.ctypes.data_as(ctypes.c_void_p)
+
+
+def glibc_seeds(series, instances):
+    out = np.zeros(instances, dtype=np.uint32)
+    lib.ol_glibc_seeds(series, instances, out.ctypes.data_as(ctypes.POINTER(ctypes.c_uint32)))
+    return out
+
+
+class Ranlux:
+    """Reference-layout RANLUX batch generator (one state per instance)."""
+
+    def __init__(self, series, instances, nskip=223):
+        self.instances = instances
+        self.seeds = glibc_seeds(series, instances)
+        self.states = ctypes.create_string_buffer(lib.ol_sizeof_ranlux() * instances)
+        lib.ol_ranlux_states(self.seeds.ctypes.data_as(ctypes.POINTER(ctypes.c_uint32)), instances, nskip,
+                             self.states)
+
+    def batch(self, samples):
+        out = np.zeros(samples * self.instances * 4, dtype=np.float32)
+        lib.ol_ranlux_batch(self.states, self.instances, samples, vp(out))
+        return out
+
+
+def prn_samples(c, instances, hot=False):
+    """PRNG_samples for one batch (SU(N)/suncl/suncl.cpp:2304-2307, random.cpp:222)."""
+    total = c.nhitpar * 3 * c.prngstep * (c.nhit + 1)
+    if hot:
+        total = c.rowsize * 4 + 3 * c.prngstep * (c.nhit + 1)
+    return 1 + (total - 1) // instances
+
+
+def phase_hb(c, tab, parity, mu, prns=None, philox=None):
+    src = Prn()
+    if prns is not None:
+        src.mode = 0
+        src.prns = prns.ctypes.data
+    else:
+        src.mode = 1
+        src.key0, src.key1, src.phase = philox
+    lib.ol_phase_hb(ctypes.byref(c), vp(tab), parity, mu, ctypes.byref(src))
+
+
+def plaquette(c, tab):
+    out = (ctypes.c_double * 2)()
+    lib.ol_plaquette(ctypes.byref(c), vp(tab), out)
+    return out[0], out[1]
+
+
+def action(c, tab):
+    out = (ctypes.c_double * 2)()
+    lib.ol_action(ctypes.byref(c), vp(tab), out)
+    return out[0], out[1]
+
+
+def polyakov(c, tab):
+    out = (ctypes.c_double * 4)()
+    lib.ol_polyakov(ctypes.byref(c), vp(tab), out)
+    return tuple(out)
+
+
+def wilson(c, tab, R, T):
+    return lib.ol_wilson(ctypes.byref(c), vp(tab), R, T)
+
+
+def philox(ctr, key):
+    o = (ctypes.c_uint32 * 4)()
+    c4 = (ctypes.c_uint32 * 4)(*ctr)
+    k2 = (ctypes.c_uint32 * 2)(*key)
+    lib.ol_philox4x32(c4, k2, o)
+    return tuple(o)
