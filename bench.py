@@ -1,0 +1,324 @@
+"""Benchmark of the SU(3) checkerboard sweep on B200.
+
+Workload (one "step" = one full sweep): SU(3) Wilson action, 32^4 lattice,
+beta = 6.0, FP32 12-real compressed links, sweep = 1 Cabibbo-Marinari
+heatbath + 4 overrelaxation sweeps, FP64 reunitarisation every 10 sweeps,
+cold start thermalised for a few untimed sweeps.  Metric: link updates per
+second (4V links x 5 updates per sweep), whole job.  The link field
+(201 MB) is larger than the 126 MB L2, so no L2 flush is needed between
+steps.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+N > 1 (torchrun): independent replicas, one lattice per GPU (distinct seed),
+no collective on the data path; barrier + max-over-ranks device time.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+SIZE = 32
+BETA = 6.0
+N_OR = 4
+REUNIT_EVERY = 10
+METRIC = "link updates/s (SU(3) 32^4 beta=6.0 FP32, 1 HB + 4 OR sweep)"
+UNIT = "link_updates/s"
+LINK_BYTES = 48          # 12 FP32 reals per stored SU(3) link
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--prng", default="philox", choices=["philox", "ranlux"])
+    ap.add_argument("--size", type=int, default=SIZE)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def dist_env():
+    return int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)), int(os.environ.get("LOCAL_RANK", 0))
+
+
+# ------------------------------------------------------------- clocks
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = tempfile.mktemp(prefix="qg_clocks_", suffix=".csv")
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), "--query-gpu=" + self.FIELDS, "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax.append(float(f[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        os.unlink(self.path)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ------------------------------------------------------ reference (CPU)
+def ref_binary():
+    return os.path.join(ROOT, "oracle", "_ref", "ref_cpurun")
+
+
+def cpu_workers(size):
+    ncpu = os.cpu_count() or 1
+    try:
+        avail = os.sysconf("SC_AVPHYS_PAGES") * os.sysconf("SC_PAGE_SIZE")
+    except (ValueError, OSError):
+        avail = 8 << 30
+    per = 4 * size ** 4 * 18 * 8 * 1.3         # the reference CPU path stores links as 18 doubles
+    return max(1, min(ncpu, int(avail // per)))
+
+
+def run_reference_phases(size, procs, warm, timed):
+    """The reference's sequential heatbath (SU(N)/suncpp) in `procs`
+    concurrent processes with distinct RANDSERIES; each does `warm` + `timed`
+    phases (V/2 link updates each) and reports per-phase wall times."""
+    cmd = [ref_binary(), "phases", "3", str(size), str(size), str(size), str(size), repr(BETA)]
+    ps = [subprocess.Popen(cmd + [str(54 + i), str(warm), str(timed)], stdout=subprocess.PIPE, text=True)
+          for i in range(procs)]
+    times = []
+    for p in ps:
+        out, _ = p.communicate()
+        if p.returncode != 0:
+            raise RuntimeError("reference CPU path failed")
+        times.append([float(x) for x in out.split()[1:]])
+    return times
+
+
+def cpu_baseline_line(size, seconds_target=15.0):
+    if not os.path.exists(ref_binary()):
+        return None
+    procs = cpu_workers(size)
+    t = run_reference_phases(size, procs, 0, 1)
+    per_phase = max(x[0] for x in t)
+    n = max(1, min(8, int(seconds_target / max(per_phase, 1e-3))))
+    t = run_reference_phases(size, procs, 0, n)
+    wall = max(sum(x) for x in t)
+    links = procs * n * (size ** 4 // 2)
+    return {"value": links / wall, "unit": UNIT, "cores": procs, "kind": "reference",
+            "sample": "reference CPU path (SU(N)/suncpp heatbath, RANLUX3, NHIT=10; it has no overrelaxation) on "
+                      "SU(3) %d^4 beta=%.1f cold start: %d concurrent processes x %d phases of %d link updates, "
+                      "%.1f s wall" % (size, BETA, procs, n, size ** 4 // 2, wall)}
+
+
+def run_reference_arm(args):
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return 0
+    if not os.path.exists(ref_binary()):
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/ref_cpurun not built"}))
+        return 0
+    procs = cpu_workers(args.size)
+    t = run_reference_phases(args.size, procs, args.warmup, args.steps)
+    step = [max(x[k] for x in t) for k in range(args.steps)]
+    total = sum(step)
+    links = procs * args.steps * (args.size ** 4 // 2)
+    value = links / total
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1e3 * total / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (cold start)",
+            "impl": "reference",
+            "config": {"workload": "SU(3) %d^4 beta=6.0 heatbath phase (V/2 link updates) per process per step"
+                                   % args.size, "processes": procs},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": procs, "kind": "reference",
+                             "sample": "%d concurrent processes of the reference CPU path, one phase each per step"
+                                       % procs},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+    return 0
+
+
+# ------------------------------------------------------------ our arm
+def peaks():
+    try:
+        d = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+        return float(d["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback"
+
+
+def profile_traffic():
+    """Per-launch DRAM bytes of the phase kernels from the committed ncu
+    summary (profiles/phase_traffic.json), scaled to this lattice."""
+    try:
+        d = json.load(open(os.path.join(ROOT, "profiles", "phase_traffic.json")))
+        return d
+    except (OSError, ValueError):
+        return None
+
+
+def run_ours(args):
+    import torch
+    import qcdgpu_b200 as Q
+
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=torch.device("cuda", local))
+    prng = Q.PRNG_PHILOX if args.prng == "philox" else Q.PRNG_RANLUX
+    cfg = Q.default_config(group=3, size=args.size, precision=0, start=Q.START_COLD, prng=prng, beta=BETA,
+                           n_or=N_OR, reunit_every=REUNIT_EVERY, reunit_fp64=1, randseries=54 + rank,
+                           prng_instances=16384)
+    L = Q.Lattice(cfg)
+    L.seed()
+    L.init()
+    L.sweep(2)                                  # leave the cold start before timing
+    stream = torch.cuda.ExternalStream(L.stream())
+    V = args.size ** 4
+    updates_per_step = 4 * V * (1 + N_OR)
+
+    for _ in range(args.warmup):
+        L.sweep(1)
+    L.sync()
+    clocks = ClockSampler(local)
+    clocks.start()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    L.sweep(args.steps)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    if dist:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+        dist.barrier()
+    clk = clocks.stop()
+    value = world * updates_per_step * args.steps / (ms / 1e3)
+
+    # dominant kernel: time single heatbath / overrelaxation phase launches
+    def time_phases(kind, reps=16):
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(2 * reps)]
+        for i in range(reps):
+            ev[2 * i].record(stream)
+            L.phase(i % 2, (i // 2) % 4, kind)
+            ev[2 * i + 1].record(stream)
+        torch.cuda.synchronize()
+        return statistics.mean(ev[2 * i].elapsed_time(ev[2 * i + 1]) for i in range(reps))
+
+    ms_hb = time_phases(Q.HEATBATH)
+    ms_or = time_phases(Q.OVERRELAX)
+    share_hb, share_or = 8 * ms_hb, 8 * N_OR * ms_or
+    dom, dom_ms = ("heatbath", ms_hb) if share_hb >= share_or else ("overrelaxation", ms_or)
+    alg_bytes = 4.5 * V * LINK_BYTES                # per phase launch (compulsory traffic)
+    peak, peak_kind = peaks()
+    achieved = alg_bytes / (dom_ms / 1e3) / 1e9
+    traffic = None
+    tr = profile_traffic()
+    if tr and dom in tr:
+        traffic = tr[dom]["dram_bytes_per_site"] * V / 2
+
+    # end to end through the C-ABI: per step the run parameters go host ->
+    # device from pinned staging (qg_set_params), one sweep, and plaquette +
+    # Polyakov sums come back to host (qg_measure)
+    e2e_steps = max(3, args.steps // 2)
+    L.sync()
+    if dist:
+        dist.barrier()
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        L.set_params(BETA)
+        L.sweep(1)
+        L.plaquette_sums()
+        L.polyakov_sums()
+    t1 = time.perf_counter()
+    e2e_s = t1 - t0
+    if dist:
+        t = torch.tensor([e2e_s], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    e2e = world * updates_per_step * e2e_steps / e2e_s
+
+    plq = L.plaquette()
+    first = 2 + args.warmup
+    reunits = sum(1 for n in range(first + 1, first + args.steps + 1) if n % REUNIT_EVERY == 0)
+    launches = args.steps * (8 + 8 * N_OR + (1 if prng == Q.PRNG_PHILOX else 0)) + reunits
+    if prng == Q.PRNG_RANLUX:
+        launches += 8 * args.steps
+    L.close()
+    if dist:
+        dist.destroy_process_group()
+    if rank != 0:
+        return 0
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic (cold start, %d untimed sweeps)" % (2 + args.warmup),
+        "config": {"workload": "SU(3) %d^4 beta=%.1f, FP32 12-real links, 1 HB + %d OR per sweep, FP64 reunit every %d"
+                               % (args.size, BETA, N_OR, REUNIT_EVERY),
+                   "global_batch": world, "lattice": [args.size] * 4, "prng": args.prng,
+                   "parallelism": "replicas x%d" % world, "l2": "field 201 MB > 126 MB L2, no flush"},
+        "roofline": {"bound": "hbm", "kernel": dom + " phase", "achieved": achieved, "peak": peak,
+                     "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
+                     "algorithmic_bytes_per_launch": alg_bytes, "ms_per_launch": dom_ms,
+                     "ms_per_launch_hb": ms_hb, "ms_per_launch_or": ms_or},
+        "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": 32, "d2h_bytes_per_step": 48,
+                "what": "qg_set_params + qg_sweep + plaquette/Polyakov read back, host wall clock"},
+        "gpu_launches": launches,
+        "clocks": clk,
+        "plaquette": plq[2],
+    }
+    if not args.no_cpu_baseline and world == 1:
+        line["cpu_baseline"] = cpu_baseline_line(args.size)
+    print(json.dumps(line))
+    return 0
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return run_reference_arm(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,168 @@
+/*
+ * qcdgpu_b200.h -- C-ABI of the B200 lattice sweep library (libqg_sun.so).
+ *
+ * This interface replaces the OpenCL kernel-ID layer through which the
+ * QCDGPU reference (vadimdi/QCDGPU) drives its SU(2)/SU(3) Monte Carlo
+ * sweep: GPU_CL::GPU::program_create / kernel_init / kernel_init_buffer /
+ * kernel_init_constant / kernel_run / buffer_init / buffer_map
+ * (SU(N)/clinterface/clinterface.cpp:921-1539) as called by
+ * model_CL::model::lattice_make_programs / lattice_simulate /
+ * lattice_analysis (SU(N)/suncl/suncl.cpp:3265-3648, 5212-5505, 1328-1612)
+ * and PRNG_CL::PRNG::initialize / produce (SU(N)/random/random.cpp:216-284).
+ *
+ * Conventions: plain pointers and sizes only; every call returns an int
+ * status (QG_OK = 0, negative on error; the message is in qg_last_error);
+ * nothing exits, aborts or traps.  A context owns all device memory and
+ * one CUDA stream; calls are asynchronous on that stream except those that
+ * return host data, which synchronise it.  Contexts are independent: one
+ * host thread per GPU may drive its own context.
+ */
+#ifndef QCDGPU_B200_H
+#define QCDGPU_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define QG_OK              0
+#define QG_ERR_ARG        -1
+#define QG_ERR_CUDA       -2
+#define QG_ERR_STATE      -3
+#define QG_ERR_NOMEM      -4
+#define QG_ERR_IO         -5
+#define QG_ERR_UNSUPPORTED -6
+
+/* start types: the reference's INTS key (0=hot, 1=cold, 2=gid),
+ * SU(N)/suncl/suncl.cpp:725-730; QG_START_HAAR is new (Haar-distributed). */
+#define QG_START_HOT   0
+#define QG_START_COLD  1
+#define QG_START_GID   2
+#define QG_START_HAAR  3
+
+/* PRN streams */
+#define QG_PRNG_RANLUX 0   /* reference layout: RANLUX batch before every heatbath phase */
+#define QG_PRNG_PHILOX 1   /* counter-based stream generated in registers              */
+
+/* link layouts for upload/download */
+#define QG_LAYOUT_REFERENCE 0  /* reference SoA planes, site index = lexicographic gid   */
+
+/* update kinds */
+#define QG_UPDATE_HEATBATH 0
+#define QG_UPDATE_OVERRELAX 1
+
+/* measurements (qg_measure) */
+#define QG_MEAS_PLAQUETTE 0   /* out[0..1] = sum ReTr spatial / temporal plaquettes     */
+#define QG_MEAS_ACTION    1   /* out[0..1] = sum (beta/N)(3N - ReTr) spatial / temporal */
+#define QG_MEAS_POLYAKOV  2   /* out[0..3] = sum Re P, Im P, |P|^2, |P|^4 (traces)      */
+#define QG_MEAS_WILSON    3   /* out[0]    = sum ReTr W(R,T) over sites and x,y,z       */
+
+typedef struct qg_ctx qg_ctx;
+
+/* Run configuration.  Field meanings follow the reference's init.dat keys
+ * and model defaults (SU(N)/QCDGPU.cpp:98-220, SU(N)/suncl/suncl.cpp:289-464). */
+typedef struct qg_config {
+    int group;            /* GROUP: 2 or 3                                   */
+    int size[4];          /* L1..L4 (N1=x, N2=y, N3=z, N4=t); N2 even        */
+    int precision;        /* 0 = FP32 links, 1 = FP64 links                  */
+    int start;            /* INTS / QG_START_*                               */
+    double beta;          /* BETA                                            */
+    double phi, omega;    /* PHI, OMEGA: twisted boundary (0,0 = periodic)   */
+    int nhit;             /* NHIT: Kennedy-Pendleton tries                   */
+    int nhitpar;          /* NHITPar                                         */
+    int prng;             /* QG_PRNG_*                                       */
+    int ranlux_nskip;     /* 24, 48, 97, 223 (RANLUX3), 389                  */
+    int prng_instances;   /* RANLUX generator instances                      */
+    uint32_t randseries;  /* RANDSERIES (seed; 0 is rejected)                */
+    int row_align;        /* alignment of ROWSIZE / PRNGSTEP                 */
+    int n_or;             /* overrelaxation sweeps after each heatbath sweep */
+    int reunit_every;     /* global reunitarisation every n sweeps (0=never) */
+    int reunit_fp64;      /* 1: global reunitarisation in FP64               */
+    int wilson_r, wilson_t; /* WILSONR, WILSONT                              */
+} qg_config;
+
+typedef struct qg_info {
+    uint32_t sites;       /* V                                               */
+    uint32_t rowsize;     /* ROWSIZE of the reference layout                 */
+    uint32_t prngstep;    /* PRNGSTEP                                        */
+    uint32_t prng_samples;/* float4 per RANLUX instance per batch            */
+    uint64_t link_bytes;  /* device bytes of the link field                  */
+    uint64_t ref_elems;   /* Real elements of a reference-layout table       */
+    uint64_t prn_quads;   /* float4 in one RANLUX batch                      */
+    uint64_t phase_counter;/* Philox phase counter (next phase)              */
+    uint32_t prng_counter;/* RANLUX batches produced (PRNG_counter)          */
+} qg_info;
+
+/* defaults of the reference main() where it has one (QCDGPU.cpp:98-220) */
+int qg_default_config(qg_config *cfg);
+
+/* model::lattice_init + lattice_create_buffers (suncl.cpp:672-706,3877-3991):
+ * validates cfg, allocates the field, PRN and measurement buffers. */
+int qg_create(const qg_config *cfg, qg_ctx **out);
+int qg_destroy(qg_ctx *ctx);
+const char *qg_last_error(const qg_ctx *ctx);  /* ctx may be NULL (last create error) */
+int qg_get_info(qg_ctx *ctx, qg_info *info);
+int qg_sync(qg_ctx *ctx);
+
+/* PRNG::initialize (random.cpp:216-277): glibc srand(series) seeding of all
+ * RANLUX instances, then one produce(); in Philox mode sets the key.      */
+int qg_prng_seed(qg_ctx *ctx, uint32_t randseries);
+/* Host only (no GPU needed): the RANLUX instance seeds PRNG::initialize
+ * derives from RANDSERIES -- instance 0 = rand() % (2^31-1), instances
+ * 1..n-1 = the next rand() values after srand(series) (random.cpp:228-235,
+ * 462-465, 508) -- computed on a private glibc random_r state.           */
+int qg_glibc_seeds(uint32_t randseries, int n, uint32_t *seeds);
+/* PRNG::produce (random.cpp:278-284): one reference-layout RANLUX batch.  */
+int qg_prng_produce(qg_ctx *ctx);
+int qg_prns_upload(qg_ctx *ctx, const float *host_quads, uint64_t nquads);
+int qg_prns_download(qg_ctx *ctx, float *host_quads, uint64_t nquads);
+
+/* lattice_init_{cold,gid,hot_X..T} kernels and their PRN cadence
+ * (suncl.cl:56-347, suncl.cpp:5236-5252).                                 */
+int qg_init_links(qg_ctx *ctx, int start);
+
+/* one update_{even,odd}_{X,Y,Z,T} kernel (suncl.cl:399-975) or its
+ * overrelaxation counterpart; parity 0 = even, 1 = odd.  In RANLUX mode the
+ * caller produces the batch first, as lattice_simulate does.              */
+int qg_phase(qg_ctx *ctx, int parity, int dir, int kind);
+/* the reference's working sweep (suncl.cpp:5393-5412): for each of odd
+ * X,Y,Z,T, even X,Y,Z,T a RANLUX batch (RANLUX mode) and a heatbath phase,
+ * then cfg.n_or overrelaxation sweeps in the same phase order, and a
+ * global reunitarisation when the sweep count hits cfg.reunit_every.
+ * Replayed from a captured CUDA graph.                                    */
+int qg_sweep(qg_ctx *ctx, int nsweeps);
+/* lattice_GramSchmidt kernel (suncl.cl:350-396); fp64 != 0 computes in FP64 */
+int qg_reunitarize(qg_ctx *ctx, int fp64);
+
+/* lattice_measurement_plq / lattice_measurement / lattice_polyakov /
+ * lattice_measurement_wilson + their reductions (sun_measurements_cl.cl:
+ * 55-184,1178-1357; polyakov.cl:54-140,405-432; wilson_loop.cl:55-465).
+ * Results are raw lattice sums (normalise as suncl.cpp:1328-1612 does).
+ * Synchronous: out is host memory.                                        */
+int qg_measure(qg_ctx *ctx, int what, double *out);
+/* same, generalised Wilson loop of extent R x T (config keys WILSONR/T)   */
+int qg_measure_wilson(qg_ctx *ctx, int R, int T, double *out);
+
+/* buffer_init / buffer_map of the link table (clinterface.cpp:1296-1434):
+ * host arrays in the reference layout, Real = float (precision 0) or
+ * double (precision 1), qg_info.ref_elems elements.                       */
+int qg_links_upload(qg_ctx *ctx, const void *host, int layout);
+int qg_links_download(qg_ctx *ctx, void *host, int layout);
+
+/* the per-run parameter block the kernels read from device memory, as
+ * the reference's lattice_parameters buffer {BETA/N, PHI, OMEGA}
+ * (suncl.cpp:3936-3949): stream-ordered host->device copy from pinned
+ * staging; later sweeps and measurements use the new values.            */
+int qg_set_params(qg_ctx *ctx, double beta, double phi, double omega);
+/* the context's CUDA stream (cudaStream_t), for event timing / interop   */
+int qg_get_stream(qg_ctx *ctx, void **stream);
+
+/* Philox phase counter (fast mode): read / set for checkpoint and resume */
+int qg_set_phase_counter(qg_ctx *ctx, uint64_t counter);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -12,6 +12,10 @@
 //   ref_cpurun bench <group> <L1> <L2> <L3> <L4> <beta> <randseries> <warm> <timed>
 //       cold start, <warm> untimed sweeps, then times <timed> sweeps and
 //       prints "link_updates_per_s <value> seconds <t>"
+//   ref_cpurun phases <group> <L1> <L2> <L3> <L4> <beta> <randseries> <warm> <timed>
+//       cold start, <warm> untimed phases, then <timed> phases (the sweep's
+//       odd X..T, even X..T order, V/2 link updates each); prints
+//       "phase_seconds t1 t2 ..."
 #include <chrono>
 #include <cstdio>
 #include <cstdlib>
@@ -30,6 +34,14 @@ static void sweep(modelCPU<su_n> *lat, PRNG_CL::PRNG *prng)
     lattice_update_even(lat, Y, prng);
     lattice_update_even(lat, Z, prng);
     lattice_update_even(lat, T, prng);
+}
+
+template <typename su_n>
+static void phase(modelCPU<su_n> *lat, PRNG_CL::PRNG *prng, int k)
+{
+    int dir = k % 4;
+    if ((k / 4) % 2 == 0) lattice_update_odd(lat, dir, prng);
+    else lattice_update_even(lat, dir, prng);
 }
 
 template <typename su_n>
@@ -58,6 +70,16 @@ static int run(int mode, int group, int *L, double beta, int ints, int series, i
             hgpu_complex p = plqConf(lat, &tot);
             printf("%d %.17g %.17g %.17g\n", s, (double)p.re, (double)p.im, (double)tot);
         }
+    } else if (mode == 2) {
+        for (int k = 0; k < a; k++) phase(lat, prng, k);
+        printf("phase_seconds");
+        for (int k = a; k < a + b; k++) {
+            auto t0 = std::chrono::steady_clock::now();
+            phase(lat, prng, k);
+            auto t1 = std::chrono::steady_clock::now();
+            printf(" %.6f", std::chrono::duration<double>(t1 - t0).count());
+        }
+        printf("\n");
     } else {
         for (int s = 0; s < a; s++) sweep(lat, prng);
         auto t0 = std::chrono::steady_clock::now();
@@ -79,14 +101,13 @@ static int run(int mode, int group, int *L, double beta, int ints, int series, i
 int main(int argc, char **argv)
 {
     if (argc < 11) { fprintf(stderr, "see source for usage\n"); return 2; }
-    int mode = strcmp(argv[1], "plaq") == 0 ? 0 : 1;
+    int mode = strcmp(argv[1], "plaq") == 0 ? 0 : strcmp(argv[1], "phases") == 0 ? 2 : 1;
     int group = atoi(argv[2]);
     int L[4] = { atoi(argv[3]), atoi(argv[4]), atoi(argv[5]), atoi(argv[6]) };
     double beta = atof(argv[7]);
     if (mode == 0)
         return group == 3 ? run<su_3>(0, 3, L, beta, atoi(argv[8]), atoi(argv[9]), atoi(argv[10]), 0)
                           : run<su_2>(0, 2, L, beta, atoi(argv[8]), atoi(argv[9]), atoi(argv[10]), 0);
-    if (argc < 11) return 2;
-    return group == 3 ? run<su_3>(1, 3, L, beta, 1, atoi(argv[8]), atoi(argv[9]), atoi(argv[10]))
-                      : run<su_2>(1, 2, L, beta, 1, atoi(argv[8]), atoi(argv[9]), atoi(argv[10]));
+    return group == 3 ? run<su_3>(mode, 3, L, beta, 1, atoi(argv[8]), atoi(argv[9]), atoi(argv[10]))
+                      : run<su_2>(mode, 2, L, beta, 1, atoi(argv[8]), atoi(argv[9]), atoi(argv[10]));
 }

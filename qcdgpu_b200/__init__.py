@@ -1,0 +1,276 @@
+"""qcdgpu_b200 -- B200-native SU(2)/SU(3) lattice Monte Carlo sweep.
+
+Python binding (ctypes) of the C-ABI in include/qcdgpu_b200.h, implemented
+by hand-written sm_100a CUDA kernels in qcdgpu_b200/lib/libqg_sun.so.  The
+binding mirrors the reference's model interface (vadimdi/QCDGPU,
+SU(N)/suncl/suncl.h: lattice_init / lattice_simulate / lattice_analysis);
+there is no CPU fallback: if the CUDA library is missing, importing the
+runtime raises.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+PKG_DIR = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(PKG_DIR, "lib", "libqg_sun.so")
+
+QG_OK = 0
+START_HOT, START_COLD, START_GID, START_HAAR = 0, 1, 2, 3
+PRNG_RANLUX, PRNG_PHILOX = 0, 1
+LAYOUT_REFERENCE = 0
+HEATBATH, OVERRELAX = 0, 1
+MEAS_PLAQUETTE, MEAS_ACTION, MEAS_POLYAKOV, MEAS_WILSON = 0, 1, 2, 3
+
+EXPORTED_SYMBOLS = (
+    "qg_default_config", "qg_create", "qg_destroy", "qg_last_error", "qg_get_info", "qg_sync",
+    "qg_prng_seed", "qg_prng_produce", "qg_prns_upload", "qg_prns_download", "qg_init_links",
+    "qg_phase", "qg_sweep", "qg_reunitarize", "qg_measure", "qg_measure_wilson",
+    "qg_links_upload", "qg_links_download", "qg_set_phase_counter", "qg_glibc_seeds", "qg_set_params", "qg_get_stream",
+)
+
+
+class Config(ctypes.Structure):
+    _fields_ = [
+        ("group", ctypes.c_int),
+        ("size", ctypes.c_int * 4),
+        ("precision", ctypes.c_int),
+        ("start", ctypes.c_int),
+        ("beta", ctypes.c_double),
+        ("phi", ctypes.c_double),
+        ("omega", ctypes.c_double),
+        ("nhit", ctypes.c_int),
+        ("nhitpar", ctypes.c_int),
+        ("prng", ctypes.c_int),
+        ("ranlux_nskip", ctypes.c_int),
+        ("prng_instances", ctypes.c_int),
+        ("randseries", ctypes.c_uint32),
+        ("row_align", ctypes.c_int),
+        ("n_or", ctypes.c_int),
+        ("reunit_every", ctypes.c_int),
+        ("reunit_fp64", ctypes.c_int),
+        ("wilson_r", ctypes.c_int),
+        ("wilson_t", ctypes.c_int),
+    ]
+
+
+class Info(ctypes.Structure):
+    _fields_ = [
+        ("sites", ctypes.c_uint32),
+        ("rowsize", ctypes.c_uint32),
+        ("prngstep", ctypes.c_uint32),
+        ("prng_samples", ctypes.c_uint32),
+        ("link_bytes", ctypes.c_uint64),
+        ("ref_elems", ctypes.c_uint64),
+        ("prn_quads", ctypes.c_uint64),
+        ("phase_counter", ctypes.c_uint64),
+        ("prng_counter", ctypes.c_uint32),
+    ]
+
+
+_lib = None
+
+
+class QGError(RuntimeError):
+    pass
+
+
+def load_library(path=LIB_PATH):
+    """Load libqg_sun.so and declare the C-ABI; raises if it is not built."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise QGError("CUDA library %s is not built (run __graft_entry__.build() or "
+                      "python qcdgpu_b200/build.py)" % path)
+    lib = ctypes.CDLL(path)
+    P = ctypes.POINTER
+    vp = ctypes.c_void_p
+    lib.qg_default_config.argtypes = [P(Config)]
+    lib.qg_create.argtypes = [P(Config), P(vp)]
+    lib.qg_destroy.argtypes = [vp]
+    lib.qg_last_error.argtypes = [vp]
+    lib.qg_last_error.restype = ctypes.c_char_p
+    lib.qg_get_info.argtypes = [vp, P(Info)]
+    lib.qg_sync.argtypes = [vp]
+    lib.qg_prng_seed.argtypes = [vp, ctypes.c_uint32]
+    lib.qg_prng_produce.argtypes = [vp]
+    lib.qg_prns_upload.argtypes = [vp, vp, ctypes.c_uint64]
+    lib.qg_prns_download.argtypes = [vp, vp, ctypes.c_uint64]
+    lib.qg_init_links.argtypes = [vp, ctypes.c_int]
+    lib.qg_phase.argtypes = [vp, ctypes.c_int, ctypes.c_int, ctypes.c_int]
+    lib.qg_sweep.argtypes = [vp, ctypes.c_int]
+    lib.qg_reunitarize.argtypes = [vp, ctypes.c_int]
+    lib.qg_measure.argtypes = [vp, ctypes.c_int, P(ctypes.c_double)]
+    lib.qg_measure_wilson.argtypes = [vp, ctypes.c_int, ctypes.c_int, P(ctypes.c_double)]
+    lib.qg_links_upload.argtypes = [vp, vp, ctypes.c_int]
+    lib.qg_links_download.argtypes = [vp, vp, ctypes.c_int]
+    lib.qg_set_phase_counter.argtypes = [vp, ctypes.c_uint64]
+    lib.qg_glibc_seeds.argtypes = [ctypes.c_uint32, ctypes.c_int, P(ctypes.c_uint32)]
+    lib.qg_set_params.argtypes = [vp, ctypes.c_double, ctypes.c_double, ctypes.c_double]
+    lib.qg_get_stream.argtypes = [vp, P(vp)]
+    _lib = lib
+    return lib
+
+
+def glibc_seeds(randseries, n):
+    """RANLUX instance seeds for RANDSERIES (host only, no GPU needed)."""
+    lib = load_library()
+    out = np.zeros(n, dtype=np.uint32)
+    rc = lib.qg_glibc_seeds(randseries, n, out.ctypes.data_as(ctypes.POINTER(ctypes.c_uint32)))
+    if rc != QG_OK:
+        raise QGError("qg_glibc_seeds failed")
+    return out
+
+
+def default_config(**kw):
+    """qg_default_config (the reference main()'s defaults) overridden by kw;
+    `size` may be an int (L^4) or a 4-tuple (L1..L4)."""
+    lib = load_library()
+    c = Config()
+    lib.qg_default_config(ctypes.byref(c))
+    for k, v in kw.items():
+        if k == "size":
+            v = (v,) * 4 if isinstance(v, int) else tuple(v)
+            for i in range(4):
+                c.size[i] = int(v[i])
+        else:
+            if not hasattr(c, k):
+                raise KeyError(k)
+            setattr(c, k, v)
+    return c
+
+
+class Lattice:
+    """One lattice on one GPU (a qg_ctx).  Mirrors model_CL::model."""
+
+    def __init__(self, cfg=None, **kw):
+        self.lib = load_library()
+        self.cfg = cfg if cfg is not None else default_config(**kw)
+        self.ctx = ctypes.c_void_p()
+        rc = self.lib.qg_create(ctypes.byref(self.cfg), ctypes.byref(self.ctx))
+        if rc != QG_OK:
+            raise QGError("qg_create: %s" % self.lib.qg_last_error(None).decode())
+
+    def _ck(self, rc, what):
+        if rc != QG_OK:
+            raise QGError("%s: %s" % (what, self.lib.qg_last_error(self.ctx).decode()))
+
+    def close(self):
+        if self.ctx:
+            self.lib.qg_destroy(self.ctx)
+            self.ctx = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    # ---- setup
+    def info(self):
+        i = Info()
+        self._ck(self.lib.qg_get_info(self.ctx, ctypes.byref(i)), "qg_get_info")
+        return i
+
+    def seed(self, randseries=None):
+        self._ck(self.lib.qg_prng_seed(self.ctx, self.cfg.randseries if randseries is None else randseries),
+                 "qg_prng_seed")
+
+    def produce(self):
+        self._ck(self.lib.qg_prng_produce(self.ctx), "qg_prng_produce")
+
+    def init(self, start=None):
+        self._ck(self.lib.qg_init_links(self.ctx, self.cfg.start if start is None else start), "qg_init_links")
+
+    # ---- updates
+    def phase(self, parity, direction, kind=HEATBATH):
+        self._ck(self.lib.qg_phase(self.ctx, parity, direction, kind), "qg_phase")
+
+    def sweep(self, n=1):
+        self._ck(self.lib.qg_sweep(self.ctx, n), "qg_sweep")
+
+    def reunitarize(self, fp64=False):
+        self._ck(self.lib.qg_reunitarize(self.ctx, 1 if fp64 else 0), "qg_reunitarize")
+
+    def sync(self):
+        self._ck(self.lib.qg_sync(self.ctx), "qg_sync")
+
+    def set_params(self, beta, phi=0.0, omega=0.0):
+        self._ck(self.lib.qg_set_params(self.ctx, beta, phi, omega), "qg_set_params")
+        self.cfg.beta, self.cfg.phi, self.cfg.omega = beta, phi, omega
+
+    def stream(self):
+        s = ctypes.c_void_p()
+        self._ck(self.lib.qg_get_stream(self.ctx, ctypes.byref(s)), "qg_get_stream")
+        return s.value
+
+    def set_phase_counter(self, v):
+        self._ck(self.lib.qg_set_phase_counter(self.ctx, v), "qg_set_phase_counter")
+
+    # ---- measurements (raw lattice sums, see include/qcdgpu_b200.h)
+    def _measure(self, what, n):
+        out = (ctypes.c_double * 4)()
+        self._ck(self.lib.qg_measure(self.ctx, what, out), "qg_measure")
+        return tuple(out[:n])
+
+    def plaquette_sums(self):
+        return self._measure(MEAS_PLAQUETTE, 2)
+
+    def action_sums(self):
+        return self._measure(MEAS_ACTION, 2)
+
+    def polyakov_sums(self):
+        return self._measure(MEAS_POLYAKOV, 4)
+
+    def wilson_sum(self, R=None, T=None):
+        out = (ctypes.c_double * 1)()
+        R = self.cfg.wilson_r if R is None else R
+        T = self.cfg.wilson_t if T is None else T
+        self._ck(self.lib.qg_measure_wilson(self.ctx, R, T, out), "qg_measure_wilson")
+        return out[0]
+
+    def plaquette(self):
+        """(Plq_spat, Plq_temp, Plq_total) normalised as lattice_analysis
+        does (SU(N)/suncl/suncl.cpp:1357-1373): sum / (3V), range [-N, N]."""
+        s, t = self.plaquette_sums()
+        V = self.info().sites
+        return s / (3 * V), t / (3 * V), (s + t) / (6 * V)
+
+    def polyakov(self):
+        """(Re P, Im P, P2, P4) normalised as suncl.cpp:1483-1494,1591-1605."""
+        re, im, p2, p4 = self.polyakov_sums()
+        n = self.cfg.size[0] * self.cfg.size[1] * self.cfg.size[2]
+        N = self.cfg.group
+        return re / (n * N), im / (n * N), p2 / (n * N * N), p4 / (n * N ** 4)
+
+    # ---- link table I/O in the reference layout
+    def _ref_dtype(self):
+        return np.float64 if self.cfg.precision else np.float32
+
+    def download(self):
+        a = np.zeros(self.info().ref_elems, dtype=self._ref_dtype())
+        self._ck(self.lib.qg_links_download(self.ctx, a.ctypes.data, LAYOUT_REFERENCE), "qg_links_download")
+        return a
+
+    def upload(self, a):
+        a = np.ascontiguousarray(a, dtype=self._ref_dtype())
+        if a.size != self.info().ref_elems:
+            raise ValueError("link table has %d elements, expected %d" % (a.size, self.info().ref_elems))
+        self._ck(self.lib.qg_links_upload(self.ctx, a.ctypes.data, LAYOUT_REFERENCE), "qg_links_upload")
+
+    def prns_download(self, nquads=None):
+        n = self.info().prn_quads if nquads is None else nquads
+        a = np.zeros(n * 4, dtype=np.float32)
+        self._ck(self.lib.qg_prns_download(self.ctx, a.ctypes.data, n), "qg_prns_download")
+        return a
+
+    def prns_upload(self, a):
+        a = np.ascontiguousarray(a, dtype=np.float32)
+        self._ck(self.lib.qg_prns_upload(self.ctx, a.ctypes.data, a.size // 4), "qg_prns_upload")

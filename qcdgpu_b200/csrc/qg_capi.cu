@@ -1,0 +1,561 @@
+// qg_capi.cu -- the C-ABI of include/qcdgpu_b200.h: context, buffers,
+// PRN cadence, sweep graphs and measurements on one CUDA stream.
+#include <stdlib.h>
+#include <string.h>
+
+#include <new>
+#include <string>
+#include <vector>
+
+#include "qg_internal.h"
+
+using namespace qg;
+
+struct qg_ctx {
+    qg_config cfg;
+    Geom G;
+    uint32_t rowsize = 0, prngstep = 0, samples = 0;
+    int instances = 0;
+    size_t link_bytes = 0;
+    void *links = nullptr;
+    float4 *prns = nullptr;
+    float4 *rl_table = nullptr;
+    uint32_t *d_seeds = nullptr;
+    double *partials = nullptr;
+    size_t partials_n = 0;
+    double *d_results = nullptr;
+    double *h_results = nullptr;    // pinned
+    uint64_t *d_phase = nullptr;
+    double *d_params = nullptr;     // {BETA/N, PHI, OMEGA, 0}: lattice_parameters
+    double *h_params = nullptr;     // pinned staging
+    int twist_built = 0;            // twist flag the cached graphs were built with
+    uint64_t phase_counter = 0;     // host mirror of *d_phase
+    uint32_t prng_counter = 0;      // RANLUX batches produced
+    uint64_t sweeps_done = 0;
+    uint2 key = { 0, 0 };
+    bool seeded = false;
+    cudaStream_t stream = nullptr;
+    cudaGraphExec_t graph[2] = { nullptr, nullptr };  // sweep without / with reunitarisation
+    std::string err;
+};
+
+static thread_local std::string g_create_err;
+
+static int fail(qg_ctx *c, int code, const std::string &msg)
+{
+    if (c) c->err = msg; else g_create_err = msg;
+    return code;
+}
+static int cuda_fail(qg_ctx *c, cudaError_t e, const char *where)
+{
+    return fail(c, QG_ERR_CUDA, std::string(where) + ": " + cudaGetErrorString(e));
+}
+#define QG_CK(call, where) do { cudaError_t e_ = (call); if (e_ != cudaSuccess) return cuda_fail(c, e_, where); } while (0)
+
+static uint32_t align_up(uint64_t n, uint32_t a) { return (uint32_t)(((n + a - 1) / a) * a); }
+
+extern "C" int qg_default_config(qg_config *cfg)
+{
+    if (!cfg) return QG_ERR_ARG;
+    memset(cfg, 0, sizeof(*cfg));
+    cfg->group = 3;
+    for (int i = 0; i < 4; i++) cfg->size[i] = 32;
+    cfg->precision = 1;
+    cfg->start = QG_START_COLD;
+    cfg->beta = 6.5;
+    cfg->nhit = 10;
+    cfg->nhitpar = 1;
+    cfg->prng = QG_PRNG_RANLUX;
+    cfg->ranlux_nskip = 223;
+    cfg->prng_instances = 16384;
+    cfg->randseries = 54;
+    cfg->row_align = 64;
+    cfg->n_or = 0;
+    cfg->reunit_every = 1;
+    cfg->reunit_fp64 = 0;
+    cfg->wilson_r = 7;
+    cfg->wilson_t = 2;
+    return QG_OK;
+}
+
+extern "C" const char *qg_last_error(const qg_ctx *c) { return c ? c->err.c_str() : g_create_err.c_str(); }
+
+static int validate(const qg_config *cfg, std::string &why)
+{
+    if (cfg->group != 2 && cfg->group != 3) { why = "GROUP must be 2 or 3"; return 0; }
+    for (int i = 0; i < 4; i++)
+        if (cfg->size[i] < 2 || cfg->size[i] > 4096) { why = "lattice extents must be in [2, 4096]"; return 0; }
+    if (cfg->size[1] % 2) { why = "L2 (y extent) must be even for the checkerboard"; return 0; }
+    uint64_t V = (uint64_t)cfg->size[0] * cfg->size[1] * cfg->size[2] * cfg->size[3];
+    if (V > (1ull << 31)) { why = "lattice volume exceeds 2^31 sites"; return 0; }
+    if (cfg->precision != 0 && cfg->precision != 1) { why = "precision must be 0 or 1"; return 0; }
+    if (cfg->start < 0 || cfg->start > 3) { why = "unknown start type"; return 0; }
+    if (cfg->nhit < 1 || cfg->nhit > 1000) { why = "NHIT must be in [1, 1000]"; return 0; }
+    if (cfg->nhitpar < 1 || cfg->nhitpar > 16) { why = "NHITPar must be in [1, 16]"; return 0; }
+    if (cfg->prng != QG_PRNG_RANLUX && cfg->prng != QG_PRNG_PHILOX) { why = "unknown PRNG"; return 0; }
+    int ns = cfg->ranlux_nskip;
+    if (ns != 24 && ns != 48 && ns != 97 && ns != 223 && ns != 389) { why = "RANLUX skip must be 24/48/97/223/389"; return 0; }
+    if (cfg->prng_instances < 1 || cfg->prng_instances > (1 << 24)) { why = "PRNG instances out of range"; return 0; }
+    if (cfg->randseries == 0) { why = "RANDSERIES 0 (time seeding) is not reproducible; give a seed"; return 0; }
+    if (cfg->row_align < 1 || cfg->row_align > 65536) { why = "row alignment out of range"; return 0; }
+    if (cfg->n_or < 0 || cfg->n_or > 64) { why = "n_or must be in [0, 64]"; return 0; }
+    if (cfg->reunit_every < 0) { why = "reunit_every must be >= 0"; return 0; }
+    if (cfg->wilson_r < 1 || cfg->wilson_t < 1) { why = "Wilson loop extents must be >= 1"; return 0; }
+    return 1;
+}
+
+static void destroy_graphs(qg_ctx *c)
+{
+    for (int i = 0; i < 2; i++)
+        if (c->graph[i]) { cudaGraphExecDestroy(c->graph[i]); c->graph[i] = nullptr; }
+}
+
+extern "C" int qg_destroy(qg_ctx *c)
+{
+    if (!c) return QG_OK;
+    if (c->stream) cudaStreamSynchronize(c->stream);
+    destroy_graphs(c);
+    cudaFree(c->links); cudaFree(c->prns); cudaFree(c->rl_table); cudaFree(c->d_seeds);
+    cudaFree(c->partials); cudaFree(c->d_results); cudaFree(c->d_phase); cudaFree(c->d_params);
+    if (c->h_results) cudaFreeHost(c->h_results);
+    if (c->h_params) cudaFreeHost(c->h_params);
+    if (c->stream) cudaStreamDestroy(c->stream);
+    delete c;
+    return QG_OK;
+}
+
+extern "C" int qg_create(const qg_config *cfg, qg_ctx **out)
+{
+    qg_ctx *c = nullptr;
+    if (!cfg || !out) return fail(nullptr, QG_ERR_ARG, "null argument");
+    *out = nullptr;
+    std::string why;
+    if (!validate(cfg, why)) return fail(nullptr, QG_ERR_ARG, why);
+    c = new (std::nothrow) qg_ctx;
+    if (!c) return fail(nullptr, QG_ERR_NOMEM, "host allocation failed");
+    c->cfg = *cfg;
+    c->G = make_geom(cfg->size);
+    const uint32_t V = c->G.V;
+    const uint32_t A = (uint32_t)cfg->row_align;
+    c->rowsize = align_up(V, A);
+    c->prngstep = align_up(V / 2, A);
+    c->instances = cfg->prng_instances;
+    uint64_t total;
+    if (cfg->start == QG_START_HOT)
+        total = align_up((uint64_t)c->rowsize * 4 + 3ull * c->prngstep * (cfg->nhit + 1), A);
+    else
+        total = align_up((uint64_t)cfg->nhitpar * 3ull * c->prngstep * (cfg->nhit + 1), A);
+    c->samples = (uint32_t)(1 + (total - 1) / (uint64_t)c->instances);
+    const int planes = cfg->group == 3 ? 12 : 4;
+    const size_t rsz = cfg->precision ? sizeof(double) : sizeof(float);
+    c->link_bytes = (size_t)planes * c->G.pstride * 4 * rsz;
+    c->partials_n = (size_t)((V + 127) / 128) * 4 + 64;
+    cudaError_t e;
+    auto bad = [&](const char *w) { int r = cuda_fail(nullptr, e, w); qg_destroy(c); return r; };
+    if ((e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking)) != cudaSuccess) return bad("cudaStreamCreate");
+    if ((e = cudaMalloc(&c->links, c->link_bytes)) != cudaSuccess) return bad("cudaMalloc(links)");
+    if ((e = cudaMemsetAsync(c->links, 0, c->link_bytes, c->stream)) != cudaSuccess) return bad("cudaMemset(links)");
+    if (cfg->prng == QG_PRNG_RANLUX) {
+        size_t nq = (size_t)c->instances * c->samples;
+        if ((e = cudaMalloc(&c->prns, nq * sizeof(float4))) != cudaSuccess) return bad("cudaMalloc(prns)");
+        if ((e = cudaMemsetAsync(c->prns, 0, nq * sizeof(float4), c->stream)) != cudaSuccess) return bad("cudaMemset(prns)");
+        if ((e = cudaMalloc(&c->rl_table, (size_t)7 * c->instances * sizeof(float4))) != cudaSuccess) return bad("cudaMalloc(table)");
+        if ((e = cudaMalloc(&c->d_seeds, (size_t)c->instances * sizeof(uint32_t))) != cudaSuccess) return bad("cudaMalloc(seeds)");
+    }
+    if ((e = cudaMalloc(&c->partials, c->partials_n * sizeof(double))) != cudaSuccess) return bad("cudaMalloc(partials)");
+    if ((e = cudaMalloc(&c->d_results, 64 * sizeof(double))) != cudaSuccess) return bad("cudaMalloc(results)");
+    if ((e = cudaMallocHost(&c->h_results, 64 * sizeof(double))) != cudaSuccess) return bad("cudaMallocHost");
+    if ((e = cudaMalloc(&c->d_phase, sizeof(uint64_t))) != cudaSuccess) return bad("cudaMalloc(phase)");
+    if ((e = cudaMemsetAsync(c->d_phase, 0, sizeof(uint64_t), c->stream)) != cudaSuccess) return bad("cudaMemset(phase)");
+    if ((e = cudaMalloc(&c->d_params, 4 * sizeof(double))) != cudaSuccess) return bad("cudaMalloc(params)");
+    if ((e = cudaMallocHost(&c->h_params, 4 * sizeof(double))) != cudaSuccess) return bad("cudaMallocHost(params)");
+    if ((e = cudaStreamSynchronize(c->stream)) != cudaSuccess) return bad("create sync");
+    if (qg_set_params(c, cfg->beta, cfg->phi, cfg->omega) != QG_OK) { g_create_err = c->err; qg_destroy(c); return QG_ERR_CUDA; }
+    *out = c;
+    return QG_OK;
+}
+
+static int twist_of(const qg_config &f) { return !(f.phi == 0.0 && f.omega == 0.0); }
+
+extern "C" int qg_set_params(qg_ctx *c, double beta, double phi, double omega)
+{
+    if (!c) return QG_ERR_ARG;
+    if (!(beta > 0.0)) return fail(c, QG_ERR_ARG, "BETA must be positive");
+    c->cfg.beta = beta;
+    c->cfg.phi = phi;
+    c->cfg.omega = omega;
+    QG_CK(cudaStreamSynchronize(c->stream), "params sync");   // staging buffer reuse
+    c->h_params[0] = beta / c->cfg.group;
+    c->h_params[1] = phi;
+    c->h_params[2] = omega;
+    c->h_params[3] = 0.0;
+    QG_CK(cudaMemcpyAsync(c->d_params, c->h_params, 4 * sizeof(double), cudaMemcpyHostToDevice, c->stream),
+          "params upload");
+    if (twist_of(c->cfg) != c->twist_built) destroy_graphs(c);
+    return QG_OK;
+}
+
+extern "C" int qg_get_stream(qg_ctx *c, void **stream)
+{
+    if (!c || !stream) return QG_ERR_ARG;
+    *stream = (void *)c->stream;
+    return QG_OK;
+}
+
+extern "C" int qg_get_info(qg_ctx *c, qg_info *info)
+{
+    if (!c || !info) return QG_ERR_ARG;
+    info->sites = c->G.V;
+    info->rowsize = c->rowsize;
+    info->prngstep = c->prngstep;
+    info->prng_samples = c->samples;
+    info->link_bytes = c->link_bytes;
+    info->ref_elems = (uint64_t)(c->cfg.group == 3 ? 12 : 4) * c->rowsize * 4;
+    info->prn_quads = (uint64_t)c->instances * c->samples;
+    info->phase_counter = c->phase_counter;
+    info->prng_counter = c->prng_counter;
+    return QG_OK;
+}
+
+extern "C" int qg_sync(qg_ctx *c)
+{
+    if (!c) return QG_ERR_ARG;
+    QG_CK(cudaStreamSynchronize(c->stream), "qg_sync");
+    return QG_OK;
+}
+
+// glibc rand() sequence after srand(seed): random_r on a private TYPE_3
+// (128-byte) state, so the process-wide rand() state is left alone.
+static void glibc_rand_seeds(uint32_t series, int n, std::vector<uint32_t> &out)
+{
+    struct random_data rd;
+    int32_t statebuf[32];
+    memset(&rd, 0, sizeof(rd));
+    memset(statebuf, 0, sizeof(statebuf));
+    initstate_r(series, (char *)statebuf, sizeof(statebuf), &rd);
+    srandom_r(series, &rd);
+    out.resize(n);
+    int32_t r;
+    random_r(&rd, &r);
+    out[0] = (uint32_t)(r % 2147483647);
+    for (int i = 1; i < n; i++) { random_r(&rd, &r); out[i] = (uint32_t)r; }
+}
+
+extern "C" int qg_glibc_seeds(uint32_t series, int n, uint32_t *seeds)
+{
+    if (n < 1 || !seeds) return QG_ERR_ARG;
+    std::vector<uint32_t> v;
+    glibc_rand_seeds(series, n, v);
+    memcpy(seeds, v.data(), (size_t)n * sizeof(uint32_t));
+    return QG_OK;
+}
+
+extern "C" int qg_prng_produce(qg_ctx *c)
+{
+    if (!c) return QG_ERR_ARG;
+    if (c->cfg.prng != QG_PRNG_RANLUX) return fail(c, QG_ERR_STATE, "qg_prng_produce needs the RANLUX stream");
+    if (!c->seeded) return fail(c, QG_ERR_STATE, "PRNG not seeded (qg_prng_seed)");
+    QG_CK(launch_ranlux_produce(c->rl_table, c->prns, c->instances, (int)c->samples, c->cfg.ranlux_nskip, c->stream),
+          "ranlux");
+    c->prng_counter++;
+    return QG_OK;
+}
+
+extern "C" int qg_prng_seed(qg_ctx *c, uint32_t series)
+{
+    if (!c) return QG_ERR_ARG;
+    if (series == 0) return fail(c, QG_ERR_ARG, "RANDSERIES 0 is not reproducible");
+    c->cfg.randseries = series;
+    destroy_graphs(c);
+    if (c->cfg.prng == QG_PRNG_RANLUX) {
+        std::vector<uint32_t> seeds;
+        glibc_rand_seeds(series, c->instances, seeds);
+        QG_CK(cudaMemcpyAsync(c->d_seeds, seeds.data(), seeds.size() * sizeof(uint32_t), cudaMemcpyHostToDevice,
+                              c->stream), "seed upload");
+        QG_CK(launch_ranlux_init(c->d_seeds, c->rl_table, c->instances, c->stream), "ranlux_init");
+        QG_CK(cudaStreamSynchronize(c->stream), "seed sync");
+        c->seeded = true;
+        c->prng_counter = 0;
+        return qg_prng_produce(c);   // PRNG::initialize ends with one produce()
+    }
+    c->key = make_uint2(series, 0x5D3E1A27u);
+    c->phase_counter = 0;
+    QG_CK(cudaMemsetAsync(c->d_phase, 0, sizeof(uint64_t), c->stream), "phase reset");
+    c->seeded = true;
+    return QG_OK;
+}
+
+extern "C" int qg_set_phase_counter(qg_ctx *c, uint64_t v)
+{
+    if (!c) return QG_ERR_ARG;
+    c->phase_counter = v;
+    QG_CK(cudaMemcpyAsync(c->d_phase, &c->phase_counter, sizeof(uint64_t), cudaMemcpyHostToDevice, c->stream),
+          "phase set");
+    QG_CK(cudaStreamSynchronize(c->stream), "phase set sync");
+    return QG_OK;
+}
+
+extern "C" int qg_prns_upload(qg_ctx *c, const float *h, uint64_t nq)
+{
+    if (!c || !h) return QG_ERR_ARG;
+    if (!c->prns) return fail(c, QG_ERR_STATE, "no PRN buffer (Philox mode)");
+    if (nq > (uint64_t)c->instances * c->samples) return fail(c, QG_ERR_ARG, "too many PRN quads");
+    QG_CK(cudaMemcpyAsync(c->prns, h, nq * sizeof(float4), cudaMemcpyHostToDevice, c->stream), "prns upload");
+    QG_CK(cudaStreamSynchronize(c->stream), "prns upload sync");
+    return QG_OK;
+}
+
+extern "C" int qg_prns_download(qg_ctx *c, float *h, uint64_t nq)
+{
+    if (!c || !h) return QG_ERR_ARG;
+    if (!c->prns) return fail(c, QG_ERR_STATE, "no PRN buffer (Philox mode)");
+    if (nq > (uint64_t)c->instances * c->samples) return fail(c, QG_ERR_ARG, "too many PRN quads");
+    QG_CK(cudaMemcpyAsync(h, c->prns, nq * sizeof(float4), cudaMemcpyDeviceToHost, c->stream), "prns download");
+    QG_CK(cudaStreamSynchronize(c->stream), "prns download sync");
+    return QG_OK;
+}
+
+extern "C" int qg_init_links(qg_ctx *c, int start)
+{
+    if (!c) return QG_ERR_ARG;
+    const qg_config &f = c->cfg;
+    cudaError_t e;
+    switch (start) {
+    case QG_START_COLD:
+        e = launch_init(c->G, c->links, f.group, f.precision, INIT_COLD, 0, nullptr, 0, c->key, c->stream);
+        break;
+    case QG_START_GID:
+        e = launch_init(c->G, c->links, f.group, f.precision, INIT_GID, 0, nullptr, 0, c->key, c->stream);
+        break;
+    case QG_START_HOT:
+        if (!c->seeded) return fail(c, QG_ERR_STATE, "hot start needs a seeded PRNG (qg_prng_seed)");
+        if (f.prng == QG_PRNG_RANLUX) {
+            // lattice_simulate: produce; init X; produce; init Y; produce; init Z; produce; init T
+            e = cudaSuccess;
+            for (int mu = 0; mu < 4 && e == cudaSuccess; mu++) {
+                int r = qg_prng_produce(c);
+                if (r) return r;
+                e = launch_init(c->G, c->links, f.group, f.precision, INIT_HOT_REF, mu, c->prns, c->rowsize, c->key,
+                                c->stream);
+            }
+        } else {
+            e = launch_init(c->G, c->links, f.group, f.precision, INIT_HOT_PHILOX, 0, nullptr, 0, c->key, c->stream);
+        }
+        break;
+    case QG_START_HAAR:
+        if (!c->seeded) return fail(c, QG_ERR_STATE, "Haar start needs a seeded PRNG (qg_prng_seed)");
+        e = launch_init(c->G, c->links, f.group, f.precision, INIT_HAAR, 0, nullptr, 0, c->key, c->stream);
+        break;
+    default:
+        return fail(c, QG_ERR_ARG, "unknown start type");
+    }
+    if (e != cudaSuccess) return cuda_fail(c, e, "init kernel");
+    return QG_OK;
+}
+
+static PhaseArgs phase_args(qg_ctx *c, int parity, int dir, int kind, uint32_t offset)
+{
+    const qg_config &f = c->cfg;
+    PhaseArgs a;
+    a.parity = parity;
+    a.dir = dir;
+    a.params = c->d_params;
+    a.twist = twist_of(f);
+    a.nhit = f.nhit;
+    a.nhitpar = f.nhitpar;
+    if (kind == QG_UPDATE_OVERRELAX) a.prn_mode = -1;
+    else if (f.start == QG_START_GID) a.prn_mode = 2;
+    else a.prn_mode = f.prng;
+    a.prns = c->prns;
+    a.prngstep = c->prngstep;
+    a.key = c->key;
+    a.phase_base = c->d_phase;
+    a.phase_offset = offset;
+    return a;
+}
+
+static cudaError_t launch_phase(qg_ctx *c, const PhaseArgs &a)
+{
+    return c->cfg.precision ? launch_phase_f64(c->G, c->links, c->cfg.group, a, c->stream)
+                            : launch_phase_f32(c->G, c->links, c->cfg.group, a, c->stream);
+}
+
+static bool needs_seed(const qg_ctx *c, int kind)
+{
+    return kind == QG_UPDATE_HEATBATH && c->cfg.start != QG_START_GID && !c->seeded;
+}
+
+extern "C" int qg_phase(qg_ctx *c, int parity, int dir, int kind)
+{
+    if (!c) return QG_ERR_ARG;
+    if ((parity != 0 && parity != 1) || dir < 0 || dir > 3) return fail(c, QG_ERR_ARG, "bad parity/direction");
+    if (kind != QG_UPDATE_HEATBATH && kind != QG_UPDATE_OVERRELAX) return fail(c, QG_ERR_ARG, "bad update kind");
+    if (needs_seed(c, kind)) return fail(c, QG_ERR_STATE, "heatbath needs a seeded PRNG (qg_prng_seed)");
+    PhaseArgs a = phase_args(c, parity, dir, kind, 0);
+    QG_CK(launch_phase(c, a), "phase kernel");
+    if (kind == QG_UPDATE_HEATBATH && a.prn_mode == QG_PRNG_PHILOX) {
+        QG_CK(launch_add_u64(c->d_phase, 1, c->stream), "phase counter");
+        c->phase_counter++;
+    }
+    return QG_OK;
+}
+
+extern "C" int qg_reunitarize(qg_ctx *c, int fp64)
+{
+    if (!c) return QG_ERR_ARG;
+    QG_CK(launch_gramschmidt(c->G, c->links, c->cfg.group, c->cfg.precision, fp64, c->stream), "gramschmidt");
+    return QG_OK;
+}
+
+// one sweep's launches: lattice_simulate's working-cycle body
+// (suncl.cpp:5393-5412) plus the overrelaxation sweeps
+static cudaError_t enqueue_sweep(qg_ctx *c, bool reunit)
+{
+    const qg_config &f = c->cfg;
+    cudaError_t e;
+    uint32_t hb = 0;
+    const int par_order[2] = { 1, 0 };   // odd first, then even
+    for (int pi = 0; pi < 2; pi++)
+        for (int mu = 0; mu < 4; mu++) {
+            PhaseArgs a = phase_args(c, par_order[pi], mu, QG_UPDATE_HEATBATH, hb);
+            if (a.prn_mode == QG_PRNG_RANLUX) {
+                e = launch_ranlux_produce(c->rl_table, c->prns, c->instances, (int)c->samples, f.ranlux_nskip, c->stream);
+                if (e != cudaSuccess) return e;
+            }
+            if ((e = launch_phase(c, a)) != cudaSuccess) return e;
+            if (a.prn_mode == QG_PRNG_PHILOX) hb++;
+        }
+    for (int k = 0; k < f.n_or; k++)
+        for (int pi = 0; pi < 2; pi++)
+            for (int mu = 0; mu < 4; mu++) {
+                PhaseArgs a = phase_args(c, par_order[pi], mu, QG_UPDATE_OVERRELAX, 0);
+                if ((e = launch_phase(c, a)) != cudaSuccess) return e;
+            }
+    if (hb) {
+        if ((e = launch_add_u64(c->d_phase, hb, c->stream)) != cudaSuccess) return e;
+    }
+    if (reunit) {
+        if ((e = launch_gramschmidt(c->G, c->links, f.group, f.precision, f.reunit_fp64, c->stream)) != cudaSuccess)
+            return e;
+    }
+    return cudaSuccess;
+}
+
+static int build_graph(qg_ctx *c, int which)
+{
+    cudaGraph_t g = nullptr;
+    QG_CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal), "begin capture");
+    cudaError_t e = enqueue_sweep(c, which == 1);
+    cudaError_t e2 = cudaStreamEndCapture(c->stream, &g);
+    if (e != cudaSuccess) { if (g) cudaGraphDestroy(g); return cuda_fail(c, e, "sweep capture"); }
+    if (e2 != cudaSuccess) return cuda_fail(c, e2, "end capture");
+    c->twist_built = twist_of(c->cfg);
+    e = cudaGraphInstantiate(&c->graph[which], g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) return cuda_fail(c, e, "graph instantiate");
+    return QG_OK;
+}
+
+extern "C" int qg_sweep(qg_ctx *c, int nsweeps)
+{
+    if (!c) return QG_ERR_ARG;
+    if (nsweeps < 0) return fail(c, QG_ERR_ARG, "negative sweep count");
+    if (needs_seed(c, QG_UPDATE_HEATBATH)) return fail(c, QG_ERR_STATE, "heatbath needs a seeded PRNG (qg_prng_seed)");
+    const qg_config &f = c->cfg;
+    const bool philox = (f.prng == QG_PRNG_PHILOX && f.start != QG_START_GID);
+    const bool ranlux = (f.prng == QG_PRNG_RANLUX && f.start != QG_START_GID);
+    for (int n = 0; n < nsweeps; n++) {
+        const bool reunit = f.reunit_every > 0 && ((c->sweeps_done + 1) % (uint64_t)f.reunit_every) == 0;
+        const int which = reunit ? 1 : 0;
+        if (!c->graph[which]) {
+            int r = build_graph(c, which);
+            if (r) return r;
+        }
+        QG_CK(cudaGraphLaunch(c->graph[which], c->stream), "graph launch");
+        c->sweeps_done++;
+        if (philox) c->phase_counter += 8;
+        if (ranlux) c->prng_counter += 8;
+    }
+    return QG_OK;
+}
+
+static int measure_to_host(qg_ctx *c, int ncomp, double *out)
+{
+    QG_CK(cudaMemcpyAsync(c->h_results, c->d_results, ncomp * sizeof(double), cudaMemcpyDeviceToHost, c->stream),
+          "result copy");
+    QG_CK(cudaStreamSynchronize(c->stream), "measure sync");
+    for (int i = 0; i < ncomp; i++) out[i] = c->h_results[i];
+    return QG_OK;
+}
+
+extern "C" int qg_measure_wilson(qg_ctx *c, int R, int T, double *out)
+{
+    if (!c || !out) return QG_ERR_ARG;
+    if (R < 1 || T < 1 || R > c->G.n[0] || T > c->G.n[3]) return fail(c, QG_ERR_ARG, "Wilson loop extent out of range");
+    const qg_config &f = c->cfg;
+    int tw = !(f.phi == 0.0 && f.omega == 0.0);
+    QG_CK(launch_wilson(c->G, c->links, f.group, f.precision, R, T, (float)f.phi, (float)f.omega, tw, c->partials,
+                        c->d_results, c->stream), "wilson");
+    return measure_to_host(c, 1, out);
+}
+
+extern "C" int qg_measure(qg_ctx *c, int what, double *out)
+{
+    if (!c || !out) return QG_ERR_ARG;
+    const qg_config &f = c->cfg;
+    int tw = !(f.phi == 0.0 && f.omega == 0.0);
+    switch (what) {
+    case QG_MEAS_PLAQUETTE:
+    case QG_MEAS_ACTION: {
+        QG_CK(launch_plaquette(c->G, c->links, f.group, f.precision, f.beta / f.group, (float)f.phi, (float)f.omega, tw,
+                               c->partials, c->d_results, c->stream), "plaquette");
+        double r[4];
+        int rc = measure_to_host(c, 4, r);
+        if (rc) return rc;
+        if (what == QG_MEAS_PLAQUETTE) { out[0] = r[0]; out[1] = r[1]; }
+        else { out[0] = r[2]; out[1] = r[3]; }
+        return QG_OK;
+    }
+    case QG_MEAS_POLYAKOV:
+        QG_CK(launch_polyakov(c->G, c->links, f.group, f.precision, (float)f.phi, (float)f.omega, tw, c->partials,
+                              c->d_results, c->stream), "polyakov");
+        return measure_to_host(c, 4, out);
+    case QG_MEAS_WILSON:
+        return qg_measure_wilson(c, f.wilson_r, f.wilson_t, out);
+    default:
+        return fail(c, QG_ERR_ARG, "unknown measurement");
+    }
+}
+
+extern "C" int qg_links_upload(qg_ctx *c, const void *host, int layout)
+{
+    if (!c || !host) return QG_ERR_ARG;
+    if (layout != QG_LAYOUT_REFERENCE) return fail(c, QG_ERR_ARG, "unknown layout");
+    const size_t rsz = c->cfg.precision ? sizeof(double) : sizeof(float);
+    const size_t bytes = (size_t)(c->cfg.group == 3 ? 12 : 4) * c->rowsize * 4 * rsz;
+    void *tmp = nullptr;
+    QG_CK(cudaMallocAsync(&tmp, bytes, c->stream), "upload staging");
+    cudaError_t e = cudaMemcpyAsync(tmp, host, bytes, cudaMemcpyHostToDevice, c->stream);
+    if (e == cudaSuccess) e = launch_to_native(c->G, tmp, c->links, c->cfg.group, c->cfg.precision, c->rowsize, c->stream);
+    cudaFreeAsync(tmp, c->stream);
+    if (e != cudaSuccess) return cuda_fail(c, e, "links upload");
+    QG_CK(cudaStreamSynchronize(c->stream), "upload sync");
+    return QG_OK;
+}
+
+extern "C" int qg_links_download(qg_ctx *c, void *host, int layout)
+{
+    if (!c || !host) return QG_ERR_ARG;
+    if (layout != QG_LAYOUT_REFERENCE) return fail(c, QG_ERR_ARG, "unknown layout");
+    const size_t rsz = c->cfg.precision ? sizeof(double) : sizeof(float);
+    const size_t bytes = (size_t)(c->cfg.group == 3 ? 12 : 4) * c->rowsize * 4 * rsz;
+    void *tmp = nullptr;
+    QG_CK(cudaMallocAsync(&tmp, bytes, c->stream), "download staging");
+    cudaError_t e = cudaMemsetAsync(tmp, 0, bytes, c->stream);
+    if (e == cudaSuccess) e = launch_to_ref(c->G, c->links, tmp, c->cfg.group, c->cfg.precision, c->rowsize, c->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(host, tmp, bytes, cudaMemcpyDeviceToHost, c->stream);
+    cudaFreeAsync(tmp, c->stream);
+    if (e != cudaSuccess) return cuda_fail(c, e, "links download");
+    QG_CK(cudaStreamSynchronize(c->stream), "download sync");
+    return QG_OK;
+}

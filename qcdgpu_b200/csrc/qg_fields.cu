@@ -1,0 +1,610 @@
+// qg_fields.cu -- whole-field kernels: start configurations, global
+// reunitarisation, reference-layout <-> checkerboard conversion and the
+// observables (plaquette/action, Polyakov loop, Wilson loops) with
+// deterministic two-pass FP64 reductions.
+#include "qg_internal.h"
+
+namespace qg {
+
+Geom make_geom(const int n[4])
+{
+    Geom G;
+    for (int i = 0; i < 4; i++) G.n[i] = n[i];
+    G.V = (uint32_t)n[0] * n[1] * n[2] * n[3];
+    G.half = G.V / 2;
+    G.cb = (G.half + 127u) & ~127u;
+    G.pstride = 2 * G.cb;
+    G.n2n3 = (uint32_t)n[1] * n[2];
+    G.n2n3n4 = G.n2n3 * n[3];
+    G.d2 = make_fastdiv((uint32_t)n[1]);
+    G.d23 = make_fastdiv(G.n2n3);
+    G.d234 = make_fastdiv(G.n2n3n4);
+    return G;
+}
+
+static __device__ __forceinline__ uint32_t native_index(const Geom &G, uint32_t s, const Crd &c)
+{
+    return (uint32_t)parity_of(c) * G.cb + (s >> 1);
+}
+
+// ---------------------------------------------------------------- starts
+// lattice_init_cold (suncl.cl:164-187)
+template <int NC, typename Real>
+__global__ void k_init_cold(Field<Real> U, Geom G)
+{
+    uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= G.V) return;
+    Crd c = lex2crd(G, s);
+    uint32_t e = native_index(G, s, c);
+    for (int mu = 0; mu < 4; mu++) {
+        if (NC == 3) {
+            G3<Real> m;
+            m.uv1 = { 1, 0, 0, 0 }; m.uv2 = { 0, 0, 0, 0 }; m.uv3 = { 0, 1, 0, 0 };
+            U.st3(mu, e, m);
+        } else {
+            U.st2(mu, e, R4<Real>{ 1, 0, 0, 0 });
+        }
+    }
+}
+
+// lattice_init_gid (suncl.cl:190-347): closed-form field, GS in Real
+template <int NC, typename Real>
+__global__ void k_init_gid(Field<Real> U, Geom G)
+{
+    uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= G.V) return;
+    Crd c = lex2crd(G, s);
+    uint32_t e = native_index(G, s, c);
+    const double V = (double)G.V, g = (double)s;
+    for (int mu = 0; mu < 4; mu++) {
+        const double o = (mu == 0) ? 0.001 : (mu == 1) ? 0.002 : (mu == 2) ? 0.003 : 0.004;
+        if (NC == 3) {
+            G3<Real> m;
+            m.uv1 = { (Real)(sin((o + 10.0 / V) * g) / 2.0), (Real)(sin((o - 18.0 / V) * g) / 4.0),
+                      (Real)(sin((o - 12.0 / V) * g) / 3.0), (Real)(sin((o - 16.0 / V) * g) / 3.0) };
+            m.uv2 = { (Real)(cos((o - 10.0 / V) * g) / 3.0), (Real)(cos((o + 12.0 / V) * g) / 4.0),
+                      (Real)(cos((o - 15.0 / V) * g) / 2.0), (Real)(cos((o - 18.0 / V) * g) / 2.0) };
+            m.uv3 = { (Real)(sin((o + 15.0 / V) * g) / 3.0), (Real)(sin((o - 11.0 / V) * g) / 3.0),
+                      (Real)(cos((o - 11.0 / V) * g) / 4.0), (Real)(cos((o + 16.0 / V) * g) / 2.0) };
+            U.st3(mu, e, gs3<Real>(m));
+        } else {
+            double f1 = sin((o + 10.0 / V) * g) / 2.0;
+            double f2 = cos((o - 10.0 / V) * g) / 3.0;
+            double f3 = sin((o - 18.0 / V) * g) / 4.0;
+            double f4 = sqrt(1.0 - f1 * f1 - f2 * f2 - f3 * f3);
+            U.st2(mu, e, R4<Real>{ (Real)f1, (Real)f3, (Real)f4, (Real)f2 });
+        }
+    }
+}
+
+// lattice_random3 / lattice_random2 from three (one) PRN quads (not Haar;
+// su3_update_cl.cl:165-225, su2_update_cl.cl:110-146)
+template <int NC, typename Real>
+__device__ __forceinline__ void random_link(const R4<Real> r[3], G3<Real> &m3, R4<Real> &m2)
+{
+    if (NC == 3) {
+        Real a0[4], a1[4], a2[4], a3[4];
+        const Real R1[4] = { r[0].x, r[0].y, r[0].z, r[0].w }, R2[4] = { r[1].x, r[1].y, r[1].z, r[1].w },
+                   R3[4] = { r[2].x, r[2].y, r[2].z, r[2].w };
+#pragma unroll
+        for (int k = 0; k < 3; k++) {
+            Real alpha = RC<Real>::PI * R1[k], phi = RC<Real>::PI2 * R2[k];
+            Real costh = (Real)2 * R3[k] - (Real)1;
+            Real sinth = RC<Real>::sq((Real)1 - costh * costh);
+            Real sinal = RC<Real>::sn(alpha);
+            a0[k] = RC<Real>::cs(alpha);
+            Real sinph = RC<Real>::sn(phi), cosph = RC<Real>::cs(phi);
+            Real t1 = sinal * sinth;
+            a1[k] = t1 * cosph; a2[k] = t1 * sinph; a3[k] = sinal * costh;
+        }
+        const int X = 0, Y = 1, Z = 2;
+        m3.uv1.x = a0[X] * a0[Y] - a3[X] * a3[Y];
+        m3.uv2.x = a0[Y] * a3[X] + a0[X] * a3[Y];
+        m3.uv1.y = -a0[X] * a1[Y] * a1[Z] + a0[Z] * a2[X] - a0[X] * a2[Y] * a2[Z] - a1[Z] * a2[Y] * a3[X] + a1[Y] * a2[Z] * a3[X] - a1[X] * a3[Z];
+        m3.uv2.y = a0[Z] * a1[X] + a0[X] * a1[Z] * a2[Y] - a0[X] * a1[Y] * a2[Z] - a1[Y] * a1[Z] * a3[X] - a2[Y] * a2[Z] * a3[X] + a2[X] * a3[Z];
+        m3.uv1.z = -a1[X] * a1[Z] + a0[X] * a0[Z] * a2[Y] + a2[X] * a2[Z] - a0[Z] * a1[Y] * a3[X] + a0[X] * a1[Y] * a3[Z] + a2[Y] * a3[X] * a3[Z];
+        m3.uv2.z = a0[X] * a0[Z] * a1[Y] + a1[Z] * a2[X] + a1[X] * a2[Z] + a0[Z] * a2[Y] * a3[X] - a0[X] * a2[Y] * a3[Z] + a1[Y] * a3[X] * a3[Z];
+        m3.uv1.w = -a0[Z] * a1[X] * a1[Y] - a0[Z] * a2[X] * a2[Y] + a0[X] * a2[Z] + a1[Z] * a3[X] - a1[Y] * a2[X] * a3[Z] + a1[X] * a2[Y] * a3[Z];
+        m3.uv2.w = a0[X] * a1[Z] - a0[Z] * a1[Y] * a2[X] + a0[Z] * a1[X] * a2[Y] - a2[Z] * a3[X] + a1[X] * a1[Y] * a3[Z] + a2[X] * a2[Y] * a3[Z];
+        m3.uv3.x = -a0[Y] * a2[X] - a1[X] * a3[Y];
+        m3.uv3.z = a0[Y] * a1[X] - a2[X] * a3[Y];
+        m3.uv3.y = a0[X] * a0[Z] + a1[Y] * a1[Z] * a2[X] - a1[X] * a1[Z] * a2[Y] + a1[X] * a1[Y] * a2[Z] + a2[X] * a2[Y] * a2[Z] + a3[X] * a3[Z];
+        m3.uv3.w = -a1[X] * a1[Y] * a1[Z] - a1[Z] * a2[X] * a2[Y] + a1[Y] * a2[X] * a2[Z] - a1[X] * a2[Y] * a2[Z] - a0[Z] * a3[X] + a0[X] * a3[Z];
+    } else {
+        Real alpha = RC<Real>::PI * r[0].x, phi = RC<Real>::PI2 * r[0].y;
+        Real costh = (Real)2 * r[0].z - (Real)1;
+        Real sinth = RC<Real>::sq((Real)1 - costh * costh);
+        Real sinal = RC<Real>::sn(alpha), a0 = RC<Real>::cs(alpha);
+        Real sinph = RC<Real>::sn(phi), cosph = RC<Real>::cs(phi);
+        Real t1 = sinal * sinth;
+        m2 = { a0, t1 * sinph, sinal * costh, t1 * cosph };
+    }
+}
+
+// lattice_init_hot_{X,Y,Z,T} (suncl.cl:56-161): quads GID + {0,1,2}*ROWSIZE
+// of the reference-layout batch, one direction per launch
+template <int NC, typename Real>
+__global__ void k_init_hot_ref(Field<Real> U, Geom G, int mu, const float4 *prns, uint32_t rowsize)
+{
+    uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= G.V) return;
+    Crd c = lex2crd(G, s);
+    uint32_t e = native_index(G, s, c);
+    R4<Real> r[3];
+    for (int j = 0; j < 3; j++) {
+        float4 q = prns[s + (size_t)j * rowsize];
+        r[j] = { (Real)q.x, (Real)q.y, (Real)q.z, (Real)q.w };
+    }
+    G3<Real> m3; R4<Real> m2;
+    random_link<NC, Real>(r, m3, m2);
+    if (NC == 3) U.st3(mu, e, m3); else U.st2(mu, e, m2);
+}
+
+// same start from the counter stream: quad j of (site, dir) is
+// Philox(site, 4*j + dir, ~0, ~0)
+template <int NC, typename Real>
+__global__ void k_init_hot_philox(Field<Real> U, Geom G, uint2 key)
+{
+    uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= G.V) return;
+    Crd c = lex2crd(G, s);
+    uint32_t e = native_index(G, s, c);
+    for (int mu = 0; mu < 4; mu++) {
+        R4<Real> r[3];
+        for (int j = 0; j < 3; j++) {
+            uint4 w = philox4x32_10(make_uint4(s, 4u * j + mu, 0xFFFFFFFFu, 0xFFFFFFFFu), key);
+            r[j] = { (Real)u32_to_unit(w.x), (Real)u32_to_unit(w.y), (Real)u32_to_unit(w.z), (Real)u32_to_unit(w.w) };
+        }
+        G3<Real> m3; R4<Real> m2;
+        random_link<NC, Real>(r, m3, m2);
+        if (NC == 3) U.st3(mu, e, m3); else U.st2(mu, e, m2);
+    }
+}
+
+// Haar-distributed start: SU(2) = normalised 4-vector of Gaussians; SU(3) =
+// Gram-Schmidt of two complex Gaussian rows (third row by conj cross
+// product), Gaussians by Box-Muller from the counter stream (~1, ~0 tag).
+template <int NC, typename Real>
+__global__ void k_init_haar(Field<Real> U, Geom G, uint2 key)
+{
+    uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= G.V) return;
+    Crd c = lex2crd(G, s);
+    uint32_t e = native_index(G, s, c);
+    for (int mu = 0; mu < 4; mu++) {
+        double gz[12];
+        for (int j = 0; j < 3; j++) {
+            uint4 w = philox4x32_10(make_uint4(s, 4u * j + mu, 0xFFFFFFFEu, 0xFFFFFFFFu), key);
+            double u1 = u32_to_unit(w.x), u2 = u32_to_unit(w.y), u3 = u32_to_unit(w.z), u4 = u32_to_unit(w.w);
+            double r1 = sqrt(-2.0 * log(u1)), r2 = sqrt(-2.0 * log(u3));
+            gz[4 * j + 0] = r1 * cos(6.283185307179586 * u2);
+            gz[4 * j + 1] = r1 * sin(6.283185307179586 * u2);
+            gz[4 * j + 2] = r2 * cos(6.283185307179586 * u4);
+            gz[4 * j + 3] = r2 * sin(6.283185307179586 * u4);
+        }
+        if (NC == 3) {
+            G3<double> m;
+            m.uv1 = { gz[0], gz[2], gz[4], gz[11] };
+            m.uv2 = { gz[1], gz[3], gz[5], gz[10] };
+            m.uv3 = { gz[6], gz[8], gz[7], gz[9] };
+            G3<double> q = gs3<double>(m);
+            G3<Real> r;
+            r.uv1 = { (Real)q.uv1.x, (Real)q.uv1.y, (Real)q.uv1.z, (Real)q.uv1.w };
+            r.uv2 = { (Real)q.uv2.x, (Real)q.uv2.y, (Real)q.uv2.z, (Real)q.uv2.w };
+            r.uv3 = { (Real)q.uv3.x, (Real)q.uv3.y, (Real)q.uv3.z, (Real)q.uv3.w };
+            U.st3(mu, e, r);
+        } else {
+            double n = sqrt(gz[0] * gz[0] + gz[1] * gz[1] + gz[2] * gz[2] + gz[3] * gz[3]);
+            U.st2(mu, e, R4<Real>{ (Real)(gz[0] / n), (Real)(gz[1] / n), (Real)(gz[2] / n), (Real)(gz[3] / n) });
+        }
+    }
+}
+
+template <int NC, typename Real>
+static cudaError_t init_T(const Geom &G, void *links, int kind, int dir, const float4 *prns, uint32_t rowsize,
+                          uint2 key, cudaStream_t s)
+{
+    Field<Real> U;
+    U.p = reinterpret_cast<typename V4<Real>::T *>(links);
+    U.pstride = G.pstride;
+    unsigned nb = (G.V + 127) / 128;
+    switch (kind) {
+    case INIT_COLD: k_init_cold<NC, Real><<<nb, 128, 0, s>>>(U, G); break;
+    case INIT_GID: k_init_gid<NC, Real><<<nb, 128, 0, s>>>(U, G); break;
+    case INIT_HOT_REF: k_init_hot_ref<NC, Real><<<nb, 128, 0, s>>>(U, G, dir, prns, rowsize); break;
+    case INIT_HOT_PHILOX: k_init_hot_philox<NC, Real><<<nb, 128, 0, s>>>(U, G, key); break;
+    default: k_init_haar<NC, Real><<<nb, 128, 0, s>>>(U, G, key); break;
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t launch_init(const Geom &G, void *links, int group, int prec, int kind, int dir, const float4 *prns,
+                        uint32_t rowsize, uint2 key, cudaStream_t s)
+{
+    if (group == 3)
+        return prec ? init_T<3, double>(G, links, kind, dir, prns, rowsize, key, s)
+                    : init_T<3, float>(G, links, kind, dir, prns, rowsize, key, s);
+    return prec ? init_T<2, double>(G, links, kind, dir, prns, rowsize, key, s)
+                : init_T<2, float>(G, links, kind, dir, prns, rowsize, key, s);
+}
+
+// ------------------------------------------------------- reunitarisation
+// lattice_GramSchmidt kernel (suncl.cl:350-396); Acc = double for the FP64
+// variant on FP32 links
+template <int NC, typename Real, typename Acc>
+__global__ void k_gramschmidt(Field<Real> U, Geom G)
+{
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= 2 * G.cb) return;
+    uint32_t h = (i < G.cb) ? i : i - G.cb;
+    if (h >= G.half) return;
+    for (int mu = 0; mu < 4; mu++) {
+        if (NC == 3) {
+            U.st3(mu, i, gs3<Acc>(U.ld3(mu, i)));
+        } else {
+            R4<Real> m = U.ld2(mu, i);
+            Acc x = m.x, y = m.y, z = m.z, w = m.w;
+            Acc det = sqrt(x * x + y * y + z * z + w * w);
+            U.st2(mu, i, R4<Real>{ (Real)(x / det), (Real)(y / det), (Real)(z / det), (Real)(w / det) });
+        }
+    }
+}
+
+cudaError_t launch_gramschmidt(const Geom &G, void *links, int group, int prec, int fp64, cudaStream_t s)
+{
+    unsigned nb = (2 * G.cb + 127) / 128;
+    if (prec) {
+        Field<double> U{ reinterpret_cast<double4 *>(links), G.pstride };
+        if (group == 3) k_gramschmidt<3, double, double><<<nb, 128, 0, s>>>(U, G);
+        else k_gramschmidt<2, double, double><<<nb, 128, 0, s>>>(U, G);
+    } else {
+        Field<float> U{ reinterpret_cast<float4 *>(links), G.pstride };
+        if (group == 3) {
+            if (fp64) k_gramschmidt<3, float, double><<<nb, 128, 0, s>>>(U, G);
+            else k_gramschmidt<3, float, float><<<nb, 128, 0, s>>>(U, G);
+        } else {
+            if (fp64) k_gramschmidt<2, float, double><<<nb, 128, 0, s>>>(U, G);
+            else k_gramschmidt<2, float, float><<<nb, 128, 0, s>>>(U, G);
+        }
+    }
+    return cudaGetLastError();
+}
+
+// ---------------------------------------------------------- layout convert
+template <typename V>
+__global__ void k_to_native(Geom G, const V *ref, V *nat, int planes, uint32_t rowsize)
+{
+    uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= G.V) return;
+    Crd c = lex2crd(G, s);
+    uint32_t e = native_index(G, s, c);
+    for (int k = 0; k < planes; k++) nat[(size_t)k * G.pstride + e] = ref[s + (size_t)k * rowsize];
+}
+template <typename V>
+__global__ void k_to_ref(Geom G, const V *nat, V *ref, int planes, uint32_t rowsize)
+{
+    uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= G.V) return;
+    Crd c = lex2crd(G, s);
+    uint32_t e = native_index(G, s, c);
+    for (int k = 0; k < planes; k++) ref[s + (size_t)k * rowsize] = nat[(size_t)k * G.pstride + e];
+}
+
+cudaError_t launch_to_native(const Geom &G, const void *ref, void *links, int group, int prec, uint32_t rowsize,
+                             cudaStream_t s)
+{
+    unsigned nb = (G.V + 127) / 128;
+    int planes = group == 3 ? 12 : 4;
+    if (prec) k_to_native<double4><<<nb, 128, 0, s>>>(G, (const double4 *)ref, (double4 *)links, planes, rowsize);
+    else k_to_native<float4><<<nb, 128, 0, s>>>(G, (const float4 *)ref, (float4 *)links, planes, rowsize);
+    return cudaGetLastError();
+}
+cudaError_t launch_to_ref(const Geom &G, const void *links, void *ref, int group, int prec, uint32_t rowsize,
+                          cudaStream_t s)
+{
+    unsigned nb = (G.V + 127) / 128;
+    int planes = group == 3 ? 12 : 4;
+    if (prec) k_to_ref<double4><<<nb, 128, 0, s>>>(G, (const double4 *)links, (double4 *)ref, planes, rowsize);
+    else k_to_ref<float4><<<nb, 128, 0, s>>>(G, (const float4 *)links, (float4 *)ref, planes, rowsize);
+    return cudaGetLastError();
+}
+
+// ------------------------------------------------------------ observables
+// FP64 view of a stored link (lattice_reconstruct3_double / 2_double,
+// su3_measurements_cl.cl:292-319, su2_measurements_cl.cl:126-141); SU(2)
+// is embedded in the upper 2x2 block with a zero third row and column.
+template <int NC, typename Real>
+__device__ __forceinline__ S3<double> load_d(const Field<Real> &U, const Geom &G, const Crd &c, int mu, float phi,
+                                             float omega, int twist)
+{
+    uint32_t e = cb_index(G, c, parity_of(c));
+    S3<double> d;
+    if (NC == 3) {
+        G3<Real> m = U.ldg3(mu, e);
+        if (twist && mu == 1 && c.x == G.n[0] - 1) m = twist3(m, (Real)phi, (Real)omega);
+        G3<double> md;
+        md.uv1 = { (double)m.uv1.x, (double)m.uv1.y, (double)m.uv1.z, (double)m.uv1.w };
+        md.uv2 = { (double)m.uv2.x, (double)m.uv2.y, (double)m.uv2.z, (double)m.uv2.w };
+        md.uv3 = { (double)m.uv3.x, (double)m.uv3.y, (double)m.uv3.z, (double)m.uv3.w };
+        d = rec3(md);
+    } else {
+        R4<Real> m = U.ldg2(mu, e);
+        if (twist && mu == 1 && c.x == G.n[0] - 1) {
+            Real ph = (Real)phi;
+            R4<Real> om = { RC<Real>::cs(ph / 2), 0, RC<Real>::sn(ph / 2), 0 };
+            m = times2(om, m);
+        }
+        d.u1 = { (double)m.x, (double)m.z }; d.u2 = { (double)m.y, (double)m.w }; d.u3 = { 0, 0 };
+        d.v1 = { -(double)m.y, (double)m.w }; d.v2 = { (double)m.x, -(double)m.z }; d.v3 = { 0, 0 };
+        d.w1 = { 0, 0 }; d.w2 = { 0, 0 }; d.w3 = { 0, 0 };
+    }
+    return d;
+}
+
+__device__ __forceinline__ S3<double> mulf(const S3<double> &u, const S3<double> &v)
+{
+    S3<double> t;
+    t.u1 = dot3(u.u1, u.u2, u.u3, v.u1, v.v1, v.w1);
+    t.u2 = dot3(u.u1, u.u2, u.u3, v.u2, v.v2, v.w2);
+    t.u3 = dot3(u.u1, u.u2, u.u3, v.u3, v.v3, v.w3);
+    t.v1 = dot3(u.v1, u.v2, u.v3, v.u1, v.v1, v.w1);
+    t.v2 = dot3(u.v1, u.v2, u.v3, v.u2, v.v2, v.w2);
+    t.v3 = dot3(u.v1, u.v2, u.v3, v.u3, v.v3, v.w3);
+    t.w1 = dot3(u.w1, u.w2, u.w3, v.u1, v.v1, v.w1);
+    t.w2 = dot3(u.w1, u.w2, u.w3, v.u2, v.v2, v.w2);
+    t.w3 = dot3(u.w1, u.w2, u.w3, v.u3, v.v3, v.w3);
+    return t;
+}
+__device__ __forceinline__ S3<double> hermf(const S3<double> &a)
+{
+    S3<double> r;
+    r.u1 = { a.u1.re, -a.u1.im }; r.u2 = { a.v1.re, -a.v1.im }; r.u3 = { a.w1.re, -a.w1.im };
+    r.v1 = { a.u2.re, -a.u2.im }; r.v2 = { a.v2.re, -a.v2.im }; r.v3 = { a.w2.re, -a.w2.im };
+    r.w1 = { a.u3.re, -a.u3.im }; r.w2 = { a.v3.re, -a.v3.im }; r.w3 = { a.w3.re, -a.w3.im };
+    return r;
+}
+// Re Tr(a b c^+ d^+)  (lattice_retrace_plaquette3, su3_measurements_cl.cl:527-548)
+__device__ __forceinline__ double retr4(const S3<double> &a, const S3<double> &b, const S3<double> &c,
+                                        const S3<double> &d)
+{
+    S3<double> w = mulf(mulf(mulf(a, b), hermf(c)), hermf(d));
+    return w.u1.re + w.v2.re + w.w3.re;
+}
+
+// warp + block sum of K doubles; thread 0 writes the block's partials
+template <int K>
+__device__ __forceinline__ void block_sum_store(double (&v)[K], double *partials)
+{
+    __shared__ double sh[K][32];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+#pragma unroll
+    for (int k = 0; k < K; k++) {
+        double x = v[k];
+        for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
+        if (lane == 0) sh[k][wid] = x;
+    }
+    __syncthreads();
+    if (wid == 0) {
+#pragma unroll
+        for (int k = 0; k < K; k++) {
+            double x = (lane < nw) ? sh[k][lane] : 0.0;
+            for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
+            if (lane == 0) partials[(size_t)blockIdx.x * K + k] = x;
+        }
+    }
+}
+
+// lattice_measurement_plq + lattice_measurement (sun_measurements_cl.cl:
+// 55-184,1178-1311): per site the xy,xz,yz (spatial) and xt,yt,zt
+// (temporal) plaquettes in FP64; also the action (beta/N)(3N - ReTr).
+template <int NC, typename Real>
+__global__ void __launch_bounds__(256) k_plaquette(Field<Real> U, Geom G, double bet, float phi, float omega,
+                                                    int twist, double *partials)
+{
+    uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+    double v[4] = { 0, 0, 0, 0 };
+    if (s < G.V) {
+        Crd c = lex2crd(G, s);
+        const Crd cx = step_plus(G, c, 0), cy = step_plus(G, c, 1), cz = step_plus(G, c, 2), ct = step_plus(G, c, 3);
+        S3<double> m1 = load_d<NC, Real>(U, G, c, 0, phi, omega, twist);
+        S3<double> m4 = load_d<NC, Real>(U, G, c, 1, phi, omega, twist);
+        S3<double> m5 = load_d<NC, Real>(U, G, c, 2, phi, omega, twist);
+        S3<double> m6 = load_d<NC, Real>(U, G, c, 3, phi, omega, twist);
+        double rs, rt;
+        rs  = retr4(m1, load_d<NC, Real>(U, G, cx, 1, phi, omega, twist), load_d<NC, Real>(U, G, cy, 0, phi, omega, twist), m4);
+        rs += retr4(m1, load_d<NC, Real>(U, G, cx, 2, phi, omega, twist), load_d<NC, Real>(U, G, cz, 0, phi, omega, twist), m5);
+        rt  = retr4(m1, load_d<NC, Real>(U, G, cx, 3, phi, omega, twist), load_d<NC, Real>(U, G, ct, 0, phi, omega, twist), m6);
+        rs += retr4(m4, load_d<NC, Real>(U, G, cy, 2, phi, omega, twist), load_d<NC, Real>(U, G, cz, 1, phi, omega, twist), m5);
+        rt += retr4(m4, load_d<NC, Real>(U, G, cy, 3, phi, omega, twist), load_d<NC, Real>(U, G, ct, 1, phi, omega, twist), m6);
+        rt += retr4(m5, load_d<NC, Real>(U, G, cz, 3, phi, omega, twist), load_d<NC, Real>(U, G, ct, 2, phi, omega, twist), m6);
+        v[0] = rs; v[1] = rt;
+        v[2] = bet * (3.0 * NC - rs);
+        v[3] = bet * (3.0 * NC - rt);
+    }
+    block_sum_store<4>(v, partials);
+}
+
+uint32_t plaq_blocks(const Geom &G) { return (G.V + 255) / 256; }
+
+cudaError_t launch_plaquette(const Geom &G, const void *links, int group, int prec, double beta_over_n, float phi,
+                             float omega, int twist, double *partials, double *out, cudaStream_t s)
+{
+    uint32_t nb = plaq_blocks(G);
+    if (prec) {
+        Field<double> U{ (double4 *)links, G.pstride };
+        double bet = beta_over_n;
+        if (group == 3) k_plaquette<3, double><<<nb, 256, 0, s>>>(U, G, bet, phi, omega, twist, partials);
+        else k_plaquette<2, double><<<nb, 256, 0, s>>>(U, G, bet, phi, omega, twist, partials);
+    } else {
+        Field<float> U{ (float4 *)links, G.pstride };
+        double bet = (double)(float)beta_over_n;
+        if (group == 3) k_plaquette<3, float><<<nb, 256, 0, s>>>(U, G, bet, phi, omega, twist, partials);
+        else k_plaquette<2, float><<<nb, 256, 0, s>>>(U, G, bet, phi, omega, twist, partials);
+    }
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    return launch_reduce(partials, nb, 4, out, s);
+}
+
+// lattice_polyakov (polyakov.cl:54-140): ordered product of the N4 T-links
+// in link precision, traces accumulated in FP64
+template <int NC, typename Real>
+__global__ void __launch_bounds__(256) k_polyakov(Field<Real> U, Geom G, float phi, float omega, int twist,
+                                                   double *partials)
+{
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t nsp = (uint32_t)G.n[0] * G.n[1] * G.n[2];
+    double v[4] = { 0, 0, 0, 0 };
+    if (i < nsp) {
+        Crd c;
+        c.y = (int)(i % (uint32_t)G.n[1]);
+        uint32_t r = i / (uint32_t)G.n[1];
+        c.z = (int)(r % (uint32_t)G.n[2]);
+        c.x = (int)(r / (uint32_t)G.n[2]);
+        c.t = 0;
+        double pr, pi;
+        if (NC == 3) {
+            G3<Real> m = U.ldg3(3, cb_index(G, c, parity_of(c)));
+            S3<Real> v0 = rec3(m);
+            for (int k = 1; k < G.n[3]; k++) {
+                c.t = k;
+                S3<Real> v1 = rec3(U.ldg3(3, cb_index(G, c, parity_of(c))));
+                S3<Real> w;
+                w.u1 = dot3(v0.u1, v0.u2, v0.u3, v1.u1, v1.v1, v1.w1);
+                w.u2 = dot3(v0.u1, v0.u2, v0.u3, v1.u2, v1.v2, v1.w2);
+                w.u3 = dot3(v0.u1, v0.u2, v0.u3, v1.u3, v1.v3, v1.w3);
+                w.v1 = dot3(v0.v1, v0.v2, v0.v3, v1.u1, v1.v1, v1.w1);
+                w.v2 = dot3(v0.v1, v0.v2, v0.v3, v1.u2, v1.v2, v1.w2);
+                w.v3 = dot3(v0.v1, v0.v2, v0.v3, v1.u3, v1.v3, v1.w3);
+                w.w1 = dot3(v0.w1, v0.w2, v0.w3, v1.u1, v1.v1, v1.w1);
+                w.w2 = dot3(v0.w1, v0.w2, v0.w3, v1.u2, v1.v2, v1.w2);
+                w.w3 = dot3(v0.w1, v0.w2, v0.w3, v1.u3, v1.v3, v1.w3);
+                v0 = w;
+            }
+            pr = (double)v0.u1.re + (double)v0.v2.re + (double)v0.w3.re;
+            pi = (double)v0.u1.im + (double)v0.v2.im + (double)v0.w3.im;
+        } else {
+            S2<Real> v0 = rec2(U.ldg2(3, cb_index(G, c, parity_of(c))));
+            for (int k = 1; k < G.n[3]; k++) {
+                c.t = k;
+                S2<Real> v1 = rec2(U.ldg2(3, cb_index(G, c, parity_of(c))));
+                v0 = mul2(v0, v1);
+            }
+            pr = (double)v0.u1.re + (double)v0.v2.re;
+            pi = (double)v0.u1.im + (double)v0.v2.im;
+        }
+        double q2 = pr * pr + pi * pi;
+        v[0] = pr; v[1] = pi; v[2] = q2; v[3] = q2 * q2;
+    }
+    (void)phi; (void)omega; (void)twist;
+    block_sum_store<4>(v, partials);
+}
+
+uint32_t poly_blocks(const Geom &G) { return ((uint32_t)G.n[0] * G.n[1] * G.n[2] + 255) / 256; }
+
+cudaError_t launch_polyakov(const Geom &G, const void *links, int group, int prec, float phi, float omega, int twist,
+                            double *partials, double *out, cudaStream_t s)
+{
+    uint32_t nb = poly_blocks(G);
+    if (prec) {
+        Field<double> U{ (double4 *)links, G.pstride };
+        if (group == 3) k_polyakov<3, double><<<nb, 256, 0, s>>>(U, G, phi, omega, twist, partials);
+        else k_polyakov<2, double><<<nb, 256, 0, s>>>(U, G, phi, omega, twist, partials);
+    } else {
+        Field<float> U{ (float4 *)links, G.pstride };
+        if (group == 3) k_polyakov<3, float><<<nb, 256, 0, s>>>(U, G, phi, omega, twist, partials);
+        else k_polyakov<2, float><<<nb, 256, 0, s>>>(U, G, phi, omega, twist, partials);
+    }
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    return launch_reduce(partials, nb, 4, out, s);
+}
+
+// lattice_measurement_wilson (wilson_loop.cl:55-454): per site and i in
+// {x,y,z}, Re Tr(L_t^T(x) L_i^R(x+T t) L_t^T(x+R i)^+ L_i^R(x)^+) in FP64
+template <int NC, typename Real>
+__global__ void __launch_bounds__(128) k_wilson(Field<Real> U, Geom G, int R, int T, float phi, float omega, int twist,
+                                                 double *partials)
+{
+    uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+    double v[1] = { 0 };
+    if (s < G.V) {
+        const Crd c1 = lex2crd(G, s);
+        Crd co = c1;
+        S3<double> m1 = load_d<NC, Real>(U, G, co, 3, phi, omega, twist);
+        for (int k = 1; k < T; k++) { co = step_plus(G, co, 3); m1 = mulf(m1, load_d<NC, Real>(U, G, co, 3, phi, omega, twist)); }
+        const Crd c2 = step_plus(G, co, 3);
+        double acc = 0;
+        for (int i = 0; i < 3; i++) {
+            Crd a = c1, b = c2;
+            S3<double> m4 = load_d<NC, Real>(U, G, a, i, phi, omega, twist);
+            S3<double> m2 = load_d<NC, Real>(U, G, b, i, phi, omega, twist);
+            for (int k = 1; k < R; k++) {
+                a = step_plus(G, a, i); b = step_plus(G, b, i);
+                m4 = mulf(m4, load_d<NC, Real>(U, G, a, i, phi, omega, twist));
+                m2 = mulf(m2, load_d<NC, Real>(U, G, b, i, phi, omega, twist));
+            }
+            Crd c4 = step_plus(G, a, i);
+            S3<double> m3 = load_d<NC, Real>(U, G, c4, 3, phi, omega, twist);
+            for (int k = 1; k < T; k++) { c4 = step_plus(G, c4, 3); m3 = mulf(m3, load_d<NC, Real>(U, G, c4, 3, phi, omega, twist)); }
+            acc += retr4(m1, m2, m3, m4);
+        }
+        v[0] = acc;
+    }
+    block_sum_store<1>(v, partials);
+}
+
+cudaError_t launch_wilson(const Geom &G, const void *links, int group, int prec, int R, int T, float phi, float omega,
+                          int twist, double *partials, double *out, cudaStream_t s)
+{
+    uint32_t nb = (G.V + 127) / 128;
+    if (prec) {
+        Field<double> U{ (double4 *)links, G.pstride };
+        if (group == 3) k_wilson<3, double><<<nb, 128, 0, s>>>(U, G, R, T, phi, omega, twist, partials);
+        else k_wilson<2, double><<<nb, 128, 0, s>>>(U, G, R, T, phi, omega, twist, partials);
+    } else {
+        Field<float> U{ (float4 *)links, G.pstride };
+        if (group == 3) k_wilson<3, float><<<nb, 128, 0, s>>>(U, G, R, T, phi, omega, twist, partials);
+        else k_wilson<2, float><<<nb, 128, 0, s>>>(U, G, R, T, phi, omega, twist, partials);
+    }
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    return launch_reduce(partials, nb, 1, out, s);
+}
+
+// final pass: one block sums the partials in a fixed order (deterministic)
+__global__ void __launch_bounds__(1024) k_reduce(const double *partials, uint32_t nblocks, int ncomp, double *out)
+{
+    __shared__ double sh[32];
+    for (int k = 0; k < ncomp; k++) {
+        double x = 0;
+        for (uint32_t b = threadIdx.x; b < nblocks; b += blockDim.x) x += partials[(size_t)b * ncomp + k];
+        for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
+        if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = x;
+        __syncthreads();
+        if (threadIdx.x < 32) {
+            x = sh[threadIdx.x];
+            for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
+            if (threadIdx.x == 0) out[k] = x;
+        }
+        __syncthreads();
+    }
+}
+
+cudaError_t launch_reduce(const double *partials, uint32_t nblocks, int ncomp, double *out, cudaStream_t s)
+{
+    k_reduce<<<1, 1024, 0, s>>>(partials, nblocks, ncomp, out);
+    return cudaGetLastError();
+}
+
+__global__ void k_add_u64(uint64_t *p, uint64_t v)
+{
+    if (threadIdx.x == 0 && blockIdx.x == 0) *p += v;
+}
+cudaError_t launch_add_u64(uint64_t *p, uint64_t v, cudaStream_t s)
+{
+    k_add_u64<<<1, 32, 0, s>>>(p, v);
+    return cudaGetLastError();
+}
+
+}  // namespace qg

@@ -1,0 +1,61 @@
+// qg_internal.h -- state shared by the CUDA translation units behind the
+// C-ABI in include/qcdgpu_b200.h.  Not part of the public interface.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+
+#include "../../include/qcdgpu_b200.h"
+#include "qg_lattice.cuh"
+
+namespace qg {
+
+struct PhaseArgs {
+    int parity, dir;
+    const double *params;    // device block {BETA/N, PHI, OMEGA} (lattice_parameters)
+    int twist;               // PHI or OMEGA non-zero
+    int nhit, nhitpar;
+    int prn_mode;            // QG_PRNG_RANLUX / QG_PRNG_PHILOX / gid (2)
+    const float4 *prns;      // reference-layout batch
+    uint32_t prngstep;
+    uint2 key;               // Philox key
+    const uint64_t *phase_base;  // device counter (graph-replayable)
+    uint32_t phase_offset;       // added to *phase_base
+};
+
+// launchers (return cudaError_t of the launch)
+cudaError_t launch_phase_f32(const Geom &G, void *links, int group, const PhaseArgs &a, cudaStream_t s);
+cudaError_t launch_phase_f64(const Geom &G, void *links, int group, const PhaseArgs &a, cudaStream_t s);
+
+enum InitKind { INIT_COLD = 0, INIT_GID = 1, INIT_HOT_REF = 2, INIT_HOT_PHILOX = 3, INIT_HAAR = 4 };
+cudaError_t launch_init(const Geom &G, void *links, int group, int prec, int kind, int dir,
+                        const float4 *prns, uint32_t rowsize, uint2 key, cudaStream_t s);
+cudaError_t launch_gramschmidt(const Geom &G, void *links, int group, int prec, int fp64, cudaStream_t s);
+cudaError_t launch_to_native(const Geom &G, const void *ref, void *links, int group, int prec, uint32_t rowsize,
+                             cudaStream_t s);
+cudaError_t launch_to_ref(const Geom &G, const void *links, void *ref, int group, int prec, uint32_t rowsize,
+                          cudaStream_t s);
+
+// measurements: per-block partials into scratch, then a fixed-order final
+// reduction into out (device).  Partials sizes returned by *_blocks().
+uint32_t plaq_blocks(const Geom &G);
+cudaError_t launch_plaquette(const Geom &G, const void *links, int group, int prec, double beta_over_n,
+                             float phi, float omega, int twist, double *partials, double *out, cudaStream_t s);
+uint32_t poly_blocks(const Geom &G);
+cudaError_t launch_polyakov(const Geom &G, const void *links, int group, int prec, float phi, float omega,
+                            int twist, double *partials, double *out, cudaStream_t s);
+cudaError_t launch_wilson(const Geom &G, const void *links, int group, int prec, int R, int T, float phi,
+                          float omega, int twist, double *partials, double *out, cudaStream_t s);
+cudaError_t launch_reduce(const double *partials, uint32_t nblocks, int ncomp, double *out, cudaStream_t s);
+cudaError_t launch_add_u64(uint64_t *p, uint64_t v, cudaStream_t s);
+
+// RANLUX, reference layout: one generator per instance, seed table of 7
+// float4 per instance (SoA), output prns[s*instances + i]
+cudaError_t launch_ranlux_init(const uint32_t *seeds, float4 *table, int instances, cudaStream_t s);
+cudaError_t launch_ranlux_produce(float4 *table, float4 *prns, int instances, int samples, int nskip,
+                                  cudaStream_t s);
+
+Geom make_geom(const int n[4]);
+
+}  // namespace qg

@@ -1,0 +1,307 @@
+"""CUDA sweep vs the CPU oracle, through the C-ABI (libqg_sun.so).
+
+Tolerances (north star): link fields after phases/sweeps fed the same PRN
+stream: max|dU| <= 1e-12 (FP64 links) / 2e-6 (FP32 links); plaquette and
+Polyakov sums on fixed configurations: 1e-13 / 1e-6 relative; RANLUX and
+Philox streams: bit-exact.
+"""
+import ctypes
+
+import numpy as np
+import pytest
+
+import _oracle as O
+import qcdgpu_b200 as Q
+
+pytestmark = pytest.mark.gpu
+
+TOL_U = {0: 2e-6, 1: 1e-12}
+INSTANCES = 512
+
+
+def make_pair(group, dims, precision, start=Q.START_COLD, prng=Q.PRNG_RANLUX, beta=6.0, nhit=10, nskip=223,
+              n_or=0, reunit_every=1, reunit_fp64=0, phi=0.0, omega=0.0):
+    L = Q.Lattice(Q.default_config(group=group, size=dims, precision=precision, start=start, prng=prng, beta=beta,
+                                   nhit=nhit, ranlux_nskip=nskip, prng_instances=INSTANCES, randseries=54,
+                                   row_align=64, n_or=n_or, reunit_every=reunit_every, reunit_fp64=reunit_fp64,
+                                   phi=phi, omega=omega))
+    c = O.make_cfg(group=group, dims=dims, precision=precision, beta=beta, nhit=nhit, row_align=64,
+                   gid_mode=(start == Q.START_GID), phi=phi, omega=omega)
+    return L, c
+
+
+def maxdiff(a, b):
+    return float(np.max(np.abs(a.astype(np.float64) - b.astype(np.float64))))
+
+
+def cold_table(c):
+    t = O.new_table(c)
+    O.lib.ol_init_cold(ctypes.byref(c), O.vp(t))
+    return t
+
+
+# ------------------------------------------------------------------ PRNG
+@pytest.mark.parametrize("nskip", [223, 389, 97, 48, 24])
+def test_ranlux_batches_bit_exact(nskip):
+    L, c = make_pair(3, (4, 4, 4, 4), 0, nskip=nskip)
+    info = L.info()
+    R = O.Ranlux(54, INSTANCES, nskip)
+    L.seed(54)                                   # PRNG::initialize: one produce()
+    for k in range(4):
+        if k:
+            L.produce()
+        ref = R.batch(info.prng_samples)
+        got = L.prns_download()
+        assert got.view(np.uint32).tolist() == ref.view(np.uint32).tolist(), "batch %d" % k
+    assert L.info().prng_counter == 4
+
+
+def test_ranlux_default_instances_bit_exact():
+    L = Q.Lattice(Q.default_config(group=3, size=(4, 4, 4, 4), precision=0, start=Q.START_COLD))
+    info = L.info()
+    R = O.Ranlux(54, 16384, 223)
+    L.seed(54)
+    L.produce()
+    R.batch(info.prng_samples)
+    assert np.array_equal(L.prns_download().view(np.uint32), R.batch(info.prng_samples).view(np.uint32))
+
+
+# ------------------------------------------------------- layout / starts
+@pytest.mark.parametrize("group,precision", [(3, 0), (3, 1), (2, 0), (2, 1)])
+def test_layout_roundtrip(group, precision):
+    L, c = make_pair(group, (4, 6, 2, 8), precision)
+    rng = np.random.default_rng(1)
+    a = rng.standard_normal(L.info().ref_elems).astype(np.float64 if precision else np.float32)
+    V = O.volume(c)
+    for p in range(12 if group == 3 else 4):       # padding rows are not stored
+        a[(p * c.rowsize + V) * 4:(p + 1) * c.rowsize * 4] = 0
+    L.upload(a)
+    assert np.array_equal(L.download(), a)
+
+
+@pytest.mark.parametrize("group,precision", [(3, 0), (3, 1), (2, 0), (2, 1)])
+def test_gid_and_cold_starts(group, precision):
+    for start, init in ((Q.START_GID, O.lib.ol_init_gid), (Q.START_COLD, O.lib.ol_init_cold)):
+        L, c = make_pair(group, (4, 4, 6, 4), precision, start=start)
+        L.init(start)
+        t = O.new_table(c)
+        init(ctypes.byref(c), O.vp(t))
+        assert maxdiff(L.download(), t) <= TOL_U[precision]
+
+
+@pytest.mark.parametrize("group,precision", [(3, 0), (3, 1), (2, 0), (2, 1)])
+def test_hot_start_ranlux(group, precision):
+    L, c = make_pair(group, (4, 4, 4, 4), precision, start=Q.START_HOT)
+    info = L.info()
+    R = O.Ranlux(54, INSTANCES)
+    L.seed(54)
+    L.init(Q.START_HOT)
+    R.batch(info.prng_samples)
+    t = O.new_table(c)
+    for mu in range(4):
+        O.lib.ol_init_hot_dir(ctypes.byref(c), O.vp(t), mu, O.vp(R.batch(info.prng_samples)))
+    assert maxdiff(L.download(), t) <= TOL_U[precision] * 4
+
+
+# ------------------------------------------------------------- updates
+def oracle_sweep_ranlux(c, t, R, samples):
+    for par in (1, 0):
+        for mu in range(4):
+            O.phase_hb(c, t, par, mu, prns=R.batch(samples))
+
+
+@pytest.mark.parametrize("group,precision,dims", [(3, 1, (4, 4, 4, 4)), (3, 0, (4, 4, 4, 4)),
+                                                  (2, 1, (4, 6, 2, 4)), (2, 0, (4, 6, 2, 4)),
+                                                  (3, 1, (2, 4, 6, 4))])
+def test_heatbath_phases_ranlux(group, precision, dims):
+    """Each update_{odd,even}_{X..T} fed the same RANLUX batch as the oracle."""
+    L, c = make_pair(group, dims, precision, start=Q.START_HOT, beta=5.7 if group == 3 else 2.3)
+    info = L.info()
+    R = O.Ranlux(54, INSTANCES)
+    L.seed(54)
+    L.init(Q.START_HOT)
+    R.batch(info.prng_samples)
+    t = O.new_table(c)
+    for mu in range(4):
+        O.lib.ol_init_hot_dir(ctypes.byref(c), O.vp(t), mu, O.vp(R.batch(info.prng_samples)))
+    L.upload(t)                                  # start both from the oracle's table
+    for par in (1, 0):
+        for mu in range(4):
+            L.produce()
+            L.phase(par, mu)
+            O.phase_hb(c, t, par, mu, prns=R.batch(info.prng_samples))
+            d = maxdiff(L.download(), t)
+            assert d <= TOL_U[precision], (par, mu, d)
+
+
+@pytest.mark.parametrize("group,precision", [(3, 1), (3, 0), (2, 1), (2, 0)])
+def test_sweeps_ranlux_reference_cadence(group, precision):
+    """qg_sweep = lattice_simulate's working cycle: 8 x (produce, phase), GS."""
+    L, c = make_pair(group, (4, 4, 4, 4), precision, start=Q.START_COLD, beta=6.0 if group == 3 else 2.3)
+    info = L.info()
+    R = O.Ranlux(54, INSTANCES)
+    L.seed(54)
+    L.init(Q.START_COLD)
+    R.batch(info.prng_samples)
+    t = cold_table(c)
+    for s in range(2):
+        L.sweep(1)
+        oracle_sweep_ranlux(c, t, R, info.prng_samples)
+        O.lib.ol_gramschmidt(ctypes.byref(c), O.vp(t))
+        d = maxdiff(L.download(), t)
+        assert d <= TOL_U[precision] * (1 + s), (s, d)
+    assert L.info().prng_counter == 1 + 16
+
+
+@pytest.mark.parametrize("group,precision", [(3, 1), (3, 0), (2, 1), (2, 0)])
+def test_sweeps_philox(group, precision):
+    L, c = make_pair(group, (4, 4, 2, 6), precision, start=Q.START_COLD, prng=Q.PRNG_PHILOX,
+                     beta=5.9 if group == 3 else 2.3)
+    L.seed(54)
+    L.init(Q.START_COLD)
+    t = cold_table(c)
+    key = (54, 0x5D3E1A27)
+    ph = 0
+    for s in range(2):
+        L.sweep(1)
+        for par in (1, 0):
+            for mu in range(4):
+                O.phase_hb(c, t, par, mu, philox=(key[0], key[1], ph))
+                ph += 1
+        O.lib.ol_gramschmidt(ctypes.byref(c), O.vp(t))
+        d = maxdiff(L.download(), t)
+        assert d <= TOL_U[precision] * (1 + s), (s, d)
+    assert L.info().phase_counter == 16
+
+
+@pytest.mark.parametrize("group,precision", [(3, 1), (3, 0), (2, 1), (2, 0)])
+def test_overrelaxation_sweeps(group, precision):
+    """1 heatbath + 2 overrelaxation sweeps, GS every 2 sweeps in FP64."""
+    L, c = make_pair(group, (4, 4, 4, 4), precision, start=Q.START_COLD, prng=Q.PRNG_PHILOX,
+                     beta=6.0 if group == 3 else 2.3, n_or=2, reunit_every=2, reunit_fp64=1)
+    L.seed(54)
+    L.init(Q.START_COLD)
+    t = cold_table(c)
+    ph = 0
+    for s in range(4):
+        L.sweep(1)
+        for par in (1, 0):
+            for mu in range(4):
+                O.phase_hb(c, t, par, mu, philox=(54, 0x5D3E1A27, ph))
+                ph += 1
+        for k in range(2):
+            for par in (1, 0):
+                for mu in range(4):
+                    O.lib.ol_phase_or(ctypes.byref(c), O.vp(t), par, mu)
+        if s % 2 == 1:
+            O.lib.ol_gramschmidt_fp64(ctypes.byref(c), O.vp(t))
+        d = maxdiff(L.download(), t)
+        assert d <= TOL_U[precision] * 4, (s, d)
+
+
+@pytest.mark.parametrize("group,precision", [(3, 1), (3, 0), (2, 1), (2, 0)])
+def test_gid_mode_sweeps(group, precision):
+    L, c = make_pair(group, (4, 4, 4, 4), precision, start=Q.START_GID, beta=6.0)
+    L.init(Q.START_GID)
+    t = O.new_table(c)
+    O.lib.ol_init_gid(ctypes.byref(c), O.vp(t))
+    for s in range(2):
+        L.sweep(1)
+        for par in (1, 0):
+            for mu in range(4):
+                O.phase_hb(c, t, par, mu, philox=(0, 0, 0))
+        O.lib.ol_gramschmidt(ctypes.byref(c), O.vp(t))
+        assert maxdiff(L.download(), t) <= TOL_U[precision] * (1 + s)
+
+
+def test_twisted_boundary_phase():
+    L, c = make_pair(3, (4, 4, 4, 4), 1, start=Q.START_HOT, phi=0.3, omega=0.7)
+    info = L.info()
+    R = O.Ranlux(54, INSTANCES)
+    L.seed(54)
+    L.init(Q.START_HOT)
+    R.batch(info.prng_samples)
+    t = O.new_table(c)
+    for mu in range(4):
+        O.lib.ol_init_hot_dir(ctypes.byref(c), O.vp(t), mu, O.vp(R.batch(info.prng_samples)))
+    for par, mu in ((1, 1), (0, 0)):
+        L.produce()
+        L.phase(par, mu)
+        O.phase_hb(c, t, par, mu, prns=R.batch(info.prng_samples))
+    assert maxdiff(L.download(), t) <= 1e-12
+    a, b = L.plaquette_sums(), O.plaquette(c, t)
+    assert np.allclose(a, b, rtol=1e-13, atol=0)
+
+
+# --------------------------------------------------------- observables
+def hot_config(group, dims, precision, sweeps=2):
+    L, c = make_pair(group, dims, precision, start=Q.START_HOT, prng=Q.PRNG_RANLUX, beta=5.8 if group == 3 else 2.3)
+    L.seed(54)
+    L.init(Q.START_HOT)
+    L.sweep(sweeps)
+    return L, c, L.download()
+
+
+@pytest.mark.parametrize("group,precision", [(3, 1), (3, 0), (2, 1), (2, 0)])
+def test_plaquette_action_polyakov_wilson(group, precision):
+    L, c, t = hot_config(group, (4, 6, 4, 8), precision)
+    sp, tp = L.plaquette_sums()
+    osp, otp = O.plaquette(c, t)
+    assert abs(sp - osp) <= 1e-13 * abs(osp) and abs(tp - otp) <= 1e-13 * abs(otp)
+    assert np.allclose(L.action_sums(), O.action(c, t), rtol=1e-13, atol=0)
+    prel = 1e-13 if precision else 1e-6
+    gp, op = L.polyakov_sums(), O.polyakov(c, t)
+    scale = 4 * 6 * 4 * group
+    assert all(abs(a - b) <= prel * scale for a, b in zip(gp, op)), (gp, op)
+    for R, T in ((1, 1), (2, 3), (3, 2)):
+        w, ow = L.wilson_sum(R, T), O.wilson(c, t, R, T)
+        assert abs(w - ow) <= 1e-12 * 3 * O.volume(c) * group, (R, T, w, ow)
+    # W(1,1) summed over i in {x,y,z} = temporal plaquette sum
+    assert abs(L.wilson_sum(1, 1) - tp) <= 1e-12 * abs(tp)
+
+
+def test_cold_observables_exact():
+    for g in (2, 3):
+        L, c = make_pair(g, (4, 4, 4, 6), 0)
+        L.init(Q.START_COLD)
+        V = O.volume(c)
+        assert L.plaquette_sums() == (3.0 * V * g, 3.0 * V * g)
+        assert L.polyakov_sums()[:2] == (4 * 4 * 4 * g, 0.0)
+        assert L.action_sums() == (0.0, 0.0)
+
+
+def test_reunitarize_parity():
+    for fp64 in (0, 1):
+        L, c, t = hot_config(3, (4, 4, 4, 4), 0, sweeps=1)
+        rng = np.random.default_rng(3)
+        t = (t + 1e-3 * rng.standard_normal(t.size)).astype(np.float32)
+        L.upload(t)
+        L.reunitarize(fp64=bool(fp64))
+        (O.lib.ol_gramschmidt_fp64 if fp64 else O.lib.ol_gramschmidt)(ctypes.byref(c), O.vp(t))
+        assert maxdiff(L.download(), t) <= 2e-7
+
+
+# ----------------------------------------------------- full-size properties
+@pytest.mark.parametrize("prng", [Q.PRNG_PHILOX, Q.PRNG_RANLUX])
+def test_bench_config_properties(prng):
+    """SU(3) 32^4 beta=6.0 FP32, HB + 4 OR: the field stays in SU(3), the
+    plaquette moves from 3 toward its equilibrium, and reruns are bitwise
+    reproducible."""
+    res = []
+    for rep in range(2):
+        L = Q.Lattice(Q.default_config(group=3, size=32, precision=0, start=Q.START_COLD, prng=prng, beta=6.0,
+                                       n_or=4, reunit_every=10, reunit_fp64=1, prng_instances=16384))
+        L.seed(54)
+        L.init(Q.START_COLD)
+        L.sweep(3)
+        p = L.plaquette()
+        res.append((p, L.polyakov()))
+        if rep == 0:
+            a = L.download().reshape(12, -1, 4)[:, :32 ** 4, :].astype(np.float64)
+            r1 = a[0:4, :, :3] + 1j * a[4:8, :, :3]
+            n = np.sum(np.abs(r1) ** 2, axis=-1)
+            assert np.max(np.abs(n - 1)) < 1e-5
+        L.close()
+    assert res[0] == res[1]
+    sp, tp, tot = res[0][0]
+    assert 1.6 < tot < 2.6

@@ -1,0 +1,147 @@
+"""Pins the CPU oracle to the reference before anything is checked against it.
+
+* RANLUX: the oracle's generator reproduces, bit for bit, the stream of the
+  reference's own host RANLUX (random/random.cpp RL_produce_one_CPU), which
+  PRNG::check (random.cpp:339-402) requires GPU instance 0 to equal.
+* glibc seeding: RANDSERIES -> instance seeds as PRNG::initialize does.
+* Philox4x32-10: the published known-answer vectors of the algorithm.
+* Deterministic INTS=2 mode: the oracle's restatement of the update kernels
+  reproduces the plaquettes of the reference's sequential CPU path
+  (SU(N)/suncpp) -- to 1e-14 on the closed-form start and to the ~1e-7
+  level after sweeps (the CPU path stores its deterministic "random" numbers
+  in float, SU(N)/suncpp/su2/update_su2.cpp:44, and sums staple planes in
+  another order).
+"""
+import ctypes
+import json
+import os
+import struct
+import subprocess
+
+import numpy as np
+import pytest
+
+import _oracle as O
+
+GOLDEN = json.load(open(os.path.join(os.path.dirname(__file__), "golden", "reference_pins.json")))
+NSKIP = [24, 48, 97, 223, 389]
+
+
+def bits(x):
+    return struct.unpack("<I", struct.pack("<f", x))[0]
+
+
+@pytest.mark.parametrize("case", GOLDEN["ranlux"], ids=lambda c: "s%d-lux%d" % (c["randseries"], c["luxury"]))
+def test_ranlux_instance0_matches_reference_stream(case):
+    seeds = O.glibc_seeds(case["randseries"], 2)
+    assert int(seeds[0]) == case["jseed"]
+    st = ctypes.create_string_buffer(O.lib.ol_sizeof_ranlux())
+    O.lib.ol_ranlux_init(st, int(seeds[0]), NSKIP[case["luxury"]])
+    got = [bits(O.lib.ol_ranlux_next(st)) for _ in range(len(case["bits"]))]
+    assert got == case["bits"]
+
+
+def test_ranlux_batch_layout_is_instance_major():
+    """ranlux kernel layout: prns[s*instances + i] = 4 consecutive outputs."""
+    R = O.Ranlux(54, 8)
+    b = R.batch(3).reshape(3, 8, 4)
+    seeds = O.glibc_seeds(54, 8)
+    for i in (0, 5):
+        st = ctypes.create_string_buffer(O.lib.ol_sizeof_ranlux())
+        O.lib.ol_ranlux_init(st, int(seeds[i]), 223)
+        ref = np.array([O.lib.ol_ranlux_next(st) for _ in range(12)], dtype=np.float32).reshape(3, 4)
+        assert np.array_equal(b[:, i, :], ref)
+
+
+def test_ranlux_values_in_open_unit_interval():
+    """PRNG::check_range (random.cpp:403-423)."""
+    b = O.Ranlux(99, 64).batch(200)
+    assert np.all(b > 0) and np.all(b < 1)
+
+
+@pytest.mark.skipif(not os.path.exists(os.path.join(O.REF_DIR, "ref_ranlux")), reason="oracle/_ref not built")
+def test_ranlux_live_against_reference_binary():
+    out = subprocess.check_output([os.path.join(O.REF_DIR, "ref_ranlux"), "31337", "3", "3000"]).decode().split()
+    ref = [bits(float.fromhex(x)) for x in out[4:]]
+    seeds = O.glibc_seeds(31337, 1)
+    st = ctypes.create_string_buffer(O.lib.ol_sizeof_ranlux())
+    O.lib.ol_ranlux_init(st, int(seeds[0]), 223)
+    assert [bits(O.lib.ol_ranlux_next(st)) for _ in range(3000)] == ref
+
+
+def test_philox_known_answers():
+    assert O.philox((0, 0, 0, 0), (0, 0)) == (0x6627E8D5, 0xE169C58D, 0xBC57AC4C, 0x9B00DBD8)
+    assert O.philox((0xFFFFFFFF,) * 4, (0xFFFFFFFF, 0xFFFFFFFF)) == (0x408F276D, 0x41C83B0E, 0xA20BC7C6, 0x6D5451FD)
+    assert O.philox((0x243F6A88, 0x85A308D3, 0x13198A2E, 0x03707344), (0xA4093822, 0x299F31D0)) == \
+        (0xD16CFE09, 0x94FDCCEB, 0x5001E420, 0x24126EA1)
+
+
+def run_gid(group, dims, beta, sweeps):
+    c = O.make_cfg(group=group, dims=dims, precision=1, beta=beta, gid_mode=True)
+    t = O.new_table(c)
+    O.lib.ol_init_gid(ctypes.byref(c), O.vp(t))
+    V = O.volume(c)
+    rows = []
+    for s in range(sweeps + 1):
+        if s:
+            for par in (1, 0):
+                for mu in range(4):
+                    O.phase_hb(c, t, par, mu, philox=(0, 0, 0))
+            O.lib.ol_gramschmidt(ctypes.byref(c), O.vp(t))
+        sp, tp = O.plaquette(c, t)
+        rows.append((sp / (3 * V), tp / (3 * V)))
+    return rows
+
+
+@pytest.mark.parametrize("case", GOLDEN["gid"], ids=lambda c: "su%d-%s" % (c["group"], "x".join(map(str, c["dims"]))))
+def test_gid_mode_matches_reference_cpu_path(case):
+    rows = run_gid(case["group"], tuple(case["dims"]), case["beta"], len(case["rows"]) - 1)
+    for (sp, tp), ref in zip(rows, case["rows"]):
+        tol = 1e-13 if ref[0] == 0 else 2e-7
+        assert abs(sp - ref[1]) <= tol * max(1, abs(ref[1])), (ref[0], sp, ref[1])
+        assert abs(tp - ref[2]) <= tol * max(1, abs(ref[2])), (ref[0], tp, ref[2])
+
+
+def test_cold_start_observables_exact():
+    """Cold start: Plq = N, P = 1 exactly (SURVEY known answer)."""
+    for g in (2, 3):
+        c = O.make_cfg(group=g, dims=(4, 4, 4, 6), precision=0)
+        t = O.new_table(c)
+        O.lib.ol_init_cold(ctypes.byref(c), O.vp(t))
+        sp, tp = O.plaquette(c, t)
+        V = O.volume(c)
+        assert sp == 3 * V * g and tp == 3 * V * g
+        re, im, p2, p4 = O.polyakov(c, t)
+        assert re == 4 * 4 * 4 * g and im == 0
+
+
+def test_overrelaxation_preserves_local_action():
+    """Microcanonical reflection: Re Tr(U*staple) of each updated link is unchanged."""
+    for g in (2, 3):
+        c = O.make_cfg(group=g, dims=(4, 4, 4, 4), precision=1, beta=5.7)
+        t = O.new_table(c)
+        R = O.Ranlux(7, 256)
+        n = O.prn_samples(c, 256, hot=True)
+        R.batch(n)
+        for mu in range(4):
+            O.lib.ol_init_hot_dir(ctypes.byref(c), O.vp(t), mu, O.vp(R.batch(n)))
+        even = [s for s in range(O.volume(c)) if sum(site_coords(c, s)) % 2 == 0]
+        before = [O.lib.ol_local_action_link(ctypes.byref(c), O.vp(t), s, 2) for s in even]
+        old = t.copy()
+        O.lib.ol_phase_or(ctypes.byref(c), O.vp(t), 0, 2)
+        after = [O.lib.ol_local_action_link(ctypes.byref(c), O.vp(t), s, 2) for s in even]
+        assert np.allclose(before, after, rtol=0, atol=1e-12)
+        assert not np.allclose(old, t)                         # the links did move
+        O.lib.ol_phase_or(ctypes.byref(c), O.vp(t), 0, 2)      # SU(2): a reflection is an involution
+        if g == 2:
+            assert np.allclose(old, t, rtol=0, atol=1e-13)
+
+
+def site_coords(c, s):
+    n1, n2, n3, n4 = c.n
+    x = s // (n2 * n3 * n4)
+    r = s - x * n2 * n3 * n4
+    tt = r // (n2 * n3)
+    r -= tt * n2 * n3
+    z = r // n2
+    return (x, r - z * n2, z, tt)
