@@ -109,7 +109,7 @@ def cpu_workers(size):
     except (ValueError, OSError):
         avail = 8 << 30
     per = 4 * size ** 4 * 18 * 8 * 1.3         # the reference CPU path stores links as 18 doubles
-    return max(1, min(ncpu, int(avail // per)))
+    return max(1, min(ncpu, 64, int(0.5 * avail // per)))
 
 
 def run_reference_phases(size, procs, warm, timed):

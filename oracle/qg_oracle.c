@@ -218,6 +218,74 @@ static double cd_retr(const cd3 *a, int N)
     return s;
 }
 
+/* ======================================================= elementary functions */
+/* sin/cos for |x| < 16: Cody-Waite reduction by pi/2 (three-part constant)
+ * and Taylor polynomials of degree 17 / 18 on [-pi/4, pi/4], Horner with
+ * fma; natural log by y = m 2^e, log m = 2 atanh((m-1)/(m+1)) to s^23.
+ * The same operation sequence as the CUDA path's routines, so both sides
+ * round identically. */
+static void ol_sincos(double x, double *s, double *c)
+{
+    const double INV_PIO2 = 0.63661977236758134308;
+    const double P1 = 1.5707963267948966, P2 = 6.123233995736766e-17, P3 = -1.4973849048591698e-33;
+    double n = rint(x * INV_PIO2);
+    double f = fma(-n, P1, x);
+    f = fma(-n, P2, f);
+    f = fma(-n, P3, f);
+    double f2 = f * f;
+    double ps = 2.8114572543455206e-15;
+    ps = fma(ps, f2, -7.6471637318198164e-13);
+    ps = fma(ps, f2, 1.6059043836821613e-10);
+    ps = fma(ps, f2, -2.5052108385441720e-08);
+    ps = fma(ps, f2, 2.7557319223985893e-06);
+    ps = fma(ps, f2, -1.9841269841269841e-04);
+    ps = fma(ps, f2, 8.3333333333333333e-03);
+    ps = fma(ps, f2, -1.6666666666666667e-01);
+    double sn = fma(ps * f2, f, f);
+    double pc = -1.5619206968586225e-16;
+    pc = fma(pc, f2, 4.7794773323873853e-14);
+    pc = fma(pc, f2, -1.1470745597729725e-11);
+    pc = fma(pc, f2, 2.0876756987868099e-09);
+    pc = fma(pc, f2, -2.7557319223985888e-07);
+    pc = fma(pc, f2, 2.4801587301587302e-05);
+    pc = fma(pc, f2, -1.3888888888888889e-03);
+    pc = fma(pc, f2, 4.1666666666666667e-02);
+    pc = fma(pc, f2, -0.5);
+    double cs = fma(pc, f2, 1.0);
+    int q = ((int)n) & 3;
+    *s = (q == 0) ? sn : (q == 1) ? cs : (q == 2) ? -sn : -cs;
+    *c = (q == 0) ? cs : (q == 1) ? -sn : (q == 2) ? -cs : sn;
+}
+
+static double ol_log(double y)
+{
+    int e;
+    double m = frexp(y, &e);
+    if (m < 0.70710678118654752440) { m = m * 2.0; e -= 1; }
+    double s = (m - 1.0) / (m + 1.0);
+    double s2 = s * s;
+    double p = 1.0 / 23.0;
+    p = fma(p, s2, 1.0 / 21.0);
+    p = fma(p, s2, 1.0 / 19.0);
+    p = fma(p, s2, 1.0 / 17.0);
+    p = fma(p, s2, 1.0 / 15.0);
+    p = fma(p, s2, 1.0 / 13.0);
+    p = fma(p, s2, 1.0 / 11.0);
+    p = fma(p, s2, 1.0 / 9.0);
+    p = fma(p, s2, 1.0 / 7.0);
+    p = fma(p, s2, 1.0 / 5.0);
+    p = fma(p, s2, 1.0 / 3.0);
+    double t = 2.0 * fma(p * s2, s, s);
+    const double LN2_HI = 6.93147180369123816490e-01, LN2_LO = 1.90821492927058770002e-10;
+    double de = (double)e;
+    return fma(de, LN2_HI, fma(de, LN2_LO, t));
+}
+
+/* exported for the accuracy tests of the two routines */
+double ol_sin(double x) { double s, c; ol_sincos(x, &s, &c); return s; }
+double ol_cos(double x) { double s, c; ol_sincos(x, &s, &c); return c; }
+double ol_logd(double x) { return ol_log(x); }
+
 /* ======================================================= precision bodies */
 #define REAL double
 #define SFX _d

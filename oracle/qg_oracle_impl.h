@@ -7,12 +7,17 @@
  * where the reference's float kernels promote to double through a double
  * literal (cl_khr_fp64 is enabled, SU(N)/suncl/model.cl:40-44) this file
  * promotes explicitly with (double).
+ *
+ * Operation order: every multiply-add is an explicit fma() in a fixed order
+ * (the file is compiled with -ffp-contract=off) and sin/cos/log on the
+ * update path are the routines ol_sincos / ol_log of qg_oracle.c, so the
+ * roundings this restatement performs are fully specified by the source.
  */
 
 #define R4  PASTE(r4,  SFX)
 #define CX  PASTE(cx,  SFX)
 #define G3  PASTE(g3,  SFX)
-#define S3  PASTE(s3,  SFX)
+#define M3  PASTE(m3,  SFX)
 #define G2  PASTE(g2,  SFX)
 #define S2  PASTE(s2,  SFX)
 #define FN(n) PASTE(n, SFX)
@@ -20,23 +25,27 @@
 #if IS_F
 #define RPI   3.141592653589793f
 #define RPI2  6.283185307179586f
-#define RSIN  sinf
-#define RCOS  cosf
 #define RSQRT sqrtf
+#define RFMA  fmaf
+static float FN(rsin)(float a) { double s, c; ol_sincos((double)a, &s, &c); return (float)s; }
+static float FN(rcos)(float a) { double s, c; ol_sincos((double)a, &s, &c); return (float)c; }
 #else
 #define RPI   3.1415926535897932384626433832795
 #define RPI2  6.2831853071795864769252867665590
-#define RSIN  sin
-#define RCOS  cos
 #define RSQRT sqrt
+#define RFMA  fma
+static double FN(rsin)(double a) { double s, c; ol_sincos(a, &s, &c); return s; }
+static double FN(rcos)(double a) { double s, c; ol_sincos(a, &s, &c); return c; }
 #endif
+#define RSIN FN(rsin)
+#define RCOS FN(rcos)
 
 typedef struct { REAL x, y, z, w; } R4;
 typedef struct { REAL re, im; } CX;
 typedef struct { R4 uv1, uv2, uv3; } G3;              /* 12-real compressed SU(3) */
-typedef struct { CX u1, u2, u3, v1, v2, v3, w1, w2, w3; } S3;
+typedef struct { CX m[3][3]; } M3;                    /* full 3x3, row major      */
 typedef struct { R4 uv1; } G2;                        /* 4-real SU(2)             */
-typedef struct { CX u1, u2, v1, v2; } S2;
+typedef struct { CX u1, u2, v1, v2; } S2;             /* 2x2 block (u1 u2; v1 v2) */
 
 /* ------------------------------------------------------------------ memory */
 /* lattice_table_3 / lattice_store_3: SU(N)/suncl/su3_matrix_memory.cl:43-176 */
@@ -52,7 +61,8 @@ static void FN(st4)(REAL *tab, int rowsize, unsigned site, int plane, R4 v)
     p[0] = v.x; p[1] = v.y; p[2] = v.z; p[3] = v.w;
 }
 
-/* twisted boundary: Y links at x = N1-1 (su3_matrix_memory.cl:57-97) */
+/* twisted boundary: Y links at x = N1-1 (su3_matrix_memory.cl:57-97):
+ * row 1 times exp(i(phi+omega)/2), row 2 times exp(i(omega-phi)/2) */
 static G3 FN(twist3)(const ol_cfg *c, G3 m)
 {
     REAL phi = (REAL)c->phi, omega = (REAL)c->omega;
@@ -60,12 +70,12 @@ static G3 FN(twist3)(const ol_cfg *c, G3 m)
     REAL cp = RCOS(p), sp = RSIN(p), cq = RCOS(q), sq = RSIN(q);
     R4 a = m.uv1, b = m.uv2, d = m.uv3;
     G3 r;
-    r.uv1.x = a.x * cp - b.x * sp;  r.uv2.x = b.x * cp + a.x * sp;
-    r.uv1.y = a.y * cp - b.y * sp;  r.uv2.y = b.y * cp + a.y * sp;
-    r.uv1.z = a.z * cp - b.z * sp;  r.uv2.z = b.z * cp + a.z * sp;
-    r.uv1.w = a.w * cq - b.w * sq;  r.uv2.w = b.w * cq + a.w * sq;
-    r.uv3.x = d.x * cq - d.z * sq;  r.uv3.y = d.y * cq - d.w * sq;
-    r.uv3.z = d.z * cq + d.x * sq;  r.uv3.w = d.w * cq + d.y * sq;
+    r.uv1.x = RFMA(-b.x, sp, a.x * cp); r.uv1.y = RFMA(-b.y, sp, a.y * cp);
+    r.uv1.z = RFMA(-b.z, sp, a.z * cp); r.uv1.w = RFMA(-b.w, sq, a.w * cq);
+    r.uv2.x = RFMA(a.x, sp, b.x * cp);  r.uv2.y = RFMA(a.y, sp, b.y * cp);
+    r.uv2.z = RFMA(a.z, sp, b.z * cp);  r.uv2.w = RFMA(a.w, sq, b.w * cq);
+    r.uv3.x = RFMA(-d.z, sq, d.x * cq); r.uv3.y = RFMA(-d.w, sq, d.y * cq);
+    r.uv3.z = RFMA(d.x, sq, d.z * cq);  r.uv3.w = RFMA(d.y, sq, d.w * cq);
     return r;
 }
 
@@ -102,7 +112,7 @@ static G2 FN(load2)(const ol_cfg *c, const REAL *tab, const crd *co, unsigned si
     if (dir == 1 && has_twist(c) && co->x == c->n[0] - 1) {
         REAL phi = (REAL)c->phi;
         R4 om;
-        om.x = RCOS(phi / 2); om.z = RSIN(phi / 2); om.y = 0; om.w = 0;
+        om.x = RCOS(phi / 2); om.y = 0; om.z = RSIN(phi / 2); om.w = 0;
         m.uv1 = FN(times2)(om, m.uv1);
     }
     return m;
@@ -113,130 +123,173 @@ static void FN(store2)(const ol_cfg *c, REAL *tab, unsigned site, int dir, G2 m)
 }
 
 /* --------------------------------------------------------------- algebra */
-/* complex helpers: every product written as (a.re*b.re - a.im*b.im) etc.   */
-static inline CX FN(cmul)(CX a, CX b) { CX r; r.re = a.re * b.re - a.im * b.im; r.im = a.re * b.im + a.im * b.re; return r; }
-static inline CX FN(cconj)(CX a) { a.im = -a.im; return a; }
-
-/* row3 = conj(row1 x row2): lattice_reconstruct3, SU(N)/suncl/su3cl.cl:137-165 */
-static S3 FN(rec3)(G3 a)
-{
-    S3 b;
-    b.u1.re = a.uv1.x; b.u1.im = a.uv2.x;
-    b.u2.re = a.uv1.y; b.u2.im = a.uv2.y;
-    b.u3.re = a.uv1.z; b.u3.im = a.uv2.z;
-    b.v1.re = a.uv3.x; b.v1.im = a.uv3.z;
-    b.v2.re = a.uv3.y; b.v2.im = a.uv3.w;
-    b.v3.re = a.uv1.w; b.v3.im = a.uv2.w;
-    b.w1.re =  b.u2.re * b.v3.re - b.u2.im * b.v3.im - b.u3.re * b.v2.re + b.u3.im * b.v2.im;
-    b.w1.im = -b.u2.re * b.v3.im - b.u2.im * b.v3.re + b.u3.re * b.v2.im + b.u3.im * b.v2.re;
-    b.w2.re =  b.u3.re * b.v1.re - b.u3.im * b.v1.im - b.u1.re * b.v3.re + b.u1.im * b.v3.im;
-    b.w2.im = -b.u3.re * b.v1.im - b.u3.im * b.v1.re + b.u1.re * b.v3.im + b.u1.im * b.v3.re;
-    b.w3.re =  b.u1.re * b.v2.re - b.u1.im * b.v2.im - b.u2.re * b.v1.re + b.u2.im * b.v1.im;
-    b.w3.im = -b.u1.re * b.v2.im - b.u1.im * b.v2.re + b.u2.re * b.v1.im + b.u2.im * b.v1.re;
-    return b;
-}
-
-static G3 FN(compress3)(const S3 *s)
-{
-    G3 g;
-    g.uv1.x = s->u1.re; g.uv1.y = s->u2.re; g.uv1.z = s->u3.re; g.uv1.w = s->v3.re;
-    g.uv2.x = s->u1.im; g.uv2.y = s->u2.im; g.uv2.z = s->u3.im; g.uv2.w = s->v3.im;
-    g.uv3.x = s->v1.re; g.uv3.y = s->v2.re; g.uv3.z = s->v1.im; g.uv3.w = s->v2.im;
-    return g;
-}
-
-/* one entry of a 3x3 complex product: sum_k a_k b_k in the order k=1,2,3 */
-static inline CX FN(dot3)(CX a1, CX a2, CX a3, CX b1, CX b2, CX b3)
+/* sum_k a_k b_k (k = 0,1,2 in order), with a, b strided */
+static CX FN(dot3)(const CX *a, int as, const CX *b, int bs)
 {
     CX r;
-    r.re = a1.re * b1.re - a1.im * b1.im + a2.re * b2.re - a2.im * b2.im + a3.re * b3.re - a3.im * b3.im;
-    r.im = a1.re * b1.im + a1.im * b1.re + a2.re * b2.im + a2.im * b2.re + a3.re * b3.im + a3.im * b3.re;
+    r.re = a[0].re * b[0].re;
+    r.re = RFMA(-a[0].im, b[0].im, r.re);
+    r.im = a[0].re * b[0].im;
+    r.im = RFMA(a[0].im, b[0].re, r.im);
+    for (int k = 1; k < 3; k++) {
+        CX x = a[k * as], y = b[k * bs];
+        r.re = RFMA(x.re, y.re, r.re);
+        r.re = RFMA(-x.im, y.im, r.re);
+        r.im = RFMA(x.re, y.im, r.im);
+        r.im = RFMA(x.im, y.re, r.im);
+    }
+    return r;
+}
+/* sum_k a_k conj(b_k) */
+static CX FN(dotc3)(const CX *a, int as, const CX *b, int bs)
+{
+    CX r;
+    r.re = a[0].re * b[0].re;
+    r.re = RFMA(a[0].im, b[0].im, r.re);
+    r.im = a[0].im * b[0].re;
+    r.im = RFMA(-a[0].re, b[0].im, r.im);
+    for (int k = 1; k < 3; k++) {
+        CX x = a[k * as], y = b[k * bs];
+        r.re = RFMA(x.re, y.re, r.re);
+        r.re = RFMA(x.im, y.im, r.re);
+        r.im = RFMA(x.im, y.re, r.im);
+        r.im = RFMA(-x.re, y.im, r.im);
+    }
+    return r;
+}
+/* sum_k conj(a_k) b_k */
+static CX FN(cdot3)(const CX *a, int as, const CX *b, int bs)
+{
+    CX r;
+    r.re = a[0].re * b[0].re;
+    r.re = RFMA(a[0].im, b[0].im, r.re);
+    r.im = a[0].re * b[0].im;
+    r.im = RFMA(-a[0].im, b[0].re, r.im);
+    for (int k = 1; k < 3; k++) {
+        CX x = a[k * as], y = b[k * bs];
+        r.re = RFMA(x.re, y.re, r.re);
+        r.re = RFMA(x.im, y.im, r.re);
+        r.im = RFMA(x.re, y.im, r.im);
+        r.im = RFMA(-x.im, y.re, r.im);
+    }
     return r;
 }
 
-/* full 3x3 product: matrix_times_su3, su3cl.cl:101-135 */
-static S3 FN(mul3)(const S3 *u, const S3 *v)
+/* row 3 = conj(row1 x row2): lattice_reconstruct3, SU(N)/suncl/su3cl.cl:137-165 */
+static void FN(fill_row3)(M3 *a)
 {
-    S3 t;
-    t.u1 = FN(dot3)(u->u1, u->u2, u->u3, v->u1, v->v1, v->w1);
-    t.u2 = FN(dot3)(u->u1, u->u2, u->u3, v->u2, v->v2, v->w2);
-    t.u3 = FN(dot3)(u->u1, u->u2, u->u3, v->u3, v->v3, v->w3);
-    t.v1 = FN(dot3)(u->v1, u->v2, u->v3, v->u1, v->v1, v->w1);
-    t.v2 = FN(dot3)(u->v1, u->v2, u->v3, v->u2, v->v2, v->w2);
-    t.v3 = FN(dot3)(u->v1, u->v2, u->v3, v->u3, v->v3, v->w3);
-    t.w1 = FN(dot3)(u->w1, u->w2, u->w3, v->u1, v->v1, v->w1);
-    t.w2 = FN(dot3)(u->w1, u->w2, u->w3, v->u2, v->v2, v->w2);
-    t.w3 = FN(dot3)(u->w1, u->w2, u->w3, v->u3, v->v3, v->w3);
+    for (int j = 0; j < 3; j++) {
+        int p = (j + 1) % 3, q = (j + 2) % 3;
+        CX u1 = a->m[0][p], u2 = a->m[0][q], v1 = a->m[1][p], v2 = a->m[1][q];
+        REAL re = u1.re * v2.re;
+        re = RFMA(-u1.im, v2.im, re);
+        re = RFMA(-u2.re, v1.re, re);
+        re = RFMA(u2.im, v1.im, re);
+        REAL im = u2.re * v1.im;
+        im = RFMA(u2.im, v1.re, im);
+        im = RFMA(-u1.re, v2.im, im);
+        im = RFMA(-u1.im, v2.re, im);
+        a->m[2][j].re = re;
+        a->m[2][j].im = im;
+    }
+}
+static M3 FN(expand)(G3 g)
+{
+    M3 a;
+    a.m[0][0].re = g.uv1.x; a.m[0][0].im = g.uv2.x;
+    a.m[0][1].re = g.uv1.y; a.m[0][1].im = g.uv2.y;
+    a.m[0][2].re = g.uv1.z; a.m[0][2].im = g.uv2.z;
+    a.m[1][0].re = g.uv3.x; a.m[1][0].im = g.uv3.z;
+    a.m[1][1].re = g.uv3.y; a.m[1][1].im = g.uv3.w;
+    a.m[1][2].re = g.uv1.w; a.m[1][2].im = g.uv2.w;
+    FN(fill_row3)(&a);
+    return a;
+}
+static G3 FN(compress)(const M3 *a)
+{
+    G3 g;
+    g.uv1.x = a->m[0][0].re; g.uv1.y = a->m[0][1].re; g.uv1.z = a->m[0][2].re; g.uv1.w = a->m[1][2].re;
+    g.uv2.x = a->m[0][0].im; g.uv2.y = a->m[0][1].im; g.uv2.z = a->m[0][2].im; g.uv2.w = a->m[1][2].im;
+    g.uv3.x = a->m[1][0].re; g.uv3.y = a->m[1][1].re; g.uv3.z = a->m[1][0].im; g.uv3.w = a->m[1][1].im;
+    return g;
+}
+/* full product (matrix_times_su3, su3cl.cl:101-135) */
+static M3 FN(mul3)(const M3 *u, const M3 *v)
+{
+    M3 t;
+    for (int i = 0; i < 3; i++)
+        for (int j = 0; j < 3; j++) t.m[i][j] = FN(dot3)(&u->m[i][0], 1, &v->m[0][j], 3);
     return t;
 }
 
-/* compressed x compressed -> compressed (rows 1,2 of the product):
- * matrix_times3, su3cl.cl:51-99 */
-static G3 FN(times3)(G3 a, G3 b)
+/* staple term U_a U_b^+ U_c^+ (lattice_staple_hermitian3, su3_update_cl.cl:294-307):
+ * rows 1,2 of P = A B^+, row 3 of P reconstructed, then P C^+ */
+static M3 FN(staple_fwd3)(G3 ga, G3 gb, G3 gc)
 {
-    S3 u = FN(rec3)(a), v = FN(rec3)(b), t;
-    t.u1 = FN(dot3)(u.u1, u.u2, u.u3, v.u1, v.v1, v.w1);
-    t.u2 = FN(dot3)(u.u1, u.u2, u.u3, v.u2, v.v2, v.w2);
-    t.u3 = FN(dot3)(u.u1, u.u2, u.u3, v.u3, v.v3, v.w3);
-    t.v1 = FN(dot3)(u.v1, u.v2, u.v3, v.u1, v.v1, v.w1);
-    t.v2 = FN(dot3)(u.v1, u.v2, u.v3, v.u2, v.v2, v.w2);
-    t.v3 = FN(dot3)(u.v1, u.v2, u.v3, v.u3, v.v3, v.w3);
-    return FN(compress3)(&t);
+    M3 A = FN(expand)(ga), B = FN(expand)(gb), C = FN(expand)(gc), P, Q;
+    for (int i = 0; i < 2; i++)
+        for (int j = 0; j < 3; j++) P.m[i][j] = FN(dotc3)(&A.m[i][0], 1, &B.m[j][0], 1);
+    FN(fill_row3)(&P);
+    for (int i = 0; i < 3; i++)
+        for (int j = 0; j < 3; j++) Q.m[i][j] = FN(dotc3)(&P.m[i][0], 1, &C.m[j][0], 1);
+    return Q;
 }
-
-/* compressed hermitian conjugate: matrix_hermitian3, su3_update_cl.cl:86-110 */
-static G3 FN(herm3)(G3 a)
+/* staple term U_a^+ U_b^+ U_c (lattice_staple_hermitian_backward3,
+ * su3_update_cl.cl:324-338): rows 1,2 of R = B A, row 3 reconstructed, R^+ C */
+static M3 FN(staple_bwd3)(G3 ga, G3 gb, G3 gc)
 {
-    S3 u = FN(rec3)(a), h;
-    h.u1 = FN(cconj)(u.u1); h.u2 = FN(cconj)(u.v1); h.u3 = FN(cconj)(u.w1);
-    h.v1 = FN(cconj)(u.u2); h.v2 = FN(cconj)(u.v2); h.v3 = FN(cconj)(u.w2);
-    h.w1 = FN(cconj)(u.u3); h.w2 = FN(cconj)(u.v3); h.w3 = FN(cconj)(u.w3);
-    return FN(compress3)(&h);
+    M3 A = FN(expand)(ga), B = FN(expand)(gb), C = FN(expand)(gc), R, Q;
+    for (int i = 0; i < 2; i++)
+        for (int j = 0; j < 3; j++) R.m[i][j] = FN(dot3)(&B.m[i][0], 1, &A.m[0][j], 3);
+    FN(fill_row3)(&R);
+    for (int i = 0; i < 3; i++)
+        for (int j = 0; j < 3; j++) Q.m[i][j] = FN(cdot3)(&R.m[0][i], 3, &C.m[0][j], 3);
+    return Q;
 }
-
-static S3 FN(add3)(const S3 *a, const S3 *b)
+static M3 FN(add3)(const M3 *a, const M3 *b)
 {
-    S3 r;
-    const REAL *pa = (const REAL *)a, *pb = (const REAL *)b;
-    REAL *pr = (REAL *)&r;
-    for (int i = 0; i < 18; i++) pr[i] = pa[i] + pb[i];
+    M3 r;
+    for (int i = 0; i < 3; i++)
+        for (int j = 0; j < 3; j++) {
+            r.m[i][j].re = a->m[i][j].re + b->m[i][j].re;
+            r.m[i][j].im = a->m[i][j].im + b->m[i][j].im;
+        }
     return r;
 }
 
-/* staple pieces, su3_update_cl.cl:293-338 */
-static S3 FN(staple_fwd3)(G3 u1, G3 u2, G3 u3)     /* u1 u2^+ u3^+ */
-{
-    G3 m2 = FN(times3)(u1, FN(herm3)(u2));
-    return FN(rec3)(FN(times3)(m2, FN(herm3)(u3)));
-}
-static S3 FN(staple_bwd3)(G3 u1, G3 u2, G3 u3)     /* u1^+ u2^+ u3 */
-{
-    G3 m3 = FN(times3)(FN(herm3)(u1), FN(herm3)(u2));
-    return FN(rec3)(FN(times3)(m3, u3));
-}
-
 /* lattice_GramSchmidt3, su3_update_cl.cl:228-291 (in REAL precision) */
-static G3 FN(gs3)(G3 m)
+static G3 FN(gs3)(G3 g)
 {
-    R4 t1 = m.uv1, t2 = m.uv2, t3 = m.uv3;
-    REAL nu = RSQRT((t1.x * t1.x + t2.x * t2.x) + (t1.y * t1.y + t2.y * t2.y) + (t1.z * t1.z + t2.z * t2.z));
-    REAL ur[3] = { t1.x / nu, t1.y / nu, t1.z / nu };
-    REAL ui[3] = { t2.x / nu, t2.y / nu, t2.z / nu };
-    REAL vr[3] = { t3.x, t3.y, t1.w };
-    REAL vi[3] = { t3.z, t3.w, t2.w };
-    /* sc = sum_k v_k * conj(u_k) */
-    REAL sr = (ur[0] * vr[0] + ui[0] * vi[0]) + (ur[1] * vr[1] + ui[1] * vi[1]) + (ur[2] * vr[2] + ui[2] * vi[2]);
-    REAL si = (ur[0] * vi[0] - ui[0] * vr[0]) + (ur[1] * vi[1] - ui[1] * vr[1]) + (ur[2] * vi[2] - ui[2] * vr[2]);
-    REAL nr[3], ni[3];
-    for (int k = 0; k < 3; k++) {
-        nr[k] = vr[k] - ur[k] * sr + ui[k] * si;
-        ni[k] = vi[k] - ur[k] * si - ui[k] * sr;
+    REAL u[3][2] = { { g.uv1.x, g.uv2.x }, { g.uv1.y, g.uv2.y }, { g.uv1.z, g.uv2.z } };
+    REAL v[3][2] = { { g.uv3.x, g.uv3.z }, { g.uv3.y, g.uv3.w }, { g.uv1.w, g.uv2.w } };
+    REAL n2 = u[0][0] * u[0][0];
+    n2 = RFMA(u[0][1], u[0][1], n2);
+    for (int k = 1; k < 3; k++) { n2 = RFMA(u[k][0], u[k][0], n2); n2 = RFMA(u[k][1], u[k][1], n2); }
+    REAL nu = RSQRT(n2);
+    for (int k = 0; k < 3; k++) { u[k][0] = u[k][0] / nu; u[k][1] = u[k][1] / nu; }
+    REAL sr = v[0][0] * u[0][0], si = v[0][1] * u[0][0];
+    sr = RFMA(v[0][1], u[0][1], sr);
+    si = RFMA(-v[0][0], u[0][1], si);
+    for (int k = 1; k < 3; k++) {
+        sr = RFMA(v[k][0], u[k][0], sr); sr = RFMA(v[k][1], u[k][1], sr);
+        si = RFMA(v[k][1], u[k][0], si); si = RFMA(-v[k][0], u[k][1], si);
     }
-    REAL nv = RSQRT((nr[0] * nr[0] + ni[0] * ni[0]) + (nr[1] * nr[1] + ni[1] * ni[1]) + (nr[2] * nr[2] + ni[2] * ni[2]));
+    for (int k = 0; k < 3; k++) {
+        REAL r = RFMA(-sr, u[k][0], v[k][0]);
+        r = RFMA(si, u[k][1], r);
+        REAL i = RFMA(-sr, u[k][1], v[k][1]);
+        i = RFMA(-si, u[k][0], i);
+        v[k][0] = r; v[k][1] = i;
+    }
+    REAL m2 = v[0][0] * v[0][0];
+    m2 = RFMA(v[0][1], v[0][1], m2);
+    for (int k = 1; k < 3; k++) { m2 = RFMA(v[k][0], v[k][0], m2); m2 = RFMA(v[k][1], v[k][1], m2); }
+    REAL nv = RSQRT(m2);
+    for (int k = 0; k < 3; k++) { v[k][0] = v[k][0] / nv; v[k][1] = v[k][1] / nv; }
     G3 r;
-    r.uv1.x = ur[0]; r.uv1.y = ur[1]; r.uv1.z = ur[2]; r.uv1.w = nr[2] / nv;
-    r.uv2.x = ui[0]; r.uv2.y = ui[1]; r.uv2.z = ui[2]; r.uv2.w = ni[2] / nv;
-    r.uv3.x = nr[0] / nv; r.uv3.y = nr[1] / nv; r.uv3.z = ni[0] / nv; r.uv3.w = ni[1] / nv;
+    r.uv1.x = u[0][0]; r.uv1.y = u[1][0]; r.uv1.z = u[2][0]; r.uv1.w = v[2][0];
+    r.uv2.x = u[0][1]; r.uv2.y = u[1][1]; r.uv2.z = u[2][1]; r.uv2.w = v[2][1];
+    r.uv3.x = v[0][0]; r.uv3.y = v[1][0]; r.uv3.z = v[0][1]; r.uv3.w = v[1][1];
     return r;
 }
 
@@ -245,10 +298,10 @@ static G3 FN(gs3)(G3 m)
 static R4 FN(times2)(R4 u, R4 v)
 {
     R4 a;
-    a.x = u.x * v.x - u.y * v.y - u.z * v.z - u.w * v.w;
-    a.z = u.x * v.z + u.z * v.x + u.y * v.w - u.w * v.y;
-    a.y = u.x * v.y + u.y * v.x + u.w * v.z - u.z * v.w;
-    a.w = u.x * v.w + u.w * v.x + u.z * v.y - u.y * v.z;
+    a.x = u.x * v.x; a.x = RFMA(-u.y, v.y, a.x); a.x = RFMA(-u.z, v.z, a.x); a.x = RFMA(-u.w, v.w, a.x);
+    a.z = u.x * v.z; a.z = RFMA(u.z, v.x, a.z); a.z = RFMA(u.y, v.w, a.z); a.z = RFMA(-u.w, v.y, a.z);
+    a.y = u.x * v.y; a.y = RFMA(u.y, v.x, a.y); a.y = RFMA(u.w, v.z, a.y); a.y = RFMA(-u.z, v.w, a.y);
+    a.w = u.x * v.w; a.w = RFMA(u.w, v.x, a.w); a.w = RFMA(u.z, v.y, a.w); a.w = RFMA(-u.y, v.z, a.w);
     return a;
 }
 static R4 FN(herm2)(R4 u) { R4 r = { u.x, -u.y, -u.z, -u.w }; return r; }
@@ -262,11 +315,21 @@ static S2 FN(rec2)(R4 a)
 /* full 2x2 complex product: matrix_times_su2, su2cl.cl:43-60 */
 static S2 FN(mul2)(const S2 *u, const S2 *v)
 {
+    CX U[2][2] = { { u->u1, u->u2 }, { u->v1, u->v2 } }, W[2][2] = { { v->u1, v->u2 }, { v->v1, v->v2 } }, T[2][2];
+    for (int i = 0; i < 2; i++)
+        for (int j = 0; j < 2; j++) {
+            REAL re = U[i][0].re * W[0][j].re;
+            re = RFMA(-U[i][0].im, W[0][j].im, re);
+            re = RFMA(U[i][1].re, W[1][j].re, re);
+            re = RFMA(-U[i][1].im, W[1][j].im, re);
+            REAL im = U[i][0].re * W[0][j].im;
+            im = RFMA(U[i][0].im, W[0][j].re, im);
+            im = RFMA(U[i][1].re, W[1][j].im, im);
+            im = RFMA(U[i][1].im, W[1][j].re, im);
+            T[i][j].re = re; T[i][j].im = im;
+        }
     S2 t;
-    t.u1 = FN(cmul)(u->u1, v->u1); { CX q = FN(cmul)(u->u2, v->v1); t.u1.re += q.re; t.u1.im += q.im; }
-    t.u2 = FN(cmul)(u->u1, v->u2); { CX q = FN(cmul)(u->u2, v->v2); t.u2.re += q.re; t.u2.im += q.im; }
-    t.v1 = FN(cmul)(u->v1, v->u1); { CX q = FN(cmul)(u->v2, v->v1); t.v1.re += q.re; t.v1.im += q.im; }
-    t.v2 = FN(cmul)(u->v1, v->u2); { CX q = FN(cmul)(u->v2, v->v2); t.v2.re += q.re; t.v2.im += q.im; }
+    t.u1 = T[0][0]; t.u2 = T[0][1]; t.v1 = T[1][0]; t.v2 = T[1][1];
     return t;
 }
 static S2 FN(add2)(S2 a, S2 b)
@@ -312,43 +375,49 @@ static void FN(prn_next)(FN(prnctx) *p, REAL r[4])
 }
 
 /* --------------------------------------------------------------- heatbath */
-/* Kennedy-Pendleton step on the SU(2) block a (su_2 form).  Returns 1 when a
- * try was accepted and a is overwritten with c*aH; on rejection the SU(3)
- * caller wants the identity and one extra PRN skip (su3_update_cl.cl:665-668).
+/* Kennedy-Pendleton step on the SU(2) block a.  Returns 1 when a try was
+ * accepted and a is overwritten with c*aH; on rejection the SU(3) caller
+ * wants the identity and one extra PRN skip (su3_update_cl.cl:665-668).
  * su3_update_cl.cl:568-669 (SU(3) path) / su2_update_cl.cl:434-531 (SU(2)). */
 static int FN(kp_step)(S2 *a, REAL beta, FN(prnctx) *p, int su3_path)
 {
     const ol_cfg *c = p->cfg;
     R4 aH, cc, d;
-    REAL det, bdet, cosrnd, delta = 0, rnd[4];
+    REAL det, bdet, cosrnd, delta = 0, rnd[4], n2;
     int flag = 0;
     if (su3_path) {
         aH.x =  (a->u1.re + a->v2.re);
         aH.z = -(a->u1.im - a->v2.im);
         aH.y = -(a->u2.re - a->v1.re);
         aH.w = -(a->u2.im + a->v1.im);
-        det = RSQRT(aH.x * aH.x + aH.y * aH.y + aH.z * aH.z + aH.w * aH.w);
+        n2 = aH.x * aH.x;
+        n2 = RFMA(aH.y, aH.y, n2); n2 = RFMA(aH.z, aH.z, n2); n2 = RFMA(aH.w, aH.w, n2);
+        det = RSQRT(n2);
         aH.x /= det; aH.z /= det; aH.y /= det; aH.w /= det;
     } else {
         REAL Mx = a->u1.re + a->v2.re, My = a->u1.im - a->v2.im;
         REAL Mz = a->u2.re - a->v1.re, Mw = a->u2.im + a->v1.im;
-        det = RSQRT(Mx * Mx + My * My + Mz * Mz + Mw * Mw);
+        n2 = Mx * Mx;
+        n2 = RFMA(My, My, n2); n2 = RFMA(Mz, Mz, n2); n2 = RFMA(Mw, Mw, n2);
+        det = RSQRT(n2);
         aH.x = Mx / det; aH.z = -My / det; aH.y = -Mz / det; aH.w = -Mw / det;
     }
     bdet = beta * det;
     for (int i = 0; i < c->nhit && !flag; i++) {
         if (c->gid_mode) {
             double g = p->gidval, V = (double)sites_of(c);
-            rnd[0] = (REAL)fabs(sin((0.005 * (1 + c->nhit) + 270.0 / V) * g));
-            rnd[1] = (REAL)fabs(cos((0.005 * (1 + c->nhit) +  60.0 / V) * g));
-            rnd[2] = (REAL)fabs(sin((0.005 * (1 + c->nhit) - 150.0 / V) * g));
-            rnd[3] = (REAL)fabs(cos((0.005 * (1 + c->nhit) - 380.0 / V) * g));
+            double a5 = 0.005 * (1 + c->nhit);
+            rnd[0] = (REAL)fabs(sin((a5 + 270.0 / V) * g));
+            rnd[1] = (REAL)fabs(cos((a5 +  60.0 / V) * g));
+            rnd[2] = (REAL)fabs(sin((a5 - 150.0 / V) * g));
+            rnd[3] = (REAL)fabs(cos((a5 - 380.0 / V) * g));
         } else {
             FN(prn_next)(p, rnd);
         }
         cosrnd = RCOS(RPI2 * rnd[1]);
-        delta = (REAL)(-(log(1.0 - (double)rnd[0]) + (double)(cosrnd * cosrnd) * log(1.0 - (double)rnd[2])) / (double)bdet);
-        if ((double)(rnd[3] * rnd[3]) <= (1.0 - 0.5 * (double)delta)) flag = 1;
+        double lx = ol_log(1.0 - (double)rnd[0]), lz = ol_log(1.0 - (double)rnd[2]);
+        delta = (REAL)(-fma((double)(cosrnd * cosrnd), lz, lx) / (double)bdet);
+        if ((double)(rnd[3] * rnd[3]) <= fma(-0.5, (double)delta, 1.0)) flag = 1;
         if (c->gid_mode) { delta = cosrnd * cosrnd / bdet; flag = 1; }
     }
     if (flag) {
@@ -362,7 +431,7 @@ static int FN(kp_step)(S2 *a, REAL beta, FN(prnctx) *p, int su3_path)
             FN(prn_next)(p, rnd);
         }
         REAL cosal = (REAL)(1.0 - (double)delta);
-        REAL costh = (REAL)(2.0 * (double)rnd[0] - 1.0);
+        REAL costh = (REAL)fma(2.0, (double)rnd[0], -1.0);
         REAL sinth = (REAL)sqrt(1.0 - (double)(costh * costh));
         REAL sinal = (REAL)sqrt(1.0 - (double)(cosal * cosal));
         REAL phi = RPI2 * rnd[1];
@@ -394,51 +463,49 @@ static void FN(or_step)(S2 *a)
     aH.z = -(a->u1.im - a->v2.im);
     aH.y = -(a->u2.re - a->v1.re);
     aH.w = -(a->u2.im + a->v1.im);
-    REAL det = RSQRT(aH.x * aH.x + aH.y * aH.y + aH.z * aH.z + aH.w * aH.w);
+    REAL n2 = aH.x * aH.x;
+    n2 = RFMA(aH.y, aH.y, n2); n2 = RFMA(aH.z, aH.z, n2); n2 = RFMA(aH.w, aH.w, n2);
+    REAL det = RSQRT(n2);
     aH.x /= det; aH.z /= det; aH.y /= det; aH.w /= det;
     *a = FN(rec2)(FN(times2)(aH, aH));
 }
 
-/* Cabibbo-Marinari over the three SU(2) subgroups; lattice_heatbath3,
- * su3_update_cl.cl:672-779.  kind 0 = heatbath, 1 = overrelaxation. */
-static G3 FN(cm3)(const S3 *staple, G3 m0, REAL beta, FN(prnctx) *p, int nhitpar, int kind)
+/* rows i, j of U <- V (rows i, j), V = (u1 u2; v1 v2) */
+static void FN(rotate_rows)(M3 *U, int i, int j, const S2 *V)
 {
-    G3 reslt = m0, Vg, m1, m2, m3 = m0;
-    S3 U0 = FN(rec3)(m0), x0;
-    S2 r0;
-    R4 z = { 0, 0, 0, 0 };
-    for (int j = 0; j < nhitpar; j++) {
-        /* subgroup (1,2) */
-        x0 = FN(mul3)(&U0, staple);
-        r0.u1 = x0.u1; r0.u2 = x0.u2; r0.v1 = x0.v1; r0.v2 = x0.v2;
-        if (kind == 0) FN(kp_step)(&r0, beta, p, 1); else FN(or_step)(&r0);
-        Vg.uv1 = z; Vg.uv2 = z;
-        Vg.uv1.x = r0.u1.re; Vg.uv1.y = r0.u2.re;
-        Vg.uv2.x = r0.u1.im; Vg.uv2.y = r0.u2.im;
-        Vg.uv3.x = r0.v1.re; Vg.uv3.y = r0.v2.re; Vg.uv3.z = r0.v1.im; Vg.uv3.w = r0.v2.im;
-        m1 = FN(times3)(Vg, m3);
-        U0 = FN(rec3)(m1);
-        /* subgroup (1,3) */
-        x0 = FN(mul3)(&U0, staple);
-        r0.u1 = x0.u1; r0.u2 = x0.u3; r0.v1 = x0.w1; r0.v2 = x0.w3;
-        if (kind == 0) FN(kp_step)(&r0, beta, p, 1); else FN(or_step)(&r0);
-        Vg.uv1 = z; Vg.uv2 = z; Vg.uv3 = z;
-        Vg.uv1.x = r0.u1.re; Vg.uv1.z = r0.u2.re;
-        Vg.uv2.x = r0.u1.im; Vg.uv2.z = r0.u2.im;
-        Vg.uv3.y = 1;
-        m2 = FN(times3)(Vg, m1);
-        U0 = FN(rec3)(m2);
-        /* subgroup (2,3) */
-        x0 = FN(mul3)(&U0, staple);
-        r0.u1 = x0.v2; r0.u2 = x0.v3; r0.v1 = x0.w2; r0.v2 = x0.w3;
-        if (kind == 0) FN(kp_step)(&r0, beta, p, 1); else FN(or_step)(&r0);
-        Vg.uv1 = z; Vg.uv2 = z; Vg.uv3 = z;
-        Vg.uv1.x = 1; Vg.uv1.w = r0.u2.re;
-        Vg.uv2.w = r0.u2.im;
-        Vg.uv3.y = r0.u1.re; Vg.uv3.w = r0.u1.im;
-        m3 = FN(times3)(Vg, m2);
-        reslt = FN(gs3)(m3);
-        U0 = FN(rec3)(reslt);
+    for (int k = 0; k < 3; k++) {
+        CX x = U->m[i][k], y = U->m[j][k];
+        REAL re = V->u1.re * x.re; re = RFMA(-V->u1.im, x.im, re); re = RFMA(V->u2.re, y.re, re); re = RFMA(-V->u2.im, y.im, re);
+        REAL im = V->u1.re * x.im; im = RFMA(V->u1.im, x.re, im); im = RFMA(V->u2.re, y.im, im); im = RFMA(V->u2.im, y.re, im);
+        REAL re2 = V->v1.re * x.re; re2 = RFMA(-V->v1.im, x.im, re2); re2 = RFMA(V->v2.re, y.re, re2); re2 = RFMA(-V->v2.im, y.im, re2);
+        REAL im2 = V->v1.re * x.im; im2 = RFMA(V->v1.im, x.re, im2); im2 = RFMA(V->v2.re, y.im, im2); im2 = RFMA(V->v2.im, y.re, im2);
+        U->m[i][k].re = re;  U->m[i][k].im = im;
+        U->m[j][k].re = re2; U->m[j][k].im = im2;
+    }
+}
+
+/* Cabibbo-Marinari over the SU(2) subgroups (1,2), (1,3), (2,3); restates
+ * lattice_heatbath3, su3_update_cl.cl:672-779: for each subgroup the block
+ * of W = U*staple (matrix_times_su3), the Kennedy-Pendleton draw and the
+ * subgroup rotation V*U of the two rows; then Gram-Schmidt.
+ * kind 0 = heatbath, 1 = overrelaxation. */
+static G3 FN(cm3)(const M3 *S, G3 m0, REAL beta, FN(prnctx) *p, int nhitpar, int kind)
+{
+    G3 reslt = m0;
+    M3 U = FN(expand)(m0);
+    for (int n = 0; n < nhitpar; n++) {
+        for (int sg = 0; sg < 3; sg++) {
+            int i = (sg == 2) ? 1 : 0, j = (sg == 0) ? 1 : 2;
+            S2 r0;
+            r0.u1 = FN(dot3)(&U.m[i][0], 1, &S->m[0][i], 3);
+            r0.u2 = FN(dot3)(&U.m[i][0], 1, &S->m[0][j], 3);
+            r0.v1 = FN(dot3)(&U.m[j][0], 1, &S->m[0][i], 3);
+            r0.v2 = FN(dot3)(&U.m[j][0], 1, &S->m[0][j], 3);
+            if (kind == 0) FN(kp_step)(&r0, beta, p, 1); else FN(or_step)(&r0);
+            FN(rotate_rows)(&U, i, j, &r0);
+        }
+        reslt = FN(gs3)(FN(compress)(&U));
+        U = FN(expand)(reslt);
     }
     return reslt;
 }
@@ -449,12 +516,12 @@ static G3 FN(cm3)(const S3 *staple, G3 m0, REAL beta, FN(prnctx) *p, int nhitpar
  * pairwise as written there (forward+backward per plane, running sum). */
 static const int FN(nu_order)[4][3] = { {1, 2, 3}, {0, 2, 3}, {1, 0, 3}, {1, 2, 0} };
 
-static S3 FN(staple3)(const ol_cfg *c, const REAL *tab, unsigned g, int mu)
+static M3 FN(staple3)(const ol_cfg *c, const REAL *tab, unsigned g, int mu)
 {
     crd co, cp, cn, cm, cmp;
     gid2c(c, g, &co);
     cp = nb_plus(c, co, mu);
-    S3 st, s2;
+    M3 st, s2;
     for (int i = 0; i < 3; i++) {
         int nu = FN(nu_order)[mu][i];
         cn = nb_plus(c, co, nu);
@@ -463,11 +530,11 @@ static S3 FN(staple3)(const ol_cfg *c, const REAL *tab, unsigned g, int mu)
         G3 a = FN(load3)(c, tab, &cp, c2gid(c, cp), nu);
         G3 b = FN(load3)(c, tab, &cn, c2gid(c, cn), mu);
         G3 d = FN(load3)(c, tab, &co, g, nu);
-        S3 fw = FN(staple_fwd3)(a, b, d);
+        M3 fw = FN(staple_fwd3)(a, b, d);
         a = FN(load3)(c, tab, &cmp, c2gid(c, cmp), nu);
         b = FN(load3)(c, tab, &cm, c2gid(c, cm), mu);
         d = FN(load3)(c, tab, &cm, c2gid(c, cm), nu);
-        S3 bw = FN(staple_bwd3)(a, b, d);
+        M3 bw = FN(staple_bwd3)(a, b, d);
         if (i == 0) {
             st = FN(add3)(&fw, &bw);                   /* staple  = f0 + b0    */
         } else {
@@ -521,7 +588,7 @@ static void FN(phase)(const ol_cfg *c, REAL *tab, int parity, int mu, const ol_p
         p.src = src; p.cfg = c; p.thread = t; p.k = 0; p.gidval = (double)(float)g;
         if (c->group == 3) {
             G3 m0 = FN(load3)(c, tab, &co, g, mu);
-            S3 st = FN(staple3)(c, tab, g, mu);
+            M3 st = FN(staple3)(c, tab, g, mu);
             G3 mU = FN(cm3)(&st, m0, beta, &p, c->nhitpar, kind);
             FN(store3)(c, tab, g, mu, mU);
         } else {
@@ -540,7 +607,9 @@ static void FN(phase)(const ol_cfg *c, REAL *tab, int parity, int mu, const ol_p
                 R4 aH;
                 REAL Mx = st.u1.re + st.v2.re, My = st.u1.im - st.v2.im;
                 REAL Mz = st.u2.re - st.v1.re, Mw = st.u2.im + st.v1.im;
-                REAL det = RSQRT(Mx * Mx + My * My + Mz * Mz + Mw * Mw);
+                REAL n2 = Mx * Mx;
+                n2 = RFMA(My, My, n2); n2 = RFMA(Mz, Mz, n2); n2 = RFMA(Mw, Mw, n2);
+                REAL det = RSQRT(n2);
                 aH.x = Mx / det; aH.z = -My / det; aH.y = -Mz / det; aH.w = -Mw / det;
                 G2 r;
                 r.uv1 = FN(times2)(FN(times2)(aH, FN(herm2)(m0.uv1)), aH);
@@ -709,7 +778,7 @@ static void FN(to_d3)(G3 a, cd3 *b)
     ad.uv1.x = (double)a.uv1.x; ad.uv1.y = (double)a.uv1.y; ad.uv1.z = (double)a.uv1.z; ad.uv1.w = (double)a.uv1.w;
     ad.uv2.x = (double)a.uv2.x; ad.uv2.y = (double)a.uv2.y; ad.uv2.z = (double)a.uv2.z; ad.uv2.w = (double)a.uv2.w;
     ad.uv3.x = (double)a.uv3.x; ad.uv3.y = (double)a.uv3.y; ad.uv3.z = (double)a.uv3.z; ad.uv3.w = (double)a.uv3.w;
-    s3_d s = rec3_d(ad);
+    m3_d s = expand_d(ad);
     memcpy(b, &s, sizeof(s));
 }
 static void FN(to_d2)(R4 a, cd3 *b)
@@ -774,14 +843,14 @@ static void FN(polyakov)(const ol_cfg *c, const REAL *tab, double out[4])
                 crd co = { x, y, z, 0 };
                 double pr, pi;
                 if (c->group == 3) {
-                    S3 v0 = FN(rec3)(FN(load3)(c, tab, &co, c2gid(c, co), 3));
+                    M3 v0 = FN(expand)(FN(load3)(c, tab, &co, c2gid(c, co), 3));
                     for (int i = 1; i < c->n[3]; i++) {
                         co = nb_plus(c, co, 3);
-                        S3 v1 = FN(rec3)(FN(load3)(c, tab, &co, c2gid(c, co), 3));
+                        M3 v1 = FN(expand)(FN(load3)(c, tab, &co, c2gid(c, co), 3));
                         v0 = FN(mul3)(&v0, &v1);
                     }
-                    pr = (double)v0.u1.re + (double)v0.v2.re + (double)v0.w3.re;
-                    pi = (double)v0.u1.im + (double)v0.v2.im + (double)v0.w3.im;
+                    pr = (double)v0.m[0][0].re + (double)v0.m[1][1].re + (double)v0.m[2][2].re;
+                    pi = (double)v0.m[0][0].im + (double)v0.m[1][1].im + (double)v0.m[2][2].im;
                 } else {
                     S2 v0 = FN(rec2)(FN(load2)(c, tab, &co, c2gid(c, co), 3).uv1);
                     for (int i = 1; i < c->n[3]; i++) {
@@ -842,10 +911,10 @@ static double FN(local_action)(const ol_cfg *c, const REAL *tab, unsigned g, int
     crd co; gid2c(c, g, &co);
     double s = 0;
     if (c->group == 3) {
-        S3 st = FN(staple3)(c, tab, g, mu);
-        S3 u = FN(rec3)(FN(load3)(c, tab, &co, g, mu));
-        S3 p = FN(mul3)(&u, &st);
-        s = (double)p.u1.re + (double)p.v2.re + (double)p.w3.re;
+        M3 st = FN(staple3)(c, tab, g, mu);
+        M3 u = FN(expand)(FN(load3)(c, tab, &co, g, mu));
+        M3 p = FN(mul3)(&u, &st);
+        s = (double)p.m[0][0].re + (double)p.m[1][1].re + (double)p.m[2][2].re;
     } else {
         S2 st = FN(staple2)(c, tab, g, mu);
         S2 u = FN(rec2)(FN(load2)(c, tab, &co, g, mu).uv1);
@@ -859,7 +928,8 @@ static double FN(local_action)(const ol_cfg *c, const REAL *tab, unsigned g, int
 #undef R4
 #undef CX
 #undef G3
-#undef S3
+#undef M3
+#undef RFMA
 #undef G2
 #undef S2
 #undef FN

@@ -22,7 +22,9 @@ BIN = os.path.join(PKG, "bin")
 INCLUDE = os.path.join(ROOT, "include")
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-NVCC_FLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-I" + INCLUDE]
+# -fmad=false: every fused multiply-add in the kernels is an explicit fma()
+# in a fixed order, so results do not depend on the compiler's contraction
+NVCC_FLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-fmad=false", "-Xcompiler", "-fPIC", "-I" + INCLUDE]
 CUDA_SOURCES = ["qg_update_f32.cu", "qg_update_f64.cu", "qg_fields.cu", "qg_ranlux.cu", "qg_capi.cu"]
 HOST_SOURCES = ["qg_host.cpp", "qcdgpu_main.cpp"]
 

@@ -140,11 +140,13 @@ extern "C" int qg_create(const qg_config *cfg, qg_ctx **out)
     c->rowsize = align_up(V, A);
     c->prngstep = align_up(V / 2, A);
     c->instances = cfg->prng_instances;
-    uint64_t total;
-    if (cfg->start == QG_START_HOT)
-        total = align_up((uint64_t)c->rowsize * 4 + 3ull * c->prngstep * (cfg->nhit + 1), A);
-    else
-        total = align_up((uint64_t)cfg->nhitpar * 3ull * c->prngstep * (cfg->nhit + 1), A);
+    // PRNG_samples (suncl.cpp:2304-2307); the hot-start batch must also
+    // cover the heatbath's NHITPar * 3 * (NHIT+1) quads per link
+    uint64_t total = align_up((uint64_t)cfg->nhitpar * 3ull * c->prngstep * (cfg->nhit + 1), A);
+    if (cfg->start == QG_START_HOT) {
+        uint64_t hot = align_up((uint64_t)c->rowsize * 4 + 3ull * c->prngstep * (cfg->nhit + 1), A);
+        if (hot > total) total = hot;
+    }
     c->samples = (uint32_t)(1 + (total - 1) / (uint64_t)c->instances);
     const int planes = cfg->group == 3 ? 12 : 4;
     const size_t rsz = cfg->precision ? sizeof(double) : sizeof(float);
@@ -494,8 +496,8 @@ extern "C" int qg_measure_wilson(qg_ctx *c, int R, int T, double *out)
     if (R < 1 || T < 1 || R > c->G.n[0] || T > c->G.n[3]) return fail(c, QG_ERR_ARG, "Wilson loop extent out of range");
     const qg_config &f = c->cfg;
     int tw = !(f.phi == 0.0 && f.omega == 0.0);
-    QG_CK(launch_wilson(c->G, c->links, f.group, f.precision, R, T, (float)f.phi, (float)f.omega, tw, c->partials,
-                        c->d_results, c->stream), "wilson");
+    QG_CK(launch_wilson(c->G, c->links, f.group, f.precision, R, T, c->d_params, tw, c->partials, c->d_results,
+                        c->stream), "wilson");
     return measure_to_host(c, 1, out);
 }
 
@@ -507,8 +509,8 @@ extern "C" int qg_measure(qg_ctx *c, int what, double *out)
     switch (what) {
     case QG_MEAS_PLAQUETTE:
     case QG_MEAS_ACTION: {
-        QG_CK(launch_plaquette(c->G, c->links, f.group, f.precision, f.beta / f.group, (float)f.phi, (float)f.omega, tw,
-                               c->partials, c->d_results, c->stream), "plaquette");
+        QG_CK(launch_plaquette(c->G, c->links, f.group, f.precision, c->d_params, tw, c->partials, c->d_results,
+                               c->stream), "plaquette");
         double r[4];
         int rc = measure_to_host(c, 4, r);
         if (rc) return rc;
@@ -517,8 +519,7 @@ extern "C" int qg_measure(qg_ctx *c, int what, double *out)
         return QG_OK;
     }
     case QG_MEAS_POLYAKOV:
-        QG_CK(launch_polyakov(c->G, c->links, f.group, f.precision, (float)f.phi, (float)f.omega, tw, c->partials,
-                              c->d_results, c->stream), "polyakov");
+        QG_CK(launch_polyakov(c->G, c->links, f.group, f.precision, c->partials, c->d_results, c->stream), "polyakov");
         return measure_to_host(c, 4, out);
     case QG_MEAS_WILSON:
         return qg_measure_wilson(c, f.wilson_r, f.wilson_t, out);

@@ -22,6 +22,11 @@ Geom make_geom(const int n[4])
     return G;
 }
 
+template <typename Real>
+__device__ __forceinline__ Real param_real(double v) { return (Real)(float)v; }
+template <>
+__device__ __forceinline__ double param_real<double>(double v) { return v; }
+
 static __device__ __forceinline__ uint32_t native_index(const Geom &G, uint32_t s, const Crd &c)
 {
     return (uint32_t)parity_of(c) * G.cb + (s >> 1);
@@ -314,61 +319,58 @@ cudaError_t launch_to_ref(const Geom &G, const void *links, void *ref, int group
 // su3_measurements_cl.cl:292-319, su2_measurements_cl.cl:126-141); SU(2)
 // is embedded in the upper 2x2 block with a zero third row and column.
 template <int NC, typename Real>
-__device__ __forceinline__ S3<double> load_d(const Field<Real> &U, const Geom &G, const Crd &c, int mu, float phi,
-                                             float omega, int twist)
+__device__ __forceinline__ M3<double> load_d(const Field<Real> &U, const Geom &G, const Crd &c, int mu,
+                                             const double *params, int twist)
 {
     uint32_t e = cb_index(G, c, parity_of(c));
-    S3<double> d;
+    M3<double> d;
     if (NC == 3) {
         G3<Real> m = U.ldg3(mu, e);
-        if (twist && mu == 1 && c.x == G.n[0] - 1) m = twist3(m, (Real)phi, (Real)omega);
+        if (twist && mu == 1 && c.x == G.n[0] - 1) m = twist3(m, param_real<Real>(params[1]), param_real<Real>(params[2]));
         G3<double> md;
         md.uv1 = { (double)m.uv1.x, (double)m.uv1.y, (double)m.uv1.z, (double)m.uv1.w };
         md.uv2 = { (double)m.uv2.x, (double)m.uv2.y, (double)m.uv2.z, (double)m.uv2.w };
         md.uv3 = { (double)m.uv3.x, (double)m.uv3.y, (double)m.uv3.z, (double)m.uv3.w };
-        d = rec3(md);
+        d = expand(md);
     } else {
         R4<Real> m = U.ldg2(mu, e);
         if (twist && mu == 1 && c.x == G.n[0] - 1) {
-            Real ph = (Real)phi;
+            Real ph = param_real<Real>(params[1]);
             R4<Real> om = { RC<Real>::cs(ph / 2), 0, RC<Real>::sn(ph / 2), 0 };
             m = times2(om, m);
         }
-        d.u1 = { (double)m.x, (double)m.z }; d.u2 = { (double)m.y, (double)m.w }; d.u3 = { 0, 0 };
-        d.v1 = { -(double)m.y, (double)m.w }; d.v2 = { (double)m.x, -(double)m.z }; d.v3 = { 0, 0 };
-        d.w1 = { 0, 0 }; d.w2 = { 0, 0 }; d.w3 = { 0, 0 };
+        for (int i = 0; i < 3; i++)
+            for (int j = 0; j < 3; j++) d.m[i][j] = { 0.0, 0.0 };
+        d.m[0][0] = { (double)m.x, (double)m.z }; d.m[0][1] = { (double)m.y, (double)m.w };
+        d.m[1][0] = { -(double)m.y, (double)m.w }; d.m[1][1] = { (double)m.x, -(double)m.z };
     }
     return d;
 }
 
-__device__ __forceinline__ S3<double> mulf(const S3<double> &u, const S3<double> &v)
+template <typename T>
+__device__ __forceinline__ M3<T> mulf(const M3<T> &u, const M3<T> &v)
 {
-    S3<double> t;
-    t.u1 = dot3(u.u1, u.u2, u.u3, v.u1, v.v1, v.w1);
-    t.u2 = dot3(u.u1, u.u2, u.u3, v.u2, v.v2, v.w2);
-    t.u3 = dot3(u.u1, u.u2, u.u3, v.u3, v.v3, v.w3);
-    t.v1 = dot3(u.v1, u.v2, u.v3, v.u1, v.v1, v.w1);
-    t.v2 = dot3(u.v1, u.v2, u.v3, v.u2, v.v2, v.w2);
-    t.v3 = dot3(u.v1, u.v2, u.v3, v.u3, v.v3, v.w3);
-    t.w1 = dot3(u.w1, u.w2, u.w3, v.u1, v.v1, v.w1);
-    t.w2 = dot3(u.w1, u.w2, u.w3, v.u2, v.v2, v.w2);
-    t.w3 = dot3(u.w1, u.w2, u.w3, v.u3, v.v3, v.w3);
+    M3<T> t;
+#pragma unroll
+    for (int i = 0; i < 3; i++)
+#pragma unroll
+        for (int j = 0; j < 3; j++) t.m[i][j] = dot3(&u.m[i][0], 1, &v.m[0][j], 3);
     return t;
 }
-__device__ __forceinline__ S3<double> hermf(const S3<double> &a)
-{
-    S3<double> r;
-    r.u1 = { a.u1.re, -a.u1.im }; r.u2 = { a.v1.re, -a.v1.im }; r.u3 = { a.w1.re, -a.w1.im };
-    r.v1 = { a.u2.re, -a.u2.im }; r.v2 = { a.v2.re, -a.v2.im }; r.v3 = { a.w2.re, -a.w2.im };
-    r.w1 = { a.u3.re, -a.u3.im }; r.w2 = { a.v3.re, -a.v3.im }; r.w3 = { a.w3.re, -a.w3.im };
-    return r;
-}
 // Re Tr(a b c^+ d^+)  (lattice_retrace_plaquette3, su3_measurements_cl.cl:527-548)
-__device__ __forceinline__ double retr4(const S3<double> &a, const S3<double> &b, const S3<double> &c,
-                                        const S3<double> &d)
+__device__ __forceinline__ double retr4(const M3<double> &a, const M3<double> &b, const M3<double> &c,
+                                        const M3<double> &d)
 {
-    S3<double> w = mulf(mulf(mulf(a, b), hermf(c)), hermf(d));
-    return w.u1.re + w.v2.re + w.w3.re;
+    M3<double> ab = mulf(a, b), abc, abcd;
+#pragma unroll
+    for (int i = 0; i < 3; i++)
+#pragma unroll
+        for (int j = 0; j < 3; j++) abc.m[i][j] = dotc3(&ab.m[i][0], 1, &c.m[j][0], 1);
+    double tr = 0;
+#pragma unroll
+    for (int i = 0; i < 3; i++) tr += dotc3(&abc.m[i][0], 1, &d.m[i][0], 1).re;
+    (void)abcd;
+    return tr;
 }
 
 // warp + block sum of K doubles; thread 0 writes the block's partials
@@ -398,25 +400,26 @@ __device__ __forceinline__ void block_sum_store(double (&v)[K], double *partials
 // 55-184,1178-1311): per site the xy,xz,yz (spatial) and xt,yt,zt
 // (temporal) plaquettes in FP64; also the action (beta/N)(3N - ReTr).
 template <int NC, typename Real>
-__global__ void __launch_bounds__(256) k_plaquette(Field<Real> U, Geom G, double bet, float phi, float omega,
-                                                    int twist, double *partials)
+__global__ void __launch_bounds__(256) k_plaquette(Field<Real> U, Geom G, const double *params, int twist,
+                                                    double *partials)
 {
     uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
     double v[4] = { 0, 0, 0, 0 };
     if (s < G.V) {
         Crd c = lex2crd(G, s);
         const Crd cx = step_plus(G, c, 0), cy = step_plus(G, c, 1), cz = step_plus(G, c, 2), ct = step_plus(G, c, 3);
-        S3<double> m1 = load_d<NC, Real>(U, G, c, 0, phi, omega, twist);
-        S3<double> m4 = load_d<NC, Real>(U, G, c, 1, phi, omega, twist);
-        S3<double> m5 = load_d<NC, Real>(U, G, c, 2, phi, omega, twist);
-        S3<double> m6 = load_d<NC, Real>(U, G, c, 3, phi, omega, twist);
+        M3<double> m1 = load_d<NC, Real>(U, G, c, 0, params, twist);
+        M3<double> m4 = load_d<NC, Real>(U, G, c, 1, params, twist);
+        M3<double> m5 = load_d<NC, Real>(U, G, c, 2, params, twist);
+        M3<double> m6 = load_d<NC, Real>(U, G, c, 3, params, twist);
+        const double bet = (double)param_real<Real>(params[0]);
         double rs, rt;
-        rs  = retr4(m1, load_d<NC, Real>(U, G, cx, 1, phi, omega, twist), load_d<NC, Real>(U, G, cy, 0, phi, omega, twist), m4);
-        rs += retr4(m1, load_d<NC, Real>(U, G, cx, 2, phi, omega, twist), load_d<NC, Real>(U, G, cz, 0, phi, omega, twist), m5);
-        rt  = retr4(m1, load_d<NC, Real>(U, G, cx, 3, phi, omega, twist), load_d<NC, Real>(U, G, ct, 0, phi, omega, twist), m6);
-        rs += retr4(m4, load_d<NC, Real>(U, G, cy, 2, phi, omega, twist), load_d<NC, Real>(U, G, cz, 1, phi, omega, twist), m5);
-        rt += retr4(m4, load_d<NC, Real>(U, G, cy, 3, phi, omega, twist), load_d<NC, Real>(U, G, ct, 1, phi, omega, twist), m6);
-        rt += retr4(m5, load_d<NC, Real>(U, G, cz, 3, phi, omega, twist), load_d<NC, Real>(U, G, ct, 2, phi, omega, twist), m6);
+        rs  = retr4(m1, load_d<NC, Real>(U, G, cx, 1, params, twist), load_d<NC, Real>(U, G, cy, 0, params, twist), m4);
+        rs += retr4(m1, load_d<NC, Real>(U, G, cx, 2, params, twist), load_d<NC, Real>(U, G, cz, 0, params, twist), m5);
+        rt  = retr4(m1, load_d<NC, Real>(U, G, cx, 3, params, twist), load_d<NC, Real>(U, G, ct, 0, params, twist), m6);
+        rs += retr4(m4, load_d<NC, Real>(U, G, cy, 2, params, twist), load_d<NC, Real>(U, G, cz, 1, params, twist), m5);
+        rt += retr4(m4, load_d<NC, Real>(U, G, cy, 3, params, twist), load_d<NC, Real>(U, G, ct, 1, params, twist), m6);
+        rt += retr4(m5, load_d<NC, Real>(U, G, cz, 3, params, twist), load_d<NC, Real>(U, G, ct, 2, params, twist), m6);
         v[0] = rs; v[1] = rt;
         v[2] = bet * (3.0 * NC - rs);
         v[3] = bet * (3.0 * NC - rt);
@@ -426,20 +429,18 @@ __global__ void __launch_bounds__(256) k_plaquette(Field<Real> U, Geom G, double
 
 uint32_t plaq_blocks(const Geom &G) { return (G.V + 255) / 256; }
 
-cudaError_t launch_plaquette(const Geom &G, const void *links, int group, int prec, double beta_over_n, float phi,
-                             float omega, int twist, double *partials, double *out, cudaStream_t s)
+cudaError_t launch_plaquette(const Geom &G, const void *links, int group, int prec, const double *params, int twist,
+                             double *partials, double *out, cudaStream_t s)
 {
     uint32_t nb = plaq_blocks(G);
     if (prec) {
         Field<double> U{ (double4 *)links, G.pstride };
-        double bet = beta_over_n;
-        if (group == 3) k_plaquette<3, double><<<nb, 256, 0, s>>>(U, G, bet, phi, omega, twist, partials);
-        else k_plaquette<2, double><<<nb, 256, 0, s>>>(U, G, bet, phi, omega, twist, partials);
+        if (group == 3) k_plaquette<3, double><<<nb, 256, 0, s>>>(U, G, params, twist, partials);
+        else k_plaquette<2, double><<<nb, 256, 0, s>>>(U, G, params, twist, partials);
     } else {
         Field<float> U{ (float4 *)links, G.pstride };
-        double bet = (double)(float)beta_over_n;
-        if (group == 3) k_plaquette<3, float><<<nb, 256, 0, s>>>(U, G, bet, phi, omega, twist, partials);
-        else k_plaquette<2, float><<<nb, 256, 0, s>>>(U, G, bet, phi, omega, twist, partials);
+        if (group == 3) k_plaquette<3, float><<<nb, 256, 0, s>>>(U, G, params, twist, partials);
+        else k_plaquette<2, float><<<nb, 256, 0, s>>>(U, G, params, twist, partials);
     }
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
@@ -449,8 +450,7 @@ cudaError_t launch_plaquette(const Geom &G, const void *links, int group, int pr
 // lattice_polyakov (polyakov.cl:54-140): ordered product of the N4 T-links
 // in link precision, traces accumulated in FP64
 template <int NC, typename Real>
-__global__ void __launch_bounds__(256) k_polyakov(Field<Real> U, Geom G, float phi, float omega, int twist,
-                                                   double *partials)
+__global__ void __launch_bounds__(256) k_polyakov(Field<Real> U, Geom G, double *partials)
 {
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     const uint32_t nsp = (uint32_t)G.n[0] * G.n[1] * G.n[2];
@@ -464,25 +464,14 @@ __global__ void __launch_bounds__(256) k_polyakov(Field<Real> U, Geom G, float p
         c.t = 0;
         double pr, pi;
         if (NC == 3) {
-            G3<Real> m = U.ldg3(3, cb_index(G, c, parity_of(c)));
-            S3<Real> v0 = rec3(m);
+            M3<Real> v0 = expand(U.ldg3(3, cb_index(G, c, parity_of(c))));
             for (int k = 1; k < G.n[3]; k++) {
                 c.t = k;
-                S3<Real> v1 = rec3(U.ldg3(3, cb_index(G, c, parity_of(c))));
-                S3<Real> w;
-                w.u1 = dot3(v0.u1, v0.u2, v0.u3, v1.u1, v1.v1, v1.w1);
-                w.u2 = dot3(v0.u1, v0.u2, v0.u3, v1.u2, v1.v2, v1.w2);
-                w.u3 = dot3(v0.u1, v0.u2, v0.u3, v1.u3, v1.v3, v1.w3);
-                w.v1 = dot3(v0.v1, v0.v2, v0.v3, v1.u1, v1.v1, v1.w1);
-                w.v2 = dot3(v0.v1, v0.v2, v0.v3, v1.u2, v1.v2, v1.w2);
-                w.v3 = dot3(v0.v1, v0.v2, v0.v3, v1.u3, v1.v3, v1.w3);
-                w.w1 = dot3(v0.w1, v0.w2, v0.w3, v1.u1, v1.v1, v1.w1);
-                w.w2 = dot3(v0.w1, v0.w2, v0.w3, v1.u2, v1.v2, v1.w2);
-                w.w3 = dot3(v0.w1, v0.w2, v0.w3, v1.u3, v1.v3, v1.w3);
-                v0 = w;
+                M3<Real> v1 = expand(U.ldg3(3, cb_index(G, c, parity_of(c))));
+                v0 = mulf(v0, v1);
             }
-            pr = (double)v0.u1.re + (double)v0.v2.re + (double)v0.w3.re;
-            pi = (double)v0.u1.im + (double)v0.v2.im + (double)v0.w3.im;
+            pr = (double)v0.m[0][0].re + (double)v0.m[1][1].re + (double)v0.m[2][2].re;
+            pi = (double)v0.m[0][0].im + (double)v0.m[1][1].im + (double)v0.m[2][2].im;
         } else {
             S2<Real> v0 = rec2(U.ldg2(3, cb_index(G, c, parity_of(c))));
             for (int k = 1; k < G.n[3]; k++) {
@@ -496,24 +485,23 @@ __global__ void __launch_bounds__(256) k_polyakov(Field<Real> U, Geom G, float p
         double q2 = pr * pr + pi * pi;
         v[0] = pr; v[1] = pi; v[2] = q2; v[3] = q2 * q2;
     }
-    (void)phi; (void)omega; (void)twist;
     block_sum_store<4>(v, partials);
 }
 
 uint32_t poly_blocks(const Geom &G) { return ((uint32_t)G.n[0] * G.n[1] * G.n[2] + 255) / 256; }
 
-cudaError_t launch_polyakov(const Geom &G, const void *links, int group, int prec, float phi, float omega, int twist,
-                            double *partials, double *out, cudaStream_t s)
+cudaError_t launch_polyakov(const Geom &G, const void *links, int group, int prec, double *partials, double *out,
+                            cudaStream_t s)
 {
     uint32_t nb = poly_blocks(G);
     if (prec) {
         Field<double> U{ (double4 *)links, G.pstride };
-        if (group == 3) k_polyakov<3, double><<<nb, 256, 0, s>>>(U, G, phi, omega, twist, partials);
-        else k_polyakov<2, double><<<nb, 256, 0, s>>>(U, G, phi, omega, twist, partials);
+        if (group == 3) k_polyakov<3, double><<<nb, 256, 0, s>>>(U, G, partials);
+        else k_polyakov<2, double><<<nb, 256, 0, s>>>(U, G, partials);
     } else {
         Field<float> U{ (float4 *)links, G.pstride };
-        if (group == 3) k_polyakov<3, float><<<nb, 256, 0, s>>>(U, G, phi, omega, twist, partials);
-        else k_polyakov<2, float><<<nb, 256, 0, s>>>(U, G, phi, omega, twist, partials);
+        if (group == 3) k_polyakov<3, float><<<nb, 256, 0, s>>>(U, G, partials);
+        else k_polyakov<2, float><<<nb, 256, 0, s>>>(U, G, partials);
     }
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
@@ -523,7 +511,7 @@ cudaError_t launch_polyakov(const Geom &G, const void *links, int group, int pre
 // lattice_measurement_wilson (wilson_loop.cl:55-454): per site and i in
 // {x,y,z}, Re Tr(L_t^T(x) L_i^R(x+T t) L_t^T(x+R i)^+ L_i^R(x)^+) in FP64
 template <int NC, typename Real>
-__global__ void __launch_bounds__(128) k_wilson(Field<Real> U, Geom G, int R, int T, float phi, float omega, int twist,
+__global__ void __launch_bounds__(128) k_wilson(Field<Real> U, Geom G, int R, int T, const double *params, int twist,
                                                  double *partials)
 {
     uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
@@ -531,22 +519,22 @@ __global__ void __launch_bounds__(128) k_wilson(Field<Real> U, Geom G, int R, in
     if (s < G.V) {
         const Crd c1 = lex2crd(G, s);
         Crd co = c1;
-        S3<double> m1 = load_d<NC, Real>(U, G, co, 3, phi, omega, twist);
-        for (int k = 1; k < T; k++) { co = step_plus(G, co, 3); m1 = mulf(m1, load_d<NC, Real>(U, G, co, 3, phi, omega, twist)); }
+        M3<double> m1 = load_d<NC, Real>(U, G, co, 3, params, twist);
+        for (int k = 1; k < T; k++) { co = step_plus(G, co, 3); m1 = mulf(m1, load_d<NC, Real>(U, G, co, 3, params, twist)); }
         const Crd c2 = step_plus(G, co, 3);
         double acc = 0;
         for (int i = 0; i < 3; i++) {
             Crd a = c1, b = c2;
-            S3<double> m4 = load_d<NC, Real>(U, G, a, i, phi, omega, twist);
-            S3<double> m2 = load_d<NC, Real>(U, G, b, i, phi, omega, twist);
+            M3<double> m4 = load_d<NC, Real>(U, G, a, i, params, twist);
+            M3<double> m2 = load_d<NC, Real>(U, G, b, i, params, twist);
             for (int k = 1; k < R; k++) {
                 a = step_plus(G, a, i); b = step_plus(G, b, i);
-                m4 = mulf(m4, load_d<NC, Real>(U, G, a, i, phi, omega, twist));
-                m2 = mulf(m2, load_d<NC, Real>(U, G, b, i, phi, omega, twist));
+                m4 = mulf(m4, load_d<NC, Real>(U, G, a, i, params, twist));
+                m2 = mulf(m2, load_d<NC, Real>(U, G, b, i, params, twist));
             }
             Crd c4 = step_plus(G, a, i);
-            S3<double> m3 = load_d<NC, Real>(U, G, c4, 3, phi, omega, twist);
-            for (int k = 1; k < T; k++) { c4 = step_plus(G, c4, 3); m3 = mulf(m3, load_d<NC, Real>(U, G, c4, 3, phi, omega, twist)); }
+            M3<double> m3 = load_d<NC, Real>(U, G, c4, 3, params, twist);
+            for (int k = 1; k < T; k++) { c4 = step_plus(G, c4, 3); m3 = mulf(m3, load_d<NC, Real>(U, G, c4, 3, params, twist)); }
             acc += retr4(m1, m2, m3, m4);
         }
         v[0] = acc;
@@ -554,18 +542,18 @@ __global__ void __launch_bounds__(128) k_wilson(Field<Real> U, Geom G, int R, in
     block_sum_store<1>(v, partials);
 }
 
-cudaError_t launch_wilson(const Geom &G, const void *links, int group, int prec, int R, int T, float phi, float omega,
+cudaError_t launch_wilson(const Geom &G, const void *links, int group, int prec, int R, int T, const double *params,
                           int twist, double *partials, double *out, cudaStream_t s)
 {
     uint32_t nb = (G.V + 127) / 128;
     if (prec) {
         Field<double> U{ (double4 *)links, G.pstride };
-        if (group == 3) k_wilson<3, double><<<nb, 128, 0, s>>>(U, G, R, T, phi, omega, twist, partials);
-        else k_wilson<2, double><<<nb, 128, 0, s>>>(U, G, R, T, phi, omega, twist, partials);
+        if (group == 3) k_wilson<3, double><<<nb, 128, 0, s>>>(U, G, R, T, params, twist, partials);
+        else k_wilson<2, double><<<nb, 128, 0, s>>>(U, G, R, T, params, twist, partials);
     } else {
         Field<float> U{ (float4 *)links, G.pstride };
-        if (group == 3) k_wilson<3, float><<<nb, 128, 0, s>>>(U, G, R, T, phi, omega, twist, partials);
-        else k_wilson<2, float><<<nb, 128, 0, s>>>(U, G, R, T, phi, omega, twist, partials);
+        if (group == 3) k_wilson<3, float><<<nb, 128, 0, s>>>(U, G, R, T, params, twist, partials);
+        else k_wilson<2, float><<<nb, 128, 0, s>>>(U, G, R, T, params, twist, partials);
     }
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;

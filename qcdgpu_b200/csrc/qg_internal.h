@@ -40,13 +40,13 @@ cudaError_t launch_to_ref(const Geom &G, const void *links, void *ref, int group
 // measurements: per-block partials into scratch, then a fixed-order final
 // reduction into out (device).  Partials sizes returned by *_blocks().
 uint32_t plaq_blocks(const Geom &G);
-cudaError_t launch_plaquette(const Geom &G, const void *links, int group, int prec, double beta_over_n,
-                             float phi, float omega, int twist, double *partials, double *out, cudaStream_t s);
+cudaError_t launch_plaquette(const Geom &G, const void *links, int group, int prec, const double *params, int twist,
+                             double *partials, double *out, cudaStream_t s);
 uint32_t poly_blocks(const Geom &G);
-cudaError_t launch_polyakov(const Geom &G, const void *links, int group, int prec, float phi, float omega,
-                            int twist, double *partials, double *out, cudaStream_t s);
-cudaError_t launch_wilson(const Geom &G, const void *links, int group, int prec, int R, int T, float phi,
-                          float omega, int twist, double *partials, double *out, cudaStream_t s);
+cudaError_t launch_polyakov(const Geom &G, const void *links, int group, int prec, double *partials, double *out,
+                            cudaStream_t s);
+cudaError_t launch_wilson(const Geom &G, const void *links, int group, int prec, int R, int T, const double *params,
+                          int twist, double *partials, double *out, cudaStream_t s);
 cudaError_t launch_reduce(const double *partials, uint32_t nblocks, int ncomp, double *out, cudaStream_t s);
 cudaError_t launch_add_u64(uint64_t *p, uint64_t v, cudaStream_t s);
 

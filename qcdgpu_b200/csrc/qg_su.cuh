@@ -4,8 +4,13 @@
 // Real is the link precision (the reference's hgpu_float, SU(N)/kernel/
 // complex.h:69-91).  In float mode the heatbath promotes to double exactly
 // where the reference's float kernels do through double literals
-// (SU(N)/suncl/su3_update_cl.cl:620,625,650-653).  Everything is
-// register-resident; no function here touches memory.
+// (SU(N)/suncl/su3_update_cl.cl:620,625,650-653).
+//
+// Every multiply-add is an explicit fma in a fixed order and the file is
+// compiled with -fmad=false, and the transcendentals on the update path
+// (sin, cos, log) are this file's own double-precision routines, so a
+// sweep is a fixed sequence of IEEE operations: the CPU oracle that
+// performs the same sequence reproduces it bit for bit.
 #pragma once
 #include <cuda_runtime.h>
 #include <stdint.h>
@@ -18,140 +23,290 @@ template <typename Real> struct CX { Real re, im; };
 // uv2 = Im(u11,u12,u13,u23), uv3 = (Re u21, Re u22, Im u21, Im u22)
 // (the gpu_su_3 form of SU(N)/suncl/model.cl:146-165)
 template <typename Real> struct G3 { R4<Real> uv1, uv2, uv3; };
-template <typename Real> struct S3 { CX<Real> u1, u2, u3, v1, v2, v3, w1, w2, w3; };
+// full 3x3 complex matrix, row major
+template <typename Real> struct M3 { CX<Real> m[3][3]; };
+// 2x2 complex block (su_2 of model.cl:168-173): (u1 u2; v1 v2)
 template <typename Real> struct S2 { CX<Real> u1, u2, v1, v2; };
+
+__device__ __forceinline__ float FMA(float a, float b, float c) { return fmaf(a, b, c); }
+__device__ __forceinline__ double FMA(double a, double b, double c) { return fma(a, b, c); }
+
+// ------------------------------------------------- elementary functions
+// sin/cos for |x| < 16: Cody-Waite reduction by pi/2 with a three-part
+// constant, Taylor polynomials of degree 17 (sin) / 18 (cos) on
+// [-pi/4, pi/4] in Horner form (truncation < 1e-19).
+__device__ __forceinline__ void qg_sincos(double x, double *s, double *c)
+{
+    const double INV_PIO2 = 0.63661977236758134308;
+    const double P1 = 1.5707963267948966, P2 = 6.123233995736766e-17, P3 = -1.4973849048591698e-33;
+    double n = rint(x * INV_PIO2);
+    double f = FMA(-n, P1, x);
+    f = FMA(-n, P2, f);
+    f = FMA(-n, P3, f);
+    double f2 = f * f;
+    double ps = 2.8114572543455206e-15;                 // 1/17!
+    ps = FMA(ps, f2, -7.6471637318198164e-13);           // -1/15!
+    ps = FMA(ps, f2, 1.6059043836821613e-10);            // 1/13!
+    ps = FMA(ps, f2, -2.5052108385441720e-08);           // -1/11!
+    ps = FMA(ps, f2, 2.7557319223985893e-06);            // 1/9!
+    ps = FMA(ps, f2, -1.9841269841269841e-04);           // -1/7!
+    ps = FMA(ps, f2, 8.3333333333333333e-03);            // 1/5!
+    ps = FMA(ps, f2, -1.6666666666666667e-01);           // -1/3!
+    double sn = FMA(ps * f2, f, f);
+    double pc = -1.5619206968586225e-16;                 // -1/18!
+    pc = FMA(pc, f2, 4.7794773323873853e-14);            // 1/16!
+    pc = FMA(pc, f2, -1.1470745597729725e-11);           // -1/14!
+    pc = FMA(pc, f2, 2.0876756987868099e-09);            // 1/12!
+    pc = FMA(pc, f2, -2.7557319223985888e-07);           // -1/10!
+    pc = FMA(pc, f2, 2.4801587301587302e-05);            // 1/8!
+    pc = FMA(pc, f2, -1.3888888888888889e-03);           // -1/6!
+    pc = FMA(pc, f2, 4.1666666666666667e-02);            // 1/4!
+    pc = FMA(pc, f2, -0.5);
+    double cs = FMA(pc, f2, 1.0);
+    int q = ((int)n) & 3;
+    double ss = (q == 0) ? sn : (q == 1) ? cs : (q == 2) ? -sn : -cs;
+    double cc = (q == 0) ? cs : (q == 1) ? -sn : (q == 2) ? -cs : sn;
+    *s = ss;
+    *c = cc;
+}
+
+// natural log for 0 < y < 2^64: y = m 2^e with m in [sqrt(1/2), sqrt(2)),
+// log m = 2 atanh(s), s = (m-1)/(m+1), odd series to s^23; ln 2 in two parts
+__device__ __forceinline__ double qg_log(double y)
+{
+    int e;
+    double m = frexp(y, &e);                             // m in [0.5, 1)
+    if (m < 0.70710678118654752440) { m = m * 2.0; e -= 1; }
+    double s = (m - 1.0) / (m + 1.0);
+    double s2 = s * s;
+    double p = 1.0 / 23.0;
+    p = FMA(p, s2, 1.0 / 21.0);
+    p = FMA(p, s2, 1.0 / 19.0);
+    p = FMA(p, s2, 1.0 / 17.0);
+    p = FMA(p, s2, 1.0 / 15.0);
+    p = FMA(p, s2, 1.0 / 13.0);
+    p = FMA(p, s2, 1.0 / 11.0);
+    p = FMA(p, s2, 1.0 / 9.0);
+    p = FMA(p, s2, 1.0 / 7.0);
+    p = FMA(p, s2, 1.0 / 5.0);
+    p = FMA(p, s2, 1.0 / 3.0);
+    double t = 2.0 * FMA(p * s2, s, s);
+    const double LN2_HI = 6.93147180369123816490e-01, LN2_LO = 1.90821492927058770002e-10;
+    double de = (double)e;
+    return FMA(de, LN2_HI, FMA(de, LN2_LO, t));
+}
 
 template <typename Real> struct RC;
 template <> struct RC<float> {
     static constexpr float PI = 3.141592653589793f;
     static constexpr float PI2 = 6.283185307179586f;
-    __device__ static float sn(float a) { return sinf(a); }
-    __device__ static float cs(float a) { return cosf(a); }
+    __device__ static float sn(float a) { double s, c; qg_sincos((double)a, &s, &c); return (float)s; }
+    __device__ static float cs(float a) { double s, c; qg_sincos((double)a, &s, &c); return (float)c; }
     __device__ static float sq(float a) { return sqrtf(a); }
 };
 template <> struct RC<double> {
     static constexpr double PI = 3.1415926535897932384626433832795;
     static constexpr double PI2 = 6.2831853071795864769252867665590;
-    __device__ static double sn(double a) { return sin(a); }
-    __device__ static double cs(double a) { return cos(a); }
+    __device__ static double sn(double a) { double s, c; qg_sincos(a, &s, &c); return s; }
+    __device__ static double cs(double a) { double s, c; qg_sincos(a, &s, &c); return c; }
     __device__ static double sq(double a) { return sqrt(a); }
 };
 
-// ---------------------------------------------------------------- SU(3)
-// third row = conj(row1 x row2)  (lattice_reconstruct3, su3cl.cl:137-165)
+// ------------------------------------------------------- complex kernels
+// sum_k a_k b_k, k = 0,1,2, accumulated in that order
 template <typename Real>
-__device__ __forceinline__ S3<Real> rec3(const G3<Real> &a)
-{
-    S3<Real> b;
-    b.u1.re = a.uv1.x; b.u1.im = a.uv2.x;
-    b.u2.re = a.uv1.y; b.u2.im = a.uv2.y;
-    b.u3.re = a.uv1.z; b.u3.im = a.uv2.z;
-    b.v1.re = a.uv3.x; b.v1.im = a.uv3.z;
-    b.v2.re = a.uv3.y; b.v2.im = a.uv3.w;
-    b.v3.re = a.uv1.w; b.v3.im = a.uv2.w;
-    b.w1.re =  b.u2.re * b.v3.re - b.u2.im * b.v3.im - b.u3.re * b.v2.re + b.u3.im * b.v2.im;
-    b.w1.im = -b.u2.re * b.v3.im - b.u2.im * b.v3.re + b.u3.re * b.v2.im + b.u3.im * b.v2.re;
-    b.w2.re =  b.u3.re * b.v1.re - b.u3.im * b.v1.im - b.u1.re * b.v3.re + b.u1.im * b.v3.im;
-    b.w2.im = -b.u3.re * b.v1.im - b.u3.im * b.v1.re + b.u1.re * b.v3.im + b.u1.im * b.v3.re;
-    b.w3.re =  b.u1.re * b.v2.re - b.u1.im * b.v2.im - b.u2.re * b.v1.re + b.u2.im * b.v1.im;
-    b.w3.im = -b.u1.re * b.v2.im - b.u1.im * b.v2.re + b.u2.re * b.v1.im + b.u2.im * b.v1.re;
-    return b;
-}
-
-template <typename Real>
-__device__ __forceinline__ G3<Real> compress3(const S3<Real> &s)
-{
-    G3<Real> g;
-    g.uv1 = { s.u1.re, s.u2.re, s.u3.re, s.v3.re };
-    g.uv2 = { s.u1.im, s.u2.im, s.u3.im, s.v3.im };
-    g.uv3 = { s.v1.re, s.v2.re, s.v1.im, s.v2.im };
-    return g;
-}
-
-// one product entry sum_k a_k b_k, k = 1,2,3 in order
-template <typename Real>
-__device__ __forceinline__ CX<Real> dot3(CX<Real> a1, CX<Real> a2, CX<Real> a3, CX<Real> b1, CX<Real> b2, CX<Real> b3)
+__device__ __forceinline__ CX<Real> dot3(const CX<Real> *a, int as, const CX<Real> *b, int bs)
 {
     CX<Real> r;
-    r.re = a1.re * b1.re - a1.im * b1.im + a2.re * b2.re - a2.im * b2.im + a3.re * b3.re - a3.im * b3.im;
-    r.im = a1.re * b1.im + a1.im * b1.re + a2.re * b2.im + a2.im * b2.re + a3.re * b3.im + a3.im * b3.re;
+    r.re = a[0].re * b[0].re;
+    r.re = FMA(-a[0].im, b[0].im, r.re);
+    r.im = a[0].re * b[0].im;
+    r.im = FMA(a[0].im, b[0].re, r.im);
+#pragma unroll
+    for (int k = 1; k < 3; k++) {
+        const CX<Real> &x = a[k * as], &y = b[k * bs];
+        r.re = FMA(x.re, y.re, r.re);
+        r.re = FMA(-x.im, y.im, r.re);
+        r.im = FMA(x.re, y.im, r.im);
+        r.im = FMA(x.im, y.re, r.im);
+    }
+    return r;
+}
+// sum_k a_k conj(b_k)
+template <typename Real>
+__device__ __forceinline__ CX<Real> dotc3(const CX<Real> *a, int as, const CX<Real> *b, int bs)
+{
+    CX<Real> r;
+    r.re = a[0].re * b[0].re;
+    r.re = FMA(a[0].im, b[0].im, r.re);
+    r.im = a[0].im * b[0].re;
+    r.im = FMA(-a[0].re, b[0].im, r.im);
+#pragma unroll
+    for (int k = 1; k < 3; k++) {
+        const CX<Real> &x = a[k * as], &y = b[k * bs];
+        r.re = FMA(x.re, y.re, r.re);
+        r.re = FMA(x.im, y.im, r.re);
+        r.im = FMA(x.im, y.re, r.im);
+        r.im = FMA(-x.re, y.im, r.im);
+    }
+    return r;
+}
+// sum_k conj(a_k) b_k
+template <typename Real>
+__device__ __forceinline__ CX<Real> cdot3(const CX<Real> *a, int as, const CX<Real> *b, int bs)
+{
+    CX<Real> r;
+    r.re = a[0].re * b[0].re;
+    r.re = FMA(a[0].im, b[0].im, r.re);
+    r.im = a[0].re * b[0].im;
+    r.im = FMA(-a[0].im, b[0].re, r.im);
+#pragma unroll
+    for (int k = 1; k < 3; k++) {
+        const CX<Real> &x = a[k * as], &y = b[k * bs];
+        r.re = FMA(x.re, y.re, r.re);
+        r.re = FMA(x.im, y.im, r.re);
+        r.im = FMA(x.re, y.im, r.im);
+        r.im = FMA(-x.im, y.re, r.im);
+    }
     return r;
 }
 
-// rows 1,2 of compressed x compressed (matrix_times3, su3cl.cl:51-99)
+// row 3 = conj(row1 x row2) (lattice_reconstruct3, su3cl.cl:137-165)
 template <typename Real>
-__device__ __forceinline__ G3<Real> times3(const G3<Real> &a, const G3<Real> &b)
+__device__ __forceinline__ void fill_row3(M3<Real> &a)
 {
-    S3<Real> u = rec3(a), v = rec3(b), t;
-    t.u1 = dot3(u.u1, u.u2, u.u3, v.u1, v.v1, v.w1);
-    t.u2 = dot3(u.u1, u.u2, u.u3, v.u2, v.v2, v.w2);
-    t.u3 = dot3(u.u1, u.u2, u.u3, v.u3, v.v3, v.w3);
-    t.v1 = dot3(u.v1, u.v2, u.v3, v.u1, v.v1, v.w1);
-    t.v2 = dot3(u.v1, u.v2, u.v3, v.u2, v.v2, v.w2);
-    t.v3 = dot3(u.v1, u.v2, u.v3, v.u3, v.v3, v.w3);
-    return compress3(t);
+#pragma unroll
+    for (int j = 0; j < 3; j++) {
+        const int p = (j + 1) % 3, q = (j + 2) % 3;
+        const CX<Real> &u1 = a.m[0][p], &u2 = a.m[0][q], &v1 = a.m[1][p], &v2 = a.m[1][q];
+        // conj(u1 v2 - u2 v1)
+        Real re = u1.re * v2.re;
+        re = FMA(-u1.im, v2.im, re);
+        re = FMA(-u2.re, v1.re, re);
+        re = FMA(u2.im, v1.im, re);
+        Real im = u2.re * v1.im;
+        im = FMA(u2.im, v1.re, im);
+        im = FMA(-u1.re, v2.im, im);
+        im = FMA(-u1.im, v2.re, im);
+        a.m[2][j].re = re;
+        a.m[2][j].im = im;
+    }
 }
 
-// compressed hermitian conjugate (matrix_hermitian3, su3_update_cl.cl:86-110)
 template <typename Real>
-__device__ __forceinline__ G3<Real> herm3(const G3<Real> &a)
+__device__ __forceinline__ M3<Real> expand(const G3<Real> &g)
 {
-    S3<Real> u = rec3(a);
+    M3<Real> a;
+    a.m[0][0] = { g.uv1.x, g.uv2.x }; a.m[0][1] = { g.uv1.y, g.uv2.y }; a.m[0][2] = { g.uv1.z, g.uv2.z };
+    a.m[1][0] = { g.uv3.x, g.uv3.z }; a.m[1][1] = { g.uv3.y, g.uv3.w }; a.m[1][2] = { g.uv1.w, g.uv2.w };
+    fill_row3(a);
+    return a;
+}
+template <typename Real>
+__device__ __forceinline__ G3<Real> compress(const M3<Real> &a)
+{
     G3<Real> g;
-    g.uv1 = { u.u1.re, u.v1.re, u.w1.re, u.w2.re };
-    g.uv2 = { -u.u1.im, -u.v1.im, -u.w1.im, -u.w2.im };
-    g.uv3 = { u.u2.re, u.v2.re, -u.u2.im, -u.v2.im };
+    g.uv1 = { a.m[0][0].re, a.m[0][1].re, a.m[0][2].re, a.m[1][2].re };
+    g.uv2 = { a.m[0][0].im, a.m[0][1].im, a.m[0][2].im, a.m[1][2].im };
+    g.uv3 = { a.m[1][0].re, a.m[1][1].re, a.m[1][0].im, a.m[1][1].im };
     return g;
 }
 
+// staple term U_a U_b^+ U_c^+ (lattice_staple_hermitian3, su3_update_cl.cl:294-307):
+// rows 1,2 of P = A B^+, row 3 of P by reconstruction, then P C^+
 template <typename Real>
-__device__ __forceinline__ void add3(S3<Real> &r, const S3<Real> &a, const S3<Real> &b)
+__device__ __forceinline__ M3<Real> staple_fwd3(const G3<Real> &ga, const G3<Real> &gb, const G3<Real> &gc)
 {
-    const Real *pa = &a.u1.re, *pb = &b.u1.re;
-    Real *pr = &r.u1.re;
+    M3<Real> A = expand(ga), B = expand(gb), C = expand(gc), P, Q;
 #pragma unroll
-    for (int i = 0; i < 18; i++) pr[i] = pa[i] + pb[i];
+    for (int i = 0; i < 2; i++)
+#pragma unroll
+        for (int j = 0; j < 3; j++) P.m[i][j] = dotc3(&A.m[i][0], 1, &B.m[j][0], 1);
+    fill_row3(P);
+#pragma unroll
+    for (int i = 0; i < 3; i++)
+#pragma unroll
+        for (int j = 0; j < 3; j++) Q.m[i][j] = dotc3(&P.m[i][0], 1, &C.m[j][0], 1);
+    return Q;
+}
+// staple term U_a^+ U_b^+ U_c (lattice_staple_hermitian_backward3,
+// su3_update_cl.cl:324-338): rows 1,2 of R = B A, row 3 by reconstruction,
+// then R^+ C
+template <typename Real>
+__device__ __forceinline__ M3<Real> staple_bwd3(const G3<Real> &ga, const G3<Real> &gb, const G3<Real> &gc)
+{
+    M3<Real> A = expand(ga), B = expand(gb), C = expand(gc), R, Q;
+#pragma unroll
+    for (int i = 0; i < 2; i++)
+#pragma unroll
+        for (int j = 0; j < 3; j++) R.m[i][j] = dot3(&B.m[i][0], 1, &A.m[0][j], 3);
+    fill_row3(R);
+#pragma unroll
+    for (int i = 0; i < 3; i++)
+#pragma unroll
+        for (int j = 0; j < 3; j++) Q.m[i][j] = cdot3(&R.m[0][i], 3, &C.m[0][j], 3);
+    return Q;
 }
 
 template <typename Real>
-__device__ __forceinline__ S3<Real> staple_fwd3(const G3<Real> &u1, const G3<Real> &u2, const G3<Real> &u3)
+__device__ __forceinline__ void add3(M3<Real> &r, const M3<Real> &a, const M3<Real> &b)
 {
-    G3<Real> m2 = times3(u1, herm3(u2));
-    return rec3(times3(m2, herm3(u3)));
-}
-template <typename Real>
-__device__ __forceinline__ S3<Real> staple_bwd3(const G3<Real> &u1, const G3<Real> &u2, const G3<Real> &u3)
-{
-    G3<Real> m3 = times3(herm3(u1), herm3(u2));
-    return rec3(times3(m3, u3));
+#pragma unroll
+    for (int i = 0; i < 3; i++)
+#pragma unroll
+        for (int j = 0; j < 3; j++) {
+            r.m[i][j].re = a.m[i][j].re + b.m[i][j].re;
+            r.m[i][j].im = a.m[i][j].im + b.m[i][j].im;
+        }
 }
 
-// Gram-Schmidt on rows 1,2 (lattice_GramSchmidt3, su3_update_cl.cl:228-291),
-// carried out in precision Acc.
+// Gram-Schmidt on rows 1,2 (lattice_GramSchmidt3, su3_update_cl.cl:228-291)
+// in precision Acc; the compressed result
 template <typename Acc, typename Real>
-__device__ __forceinline__ G3<Real> gs3(const G3<Real> &m)
+__device__ __forceinline__ G3<Real> gs3(const G3<Real> &g)
 {
-    Acc t1x = m.uv1.x, t1y = m.uv1.y, t1z = m.uv1.z, t1w = m.uv1.w;
-    Acc t2x = m.uv2.x, t2y = m.uv2.y, t2z = m.uv2.z, t2w = m.uv2.w;
-    Acc nu = sqrt((t1x * t1x + t2x * t2x) + (t1y * t1y + t2y * t2y) + (t1z * t1z + t2z * t2z));
-    Acc ur0 = t1x / nu, ur1 = t1y / nu, ur2 = t1z / nu;
-    Acc ui0 = t2x / nu, ui1 = t2y / nu, ui2 = t2z / nu;
-    Acc vr0 = m.uv3.x, vr1 = m.uv3.y, vr2 = t1w;
-    Acc vi0 = m.uv3.z, vi1 = m.uv3.w, vi2 = t2w;
-    Acc sr = (ur0 * vr0 + ui0 * vi0) + (ur1 * vr1 + ui1 * vi1) + (ur2 * vr2 + ui2 * vi2);
-    Acc si = (ur0 * vi0 - ui0 * vr0) + (ur1 * vi1 - ui1 * vr1) + (ur2 * vi2 - ui2 * vr2);
-    Acc nr0 = vr0 - ur0 * sr + ui0 * si, ni0 = vi0 - ur0 * si - ui0 * sr;
-    Acc nr1 = vr1 - ur1 * sr + ui1 * si, ni1 = vi1 - ur1 * si - ui1 * sr;
-    Acc nr2 = vr2 - ur2 * sr + ui2 * si, ni2 = vi2 - ur2 * si - ui2 * sr;
-    Acc nv = sqrt((nr0 * nr0 + ni0 * ni0) + (nr1 * nr1 + ni1 * ni1) + (nr2 * nr2 + ni2 * ni2));
+    Acc u[3][2] = { { (Acc)g.uv1.x, (Acc)g.uv2.x }, { (Acc)g.uv1.y, (Acc)g.uv2.y }, { (Acc)g.uv1.z, (Acc)g.uv2.z } };
+    Acc v[3][2] = { { (Acc)g.uv3.x, (Acc)g.uv3.z }, { (Acc)g.uv3.y, (Acc)g.uv3.w }, { (Acc)g.uv1.w, (Acc)g.uv2.w } };
+    Acc n2 = u[0][0] * u[0][0];
+    n2 = FMA(u[0][1], u[0][1], n2);
+#pragma unroll
+    for (int k = 1; k < 3; k++) { n2 = FMA(u[k][0], u[k][0], n2); n2 = FMA(u[k][1], u[k][1], n2); }
+    Acc nu = sqrt(n2);
+#pragma unroll
+    for (int k = 0; k < 3; k++) { u[k][0] = u[k][0] / nu; u[k][1] = u[k][1] / nu; }
+    // sc = sum_k v_k conj(u_k)
+    Acc sr = v[0][0] * u[0][0], si = v[0][1] * u[0][0];
+    sr = FMA(v[0][1], u[0][1], sr);
+    si = FMA(-v[0][0], u[0][1], si);
+#pragma unroll
+    for (int k = 1; k < 3; k++) {
+        sr = FMA(v[k][0], u[k][0], sr); sr = FMA(v[k][1], u[k][1], sr);
+        si = FMA(v[k][1], u[k][0], si); si = FMA(-v[k][0], u[k][1], si);
+    }
+#pragma unroll
+    for (int k = 0; k < 3; k++) {          // v <- v - sc u
+        Acc r = FMA(-sr, u[k][0], v[k][0]);
+        r = FMA(si, u[k][1], r);
+        Acc i = FMA(-sr, u[k][1], v[k][1]);
+        i = FMA(-si, u[k][0], i);
+        v[k][0] = r; v[k][1] = i;
+    }
+    Acc m2 = v[0][0] * v[0][0];
+    m2 = FMA(v[0][1], v[0][1], m2);
+#pragma unroll
+    for (int k = 1; k < 3; k++) { m2 = FMA(v[k][0], v[k][0], m2); m2 = FMA(v[k][1], v[k][1], m2); }
+    Acc nv = sqrt(m2);
+#pragma unroll
+    for (int k = 0; k < 3; k++) { v[k][0] = v[k][0] / nv; v[k][1] = v[k][1] / nv; }
     G3<Real> r;
-    r.uv1 = { (Real)ur0, (Real)ur1, (Real)ur2, (Real)(nr2 / nv) };
-    r.uv2 = { (Real)ui0, (Real)ui1, (Real)ui2, (Real)(ni2 / nv) };
-    r.uv3 = { (Real)(nr0 / nv), (Real)(nr1 / nv), (Real)(ni0 / nv), (Real)(ni1 / nv) };
+    r.uv1 = { (Real)u[0][0], (Real)u[1][0], (Real)u[2][0], (Real)v[2][0] };
+    r.uv2 = { (Real)u[0][1], (Real)u[1][1], (Real)u[2][1], (Real)v[2][1] };
+    r.uv3 = { (Real)v[0][0], (Real)v[1][0], (Real)v[0][1], (Real)v[1][1] };
     return r;
 }
 
-// twisted boundary factor on Y links at x = N1-1 (su3_matrix_memory.cl:57-97)
+// twisted boundary factor on Y links at x = N1-1 (su3_matrix_memory.cl:57-97):
+// row 1 times exp(i(phi+omega)/2), row 2 times exp(i(omega-phi)/2)
 template <typename Real>
 __device__ __forceinline__ G3<Real> twist3(const G3<Real> &m, Real phi, Real omega)
 {
@@ -159,9 +314,9 @@ __device__ __forceinline__ G3<Real> twist3(const G3<Real> &m, Real phi, Real ome
     Real cp = RC<Real>::cs(p), sp = RC<Real>::sn(p), cq = RC<Real>::cs(q), sq = RC<Real>::sn(q);
     const R4<Real> &a = m.uv1, &b = m.uv2, &d = m.uv3;
     G3<Real> r;
-    r.uv1 = { a.x * cp - b.x * sp, a.y * cp - b.y * sp, a.z * cp - b.z * sp, a.w * cq - b.w * sq };
-    r.uv2 = { b.x * cp + a.x * sp, b.y * cp + a.y * sp, b.z * cp + a.z * sp, b.w * cq + a.w * sq };
-    r.uv3 = { d.x * cq - d.z * sq, d.y * cq - d.w * sq, d.z * cq + d.x * sq, d.w * cq + d.y * sq };
+    r.uv1 = { FMA(-b.x, sp, a.x * cp), FMA(-b.y, sp, a.y * cp), FMA(-b.z, sp, a.z * cp), FMA(-b.w, sq, a.w * cq) };
+    r.uv2 = { FMA(a.x, sp, b.x * cp), FMA(a.y, sp, b.y * cp), FMA(a.z, sp, b.z * cp), FMA(a.w, sq, b.w * cq) };
+    r.uv3 = { FMA(-d.z, sq, d.x * cq), FMA(-d.w, sq, d.y * cq), FMA(d.x, sq, d.z * cq), FMA(d.y, sq, d.w * cq) };
     return r;
 }
 
@@ -172,10 +327,10 @@ template <typename Real>
 __device__ __forceinline__ R4<Real> times2(const R4<Real> &u, const R4<Real> &v)
 {
     R4<Real> a;
-    a.x = u.x * v.x - u.y * v.y - u.z * v.z - u.w * v.w;
-    a.z = u.x * v.z + u.z * v.x + u.y * v.w - u.w * v.y;
-    a.y = u.x * v.y + u.y * v.x + u.w * v.z - u.z * v.w;
-    a.w = u.x * v.w + u.w * v.x + u.z * v.y - u.y * v.z;
+    a.x = u.x * v.x; a.x = FMA(-u.y, v.y, a.x); a.x = FMA(-u.z, v.z, a.x); a.x = FMA(-u.w, v.w, a.x);
+    a.z = u.x * v.z; a.z = FMA(u.z, v.x, a.z); a.z = FMA(u.y, v.w, a.z); a.z = FMA(-u.w, v.y, a.z);
+    a.y = u.x * v.y; a.y = FMA(u.y, v.x, a.y); a.y = FMA(u.w, v.z, a.y); a.y = FMA(-u.z, v.w, a.y);
+    a.w = u.x * v.w; a.w = FMA(u.w, v.x, a.w); a.w = FMA(u.z, v.y, a.w); a.w = FMA(-u.y, v.z, a.w);
     return a;
 }
 template <typename Real>
@@ -208,26 +363,37 @@ __device__ __forceinline__ S2<Real> staple_bwd2(const R4<Real> &u1, const R4<Rea
 {
     return rec2(times2(times2(herm2(u1), herm2(u2)), u3));
 }
+// full 2x2 product (matrix_times_su2, su2cl.cl:43-60)
 template <typename Real>
 __device__ __forceinline__ S2<Real> mul2(const S2<Real> &u, const S2<Real> &v)
 {
     S2<Real> t;
-    t.u1.re = (u.u1.re * v.u1.re - u.u1.im * v.u1.im) + (u.u2.re * v.v1.re - u.u2.im * v.v1.im);
-    t.u1.im = (u.u1.re * v.u1.im + u.u1.im * v.u1.re) + (u.u2.re * v.v1.im + u.u2.im * v.v1.re);
-    t.u2.re = (u.u1.re * v.u2.re - u.u1.im * v.u2.im) + (u.u2.re * v.v2.re - u.u2.im * v.v2.im);
-    t.u2.im = (u.u1.re * v.u2.im + u.u1.im * v.u2.re) + (u.u2.re * v.v2.im + u.u2.im * v.v2.re);
-    t.v1.re = (u.v1.re * v.u1.re - u.v1.im * v.u1.im) + (u.v2.re * v.v1.re - u.v2.im * v.v1.im);
-    t.v1.im = (u.v1.re * v.u1.im + u.v1.im * v.u1.re) + (u.v2.re * v.v1.im + u.v2.im * v.v1.re);
-    t.v2.re = (u.v1.re * v.u2.re - u.v1.im * v.u2.im) + (u.v2.re * v.v2.re - u.v2.im * v.v2.im);
-    t.v2.im = (u.v1.re * v.u2.im + u.v1.im * v.u2.re) + (u.v2.re * v.v2.im + u.v2.im * v.v2.re);
+    const CX<Real> U[2][2] = { { u.u1, u.u2 }, { u.v1, u.v2 } }, W[2][2] = { { v.u1, v.u2 }, { v.v1, v.v2 } };
+    CX<Real> T[2][2];
+#pragma unroll
+    for (int i = 0; i < 2; i++)
+#pragma unroll
+        for (int j = 0; j < 2; j++) {
+            Real re = U[i][0].re * W[0][j].re;
+            re = FMA(-U[i][0].im, W[0][j].im, re);
+            re = FMA(U[i][1].re, W[1][j].re, re);
+            re = FMA(-U[i][1].im, W[1][j].im, re);
+            Real im = U[i][0].re * W[0][j].im;
+            im = FMA(U[i][0].im, W[0][j].re, im);
+            im = FMA(U[i][1].re, W[1][j].im, im);
+            im = FMA(U[i][1].im, W[1][j].re, im);
+            T[i][j] = { re, im };
+        }
+    t.u1 = T[0][0]; t.u2 = T[0][1]; t.v1 = T[1][0]; t.v2 = T[1][1];
     return t;
 }
 
 // ------------------------------------------------------------ heatbath
-// Kennedy-Pendleton step on a 2x2 block a.  Prn::next(k) returns the k-th
-// float4 of this thread's stream.  Returns true when a try was accepted
-// (a <- c*aH); on rejection the SU(3) path sets a to the identity and skips
-// one PRN quad (su3_update_cl.cl:568-669; SU(2) group: su2_update_cl.cl:434-531).
+// Kennedy-Pendleton step on a 2x2 block a.  Prn::try_quad / dir_quad give
+// the next float4 of this thread's stream.  Returns true when a try was
+// accepted (a <- c*aH); on rejection the SU(3) path sets a to the identity
+// and skips one PRN quad (su3_update_cl.cl:568-669; SU(2) group:
+// su2_update_cl.cl:434-531).
 template <typename Real, bool SU3PATH, class Prn>
 __device__ __forceinline__ bool kp_step(S2<Real> &a, Real beta, Prn &prn, int nhit)
 {
@@ -238,12 +404,16 @@ __device__ __forceinline__ bool kp_step(S2<Real> &a, Real beta, Prn &prn, int nh
         aH.z = -(a.u1.im - a.v2.im);
         aH.y = -(a.u2.re - a.v1.re);
         aH.w = -(a.u2.im + a.v1.im);
-        det = RC<Real>::sq(aH.x * aH.x + aH.y * aH.y + aH.z * aH.z + aH.w * aH.w);
+        Real n2 = aH.x * aH.x;
+        n2 = FMA(aH.y, aH.y, n2); n2 = FMA(aH.z, aH.z, n2); n2 = FMA(aH.w, aH.w, n2);
+        det = RC<Real>::sq(n2);
         aH.x /= det; aH.z /= det; aH.y /= det; aH.w /= det;
     } else {
         Real Mx = a.u1.re + a.v2.re, My = a.u1.im - a.v2.im;
         Real Mz = a.u2.re - a.v1.re, Mw = a.u2.im + a.v1.im;
-        det = RC<Real>::sq(Mx * Mx + My * My + Mz * Mz + Mw * Mw);
+        Real n2 = Mx * Mx;
+        n2 = FMA(My, My, n2); n2 = FMA(Mz, Mz, n2); n2 = FMA(Mw, Mw, n2);
+        det = RC<Real>::sq(n2);
         aH.x = Mx / det; aH.z = -My / det; aH.y = -Mz / det; aH.w = -Mw / det;
     }
     Real bdet = beta * det;
@@ -252,14 +422,15 @@ __device__ __forceinline__ bool kp_step(S2<Real> &a, Real beta, Prn &prn, int nh
     for (int i = 0; i < nhit && !flag; i++) {
         R4<Real> rnd = prn.try_quad();
         Real cosrnd = RC<Real>::cs(RC<Real>::PI2 * rnd.y);
-        delta = (Real)(-(log(1.0 - (double)rnd.x) + (double)(cosrnd * cosrnd) * log(1.0 - (double)rnd.z)) / (double)bdet);
-        if ((double)(rnd.w * rnd.w) <= (1.0 - 0.5 * (double)delta)) flag = true;
+        double lx = qg_log(1.0 - (double)rnd.x), lz = qg_log(1.0 - (double)rnd.z);
+        delta = (Real)(-FMA((double)(cosrnd * cosrnd), lz, lx) / (double)bdet);
+        if ((double)(rnd.w * rnd.w) <= FMA(-0.5, (double)delta, 1.0)) flag = true;
         if (Prn::GID) { delta = cosrnd * cosrnd / bdet; flag = true; }
     }
     if (flag) {
         R4<Real> rnd = prn.dir_quad();
         Real cosal = (Real)(1.0 - (double)delta);
-        Real costh = (Real)(2.0 * (double)rnd.x - 1.0);
+        Real costh = (Real)FMA(2.0, (double)rnd.x, -1.0);
         Real sinth = (Real)sqrt(1.0 - (double)(costh * costh));
         Real sinal = (Real)sqrt(1.0 - (double)(cosal * cosal));
         Real phi = RC<Real>::PI2 * rnd.y;
@@ -290,61 +461,54 @@ __device__ __forceinline__ void or_step(S2<Real> &a)
     aH.z = -(a.u1.im - a.v2.im);
     aH.y = -(a.u2.re - a.v1.re);
     aH.w = -(a.u2.im + a.v1.im);
-    Real det = RC<Real>::sq(aH.x * aH.x + aH.y * aH.y + aH.z * aH.z + aH.w * aH.w);
+    Real n2 = aH.x * aH.x;
+    n2 = FMA(aH.y, aH.y, n2); n2 = FMA(aH.z, aH.z, n2); n2 = FMA(aH.w, aH.w, n2);
+    Real det = RC<Real>::sq(n2);
     aH.x /= det; aH.z /= det; aH.y /= det; aH.w /= det;
     a = rec2(times2(aH, aH));
 }
 
-// entries of U0 * staple restricted to one subgroup block
+// rows i, j of U <- V (rows i, j) for the 2x2 block V = (u1 u2; v1 v2)
 template <typename Real>
-__device__ __forceinline__ CX<Real> row_col(const S3<Real> &u, int r, const S3<Real> &s, int c)
+__device__ __forceinline__ void rotate_rows(M3<Real> &U, int i, int j, const S2<Real> &V)
 {
-    const CX<Real> *ur = (r == 0) ? &u.u1 : (r == 1) ? &u.v1 : &u.w1;
-    const CX<Real> *s0 = &s.u1, *s1 = &s.v1, *s2 = &s.w1;
-    return dot3(ur[0], ur[1], ur[2], s0[c], s1[c], s2[c]);
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+        const CX<Real> x = U.m[i][k], y = U.m[j][k];
+        Real re = V.u1.re * x.re; re = FMA(-V.u1.im, x.im, re); re = FMA(V.u2.re, y.re, re); re = FMA(-V.u2.im, y.im, re);
+        Real im = V.u1.re * x.im; im = FMA(V.u1.im, x.re, im); im = FMA(V.u2.re, y.im, im); im = FMA(V.u2.im, y.re, im);
+        Real re2 = V.v1.re * x.re; re2 = FMA(-V.v1.im, x.im, re2); re2 = FMA(V.v2.re, y.re, re2); re2 = FMA(-V.v2.im, y.im, re2);
+        Real im2 = V.v1.re * x.im; im2 = FMA(V.v1.im, x.re, im2); im2 = FMA(V.v2.re, y.im, im2); im2 = FMA(V.v2.im, y.re, im2);
+        U.m[i][k] = { re, im };
+        U.m[j][k] = { re2, im2 };
+    }
 }
 
-// Cabibbo-Marinari over the SU(2) subgroups (1,2), (1,3), (2,3);
-// lattice_heatbath3, su3_update_cl.cl:672-779.  OR = true replaces each
-// Kennedy-Pendleton step by the reflection.
+// Cabibbo-Marinari over the SU(2) subgroups (1,2), (1,3), (2,3)
+// (lattice_heatbath3, su3_update_cl.cl:672-779): for each subgroup the 2x2
+// block of W = U staple, a Kennedy-Pendleton draw (or the reflection when
+// OR), and the rotation of the two rows of U; then Gram-Schmidt.
 template <typename Real, bool OR, class Prn>
-__device__ __forceinline__ G3<Real> cm3(const S3<Real> &staple, const G3<Real> &m0, Real beta, Prn &prn,
-                                        int nhit, int nhitpar)
+__device__ __forceinline__ G3<Real> cm3(const M3<Real> &S, const G3<Real> &m0, Real beta, Prn &prn, int nhit,
+                                        int nhitpar)
 {
-    G3<Real> reslt = m0, Vg, m1, m2, m3 = m0;
-    S3<Real> U0 = rec3(m0);
-    S2<Real> r0;
-    const R4<Real> z = { 0, 0, 0, 0 };
-    for (int j = 0; j < nhitpar; j++) {
-        r0.u1 = row_col(U0, 0, staple, 0); r0.u2 = row_col(U0, 0, staple, 1);
-        r0.v1 = row_col(U0, 1, staple, 0); r0.v2 = row_col(U0, 1, staple, 1);
-        if (OR) or_step(r0); else kp_step<Real, true>(r0, beta, prn, nhit);
-        Vg.uv1 = { r0.u1.re, r0.u2.re, 0, 0 };
-        Vg.uv2 = { r0.u1.im, r0.u2.im, 0, 0 };
-        Vg.uv3 = { r0.v1.re, r0.v2.re, r0.v1.im, r0.v2.im };
-        m1 = times3(Vg, m3);
-        U0 = rec3(m1);
-
-        r0.u1 = row_col(U0, 0, staple, 0); r0.u2 = row_col(U0, 0, staple, 2);
-        r0.v1 = row_col(U0, 2, staple, 0); r0.v2 = row_col(U0, 2, staple, 2);
-        if (OR) or_step(r0); else kp_step<Real, true>(r0, beta, prn, nhit);
-        Vg.uv1 = { r0.u1.re, 0, r0.u2.re, 0 };
-        Vg.uv2 = { r0.u1.im, 0, r0.u2.im, 0 };
-        Vg.uv3 = { 0, 1, 0, 0 };
-        m2 = times3(Vg, m1);
-        U0 = rec3(m2);
-
-        r0.u1 = row_col(U0, 1, staple, 1); r0.u2 = row_col(U0, 1, staple, 2);
-        r0.v1 = row_col(U0, 2, staple, 1); r0.v2 = row_col(U0, 2, staple, 2);
-        if (OR) or_step(r0); else kp_step<Real, true>(r0, beta, prn, nhit);
-        Vg.uv1 = { 1, 0, 0, r0.u2.re };
-        Vg.uv2 = { 0, 0, 0, r0.u2.im };
-        Vg.uv3 = { 0, r0.u1.re, 0, r0.u1.im };
-        m3 = times3(Vg, m2);
-        reslt = gs3<Real>(m3);
-        U0 = rec3(reslt);
+    G3<Real> reslt = m0;
+    M3<Real> U = expand(m0);
+    for (int n = 0; n < nhitpar; n++) {
+#pragma unroll
+        for (int sg = 0; sg < 3; sg++) {
+            const int i = (sg == 2) ? 1 : 0, j = (sg == 0) ? 1 : 2;
+            S2<Real> r0;
+            r0.u1 = dot3(&U.m[i][0], 1, &S.m[0][i], 3);
+            r0.u2 = dot3(&U.m[i][0], 1, &S.m[0][j], 3);
+            r0.v1 = dot3(&U.m[j][0], 1, &S.m[0][i], 3);
+            r0.v2 = dot3(&U.m[j][0], 1, &S.m[0][j], 3);
+            if (OR) or_step(r0); else kp_step<Real, true>(r0, beta, prn, nhit);
+            rotate_rows(U, i, j, r0);
+        }
+        reslt = gs3<Real>(compress(U));
+        U = expand(reslt);
     }
-    (void)z;
     return reslt;
 }
 

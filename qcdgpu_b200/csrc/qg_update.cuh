@@ -42,13 +42,13 @@ __device__ __forceinline__ int nu_of(int mu, int i)
 }
 
 template <typename Real>
-__device__ __forceinline__ S3<Real> staple3(const Field<Real> &U, const Geom &G, const Crd &c, int p, int mu,
+__device__ __forceinline__ M3<Real> staple3(const Field<Real> &U, const Geom &G, const Crd &c, int p, int mu,
                                            const Twist<Real> &tw)
 {
     const Crd cp = step_plus(G, c, mu);
     const uint32_t e_cp = cb_index(G, cp, p ^ 1);
     const uint32_t e_c = (uint32_t)p * G.cb + (crd2lex(G, c) >> 1);
-    S3<Real> st, s2;
+    M3<Real> st, s2;
 #pragma unroll
     for (int i = 0; i < 3; i++) {
         const int nu = nu_of(mu, i);
@@ -56,8 +56,8 @@ __device__ __forceinline__ S3<Real> staple3(const Field<Real> &U, const Geom &G,
         const Crd cm = step_minus(G, c, nu);
         const Crd cmp = step_plus(G, cm, mu);
         const uint32_t e_cn = cb_index(G, cn, p ^ 1), e_cm = cb_index(G, cm, p ^ 1), e_cmp = cb_index(G, cmp, p);
-        S3<Real> fw = staple_fwd3(load3t(U, nu, e_cp, cp, tw), load3t(U, mu, e_cn, cn, tw), load3t(U, nu, e_c, c, tw));
-        S3<Real> bw = staple_bwd3(load3t(U, nu, e_cmp, cmp, tw), load3t(U, mu, e_cm, cm, tw), load3t(U, nu, e_cm, cm, tw));
+        M3<Real> fw = staple_fwd3(load3t(U, nu, e_cp, cp, tw), load3t(U, mu, e_cn, cn, tw), load3t(U, nu, e_c, c, tw));
+        M3<Real> bw = staple_bwd3(load3t(U, nu, e_cmp, cmp, tw), load3t(U, mu, e_cm, cm, tw), load3t(U, nu, e_cm, cm, tw));
         if (i == 0) {
             add3(st, fw, bw);
         } else {
@@ -139,7 +139,7 @@ __global__ void __launch_bounds__(128) k_phase(Field<Real> U, Geom G, PhaseArgs 
     if (NC == 3) {
         G3<Real> m0 = U.ld3(mu, e0);
         if (tw.on && mu == 1 && c.x == tw.xlast) m0 = twist3(m0, tw.phi, tw.omega);
-        S3<Real> st = staple3(U, G, c, p, mu, tw);
+        M3<Real> st = staple3(U, G, c, p, mu, tw);
         G3<Real> mU = cm3<Real, OR>(st, m0, beta, prn, A.nhit, A.nhitpar);
         U.st3(mu, e0, mU);
     } else {

@@ -1,0 +1,43 @@
+"""Launches the sweep's phase kernels on one lattice, for a profiler.
+
+  python -m qcdgpu_b200.phase_profile [--size 32] [--precision 0] [--group 3]
+                                      [--prng philox|ranlux] [--warm 2] [--phases 1]
+
+Cold start, `warm` heatbath sweeps (8 heatbath phase launches each, so a
+profiler skips 8*warm + 1 kernel launches to reach the measured ones), then
+`phases` heatbath phase launches followed by `phases` overrelaxation phase
+launches (odd X first), then a synchronise.
+"""
+import argparse
+
+import qcdgpu_b200 as Q
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--size", type=int, default=32)
+    ap.add_argument("--precision", type=int, default=0)
+    ap.add_argument("--group", type=int, default=3)
+    ap.add_argument("--prng", default="philox", choices=["philox", "ranlux"])
+    ap.add_argument("--warm", type=int, default=2)
+    ap.add_argument("--phases", type=int, default=1)
+    a = ap.parse_args()
+    cfg = Q.default_config(group=a.group, size=a.size, precision=a.precision, start=Q.START_COLD,
+                           prng=Q.PRNG_PHILOX if a.prng == "philox" else Q.PRNG_RANLUX, beta=6.0, n_or=0,
+                           reunit_every=0)
+    L = Q.Lattice(cfg)
+    L.seed()
+    L.init()
+    L.sweep(a.warm)
+    for k in range(a.phases):
+        if a.prng == "ranlux":
+            L.produce()
+        L.phase(1, k % 4, Q.HEATBATH)
+    for k in range(a.phases):
+        L.phase(1, k % 4, Q.OVERRELAX)
+    L.sync()
+    print("plaquette", L.plaquette())
+
+
+if __name__ == "__main__":
+    main()

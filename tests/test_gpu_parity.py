@@ -175,6 +175,30 @@ def test_sweeps_philox(group, precision):
 
 
 @pytest.mark.parametrize("group,precision", [(3, 1), (3, 0), (2, 1), (2, 0)])
+def test_sweeps_bit_exact(group, precision):
+    """Same operation sequence on both sides (explicit fma, own sin/cos/log):
+    three heatbath + overrelaxation sweeps reproduce the oracle bit for bit."""
+    L, c = make_pair(group, (4, 4, 4, 4), precision, start=Q.START_COLD, prng=Q.PRNG_PHILOX,
+                     beta=5.8 if group == 3 else 2.3, n_or=1, reunit_every=3, reunit_fp64=0)
+    L.seed(54)
+    L.init(Q.START_COLD)
+    t = cold_table(c)
+    ph = 0
+    for s in range(3):
+        L.sweep(1)
+        for par in (1, 0):
+            for mu in range(4):
+                O.phase_hb(c, t, par, mu, philox=(54, 0x5D3E1A27, ph))
+                ph += 1
+        for par in (1, 0):
+            for mu in range(4):
+                O.lib.ol_phase_or(ctypes.byref(c), O.vp(t), par, mu)
+    O.lib.ol_gramschmidt(ctypes.byref(c), O.vp(t))
+    g = L.download()
+    assert np.array_equal(g, t), "max|dU| = %g" % maxdiff(g, t)
+
+
+@pytest.mark.parametrize("group,precision", [(3, 1), (3, 0), (2, 1), (2, 0)])
 def test_overrelaxation_sweeps(group, precision):
     """1 heatbath + 2 overrelaxation sweeps, GS every 2 sweeps in FP64."""
     L, c = make_pair(group, (4, 4, 4, 4), precision, start=Q.START_COLD, prng=Q.PRNG_PHILOX,
