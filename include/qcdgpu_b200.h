@@ -162,6 +162,68 @@ int qg_get_stream(qg_ctx *ctx, void **stream);
 /* Philox phase counter (fast mode): read / set for checkpoint and resume */
 int qg_set_phase_counter(qg_ctx *ctx, uint64_t counter);
 
+/* ===================================================================== */
+/* Host driver: the reference's init.dat run setup, run loop and output   */
+/* (SU(N)/QCDGPU.cpp:61-269, model::lattice_get_init_file / lattice_init / */
+/* lattice_simulate / lattice_analysis / lattice_write_results,            */
+/* SU(N)/suncl/suncl.cpp:289-464, 5212-5505, 1328-1854).                   */
+/* ===================================================================== */
+
+/* observables of a run, in the reference's results order */
+#define QG_OBS_S_TOTAL      0
+#define QG_OBS_PLQ_TOTAL    1
+#define QG_OBS_POLYAKOV     2
+#define QG_OBS_POLYAKOV_IM  3
+#define QG_OBS_POLYAKOV_P2  4
+#define QG_OBS_POLYAKOV_P4  5
+#define QG_OBS_WILSON       6
+#define QG_OBS_PLQ_SPAT     7
+#define QG_OBS_PLQ_TEMP     8
+#define QG_OBS_S_SPAT       9
+#define QG_OBS_S_TEMP      10
+#define QG_OBS_COUNT       11
+
+typedef struct qg_run_options {
+    int iter;              /* ITER: measurements, the first on the start configuration */
+    int niter;             /* NITER: sweeps between measurements                       */
+    int nav;               /* NAV: thermalisation sweeps                               */
+    int pl_level;          /* PL_LEVEL: 0 none, 1 P, >= 2 P, |P|^2, |P|^4              */
+    int get_wilson;        /* GETWILSON                                                */
+    int get_plaquettes;    /* GETRETRACE / plaquette averages                         */
+    int get_actions;       /* action averages                                          */
+    int verify;            /* CPU FP64 re-measurement of the last configuration       */
+    int write_results;     /* write the results .txt                                   */
+    int quiet;             /* no console output                                        */
+    char output_path[512]; /* OUTPUTPATH (directory prefix of the results file)        */
+    char prefix[32];       /* file prefix, "su3-" / "su2-"                              */
+} qg_run_options;
+
+typedef struct qg_run_result {
+    double mean[QG_OBS_COUNT];       /* over samples 1..ITER-1 (sample 0 dropped)  */
+    double variance[QG_OBS_COUNT];
+    double gpu_last[QG_OBS_COUNT];
+    double cpu_last[QG_OBS_COUNT];   /* host FP64 re-measurement (verify)          */
+    int verification_passed;         /* 1 passed, 0 failed, -1 not run             */
+    int samples;
+    double seconds;                  /* wall time of the update + measure loop     */
+    double link_updates_per_second;
+    char results_file[640];
+} qg_run_result;
+
+/* defaults of the reference main() (QCDGPU.cpp:183-205) */
+int qg_default_run_options(qg_run_options *opts);
+/* Host only: read KEY = value lines ('#' starts a comment) and apply the
+ * keys onto cfg / opts as lattice_get_init_file does.  Keys: GROUP ND L1..L4
+ * LS LT ITER NITER NAV NHIT BETA PHI OMEGA INTS RANDSERIES PRNG OUTPUTPATH
+ * GETWILSON GETRETRACE PL_LEVEL WILSONR WILSONT (reference) and PRECISION
+ * NHITPAR NOR REUNIT_EVERY REUNIT_FP64 PRNG_INSTANCES ROW_ALIGN (this build);
+ * PLATFORM DEVICE FINISHPATH TURNOFFWAITING REBUILDBINARY and the F_munu
+ * keys are accepted and ignored.  Unknown generators are an error.        */
+int qg_parse_init_file(const char *path, qg_config *cfg, qg_run_options *opts);
+/* lattice_init + lattice_simulate + LatticeCheckCPU + lattice_analysis +
+ * lattice_write_results on the current CUDA device.                       */
+int qg_run(const qg_config *cfg, const qg_run_options *opts, qg_run_result *res);
+
 #ifdef __cplusplus
 }
 #endif

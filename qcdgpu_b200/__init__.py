@@ -27,6 +27,7 @@ EXPORTED_SYMBOLS = (
     "qg_prng_seed", "qg_prng_produce", "qg_prns_upload", "qg_prns_download", "qg_init_links",
     "qg_phase", "qg_sweep", "qg_reunitarize", "qg_measure", "qg_measure_wilson",
     "qg_links_upload", "qg_links_download", "qg_set_phase_counter", "qg_glibc_seeds", "qg_set_params", "qg_get_stream",
+    "qg_default_run_options", "qg_parse_init_file", "qg_run",
 )
 
 
@@ -65,6 +66,41 @@ class Info(ctypes.Structure):
         ("prn_quads", ctypes.c_uint64),
         ("phase_counter", ctypes.c_uint64),
         ("prng_counter", ctypes.c_uint32),
+    ]
+
+
+OBS_NAMES = ("S_total", "Plq_total", "Polyakov_loop", "Polyakov_loop_im", "Polyakov_loop_P2",
+             "Polyakov_loop_P4", "Wilson_loop", "Plq_spat", "Plq_temp", "S_spat", "S_temp")
+
+
+class RunOptions(ctypes.Structure):
+    _fields_ = [
+        ("iter", ctypes.c_int),
+        ("niter", ctypes.c_int),
+        ("nav", ctypes.c_int),
+        ("pl_level", ctypes.c_int),
+        ("get_wilson", ctypes.c_int),
+        ("get_plaquettes", ctypes.c_int),
+        ("get_actions", ctypes.c_int),
+        ("verify", ctypes.c_int),
+        ("write_results", ctypes.c_int),
+        ("quiet", ctypes.c_int),
+        ("output_path", ctypes.c_char * 512),
+        ("prefix", ctypes.c_char * 32),
+    ]
+
+
+class RunResult(ctypes.Structure):
+    _fields_ = [
+        ("mean", ctypes.c_double * 11),
+        ("variance", ctypes.c_double * 11),
+        ("gpu_last", ctypes.c_double * 11),
+        ("cpu_last", ctypes.c_double * 11),
+        ("verification_passed", ctypes.c_int),
+        ("samples", ctypes.c_int),
+        ("seconds", ctypes.c_double),
+        ("link_updates_per_second", ctypes.c_double),
+        ("results_file", ctypes.c_char * 640),
     ]
 
 
@@ -109,6 +145,9 @@ def load_library(path=LIB_PATH):
     lib.qg_glibc_seeds.argtypes = [ctypes.c_uint32, ctypes.c_int, P(ctypes.c_uint32)]
     lib.qg_set_params.argtypes = [vp, ctypes.c_double, ctypes.c_double, ctypes.c_double]
     lib.qg_get_stream.argtypes = [vp, P(vp)]
+    lib.qg_default_run_options.argtypes = [P(RunOptions)]
+    lib.qg_parse_init_file.argtypes = [ctypes.c_char_p, P(Config), P(RunOptions)]
+    lib.qg_run.argtypes = [P(Config), P(RunOptions), P(RunResult)]
     _lib = lib
     return lib
 
@@ -139,6 +178,40 @@ def default_config(**kw):
                 raise KeyError(k)
             setattr(c, k, v)
     return c
+
+
+def default_run_options(**kw):
+    """qg_default_run_options (the reference main()'s run cadence) + kw."""
+    lib = load_library()
+    o = RunOptions()
+    lib.qg_default_run_options(ctypes.byref(o))
+    for k, v in kw.items():
+        if k in ("output_path", "prefix"):
+            v = v.encode()
+        setattr(o, k, v)
+    return o
+
+
+def parse_init_file(path, cfg=None, opts=None):
+    """Apply an init.dat onto (cfg, opts) -- host only, no GPU needed."""
+    lib = load_library()
+    cfg = default_config() if cfg is None else cfg
+    opts = default_run_options() if opts is None else opts
+    rc = lib.qg_parse_init_file(path.encode(), ctypes.byref(cfg), ctypes.byref(opts))
+    if rc != QG_OK:
+        raise QGError("qg_parse_init_file: %s" % lib.qg_last_error(None).decode())
+    return cfg, opts
+
+
+def run(cfg, opts):
+    """One run as the reference's main() does it: start, measurements every
+    NITER sweeps, statistics, CPU re-check, results file.  Returns RunResult."""
+    lib = load_library()
+    res = RunResult()
+    rc = lib.qg_run(ctypes.byref(cfg), ctypes.byref(opts), ctypes.byref(res))
+    if rc != QG_OK:
+        raise QGError("qg_run: %s" % lib.qg_last_error(None).decode())
+    return res
 
 
 class Lattice:

@@ -26,7 +26,8 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 # in a fixed order, so results do not depend on the compiler's contraction
 NVCC_FLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-fmad=false", "-Xcompiler", "-fPIC", "-I" + INCLUDE]
 CUDA_SOURCES = ["qg_update_f32.cu", "qg_update_f64.cu", "qg_fields.cu", "qg_ranlux.cu", "qg_capi.cu"]
-HOST_SOURCES = ["qg_host.cpp", "qcdgpu_main.cpp"]
+LIB_HOST_SOURCES = ["qg_host.cpp"]          # C++ host code linked into the library
+CLI_SOURCES = ["qcdgpu_main.cpp"]
 
 
 def nvcc():
@@ -75,6 +76,12 @@ def build(verbose=False, ptxas_info=False):
         if _stale(o, [s] + hdrs) or ptxas_info:
             extra = ["-Xptxas", "-v"] if ptxas_info else []
             jobs.append([nvcc()] + NVCC_FLAGS + extra + ["-c", s, "-o", o])
+    for src in LIB_HOST_SOURCES:
+        s = os.path.join(CSRC, src)
+        o = os.path.join(OBJ, src + ".o")
+        objs.append(o)
+        if _stale(o, [s] + hdrs):
+            jobs.append(["g++", "-O2", "-std=c++17", "-fPIC", "-Wall", "-I" + INCLUDE, "-c", s, "-o", o])
     logs = []
     if jobs:
         with ThreadPoolExecutor(max_workers=min(len(jobs), os.cpu_count() or 4)) as ex:
@@ -82,10 +89,10 @@ def build(verbose=False, ptxas_info=False):
     lib = os.path.join(LIB, "libqg_sun.so")
     if _stale(lib, objs):
         _run([nvcc()] + ARCH + ["-shared", "-o", lib] + objs + ["-lcudart"], verbose)
-    host_srcs = [os.path.join(CSRC, s) for s in HOST_SOURCES if os.path.exists(os.path.join(CSRC, s))]
+    cli = [os.path.join(CSRC, s) for s in CLI_SOURCES]
     exe = os.path.join(BIN, "qcdgpu")
-    if len(host_srcs) == len(HOST_SOURCES) and _stale(exe, host_srcs + hdrs + [lib]):
-        _run(["g++", "-O2", "-std=c++17", "-I" + INCLUDE, "-o", exe] + host_srcs +
+    if _stale(exe, cli + hdrs + [lib]):
+        _run(["g++", "-O2", "-std=c++17", "-I" + INCLUDE, "-o", exe] + cli +
              ["-L" + LIB, "-lqg_sun", "-Wl,-rpath,$ORIGIN/../lib", "-lm"], verbose)
     return "\n".join(logs)
 

@@ -41,6 +41,9 @@ struct qg_ctx {
 
 static thread_local std::string g_create_err;
 
+// errors of calls without a context (qg_create, the host driver)
+void qg_set_global_error(const std::string &m) { g_create_err = m; }
+
 static int fail(qg_ctx *c, int code, const std::string &msg)
 {
     if (c) c->err = msg; else g_create_err = msg;

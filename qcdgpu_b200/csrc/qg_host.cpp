@@ -1,0 +1,489 @@
+// qg_host.cpp -- the host side of a run: init.dat parsing, the run loop
+// with its measurement cadence, the statistics, the CPU re-measurement of
+// the last configuration and the results file.  Restates the reference's
+// model class behaviour (SU(N)/suncl/suncl.cpp) on top of the C-ABI.
+#include <math.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+#include <time.h>
+
+#include <chrono>
+#include <string>
+#include <vector>
+
+#include "../../include/qcdgpu_b200.h"
+
+void qg_set_global_error(const std::string &m);   // qg_capi.cu: qg_last_error(NULL)
+
+namespace {
+
+int host_fail(int code, const std::string &m)
+{
+    qg_set_global_error(m);
+    return code;
+}
+
+std::string trim(const std::string &s)
+{
+    size_t a = s.find_first_not_of(" \t\r\n"), b = s.find_last_not_of(" \t\r\n");
+    return a == std::string::npos ? std::string() : s.substr(a, b - a + 1);
+}
+
+// ------------------------------------------------------------------ FP64
+// host re-measurement of the last configuration from the reference-layout
+// table, as LatticeCheckCPU does (SU(N)/suncl/su3cpu.cpp:1155-1433)
+struct C { double re, im; };
+struct M { C m[3][3]; };
+
+struct Table {
+    int group, n[4], prec;
+    uint32_t rowsize;
+    const void *p;
+    double at(uint32_t site, int plane, int c) const
+    {
+        size_t i = ((size_t)site + (size_t)plane * rowsize) * 4 + c;
+        return prec ? ((const double *)p)[i] : (double)((const float *)p)[i];
+    }
+    uint32_t site(const int x[4]) const
+    {
+        return (uint32_t)(x[1] + x[2] * n[1] + x[3] * n[1] * n[2] + x[0] * n[1] * n[2] * n[3]);
+    }
+    M link(const int x[4], int mu, double phi, double omega) const
+    {
+        uint32_t s = site(x);
+        M a;
+        memset(&a, 0, sizeof(a));
+        if (group == 3) {
+            double r1[4], i1[4], v[4];
+            for (int c = 0; c < 4; c++) { r1[c] = at(s, mu, c); i1[c] = at(s, mu + 4, c); v[c] = at(s, mu + 8, c); }
+            a.m[0][0] = { r1[0], i1[0] }; a.m[0][1] = { r1[1], i1[1] }; a.m[0][2] = { r1[2], i1[2] };
+            a.m[1][0] = { v[0], v[2] };   a.m[1][1] = { v[1], v[3] };   a.m[1][2] = { r1[3], i1[3] };
+            if (mu == 1 && x[0] == n[0] - 1 && !(phi == 0.0 && omega == 0.0)) {
+                double p = (phi + omega) / 2, q = (omega - phi) / 2;
+                C e1 = { cos(p), sin(p) }, e2 = { cos(q), sin(q) };
+                for (int j = 0; j < 3; j++) {
+                    C u = a.m[0][j], w = a.m[1][j];
+                    a.m[0][j] = { u.re * e1.re - u.im * e1.im, u.re * e1.im + u.im * e1.re };
+                    a.m[1][j] = { w.re * e2.re - w.im * e2.im, w.re * e2.im + w.im * e2.re };
+                }
+            }
+            for (int j = 0; j < 3; j++) {     // row 3 = conj(row1 x row2)
+                int p = (j + 1) % 3, q = (j + 2) % 3;
+                C u1 = a.m[0][p], u2 = a.m[0][q], v1 = a.m[1][p], v2 = a.m[1][q];
+                a.m[2][j] = { u1.re * v2.re - u1.im * v2.im - u2.re * v1.re + u2.im * v1.im,
+                              -(u1.re * v2.im + u1.im * v2.re - u2.re * v1.im - u2.im * v1.re) };
+            }
+        } else {
+            double q[4];
+            for (int c = 0; c < 4; c++) q[c] = at(s, mu, c);
+            if (mu == 1 && x[0] == n[0] - 1 && phi != 0.0) {
+                double o[4] = { cos(phi / 2), 0.0, sin(phi / 2), 0.0 }, r[4];
+                r[0] = o[0] * q[0] - o[1] * q[1] - o[2] * q[2] - o[3] * q[3];
+                r[2] = o[0] * q[2] + o[2] * q[0] + o[1] * q[3] - o[3] * q[1];
+                r[1] = o[0] * q[1] + o[1] * q[0] + o[3] * q[2] - o[2] * q[3];
+                r[3] = o[0] * q[3] + o[3] * q[0] + o[2] * q[1] - o[1] * q[2];
+                memcpy(q, r, sizeof(q));
+            }
+            a.m[0][0] = { q[0], q[2] };  a.m[0][1] = { q[1], q[3] };
+            a.m[1][0] = { -q[1], q[3] }; a.m[1][1] = { q[0], -q[2] };
+        }
+        return a;
+    }
+};
+
+M mul(const M &a, const M &b, int N)
+{
+    M r;
+    memset(&r, 0, sizeof(r));
+    for (int i = 0; i < N; i++)
+        for (int j = 0; j < N; j++) {
+            double re = 0, im = 0;
+            for (int k = 0; k < N; k++) {
+                re += a.m[i][k].re * b.m[k][j].re - a.m[i][k].im * b.m[k][j].im;
+                im += a.m[i][k].re * b.m[k][j].im + a.m[i][k].im * b.m[k][j].re;
+            }
+            r.m[i][j] = { re, im };
+        }
+    return r;
+}
+M dag(const M &a, int N)
+{
+    M r;
+    memset(&r, 0, sizeof(r));
+    for (int i = 0; i < N; i++)
+        for (int j = 0; j < N; j++) r.m[i][j] = { a.m[j][i].re, -a.m[j][i].im };
+    return r;
+}
+double retr(const M &a, int N)
+{
+    double s = 0;
+    for (int i = 0; i < N; i++) s += a.m[i][i].re;
+    return s;
+}
+void shift(int x[4], int d, int s, const int n[4]) { x[d] = (x[d] + s + n[d]) % n[d]; }
+
+struct HostObs { double plq_s, plq_t, s_s, s_t, pre, pim, p2, p4, wilson; };
+
+HostObs host_measure(const Table &T, const qg_config &f, const qg_run_options &o)
+{
+    HostObs h;
+    memset(&h, 0, sizeof(h));
+    const int N = T.group;
+    const int *n = T.n;
+    const double bet = f.precision ? f.beta / N : (double)(float)(f.beta / N);
+    const double phi = f.precision ? f.phi : (double)(float)f.phi, om = f.precision ? f.omega : (double)(float)f.omega;
+    int x[4];
+    const long V = (long)n[0] * n[1] * n[2] * n[3];
+    for (x[0] = 0; x[0] < n[0]; x[0]++)
+        for (x[3] = 0; x[3] < n[3]; x[3]++)
+            for (x[2] = 0; x[2] < n[2]; x[2]++)
+                for (x[1] = 0; x[1] < n[1]; x[1]++) {
+                    double rs = 0, rt = 0;
+                    for (int mu = 0; mu < 3; mu++)
+                        for (int nu = mu + 1; nu < 4; nu++) {
+                            int a[4], b[4];
+                            memcpy(a, x, sizeof(a)); shift(a, mu, 1, n);
+                            memcpy(b, x, sizeof(b)); shift(b, nu, 1, n);
+                            M p = mul(mul(mul(T.link(x, mu, phi, om), T.link(a, nu, phi, om), N),
+                                          dag(T.link(b, mu, phi, om), N), N), dag(T.link(x, nu, phi, om), N), N);
+                            (nu == 3 ? rt : rs) += retr(p, N);
+                        }
+                    h.plq_s += rs; h.plq_t += rt;
+                    h.s_s += bet * (3.0 * N - rs);
+                    h.s_t += bet * (3.0 * N - rt);
+                    if (o.get_wilson) {
+                        const int R = f.wilson_r, TT = f.wilson_t;
+                        for (int i = 0; i < 3; i++) {
+                            int c[4];
+                            memcpy(c, x, sizeof(c));
+                            M w = T.link(c, i, phi, om);
+                            for (int k = 1; k < R; k++) { shift(c, i, 1, n); w = mul(w, T.link(c, i, phi, om), N); }
+                            shift(c, i, 1, n);
+                            for (int k = 0; k < TT; k++) { w = mul(w, T.link(c, 3, phi, om), N); shift(c, 3, 1, n); }
+                            for (int k = 0; k < R; k++) { shift(c, i, -1, n); w = mul(w, dag(T.link(c, i, phi, om), N), N); }
+                            for (int k = 0; k < TT; k++) { shift(c, 3, -1, n); w = mul(w, dag(T.link(c, 3, phi, om), N), N); }
+                            h.wilson += retr(w, N);
+                        }
+                    }
+                }
+    if (o.pl_level > 0) {
+        for (x[0] = 0; x[0] < n[0]; x[0]++)
+            for (x[2] = 0; x[2] < n[2]; x[2]++)
+                for (x[1] = 0; x[1] < n[1]; x[1]++) {
+                    x[3] = 0;
+                    M p = T.link(x, 3, phi, om);
+                    for (int k = 1; k < n[3]; k++) { x[3] = k; p = mul(p, T.link(x, 3, phi, om), N); }
+                    double re = 0, im = 0;
+                    for (int i = 0; i < N; i++) { re += p.m[i][i].re; im += p.m[i][i].im; }
+                    double q2 = re * re + im * im;
+                    h.pre += re; h.pim += im; h.p2 += q2; h.p4 += q2 * q2;
+                }
+    }
+    (void)V;
+    return h;
+}
+
+// data_analysis::lattice_data_analysis (SU(N)/data_analysis/data_analysis.cpp:107-134):
+// mean and population variance over samples 1..n-1
+void mean_var(const std::vector<double> &d, double &mean, double &var)
+{
+    mean = 0; var = 0;
+    int last = (int)d.size() - 1;
+    for (int i = 1; i <= last; i++) mean += d[i];
+    if (last > 0) mean /= last;
+    for (int i = 1; i <= last; i++) var += (d[i] - mean) * (d[i] - mean);
+    if (last > 0) var /= last;
+}
+
+// CPU_GPU_verification_single / _double (data_analysis.cpp:40-43,76-100)
+bool verify(double gpu, double cpu, bool single)
+{
+    const double floor_ = single ? 1e-6 : 1e-12, tol = single ? 0.00005 : 0.00000000001;
+    if (fabs(gpu) > floor_ && fabs(cpu) > floor_) return fabs(1.0 - cpu / gpu) <= tol;
+    return true;
+}
+
+}  // namespace
+
+extern "C" int qg_default_run_options(qg_run_options *o)
+{
+    if (!o) return QG_ERR_ARG;
+    memset(o, 0, sizeof(*o));
+    o->iter = 2;
+    o->niter = 1;
+    o->nav = 0;
+    o->pl_level = 2;
+    o->get_wilson = 0;
+    o->get_plaquettes = 1;
+    o->get_actions = 1;
+    o->verify = 1;
+    o->write_results = 1;
+    snprintf(o->prefix, sizeof(o->prefix), "su3-");
+    return QG_OK;
+}
+
+// GPU::get_init_file + model::lattice_get_init_file
+// (SU(N)/clinterface/clinterface.cpp:2060-2154, SU(N)/suncl/suncl.cpp:289-464)
+extern "C" int qg_parse_init_file(const char *path, qg_config *cfg, qg_run_options *o)
+{
+    if (!path || !cfg || !o) return host_fail(QG_ERR_ARG, "null argument");
+    FILE *fp = fopen(path, "r");
+    if (!fp) return host_fail(QG_ERR_IO, std::string("cannot open ") + path);
+    char line[1024];
+    int lineno = 0;
+    while (fgets(line, sizeof(line), fp)) {
+        lineno++;
+        std::string s(line);
+        size_t hash = s.find('#');
+        if (hash != std::string::npos) s = s.substr(0, hash);
+        size_t eq = s.find('=');
+        if (eq == std::string::npos) continue;
+        std::string key = trim(s.substr(0, eq)), val = trim(s.substr(eq + 1));
+        if (key.empty()) continue;
+        long iv = strtol(val.c_str(), nullptr, 10);
+        double dv = strtod(val.c_str(), nullptr);
+        if (key == "GROUP") { cfg->group = (int)iv; snprintf(o->prefix, sizeof(o->prefix), "su%ld-", iv); }
+        else if (key == "ND") { if (iv != 4) { fclose(fp); return host_fail(QG_ERR_UNSUPPORTED, "only ND = 4 is supported"); } }
+        else if (key == "L1") cfg->size[0] = (int)iv;
+        else if (key == "L2") cfg->size[1] = (int)iv;
+        else if (key == "L3") cfg->size[2] = (int)iv;
+        else if (key == "L4") cfg->size[3] = (int)iv;
+        else if (key == "LS") { cfg->size[0] = cfg->size[1] = cfg->size[2] = (int)iv; }
+        else if (key == "LT") cfg->size[3] = (int)iv;
+        else if (key == "ITER") o->iter = (int)iv;
+        else if (key == "NITER") o->niter = (int)iv;
+        else if (key == "NAV") o->nav = (int)iv;
+        else if (key == "NHIT") cfg->nhit = (int)iv;
+        else if (key == "BETA") cfg->beta = dv;
+        else if (key == "PHI") cfg->phi = dv;
+        else if (key == "OMEGA") cfg->omega = dv;
+        else if (key == "INTS") cfg->start = (iv == 1) ? QG_START_COLD : (iv == 2) ? QG_START_GID : (iv == 3) ? QG_START_HAAR : QG_START_HOT;
+        else if (key == "RANDSERIES") cfg->randseries = (uint32_t)iv;
+        else if (key == "PRNG") {
+            static const char *lux[] = { "RANLUX0", "RANLUX1", "RANLUX2", "RANLUX3", "RANLUX4" };
+            static const int skips[] = { 24, 48, 97, 223, 389 };
+            bool ok = false;
+            for (int k = 0; k < 5; k++)
+                if (val == lux[k]) { cfg->prng = QG_PRNG_RANLUX; cfg->ranlux_nskip = skips[k]; ok = true; }
+            if (val == "RANLUX") { cfg->prng = QG_PRNG_RANLUX; ok = true; }
+            if (val == "PHILOX") { cfg->prng = QG_PRNG_PHILOX; ok = true; }
+            if (!ok) {
+                fclose(fp);
+                return host_fail(QG_ERR_UNSUPPORTED, "PRNG " + val + " is not available (RANLUX0..4, RANLUX, PHILOX)");
+            }
+        }
+        else if (key == "OUTPUTPATH") snprintf(o->output_path, sizeof(o->output_path), "%s", val.c_str());
+        else if (key == "GETWILSON") o->get_wilson = 1;
+        else if (key == "GETRETRACE") o->get_plaquettes = 1;
+        else if (key == "PL_LEVEL") o->pl_level = (int)iv;
+        else if (key == "WILSONR") cfg->wilson_r = (int)iv;
+        else if (key == "WILSONT") cfg->wilson_t = (int)iv;
+        else if (key == "PRECISION") cfg->precision = (int)iv;
+        else if (key == "NHITPAR") cfg->nhitpar = (int)iv;
+        else if (key == "NOR") cfg->n_or = (int)iv;
+        else if (key == "REUNIT_EVERY") cfg->reunit_every = (int)iv;
+        else if (key == "REUNIT_FP64") cfg->reunit_fp64 = (int)iv;
+        else if (key == "PRNG_INSTANCES") cfg->prng_instances = (int)iv;
+        else if (key == "ROW_ALIGN") cfg->row_align = (int)iv;
+        else if (key == "PLATFORM" || key == "DEVICE" || key == "FINISHPATH" || key == "TURNOFFWAITING" ||
+                 key == "REBUILDBINARY" || key == "TURNOFFFMUNU" || key == "FMUNU" || key == "F0MU" ||
+                 key.rfind("FMUNU", 0) == 0 || key == "N1") {
+            /* device selection, dispatcher handshake, OpenCL binaries and the
+               F_munu measurements have no role in this build */
+        }
+        else {
+            fclose(fp);
+            return host_fail(QG_ERR_ARG, "unknown key " + key + " at line " + std::to_string(lineno));
+        }
+    }
+    fclose(fp);
+    return QG_OK;
+}
+
+extern "C" int qg_run(const qg_config *cfg_in, const qg_run_options *o, qg_run_result *res)
+{
+    if (!cfg_in || !o || !res) return host_fail(QG_ERR_ARG, "null argument");
+    if (o->iter < 1 || o->niter < 0 || o->nav < 0) return host_fail(QG_ERR_ARG, "ITER >= 1, NITER >= 0, NAV >= 0");
+    memset(res, 0, sizeof(*res));
+    res->verification_passed = -1;
+    qg_config cfg = *cfg_in;
+    qg_ctx *ctx = nullptr;
+    int rc = qg_create(&cfg, &ctx);
+    if (rc) return host_fail(rc, std::string("qg_create: ") + qg_last_error(nullptr));
+    auto bail = [&](int code) {
+        std::string m = qg_last_error(ctx);
+        qg_destroy(ctx);
+        return host_fail(code, m);
+    };
+    // lattice_init: PRNG::initialize, then the start configuration
+    if ((rc = qg_prng_seed(ctx, cfg.randseries))) return bail(rc);
+    if ((rc = qg_init_links(ctx, cfg.start))) return bail(rc);
+    qg_info info;
+    qg_get_info(ctx, &info);
+    const int N = cfg.group;
+    const double V = info.sites;
+    const double nsp = (double)cfg.size[0] * cfg.size[1] * cfg.size[2];
+    std::vector<double> d[QG_OBS_COUNT];
+    time_t t_start = time(nullptr);
+    auto measure = [&]() -> int {
+        double a[4];
+        int r;
+        if (o->get_plaquettes) {
+            if ((r = qg_measure(ctx, QG_MEAS_PLAQUETTE, a))) return r;
+            d[QG_OBS_PLQ_SPAT].push_back(a[0] / (3 * V));
+            d[QG_OBS_PLQ_TEMP].push_back(a[1] / (3 * V));
+            d[QG_OBS_PLQ_TOTAL].push_back(0.5 * (a[0] + a[1]) / (3 * V));
+        }
+        if (o->get_wilson) {
+            if ((r = qg_measure(ctx, QG_MEAS_WILSON, a))) return r;
+            d[QG_OBS_WILSON].push_back(a[0] / (3 * V));
+        }
+        if (o->get_actions) {
+            if ((r = qg_measure(ctx, QG_MEAS_ACTION, a))) return r;
+            d[QG_OBS_S_SPAT].push_back(a[0] / (3 * V));
+            d[QG_OBS_S_TEMP].push_back(a[1] / (3 * V));
+            d[QG_OBS_S_TOTAL].push_back(0.5 * (a[0] + a[1]) / (3 * V));
+        }
+        if (o->pl_level > 0) {
+            if ((r = qg_measure(ctx, QG_MEAS_POLYAKOV, a))) return r;
+            d[QG_OBS_POLYAKOV].push_back(a[0] / (nsp * N));
+            d[QG_OBS_POLYAKOV_IM].push_back(a[1] / (nsp * N));
+            if (o->pl_level > 1) {
+                d[QG_OBS_POLYAKOV_P2].push_back(a[2] / (nsp * N * N));
+                d[QG_OBS_POLYAKOV_P4].push_back(a[3] / (nsp * N * N * N * N));
+            }
+        }
+        return QG_OK;
+    };
+    auto t0 = std::chrono::steady_clock::now();
+    if ((rc = measure())) return bail(rc);                       // iteration 0: start configuration
+    if ((rc = qg_sweep(ctx, o->nav))) return bail(rc);           // thermalisation
+    for (int i = 1; i < o->iter; i++) {
+        if ((rc = qg_sweep(ctx, o->niter))) return bail(rc);
+        if ((rc = measure())) return bail(rc);
+        if (!o->quiet && i % 10 == 0) { printf("\rGPU working iteration [%d]", i); fflush(stdout); }
+    }
+    if ((rc = qg_sync(ctx))) return bail(rc);
+    auto t1 = std::chrono::steady_clock::now();
+    time_t t_end = time(nullptr);
+    res->seconds = std::chrono::duration<double>(t1 - t0).count();
+    double sweeps = (double)o->nav + (double)(o->iter - 1) * o->niter;
+    res->link_updates_per_second = res->seconds > 0 ? 4.0 * V * sweeps * (1 + cfg.n_or) / res->seconds : 0.0;
+    res->samples = o->iter;
+    for (int k = 0; k < QG_OBS_COUNT; k++) {
+        if (d[k].empty()) continue;
+        mean_var(d[k], res->mean[k], res->variance[k]);
+        res->gpu_last[k] = d[k].back();
+    }
+    // LatticeCheckCPU: FP64 re-measurement of the final configuration
+    if (o->verify) {
+        std::vector<char> buf(info.ref_elems * (cfg.precision ? 8 : 4));
+        if ((rc = qg_links_download(ctx, buf.data(), QG_LAYOUT_REFERENCE))) return bail(rc);
+        Table T;
+        T.group = N; memcpy(T.n, cfg.size, sizeof(T.n)); T.prec = cfg.precision; T.rowsize = info.rowsize;
+        T.p = buf.data();
+        HostObs h = host_measure(T, cfg, *o);
+        res->cpu_last[QG_OBS_PLQ_SPAT] = h.plq_s / (3 * V);
+        res->cpu_last[QG_OBS_PLQ_TEMP] = h.plq_t / (3 * V);
+        res->cpu_last[QG_OBS_PLQ_TOTAL] = 0.5 * (h.plq_s + h.plq_t) / (3 * V);
+        res->cpu_last[QG_OBS_S_SPAT] = h.s_s / (3 * V);
+        res->cpu_last[QG_OBS_S_TEMP] = h.s_t / (3 * V);
+        res->cpu_last[QG_OBS_S_TOTAL] = 0.5 * (h.s_s + h.s_t) / (3 * V);
+        res->cpu_last[QG_OBS_POLYAKOV] = h.pre / (nsp * N);
+        res->cpu_last[QG_OBS_POLYAKOV_IM] = h.pim / (nsp * N);
+        res->cpu_last[QG_OBS_POLYAKOV_P2] = h.p2 / (nsp * N * N);
+        res->cpu_last[QG_OBS_POLYAKOV_P4] = h.p4 / (nsp * N * N * N * N);
+        res->cpu_last[QG_OBS_WILSON] = h.wilson / (3 * V);
+        bool ok = true;
+        for (int k = 0; k < QG_OBS_COUNT; k++)
+            if (!d[k].empty()) ok = verify(res->gpu_last[k], res->cpu_last[k], cfg.precision == 0) && ok;
+        res->verification_passed = ok ? 1 : 0;
+    }
+    qg_destroy(ctx);
+    // lattice_write_results (suncl.cpp:1679-1854): header, statistics, rows
+    if (o->write_results) {
+        char tbuf[64];
+        snprintf(tbuf, sizeof(tbuf), "%s", ctime(&t_end));
+        char name[96];
+        snprintf(name, sizeof(name), "%.2s-%.3s-%.2s-%.2s-%.2s-%.2s.txt", tbuf + 22, tbuf + 4, tbuf + 8, tbuf + 11,
+                 tbuf + 14, tbuf + 17);
+        snprintf(res->results_file, sizeof(res->results_file), "%s%s%s", o->output_path, o->prefix, name);
+        FILE *fp = fopen(res->results_file, "w");
+        if (!fp) return host_fail(QG_ERR_IO, std::string("cannot write ") + res->results_file);
+        const char *start_name[] = { "0", "1", "2", "3" };
+        fprintf(fp, " B200 SU(%d) simulator (qcdgpu_b200)\n\n", N);
+        fprintf(fp, " Monte Carlo simulation of 4D SU(%d) LGT\n\n", N);
+        fprintf(fp, " ***************************************************\n");
+        fprintf(fp, " lattice size                : %3d x %3d x %3d x %3d\n", cfg.size[0], cfg.size[1], cfg.size[2],
+                cfg.size[3]);
+        fprintf(fp, " init                        : 1\n");
+        fprintf(fp, " ints (0=hot, 1=cold, 2=gid) : %s\n", start_name[cfg.start]);
+        fprintf(fp, " random series               : %u\n", cfg.randseries);
+        if (cfg.prng == QG_PRNG_RANLUX) fprintf(fp, " PRN generator (%3d)         : RANLUX\n", cfg.ranlux_nskip);
+        else fprintf(fp, " PRN generator               : PHILOX4x32-10\n");
+        fprintf(fp, " nav                         : %d\n", o->nav);
+        fprintf(fp, " niter                       : %d\n", o->niter);
+        fprintf(fp, " iter (# of samples)         : %d\n", o->iter);
+        fprintf(fp, " nhit                        : %d\n", cfg.nhit);
+        fprintf(fp, " nhitPar                     : %d\n", cfg.nhitpar);
+        fprintf(fp, " overrelaxation sweeps       : %d\n", cfg.n_or);
+        fprintf(fp, " precision                   : %s\n", cfg.precision ? "double" : "single");
+        fprintf(fp, " ***************************************************\n");
+        fprintf(fp, " Wilson loop R               : %d\n", cfg.wilson_r);
+        fprintf(fp, " Wilson loop T               : %d\n", cfg.wilson_t);
+        fprintf(fp, " BETA                        : %16.13e\n", cfg.beta);
+        fprintf(fp, " PHI   (lambda_3)            : %16.13e\n", cfg.phi);
+        fprintf(fp, " OMEGA (lambda_8)            : %16.13e\n", cfg.omega);
+        fprintf(fp, " ***************************************************\n");
+        char ts[64], te[64];
+        snprintf(ts, sizeof(ts), "%s", ctime(&t_start));
+        snprintf(te, sizeof(te), "%s", ctime(&t_end));
+        int el = (int)difftime(t_end, t_start);
+        fprintf(fp, " Start time               : %s", ts);
+        fprintf(fp, " Finish time              : %s", te);
+        fprintf(fp, " Elapsed time             : %d:%2.2d:%2.2d:%2.2d\n", el / 86400, (el / 3600) % 24, (el / 60) % 60,
+                el % 60);
+        fprintf(fp, " ***************************************************\n");
+        static const char *names[QG_OBS_COUNT] = { "S_total", "Plq_total", "Polyakov_loop", "Polyakov_loop_im",
+                                                   "Polyakov_loop_P2", "Polyakov_loop_P4", "Wilson_loop",
+                                                   "Plq_spat", "Plq_temp", "S_spat", "S_temp" };
+        for (int k = 0; k <= QG_OBS_WILSON; k++) {
+            fprintf(fp, " Mean %-20s: % 16.13e\n", names[k], res->mean[k]);
+            fprintf(fp, " Variance %-16s: % 16.13e\n", names[k], res->variance[k]);
+        }
+        fprintf(fp, " ***************************************************\n");
+        for (int k = 0; k <= QG_OBS_WILSON; k++) {
+            fprintf(fp, " CPU last %-16s: % 16.13e\n", names[k], res->cpu_last[k]);
+            fprintf(fp, " GPU last %-16s: % 16.13e\n", names[k], res->gpu_last[k]);
+        }
+        if (res->verification_passed == 1) fprintf(fp, " *** Verification successfully passed! *************\n");
+        else if (res->verification_passed == 0) fprintf(fp, " --- Verification failed! --------------------------\n");
+        fprintf(fp, " ***************************************************\n");
+        fprintf(fp, " Data fields:\n    #,  ");
+        std::vector<int> cols;
+        if (o->get_plaquettes) { cols.push_back(QG_OBS_PLQ_SPAT); cols.push_back(QG_OBS_PLQ_TEMP); cols.push_back(QG_OBS_PLQ_TOTAL); }
+        if (o->get_wilson) cols.push_back(QG_OBS_WILSON);
+        if (o->get_actions) { cols.push_back(QG_OBS_S_SPAT); cols.push_back(QG_OBS_S_TEMP); cols.push_back(QG_OBS_S_TOTAL); }
+        if (o->pl_level > 0) { cols.push_back(QG_OBS_POLYAKOV); cols.push_back(QG_OBS_POLYAKOV_IM); }
+        if (o->pl_level > 1) { cols.push_back(QG_OBS_POLYAKOV_P2); cols.push_back(QG_OBS_POLYAKOV_P4); }
+        for (int k : cols) fprintf(fp, "%-21s ", names[k]);
+        fprintf(fp, "\n ***************************************************\n");
+        for (int i = 0; i < o->iter; i++) {
+            fprintf(fp, "%5i", i);
+            for (int k : cols) fprintf(fp, " % 16.13e", d[k][i]);
+            fprintf(fp, "\n");
+        }
+        fclose(fp);
+    }
+    if (!o->quiet) {
+        printf("\n #        ");
+        printf(" Plq_spat    Plq_temp    S_spat      S_temp\n");
+        for (int i = 0; i < o->iter && o->get_plaquettes && o->get_actions; i++)
+            printf("[%5d]:   %.8f  %.8f  %.8f  %.8f\n", i, d[QG_OBS_PLQ_SPAT][i], d[QG_OBS_PLQ_TEMP][i],
+                   d[QG_OBS_S_SPAT][i], d[QG_OBS_S_TEMP][i]);
+        if (res->verification_passed >= 0)
+            printf("%s\n", res->verification_passed ? "Verification successfully passed!" : "Verification failed!");
+    }
+    return QG_OK;
+}
