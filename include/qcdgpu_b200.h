@@ -133,6 +133,12 @@ int qg_phase(qg_ctx *ctx, int parity, int dir, int kind);
  * global reunitarisation when the sweep count hits cfg.reunit_every.
  * Replayed from a captured CUDA graph.                                    */
 int qg_sweep(qg_ctx *ctx, int nsweeps);
+/* Autotuner (new): times each launch shape of the heatbath and the
+ * overrelaxation phase kernels on this context's lattice (`reps` launches
+ * each; the field is restored and no PRN counter moves) and keeps the
+ * fastest for later phases and sweeps.  times_ms (optional, 6 floats):
+ * per shape v = 0..2, [2v] heatbath and [2v+1] overrelaxation ms/launch.  */
+int qg_tune(qg_ctx *ctx, int reps, float *times_ms);
 /* lattice_GramSchmidt kernel (suncl.cl:350-396); fp64 != 0 computes in FP64 */
 int qg_reunitarize(qg_ctx *ctx, int fp64);
 

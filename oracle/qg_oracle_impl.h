@@ -265,8 +265,8 @@ static G3 FN(gs3)(G3 g)
     REAL n2 = u[0][0] * u[0][0];
     n2 = RFMA(u[0][1], u[0][1], n2);
     for (int k = 1; k < 3; k++) { n2 = RFMA(u[k][0], u[k][0], n2); n2 = RFMA(u[k][1], u[k][1], n2); }
-    REAL nu = RSQRT(n2);
-    for (int k = 0; k < 3; k++) { u[k][0] = u[k][0] / nu; u[k][1] = u[k][1] / nu; }
+    REAL inu = (REAL)1 / RSQRT(n2);
+    for (int k = 0; k < 3; k++) { u[k][0] = u[k][0] * inu; u[k][1] = u[k][1] * inu; }
     REAL sr = v[0][0] * u[0][0], si = v[0][1] * u[0][0];
     sr = RFMA(v[0][1], u[0][1], sr);
     si = RFMA(-v[0][0], u[0][1], si);
@@ -284,8 +284,8 @@ static G3 FN(gs3)(G3 g)
     REAL m2 = v[0][0] * v[0][0];
     m2 = RFMA(v[0][1], v[0][1], m2);
     for (int k = 1; k < 3; k++) { m2 = RFMA(v[k][0], v[k][0], m2); m2 = RFMA(v[k][1], v[k][1], m2); }
-    REAL nv = RSQRT(m2);
-    for (int k = 0; k < 3; k++) { v[k][0] = v[k][0] / nv; v[k][1] = v[k][1] / nv; }
+    REAL inv = (REAL)1 / RSQRT(m2);
+    for (int k = 0; k < 3; k++) { v[k][0] = v[k][0] * inv; v[k][1] = v[k][1] * inv; }
     G3 r;
     r.uv1.x = u[0][0]; r.uv1.y = u[1][0]; r.uv1.z = u[2][0]; r.uv1.w = v[2][0];
     r.uv2.x = u[0][1]; r.uv2.y = u[1][1]; r.uv2.z = u[2][1]; r.uv2.w = v[2][1];
@@ -393,14 +393,16 @@ static int FN(kp_step)(S2 *a, REAL beta, FN(prnctx) *p, int su3_path)
         n2 = aH.x * aH.x;
         n2 = RFMA(aH.y, aH.y, n2); n2 = RFMA(aH.z, aH.z, n2); n2 = RFMA(aH.w, aH.w, n2);
         det = RSQRT(n2);
-        aH.x /= det; aH.z /= det; aH.y /= det; aH.w /= det;
+        REAL id = (REAL)1 / det;
+        aH.x *= id; aH.z *= id; aH.y *= id; aH.w *= id;
     } else {
         REAL Mx = a->u1.re + a->v2.re, My = a->u1.im - a->v2.im;
         REAL Mz = a->u2.re - a->v1.re, Mw = a->u2.im + a->v1.im;
         n2 = Mx * Mx;
         n2 = RFMA(My, My, n2); n2 = RFMA(Mz, Mz, n2); n2 = RFMA(Mw, Mw, n2);
         det = RSQRT(n2);
-        aH.x = Mx / det; aH.z = -My / det; aH.y = -Mz / det; aH.w = -Mw / det;
+        REAL id = (REAL)1 / det;
+        aH.x = Mx * id; aH.z = -My * id; aH.y = -Mz * id; aH.w = -Mw * id;
     }
     bdet = beta * det;
     for (int i = 0; i < c->nhit && !flag; i++) {
@@ -465,8 +467,8 @@ static void FN(or_step)(S2 *a)
     aH.w = -(a->u2.im + a->v1.im);
     REAL n2 = aH.x * aH.x;
     n2 = RFMA(aH.y, aH.y, n2); n2 = RFMA(aH.z, aH.z, n2); n2 = RFMA(aH.w, aH.w, n2);
-    REAL det = RSQRT(n2);
-    aH.x /= det; aH.z /= det; aH.y /= det; aH.w /= det;
+    REAL id = (REAL)1 / RSQRT(n2);
+    aH.x *= id; aH.z *= id; aH.y *= id; aH.w *= id;
     *a = FN(rec2)(FN(times2)(aH, aH));
 }
 
@@ -609,8 +611,8 @@ static void FN(phase)(const ol_cfg *c, REAL *tab, int parity, int mu, const ol_p
                 REAL Mz = st.u2.re - st.v1.re, Mw = st.u2.im + st.v1.im;
                 REAL n2 = Mx * Mx;
                 n2 = RFMA(My, My, n2); n2 = RFMA(Mz, Mz, n2); n2 = RFMA(Mw, Mw, n2);
-                REAL det = RSQRT(n2);
-                aH.x = Mx / det; aH.z = -My / det; aH.y = -Mz / det; aH.w = -Mw / det;
+                REAL id = (REAL)1 / RSQRT(n2);
+                aH.x = Mx * id; aH.z = -My * id; aH.y = -Mz * id; aH.w = -Mw * id;
                 G2 r;
                 r.uv1 = FN(times2)(FN(times2)(aH, FN(herm2)(m0.uv1)), aH);
                 FN(store2)(c, tab, g, mu, r);

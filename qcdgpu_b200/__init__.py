@@ -27,7 +27,7 @@ EXPORTED_SYMBOLS = (
     "qg_prng_seed", "qg_prng_produce", "qg_prns_upload", "qg_prns_download", "qg_init_links",
     "qg_phase", "qg_sweep", "qg_reunitarize", "qg_measure", "qg_measure_wilson",
     "qg_links_upload", "qg_links_download", "qg_set_phase_counter", "qg_glibc_seeds", "qg_set_params", "qg_get_stream",
-    "qg_default_run_options", "qg_parse_init_file", "qg_run",
+    "qg_default_run_options", "qg_parse_init_file", "qg_run", "qg_tune",
 )
 
 
@@ -145,6 +145,7 @@ def load_library(path=LIB_PATH):
     lib.qg_glibc_seeds.argtypes = [ctypes.c_uint32, ctypes.c_int, P(ctypes.c_uint32)]
     lib.qg_set_params.argtypes = [vp, ctypes.c_double, ctypes.c_double, ctypes.c_double]
     lib.qg_get_stream.argtypes = [vp, P(vp)]
+    lib.qg_tune.argtypes = [vp, ctypes.c_int, P(ctypes.c_float)]
     lib.qg_default_run_options.argtypes = [P(RunOptions)]
     lib.qg_parse_init_file.argtypes = [ctypes.c_char_p, P(Config), P(RunOptions)]
     lib.qg_run.argtypes = [P(Config), P(RunOptions), P(RunResult)]
@@ -271,6 +272,13 @@ class Lattice:
 
     def reunitarize(self, fp64=False):
         self._ck(self.lib.qg_reunitarize(self.ctx, 1 if fp64 else 0), "qg_reunitarize")
+
+    def tune(self, reps=4):
+        """Pick the fastest phase-kernel launch shapes on this lattice; returns
+        the measured ms per launch as [(heatbath, overrelaxation)] per shape."""
+        t = (ctypes.c_float * 6)()
+        self._ck(self.lib.qg_tune(self.ctx, reps, t), "qg_tune")
+        return [(t[2 * v], t[2 * v + 1]) for v in range(3)]
 
     def sync(self):
         self._ck(self.lib.qg_sync(self.ctx), "qg_sync")

@@ -29,6 +29,7 @@ struct qg_ctx {
     double *d_params = nullptr;     // {BETA/N, PHI, OMEGA, 0}: lattice_parameters
     double *h_params = nullptr;     // pinned staging
     int twist_built = 0;            // twist flag the cached graphs were built with
+    int variant_hb = 0, variant_or = 0;   // phase-kernel launch shapes (qg_tune)
     uint64_t phase_counter = 0;     // host mirror of *d_phase
     uint32_t prng_counter = 0;      // RANLUX batches produced
     uint64_t sweeps_done = 0;
@@ -376,6 +377,7 @@ static PhaseArgs phase_args(qg_ctx *c, int parity, int dir, int kind, uint32_t o
     a.key = c->key;
     a.phase_base = c->d_phase;
     a.phase_offset = offset;
+    a.variant = (kind == QG_UPDATE_OVERRELAX) ? c->variant_or : c->variant_hb;
     return a;
 }
 
@@ -402,6 +404,55 @@ extern "C" int qg_phase(qg_ctx *c, int parity, int dir, int kind)
         QG_CK(launch_add_u64(c->d_phase, 1, c->stream), "phase counter");
         c->phase_counter++;
     }
+    return QG_OK;
+}
+
+// times each launch shape of the heatbath and overrelaxation phase kernels
+// on the live field (restored afterwards, PRN counters untouched) and keeps
+// the fastest per kind
+extern "C" int qg_tune(qg_ctx *c, int reps, float *times_ms)
+{
+    if (!c) return QG_ERR_ARG;
+    if (reps < 1) reps = 4;
+    if (needs_seed(c, QG_UPDATE_HEATBATH)) return fail(c, QG_ERR_STATE, "tuning needs a seeded PRNG (qg_prng_seed)");
+    void *backup = nullptr;
+    QG_CK(cudaMallocAsync(&backup, c->link_bytes, c->stream), "tune backup");
+    QG_CK(cudaMemcpyAsync(backup, c->links, c->link_bytes, cudaMemcpyDeviceToDevice, c->stream), "tune backup copy");
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    float best[2] = { 1e30f, 1e30f };
+    int arg[2] = { 0, 0 };
+    cudaError_t e = cudaSuccess;
+    for (int v = 0; v < kPhaseVariants && e == cudaSuccess; v++)
+        for (int kind = 0; kind < 2 && e == cudaSuccess; kind++) {
+            PhaseArgs a = phase_args(c, 0, 0, kind, 0);
+            a.variant = v;
+            // one untimed launch, then reps timed ones over the 8 phase classes
+            for (int r = -1; r < reps && e == cudaSuccess; r++) {
+                if (r == 0) cudaEventRecord(e0, c->stream);
+                a.parity = (r + 1) & 1;
+                a.dir = ((r + 1) >> 1) & 3;
+                e = launch_phase(c, a);
+            }
+            cudaEventRecord(e1, c->stream);
+            cudaEventSynchronize(e1);
+            float ms = 0;
+            cudaEventElapsedTime(&ms, e0, e1);
+            ms /= reps;
+            if (times_ms) times_ms[2 * v + kind] = ms;
+            if (ms < best[kind]) { best[kind] = ms; arg[kind] = v; }
+        }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaError_t e2 = cudaMemcpyAsync(c->links, backup, c->link_bytes, cudaMemcpyDeviceToDevice, c->stream);
+    cudaFreeAsync(backup, c->stream);
+    if (e != cudaSuccess) return cuda_fail(c, e, "tune launch");
+    if (e2 != cudaSuccess) return cuda_fail(c, e2, "tune restore");
+    QG_CK(cudaStreamSynchronize(c->stream), "tune sync");
+    c->variant_hb = arg[0];
+    c->variant_or = arg[1];
+    destroy_graphs(c);
     return QG_OK;
 }
 

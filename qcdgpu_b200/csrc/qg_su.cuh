@@ -271,9 +271,9 @@ __device__ __forceinline__ G3<Real> gs3(const G3<Real> &g)
     n2 = FMA(u[0][1], u[0][1], n2);
 #pragma unroll
     for (int k = 1; k < 3; k++) { n2 = FMA(u[k][0], u[k][0], n2); n2 = FMA(u[k][1], u[k][1], n2); }
-    Acc nu = sqrt(n2);
+    Acc inu = (Acc)1 / sqrt(n2);
 #pragma unroll
-    for (int k = 0; k < 3; k++) { u[k][0] = u[k][0] / nu; u[k][1] = u[k][1] / nu; }
+    for (int k = 0; k < 3; k++) { u[k][0] = u[k][0] * inu; u[k][1] = u[k][1] * inu; }
     // sc = sum_k v_k conj(u_k)
     Acc sr = v[0][0] * u[0][0], si = v[0][1] * u[0][0];
     sr = FMA(v[0][1], u[0][1], sr);
@@ -295,9 +295,9 @@ __device__ __forceinline__ G3<Real> gs3(const G3<Real> &g)
     m2 = FMA(v[0][1], v[0][1], m2);
 #pragma unroll
     for (int k = 1; k < 3; k++) { m2 = FMA(v[k][0], v[k][0], m2); m2 = FMA(v[k][1], v[k][1], m2); }
-    Acc nv = sqrt(m2);
+    Acc inv = (Acc)1 / sqrt(m2);
 #pragma unroll
-    for (int k = 0; k < 3; k++) { v[k][0] = v[k][0] / nv; v[k][1] = v[k][1] / nv; }
+    for (int k = 0; k < 3; k++) { v[k][0] = v[k][0] * inv; v[k][1] = v[k][1] * inv; }
     G3<Real> r;
     r.uv1 = { (Real)u[0][0], (Real)u[1][0], (Real)u[2][0], (Real)v[2][0] };
     r.uv2 = { (Real)u[0][1], (Real)u[1][1], (Real)u[2][1], (Real)v[2][1] };
@@ -407,14 +407,16 @@ __device__ __forceinline__ bool kp_step(S2<Real> &a, Real beta, Prn &prn, int nh
         Real n2 = aH.x * aH.x;
         n2 = FMA(aH.y, aH.y, n2); n2 = FMA(aH.z, aH.z, n2); n2 = FMA(aH.w, aH.w, n2);
         det = RC<Real>::sq(n2);
-        aH.x /= det; aH.z /= det; aH.y /= det; aH.w /= det;
+        Real id = (Real)1 / det;
+        aH.x *= id; aH.z *= id; aH.y *= id; aH.w *= id;
     } else {
         Real Mx = a.u1.re + a.v2.re, My = a.u1.im - a.v2.im;
         Real Mz = a.u2.re - a.v1.re, Mw = a.u2.im + a.v1.im;
         Real n2 = Mx * Mx;
         n2 = FMA(My, My, n2); n2 = FMA(Mz, Mz, n2); n2 = FMA(Mw, Mw, n2);
         det = RC<Real>::sq(n2);
-        aH.x = Mx / det; aH.z = -My / det; aH.y = -Mz / det; aH.w = -Mw / det;
+        Real id = (Real)1 / det;
+        aH.x = Mx * id; aH.z = -My * id; aH.y = -Mz * id; aH.w = -Mw * id;
     }
     Real bdet = beta * det;
     Real delta = 0;
@@ -463,8 +465,8 @@ __device__ __forceinline__ void or_step(S2<Real> &a)
     aH.w = -(a.u2.im + a.v1.im);
     Real n2 = aH.x * aH.x;
     n2 = FMA(aH.y, aH.y, n2); n2 = FMA(aH.z, aH.z, n2); n2 = FMA(aH.w, aH.w, n2);
-    Real det = RC<Real>::sq(n2);
-    aH.x /= det; aH.z /= det; aH.y /= det; aH.w /= det;
+    Real id = (Real)1 / RC<Real>::sq(n2);
+    aH.x *= id; aH.z *= id; aH.y *= id; aH.w *= id;
     a = rec2(times2(aH, aH));
 }
 

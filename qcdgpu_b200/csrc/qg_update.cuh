@@ -18,17 +18,17 @@ struct Twist {
 };
 
 template <typename Real>
-__device__ __forceinline__ G3<Real> load3t(const Field<Real> &U, int dir, uint32_t e, const Crd &c, const Twist<Real> &tw)
+__device__ __forceinline__ G3<Real> load3t(const Field<Real> &U, int dir, uint32_t e, int xc, const Twist<Real> &tw)
 {
     G3<Real> m = U.ldg3(dir, e);
-    if (tw.on && dir == 1 && c.x == tw.xlast) m = twist3(m, tw.phi, tw.omega);
+    if (tw.on && dir == 1 && xc == tw.xlast) m = twist3(m, tw.phi, tw.omega);
     return m;
 }
 template <typename Real>
-__device__ __forceinline__ R4<Real> load2t(const Field<Real> &U, int dir, uint32_t e, const Crd &c, const Twist<Real> &tw)
+__device__ __forceinline__ R4<Real> load2t(const Field<Real> &U, int dir, uint32_t e, int xc, const Twist<Real> &tw)
 {
     R4<Real> m = U.ldg2(dir, e);
-    if (tw.on && dir == 1 && c.x == tw.xlast) {
+    if (tw.on && dir == 1 && xc == tw.xlast) {
         R4<Real> om = { RC<Real>::cs(tw.phi / 2), 0, RC<Real>::sn(tw.phi / 2), 0 };
         m = times2(om, m);
     }
@@ -36,28 +36,61 @@ __device__ __forceinline__ R4<Real> load2t(const Field<Real> &U, int dir, uint32
 }
 
 // the reference's fixed plane order: mu=X: Y,Z,T; Y: X,Z,T; Z: Y,X,T; T: Y,Z,X
-__device__ __forceinline__ int nu_of(int mu, int i)
+__host__ __device__ constexpr int nu_of(int mu, int i)
 {
     return (i == 0) ? (mu == 1 ? 0 : 1) : (i == 1) ? (mu == 2 ? 0 : 2) : (mu == 3 ? 0 : 3);
 }
 
-template <typename Real>
-__device__ __forceinline__ M3<Real> staple3(const Field<Real> &U, const Geom &G, const Crd &c, int p, int mu,
+// Neighbour offsets in checkerboard half-index space.  With N2 even the
+// half index of a site is h = (y>>1) + (N2/2)(z + N3 t + N3 N4 x), so a
+// shift along one direction changes h by an amount that depends only on
+// that direction's coordinate (and y's parity), and two shifts along
+// different directions add: h(x - nu + mu) = h + dm[nu] + dp[mu].
+struct Nbr {
+    int32_t dp[4], dm[4];
+    int x, xp, xm;          // x coordinates of the site and of its x neighbours
+};
+
+__device__ __forceinline__ Nbr neighbours(const Geom &G, const Crd &c)
+{
+    Nbr n;
+    const int32_t Y2 = G.n[1] >> 1;
+    const int32_t sz = Y2, st = Y2 * G.n[2], sx = st * G.n[3];
+    // y: y+1 changes y>>1 by (y odd); the wrap from N2-1 to 0 by -(Y2-1)
+    n.dp[1] = (c.y == G.n[1] - 1) ? -(Y2 - 1) : (c.y & 1);
+    n.dm[1] = (c.y == 0) ? (Y2 - 1) : -((c.y & 1) ^ 1);
+    n.dp[2] = (c.z == G.n[2] - 1) ? -sz * (G.n[2] - 1) : sz;
+    n.dm[2] = (c.z == 0) ? sz * (G.n[2] - 1) : -sz;
+    n.dp[3] = (c.t == G.n[3] - 1) ? -st * (G.n[3] - 1) : st;
+    n.dm[3] = (c.t == 0) ? st * (G.n[3] - 1) : -st;
+    n.dp[0] = (c.x == G.n[0] - 1) ? -sx * (G.n[0] - 1) : sx;
+    n.dm[0] = (c.x == 0) ? sx * (G.n[0] - 1) : -sx;
+    n.x = c.x;
+    n.xp = (c.x == G.n[0] - 1) ? 0 : c.x + 1;
+    n.xm = (c.x == 0) ? G.n[0] - 1 : c.x - 1;
+    return n;
+}
+
+// staple of U_mu(x), lattice_staple_3 (su3_update_cl.cl:341-565): per
+// plane nu the forward term U_nu(x+mu) U_mu(x+nu)^+ U_nu(x)^+ and the
+// backward term U_nu(x-nu+mu)^+ U_mu(x-nu)^+ U_nu(x-nu), summed as
+// st = f0 + b0; st = b_i + (st + f_i)
+template <int mu, typename Real>
+__device__ __forceinline__ M3<Real> staple3(const Field<Real> &U, const Geom &G, uint32_t t, const Nbr &n, int p,
                                            const Twist<Real> &tw)
 {
-    const Crd cp = step_plus(G, c, mu);
-    const uint32_t e_cp = cb_index(G, cp, p ^ 1);
-    const uint32_t e_c = (uint32_t)p * G.cb + (crd2lex(G, c) >> 1);
+    const uint32_t own = (uint32_t)p * G.cb + t, opp = (uint32_t)(p ^ 1) * G.cb + t;
+    const int xmu = (mu == 0) ? n.xp : n.x;
     M3<Real> st, s2;
 #pragma unroll
     for (int i = 0; i < 3; i++) {
         const int nu = nu_of(mu, i);
-        const Crd cn = step_plus(G, c, nu);
-        const Crd cm = step_minus(G, c, nu);
-        const Crd cmp = step_plus(G, cm, mu);
-        const uint32_t e_cn = cb_index(G, cn, p ^ 1), e_cm = cb_index(G, cm, p ^ 1), e_cmp = cb_index(G, cmp, p);
-        M3<Real> fw = staple_fwd3(load3t(U, nu, e_cp, cp, tw), load3t(U, mu, e_cn, cn, tw), load3t(U, nu, e_c, c, tw));
-        M3<Real> bw = staple_bwd3(load3t(U, nu, e_cmp, cmp, tw), load3t(U, mu, e_cm, cm, tw), load3t(U, nu, e_cm, cm, tw));
+        const int xnp = (nu == 0) ? n.xp : n.x, xnm = (nu == 0) ? n.xm : n.x;
+        const int xnmmu = (nu == 0) ? n.xm : xmu;
+        M3<Real> fw = staple_fwd3(load3t(U, nu, opp + n.dp[mu], xmu, tw), load3t(U, mu, opp + n.dp[nu], xnp, tw),
+                                  load3t(U, nu, own, n.x, tw));
+        M3<Real> bw = staple_bwd3(load3t(U, nu, own + n.dm[nu] + n.dp[mu], xnmmu, tw),
+                                  load3t(U, mu, opp + n.dm[nu], xnm, tw), load3t(U, nu, opp + n.dm[nu], xnm, tw));
         if (i == 0) {
             add3(st, fw, bw);
         } else {
@@ -68,23 +101,22 @@ __device__ __forceinline__ M3<Real> staple3(const Field<Real> &U, const Geom &G,
     return st;
 }
 
-template <typename Real>
-__device__ __forceinline__ S2<Real> staple2(const Field<Real> &U, const Geom &G, const Crd &c, int p, int mu,
+template <int mu, typename Real>
+__device__ __forceinline__ S2<Real> staple2(const Field<Real> &U, const Geom &G, uint32_t t, const Nbr &n, int p,
                                            const Twist<Real> &tw)
 {
-    const Crd cp = step_plus(G, c, mu);
-    const uint32_t e_cp = cb_index(G, cp, p ^ 1);
-    const uint32_t e_c = (uint32_t)p * G.cb + (crd2lex(G, c) >> 1);
+    const uint32_t own = (uint32_t)p * G.cb + t, opp = (uint32_t)(p ^ 1) * G.cb + t;
+    const int xmu = (mu == 0) ? n.xp : n.x;
     S2<Real> st, s2;
 #pragma unroll
     for (int i = 0; i < 3; i++) {
         const int nu = nu_of(mu, i);
-        const Crd cn = step_plus(G, c, nu);
-        const Crd cm = step_minus(G, c, nu);
-        const Crd cmp = step_plus(G, cm, mu);
-        const uint32_t e_cn = cb_index(G, cn, p ^ 1), e_cm = cb_index(G, cm, p ^ 1), e_cmp = cb_index(G, cmp, p);
-        S2<Real> fw = staple_fwd2(load2t(U, nu, e_cp, cp, tw), load2t(U, mu, e_cn, cn, tw), load2t(U, nu, e_c, c, tw));
-        S2<Real> bw = staple_bwd2(load2t(U, nu, e_cmp, cmp, tw), load2t(U, mu, e_cm, cm, tw), load2t(U, nu, e_cm, cm, tw));
+        const int xnp = (nu == 0) ? n.xp : n.x, xnm = (nu == 0) ? n.xm : n.x;
+        const int xnmmu = (nu == 0) ? n.xm : xmu;
+        S2<Real> fw = staple_fwd2(load2t(U, nu, opp + n.dp[mu], xmu, tw), load2t(U, mu, opp + n.dp[nu], xnp, tw),
+                                  load2t(U, nu, own, n.x, tw));
+        S2<Real> bw = staple_bwd2(load2t(U, nu, own + n.dm[nu] + n.dp[mu], xnmmu, tw),
+                                  load2t(U, mu, opp + n.dm[nu], xnm, tw), load2t(U, nu, opp + n.dm[nu], xnm, tw));
         if (i == 0) {
             st = add2(fw, bw);
         } else {
@@ -119,16 +151,19 @@ template <typename Real> struct PrnOf<Real, 2> {
     }
 };
 
-template <int NC, typename Real, int PMODE, bool OR>
-__global__ void __launch_bounds__(128) k_phase(Field<Real> U, Geom G, PhaseArgs A)
+// MINB: minimum resident blocks of 128 threads per SM asked of the
+// compiler (0 = its own register choice); the launch shapes the tuner picks
+template <int NC, typename Real, int PMODE, bool OR, int mu, int MINB>
+__global__ void __launch_bounds__(128, MINB) k_phase(Field<Real> U, Geom G, PhaseArgs A)
 {
     const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= G.half) return;
-    const int p = A.parity, mu = A.dir;
+    const int p = A.parity;
     Crd c = lex2crd(G, 2 * t);
     if (parity_of(c) != p) c.y += 1;                 // lattice_{even,odd}_gid
-    const uint32_t site = crd2lex(G, c);
+    const uint32_t site = 2 * t + (uint32_t)(c.y & 1);
     const uint32_t e0 = (uint32_t)p * G.cb + t;
+    const Nbr nb = neighbours(G, c);
     Twist<Real> tw;
     tw.on = A.twist; tw.xlast = G.n[0] - 1;
     tw.phi = (Real)(float)A.params[1]; tw.omega = (Real)(float)A.params[2];
@@ -139,7 +174,7 @@ __global__ void __launch_bounds__(128) k_phase(Field<Real> U, Geom G, PhaseArgs 
     if (NC == 3) {
         G3<Real> m0 = U.ld3(mu, e0);
         if (tw.on && mu == 1 && c.x == tw.xlast) m0 = twist3(m0, tw.phi, tw.omega);
-        M3<Real> st = staple3(U, G, c, p, mu, tw);
+        M3<Real> st = staple3<mu>(U, G, t, nb, p, tw);
         G3<Real> mU = cm3<Real, OR>(st, m0, beta, prn, A.nhit, A.nhitpar);
         U.st3(mu, e0, mU);
     } else {
@@ -148,7 +183,7 @@ __global__ void __launch_bounds__(128) k_phase(Field<Real> U, Geom G, PhaseArgs 
             R4<Real> om = { RC<Real>::cs(tw.phi / 2), 0, RC<Real>::sn(tw.phi / 2), 0 };
             m0 = times2(om, m0);
         }
-        S2<Real> st = staple2(U, G, c, p, mu, tw);
+        S2<Real> st = staple2<mu>(U, G, t, nb, p, tw);
         if (!OR) {
             S2<Real> a = st;
             if (kp_step<Real, false>(a, beta, prn, A.nhit))
@@ -158,8 +193,10 @@ __global__ void __launch_bounds__(128) k_phase(Field<Real> U, Geom G, PhaseArgs 
         } else {
             Real Mx = st.u1.re + st.v2.re, My = st.u1.im - st.v2.im;
             Real Mz = st.u2.re - st.v1.re, Mw = st.u2.im + st.v1.im;
-            Real det = RC<Real>::sq(Mx * Mx + My * My + Mz * Mz + Mw * Mw);
-            R4<Real> aH = { Mx / det, -Mz / det, -My / det, -Mw / det };
+            Real n2 = Mx * Mx;
+            n2 = FMA(My, My, n2); n2 = FMA(Mz, Mz, n2); n2 = FMA(Mw, Mw, n2);
+            Real id = (Real)1 / RC<Real>::sq(n2);
+            R4<Real> aH = { Mx * id, -Mz * id, -My * id, -Mw * id };
             U.st2(mu, e0, times2(times2(aH, herm2(m0)), aH));
         }
     }
@@ -174,7 +211,22 @@ cudaError_t launch_phase_T(const Geom &G, void *links, int group, const PhaseArg
     const int bs = 128;
     const unsigned nb = (G.half + bs - 1) / bs;
     const int pm = a.prn_mode;   // -1 selects overrelaxation (no PRNs)
-#define QG_LAUNCH(NC, PM, OR) k_phase<NC, Real, PM, OR><<<nb, bs, 0, s>>>(U, G, a)
+#define QG_LAUNCH2(NC, PM, OR, MU, MB) k_phase<NC, Real, PM, OR, MU, MB><<<nb, bs, 0, s>>>(U, G, a)
+#define QG_LAUNCH1(NC, PM, OR, MU)                                \
+    do {                                                          \
+        if (a.variant == 1) QG_LAUNCH2(NC, PM, OR, MU, 5);        \
+        else if (a.variant == 2) QG_LAUNCH2(NC, PM, OR, MU, 6);   \
+        else QG_LAUNCH2(NC, PM, OR, MU, 0);                       \
+    } while (0)
+#define QG_LAUNCH(NC, PM, OR)                                     \
+    do {                                                          \
+        switch (a.dir) {                                          \
+        case 0: QG_LAUNCH1(NC, PM, OR, 0); break;                 \
+        case 1: QG_LAUNCH1(NC, PM, OR, 1); break;                 \
+        case 2: QG_LAUNCH1(NC, PM, OR, 2); break;                 \
+        default: QG_LAUNCH1(NC, PM, OR, 3); break;                \
+        }                                                         \
+    } while (0)
     if (group == 3) {
         if (pm == -1) QG_LAUNCH(3, 0, true);
         else if (pm == 0) QG_LAUNCH(3, 0, false);
@@ -187,6 +239,8 @@ cudaError_t launch_phase_T(const Geom &G, void *links, int group, const PhaseArg
         else QG_LAUNCH(2, 2, false);
     }
 #undef QG_LAUNCH
+#undef QG_LAUNCH1
+#undef QG_LAUNCH2
     return cudaGetLastError();
 }
 

@@ -329,3 +329,25 @@ def test_bench_config_properties(prng):
     assert res[0] == res[1]
     sp, tp, tot = res[0][0]
     assert 1.6 < tot < 2.6
+
+
+def test_tune_restores_field_and_keeps_results():
+    """qg_tune times launch shapes on a copy of the state it restores; the
+    shapes compute the same sequence, so tuned and untuned chains agree."""
+    outs = []
+    for tune in (False, True):
+        L = Q.Lattice(Q.default_config(group=3, size=(8, 8, 8, 8), precision=0, start=Q.START_COLD,
+                                       prng=Q.PRNG_PHILOX, beta=6.0, n_or=2, reunit_every=2))
+        L.seed(54)
+        L.init()
+        L.sweep(1)
+        before = L.download()
+        if tune:
+            t = L.tune(reps=2)
+            assert len(t) == 3 and all(a > 0 and b > 0 for a, b in t)
+            assert np.array_equal(L.download(), before)
+            assert L.info().phase_counter == 8
+        L.sweep(2)
+        outs.append(L.download())
+        L.close()
+    assert np.array_equal(outs[0], outs[1])
