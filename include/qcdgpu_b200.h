@@ -168,6 +168,26 @@ int qg_get_stream(qg_ctx *ctx, void **stream);
 /* Philox phase counter (fast mode): read / set for checkpoint and resume */
 int qg_set_phase_counter(qg_ctx *ctx, uint64_t counter);
 
+/* Allocation-free plaquette/action sums.  No counterpart in the reference:
+ * it exists for callers that may not allocate device memory at the call
+ * site -- a program embedded in a framework that owns the device memory
+ * pool, or a latency-critical loop where cudaMalloc/cudaFree would
+ * synchronise the device.  The caller passes device pointers: `links`, a
+ * reference-layout table (QG_LAYOUT_REFERENCE; float if precision == 0,
+ * double if 1; `rowsize` >= sites) and `out`, four doubles receiving the
+ * sums of qg_measure: spatial and temporal Re Tr plaquette, spatial and
+ * temporal (beta/N)(3N - Re Tr).  Periodic boundaries.  Work is queued on
+ * `stream` (NULL = legacy default stream); nothing is allocated or freed.
+ * The per-block partial sums use a fixed 512 KiB array inside the library,
+ * present on every GPU that loads it until the process exits, so lattices
+ * are limited to 2^24 sites (64^4); larger ones are rejected with
+ * QG_ERR_ARG.  The first call on a device looks up that array's device
+ * address (cudaGetSymbolAddress); make that first call before any stream
+ * capture.  All calls share the array: calls whose kernels may overlap on
+ * the GPU race and must be ordered by the caller.  Errors: qg_last_error(NULL). */
+int qg_plaquette_noalloc(const void *links, int group, int precision, const int size[4], uint32_t rowsize,
+                         double beta, double *out, void *stream);
+
 /* ===================================================================== */
 /* Host driver: the reference's init.dat run setup, run loop and output   */
 /* (SU(N)/QCDGPU.cpp:61-269, model::lattice_get_init_file / lattice_init / */

@@ -27,7 +27,7 @@ EXPORTED_SYMBOLS = (
     "qg_prng_seed", "qg_prng_produce", "qg_prns_upload", "qg_prns_download", "qg_init_links",
     "qg_phase", "qg_sweep", "qg_reunitarize", "qg_measure", "qg_measure_wilson",
     "qg_links_upload", "qg_links_download", "qg_set_phase_counter", "qg_glibc_seeds", "qg_set_params", "qg_get_stream",
-    "qg_default_run_options", "qg_parse_init_file", "qg_run", "qg_tune",
+    "qg_default_run_options", "qg_parse_init_file", "qg_run", "qg_tune", "qg_plaquette_noalloc",
 )
 
 
@@ -146,6 +146,8 @@ def load_library(path=LIB_PATH):
     lib.qg_set_params.argtypes = [vp, ctypes.c_double, ctypes.c_double, ctypes.c_double]
     lib.qg_get_stream.argtypes = [vp, P(vp)]
     lib.qg_tune.argtypes = [vp, ctypes.c_int, P(ctypes.c_float)]
+    lib.qg_plaquette_noalloc.argtypes = [vp, ctypes.c_int, ctypes.c_int, P(ctypes.c_int), ctypes.c_uint32,
+                                         ctypes.c_double, vp, vp]
     lib.qg_default_run_options.argtypes = [P(RunOptions)]
     lib.qg_parse_init_file.argtypes = [ctypes.c_char_p, P(Config), P(RunOptions)]
     lib.qg_run.argtypes = [P(Config), P(RunOptions), P(RunResult)]
