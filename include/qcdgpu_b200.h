@@ -136,9 +136,18 @@ int qg_sweep(qg_ctx *ctx, int nsweeps);
 /* Autotuner (new): times each launch shape of the heatbath and the
  * overrelaxation phase kernels on this context's lattice (`reps` launches
  * each; the field is restored and no PRN counter moves) and keeps the
- * fastest for later phases and sweeps.  times_ms (optional, 6 floats):
- * per shape v = 0..2, [2v] heatbath and [2v+1] overrelaxation ms/launch.  */
+ * fastest for later phases and sweeps.  Shapes: 0 = links loaded straight
+ * into registers, compiler's register count; 1, 2 = the same held to 5 / 6
+ * resident blocks per SM; 3, 4 = staple links streamed through shared
+ * memory two staple terms ahead (SU(3) FP32; other cases run shape 0 / 1).
+ * All shapes compute the same operation sequence.  times_ms (optional,
+ * 2*QG_TUNE_SHAPES floats): per shape v, [2v] heatbath and [2v+1]
+ * overrelaxation ms/launch.                                               */
+#define QG_TUNE_SHAPES 5
 int qg_tune(qg_ctx *ctx, int reps, float *times_ms);
+/* pin / read the launch shapes (0 .. QG_TUNE_SHAPES-1) without tuning     */
+int qg_set_shapes(qg_ctx *ctx, int heatbath_shape, int overrelax_shape);
+int qg_get_shapes(qg_ctx *ctx, int *heatbath_shape, int *overrelax_shape);
 /* lattice_GramSchmidt kernel (suncl.cl:350-396); fp64 != 0 computes in FP64 */
 int qg_reunitarize(qg_ctx *ctx, int fp64);
 

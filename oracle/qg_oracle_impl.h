@@ -223,28 +223,35 @@ static M3 FN(mul3)(const M3 *u, const M3 *v)
 }
 
 /* staple term U_a U_b^+ U_c^+ (lattice_staple_hermitian3, su3_update_cl.cl:294-307):
- * rows 1,2 of P = A B^+, row 3 of P reconstructed, then P C^+ */
+ * rows 1,2 of P = A B^+, rows 1,2 of T = P C^+, row 3 of T reconstructed */
 static M3 FN(staple_fwd3)(G3 ga, G3 gb, G3 gc)
 {
-    M3 A = FN(expand)(ga), B = FN(expand)(gb), C = FN(expand)(gc), P, Q;
+    M3 A = FN(expand)(ga), B = FN(expand)(gb), C = FN(expand)(gc), P, T;
     for (int i = 0; i < 2; i++)
         for (int j = 0; j < 3; j++) P.m[i][j] = FN(dotc3)(&A.m[i][0], 1, &B.m[j][0], 1);
-    FN(fill_row3)(&P);
-    for (int i = 0; i < 3; i++)
-        for (int j = 0; j < 3; j++) Q.m[i][j] = FN(dotc3)(&P.m[i][0], 1, &C.m[j][0], 1);
-    return Q;
+    for (int i = 0; i < 2; i++)
+        for (int j = 0; j < 3; j++) T.m[i][j] = FN(dotc3)(&P.m[i][0], 1, &C.m[j][0], 1);
+    FN(fill_row3)(&T);
+    return T;
 }
 /* staple term U_a^+ U_b^+ U_c (lattice_staple_hermitian_backward3,
- * su3_update_cl.cl:324-338): rows 1,2 of R = B A, row 3 reconstructed, R^+ C */
+ * su3_update_cl.cl:324-338) as the adjoint of H = C^+ R, R = B A: rows 1,2
+ * of R, row 3 of R reconstructed, rows 1,2 of H, row 3 of H reconstructed */
 static M3 FN(staple_bwd3)(G3 ga, G3 gb, G3 gc)
 {
-    M3 A = FN(expand)(ga), B = FN(expand)(gb), C = FN(expand)(gc), R, Q;
+    M3 A = FN(expand)(ga), B = FN(expand)(gb), C = FN(expand)(gc), R, H, T;
     for (int i = 0; i < 2; i++)
         for (int j = 0; j < 3; j++) R.m[i][j] = FN(dot3)(&B.m[i][0], 1, &A.m[0][j], 3);
     FN(fill_row3)(&R);
+    for (int i = 0; i < 2; i++)
+        for (int j = 0; j < 3; j++) H.m[i][j] = FN(cdot3)(&C.m[0][i], 3, &R.m[0][j], 3);
+    FN(fill_row3)(&H);
     for (int i = 0; i < 3; i++)
-        for (int j = 0; j < 3; j++) Q.m[i][j] = FN(cdot3)(&R.m[0][i], 3, &C.m[0][j], 3);
-    return Q;
+        for (int j = 0; j < 3; j++) {
+            T.m[i][j].re = H.m[j][i].re;
+            T.m[i][j].im = -H.m[j][i].im;
+        }
+    return T;
 }
 static M3 FN(add3)(const M3 *a, const M3 *b)
 {

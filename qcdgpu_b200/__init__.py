@@ -21,6 +21,7 @@ PRNG_RANLUX, PRNG_PHILOX = 0, 1
 LAYOUT_REFERENCE = 0
 HEATBATH, OVERRELAX = 0, 1
 MEAS_PLAQUETTE, MEAS_ACTION, MEAS_POLYAKOV, MEAS_WILSON = 0, 1, 2, 3
+TUNE_SHAPES = 5                     # QG_TUNE_SHAPES
 
 EXPORTED_SYMBOLS = (
     "qg_default_config", "qg_create", "qg_destroy", "qg_last_error", "qg_get_info", "qg_sync",
@@ -28,6 +29,7 @@ EXPORTED_SYMBOLS = (
     "qg_phase", "qg_sweep", "qg_reunitarize", "qg_measure", "qg_measure_wilson",
     "qg_links_upload", "qg_links_download", "qg_set_phase_counter", "qg_glibc_seeds", "qg_set_params", "qg_get_stream",
     "qg_default_run_options", "qg_parse_init_file", "qg_run", "qg_tune", "qg_plaquette_noalloc",
+    "qg_set_shapes", "qg_get_shapes",
 )
 
 
@@ -146,6 +148,8 @@ def load_library(path=LIB_PATH):
     lib.qg_set_params.argtypes = [vp, ctypes.c_double, ctypes.c_double, ctypes.c_double]
     lib.qg_get_stream.argtypes = [vp, P(vp)]
     lib.qg_tune.argtypes = [vp, ctypes.c_int, P(ctypes.c_float)]
+    lib.qg_set_shapes.argtypes = [vp, ctypes.c_int, ctypes.c_int]
+    lib.qg_get_shapes.argtypes = [vp, P(ctypes.c_int), P(ctypes.c_int)]
     lib.qg_plaquette_noalloc.argtypes = [vp, ctypes.c_int, ctypes.c_int, P(ctypes.c_int), ctypes.c_uint32,
                                          ctypes.c_double, vp, vp]
     lib.qg_default_run_options.argtypes = [P(RunOptions)]
@@ -278,9 +282,18 @@ class Lattice:
     def tune(self, reps=4):
         """Pick the fastest phase-kernel launch shapes on this lattice; returns
         the measured ms per launch as [(heatbath, overrelaxation)] per shape."""
-        t = (ctypes.c_float * 6)()
+        t = (ctypes.c_float * (2 * TUNE_SHAPES))()
         self._ck(self.lib.qg_tune(self.ctx, reps, t), "qg_tune")
-        return [(t[2 * v], t[2 * v + 1]) for v in range(3)]
+        return [(t[2 * v], t[2 * v + 1]) for v in range(TUNE_SHAPES)]
+
+    def set_shapes(self, heatbath, overrelax):
+        """Pin the phase-kernel launch shapes (0 .. TUNE_SHAPES-1)."""
+        self._ck(self.lib.qg_set_shapes(self.ctx, heatbath, overrelax), "qg_set_shapes")
+
+    def shapes(self):
+        h, o = ctypes.c_int(), ctypes.c_int()
+        self._ck(self.lib.qg_get_shapes(self.ctx, ctypes.byref(h), ctypes.byref(o)), "qg_get_shapes")
+        return h.value, o.value
 
     def sync(self):
         self._ck(self.lib.qg_sync(self.ctx), "qg_sync")

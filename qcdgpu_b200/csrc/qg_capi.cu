@@ -456,6 +456,26 @@ extern "C" int qg_tune(qg_ctx *c, int reps, float *times_ms)
     return QG_OK;
 }
 
+extern "C" int qg_set_shapes(qg_ctx *c, int heatbath_shape, int overrelax_shape)
+{
+    if (!c) return QG_ERR_ARG;
+    if (heatbath_shape < 0 || heatbath_shape >= kPhaseVariants || overrelax_shape < 0 ||
+        overrelax_shape >= kPhaseVariants)
+        return fail(c, QG_ERR_ARG, "launch shape out of range [0, QG_TUNE_SHAPES)");
+    c->variant_hb = heatbath_shape;
+    c->variant_or = overrelax_shape;
+    destroy_graphs(c);
+    return QG_OK;
+}
+
+extern "C" int qg_get_shapes(qg_ctx *c, int *heatbath_shape, int *overrelax_shape)
+{
+    if (!c || !heatbath_shape || !overrelax_shape) return QG_ERR_ARG;
+    *heatbath_shape = c->variant_hb;
+    *overrelax_shape = c->variant_or;
+    return QG_OK;
+}
+
 extern "C" int qg_reunitarize(qg_ctx *c, int fp64)
 {
     if (!c) return QG_ERR_ARG;

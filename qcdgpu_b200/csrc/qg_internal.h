@@ -22,9 +22,9 @@ struct PhaseArgs {
     uint2 key;               // Philox key
     const uint64_t *phase_base;  // device counter (graph-replayable)
     uint32_t phase_offset;       // added to *phase_base
-    int variant;                 // launch shape: 0 compiler registers, 1 >=5, 2 >=6 blocks/SM
+    int variant;                 // launch shape, 0 .. kPhaseVariants-1 (launch_phase_T)
 };
-constexpr int kPhaseVariants = 3;
+constexpr int kPhaseVariants = QG_TUNE_SHAPES;
 
 // launchers (return cudaError_t of the launch)
 cudaError_t launch_phase_f32(const Geom &G, void *links, int group, const PhaseArgs &a, cudaStream_t s);

@@ -213,39 +213,46 @@ __device__ __forceinline__ G3<Real> compress(const M3<Real> &a)
 }
 
 // staple term U_a U_b^+ U_c^+ (lattice_staple_hermitian3, su3_update_cl.cl:294-307):
-// rows 1,2 of P = A B^+, row 3 of P by reconstruction, then P C^+
+// rows 1,2 of P = A B^+, rows 1,2 of T = P C^+, row 3 of T by reconstruction
+// (T is in SU(3)); row 3 of A is never formed
 template <typename Real>
 __device__ __forceinline__ M3<Real> staple_fwd3(const G3<Real> &ga, const G3<Real> &gb, const G3<Real> &gc)
 {
-    M3<Real> A = expand(ga), B = expand(gb), C = expand(gc), P, Q;
+    M3<Real> A = expand(ga), B = expand(gb), C = expand(gc), P, T;
 #pragma unroll
     for (int i = 0; i < 2; i++)
 #pragma unroll
         for (int j = 0; j < 3; j++) P.m[i][j] = dotc3(&A.m[i][0], 1, &B.m[j][0], 1);
-    fill_row3(P);
 #pragma unroll
-    for (int i = 0; i < 3; i++)
+    for (int i = 0; i < 2; i++)
 #pragma unroll
-        for (int j = 0; j < 3; j++) Q.m[i][j] = dotc3(&P.m[i][0], 1, &C.m[j][0], 1);
-    return Q;
+        for (int j = 0; j < 3; j++) T.m[i][j] = dotc3(&P.m[i][0], 1, &C.m[j][0], 1);
+    fill_row3(T);
+    return T;
 }
 // staple term U_a^+ U_b^+ U_c (lattice_staple_hermitian_backward3,
-// su3_update_cl.cl:324-338): rows 1,2 of R = B A, row 3 by reconstruction,
-// then R^+ C
+// su3_update_cl.cl:324-338) as the adjoint of H = C^+ R, R = B A: rows 1,2
+// of R, row 3 of R by reconstruction, rows 1,2 of H, row 3 of H by
+// reconstruction, T = H^+
 template <typename Real>
 __device__ __forceinline__ M3<Real> staple_bwd3(const G3<Real> &ga, const G3<Real> &gb, const G3<Real> &gc)
 {
-    M3<Real> A = expand(ga), B = expand(gb), C = expand(gc), R, Q;
+    M3<Real> A = expand(ga), B = expand(gb), C = expand(gc), R, H, T;
 #pragma unroll
     for (int i = 0; i < 2; i++)
 #pragma unroll
         for (int j = 0; j < 3; j++) R.m[i][j] = dot3(&B.m[i][0], 1, &A.m[0][j], 3);
     fill_row3(R);
 #pragma unroll
+    for (int i = 0; i < 2; i++)
+#pragma unroll
+        for (int j = 0; j < 3; j++) H.m[i][j] = cdot3(&C.m[0][i], 3, &R.m[0][j], 3);
+    fill_row3(H);
+#pragma unroll
     for (int i = 0; i < 3; i++)
 #pragma unroll
-        for (int j = 0; j < 3; j++) Q.m[i][j] = cdot3(&R.m[0][i], 3, &C.m[0][j], 3);
-    return Q;
+        for (int j = 0; j < 3; j++) T.m[i][j] = { H.m[j][i].re, -H.m[j][i].im };
+    return T;
 }
 
 template <typename Real>
@@ -490,23 +497,62 @@ __device__ __forceinline__ void rotate_rows(M3<Real> &U, int i, int j, const S2<
 // (lattice_heatbath3, su3_update_cl.cl:672-779): for each subgroup the 2x2
 // block of W = U staple, a Kennedy-Pendleton draw (or the reflection when
 // OR), and the rotation of the two rows of U; then Gram-Schmidt.
-template <typename Real, bool OR, class Prn>
+// LOOP runs the three subgroups as a runtime loop (rows and columns picked
+// by selects) so that the heatbath draw's code appears once; the
+// arithmetic is the unrolled form's.
+template <typename Real>
+__device__ __forceinline__ CX<Real> pick3(const CX<Real> &a, const CX<Real> &b, const CX<Real> &c, int k)
+{
+    return k == 0 ? a : (k == 1 ? b : c);
+}
+
+template <typename Real, bool OR, class Prn, bool LOOP = false>
 __device__ __forceinline__ G3<Real> cm3(const M3<Real> &S, const G3<Real> &m0, Real beta, Prn &prn, int nhit,
                                         int nhitpar)
 {
     G3<Real> reslt = m0;
     M3<Real> U = expand(m0);
     for (int n = 0; n < nhitpar; n++) {
+        if constexpr (LOOP) {
+#pragma unroll 1
+            for (int sg = 0; sg < 3; sg++) {
+                const int i = (sg == 2) ? 1 : 0, j = (sg == 0) ? 1 : 2;
+                CX<Real> ri[3], rj[3], ci[3], cj[3];
 #pragma unroll
-        for (int sg = 0; sg < 3; sg++) {
-            const int i = (sg == 2) ? 1 : 0, j = (sg == 0) ? 1 : 2;
-            S2<Real> r0;
-            r0.u1 = dot3(&U.m[i][0], 1, &S.m[0][i], 3);
-            r0.u2 = dot3(&U.m[i][0], 1, &S.m[0][j], 3);
-            r0.v1 = dot3(&U.m[j][0], 1, &S.m[0][i], 3);
-            r0.v2 = dot3(&U.m[j][0], 1, &S.m[0][j], 3);
-            if (OR) or_step(r0); else kp_step<Real, true>(r0, beta, prn, nhit);
-            rotate_rows(U, i, j, r0);
+                for (int k = 0; k < 3; k++) {
+                    ri[k] = pick3(U.m[0][k], U.m[1][k], U.m[2][k], i);
+                    rj[k] = pick3(U.m[0][k], U.m[1][k], U.m[2][k], j);
+                    ci[k] = pick3(S.m[k][0], S.m[k][1], S.m[k][2], i);
+                    cj[k] = pick3(S.m[k][0], S.m[k][1], S.m[k][2], j);
+                }
+                S2<Real> r0;
+                r0.u1 = dot3(ri, 1, ci, 1);
+                r0.u2 = dot3(ri, 1, cj, 1);
+                r0.v1 = dot3(rj, 1, ci, 1);
+                r0.v2 = dot3(rj, 1, cj, 1);
+                if (OR) or_step(r0); else kp_step<Real, true>(r0, beta, prn, nhit);
+                M3<Real> R;
+#pragma unroll
+                for (int k = 0; k < 3; k++) { R.m[0][k] = ri[k]; R.m[1][k] = rj[k]; }
+                rotate_rows(R, 0, 1, r0);
+#pragma unroll
+                for (int k = 0; k < 3; k++) {
+                    if (i == 0) U.m[0][k] = R.m[0][k]; else U.m[1][k] = R.m[0][k];
+                    if (j == 1) U.m[1][k] = R.m[1][k]; else U.m[2][k] = R.m[1][k];
+                }
+            }
+        } else {
+#pragma unroll
+            for (int sg = 0; sg < 3; sg++) {
+                const int i = (sg == 2) ? 1 : 0, j = (sg == 0) ? 1 : 2;
+                S2<Real> r0;
+                r0.u1 = dot3(&U.m[i][0], 1, &S.m[0][i], 3);
+                r0.u2 = dot3(&U.m[i][0], 1, &S.m[0][j], 3);
+                r0.v1 = dot3(&U.m[j][0], 1, &S.m[0][i], 3);
+                r0.v2 = dot3(&U.m[j][0], 1, &S.m[0][j], 3);
+                if (OR) or_step(r0); else kp_step<Real, true>(r0, beta, prn, nhit);
+                rotate_rows(U, i, j, r0);
+            }
         }
         reslt = gs3<Real>(compress(U));
         U = expand(reslt);

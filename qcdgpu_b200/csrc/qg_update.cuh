@@ -127,6 +127,111 @@ __device__ __forceinline__ S2<Real> staple2(const Field<Real> &U, const Geom &G,
     return st;
 }
 
+// ------------------------------------------ staple links through shared memory
+// The staged form of staple3 (SU(3), FP32 links): each staple term's three
+// links (nine 16-byte plane entries per thread) are copied global -> shared
+// with cp.async two terms ahead of their use, so a warp keeps the next
+// term's loads in flight while it multiplies the current one instead of
+// holding them in registers.  A thread only reads back what it copied
+// itself, so no block barrier is needed; the arithmetic is staple3's.
+constexpr int kPhaseBlock = 128;
+
+__device__ __forceinline__ void cp_async16(void *smem, const void *gmem)
+{
+    const uint32_t s = (uint32_t)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
+
+// slots of 16 bytes x kPhaseBlock threads: two term buffers of 9 slots
+// (3 links x 3 planes) and 3 slots for the updated link itself
+constexpr int kTermSlots = 9, kOwnSlot = 2 * kTermSlots, kStageSlots = 2 * kTermSlots + 3;
+using StageBuf = float4[kStageSlots][kPhaseBlock];
+
+__device__ __forceinline__ void stage_link(const Field<float> &U, int dir, uint32_t e, StageBuf &sb, int slot)
+{
+#pragma unroll
+    for (int c = 0; c < 3; c++) cp_async16(&sb[slot + c][threadIdx.x], U.p + (size_t)(dir + 4 * c) * U.pstride + e);
+}
+__device__ __forceinline__ G3<float> unstage_link(const StageBuf &sb, int slot)
+{
+    G3<float> m;
+    float4 a = sb[slot][threadIdx.x], b = sb[slot + 1][threadIdx.x], d = sb[slot + 2][threadIdx.x];
+    m.uv1 = { a.x, a.y, a.z, a.w };
+    m.uv2 = { b.x, b.y, b.z, b.w };
+    m.uv3 = { d.x, d.y, d.z, d.w };
+    return m;
+}
+
+// the plane-nu neighbour offsets for a runtime nu (selects, no local memory)
+__device__ __forceinline__ int32_t pick4(const int32_t (&a)[4], int k)
+{
+    return k == 0 ? a[0] : k == 1 ? a[1] : k == 2 ? a[2] : a[3];
+}
+
+// staple3 with staged loads, as a loop over the three planes (one copy of
+// the forward and backward term code, so the kernel's instruction stream
+// stays small); also brings in the updated link U_mu(x).  Term buffer 0
+// holds the forward term of the plane, buffer 1 the backward term; the
+// next plane's copies are issued as soon as a buffer has been read.
+// Every iteration commits one group per buffer (empty on the last plane)
+// so that wait_group 1 always means "this buffer has landed".
+template <int mu>
+__device__ __forceinline__ M3<float> staple3_staged(const Field<float> &U, const Geom &G, uint32_t t, const Nbr &n,
+                                                   int p, const Twist<float> &tw, StageBuf &sb, G3<float> &m0)
+{
+    const uint32_t own = (uint32_t)p * G.cb + t, opp = (uint32_t)(p ^ 1) * G.cb + t;
+    const int xmu = (mu == 0) ? n.xp : n.x;
+    auto fwd_copy = [&](int nu) {
+        stage_link(U, nu, opp + n.dp[mu], sb, 0);
+        stage_link(U, mu, opp + pick4(n.dp, nu), sb, 3);
+        stage_link(U, nu, own, sb, 6);
+    };
+    auto bwd_copy = [&](int nu) {
+        const int32_t dmn = pick4(n.dm, nu);
+        stage_link(U, nu, own + dmn + n.dp[mu], sb, kTermSlots);
+        stage_link(U, mu, opp + dmn, sb, kTermSlots + 3);
+        stage_link(U, nu, opp + dmn, sb, kTermSlots + 6);
+    };
+    auto get = [&](int slot, int dir, int xc) {
+        G3<float> m = unstage_link(sb, slot);
+        if (tw.on && dir == 1 && xc == tw.xlast) m = twist3(m, tw.phi, tw.omega);
+        return m;
+    };
+    stage_link(U, mu, own, sb, kOwnSlot);
+    fwd_copy(nu_of(mu, 0));
+    cp_async_commit();
+    bwd_copy(nu_of(mu, 0));
+    cp_async_commit();
+    M3<float> st, s2;
+#pragma unroll 1
+    for (int i = 0; i < 3; i++) {
+        const int nu = nu_of(mu, i);
+        const int xnp = (nu == 0) ? n.xp : n.x, xnm = (nu == 0) ? n.xm : n.x;
+        const int xnmmu = (nu == 0) ? n.xm : xmu;
+        cp_async_wait<1>();
+        M3<float> fw = staple_fwd3(get(0, nu, xmu), get(3, mu, xnp), get(6, nu, n.x));
+        if (i < 2) fwd_copy(nu_of(mu, i + 1));
+        cp_async_commit();
+        cp_async_wait<1>();
+        M3<float> bw = staple_bwd3(get(kTermSlots, nu, xnmmu), get(kTermSlots + 3, mu, xnm),
+                                   get(kTermSlots + 6, nu, xnm));
+        if (i < 2) bwd_copy(nu_of(mu, i + 1));
+        cp_async_commit();
+        if (i == 0) {
+            add3(st, fw, bw);
+        } else {
+            add3(s2, st, fw);
+            add3(st, bw, s2);
+        }
+    }
+    cp_async_wait<0>();
+    m0 = unstage_link(sb, kOwnSlot);
+    return st;
+}
+
 // PRN source of thread t (PMODE 0 = RANLUX buffer, 1 = Philox, 2 = gid)
 template <typename Real, int PMODE> struct PrnOf;
 template <typename Real> struct PrnOf<Real, 0> {
@@ -153,8 +258,9 @@ template <typename Real> struct PrnOf<Real, 2> {
 
 // MINB: minimum resident blocks of 128 threads per SM asked of the
 // compiler (0 = its own register choice); the launch shapes the tuner picks
-template <int NC, typename Real, int PMODE, bool OR, int mu, int MINB>
-__global__ void __launch_bounds__(128, MINB) k_phase(Field<Real> U, Geom G, PhaseArgs A)
+// STAGED: staple links through shared memory (staple3_staged; SU(3) FP32)
+template <int NC, typename Real, int PMODE, bool OR, int mu, int MINB, bool STAGED>
+__global__ void __launch_bounds__(kPhaseBlock, MINB) k_phase(Field<Real> U, Geom G, PhaseArgs A)
 {
     const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= G.half) return;
@@ -172,10 +278,17 @@ __global__ void __launch_bounds__(128, MINB) k_phase(Field<Real> U, Geom G, Phas
     const uint64_t phase = (PMODE == 1) ? (*A.phase_base + A.phase_offset) : 0;
     auto prn = PrnOf<Real, PMODE>::make(A, t, site, phase, G);
     if (NC == 3) {
-        G3<Real> m0 = U.ld3(mu, e0);
+        G3<Real> m0;
+        M3<Real> st;
+        if constexpr (STAGED) {
+            __shared__ __align__(16) StageBuf sb;
+            st = staple3_staged<mu>(U, G, t, nb, p, tw, sb, m0);
+        } else {
+            m0 = U.ld3(mu, e0);
+            st = staple3<mu>(U, G, t, nb, p, tw);
+        }
         if (tw.on && mu == 1 && c.x == tw.xlast) m0 = twist3(m0, tw.phi, tw.omega);
-        M3<Real> st = staple3<mu>(U, G, t, nb, p, tw);
-        G3<Real> mU = cm3<Real, OR>(st, m0, beta, prn, A.nhit, A.nhitpar);
+        G3<Real> mU = cm3<Real, OR, decltype(prn), STAGED && !OR>(st, m0, beta, prn, A.nhit, A.nhitpar);
         U.st3(mu, e0, mU);
     } else {
         R4<Real> m0 = U.ld2(mu, e0);
@@ -208,15 +321,20 @@ cudaError_t launch_phase_T(const Geom &G, void *links, int group, const PhaseArg
     Field<Real> U;
     U.p = reinterpret_cast<typename V4<Real>::T *>(links);
     U.pstride = G.pstride;
-    const int bs = 128;
+    const int bs = kPhaseBlock;
     const unsigned nb = (G.half + bs - 1) / bs;
     const int pm = a.prn_mode;   // -1 selects overrelaxation (no PRNs)
-#define QG_LAUNCH2(NC, PM, OR, MU, MB) k_phase<NC, Real, PM, OR, MU, MB><<<nb, bs, 0, s>>>(U, G, a)
-#define QG_LAUNCH1(NC, PM, OR, MU)                                \
-    do {                                                          \
-        if (a.variant == 1) QG_LAUNCH2(NC, PM, OR, MU, 5);        \
-        else if (a.variant == 2) QG_LAUNCH2(NC, PM, OR, MU, 6);   \
-        else QG_LAUNCH2(NC, PM, OR, MU, 0);                       \
+    // shapes 3, 4 stage the staple through shared memory where that form
+    // exists (SU(3), FP32 links); elsewhere they run shapes 0, 1
+    constexpr bool kStage = sizeof(Real) == 4;
+#define QG_LAUNCH2(NC, PM, OR, MU, MB, ST) k_phase<NC, Real, PM, OR, MU, MB, ST><<<nb, bs, 0, s>>>(U, G, a)
+#define QG_LAUNCH1(NC, PM, OR, MU)                                                  \
+    do {                                                                            \
+        if (a.variant == 1) QG_LAUNCH2(NC, PM, OR, MU, 5, false);                   \
+        else if (a.variant == 2) QG_LAUNCH2(NC, PM, OR, MU, 6, false);              \
+        else if (a.variant == 3) QG_LAUNCH2(NC, PM, OR, MU, 0, NC == 3 && kStage);  \
+        else if (a.variant == 4) QG_LAUNCH2(NC, PM, OR, MU, 5, NC == 3 && kStage);  \
+        else QG_LAUNCH2(NC, PM, OR, MU, 0, false);                                  \
     } while (0)
 #define QG_LAUNCH(NC, PM, OR)                                     \
     do {                                                          \

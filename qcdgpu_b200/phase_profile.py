@@ -2,11 +2,13 @@
 
   python -m qcdgpu_b200.phase_profile [--size 32] [--precision 0] [--group 3]
                                       [--prng philox|ranlux] [--warm 2] [--phases 1]
+                                      [--shape S]
 
 Cold start, `warm` heatbath sweeps (8 heatbath phase launches each, so a
 profiler skips 8*warm + 1 kernel launches to reach the measured ones), then
 `phases` heatbath phase launches followed by `phases` overrelaxation phase
-launches (odd X first), then a synchronise.
+launches (odd X first), then a synchronise.  --shape pins the launch
+shape of both kinds (0 .. QG_TUNE_SHAPES-1) before the warm-up sweeps.
 """
 import argparse
 
@@ -21,11 +23,13 @@ def main():
     ap.add_argument("--prng", default="philox", choices=["philox", "ranlux"])
     ap.add_argument("--warm", type=int, default=2)
     ap.add_argument("--phases", type=int, default=1)
+    ap.add_argument("--shape", type=int, default=0)
     a = ap.parse_args()
     cfg = Q.default_config(group=a.group, size=a.size, precision=a.precision, start=Q.START_COLD,
                            prng=Q.PRNG_PHILOX if a.prng == "philox" else Q.PRNG_RANLUX, beta=6.0, n_or=0,
                            reunit_every=0)
     L = Q.Lattice(cfg)
+    L.set_shapes(a.shape, a.shape)
     L.seed()
     L.init()
     L.sweep(a.warm)

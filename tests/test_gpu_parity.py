@@ -344,10 +344,42 @@ def test_tune_restores_field_and_keeps_results():
         before = L.download()
         if tune:
             t = L.tune(reps=2)
-            assert len(t) == 3 and all(a > 0 and b > 0 for a, b in t)
+            assert len(t) == Q.TUNE_SHAPES and all(a > 0 and b > 0 for a, b in t)
             assert np.array_equal(L.download(), before)
             assert L.info().phase_counter == 8
         L.sweep(2)
         outs.append(L.download())
         L.close()
     assert np.array_equal(outs[0], outs[1])
+
+
+@pytest.mark.parametrize("group,precision,prng", [(3, 0, Q.PRNG_PHILOX), (3, 0, Q.PRNG_RANLUX), (3, 1, Q.PRNG_PHILOX),
+                                                  (2, 0, Q.PRNG_PHILOX), (2, 1, Q.PRNG_RANLUX)])
+def test_every_launch_shape_gives_the_same_chain(group, precision, prng):
+    """Each launch shape (registers, register caps, staple staged through
+    shared memory) performs the same operation sequence: heatbath and
+    overrelaxation sweeps from a hot start agree bit for bit."""
+    dims = (6, 4, 4, 8)
+    outs = []
+    for shape in range(Q.TUNE_SHAPES):
+        L = Q.Lattice(Q.default_config(group=group, size=dims, precision=precision, start=Q.START_HOT, prng=prng,
+                                       beta=5.9 if group == 3 else 2.3, prng_instances=INSTANCES, randseries=54,
+                                       n_or=2, reunit_every=2))
+        L.set_shapes(shape, shape)
+        assert L.shapes() == (shape, shape)
+        L.seed(54)
+        L.init()
+        L.sweep(2)
+        outs.append(L.download())
+        L.close()
+    for k in range(1, len(outs)):
+        assert np.array_equal(outs[0], outs[k]), "shape %d differs from shape 0" % k
+
+
+def test_set_shapes_rejects_out_of_range():
+    L = Q.Lattice(Q.default_config(group=3, size=(4, 4, 4, 4), precision=0, start=Q.START_COLD))
+    with pytest.raises(Q.QGError):
+        L.set_shapes(Q.TUNE_SHAPES, 0)
+    with pytest.raises(Q.QGError):
+        L.set_shapes(0, -1)
+    L.close()
