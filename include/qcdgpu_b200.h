@@ -93,6 +93,7 @@ typedef struct qg_info {
     uint64_t prn_quads;   /* float4 in one RANLUX batch                      */
     uint64_t phase_counter;/* Philox phase counter (next phase)              */
     uint32_t prng_counter;/* RANLUX batches produced (PRNG_counter)          */
+    uint64_t sweeps_done; /* sweeps since the start (reunitarisation cadence)*/
 } qg_info;
 
 /* defaults of the reference main() where it has one (QCDGPU.cpp:98-220) */
@@ -104,6 +105,9 @@ int qg_create(const qg_config *cfg, qg_ctx **out);
 int qg_destroy(qg_ctx *ctx);
 const char *qg_last_error(const qg_ctx *ctx);  /* ctx may be NULL (last create error) */
 int qg_get_info(qg_ctx *ctx, qg_info *info);
+/* the context's configuration: as created, with beta/phi/omega as last set
+ * by qg_set_params                                                        */
+int qg_get_config(qg_ctx *ctx, qg_config *cfg);
 int qg_sync(qg_ctx *ctx);
 
 /* PRNG::initialize (random.cpp:216-277): glibc srand(series) seeding of all
@@ -176,6 +180,9 @@ int qg_get_stream(qg_ctx *ctx, void **stream);
 
 /* Philox phase counter (fast mode): read / set for checkpoint and resume */
 int qg_set_phase_counter(qg_ctx *ctx, uint64_t counter);
+/* sweeps counted for the reunitarisation cadence (qg_info.sweeps_done):
+ * set on resume so that the global Gram-Schmidt falls on the same sweeps */
+int qg_set_sweeps_done(qg_ctx *ctx, uint64_t sweeps);
 
 /* Allocation-free plaquette/action sums.  No counterpart in the reference:
  * it exists for callers that may not allocate device memory at the call
@@ -231,6 +238,13 @@ typedef struct qg_run_options {
     int quiet;             /* no console output                                        */
     char output_path[512]; /* OUTPUTPATH (directory prefix of the results file)        */
     char prefix[32];       /* file prefix, "su3-" / "su2-"                              */
+    int init;              /* INIT: 1 start from cfg.start, 0 continue from state_file  */
+    char state_file[512];  /* STATEFILE: .qcg read when init == 0                       */
+    int save_state;        /* SAVESTATE: 1 write a .qcg after the start measurement and */
+                           /* at the end, as lattice_simulate does                      */
+    int save_every_iter;   /* SAVEEVERY: also after every n-th measured iteration (0 off)*/
+    char state_out[512];   /* STATEOUT: .qcg path written (empty: OUTPUTPATH + prefix + */
+                           /* the reference's date-stamped name)                       */
 } qg_run_options;
 
 typedef struct qg_run_result {
@@ -243,6 +257,12 @@ typedef struct qg_run_result {
     double seconds;                  /* wall time of the update + measure loop     */
     double link_updates_per_second;
     char results_file[640];
+    /* new: integrated autocorrelation time of each series over samples
+     * 1..ITER-1 (Madras-Sokal window, c = 6) and the error of its mean,
+     * sqrt(2 tau_int variance / n); the reference reports neither        */
+    double tau_int[QG_OBS_COUNT];
+    double error[QG_OBS_COUNT];
+    char state_file[640];            /* last .qcg written ("" if none)             */
 } qg_run_result;
 
 /* defaults of the reference main() (QCDGPU.cpp:183-205) */
@@ -251,13 +271,71 @@ int qg_default_run_options(qg_run_options *opts);
  * keys onto cfg / opts as lattice_get_init_file does.  Keys: GROUP ND L1..L4
  * LS LT ITER NITER NAV NHIT BETA PHI OMEGA INTS RANDSERIES PRNG OUTPUTPATH
  * GETWILSON GETRETRACE PL_LEVEL WILSONR WILSONT (reference) and PRECISION
- * NHITPAR NOR REUNIT_EVERY REUNIT_FP64 PRNG_INSTANCES ROW_ALIGN (this build);
+ * NHITPAR NOR REUNIT_EVERY REUNIT_FP64 PRNG_INSTANCES ROW_ALIGN INIT
+ * STATEFILE SAVESTATE SAVEEVERY STATEOUT (this build; the reference sets
+ * INIT and the state file name in main());
  * PLATFORM DEVICE FINISHPATH TURNOFFWAITING REBUILDBINARY and the F_munu
  * keys are accepted and ignored.  Unknown generators are an error.        */
 int qg_parse_init_file(const char *path, qg_config *cfg, qg_run_options *opts);
 /* lattice_init + lattice_simulate + LatticeCheckCPU + lattice_analysis +
- * lattice_write_results on the current CUDA device.                       */
+ * lattice_write_results on the current CUDA device.  With opts->init == 0
+ * the run continues from opts->state_file: the file's header replaces the
+ * lattice, coupling, PRNG and cadence settings of cfg/opts (as
+ * lattice_load_bin_header does), the link table and the measured series
+ * are restored, the RANLUX stream is replayed to the saved PRNG_counter
+ * (suncl.cpp:5349-5354) or the Philox phase counter is set, and the
+ * thermalisation and measurement loops resume at NAV_counter and
+ * ITER_counter.                                                           */
 int qg_run(const qg_config *cfg, const qg_run_options *opts, qg_run_result *res);
+
+/* ----------------------------------------------------------------------- */
+/* Lattice state files (.qcg): model::lattice_save_state / lattice_load_state
+ * / lattice_make_bin_header / lattice_load_bin_header (suncl.cpp:1857-2079).
+ * Layout: a header of 64 uint32 (QCDGPU_STATE_HEADER_WORDS), then
+ * lattice_measurement (double2 x header[32]), lattice_energies (double2 x
+ * header[33]: S_spat, S_temp sums per iteration), lattice_energies_plq
+ * (double2 x header[34]: ReTr spatial, temporal sums) if header[30],
+ * lattice_wilson_loop (double x header[33]) if header[31],
+ * lattice_polyakov_loop (double2 x header[35]: Re, Im sums) if header[25],
+ * then the link table in the reference layout (float4 / double4).  Words
+ * 48-59 of the header and a tagged block after the link table (|P|^2,
+ * |P|^4 sums) are this build's additions; the reference's loader does not
+ * read them.                                                              */
+#define QCDGPU_STATE_HEADER_WORDS 64
+typedef struct qg_run_state {
+    int init;               /* INIT of the run that wrote the file           */
+    int nav, nav_counter;   /* NAV, thermalisation sweeps done               */
+    int niter, iter, iter_counter; /* NITER, ITER, measured iterations done  */
+    int pl_level, get_actions, get_plaquettes, get_wilson;
+    uint32_t prng_counter;  /* RANLUX batches produced (PRNG_counter)        */
+    uint64_t phase_counter; /* Philox phase counter                          */
+    uint64_t sweeps_done;   /* sweeps since the start                        */
+    /* measured series as raw lattice sums, `iter` entries each (the first
+     * iter_counter used); NULL when absent / not wanted                     */
+    double *actions;        /* 2 per iteration: S_spat, S_temp               */
+    double *plaquettes;     /* 2 per iteration: ReTr spatial, temporal       */
+    double *wilson;         /* 1 per iteration                               */
+    double *polyakov;       /* 4 per iteration: Re P, Im P, |P|^2, |P|^4     */
+} qg_run_state;
+/* Host only: write a state file from a reference-layout link table
+ * (links_bytes = qg_info.ref_elems * sizeof(Real)).                       */
+int qg_write_state_file(const char *path, const qg_config *cfg, const qg_run_state *st, const void *links_ref,
+                        uint64_t links_bytes);
+/* Host only: read a state file's header into cfg and st (settings and
+ * counters; the series pointers are left alone), and, where st's series
+ * pointers and links_ref are non-NULL, the series and the link table.
+ * Errors: wrong magic/version, truncated file, size mismatch.             */
+int qg_read_state_file(const char *path, qg_config *cfg, qg_run_state *st, void *links_ref,
+                       uint64_t links_bytes);
+/* the context's link table and counters into a state file                 */
+int qg_save_state(qg_ctx *ctx, const char *path, const qg_run_state *st);
+
+/* Host only, new: integrated autocorrelation time of x[0..n-1],
+ * tau = 1/2 + sum_{t=1..W} rho(t) with the smallest window W >= c tau(W)
+ * (Madras & Sokal 1988, automatic windowing; c = 6 is customary).
+ * Returns tau in *tau and W in *window; n < 2 or zero variance gives
+ * tau = 0.5, W = 0.                                                       */
+int qg_tau_int(const double *x, int n, double c, double *tau, int *window);
 
 #ifdef __cplusplus
 }

@@ -29,7 +29,8 @@ EXPORTED_SYMBOLS = (
     "qg_phase", "qg_sweep", "qg_reunitarize", "qg_measure", "qg_measure_wilson",
     "qg_links_upload", "qg_links_download", "qg_set_phase_counter", "qg_glibc_seeds", "qg_set_params", "qg_get_stream",
     "qg_default_run_options", "qg_parse_init_file", "qg_run", "qg_tune", "qg_plaquette_noalloc",
-    "qg_set_shapes", "qg_get_shapes",
+    "qg_set_shapes", "qg_get_shapes", "qg_get_config", "qg_set_sweeps_done",
+    "qg_write_state_file", "qg_read_state_file", "qg_save_state", "qg_tau_int",
 )
 
 
@@ -68,6 +69,7 @@ class Info(ctypes.Structure):
         ("prn_quads", ctypes.c_uint64),
         ("phase_counter", ctypes.c_uint64),
         ("prng_counter", ctypes.c_uint32),
+        ("sweeps_done", ctypes.c_uint64),
     ]
 
 
@@ -89,6 +91,11 @@ class RunOptions(ctypes.Structure):
         ("quiet", ctypes.c_int),
         ("output_path", ctypes.c_char * 512),
         ("prefix", ctypes.c_char * 32),
+        ("init", ctypes.c_int),
+        ("state_file", ctypes.c_char * 512),
+        ("save_state", ctypes.c_int),
+        ("save_every_iter", ctypes.c_int),
+        ("state_out", ctypes.c_char * 512),
     ]
 
 
@@ -103,6 +110,32 @@ class RunResult(ctypes.Structure):
         ("seconds", ctypes.c_double),
         ("link_updates_per_second", ctypes.c_double),
         ("results_file", ctypes.c_char * 640),
+        ("tau_int", ctypes.c_double * 11),
+        ("error", ctypes.c_double * 11),
+        ("state_file", ctypes.c_char * 640),
+    ]
+
+
+class RunState(ctypes.Structure):
+    """qg_run_state: counters of a run and its measured series (raw sums)."""
+    _fields_ = [
+        ("init", ctypes.c_int),
+        ("nav", ctypes.c_int),
+        ("nav_counter", ctypes.c_int),
+        ("niter", ctypes.c_int),
+        ("iter", ctypes.c_int),
+        ("iter_counter", ctypes.c_int),
+        ("pl_level", ctypes.c_int),
+        ("get_actions", ctypes.c_int),
+        ("get_plaquettes", ctypes.c_int),
+        ("get_wilson", ctypes.c_int),
+        ("prng_counter", ctypes.c_uint32),
+        ("phase_counter", ctypes.c_uint64),
+        ("sweeps_done", ctypes.c_uint64),
+        ("actions", ctypes.POINTER(ctypes.c_double)),
+        ("plaquettes", ctypes.POINTER(ctypes.c_double)),
+        ("wilson", ctypes.POINTER(ctypes.c_double)),
+        ("polyakov", ctypes.POINTER(ctypes.c_double)),
     ]
 
 
@@ -152,6 +185,13 @@ def load_library(path=LIB_PATH):
     lib.qg_get_shapes.argtypes = [vp, P(ctypes.c_int), P(ctypes.c_int)]
     lib.qg_plaquette_noalloc.argtypes = [vp, ctypes.c_int, ctypes.c_int, P(ctypes.c_int), ctypes.c_uint32,
                                          ctypes.c_double, vp, vp]
+    lib.qg_get_config.argtypes = [vp, P(Config)]
+    lib.qg_set_sweeps_done.argtypes = [vp, ctypes.c_uint64]
+    lib.qg_write_state_file.argtypes = [ctypes.c_char_p, P(Config), P(RunState), vp, ctypes.c_uint64]
+    lib.qg_read_state_file.argtypes = [ctypes.c_char_p, P(Config), P(RunState), vp, ctypes.c_uint64]
+    lib.qg_save_state.argtypes = [vp, ctypes.c_char_p, P(RunState)]
+    lib.qg_tau_int.argtypes = [P(ctypes.c_double), ctypes.c_int, ctypes.c_double, P(ctypes.c_double),
+                               P(ctypes.c_int)]
     lib.qg_default_run_options.argtypes = [P(RunOptions)]
     lib.qg_parse_init_file.argtypes = [ctypes.c_char_p, P(Config), P(RunOptions)]
     lib.qg_run.argtypes = [P(Config), P(RunOptions), P(RunResult)]
@@ -167,6 +207,70 @@ def glibc_seeds(randseries, n):
     if rc != QG_OK:
         raise QGError("qg_glibc_seeds failed")
     return out
+
+
+def tau_int(x, c=6.0):
+    """qg_tau_int: integrated autocorrelation time of a series (Madras-Sokal
+    automatic window, W >= c tau); returns (tau, W).  Host only."""
+    lib = load_library()
+    a = np.ascontiguousarray(x, dtype=np.float64)
+    t = ctypes.c_double()
+    w = ctypes.c_int()
+    rc = lib.qg_tau_int(a.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), len(a), c, ctypes.byref(t),
+                        ctypes.byref(w))
+    if rc != QG_OK:
+        raise QGError("qg_tau_int: " + lib.qg_last_error(None).decode())
+    return t.value, w.value
+
+
+def read_state_file(path, cfg=None):
+    """qg_read_state_file: (config, state, series dict, link table) of a .qcg
+    file; the table is the reference layout (float32 / float64).  Host only."""
+    lib = load_library()
+    cfg = cfg if cfg is not None else default_config()
+    st = RunState()
+    rc = lib.qg_read_state_file(path.encode(), ctypes.byref(cfg), ctypes.byref(st), None, 0)
+    if rc != QG_OK:
+        raise QGError("qg_read_state_file: " + lib.qg_last_error(None).decode())
+    n = max(st.iter, 1)
+    ser = {"actions": np.zeros(2 * n), "plaquettes": np.zeros(2 * n), "wilson": np.zeros(n),
+           "polyakov": np.zeros(4 * n)}
+    dp = ctypes.POINTER(ctypes.c_double)
+    for k, v in ser.items():
+        setattr(st, k, v.ctypes.data_as(dp))
+    V = cfg.size[0] * cfg.size[1] * cfg.size[2] * cfg.size[3]
+    a = cfg.row_align if cfg.row_align > 0 else 64
+    rowsize = (V + a - 1) // a * a
+    elems = (12 if cfg.group == 3 else 4) * rowsize * 4
+    table = np.zeros(elems, dtype=np.float64 if cfg.precision else np.float32)
+    rc = lib.qg_read_state_file(path.encode(), ctypes.byref(cfg), ctypes.byref(st),
+                                table.ctypes.data_as(ctypes.c_void_p), table.nbytes)
+    if rc != QG_OK:
+        raise QGError("qg_read_state_file: " + lib.qg_last_error(None).decode())
+    for k in ser:
+        setattr(st, k, None)
+    return cfg, st, ser, table
+
+
+def write_state_file(path, cfg, st, table, series=None):
+    """qg_write_state_file from host arrays (series: dict as read_state_file
+    returns; missing entries are written as zeros).  Host only."""
+    lib = load_library()
+    n = max(st.iter, 1)
+    series = dict(series or {})
+    keep = {}
+    dp = ctypes.POINTER(ctypes.c_double)
+    for k, m in (("actions", 2), ("plaquettes", 2), ("wilson", 1), ("polyakov", 4)):
+        v = np.ascontiguousarray(series.get(k, np.zeros(m * n)), dtype=np.float64)
+        keep[k] = v
+        setattr(st, k, v.ctypes.data_as(dp))
+    t = np.ascontiguousarray(table)
+    rc = lib.qg_write_state_file(path.encode(), ctypes.byref(cfg), ctypes.byref(st),
+                                 t.ctypes.data_as(ctypes.c_void_p), t.nbytes)
+    for k in keep:
+        setattr(st, k, None)
+    if rc != QG_OK:
+        raise QGError("qg_write_state_file: " + lib.qg_last_error(None).decode())
 
 
 def default_config(**kw):
@@ -193,7 +297,7 @@ def default_run_options(**kw):
     o = RunOptions()
     lib.qg_default_run_options(ctypes.byref(o))
     for k, v in kw.items():
-        if k in ("output_path", "prefix"):
+        if k in ("output_path", "prefix", "state_file", "state_out"):
             v = v.encode()
         setattr(o, k, v)
     return o

@@ -220,6 +220,7 @@ extern "C" int qg_get_info(qg_ctx *c, qg_info *info)
     info->prn_quads = (uint64_t)c->instances * c->samples;
     info->phase_counter = c->phase_counter;
     info->prng_counter = c->prng_counter;
+    info->sweeps_done = c->sweeps_done;
     return QG_OK;
 }
 
@@ -298,6 +299,20 @@ extern "C" int qg_set_phase_counter(qg_ctx *c, uint64_t v)
     QG_CK(cudaMemcpyAsync(c->d_phase, &c->phase_counter, sizeof(uint64_t), cudaMemcpyHostToDevice, c->stream),
           "phase set");
     QG_CK(cudaStreamSynchronize(c->stream), "phase set sync");
+    return QG_OK;
+}
+
+extern "C" int qg_get_config(qg_ctx *c, qg_config *cfg)
+{
+    if (!c || !cfg) return QG_ERR_ARG;
+    *cfg = c->cfg;
+    return QG_OK;
+}
+
+extern "C" int qg_set_sweeps_done(qg_ctx *c, uint64_t v)
+{
+    if (!c) return QG_ERR_ARG;
+    c->sweeps_done = v;
     return QG_OK;
 }
 

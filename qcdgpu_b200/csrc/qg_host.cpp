@@ -219,6 +219,7 @@ extern "C" int qg_default_run_options(qg_run_options *o)
     o->get_actions = 1;
     o->verify = 1;
     o->write_results = 1;
+    o->init = 1;
     snprintf(o->prefix, sizeof(o->prefix), "su3-");
     return QG_OK;
 }
@@ -286,6 +287,11 @@ extern "C" int qg_parse_init_file(const char *path, qg_config *cfg, qg_run_optio
         else if (key == "REUNIT_FP64") cfg->reunit_fp64 = (int)iv;
         else if (key == "PRNG_INSTANCES") cfg->prng_instances = (int)iv;
         else if (key == "ROW_ALIGN") cfg->row_align = (int)iv;
+        else if (key == "INIT") o->init = (int)iv;
+        else if (key == "STATEFILE") snprintf(o->state_file, sizeof(o->state_file), "%s", val.c_str());
+        else if (key == "SAVESTATE") o->save_state = (int)iv;
+        else if (key == "SAVEEVERY") o->save_every_iter = (int)iv;
+        else if (key == "STATEOUT") snprintf(o->state_out, sizeof(o->state_out), "%s", val.c_str());
         else if (key == "PLATFORM" || key == "DEVICE" || key == "FINISHPATH" || key == "TURNOFFWAITING" ||
                  key == "REBUILDBINARY" || key == "TURNOFFFMUNU" || key == "FMUNU" || key == "F0MU" ||
                  key.rfind("FMUNU", 0) == 0 || key == "N1") {
@@ -301,80 +307,184 @@ extern "C" int qg_parse_init_file(const char *path, qg_config *cfg, qg_run_optio
     return QG_OK;
 }
 
-extern "C" int qg_run(const qg_config *cfg_in, const qg_run_options *o, qg_run_result *res)
+extern "C" int qg_run(const qg_config *cfg_in, const qg_run_options *o_in, qg_run_result *res)
 {
-    if (!cfg_in || !o || !res) return host_fail(QG_ERR_ARG, "null argument");
-    if (o->iter < 1 || o->niter < 0 || o->nav < 0) return host_fail(QG_ERR_ARG, "ITER >= 1, NITER >= 0, NAV >= 0");
+    if (!cfg_in || !o_in || !res) return host_fail(QG_ERR_ARG, "null argument");
     memset(res, 0, sizeof(*res));
     res->verification_passed = -1;
     qg_config cfg = *cfg_in;
+    qg_run_options opts = *o_in;
+    const qg_run_options *o = &opts;
+    const bool resume = (opts.init == 0);
+    qg_run_state rs;
+    memset(&rs, 0, sizeof(rs));
+    int rc;
+    if (resume) {
+        // lattice_load_bin_header: the file's settings replace init.dat's
+        if (!opts.state_file[0]) return host_fail(QG_ERR_ARG, "INIT = 0 needs STATEFILE");
+        if ((rc = qg_read_state_file(opts.state_file, &cfg, &rs, nullptr, 0))) return rc;
+        opts.nav = rs.nav;
+        opts.niter = rs.niter;
+        opts.iter = rs.iter;
+        opts.pl_level = rs.pl_level;
+        opts.get_actions = rs.get_actions;
+        opts.get_plaquettes = rs.get_plaquettes;
+        opts.get_wilson = rs.get_wilson;
+    }
+    if (o->iter < 1 || o->niter < 0 || o->nav < 0) return host_fail(QG_ERR_ARG, "ITER >= 1, NITER >= 0, NAV >= 0");
+    // raw lattice sums per measured iteration, the reference's buffers
+    std::vector<double> s_act(2 * (size_t)o->iter, 0.0), s_plq(2 * (size_t)o->iter, 0.0),
+        s_wil((size_t)o->iter, 0.0), s_pol(4 * (size_t)o->iter, 0.0);
+    rs.actions = s_act.data();
+    rs.plaquettes = s_plq.data();
+    rs.wilson = s_wil.data();
+    rs.polyakov = s_pol.data();
     qg_ctx *ctx = nullptr;
-    int rc = qg_create(&cfg, &ctx);
+    rc = qg_create(&cfg, &ctx);
     if (rc) return host_fail(rc, std::string("qg_create: ") + qg_last_error(nullptr));
     auto bail = [&](int code) {
         std::string m = qg_last_error(ctx);
+        if (m.empty()) m = qg_last_error(nullptr);
         qg_destroy(ctx);
         return host_fail(code, m);
     };
-    // lattice_init: PRNG::initialize, then the start configuration
-    if ((rc = qg_prng_seed(ctx, cfg.randseries))) return bail(rc);
-    if ((rc = qg_init_links(ctx, cfg.start))) return bail(rc);
     qg_info info;
     qg_get_info(ctx, &info);
+    const size_t real = cfg.precision ? 8 : 4;
     const int N = cfg.group;
     const double V = info.sites;
     const double nsp = (double)cfg.size[0] * cfg.size[1] * cfg.size[2];
-    std::vector<double> d[QG_OBS_COUNT];
+    // lattice_init: PRNG::initialize, then the start configuration -- or
+    // the saved table, with the PRN stream brought to where it stopped
+    if ((rc = qg_prng_seed(ctx, cfg.randseries))) return bail(rc);
+    if (resume) {
+        std::vector<char> table((size_t)info.ref_elems * real);
+        if ((rc = qg_read_state_file(opts.state_file, &cfg, &rs, table.data(), (uint64_t)table.size()))) {
+            qg_destroy(ctx);
+            return rc;
+        }
+        if ((rc = qg_links_upload(ctx, table.data(), QG_LAYOUT_REFERENCE))) return bail(rc);
+        if (cfg.prng == QG_PRNG_RANLUX) {
+            for (;;) {                                  // suncl.cpp:5349-5351
+                qg_get_info(ctx, &info);
+                if (info.prng_counter >= rs.prng_counter) break;
+                if ((rc = qg_prng_produce(ctx))) return bail(rc);
+            }
+        } else if ((rc = qg_set_phase_counter(ctx, rs.phase_counter))) {
+            return bail(rc);
+        }
+        if ((rc = qg_set_sweeps_done(ctx, rs.sweeps_done))) return bail(rc);
+    } else {
+        if ((rc = qg_init_links(ctx, cfg.start))) return bail(rc);
+        rs.init = 1;
+        rs.nav = o->nav;
+        rs.niter = o->niter;
+        rs.iter = o->iter;
+        rs.pl_level = o->pl_level;
+        rs.get_actions = o->get_actions;
+        rs.get_plaquettes = o->get_plaquettes;
+        rs.get_wilson = o->get_wilson;
+    }
     time_t t_start = time(nullptr);
-    auto measure = [&]() -> int {
+    auto measure = [&](int i) -> int {
         double a[4];
         int r;
         if (o->get_plaquettes) {
             if ((r = qg_measure(ctx, QG_MEAS_PLAQUETTE, a))) return r;
-            d[QG_OBS_PLQ_SPAT].push_back(a[0] / (3 * V));
-            d[QG_OBS_PLQ_TEMP].push_back(a[1] / (3 * V));
-            d[QG_OBS_PLQ_TOTAL].push_back(0.5 * (a[0] + a[1]) / (3 * V));
+            s_plq[2 * i] = a[0]; s_plq[2 * i + 1] = a[1];
         }
         if (o->get_wilson) {
             if ((r = qg_measure(ctx, QG_MEAS_WILSON, a))) return r;
-            d[QG_OBS_WILSON].push_back(a[0] / (3 * V));
+            s_wil[i] = a[0];
         }
         if (o->get_actions) {
             if ((r = qg_measure(ctx, QG_MEAS_ACTION, a))) return r;
-            d[QG_OBS_S_SPAT].push_back(a[0] / (3 * V));
-            d[QG_OBS_S_TEMP].push_back(a[1] / (3 * V));
-            d[QG_OBS_S_TOTAL].push_back(0.5 * (a[0] + a[1]) / (3 * V));
+            s_act[2 * i] = a[0]; s_act[2 * i + 1] = a[1];
         }
         if (o->pl_level > 0) {
             if ((r = qg_measure(ctx, QG_MEAS_POLYAKOV, a))) return r;
-            d[QG_OBS_POLYAKOV].push_back(a[0] / (nsp * N));
-            d[QG_OBS_POLYAKOV_IM].push_back(a[1] / (nsp * N));
-            if (o->pl_level > 1) {
-                d[QG_OBS_POLYAKOV_P2].push_back(a[2] / (nsp * N * N));
-                d[QG_OBS_POLYAKOV_P4].push_back(a[3] / (nsp * N * N * N * N));
-            }
+            for (int k = 0; k < 4; k++) s_pol[4 * i + k] = a[k];
         }
         return QG_OK;
     };
+    // lattice_save_state: the name the reference gives it, or STATEOUT
+    auto save = [&]() -> int {
+        char name[640];
+        if (o->state_out[0]) {
+            snprintf(name, sizeof(name), "%s", o->state_out);
+        } else {
+            time_t now = time(nullptr);
+            char tb[64];
+            snprintf(tb, sizeof(tb), "%s", ctime(&now));
+            snprintf(name, sizeof(name), "%s%s%.2s-%.3s-%.2s-%.2s-%.2s-%.2s.qcg", o->output_path, o->prefix, tb + 22,
+                     tb + 4, tb + 8, tb + 11, tb + 14, tb + 17);
+        }
+        int r = qg_save_state(ctx, name, &rs);
+        if (r == QG_OK) snprintf(res->state_file, sizeof(res->state_file), "%s", name);
+        return r;
+    };
     auto t0 = std::chrono::steady_clock::now();
-    if ((rc = measure())) return bail(rc);                       // iteration 0: start configuration
-    if ((rc = qg_sweep(ctx, o->nav))) return bail(rc);           // thermalisation
-    for (int i = 1; i < o->iter; i++) {
+    if (!resume) {
+        if ((rc = measure(0))) return bail(rc);                  // iteration 0: start configuration
+        rs.iter_counter = 1;
+        if (o->save_state && (rc = save())) return bail(rc);
+    }
+    const int nav_start = rs.nav_counter;
+    if (rs.nav_counter < o->nav) {                                // thermalisation
+        if ((rc = qg_sweep(ctx, o->nav - rs.nav_counter))) return bail(rc);
+        rs.nav_counter = o->nav;
+    }
+    const int first = rs.iter_counter;
+    for (int i = first; i < o->iter; i++) {
         if ((rc = qg_sweep(ctx, o->niter))) return bail(rc);
-        if ((rc = measure())) return bail(rc);
+        if ((rc = measure(i))) return bail(rc);
+        rs.iter_counter = i + 1;
+        if (o->save_every_iter > 0 && rs.iter_counter % o->save_every_iter == 0 && rs.iter_counter < o->iter &&
+            (rc = save()))
+            return bail(rc);
         if (!o->quiet && i % 10 == 0) { printf("\rGPU working iteration [%d]", i); fflush(stdout); }
     }
     if ((rc = qg_sync(ctx))) return bail(rc);
+    if (o->save_state && (rc = save())) return bail(rc);
     auto t1 = std::chrono::steady_clock::now();
     time_t t_end = time(nullptr);
     res->seconds = std::chrono::duration<double>(t1 - t0).count();
-    double sweeps = (double)o->nav + (double)(o->iter - 1) * o->niter;
+    const double sweeps = (double)(o->nav - nav_start) + (double)(o->iter - first) * o->niter;
     res->link_updates_per_second = res->seconds > 0 ? 4.0 * V * sweeps * (1 + cfg.n_or) / res->seconds : 0.0;
     res->samples = o->iter;
+    // lattice_analysis: normalised series (suncl.cpp:1328-1612)
+    std::vector<double> d[QG_OBS_COUNT];
+    for (int i = 0; i < o->iter; i++) {
+        if (o->get_plaquettes) {
+            d[QG_OBS_PLQ_SPAT].push_back(s_plq[2 * i] / (3 * V));
+            d[QG_OBS_PLQ_TEMP].push_back(s_plq[2 * i + 1] / (3 * V));
+            d[QG_OBS_PLQ_TOTAL].push_back(0.5 * (s_plq[2 * i] + s_plq[2 * i + 1]) / (3 * V));
+        }
+        if (o->get_wilson) d[QG_OBS_WILSON].push_back(s_wil[i] / (3 * V));
+        if (o->get_actions) {
+            d[QG_OBS_S_SPAT].push_back(s_act[2 * i] / (3 * V));
+            d[QG_OBS_S_TEMP].push_back(s_act[2 * i + 1] / (3 * V));
+            d[QG_OBS_S_TOTAL].push_back(0.5 * (s_act[2 * i] + s_act[2 * i + 1]) / (3 * V));
+        }
+        if (o->pl_level > 0) {
+            d[QG_OBS_POLYAKOV].push_back(s_pol[4 * i] / (nsp * N));
+            d[QG_OBS_POLYAKOV_IM].push_back(s_pol[4 * i + 1] / (nsp * N));
+            if (o->pl_level > 1) {
+                d[QG_OBS_POLYAKOV_P2].push_back(s_pol[4 * i + 2] / (nsp * N * N));
+                d[QG_OBS_POLYAKOV_P4].push_back(s_pol[4 * i + 3] / (nsp * N * N * N * N));
+            }
+        }
+    }
     for (int k = 0; k < QG_OBS_COUNT; k++) {
         if (d[k].empty()) continue;
         mean_var(d[k], res->mean[k], res->variance[k]);
         res->gpu_last[k] = d[k].back();
+        // tau_int and the error of the mean over samples 1..ITER-1
+        const int n = (int)d[k].size() - 1;
+        int w = 0;
+        res->tau_int[k] = 0.5;
+        if (n > 1) qg_tau_int(d[k].data() + 1, n, 6.0, &res->tau_int[k], &w);
+        res->error[k] = n > 0 ? sqrt(2.0 * res->tau_int[k] * res->variance[k] / n) : 0.0;
     }
     // LatticeCheckCPU: FP64 re-measurement of the final configuration
     if (o->verify) {
@@ -417,7 +527,7 @@ extern "C" int qg_run(const qg_config *cfg_in, const qg_run_options *o, qg_run_r
         fprintf(fp, " ***************************************************\n");
         fprintf(fp, " lattice size                : %3d x %3d x %3d x %3d\n", cfg.size[0], cfg.size[1], cfg.size[2],
                 cfg.size[3]);
-        fprintf(fp, " init                        : 1\n");
+        fprintf(fp, " init                        : %d\n", resume ? 0 : 1);
         fprintf(fp, " ints (0=hot, 1=cold, 2=gid) : %s\n", start_name[cfg.start]);
         fprintf(fp, " random series               : %u\n", cfg.randseries);
         if (cfg.prng == QG_PRNG_RANLUX) fprintf(fp, " PRN generator (%3d)         : RANLUX\n", cfg.ranlux_nskip);
@@ -451,6 +561,11 @@ extern "C" int qg_run(const qg_config *cfg_in, const qg_run_options *o, qg_run_r
         for (int k = 0; k <= QG_OBS_WILSON; k++) {
             fprintf(fp, " Mean %-20s: % 16.13e\n", names[k], res->mean[k]);
             fprintf(fp, " Variance %-16s: % 16.13e\n", names[k], res->variance[k]);
+        }
+        fprintf(fp, " ***************************************************\n");
+        for (int k = 0; k <= QG_OBS_WILSON; k++) {
+            fprintf(fp, " Tau_int %-17s: % 16.13e\n", names[k], res->tau_int[k]);
+            fprintf(fp, " Error %-19s: % 16.13e\n", names[k], res->error[k]);
         }
         fprintf(fp, " ***************************************************\n");
         for (int k = 0; k <= QG_OBS_WILSON; k++) {

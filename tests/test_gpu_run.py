@@ -61,3 +61,34 @@ def test_cli_runs_init_file(tmp_path):
     assert "Verification successfully passed!" in out.stdout
     files = [f for f in os.listdir(str(tmp_path)) if f.startswith("su3-") and f.endswith(".txt")]
     assert len(files) == 1
+
+
+@pytest.mark.parametrize("prng,start,precision", [(Q.PRNG_PHILOX, Q.START_HOT, 0), (Q.PRNG_RANLUX, Q.START_HOT, 0),
+                                                  (Q.PRNG_RANLUX, Q.START_COLD, 1)])
+def test_resume_from_state_file_continues_the_same_chain(tmp_path, prng, start, precision):
+    """INIT = 0: a run stopped after ITER_counter = 3 and continued from its
+    .qcg (RANLUX replayed to PRNG_counter, or the Philox counter restored)
+    ends in the same link table and measured series as an uninterrupted
+    run -- bit for bit."""
+    import struct
+    base = dict(group=3, size=(4, 4, 4, 8), precision=precision, start=start, prng=prng, beta=5.9,
+                prng_instances=256, row_align=64, n_or=2, reunit_every=3, wilson_r=2, wilson_t=2)
+    common = dict(niter=2, nav=3, pl_level=2, get_wilson=1, quiet=1, write_results=0, verify=0, save_state=1)
+    full, half, resumed = (str(tmp_path / n) for n in ("full.qcg", "half.qcg", "resumed.qcg"))
+    Q.run(Q.default_config(**base), Q.default_run_options(iter=6, state_out=full, **common))
+    Q.run(Q.default_config(**base), Q.default_run_options(iter=3, state_out=half, **common))
+    raw = bytearray(open(half, "rb").read())
+    assert struct.unpack_from("<I", raw, 14 * 4)[0] == 3          # ITER_counter
+    struct.pack_into("<I", raw, 13 * 4, 6)                         # extend ITER to 6
+    open(half, "wb").write(bytes(raw))
+    res = Q.run(Q.default_config(), Q.default_run_options(init=0, state_file=half, state_out=resumed, quiet=1,
+                                                          write_results=0, verify=0, save_state=1))
+    assert res.samples == 6
+    c1, s1, ser1, t1 = Q.read_state_file(full)
+    c2, s2, ser2, t2 = Q.read_state_file(resumed)
+    assert s1.iter_counter == s2.iter_counter == 6
+    assert s1.prng_counter == s2.prng_counter and s1.phase_counter == s2.phase_counter
+    assert s1.sweeps_done == s2.sweeps_done == 3 + 5 * 2
+    assert np.array_equal(t1, t2)
+    for k in ser1:
+        assert np.array_equal(ser1[k], ser2[k]), k
