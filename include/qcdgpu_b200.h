@@ -205,6 +205,50 @@ int qg_plaquette_noalloc(const void *links, int group, int precision, const int 
                          double beta, double *out, void *stream);
 
 /* ===================================================================== */
+/* Batched ensembles (new; no counterpart in the reference, which runs one */
+/* lattice per process): many independent lattices of one group and link   */
+/* precision -- different extents, couplings and seeds, e.g. a beta scan --  */
+/* updated together.  Each phase is ONE launch over all ensembles (a block  */
+/* finds its ensemble in a prefix table of block counts), the sweep and the */
+/* measurement are captured in one CUDA graph, and the measurements stay in */
+/* device memory until read.  Philox stream only.  Ensemble e's chain is    */
+/* bit-identical to a single context (qg_create) with its extents, coupling */
+/* and RANDSERIES and the common settings (start, NHIT, n_or, cadences).    */
+/* Errors: qg_last_error(NULL).                                             */
+/* ===================================================================== */
+typedef struct qg_ensemble {
+    int size[4];          /* L1..L4, N2 even                                 */
+    double beta;          /* BETA                                            */
+    uint32_t randseries;  /* Philox key (non-zero)                           */
+} qg_ensemble;
+typedef struct qg_batch qg_batch;
+/* common: group, precision, prng (must be QG_PRNG_PHILOX), nhit, nhitpar,
+ * n_or, reunit_every, reunit_fp64, row_align (for downloads); its size,
+ * beta and randseries are ignored.  max_measurements: capacity of the
+ * device series (measurements beyond it are dropped and reported).        */
+int qg_batch_create(const qg_config *common, const qg_ensemble *ens, int n, int max_measurements, qg_batch **out);
+int qg_batch_destroy(qg_batch *b);
+/* QG_START_COLD / HOT (Philox hot start) / HAAR for every ensemble; resets
+ * the phase and measurement counters                                      */
+int qg_batch_init(qg_batch *b, int start);
+/* phase-kernel shape of the batched launches: 0 registers, 4 staged      */
+int qg_batch_set_shape(qg_batch *b, int shape);
+/* nsweeps sweeps of every ensemble (graph replays); after every
+ * measure_every-th sweep (0 = never) plaquette, action and Polyakov sums of
+ * every ensemble are appended to the device series                         */
+int qg_batch_run(qg_batch *b, int nsweeps, int measure_every);
+int qg_batch_sync(qg_batch *b);
+int qg_batch_get_stream(qg_batch *b, void **stream);
+/* the series: out[m][e][8] = sum ReTr spatial, temporal, sum (beta/N)(3N -
+ * ReTr) spatial, temporal, sum Re P, Im P, |P|^2, |P|^4 (qg_measure's raw
+ * sums); *n_measurements = measurements held.  QG_ERR_STATE if any were
+ * dropped for capacity.                                                   */
+int qg_batch_series(qg_batch *b, double *out, uint64_t max_measurements, uint64_t *n_measurements);
+/* ensemble e's links in the reference layout (row_align of common)        */
+int qg_batch_links_download(qg_batch *b, int e, void *host);
+int qg_batch_info(qg_batch *b, uint64_t *total_sites, uint64_t *sweeps_done, uint64_t *field_bytes);
+
+/* ===================================================================== */
 /* Host driver: the reference's init.dat run setup, run loop and output   */
 /* (SU(N)/QCDGPU.cpp:61-269, model::lattice_get_init_file / lattice_init / */
 /* lattice_simulate / lattice_analysis / lattice_write_results,            */

@@ -31,6 +31,8 @@ EXPORTED_SYMBOLS = (
     "qg_default_run_options", "qg_parse_init_file", "qg_run", "qg_tune", "qg_plaquette_noalloc",
     "qg_set_shapes", "qg_get_shapes", "qg_get_config", "qg_set_sweeps_done",
     "qg_write_state_file", "qg_read_state_file", "qg_save_state", "qg_tau_int",
+    "qg_batch_create", "qg_batch_destroy", "qg_batch_init", "qg_batch_set_shape", "qg_batch_run", "qg_batch_sync",
+    "qg_batch_get_stream", "qg_batch_series", "qg_batch_links_download", "qg_batch_info",
 )
 
 
@@ -116,6 +118,11 @@ class RunResult(ctypes.Structure):
     ]
 
 
+class Ensemble(ctypes.Structure):
+    """qg_ensemble: one lattice of a batch."""
+    _fields_ = [("size", ctypes.c_int * 4), ("beta", ctypes.c_double), ("randseries", ctypes.c_uint32)]
+
+
 class RunState(ctypes.Structure):
     """qg_run_state: counters of a run and its measured series (raw sums)."""
     _fields_ = [
@@ -192,6 +199,16 @@ def load_library(path=LIB_PATH):
     lib.qg_save_state.argtypes = [vp, ctypes.c_char_p, P(RunState)]
     lib.qg_tau_int.argtypes = [P(ctypes.c_double), ctypes.c_int, ctypes.c_double, P(ctypes.c_double),
                                P(ctypes.c_int)]
+    lib.qg_batch_create.argtypes = [P(Config), P(Ensemble), ctypes.c_int, ctypes.c_int, P(vp)]
+    lib.qg_batch_destroy.argtypes = [vp]
+    lib.qg_batch_init.argtypes = [vp, ctypes.c_int]
+    lib.qg_batch_set_shape.argtypes = [vp, ctypes.c_int]
+    lib.qg_batch_run.argtypes = [vp, ctypes.c_int, ctypes.c_int]
+    lib.qg_batch_sync.argtypes = [vp]
+    lib.qg_batch_get_stream.argtypes = [vp, P(vp)]
+    lib.qg_batch_series.argtypes = [vp, P(ctypes.c_double), ctypes.c_uint64, P(ctypes.c_uint64)]
+    lib.qg_batch_links_download.argtypes = [vp, ctypes.c_int, vp]
+    lib.qg_batch_info.argtypes = [vp, P(ctypes.c_uint64), P(ctypes.c_uint64), P(ctypes.c_uint64)]
     lib.qg_default_run_options.argtypes = [P(RunOptions)]
     lib.qg_parse_init_file.argtypes = [ctypes.c_char_p, P(Config), P(RunOptions)]
     lib.qg_run.argtypes = [P(Config), P(RunOptions), P(RunResult)]
@@ -474,3 +491,84 @@ class Lattice:
     def prns_upload(self, a):
         a = np.ascontiguousarray(a, dtype=np.float32)
         self._ck(self.lib.qg_prns_upload(self.ctx, a.ctypes.data, a.size // 4), "qg_prns_upload")
+
+
+class Batch:
+    """Many independent lattices updated together (qg_batch): one launch per
+    phase over all ensembles, sweep + measurement in one CUDA graph.
+    `ensembles` is a list of (size 4-tuple, beta, randseries)."""
+
+    def __init__(self, common, ensembles, max_measurements=0):
+        self.lib = load_library()
+        self.cfg = common
+        self.n = len(ensembles)
+        arr = (Ensemble * self.n)()
+        for k, (size, beta, series) in enumerate(ensembles):
+            for i in range(4):
+                arr[k].size[i] = int(size[i])
+            arr[k].beta = float(beta)
+            arr[k].randseries = int(series)
+        self.ens = [(tuple(s), b, r) for s, b, r in ensembles]
+        self.b = ctypes.c_void_p()
+        rc = self.lib.qg_batch_create(ctypes.byref(common), arr, self.n, int(max_measurements), ctypes.byref(self.b))
+        if rc != QG_OK:
+            raise QGError("qg_batch_create: %s" % self.lib.qg_last_error(None).decode())
+
+    def _ck(self, rc, what):
+        if rc != QG_OK:
+            raise QGError("%s: %s" % (what, self.lib.qg_last_error(None).decode()))
+
+    def close(self):
+        if self.b:
+            self.lib.qg_batch_destroy(self.b)
+            self.b = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def init(self, start=START_COLD):
+        self._ck(self.lib.qg_batch_init(self.b, start), "qg_batch_init")
+
+    def set_shape(self, shape):
+        self._ck(self.lib.qg_batch_set_shape(self.b, shape), "qg_batch_set_shape")
+
+    def run(self, nsweeps, measure_every=0):
+        self._ck(self.lib.qg_batch_run(self.b, nsweeps, measure_every), "qg_batch_run")
+
+    def sync(self):
+        self._ck(self.lib.qg_batch_sync(self.b), "qg_batch_sync")
+
+    def stream(self):
+        s = ctypes.c_void_p()
+        self._ck(self.lib.qg_batch_get_stream(self.b, ctypes.byref(s)), "qg_batch_get_stream")
+        return s.value
+
+    def series(self):
+        """[measurement][ensemble][8] raw sums (plaquette s/t, action s/t,
+        Re P, Im P, |P|^2, |P|^4)."""
+        n = ctypes.c_uint64()
+        self._ck(self.lib.qg_batch_series(self.b, None, 0, ctypes.byref(n)), "qg_batch_series")
+        out = np.zeros((n.value, self.n, 8))
+        if n.value:
+            self._ck(self.lib.qg_batch_series(self.b, out.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), n.value,
+                                              ctypes.byref(n)), "qg_batch_series")
+        return out
+
+    def download(self, e):
+        size = self.ens[e][0]
+        V = int(np.prod(size))
+        a = self.cfg.row_align if self.cfg.row_align > 0 else 64
+        rowsize = (V + a - 1) // a * a
+        elems = (12 if self.cfg.group == 3 else 4) * rowsize * 4
+        out = np.zeros(elems, dtype=np.float64 if self.cfg.precision else np.float32)
+        self._ck(self.lib.qg_batch_links_download(self.b, e, out.ctypes.data_as(ctypes.c_void_p)),
+                 "qg_batch_links_download")
+        return out
+
+    def info(self):
+        v, s, f = ctypes.c_uint64(), ctypes.c_uint64(), ctypes.c_uint64()
+        self._ck(self.lib.qg_batch_info(self.b, ctypes.byref(v), ctypes.byref(s), ctypes.byref(f)), "qg_batch_info")
+        return {"sites": v.value, "sweeps": s.value, "field_bytes": f.value}

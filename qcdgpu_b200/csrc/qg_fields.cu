@@ -3,6 +3,7 @@
 // observables (plaquette/action, Polyakov loop, Wilson loops) with
 // deterministic two-pass FP64 reductions.
 #include "qg_internal.h"
+#include "qg_observe.cuh"
 
 namespace qg {
 
@@ -21,11 +22,6 @@ Geom make_geom(const int n[4])
     G.d234 = make_fastdiv(G.n2n3n4);
     return G;
 }
-
-template <typename Real>
-__device__ __forceinline__ Real param_real(double v) { return (Real)(float)v; }
-template <>
-__device__ __forceinline__ double param_real<double>(double v) { return v; }
 
 static __device__ __forceinline__ uint32_t native_index(const Geom &G, uint32_t s, const Crd &c)
 {
@@ -243,16 +239,7 @@ __global__ void k_gramschmidt(Field<Real> U, Geom G)
     if (i >= 2 * G.cb) return;
     uint32_t h = (i < G.cb) ? i : i - G.cb;
     if (h >= G.half) return;
-    for (int mu = 0; mu < 4; mu++) {
-        if (NC == 3) {
-            U.st3(mu, i, gs3<Acc>(U.ld3(mu, i)));
-        } else {
-            R4<Real> m = U.ld2(mu, i);
-            Acc x = m.x, y = m.y, z = m.z, w = m.w;
-            Acc det = sqrt(x * x + y * y + z * z + w * w);
-            U.st2(mu, i, R4<Real>{ (Real)(x / det), (Real)(y / det), (Real)(z / det), (Real)(w / det) });
-        }
-    }
+    gs_site<NC, Real, Acc>(U, i);
 }
 
 cudaError_t launch_gramschmidt(const Geom &G, void *links, int group, int prec, int fp64, cudaStream_t s)
@@ -315,115 +302,15 @@ cudaError_t launch_to_ref(const Geom &G, const void *links, void *ref, int group
 }
 
 // ------------------------------------------------------------ observables
-// FP64 view of a stored link (lattice_reconstruct3_double / 2_double,
-// su3_measurements_cl.cl:292-319, su2_measurements_cl.cl:126-141); SU(2)
-// is embedded in the upper 2x2 block with a zero third row and column.
-template <int NC, typename Real>
-__device__ __forceinline__ M3<double> load_d(const Field<Real> &U, const Geom &G, const Crd &c, int mu,
-                                             const double *params, int twist)
-{
-    uint32_t e = cb_index(G, c, parity_of(c));
-    M3<double> d;
-    if (NC == 3) {
-        G3<Real> m = U.ldg3(mu, e);
-        if (twist && mu == 1 && c.x == G.n[0] - 1) m = twist3(m, param_real<Real>(params[1]), param_real<Real>(params[2]));
-        G3<double> md;
-        md.uv1 = { (double)m.uv1.x, (double)m.uv1.y, (double)m.uv1.z, (double)m.uv1.w };
-        md.uv2 = { (double)m.uv2.x, (double)m.uv2.y, (double)m.uv2.z, (double)m.uv2.w };
-        md.uv3 = { (double)m.uv3.x, (double)m.uv3.y, (double)m.uv3.z, (double)m.uv3.w };
-        d = expand(md);
-    } else {
-        R4<Real> m = U.ldg2(mu, e);
-        if (twist && mu == 1 && c.x == G.n[0] - 1) {
-            Real ph = param_real<Real>(params[1]);
-            R4<Real> om = { RC<Real>::cs(ph / 2), 0, RC<Real>::sn(ph / 2), 0 };
-            m = times2(om, m);
-        }
-        for (int i = 0; i < 3; i++)
-            for (int j = 0; j < 3; j++) d.m[i][j] = { 0.0, 0.0 };
-        d.m[0][0] = { (double)m.x, (double)m.z }; d.m[0][1] = { (double)m.y, (double)m.w };
-        d.m[1][0] = { -(double)m.y, (double)m.w }; d.m[1][1] = { (double)m.x, -(double)m.z };
-    }
-    return d;
-}
-
-template <typename T>
-__device__ __forceinline__ M3<T> mulf(const M3<T> &u, const M3<T> &v)
-{
-    M3<T> t;
-#pragma unroll
-    for (int i = 0; i < 3; i++)
-#pragma unroll
-        for (int j = 0; j < 3; j++) t.m[i][j] = dot3(&u.m[i][0], 1, &v.m[0][j], 3);
-    return t;
-}
-// Re Tr(a b c^+ d^+)  (lattice_retrace_plaquette3, su3_measurements_cl.cl:527-548)
-__device__ __forceinline__ double retr4(const M3<double> &a, const M3<double> &b, const M3<double> &c,
-                                        const M3<double> &d)
-{
-    M3<double> ab = mulf(a, b), abc, abcd;
-#pragma unroll
-    for (int i = 0; i < 3; i++)
-#pragma unroll
-        for (int j = 0; j < 3; j++) abc.m[i][j] = dotc3(&ab.m[i][0], 1, &c.m[j][0], 1);
-    double tr = 0;
-#pragma unroll
-    for (int i = 0; i < 3; i++) tr += dotc3(&abc.m[i][0], 1, &d.m[i][0], 1).re;
-    (void)abcd;
-    return tr;
-}
-
-// warp + block sum of K doubles; thread 0 writes the block's partials
-template <int K>
-__device__ __forceinline__ void block_sum_store(double (&v)[K], double *partials)
-{
-    __shared__ double sh[K][32];
-    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
-#pragma unroll
-    for (int k = 0; k < K; k++) {
-        double x = v[k];
-        for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
-        if (lane == 0) sh[k][wid] = x;
-    }
-    __syncthreads();
-    if (wid == 0) {
-#pragma unroll
-        for (int k = 0; k < K; k++) {
-            double x = (lane < nw) ? sh[k][lane] : 0.0;
-            for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
-            if (lane == 0) partials[(size_t)blockIdx.x * K + k] = x;
-        }
-    }
-}
-
 // lattice_measurement_plq + lattice_measurement (sun_measurements_cl.cl:
-// 55-184,1178-1311): per site the xy,xz,yz (spatial) and xt,yt,zt
-// (temporal) plaquettes in FP64; also the action (beta/N)(3N - ReTr).
+// 55-184,1178-1311): per-site plaquette and action sums, block partials
 template <int NC, typename Real>
 __global__ void __launch_bounds__(256) k_plaquette(Field<Real> U, Geom G, const double *params, int twist,
                                                     double *partials)
 {
     uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
     double v[4] = { 0, 0, 0, 0 };
-    if (s < G.V) {
-        Crd c = lex2crd(G, s);
-        const Crd cx = step_plus(G, c, 0), cy = step_plus(G, c, 1), cz = step_plus(G, c, 2), ct = step_plus(G, c, 3);
-        M3<double> m1 = load_d<NC, Real>(U, G, c, 0, params, twist);
-        M3<double> m4 = load_d<NC, Real>(U, G, c, 1, params, twist);
-        M3<double> m5 = load_d<NC, Real>(U, G, c, 2, params, twist);
-        M3<double> m6 = load_d<NC, Real>(U, G, c, 3, params, twist);
-        const double bet = (double)param_real<Real>(params[0]);
-        double rs, rt;
-        rs  = retr4(m1, load_d<NC, Real>(U, G, cx, 1, params, twist), load_d<NC, Real>(U, G, cy, 0, params, twist), m4);
-        rs += retr4(m1, load_d<NC, Real>(U, G, cx, 2, params, twist), load_d<NC, Real>(U, G, cz, 0, params, twist), m5);
-        rt  = retr4(m1, load_d<NC, Real>(U, G, cx, 3, params, twist), load_d<NC, Real>(U, G, ct, 0, params, twist), m6);
-        rs += retr4(m4, load_d<NC, Real>(U, G, cy, 2, params, twist), load_d<NC, Real>(U, G, cz, 1, params, twist), m5);
-        rt += retr4(m4, load_d<NC, Real>(U, G, cy, 3, params, twist), load_d<NC, Real>(U, G, ct, 1, params, twist), m6);
-        rt += retr4(m5, load_d<NC, Real>(U, G, cz, 3, params, twist), load_d<NC, Real>(U, G, ct, 2, params, twist), m6);
-        v[0] = rs; v[1] = rt;
-        v[2] = bet * (3.0 * NC - rs);
-        v[3] = bet * (3.0 * NC - rt);
-    }
+    if (s < G.V) plaq_site<NC, Real>(U, G, params, twist, s, v);
     block_sum_store<4>(v, partials);
 }
 
@@ -447,44 +334,13 @@ cudaError_t launch_plaquette(const Geom &G, const void *links, int group, int pr
     return launch_reduce(partials, nb, 4, out, s);
 }
 
-// lattice_polyakov (polyakov.cl:54-140): ordered product of the N4 T-links
-// in link precision, traces accumulated in FP64
+// lattice_polyakov (polyakov.cl:54-140): one thread per spatial site
 template <int NC, typename Real>
 __global__ void __launch_bounds__(256) k_polyakov(Field<Real> U, Geom G, double *partials)
 {
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    const uint32_t nsp = (uint32_t)G.n[0] * G.n[1] * G.n[2];
     double v[4] = { 0, 0, 0, 0 };
-    if (i < nsp) {
-        Crd c;
-        c.y = (int)(i % (uint32_t)G.n[1]);
-        uint32_t r = i / (uint32_t)G.n[1];
-        c.z = (int)(r % (uint32_t)G.n[2]);
-        c.x = (int)(r / (uint32_t)G.n[2]);
-        c.t = 0;
-        double pr, pi;
-        if (NC == 3) {
-            M3<Real> v0 = expand(U.ldg3(3, cb_index(G, c, parity_of(c))));
-            for (int k = 1; k < G.n[3]; k++) {
-                c.t = k;
-                M3<Real> v1 = expand(U.ldg3(3, cb_index(G, c, parity_of(c))));
-                v0 = mulf(v0, v1);
-            }
-            pr = (double)v0.m[0][0].re + (double)v0.m[1][1].re + (double)v0.m[2][2].re;
-            pi = (double)v0.m[0][0].im + (double)v0.m[1][1].im + (double)v0.m[2][2].im;
-        } else {
-            S2<Real> v0 = rec2(U.ldg2(3, cb_index(G, c, parity_of(c))));
-            for (int k = 1; k < G.n[3]; k++) {
-                c.t = k;
-                S2<Real> v1 = rec2(U.ldg2(3, cb_index(G, c, parity_of(c))));
-                v0 = mul2(v0, v1);
-            }
-            pr = (double)v0.u1.re + (double)v0.v2.re;
-            pi = (double)v0.u1.im + (double)v0.v2.im;
-        }
-        double q2 = pr * pr + pi * pi;
-        v[0] = pr; v[1] = pi; v[2] = q2; v[3] = q2 * q2;
-    }
+    if (i < (uint32_t)G.n[0] * G.n[1] * G.n[2]) poly_site<NC, Real>(U, G, i, v);
     block_sum_store<4>(v, partials);
 }
 
@@ -563,20 +419,7 @@ cudaError_t launch_wilson(const Geom &G, const void *links, int group, int prec,
 // final pass: one block sums the partials in a fixed order (deterministic)
 __global__ void __launch_bounds__(1024) k_reduce(const double *partials, uint32_t nblocks, int ncomp, double *out)
 {
-    __shared__ double sh[32];
-    for (int k = 0; k < ncomp; k++) {
-        double x = 0;
-        for (uint32_t b = threadIdx.x; b < nblocks; b += blockDim.x) x += partials[(size_t)b * ncomp + k];
-        for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
-        if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = x;
-        __syncthreads();
-        if (threadIdx.x < 32) {
-            x = sh[threadIdx.x];
-            for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
-            if (threadIdx.x == 0) out[k] = x;
-        }
-        __syncthreads();
-    }
+    reduce_partials(partials, nblocks, ncomp, out);
 }
 
 cudaError_t launch_reduce(const double *partials, uint32_t nblocks, int ncomp, double *out, cudaStream_t s)

@@ -258,12 +258,12 @@ template <typename Real> struct PrnOf<Real, 2> {
 
 // MINB: minimum resident blocks of 128 threads per SM asked of the
 // compiler (0 = its own register choice); the launch shapes the tuner picks
-// STAGED: staple links through shared memory (staple3_staged; SU(3) FP32)
-template <int NC, typename Real, int PMODE, bool OR, int mu, int MINB, bool STAGED>
-__global__ void __launch_bounds__(kPhaseBlock, MINB) k_phase(Field<Real> U, Geom G, PhaseArgs A)
+// The update of link U_mu(x) for thread t of a (parity, mu) phase: the
+// body of update_{even,odd}_{X,Y,Z,T}.  STAGED: staple links through
+// shared memory (staple3_staged; SU(3) FP32 links).
+template <int NC, typename Real, int PMODE, bool OR, int mu, bool STAGED>
+__device__ __forceinline__ void phase_site(const Field<Real> &U, const Geom &G, const PhaseArgs &A, uint32_t t)
 {
-    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= G.half) return;
     const int p = A.parity;
     Crd c = lex2crd(G, 2 * t);
     if (parity_of(c) != p) c.y += 1;                 // lattice_{even,odd}_gid
@@ -313,6 +313,14 @@ __global__ void __launch_bounds__(kPhaseBlock, MINB) k_phase(Field<Real> U, Geom
             U.st2(mu, e0, times2(times2(aH, herm2(m0)), aH));
         }
     }
+}
+
+template <int NC, typename Real, int PMODE, bool OR, int mu, int MINB, bool STAGED>
+__global__ void __launch_bounds__(kPhaseBlock, MINB) k_phase(Field<Real> U, Geom G, PhaseArgs A)
+{
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= G.half) return;
+    phase_site<NC, Real, PMODE, OR, mu, STAGED>(U, G, A, t);
 }
 
 template <typename Real>

@@ -1,0 +1,63 @@
+"""Batched ensembles (qg_batch) against single contexts: every ensemble of
+a heterogeneous batch -- different extents, couplings and seeds, one launch
+per phase over all of them -- follows the chain a single context with its
+settings follows, bit for bit, and the device-resident measurement series
+equals the single context's qg_measure sums at the same sweeps."""
+import numpy as np
+import pytest
+
+import qcdgpu_b200 as Q
+
+pytestmark = pytest.mark.gpu
+
+ENSEMBLES = [((4, 4, 4, 4), 5.5, 101), ((6, 4, 4, 8), 5.8, 102), ((4, 6, 6, 4), 6.0, 103),
+             ((8, 8, 8, 4), 6.2, 104), ((4, 4, 8, 6), 5.9, 105)]
+
+
+def common(group, precision, **kw):
+    return Q.default_config(group=group, precision=precision, prng=Q.PRNG_PHILOX, n_or=2, reunit_every=3,
+                            reunit_fp64=1, nhit=10, row_align=64, **kw)
+
+
+@pytest.mark.parametrize("group,precision,shape,start", [(3, 0, 4, Q.START_HOT), (3, 0, 0, Q.START_COLD),
+                                                         (3, 1, 0, Q.START_HAAR), (2, 1, 0, Q.START_HOT),
+                                                         (2, 0, 4, Q.START_COLD)])
+def test_batch_equals_single_contexts(group, precision, shape, start):
+    sweeps, every = 7, 2
+    B = Q.Batch(common(group, precision), ENSEMBLES, max_measurements=8)
+    B.set_shape(shape)
+    B.init(start)
+    B.run(sweeps, measure_every=every)
+    ser = B.series()
+    assert ser.shape == (sweeps // every, len(ENSEMBLES), 8)
+    info = B.info()
+    assert info["sweeps"] == sweeps and info["sites"] == sum(int(np.prod(s)) for s, _, _ in ENSEMBLES)
+    for e, (size, beta, series) in enumerate(ENSEMBLES):
+        L = Q.Lattice(common(group, precision, size=size, beta=beta, randseries=series, start=start))
+        L.seed(series)
+        L.init(start)
+        m = 0
+        for k in range(1, sweeps + 1):
+            L.sweep(1)
+            if k % every == 0:
+                got = np.concatenate([L.plaquette_sums(), L.action_sums(), L.polyakov_sums()])
+                assert np.array_equal(got, ser[m, e]), (e, k, got, ser[m, e])
+                m += 1
+        assert np.array_equal(L.download(), B.download(e)), e
+        L.close()
+    B.close()
+
+
+def test_batch_series_capacity_and_argument_checks():
+    B = Q.Batch(common(3, 0), ENSEMBLES[:2], max_measurements=1)
+    B.init(Q.START_COLD)
+    B.run(3, measure_every=1)
+    with pytest.raises(Q.QGError):
+        B.series()
+    B.close()
+    with pytest.raises(Q.QGError):
+        Q.Batch(Q.default_config(group=3, precision=0, prng=Q.PRNG_RANLUX), ENSEMBLES[:1])
+    with pytest.raises(Q.QGError):
+        Q.Batch(common(3, 0), [((4, 5, 4, 4), 6.0, 1)])
+    with pytest.raises(Q.QGError):
+        Q.Batch(common(3, 0), [((4, 4, 4, 4), 6.0, 0)])
