@@ -205,6 +205,46 @@ int qg_plaquette_noalloc(const void *links, int group, int precision, const int 
                          double beta, double *out, void *stream);
 
 /* ===================================================================== */
+/* Learned local proposal with an exact Metropolis step (new; the          */
+/* reference has only the heatbath).  SU(3), FP32 links, Philox stream,    */
+/* periodic boundaries.  Each hit proposes, per SU(2) subgroup of the link */
+/* U_mu(x), U' = X U with X = exp(i eps a.sigma), a ~ N(0,1)^3, accepted   */
+/* with min(1, exp(-dS)) for the Wilson action.  eps = eps_max sigmoid(f)  */
+/* with f a 3-layer network (QG_NET_FEATURES -> QG_NET_HIDDEN ->           */
+/* QG_NET_HIDDEN -> 1, ReLU) of gauge-invariant features of the staple     */
+/* alone (Tr AA^+, Tr (AA^+)^2, det A, 1x2 loop traces Tr F B^+ per plane),*/
+/* which no link of the phase changes: the proposal is symmetric and the   */
+/* chain exact for any weights.  Weights are BF16 in the kernels, FP32 for */
+/* the optimiser; the network is trained on the GPU to maximise the        */
+/* expected squared jump distance.  Layout of the QG_NET_PARAMS floats:     */
+/* W1[32][8], b1[32], W2[32][32], b2[32], w3[32], b3.                       */
+/* ===================================================================== */
+#define QG_NET_FEATURES 8
+#define QG_NET_HIDDEN 32
+#define QG_NET_PARAMS 1377
+/* set the FP32 master weights (the kernels use their BF16 rounding) and
+ * eps_max in (0, 3.2]; resets the optimiser state                          */
+int qg_net_set(qg_ctx *ctx, const float *params, double eps_max);
+/* master: FP32 master weights; weights_bf16: the BF16 weights as floats   */
+int qg_net_get(qg_ctx *ctx, float *master, float *weights_bf16);
+/* one Metropolis phase (parity, dir) with nhit hits per subgroup and link */
+int qg_mh_phase(qg_ctx *ctx, int parity, int dir, int nhit);
+/* nsweeps sweeps of Metropolis phases in the heatbath's phase order, with
+ * the global reunitarisation on qg_sweep's cadence                         */
+int qg_mh_sweep(qg_ctx *ctx, int nsweeps, int nhit);
+/* acceptance rate and mean squared jump angle per proposal since the last
+ * reset, and the number of proposals; reset != 0 clears them             */
+int qg_mh_stats(qg_ctx *ctx, double *accept_rate, double *jump_per_hit, uint64_t *hits, int reset);
+/* gradient (QG_NET_PARAMS floats) of the training loss -- minus the mean
+ * over the phase's links of sum_subgroups min(1, exp(-dS)) (eps|a|)^2 for
+ * proposals from the current links -- and stats = {loss, ESJD, mean
+ * acceptance, links}; the field is not changed                             */
+int qg_net_grad(qg_ctx *ctx, int parity, int dir, float *grad, double *stats);
+/* steps Adam steps (learning rate lr) on the current field, step s on the
+ * links of phase s % 8; stats (optional) = mean of qg_net_grad's stats     */
+int qg_net_train(qg_ctx *ctx, int steps, double lr, double *stats);
+
+/* ===================================================================== */
 /* Batched ensembles (new; no counterpart in the reference, which runs one */
 /* lattice per process): many independent lattices of one group and link   */
 /* precision -- different extents, couplings and seeds, e.g. a beta scan --  */

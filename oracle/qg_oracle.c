@@ -281,6 +281,34 @@ static double ol_log(double y)
     return fma(de, LN2_HI, fma(de, LN2_LO, t));
 }
 
+/* exp(x), |x| <= 700: x = k ln2 + r (Cody-Waite, two-part ln 2), Taylor
+ * polynomial of degree 13 in Horner form, scaled by 2^k (exact); the
+ * device routine qg_exp performs the same operations */
+static double ol_exp(double x)
+{
+    x = fmin(fmax(x, -700.0), 700.0);
+    const double LN2_HI = 6.93147180369123816490e-01, LN2_LO = 1.90821492927058770002e-10;
+    const double k = rint(x * 1.44269504088896340736);
+    double r = fma(-k, LN2_HI, x);
+    r = fma(-k, LN2_LO, r);
+    double p = 1.0 / 6227020800.0;
+    p = fma(p, r, 1.0 / 479001600.0);
+    p = fma(p, r, 1.0 / 39916800.0);
+    p = fma(p, r, 1.0 / 3628800.0);
+    p = fma(p, r, 1.0 / 362880.0);
+    p = fma(p, r, 1.0 / 40320.0);
+    p = fma(p, r, 1.0 / 5040.0);
+    p = fma(p, r, 1.0 / 720.0);
+    p = fma(p, r, 1.0 / 120.0);
+    p = fma(p, r, 1.0 / 24.0);
+    p = fma(p, r, 1.0 / 6.0);
+    p = fma(p, r, 0.5);
+    p = fma(p, r, 1.0);
+    p = fma(p, r, 1.0);
+    return ldexp(p, (int)k);
+}
+double ol_expd(double x) { return ol_exp(x); }
+
 /* exported for the accuracy tests of the two routines */
 double ol_sin(double x) { double s, c; ol_sincos(x, &s, &c); return s; }
 double ol_cos(double x) { double s, c; ol_sincos(x, &s, &c); return c; }
@@ -379,3 +407,6 @@ double ol_local_action_link(const ol_cfg *c, const void *t, int gid, int dir)
     DISPATCH(r = local_action_f(c, (const float *)t, gid, dir), r = local_action_d(c, (const double *)t, gid, dir));
     return r;
 }
+
+/* ======================================================= learned proposal */
+#include "qg_oracle_learned.h"

@@ -78,6 +78,17 @@ void ol_polyakov(const ol_cfg *c, const void *table, double out[4]);
 double ol_wilson(const ol_cfg *c, const void *table, int R, int T);
 double ol_local_action_link(const ol_cfg *c, const void *table, int gid, int dir);
 
+/* ---- learned-proposal Metropolis (SU(3), float links; qg_oracle_learned.h) */
+double ol_expd(double x);
+void   ol_mh_features(const ol_cfg *c, const void *table, int gid, int mu, float x[8]);
+float  ol_mlp_out(const float *w, const float x[8]);
+void   ol_mh_phase(const ol_cfg *c, void *table, int parity, int mu, const float *w, double eps_max, int nhit,
+                   uint32_t key0, uint32_t key1, uint64_t phase, uint64_t *acc, double *jump);
+void   ol_mh_grad(const ol_cfg *c, const void *table, int parity, int mu, const float *w, double eps_max,
+                  uint32_t key0, uint32_t key1, uint64_t phase, double *grad, double stats[4]);
+double ol_mh_loss(const ol_cfg *c, const void *table, int parity, int mu, const double *w, double eps_max,
+                  uint32_t key0, uint32_t key1, uint64_t phase);
+
 #ifdef __cplusplus
 }
 #endif

@@ -22,6 +22,7 @@ LAYOUT_REFERENCE = 0
 HEATBATH, OVERRELAX = 0, 1
 MEAS_PLAQUETTE, MEAS_ACTION, MEAS_POLYAKOV, MEAS_WILSON = 0, 1, 2, 3
 TUNE_SHAPES = 5                     # QG_TUNE_SHAPES
+NET_FEATURES, NET_HIDDEN, NET_PARAMS = 8, 32, 1377   # QG_NET_*
 
 EXPORTED_SYMBOLS = (
     "qg_default_config", "qg_create", "qg_destroy", "qg_last_error", "qg_get_info", "qg_sync",
@@ -33,6 +34,7 @@ EXPORTED_SYMBOLS = (
     "qg_write_state_file", "qg_read_state_file", "qg_save_state", "qg_tau_int",
     "qg_batch_create", "qg_batch_destroy", "qg_batch_init", "qg_batch_set_shape", "qg_batch_run", "qg_batch_sync",
     "qg_batch_get_stream", "qg_batch_series", "qg_batch_links_download", "qg_batch_info",
+    "qg_net_set", "qg_net_get", "qg_mh_phase", "qg_mh_sweep", "qg_mh_stats", "qg_net_grad", "qg_net_train",
 )
 
 
@@ -199,6 +201,14 @@ def load_library(path=LIB_PATH):
     lib.qg_save_state.argtypes = [vp, ctypes.c_char_p, P(RunState)]
     lib.qg_tau_int.argtypes = [P(ctypes.c_double), ctypes.c_int, ctypes.c_double, P(ctypes.c_double),
                                P(ctypes.c_int)]
+    fp = P(ctypes.c_float)
+    lib.qg_net_set.argtypes = [vp, fp, ctypes.c_double]
+    lib.qg_net_get.argtypes = [vp, fp, fp]
+    lib.qg_mh_phase.argtypes = [vp, ctypes.c_int, ctypes.c_int, ctypes.c_int]
+    lib.qg_mh_sweep.argtypes = [vp, ctypes.c_int, ctypes.c_int]
+    lib.qg_mh_stats.argtypes = [vp, P(ctypes.c_double), P(ctypes.c_double), P(ctypes.c_uint64), ctypes.c_int]
+    lib.qg_net_grad.argtypes = [vp, ctypes.c_int, ctypes.c_int, fp, P(ctypes.c_double)]
+    lib.qg_net_train.argtypes = [vp, ctypes.c_int, ctypes.c_double, P(ctypes.c_double)]
     lib.qg_batch_create.argtypes = [P(Config), P(Ensemble), ctypes.c_int, ctypes.c_int, P(vp)]
     lib.qg_batch_destroy.argtypes = [vp]
     lib.qg_batch_init.argtypes = [vp, ctypes.c_int]
@@ -224,6 +234,39 @@ def glibc_seeds(randseries, n):
     if rc != QG_OK:
         raise QGError("qg_glibc_seeds failed")
     return out
+
+
+def bf16_round(a):
+    """Round float32 values to the nearest BF16 (ties to even), as floats --
+    the weights the learned-proposal kernels compute with."""
+    u = np.ascontiguousarray(a, dtype=np.float32).view(np.uint32).astype(np.uint64)
+    u = (u + 0x7FFF + ((u >> 16) & 1)) >> 16
+    return (u.astype(np.uint32) << 16).view(np.float32)
+
+
+def net_init(seed=0, out_bias=0.0):
+    """He-normal initial weights of the step-size network (QG_NET_PARAMS
+    floats: W1[32][8], b1[32], W2[32][32], b2[32], w3[32], b3)."""
+    rng = np.random.default_rng(seed)
+    p = np.zeros(NET_PARAMS, dtype=np.float32)
+    nf, nh = NET_FEATURES, NET_HIDDEN
+    o = 0
+    p[o:o + nh * nf] = rng.standard_normal(nh * nf) * np.sqrt(2.0 / nf); o += nh * nf
+    o += nh
+    p[o:o + nh * nh] = rng.standard_normal(nh * nh) * np.sqrt(2.0 / nh); o += nh * nh
+    o += nh
+    p[o:o + nh] = rng.standard_normal(nh) * np.sqrt(1.0 / nh) * 0.1; o += nh
+    p[o] = out_bias
+    return p
+
+
+def net_constant(eps, eps_max):
+    """Weights that give the constant step eps (the proposal without a
+    network): everything zero except the output bias logit(eps/eps_max)."""
+    p = np.zeros(NET_PARAMS, dtype=np.float32)
+    r = eps / eps_max
+    p[-1] = np.log(r / (1.0 - r))
+    return p
 
 
 def tau_int(x, c=6.0):
@@ -415,6 +458,48 @@ class Lattice:
         h, o = ctypes.c_int(), ctypes.c_int()
         self._ck(self.lib.qg_get_shapes(self.ctx, ctypes.byref(h), ctypes.byref(o)), "qg_get_shapes")
         return h.value, o.value
+
+    # ---- learned proposal (SU(3), FP32 links, Philox)
+    def net_set(self, params, eps_max):
+        a = np.ascontiguousarray(params, dtype=np.float32)
+        assert a.size == NET_PARAMS
+        self._ck(self.lib.qg_net_set(self.ctx, a.ctypes.data_as(ctypes.POINTER(ctypes.c_float)), eps_max),
+                 "qg_net_set")
+        self.eps_max = eps_max
+
+    def net_get(self):
+        """(FP32 master weights, the BF16 weights as floats)"""
+        m = np.zeros(NET_PARAMS, dtype=np.float32)
+        b = np.zeros(NET_PARAMS, dtype=np.float32)
+        fp = ctypes.POINTER(ctypes.c_float)
+        self._ck(self.lib.qg_net_get(self.ctx, m.ctypes.data_as(fp), b.ctypes.data_as(fp)), "qg_net_get")
+        return m, b
+
+    def mh_phase(self, parity, direction, nhit=1):
+        self._ck(self.lib.qg_mh_phase(self.ctx, parity, direction, nhit), "qg_mh_phase")
+
+    def mh_sweep(self, n=1, nhit=1):
+        self._ck(self.lib.qg_mh_sweep(self.ctx, n, nhit), "qg_mh_sweep")
+
+    def mh_stats(self, reset=False):
+        """(acceptance rate, mean squared jump angle per proposal, proposals)"""
+        a, j, h = ctypes.c_double(), ctypes.c_double(), ctypes.c_uint64()
+        self._ck(self.lib.qg_mh_stats(self.ctx, ctypes.byref(a), ctypes.byref(j), ctypes.byref(h), int(reset)),
+                 "qg_mh_stats")
+        return a.value, j.value, h.value
+
+    def net_grad(self, parity, direction):
+        """(gradient, stats = [loss, ESJD, acceptance, links])"""
+        g = np.zeros(NET_PARAMS, dtype=np.float32)
+        st = (ctypes.c_double * 4)()
+        self._ck(self.lib.qg_net_grad(self.ctx, parity, direction, g.ctypes.data_as(ctypes.POINTER(ctypes.c_float)),
+                                      st), "qg_net_grad")
+        return g, list(st)
+
+    def net_train(self, steps, lr):
+        st = (ctypes.c_double * 4)()
+        self._ck(self.lib.qg_net_train(self.ctx, steps, lr, st), "qg_net_train")
+        return list(st)
 
     def sync(self):
         self._ck(self.lib.qg_sync(self.ctx), "qg_sync")

@@ -37,6 +37,15 @@ struct qg_ctx {
     bool seeded = false;
     cudaStream_t stream = nullptr;
     cudaGraphExec_t graph[2] = { nullptr, nullptr };  // sweep without / with reunitarisation
+    // learned-proposal Metropolis (qg_net_*, qg_mh_*)
+    uint16_t *d_netw = nullptr;     // BF16 weights the kernels read
+    float *d_master = nullptr, *d_adam_m = nullptr, *d_adam_v = nullptr;
+    float *d_grad = nullptr, *d_gpart = nullptr;    // QG_NET_PARAMS + 4 stats; per-block partials
+    unsigned long long *d_mh_acc = nullptr;
+    double *d_mh_jump = nullptr;
+    double eps_max = 0.0;
+    int adam_t = 0;
+    uint64_t train_phase = 0, mh_hits = 0;
     std::string err;
 };
 
@@ -121,6 +130,8 @@ extern "C" int qg_destroy(qg_ctx *c)
     destroy_graphs(c);
     cudaFree(c->links); cudaFree(c->prns); cudaFree(c->rl_table); cudaFree(c->d_seeds);
     cudaFree(c->partials); cudaFree(c->d_results); cudaFree(c->d_phase); cudaFree(c->d_params);
+    cudaFree(c->d_netw); cudaFree(c->d_master); cudaFree(c->d_adam_m); cudaFree(c->d_adam_v);
+    cudaFree(c->d_grad); cudaFree(c->d_gpart); cudaFree(c->d_mh_acc); cudaFree(c->d_mh_jump);
     if (c->h_results) cudaFreeHost(c->h_results);
     if (c->h_params) cudaFreeHost(c->h_params);
     if (c->stream) cudaStreamDestroy(c->stream);
@@ -567,6 +578,200 @@ extern "C" int qg_sweep(qg_ctx *c, int nsweeps)
         if (philox) c->phase_counter += 8;
         if (ranlux) c->prng_counter += 8;
     }
+    return QG_OK;
+}
+
+// ------------------------------------------------- learned-proposal Metropolis
+static int net_check(qg_ctx *c)
+{
+    if (c->cfg.group != 3 || c->cfg.precision != 0 || c->cfg.prng != QG_PRNG_PHILOX)
+        return fail(c, QG_ERR_UNSUPPORTED, "the learned proposal runs on SU(3) FP32 links with the Philox stream");
+    if (c->cfg.phi != 0.0 || c->cfg.omega != 0.0)
+        return fail(c, QG_ERR_UNSUPPORTED, "the learned proposal needs periodic boundaries (PHI = OMEGA = 0)");
+    return QG_OK;
+}
+
+extern "C" int qg_net_set(qg_ctx *c, const float *params, double eps_max)
+{
+    if (!c || !params) return QG_ERR_ARG;
+    int r = net_check(c);
+    if (r) return r;
+    if (!(eps_max > 0.0 && eps_max <= 3.2)) return fail(c, QG_ERR_ARG, "eps_max must be in (0, 3.2]");
+    const size_t np = QG_NET_PARAMS;
+    if (!c->d_master) {
+        QG_CK(cudaMalloc(&c->d_netw, np * sizeof(uint16_t)), "net alloc");
+        QG_CK(cudaMalloc(&c->d_master, np * sizeof(float)), "net alloc");
+        QG_CK(cudaMalloc(&c->d_adam_m, np * sizeof(float)), "net alloc");
+        QG_CK(cudaMalloc(&c->d_adam_v, np * sizeof(float)), "net alloc");
+        QG_CK(cudaMalloc(&c->d_grad, (np + 4) * sizeof(float)), "net alloc");
+        QG_CK(cudaMalloc(&c->d_gpart, (size_t)mh_grad_blocks(c->G) * (np + 4) * sizeof(float)), "net alloc");
+        QG_CK(cudaMalloc(&c->d_mh_acc, sizeof(unsigned long long)), "net alloc");
+        QG_CK(cudaMalloc(&c->d_mh_jump, sizeof(double)), "net alloc");
+        QG_CK(cudaMemsetAsync(c->d_mh_acc, 0, sizeof(unsigned long long), c->stream), "net clear");
+        QG_CK(cudaMemsetAsync(c->d_mh_jump, 0, sizeof(double), c->stream), "net clear");
+    }
+    QG_CK(cudaMemcpyAsync(c->d_master, params, np * sizeof(float), cudaMemcpyHostToDevice, c->stream), "net upload");
+    QG_CK(cudaMemsetAsync(c->d_adam_m, 0, np * sizeof(float), c->stream), "net clear");
+    QG_CK(cudaMemsetAsync(c->d_adam_v, 0, np * sizeof(float), c->stream), "net clear");
+    QG_CK(launch_to_bf16(c->d_master, c->d_netw, c->stream), "net bf16");
+    QG_CK(cudaStreamSynchronize(c->stream), "net sync");
+    c->eps_max = eps_max;
+    c->adam_t = 0;
+    return QG_OK;
+}
+
+extern "C" int qg_net_get(qg_ctx *c, float *master, float *weights_bf16)
+{
+    if (!c) return QG_ERR_ARG;
+    if (!c->d_master) return fail(c, QG_ERR_STATE, "no network set (qg_net_set)");
+    const size_t np = QG_NET_PARAMS;
+    if (master) QG_CK(cudaMemcpyAsync(master, c->d_master, np * sizeof(float), cudaMemcpyDeviceToHost, c->stream), "net get");
+    std::vector<uint16_t> b(np);
+    QG_CK(cudaMemcpyAsync(b.data(), c->d_netw, np * sizeof(uint16_t), cudaMemcpyDeviceToHost, c->stream), "net get");
+    QG_CK(cudaStreamSynchronize(c->stream), "net get sync");
+    if (weights_bf16)
+        for (size_t i = 0; i < np; i++) {
+            uint32_t u = (uint32_t)b[i] << 16;
+            memcpy(&weights_bf16[i], &u, 4);
+        }
+    return QG_OK;
+}
+
+static int mh_ready(qg_ctx *c)
+{
+    int r = net_check(c);
+    if (r) return r;
+    if (!c->d_master) return fail(c, QG_ERR_STATE, "no network set (qg_net_set)");
+    if (!c->seeded) return fail(c, QG_ERR_STATE, "the learned proposal needs a seeded PRNG (qg_prng_seed)");
+    return QG_OK;
+}
+
+static cudaError_t mh_launch(qg_ctx *c, int parity, int dir, int nhit, uint32_t offset)
+{
+    PhaseArgs a = phase_args(c, parity, dir, QG_UPDATE_HEATBATH, offset);
+    return launch_mh_phase(c->G, c->links, a, c->d_netw, c->eps_max, nhit, c->d_mh_acc, c->d_mh_jump, c->stream);
+}
+
+extern "C" int qg_mh_phase(qg_ctx *c, int parity, int dir, int nhit)
+{
+    if (!c) return QG_ERR_ARG;
+    if (parity < 0 || parity > 1 || dir < 0 || dir > 3 || nhit < 1) return fail(c, QG_ERR_ARG, "bad phase");
+    int r = mh_ready(c);
+    if (r) return r;
+    QG_CK(mh_launch(c, parity, dir, nhit, 0), "mh phase");
+    QG_CK(launch_add_u64(c->d_phase, 1, c->stream), "phase counter");
+    c->phase_counter++;
+    c->mh_hits += (uint64_t)c->G.half * 3 * nhit;
+    return QG_OK;
+}
+
+// learned-proposal sweeps: odd X..T, even X..T Metropolis phases (nhit
+// hits per subgroup and link), the global Gram-Schmidt on the cadence of
+// qg_sweep (the sweep counter is shared)
+extern "C" int qg_mh_sweep(qg_ctx *c, int nsweeps, int nhit)
+{
+    if (!c) return QG_ERR_ARG;
+    if (nsweeps < 0 || nhit < 1) return fail(c, QG_ERR_ARG, "bad sweep arguments");
+    int r = mh_ready(c);
+    if (r) return r;
+    const qg_config &f = c->cfg;
+    const int par_order[2] = { 1, 0 };
+    for (int n = 0; n < nsweeps; n++) {
+        uint32_t k = 0;
+        for (int pi = 0; pi < 2; pi++)
+            for (int mu = 0; mu < 4; mu++) QG_CK(mh_launch(c, par_order[pi], mu, nhit, k++), "mh phase");
+        QG_CK(launch_add_u64(c->d_phase, 8, c->stream), "phase counter");
+        c->phase_counter += 8;
+        c->mh_hits += (uint64_t)c->G.half * 2 * 4 * 3 * nhit;
+        const bool reunit = f.reunit_every > 0 && ((c->sweeps_done + 1) % (uint64_t)f.reunit_every) == 0;
+        if (reunit)
+            QG_CK(launch_gramschmidt(c->G, c->links, f.group, f.precision, f.reunit_fp64, c->stream), "gramschmidt");
+        c->sweeps_done++;
+    }
+    return QG_OK;
+}
+
+extern "C" int qg_mh_stats(qg_ctx *c, double *accept_rate, double *jump_per_hit, uint64_t *hits, int reset)
+{
+    if (!c) return QG_ERR_ARG;
+    unsigned long long acc = 0;
+    double jump = 0.0;
+    if (c->d_mh_acc) {
+        QG_CK(cudaMemcpyAsync(&acc, c->d_mh_acc, sizeof(acc), cudaMemcpyDeviceToHost, c->stream), "stats");
+        QG_CK(cudaMemcpyAsync(&jump, c->d_mh_jump, sizeof(jump), cudaMemcpyDeviceToHost, c->stream), "stats");
+        QG_CK(cudaStreamSynchronize(c->stream), "stats sync");
+    }
+    const double h = (double)c->mh_hits;
+    if (accept_rate) *accept_rate = h > 0 ? (double)acc / h : 0.0;
+    if (jump_per_hit) *jump_per_hit = h > 0 ? jump / h : 0.0;
+    if (hits) *hits = c->mh_hits;
+    if (reset && c->d_mh_acc) {
+        QG_CK(cudaMemsetAsync(c->d_mh_acc, 0, sizeof(unsigned long long), c->stream), "stats reset");
+        QG_CK(cudaMemsetAsync(c->d_mh_jump, 0, sizeof(double), c->stream), "stats reset");
+        c->mh_hits = 0;
+    }
+    return QG_OK;
+}
+
+static const uint32_t kTrainKey = 0x2C1B3A49u;
+
+extern "C" int qg_net_grad(qg_ctx *c, int parity, int dir, float *grad, double *stats)
+{
+    if (!c) return QG_ERR_ARG;
+    if (parity < 0 || parity > 1 || dir < 0 || dir > 3) return fail(c, QG_ERR_ARG, "bad phase");
+    int r = mh_ready(c);
+    if (r) return r;
+    QG_CK(launch_mh_grad(c->G, c->links, parity, dir, c->d_params, c->d_netw, c->eps_max,
+                         make_uint2(c->cfg.randseries, kTrainKey), c->train_phase++, c->d_gpart, c->d_grad, c->stream),
+          "net grad");
+    std::vector<float> h(QG_NET_PARAMS + 4);
+    QG_CK(cudaMemcpyAsync(h.data(), c->d_grad, h.size() * sizeof(float), cudaMemcpyDeviceToHost, c->stream), "grad copy");
+    QG_CK(cudaStreamSynchronize(c->stream), "grad sync");
+    if (grad) memcpy(grad, h.data(), QG_NET_PARAMS * sizeof(float));
+    if (stats) {
+        const double n = h[QG_NET_PARAMS + 3] > 0 ? h[QG_NET_PARAMS + 3] : 1.0;
+        stats[0] = h[QG_NET_PARAMS] / n;          // loss per link
+        stats[1] = h[QG_NET_PARAMS + 1] / n;      // ESJD per link (3 proposals)
+        stats[2] = h[QG_NET_PARAMS + 2] / n;      // mean acceptance
+        stats[3] = h[QG_NET_PARAMS + 3];          // links
+    }
+    return QG_OK;
+}
+
+// steps Adam steps; step s uses the links of phase (s % 8) in the sweep
+// order; stats: the mean over the steps of (loss, ESJD, acceptance, links)
+extern "C" int qg_net_train(qg_ctx *c, int steps, double lr, double *stats)
+{
+    if (!c) return QG_ERR_ARG;
+    if (steps < 0 || !(lr > 0.0)) return fail(c, QG_ERR_ARG, "bad training arguments");
+    int r = mh_ready(c);
+    if (r) return r;
+    const int par_order[2] = { 1, 0 };
+    double acc[4] = { 0, 0, 0, 0 };
+    std::vector<float> h(QG_NET_PARAMS + 4);
+    for (int s = 0; s < steps; s++) {
+        const int k = s % 8;
+        QG_CK(launch_mh_grad(c->G, c->links, par_order[k / 4], k % 4, c->d_params, c->d_netw, c->eps_max,
+                             make_uint2(c->cfg.randseries, kTrainKey), c->train_phase++, c->d_gpart, c->d_grad,
+                             c->stream), "net grad");
+        c->adam_t++;
+        const float b1 = 0.9f, b2 = 0.999f;
+        const float c1 = 1.0f - powf(b1, (float)c->adam_t), c2 = 1.0f - powf(b2, (float)c->adam_t);
+        QG_CK(launch_adam(c->d_master, c->d_adam_m, c->d_adam_v, c->d_grad, c->d_netw, (float)lr, b1, b2, c1, c2,
+                          1e-8f, c->stream), "adam");
+        if (stats) {
+            QG_CK(cudaMemcpyAsync(h.data(), c->d_grad, h.size() * sizeof(float), cudaMemcpyDeviceToHost, c->stream),
+                  "grad copy");
+            QG_CK(cudaStreamSynchronize(c->stream), "train sync");
+            const double n = h[QG_NET_PARAMS + 3] > 0 ? h[QG_NET_PARAMS + 3] : 1.0;
+            acc[0] += h[QG_NET_PARAMS] / n;
+            acc[1] += h[QG_NET_PARAMS + 1] / n;
+            acc[2] += h[QG_NET_PARAMS + 2] / n;
+            acc[3] += h[QG_NET_PARAMS + 3];
+        }
+    }
+    if (stats)
+        for (int k = 0; k < 4; k++) stats[k] = steps > 0 ? acc[k] / steps : 0.0;
     return QG_OK;
 }
 

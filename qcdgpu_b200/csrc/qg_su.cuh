@@ -96,6 +96,33 @@ __device__ __forceinline__ double qg_log(double y)
     return FMA(de, LN2_HI, FMA(de, LN2_LO, t));
 }
 
+// exp(x) for |x| <= 700: x = k ln2 + r (Cody-Waite, ln 2 in two parts),
+// |r| <= ln2/2, Taylor polynomial of degree 13 in Horner form (truncation
+// < 1e-17 relative), scaled by 2^k (exact)
+__device__ __forceinline__ double qg_exp(double x)
+{
+    x = fmin(fmax(x, -700.0), 700.0);
+    const double LN2_HI = 6.93147180369123816490e-01, LN2_LO = 1.90821492927058770002e-10;
+    const double k = rint(x * 1.44269504088896340736);
+    double r = FMA(-k, LN2_HI, x);
+    r = FMA(-k, LN2_LO, r);
+    double p = 1.0 / 6227020800.0;                      // 1/13!
+    p = FMA(p, r, 1.0 / 479001600.0);                    // 1/12!
+    p = FMA(p, r, 1.0 / 39916800.0);
+    p = FMA(p, r, 1.0 / 3628800.0);
+    p = FMA(p, r, 1.0 / 362880.0);
+    p = FMA(p, r, 1.0 / 40320.0);
+    p = FMA(p, r, 1.0 / 5040.0);
+    p = FMA(p, r, 1.0 / 720.0);
+    p = FMA(p, r, 1.0 / 120.0);
+    p = FMA(p, r, 1.0 / 24.0);
+    p = FMA(p, r, 1.0 / 6.0);
+    p = FMA(p, r, 0.5);
+    p = FMA(p, r, 1.0);
+    p = FMA(p, r, 1.0);
+    return ldexp(p, (int)k);
+}
+
 template <typename Real> struct RC;
 template <> struct RC<float> {
     static constexpr float PI = 3.141592653589793f;

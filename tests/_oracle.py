@@ -42,7 +42,8 @@ class Prn(ctypes.Structure):
 
 
 def _load():
-    src = [os.path.join(ORACLE_DIR, f) for f in ("qg_oracle.c", "qg_oracle_impl.h", "qg_oracle.h")]
+    src = [os.path.join(ORACLE_DIR, f) for f in ("qg_oracle.c", "qg_oracle_impl.h", "qg_oracle_learned.h",
+                                                 "qg_oracle.h")]
     if not os.path.exists(LIB_PATH) or any(os.path.getmtime(s) > os.path.getmtime(LIB_PATH) for s in src):
         subprocess.check_call(["make", "-s", "-C", ORACLE_DIR])
     lib = ctypes.CDLL(LIB_PATH)
@@ -68,6 +69,19 @@ def _load():
     lib.ol_wilson.restype = ctypes.c_double
     lib.ol_local_action_link.argtypes = [P(Cfg), ctypes.c_void_p, ctypes.c_int, ctypes.c_int]
     lib.ol_local_action_link.restype = ctypes.c_double
+    fp, dp = P(ctypes.c_float), P(ctypes.c_double)
+    lib.ol_expd.argtypes = [ctypes.c_double]
+    lib.ol_expd.restype = ctypes.c_double
+    lib.ol_mh_features.argtypes = [P(Cfg), ctypes.c_void_p, ctypes.c_int, ctypes.c_int, fp]
+    lib.ol_mlp_out.argtypes = [fp, fp]
+    lib.ol_mlp_out.restype = ctypes.c_float
+    lib.ol_mh_phase.argtypes = [P(Cfg), ctypes.c_void_p, ctypes.c_int, ctypes.c_int, fp, ctypes.c_double, ctypes.c_int,
+                                ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint64, P(ctypes.c_uint64), dp]
+    lib.ol_mh_grad.argtypes = [P(Cfg), ctypes.c_void_p, ctypes.c_int, ctypes.c_int, fp, ctypes.c_double,
+                               ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint64, dp, dp]
+    lib.ol_mh_loss.argtypes = [P(Cfg), ctypes.c_void_p, ctypes.c_int, ctypes.c_int, dp, ctypes.c_double,
+                               ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint64]
+    lib.ol_mh_loss.restype = ctypes.c_double
     return lib
 
 
@@ -180,3 +194,41 @@ def philox(ctr, key):
     k2 = (ctypes.c_uint32 * 2)(*key)
     lib.ol_philox4x32(c4, k2, o)
     return tuple(o)
+
+
+# ---- learned-proposal Metropolis (SU(3), float links)
+CHAIN_KEY1, TRAIN_KEY1 = 0x5D3E1A27, 0x2C1B3A49
+
+
+def _fp(a):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_float))
+
+
+def mh_features(c, tab, gid, mu):
+    x = np.zeros(8, dtype=np.float32)
+    lib.ol_mh_features(ctypes.byref(c), vp(tab), gid, mu, _fp(x))
+    return x
+
+
+def mh_phase(c, tab, parity, mu, w, eps_max, nhit, key0, phase, key1=CHAIN_KEY1):
+    w = np.ascontiguousarray(w, dtype=np.float32)
+    acc = ctypes.c_uint64()
+    jump = ctypes.c_double()
+    lib.ol_mh_phase(ctypes.byref(c), vp(tab), parity, mu, _fp(w), eps_max, nhit, key0, key1, phase,
+                    ctypes.byref(acc), ctypes.byref(jump))
+    return acc.value, jump.value
+
+
+def mh_grad(c, tab, parity, mu, w, eps_max, key0, phase, key1=TRAIN_KEY1):
+    w = np.ascontiguousarray(w, dtype=np.float32)
+    g = np.zeros(w.size, dtype=np.float64)
+    st = (ctypes.c_double * 4)()
+    lib.ol_mh_grad(ctypes.byref(c), vp(tab), parity, mu, _fp(w), eps_max, key0, key1, phase,
+                   g.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), st)
+    return g, list(st)
+
+
+def mh_loss(c, tab, parity, mu, w, eps_max, key0, phase, key1=TRAIN_KEY1):
+    w = np.ascontiguousarray(w, dtype=np.float64)
+    return lib.ol_mh_loss(ctypes.byref(c), vp(tab), parity, mu, w.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
+                          eps_max, key0, key1, phase)
