@@ -163,6 +163,12 @@ int qg_reunitarize(qg_ctx *ctx, int fp64);
 int qg_measure(qg_ctx *ctx, int what, double *out);
 /* same, generalised Wilson loop of extent R x T (config keys WILSONR/T)   */
 int qg_measure_wilson(qg_ctx *ctx, int R, int T, double *out);
+/* all planar Wilson loops R x T for R <= Rmax, T <= Tmax (both <= 16): in
+ * one launch, out[(R-1)*Tmax + (T-1)] = the raw sum qg_measure_wilson
+ * gives (new; the reference measures one R x T per run).  fp64_products:
+ * 1 = matrix products in FP64 as qg_measure_wilson; 0 = in FP32 on FP32
+ * links (traces summed in FP64; about 4x faster, relative error ~1e-6)  */
+int qg_measure_wilson_all(qg_ctx *ctx, int Rmax, int Tmax, int fp64_products, double *out);
 
 /* buffer_init / buffer_map of the link table (clinterface.cpp:1296-1434):
  * host arrays in the reference layout, Real = float (precision 0) or

@@ -34,7 +34,7 @@ EXPORTED_SYMBOLS = (
     "qg_write_state_file", "qg_read_state_file", "qg_save_state", "qg_tau_int",
     "qg_batch_create", "qg_batch_destroy", "qg_batch_init", "qg_batch_set_shape", "qg_batch_run", "qg_batch_sync",
     "qg_batch_get_stream", "qg_batch_series", "qg_batch_links_download", "qg_batch_info",
-    "qg_net_set", "qg_net_get", "qg_mh_phase", "qg_mh_sweep", "qg_mh_stats", "qg_net_grad", "qg_net_train",
+    "qg_measure_wilson_all", "qg_net_set", "qg_net_get", "qg_mh_phase", "qg_mh_sweep", "qg_mh_stats", "qg_net_grad", "qg_net_train",
 )
 
 
@@ -183,6 +183,7 @@ def load_library(path=LIB_PATH):
     lib.qg_reunitarize.argtypes = [vp, ctypes.c_int]
     lib.qg_measure.argtypes = [vp, ctypes.c_int, P(ctypes.c_double)]
     lib.qg_measure_wilson.argtypes = [vp, ctypes.c_int, ctypes.c_int, P(ctypes.c_double)]
+    lib.qg_measure_wilson_all.argtypes = [vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, P(ctypes.c_double)]
     lib.qg_links_upload.argtypes = [vp, vp, ctypes.c_int]
     lib.qg_links_download.argtypes = [vp, vp, ctypes.c_int]
     lib.qg_set_phase_counter.argtypes = [vp, ctypes.c_uint64]
@@ -530,6 +531,14 @@ class Lattice:
 
     def polyakov_sums(self):
         return self._measure(MEAS_POLYAKOV, 4)
+
+    def wilson_all(self, Rmax, Tmax, fp64_products=True):
+        """raw sums of all R x T Wilson loops, array [Rmax][Tmax]"""
+        out = np.zeros(Rmax * Tmax)
+        self._ck(self.lib.qg_measure_wilson_all(self.ctx, Rmax, Tmax, int(bool(fp64_products)),
+                                                out.ctypes.data_as(ctypes.POINTER(ctypes.c_double))),
+                 "qg_measure_wilson_all")
+        return out.reshape(Rmax, Tmax)
 
     def wilson_sum(self, R=None, T=None):
         out = (ctypes.c_double * 1)()

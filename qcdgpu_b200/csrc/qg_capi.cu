@@ -5,6 +5,7 @@
 
 #include <new>
 #include <string>
+#include <algorithm>
 #include <vector>
 
 #include "qg_internal.h"
@@ -41,6 +42,8 @@ struct qg_ctx {
     uint16_t *d_netw = nullptr;     // BF16 weights the kernels read
     float *d_master = nullptr, *d_adam_m = nullptr, *d_adam_v = nullptr;
     float *d_grad = nullptr, *d_gpart = nullptr;    // QG_NET_PARAMS + 4 stats; per-block partials
+    double *d_wpart = nullptr, *d_wout = nullptr;   // all-loops Wilson measurement (lazy)
+    int wpart_rmax = 0;
     unsigned long long *d_mh_acc = nullptr;
     double *d_mh_jump = nullptr;
     double eps_max = 0.0;
@@ -132,6 +135,7 @@ extern "C" int qg_destroy(qg_ctx *c)
     cudaFree(c->partials); cudaFree(c->d_results); cudaFree(c->d_phase); cudaFree(c->d_params);
     cudaFree(c->d_netw); cudaFree(c->d_master); cudaFree(c->d_adam_m); cudaFree(c->d_adam_v);
     cudaFree(c->d_grad); cudaFree(c->d_gpart); cudaFree(c->d_mh_acc); cudaFree(c->d_mh_jump);
+    cudaFree(c->d_wpart); cudaFree(c->d_wout);
     if (c->h_results) cudaFreeHost(c->h_results);
     if (c->h_params) cudaFreeHost(c->h_params);
     if (c->stream) cudaStreamDestroy(c->stream);
@@ -793,6 +797,30 @@ extern "C" int qg_measure_wilson(qg_ctx *c, int R, int T, double *out)
     QG_CK(launch_wilson(c->G, c->links, f.group, f.precision, R, T, c->d_params, tw, c->partials, c->d_results,
                         c->stream), "wilson");
     return measure_to_host(c, 1, out);
+}
+
+extern "C" int qg_measure_wilson_all(qg_ctx *c, int Rmax, int Tmax, int fp64_products, double *out)
+{
+    if (!c || !out) return QG_ERR_ARG;
+    const int ns = std::min(c->G.n[0], std::min(c->G.n[1], c->G.n[2]));
+    if (Rmax < 1 || Tmax < 1 || Rmax > 16 || Tmax > 16 || Rmax > ns || Tmax > c->G.n[3])
+        return fail(c, QG_ERR_ARG, "Wilson loop extents must be in [1, 16] and within the lattice");
+    const qg_config &f = c->cfg;
+    int tw = !(f.phi == 0.0 && f.omega == 0.0);
+    if (c->wpart_rmax < Rmax) {
+        cudaFree(c->d_wpart);
+        c->d_wpart = nullptr;
+        QG_CK(cudaMalloc(&c->d_wpart, wilson_all_partials(wilson_all_blocks(c->G), Rmax) * sizeof(double)),
+              "wilson scratch");
+        c->wpart_rmax = Rmax;
+    }
+    if (!c->d_wout) QG_CK(cudaMalloc(&c->d_wout, 256 * sizeof(double)), "wilson scratch");
+    QG_CK(launch_wilson_all(c->G, c->links, f.group, f.precision, Rmax, Tmax, fp64_products, c->d_params, tw,
+                            c->d_wpart, c->d_wout, c->stream), "wilson all");
+    QG_CK(cudaMemcpyAsync(out, c->d_wout, (size_t)Rmax * Tmax * sizeof(double), cudaMemcpyDeviceToHost, c->stream),
+          "wilson copy");
+    QG_CK(cudaStreamSynchronize(c->stream), "wilson sync");
+    return QG_OK;
 }
 
 extern "C" int qg_measure(qg_ctx *c, int what, double *out)

@@ -416,6 +416,91 @@ cudaError_t launch_wilson(const Geom &G, const void *links, int group, int prec,
     return launch_reduce(partials, nb, 1, out, s);
 }
 
+// All planar Wilson loops R x T, R <= Rmax, T <= Tmax (<= 16), in one
+// launch: block (bx, R-1, i) walks sites bx, bx + gridDim.x, ... and for each
+// site x builds the spatial line L_i^R(x) once and extends the time lines
+// L_t^T(x), L_t^T(x+R i) one link per T, so that every T <= Tmax costs only
+// the top line L_i^R(x+T t).  Products in P: FP64 as k_wilson, or FP32 on
+// FP32 links (traces still summed in FP64); per-block sums of the Tmax
+// traces, then k_wilson_all_reduce in a fixed order.
+constexpr int kWilsonMax = 16;
+
+template <int NC, typename Real, typename P>
+__global__ void __launch_bounds__(128) k_wilson_all(Field<Real> U, Geom G, int Tmax, const double *params, int twist,
+                                                     double *partials)
+{
+    const int R = blockIdx.y + 1, i = blockIdx.z;
+    double w[kWilsonMax];
+#pragma unroll
+    for (int k = 0; k < kWilsonMax; k++) w[k] = 0.0;
+    for (uint32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < G.V; s += gridDim.x * blockDim.x) {
+        const Crd x = lex2crd(G, s);
+        Crd a = x;
+        M3<P> m4 = load_as<NC, Real, P>(U, G, a, i, params, twist);
+        for (int k = 1; k < R; k++) { a = step_plus(G, a, i); m4 = mulf(m4, load_as<NC, Real, P>(U, G, a, i, params, twist)); }
+        Crd cx = x, cy = step_plus(G, a, i);
+        M3<P> mx = load_as<NC, Real, P>(U, G, cx, 3, params, twist);
+        M3<P> my = load_as<NC, Real, P>(U, G, cy, 3, params, twist);
+#pragma unroll
+        for (int T = 1; T <= kWilsonMax; T++) {
+            if (T <= Tmax) {
+                if (T > 1) {
+                    cx = step_plus(G, cx, 3);
+                    mx = mulf(mx, load_as<NC, Real, P>(U, G, cx, 3, params, twist));
+                    cy = step_plus(G, cy, 3);
+                    my = mulf(my, load_as<NC, Real, P>(U, G, cy, 3, params, twist));
+                }
+                Crd b = step_plus(G, cx, 3);
+                M3<P> m2 = load_as<NC, Real, P>(U, G, b, i, params, twist);
+                for (int k = 1; k < R; k++) { b = step_plus(G, b, i); m2 = mulf(m2, load_as<NC, Real, P>(U, G, b, i, params, twist)); }
+                w[T - 1] += retr4(mx, m2, my, m4);
+            }
+        }
+    }
+    block_sum_store<kWilsonMax>(w, partials, (blockIdx.z * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x);
+}
+
+// out[(R-1) Tmax + T-1] = sum over i and blocks (in that order)
+__global__ void k_wilson_all_reduce(const double *partials, int nbx, int Rmax, int Tmax, double *out)
+{
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= Rmax * Tmax) return;
+    const int R = q / Tmax + 1, T = q % Tmax + 1;
+    double s = 0.0;
+    for (int i = 0; i < 3; i++)
+        for (int b = 0; b < nbx; b++) s += partials[((size_t)(i * Rmax + R - 1) * nbx + b) * kWilsonMax + T - 1];
+    out[q] = s;
+}
+
+int wilson_all_blocks(const Geom &G) { return (int)min((G.V + 127u) / 128u, 296u); }
+size_t wilson_all_partials(int nbx, int Rmax) { return (size_t)3 * Rmax * nbx * kWilsonMax; }
+
+cudaError_t launch_wilson_all(const Geom &G, const void *links, int group, int prec, int Rmax, int Tmax,
+                              int fp64_products, const double *params, int twist, double *partials, double *out,
+                              cudaStream_t s)
+{
+    const int nbx = wilson_all_blocks(G);
+    dim3 grid(nbx, Rmax, 3);
+    if (prec) {
+        Field<double> U{ (double4 *)links, G.pstride };
+        if (group == 3) k_wilson_all<3, double, double><<<grid, 128, 0, s>>>(U, G, Tmax, params, twist, partials);
+        else k_wilson_all<2, double, double><<<grid, 128, 0, s>>>(U, G, Tmax, params, twist, partials);
+    } else {
+        Field<float> U{ (float4 *)links, G.pstride };
+        if (fp64_products) {
+            if (group == 3) k_wilson_all<3, float, double><<<grid, 128, 0, s>>>(U, G, Tmax, params, twist, partials);
+            else k_wilson_all<2, float, double><<<grid, 128, 0, s>>>(U, G, Tmax, params, twist, partials);
+        } else {
+            if (group == 3) k_wilson_all<3, float, float><<<grid, 128, 0, s>>>(U, G, Tmax, params, twist, partials);
+            else k_wilson_all<2, float, float><<<grid, 128, 0, s>>>(U, G, Tmax, params, twist, partials);
+        }
+    }
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    k_wilson_all_reduce<<<(Rmax * Tmax + 127) / 128, 128, 0, s>>>(partials, nbx, Rmax, Tmax, out);
+    return cudaGetLastError();
+}
+
 // final pass: one block sums the partials in a fixed order (deterministic)
 __global__ void __launch_bounds__(1024) k_reduce(const double *partials, uint32_t nblocks, int ncomp, double *out)
 {

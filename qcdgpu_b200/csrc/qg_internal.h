@@ -50,6 +50,11 @@ cudaError_t launch_polyakov(const Geom &G, const void *links, int group, int pre
 cudaError_t launch_wilson(const Geom &G, const void *links, int group, int prec, int R, int T, const double *params,
                           int twist, double *partials, double *out, cudaStream_t s);
 cudaError_t launch_reduce(const double *partials, uint32_t nblocks, int ncomp, double *out, cudaStream_t s);
+int wilson_all_blocks(const Geom &G);
+size_t wilson_all_partials(int nbx, int Rmax);
+cudaError_t launch_wilson_all(const Geom &G, const void *links, int group, int prec, int Rmax, int Tmax,
+                              int fp64_products, const double *params, int twist, double *partials, double *out,
+                              cudaStream_t s);
 cudaError_t launch_add_u64(uint64_t *p, uint64_t v, cudaStream_t s);
 
 // RANLUX, reference layout: one generator per instance, seed table of 7

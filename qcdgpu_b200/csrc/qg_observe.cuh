@@ -12,22 +12,23 @@ __device__ __forceinline__ Real param_real(double v) { return (Real)(float)v; }
 template <>
 __device__ __forceinline__ double param_real<double>(double v) { return v; }
 
-// FP64 view of a stored link (lattice_reconstruct3_double / 2_double,
+// A stored link as a full 3x3 matrix in precision P -- FP64 for the
+// observables (lattice_reconstruct3_double / 2_double,
 // su3_measurements_cl.cl:292-319, su2_measurements_cl.cl:126-141); SU(2)
 // is embedded in the upper 2x2 block with a zero third row and column.
-template <int NC, typename Real>
-__device__ __forceinline__ M3<double> load_d(const Field<Real> &U, const Geom &G, const Crd &c, int mu,
-                                             const double *params, int twist)
+template <int NC, typename Real, typename P>
+__device__ __forceinline__ M3<P> load_as(const Field<Real> &U, const Geom &G, const Crd &c, int mu,
+                                         const double *params, int twist)
 {
     uint32_t e = cb_index(G, c, parity_of(c));
-    M3<double> d;
+    M3<P> d;
     if (NC == 3) {
         G3<Real> m = U.ldg3(mu, e);
         if (twist && mu == 1 && c.x == G.n[0] - 1) m = twist3(m, param_real<Real>(params[1]), param_real<Real>(params[2]));
-        G3<double> md;
-        md.uv1 = { (double)m.uv1.x, (double)m.uv1.y, (double)m.uv1.z, (double)m.uv1.w };
-        md.uv2 = { (double)m.uv2.x, (double)m.uv2.y, (double)m.uv2.z, (double)m.uv2.w };
-        md.uv3 = { (double)m.uv3.x, (double)m.uv3.y, (double)m.uv3.z, (double)m.uv3.w };
+        G3<P> md;
+        md.uv1 = { (P)m.uv1.x, (P)m.uv1.y, (P)m.uv1.z, (P)m.uv1.w };
+        md.uv2 = { (P)m.uv2.x, (P)m.uv2.y, (P)m.uv2.z, (P)m.uv2.w };
+        md.uv3 = { (P)m.uv3.x, (P)m.uv3.y, (P)m.uv3.z, (P)m.uv3.w };
         d = expand(md);
     } else {
         R4<Real> m = U.ldg2(mu, e);
@@ -37,11 +38,17 @@ __device__ __forceinline__ M3<double> load_d(const Field<Real> &U, const Geom &G
             m = times2(om, m);
         }
         for (int i = 0; i < 3; i++)
-            for (int j = 0; j < 3; j++) d.m[i][j] = { 0.0, 0.0 };
-        d.m[0][0] = { (double)m.x, (double)m.z }; d.m[0][1] = { (double)m.y, (double)m.w };
-        d.m[1][0] = { -(double)m.y, (double)m.w }; d.m[1][1] = { (double)m.x, -(double)m.z };
+            for (int j = 0; j < 3; j++) d.m[i][j] = { (P)0, (P)0 };
+        d.m[0][0] = { (P)m.x, (P)m.z }; d.m[0][1] = { (P)m.y, (P)m.w };
+        d.m[1][0] = { -(P)m.y, (P)m.w }; d.m[1][1] = { (P)m.x, -(P)m.z };
     }
     return d;
+}
+template <int NC, typename Real>
+__device__ __forceinline__ M3<double> load_d(const Field<Real> &U, const Geom &G, const Crd &c, int mu,
+                                             const double *params, int twist)
+{
+    return load_as<NC, Real, double>(U, G, c, mu, params, twist);
 }
 
 template <typename T>
@@ -53,6 +60,23 @@ __device__ __forceinline__ M3<T> mulf(const M3<T> &u, const M3<T> &v)
 #pragma unroll
         for (int j = 0; j < 3; j++) t.m[i][j] = dot3(&u.m[i][0], 1, &v.m[0][j], 3);
     return t;
+}
+// Re Tr(a b c^+ d^+) of FP32 products, the trace summed in FP64
+__device__ __forceinline__ double retr4(const M3<float> &a, const M3<float> &b, const M3<float> &c,
+                                        const M3<float> &d)
+{
+    M3<float> ab = mulf(a, b), abc;
+#pragma unroll
+    for (int i = 0; i < 3; i++)
+#pragma unroll
+        for (int j = 0; j < 3; j++) abc.m[i][j] = dotc3(&ab.m[i][0], 1, &c.m[j][0], 1);
+    double tr = 0;
+#pragma unroll
+    for (int i = 0; i < 3; i++)
+#pragma unroll
+        for (int k = 0; k < 3; k++)
+            tr += (double)abc.m[i][k].re * (double)d.m[i][k].re + (double)abc.m[i][k].im * (double)d.m[i][k].im;
+    return tr;
 }
 // Re Tr(a b c^+ d^+)  (lattice_retrace_plaquette3, su3_measurements_cl.cl:527-548)
 __device__ __forceinline__ double retr4(const M3<double> &a, const M3<double> &b, const M3<double> &c,

@@ -383,3 +383,33 @@ def test_set_shapes_rejects_out_of_range():
     with pytest.raises(Q.QGError):
         L.set_shapes(0, -1)
     L.close()
+
+
+@pytest.mark.parametrize("group,precision", [(3, 0), (3, 1), (2, 1)])
+def test_wilson_all_loops_match_single_loops_and_oracle(group, precision):
+    """qg_measure_wilson_all (every R x T up to Rmax x Tmax in one launch)
+    equals qg_measure_wilson loop by loop and the oracle's Wilson loops, to
+    the FP64 summation-order level"""
+    L, c = make_pair(group, (4, 6, 6, 8), precision, start=Q.START_HOT, prng=Q.PRNG_PHILOX, beta=5.8)
+    L.seed(54)
+    L.init()
+    L.sweep(2)
+    tab = L.download()
+    W = L.wilson_all(4, 6)
+    assert W.shape == (4, 6)
+    for R in range(1, 5):
+        for T in range(1, 7):
+            single = L.wilson_sum(R, T)
+            assert abs(W[R - 1, T - 1] - single) <= 1e-12 * abs(single) + 1e-9, (R, T)
+    for R, T in ((1, 1), (2, 3), (4, 6)):
+        ow = O.wilson(c, tab, R, T)
+        assert abs(W[R - 1, T - 1] - ow) <= 1e-11 * abs(ow) + 1e-8, (R, T)
+    if precision == 0:                                   # FP32 products, FP64 trace sums
+        W32 = L.wilson_all(4, 6, fp64_products=False)
+        V = 4 * 6 * 6 * 8
+        assert np.max(np.abs(W32 - W)) <= 3e-6 * 3 * V
+    with pytest.raises(Q.QGError):
+        L.wilson_all(5, 6)
+    with pytest.raises(Q.QGError):
+        L.wilson_all(4, 17)
+    L.close()
