@@ -47,9 +47,6 @@ def parse():
     return ap.parse_args()
 
 
-def dist_env():
-    return int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)), int(os.environ.get("LOCAL_RANK", 0))
-
 
 # ------------------------------------------------------------- clocks
 class ClockSampler:
@@ -145,8 +142,9 @@ def cpu_baseline_line(size, seconds_target=15.0):
 
 
 def run_reference_arm(args):
-    rank, world, _ = dist_env()
-    if rank != 0:
+    from qcdgpu_b200 import replicas as RP
+    rank, world, _ = RP.dist_env()
+    if not RP.reference_arm_runs_here(rank):
         return 0
     if not os.path.exists(ref_binary()):
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/ref_cpurun not built"}))
@@ -194,16 +192,14 @@ def run_ours(args):
     import torch
     import qcdgpu_b200 as Q
 
-    rank, world, local = dist_env()
+    from qcdgpu_b200 import replicas as RP
+
+    rank, world, local = RP.dist_env()
     torch.cuda.set_device(local)
-    dist = None
-    if world > 1:
-        import torch.distributed as dist
-        from datetime import timedelta
-        dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=torch.device("cuda", local))
+    dist = RP.init("nccl", 120, torch.device("cuda", local)) if world > 1 else None
     prng = Q.PRNG_PHILOX if args.prng == "philox" else Q.PRNG_RANLUX
     cfg = Q.default_config(group=3, size=args.size, precision=0, start=Q.START_COLD, prng=prng, beta=BETA,
-                           n_or=N_OR, reunit_every=REUNIT_EVERY, reunit_fp64=1, randseries=54 + rank,
+                           n_or=N_OR, reunit_every=REUNIT_EVERY, reunit_fp64=1, randseries=RP.replica_seed(rank),
                            prng_instances=16384)
     L = Q.Lattice(cfg)
     L.seed()
@@ -219,22 +215,17 @@ def run_ours(args):
     L.sync()
     clocks = ClockSampler(local)
     clocks.start()
-    if dist:
-        dist.barrier()
+    RP.barrier(dist)
     torch.cuda.synchronize()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record(stream)
     L.sweep(args.steps)
     e1.record(stream)
     torch.cuda.synchronize()
-    ms = e0.elapsed_time(e1)
-    if dist:
-        t = torch.tensor([ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
-        dist.barrier()
+    ms = RP.max_over_ranks(e0.elapsed_time(e1), dist, "cuda")
+    RP.barrier(dist)
     clk = clocks.stop()
-    value = world * updates_per_step * args.steps / (ms / 1e3)
+    value = RP.whole_job_rate(world, updates_per_step * args.steps, ms / 1e3)
 
     # dominant kernel: time single heatbath / overrelaxation phase launches
     def time_phases(kind, reps=16):
@@ -263,8 +254,7 @@ def run_ours(args):
     # Polyakov sums come back to host (qg_measure)
     e2e_steps = max(3, args.steps // 2)
     L.sync()
-    if dist:
-        dist.barrier()
+    RP.barrier(dist)
     t0 = time.perf_counter()
     for _ in range(e2e_steps):
         L.set_params(BETA)
@@ -272,12 +262,8 @@ def run_ours(args):
         L.plaquette_sums()
         L.polyakov_sums()
     t1 = time.perf_counter()
-    e2e_s = t1 - t0
-    if dist:
-        t = torch.tensor([e2e_s], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_s = float(t.item())
-    e2e = world * updates_per_step * e2e_steps / e2e_s
+    e2e_s = RP.max_over_ranks(t1 - t0, dist, "cuda")
+    e2e = RP.whole_job_rate(world, updates_per_step * e2e_steps, e2e_s)
 
     plq = L.plaquette()
     first = 2 + args.warmup
@@ -286,8 +272,7 @@ def run_ours(args):
     if prng == Q.PRNG_RANLUX:
         launches += 8 * args.steps
     L.close()
-    if dist:
-        dist.destroy_process_group()
+    RP.finish(dist)
     if rank != 0:
         return 0
     line = {
