@@ -143,11 +143,13 @@ int qg_sweep(qg_ctx *ctx, int nsweeps);
  * fastest for later phases and sweeps.  Shapes: 0 = links loaded straight
  * into registers, compiler's register count; 1, 2 = the same held to 5 / 6
  * resident blocks per SM; 3, 4 = staple links streamed through shared
- * memory two staple terms ahead (SU(3) FP32; other cases run shape 0 / 1).
+ * memory two staple terms ahead (SU(3) FP32; other cases run shape 0 / 1);
+ * 5 = overrelaxation two links per thread with packed FP32 (FFMA2)
+ * arithmetic (SU(3) FP32, periodic boundaries; otherwise shape 4).
  * All shapes compute the same operation sequence.  times_ms (optional,
  * 2*QG_TUNE_SHAPES floats): per shape v, [2v] heatbath and [2v+1]
  * overrelaxation ms/launch.                                               */
-#define QG_TUNE_SHAPES 5
+#define QG_TUNE_SHAPES 6
 int qg_tune(qg_ctx *ctx, int reps, float *times_ms);
 /* pin / read the launch shapes (0 .. QG_TUNE_SHAPES-1) without tuning     */
 int qg_set_shapes(qg_ctx *ctx, int heatbath_shape, int overrelax_shape);

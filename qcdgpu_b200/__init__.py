@@ -21,7 +21,7 @@ PRNG_RANLUX, PRNG_PHILOX = 0, 1
 LAYOUT_REFERENCE = 0
 HEATBATH, OVERRELAX = 0, 1
 MEAS_PLAQUETTE, MEAS_ACTION, MEAS_POLYAKOV, MEAS_WILSON = 0, 1, 2, 3
-TUNE_SHAPES = 5                     # QG_TUNE_SHAPES
+TUNE_SHAPES = 6                     # QG_TUNE_SHAPES
 NET_FEATURES, NET_HIDDEN, NET_PARAMS = 8, 32, 1377   # QG_NET_*
 
 EXPORTED_SYMBOLS = (

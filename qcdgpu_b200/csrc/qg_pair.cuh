@@ -1,0 +1,330 @@
+// qg_pair.cuh -- the SU(3) algebra of qg_su.cuh on pairs of links.
+//
+// Each value is a float2 holding the same quantity of two different links
+// (lane x = link 0, lane y = link 1), and every operation is the packed
+// FP32 instruction (__ffma2_rn / __fmul2_rn / __fadd2_rn) that performs, in
+// each lane, exactly the IEEE operation the scalar code performs in the
+// same order -- so a lane's result is bit-identical to the scalar path,
+// while one instruction issue does the work of two.  Negations are exact,
+// so fma(-a, b, c) is written with whichever operand is cheaper to negate.
+#pragma once
+#include "qg_su.cuh"
+
+namespace qg {
+
+using F2 = float2;
+__device__ __forceinline__ F2 pmul(F2 a, F2 b) { return __fmul2_rn(a, b); }
+__device__ __forceinline__ F2 pfma(F2 a, F2 b, F2 c) { return __ffma2_rn(a, b, c); }
+__device__ __forceinline__ F2 padd(F2 a, F2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ F2 pneg(F2 a) { return make_float2(-a.x, -a.y); }
+__device__ __forceinline__ F2 psub(F2 a, F2 b) { return __fadd2_rn(a, pneg(b)); }
+__device__ __forceinline__ F2 pair(float a, float b) { return make_float2(a, b); }
+
+struct CX2 { F2 re, im; };
+struct M32 { CX2 m[3][3]; };
+struct G32 { F2 uv1[4], uv2[4], uv3[4]; };     // the 12-real form, component-wise
+struct S22 { CX2 u1, u2, v1, v2; };
+
+__device__ __forceinline__ G32 gpair(const G3<float> &a, const G3<float> &b)
+{
+    G32 g;
+    g.uv1[0] = pair(a.uv1.x, b.uv1.x); g.uv1[1] = pair(a.uv1.y, b.uv1.y);
+    g.uv1[2] = pair(a.uv1.z, b.uv1.z); g.uv1[3] = pair(a.uv1.w, b.uv1.w);
+    g.uv2[0] = pair(a.uv2.x, b.uv2.x); g.uv2[1] = pair(a.uv2.y, b.uv2.y);
+    g.uv2[2] = pair(a.uv2.z, b.uv2.z); g.uv2[3] = pair(a.uv2.w, b.uv2.w);
+    g.uv3[0] = pair(a.uv3.x, b.uv3.x); g.uv3[1] = pair(a.uv3.y, b.uv3.y);
+    g.uv3[2] = pair(a.uv3.z, b.uv3.z); g.uv3[3] = pair(a.uv3.w, b.uv3.w);
+    return g;
+}
+__device__ __forceinline__ void gsplit(const G32 &g, G3<float> &a, G3<float> &b)
+{
+    a.uv1 = { g.uv1[0].x, g.uv1[1].x, g.uv1[2].x, g.uv1[3].x };
+    a.uv2 = { g.uv2[0].x, g.uv2[1].x, g.uv2[2].x, g.uv2[3].x };
+    a.uv3 = { g.uv3[0].x, g.uv3[1].x, g.uv3[2].x, g.uv3[3].x };
+    b.uv1 = { g.uv1[0].y, g.uv1[1].y, g.uv1[2].y, g.uv1[3].y };
+    b.uv2 = { g.uv2[0].y, g.uv2[1].y, g.uv2[2].y, g.uv2[3].y };
+    b.uv3 = { g.uv3[0].y, g.uv3[1].y, g.uv3[2].y, g.uv3[3].y };
+}
+
+// sum_k a_k b_k (dot3)
+__device__ __forceinline__ CX2 pdot3(const CX2 *a, int as, const CX2 *b, int bs)
+{
+    CX2 r;
+    r.re = pmul(a[0].re, b[0].re);
+    r.re = pfma(pneg(a[0].im), b[0].im, r.re);
+    r.im = pmul(a[0].re, b[0].im);
+    r.im = pfma(a[0].im, b[0].re, r.im);
+#pragma unroll
+    for (int k = 1; k < 3; k++) {
+        const CX2 &x = a[k * as], &y = b[k * bs];
+        r.re = pfma(x.re, y.re, r.re);
+        r.re = pfma(pneg(x.im), y.im, r.re);
+        r.im = pfma(x.re, y.im, r.im);
+        r.im = pfma(x.im, y.re, r.im);
+    }
+    return r;
+}
+// sum_k a_k conj(b_k) (dotc3)
+__device__ __forceinline__ CX2 pdotc3(const CX2 *a, int as, const CX2 *b, int bs)
+{
+    CX2 r;
+    r.re = pmul(a[0].re, b[0].re);
+    r.re = pfma(a[0].im, b[0].im, r.re);
+    r.im = pmul(a[0].im, b[0].re);
+    r.im = pfma(pneg(a[0].re), b[0].im, r.im);
+#pragma unroll
+    for (int k = 1; k < 3; k++) {
+        const CX2 &x = a[k * as], &y = b[k * bs];
+        r.re = pfma(x.re, y.re, r.re);
+        r.re = pfma(x.im, y.im, r.re);
+        r.im = pfma(x.im, y.re, r.im);
+        r.im = pfma(pneg(x.re), y.im, r.im);
+    }
+    return r;
+}
+// sum_k conj(a_k) b_k (cdot3)
+__device__ __forceinline__ CX2 pcdot3(const CX2 *a, int as, const CX2 *b, int bs)
+{
+    CX2 r;
+    r.re = pmul(a[0].re, b[0].re);
+    r.re = pfma(a[0].im, b[0].im, r.re);
+    r.im = pmul(a[0].re, b[0].im);
+    r.im = pfma(pneg(a[0].im), b[0].re, r.im);
+#pragma unroll
+    for (int k = 1; k < 3; k++) {
+        const CX2 &x = a[k * as], &y = b[k * bs];
+        r.re = pfma(x.re, y.re, r.re);
+        r.re = pfma(x.im, y.im, r.re);
+        r.im = pfma(x.re, y.im, r.im);
+        r.im = pfma(pneg(x.im), y.re, r.im);
+    }
+    return r;
+}
+
+// row 3 = conj(row1 x row2) (fill_row3)
+__device__ __forceinline__ void pfill_row3(M32 &a)
+{
+#pragma unroll
+    for (int j = 0; j < 3; j++) {
+        const int p = (j + 1) % 3, q = (j + 2) % 3;
+        const CX2 &u1 = a.m[0][p], &u2 = a.m[0][q], &v1 = a.m[1][p], &v2 = a.m[1][q];
+        F2 re = pmul(u1.re, v2.re);
+        re = pfma(pneg(u1.im), v2.im, re);
+        re = pfma(pneg(u2.re), v1.re, re);
+        re = pfma(u2.im, v1.im, re);
+        F2 im = pmul(u2.re, v1.im);
+        im = pfma(u2.im, v1.re, im);
+        im = pfma(pneg(u1.re), v2.im, im);
+        im = pfma(pneg(u1.im), v2.re, im);
+        a.m[2][j].re = re;
+        a.m[2][j].im = im;
+    }
+}
+
+__device__ __forceinline__ M32 pexpand(const G32 &g)
+{
+    M32 a;
+    a.m[0][0] = { g.uv1[0], g.uv2[0] }; a.m[0][1] = { g.uv1[1], g.uv2[1] }; a.m[0][2] = { g.uv1[2], g.uv2[2] };
+    a.m[1][0] = { g.uv3[0], g.uv3[2] }; a.m[1][1] = { g.uv3[1], g.uv3[3] }; a.m[1][2] = { g.uv1[3], g.uv2[3] };
+    pfill_row3(a);
+    return a;
+}
+__device__ __forceinline__ G32 pcompress(const M32 &a)
+{
+    G32 g;
+    g.uv1[0] = a.m[0][0].re; g.uv1[1] = a.m[0][1].re; g.uv1[2] = a.m[0][2].re; g.uv1[3] = a.m[1][2].re;
+    g.uv2[0] = a.m[0][0].im; g.uv2[1] = a.m[0][1].im; g.uv2[2] = a.m[0][2].im; g.uv2[3] = a.m[1][2].im;
+    g.uv3[0] = a.m[1][0].re; g.uv3[1] = a.m[1][1].re; g.uv3[2] = a.m[1][0].im; g.uv3[3] = a.m[1][1].im;
+    return g;
+}
+
+
+// staple terms (staple_fwd3 / staple_bwd3)
+__device__ __forceinline__ M32 pstaple_fwd3(const G32 &ga, const G32 &gb, const G32 &gc)
+{
+    M32 A = pexpand(ga), B = pexpand(gb), C = pexpand(gc), P, T;
+#pragma unroll
+    for (int i = 0; i < 2; i++)
+#pragma unroll
+        for (int j = 0; j < 3; j++) P.m[i][j] = pdotc3(&A.m[i][0], 1, &B.m[j][0], 1);
+#pragma unroll
+    for (int i = 0; i < 2; i++)
+#pragma unroll
+        for (int j = 0; j < 3; j++) T.m[i][j] = pdotc3(&P.m[i][0], 1, &C.m[j][0], 1);
+    pfill_row3(T);
+    return T;
+}
+__device__ __forceinline__ M32 pstaple_bwd3(const G32 &ga, const G32 &gb, const G32 &gc)
+{
+    M32 A = pexpand(ga), B = pexpand(gb), C = pexpand(gc), R, H, T;
+#pragma unroll
+    for (int i = 0; i < 2; i++)
+#pragma unroll
+        for (int j = 0; j < 3; j++) R.m[i][j] = pdot3(&B.m[i][0], 1, &A.m[0][j], 3);
+    pfill_row3(R);
+#pragma unroll
+    for (int i = 0; i < 2; i++)
+#pragma unroll
+        for (int j = 0; j < 3; j++) H.m[i][j] = pcdot3(&C.m[0][i], 3, &R.m[0][j], 3);
+    pfill_row3(H);
+#pragma unroll
+    for (int i = 0; i < 3; i++)
+#pragma unroll
+        for (int j = 0; j < 3; j++) T.m[i][j] = { H.m[j][i].re, pneg(H.m[j][i].im) };
+    return T;
+}
+__device__ __forceinline__ void padd3(M32 &r, const M32 &a, const M32 &b)
+{
+#pragma unroll
+    for (int i = 0; i < 3; i++)
+#pragma unroll
+        for (int j = 0; j < 3; j++) {
+            r.m[i][j].re = padd(a.m[i][j].re, b.m[i][j].re);
+            r.m[i][j].im = padd(a.m[i][j].im, b.m[i][j].im);
+        }
+}
+
+// per-lane 1 / sqrt(x) as the scalar code computes it ((Real)1 / sqrtf(x))
+__device__ __forceinline__ F2 prsqrt_div(F2 x) { return pair(1.0f / sqrtf(x.x), 1.0f / sqrtf(x.y)); }
+
+// the SU(2) reflection of a 2x2 block (or_step, with times2 / rec2)
+__device__ __forceinline__ void por_step(S22 &a)
+{
+    F2 hx = padd(a.u1.re, a.v2.re);
+    F2 hz = pneg(psub(a.u1.im, a.v2.im));
+    F2 hy = pneg(psub(a.u2.re, a.v1.re));
+    F2 hw = pneg(padd(a.u2.im, a.v1.im));
+    F2 n2 = pmul(hx, hx);
+    n2 = pfma(hy, hy, n2);
+    n2 = pfma(hz, hz, n2);
+    n2 = pfma(hw, hw, n2);
+    const F2 id = prsqrt_div(n2);
+    hx = pmul(hx, id); hz = pmul(hz, id); hy = pmul(hy, id); hw = pmul(hw, id);
+    // times2(aH, aH)
+    F2 ax = pmul(hx, hx); ax = pfma(pneg(hy), hy, ax); ax = pfma(pneg(hz), hz, ax); ax = pfma(pneg(hw), hw, ax);
+    F2 az = pmul(hx, hz); az = pfma(hz, hx, az); az = pfma(hy, hw, az); az = pfma(pneg(hw), hy, az);
+    F2 ay = pmul(hx, hy); ay = pfma(hy, hx, ay); ay = pfma(hw, hz, ay); ay = pfma(pneg(hz), hw, ay);
+    F2 aw = pmul(hx, hw); aw = pfma(hw, hx, aw); aw = pfma(hz, hy, aw); aw = pfma(pneg(hy), hz, aw);
+    // rec2
+    a.u1 = { ax, az }; a.u2 = { ay, aw };
+    a.v1 = { pneg(ay), aw }; a.v2 = { ax, pneg(az) };
+}
+
+// rows i, j of U <- V (rows i, j) (rotate_rows)
+__device__ __forceinline__ void protate_rows(M32 &U, int i, int j, const S22 &V)
+{
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+        const CX2 x = U.m[i][k], y = U.m[j][k];
+        F2 re = pmul(V.u1.re, x.re); re = pfma(pneg(V.u1.im), x.im, re); re = pfma(V.u2.re, y.re, re);
+        re = pfma(pneg(V.u2.im), y.im, re);
+        F2 im = pmul(V.u1.re, x.im); im = pfma(V.u1.im, x.re, im); im = pfma(V.u2.re, y.im, im);
+        im = pfma(V.u2.im, y.re, im);
+        F2 re2 = pmul(V.v1.re, x.re); re2 = pfma(pneg(V.v1.im), x.im, re2); re2 = pfma(V.v2.re, y.re, re2);
+        re2 = pfma(pneg(V.v2.im), y.im, re2);
+        F2 im2 = pmul(V.v1.re, x.im); im2 = pfma(V.v1.im, x.re, im2); im2 = pfma(V.v2.re, y.im, im2);
+        im2 = pfma(V.v2.im, y.re, im2);
+        U.m[i][k] = { re, im };
+        U.m[j][k] = { re2, im2 };
+    }
+}
+
+// Gram-Schmidt of rows 1, 2 in FP32 (gs3<float>)
+__device__ __forceinline__ G32 pgs3(const G32 &g)
+{
+    F2 u[3][2] = { { g.uv1[0], g.uv2[0] }, { g.uv1[1], g.uv2[1] }, { g.uv1[2], g.uv2[2] } };
+    F2 v[3][2] = { { g.uv3[0], g.uv3[2] }, { g.uv3[1], g.uv3[3] }, { g.uv1[3], g.uv2[3] } };
+    F2 n2 = pmul(u[0][0], u[0][0]);
+    n2 = pfma(u[0][1], u[0][1], n2);
+#pragma unroll
+    for (int k = 1; k < 3; k++) { n2 = pfma(u[k][0], u[k][0], n2); n2 = pfma(u[k][1], u[k][1], n2); }
+    const F2 inu = prsqrt_div(n2);
+#pragma unroll
+    for (int k = 0; k < 3; k++) { u[k][0] = pmul(u[k][0], inu); u[k][1] = pmul(u[k][1], inu); }
+    F2 sr = pmul(v[0][0], u[0][0]), si = pmul(v[0][1], u[0][0]);
+    sr = pfma(v[0][1], u[0][1], sr);
+    si = pfma(pneg(v[0][0]), u[0][1], si);
+#pragma unroll
+    for (int k = 1; k < 3; k++) {
+        sr = pfma(v[k][0], u[k][0], sr); sr = pfma(v[k][1], u[k][1], sr);
+        si = pfma(v[k][1], u[k][0], si); si = pfma(pneg(v[k][0]), u[k][1], si);
+    }
+    const F2 nsr = pneg(sr), nsi = pneg(si);
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+        F2 r = pfma(nsr, u[k][0], v[k][0]);
+        r = pfma(si, u[k][1], r);
+        F2 i = pfma(nsr, u[k][1], v[k][1]);
+        i = pfma(nsi, u[k][0], i);
+        v[k][0] = r; v[k][1] = i;
+    }
+    F2 m2 = pmul(v[0][0], v[0][0]);
+    m2 = pfma(v[0][1], v[0][1], m2);
+#pragma unroll
+    for (int k = 1; k < 3; k++) { m2 = pfma(v[k][0], v[k][0], m2); m2 = pfma(v[k][1], v[k][1], m2); }
+    const F2 inv = prsqrt_div(m2);
+#pragma unroll
+    for (int k = 0; k < 3; k++) { v[k][0] = pmul(v[k][0], inv); v[k][1] = pmul(v[k][1], inv); }
+    G32 r;
+    r.uv1[0] = u[0][0]; r.uv1[1] = u[1][0]; r.uv1[2] = u[2][0]; r.uv1[3] = v[2][0];
+    r.uv2[0] = u[0][1]; r.uv2[1] = u[1][1]; r.uv2[2] = u[2][1]; r.uv2[3] = v[2][1];
+    r.uv3[0] = v[0][0]; r.uv3[1] = v[1][0]; r.uv3[2] = v[0][1]; r.uv3[3] = v[1][1];
+    return r;
+}
+
+// Cabibbo-Marinari overrelaxation of a pair (cm3<float, true>)
+__device__ __forceinline__ G32 pcm3_or(const M32 &S, const G32 &m0, int nhitpar)
+{
+    G32 reslt = m0;
+    M32 U = pexpand(m0);
+    for (int n = 0; n < nhitpar; n++) {
+#pragma unroll
+        for (int sg = 0; sg < 3; sg++) {
+            const int i = (sg == 2) ? 1 : 0, j = (sg == 0) ? 1 : 2;
+            S22 r0;
+            r0.u1 = pdot3(&U.m[i][0], 1, &S.m[0][i], 3);
+            r0.u2 = pdot3(&U.m[i][0], 1, &S.m[0][j], 3);
+            r0.v1 = pdot3(&U.m[j][0], 1, &S.m[0][i], 3);
+            r0.v2 = pdot3(&U.m[j][0], 1, &S.m[0][j], 3);
+            por_step(r0);
+            protate_rows(U, i, j, r0);
+        }
+        reslt = pgs3(pcompress(U));
+        U = pexpand(reslt);
+    }
+    return reslt;
+}
+
+// ----------------------------------------------------- rows of one link
+// Pairing inside one link: lane x = row 0, lane y = row 1 of a matrix, the
+// other operand broadcast to both lanes (free in an FFMA2).  Each lane is
+// the scalar dotc3 / dot3 / cdot3 of its row, in the same order.
+__device__ __forceinline__ CX2 bcast(const CX<float> &a) { return { pair(a.re, a.re), pair(a.im, a.im) }; }
+
+// staple_fwd3 with rows 0, 1 of P = A B^+ and of T = P C^+ computed as pairs
+__device__ __forceinline__ M3<float> staple_fwd3_rows(const G3<float> &ga, const G3<float> &gb, const G3<float> &gc)
+{
+    const M3<float> B = expand(gb), C = expand(gc);
+    CX2 a[3];
+    a[0] = { pair(ga.uv1.x, ga.uv3.x), pair(ga.uv2.x, ga.uv3.z) };
+    a[1] = { pair(ga.uv1.y, ga.uv3.y), pair(ga.uv2.y, ga.uv3.w) };
+    a[2] = { pair(ga.uv1.z, ga.uv1.w), pair(ga.uv2.z, ga.uv2.w) };
+    CX2 pr[3];
+#pragma unroll
+    for (int j = 0; j < 3; j++) {
+        const CX2 b[3] = { bcast(B.m[j][0]), bcast(B.m[j][1]), bcast(B.m[j][2]) };
+        pr[j] = pdotc3(a, 1, b, 1);
+    }
+    M3<float> T;
+#pragma unroll
+    for (int j = 0; j < 3; j++) {
+        const CX2 c[3] = { bcast(C.m[j][0]), bcast(C.m[j][1]), bcast(C.m[j][2]) };
+        const CX2 t = pdotc3(pr, 1, c, 1);
+        T.m[0][j] = { t.re.x, t.im.x };
+        T.m[1][j] = { t.re.y, t.im.y };
+    }
+    fill_row3(T);
+    return T;
+}
+
+}  // namespace qg

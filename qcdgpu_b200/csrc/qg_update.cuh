@@ -7,6 +7,7 @@
 // su2_update_cl.cl:206-431).
 #pragma once
 #include "qg_internal.h"
+#include "qg_pair.cuh"
 
 namespace qg {
 
@@ -323,6 +324,55 @@ __global__ void __launch_bounds__(kPhaseBlock, MINB) k_phase(Field<Real> U, Geom
     phase_site<NC, Real, PMODE, OR, mu, STAGED>(U, G, A, t);
 }
 
+// Overrelaxation of two links per thread (t and t + ceil(half/2)) with the
+// packed FP32 algebra of qg_pair.cuh: each lane performs the scalar
+// kernel's operations in the same order (bit-identical results) while one
+// FFMA2 issue serves both links.  SU(3), FP32 links, periodic boundaries;
+// the running staple sum is kept as s2 = st + f_i (f_0 alone for the first
+// plane), then st = b_i + s2 -- the scalar order, with the first sum
+// written b_0 + f_0 (addition commutes exactly).
+template <int mu>
+__global__ void __launch_bounds__(kPhaseBlock, 1) k_phase_or_pair(Field<float> U, Geom G, PhaseArgs A)
+{
+    const uint32_t H = (G.half + 1) >> 1;
+    const uint32_t t0 = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t0 >= H) return;
+    uint32_t t1 = t0 + H;
+    const bool two = t1 < G.half;
+    if (!two) t1 = t0;
+    const int p = A.parity;
+    Crd c0 = lex2crd(G, 2 * t0);
+    if (parity_of(c0) != p) c0.y += 1;
+    Crd c1 = lex2crd(G, 2 * t1);
+    if (parity_of(c1) != p) c1.y += 1;
+    const Nbr n0 = neighbours(G, c0), n1 = neighbours(G, c1);
+    const uint32_t own0 = (uint32_t)p * G.cb + t0, opp0 = (uint32_t)(p ^ 1) * G.cb + t0;
+    const uint32_t own1 = (uint32_t)p * G.cb + t1, opp1 = (uint32_t)(p ^ 1) * G.cb + t1;
+    M32 st, s2;
+#pragma unroll 1
+    for (int i = 0; i < 3; i++) {
+        const int nu = nu_of(mu, i);
+        const int32_t dpn0 = pick4(n0.dp, nu), dpn1 = pick4(n1.dp, nu);
+        const int32_t dmn0 = pick4(n0.dm, nu), dmn1 = pick4(n1.dm, nu);
+        {
+            M32 fw = pstaple_fwd3(gpair(U.ldg3(nu, opp0 + n0.dp[mu]), U.ldg3(nu, opp1 + n1.dp[mu])),
+                                  gpair(U.ldg3(mu, opp0 + dpn0), U.ldg3(mu, opp1 + dpn1)),
+                                  gpair(U.ldg3(nu, own0), U.ldg3(nu, own1)));
+            if (i == 0) s2 = fw;
+            else padd3(s2, st, fw);
+        }
+        M32 bw = pstaple_bwd3(gpair(U.ldg3(nu, own0 + dmn0 + n0.dp[mu]), U.ldg3(nu, own1 + dmn1 + n1.dp[mu])),
+                              gpair(U.ldg3(mu, opp0 + dmn0), U.ldg3(mu, opp1 + dmn1)),
+                              gpair(U.ldg3(nu, opp0 + dmn0), U.ldg3(nu, opp1 + dmn1)));
+        padd3(st, bw, s2);
+    }
+    const G32 r = pcm3_or(st, gpair(U.ld3(mu, own0), U.ld3(mu, own1)), A.nhitpar);
+    G3<float> r0, r1;
+    gsplit(r, r0, r1);
+    U.st3(mu, own0, r0);
+    if (two) U.st3(mu, own1, r1);
+}
+
 template <typename Real>
 cudaError_t launch_phase_T(const Geom &G, void *links, int group, const PhaseArgs &a, cudaStream_t s)
 {
@@ -335,13 +385,27 @@ cudaError_t launch_phase_T(const Geom &G, void *links, int group, const PhaseArg
     // shapes 3, 4 stage the staple through shared memory where that form
     // exists (SU(3), FP32 links); elsewhere they run shapes 0, 1
     constexpr bool kStage = sizeof(Real) == 4;
+    // shape 5: overrelaxation two links per thread (SU(3), FP32, periodic);
+    // otherwise it runs shape 4
+    if constexpr (sizeof(Real) == 4) {
+        if (a.variant == 5 && group == 3 && pm == -1 && !a.twist) {
+            const unsigned nbp = ((G.half + 1) / 2 + bs - 1) / bs;
+            switch (a.dir) {
+            case 0: k_phase_or_pair<0><<<nbp, bs, 0, s>>>(U, G, a); break;
+            case 1: k_phase_or_pair<1><<<nbp, bs, 0, s>>>(U, G, a); break;
+            case 2: k_phase_or_pair<2><<<nbp, bs, 0, s>>>(U, G, a); break;
+            default: k_phase_or_pair<3><<<nbp, bs, 0, s>>>(U, G, a); break;
+            }
+            return cudaGetLastError();
+        }
+    }
 #define QG_LAUNCH2(NC, PM, OR, MU, MB, ST) k_phase<NC, Real, PM, OR, MU, MB, ST><<<nb, bs, 0, s>>>(U, G, a)
 #define QG_LAUNCH1(NC, PM, OR, MU)                                                  \
     do {                                                                            \
         if (a.variant == 1) QG_LAUNCH2(NC, PM, OR, MU, 5, false);                   \
         else if (a.variant == 2) QG_LAUNCH2(NC, PM, OR, MU, 6, false);              \
         else if (a.variant == 3) QG_LAUNCH2(NC, PM, OR, MU, 0, NC == 3 && kStage);  \
-        else if (a.variant == 4) QG_LAUNCH2(NC, PM, OR, MU, 5, NC == 3 && kStage);  \
+        else if (a.variant >= 4) QG_LAUNCH2(NC, PM, OR, MU, 5, NC == 3 && kStage);  \
         else QG_LAUNCH2(NC, PM, OR, MU, 0, false);                                  \
     } while (0)
 #define QG_LAUNCH(NC, PM, OR)                                     \
