@@ -296,13 +296,41 @@ __device__ __forceinline__ G32 pcm3_or(const M32 &S, const G32 &m0, int nhitpar)
 }
 
 // ----------------------------------------------------- rows of one link
-// Pairing inside one link: lane x = row 0, lane y = row 1 of a matrix, the
-// other operand broadcast to both lanes (free in an FFMA2).  Each lane is
-// the scalar dotc3 / dot3 / cdot3 of its row, in the same order.
+// Pairing inside one link: a CX2 holds two entries of the SAME matrix
+// (rows 0 and 1 of a column, or columns 0 and 1 of a row) and the other
+// factor of each product is one scalar broadcast to both lanes, which costs
+// the packed instruction nothing.  Every entry is still the scalar
+// dot3 / dotc3 / cdot3 of qg_su.cuh in the same order, so the staple terms
+// below equal staple_fwd3 / staple_bwd3 bit for bit.
 __device__ __forceinline__ CX2 bcast(const CX<float> &a) { return { pair(a.re, a.re), pair(a.im, a.im) }; }
+__device__ __forceinline__ CX2 cpair(const CX<float> &a, const CX<float> &b) { return { pair(a.re, b.re), pair(a.im, b.im) }; }
+__device__ __forceinline__ CX<float> lane0(const CX2 &a) { return { a.re.x, a.im.x }; }
+__device__ __forceinline__ CX<float> lane1(const CX2 &a) { return { a.re.y, a.im.y }; }
 
-// staple_fwd3 with rows 0, 1 of P = A B^+ and of T = P C^+ computed as pairs
-__device__ __forceinline__ M3<float> staple_fwd3_rows(const G3<float> &ga, const G3<float> &gb, const G3<float> &gc)
+// SU(3) matrix with rows 0, 1 held column-wise in pairs: r01[j] = (m0j, m1j)
+struct MR3 { CX2 r01[3]; CX<float> r2[3]; };
+
+__device__ __forceinline__ M3<float> mr_unpack(const MR3 &a)
+{
+    M3<float> m;
+#pragma unroll
+    for (int j = 0; j < 3; j++) { m.m[0][j] = lane0(a.r01[j]); m.m[1][j] = lane1(a.r01[j]); m.m[2][j] = a.r2[j]; }
+    return m;
+}
+// r = a + b entry-wise (add3)
+__device__ __forceinline__ void mr_add(MR3 &r, const MR3 &a, const MR3 &b)
+{
+#pragma unroll
+    for (int j = 0; j < 3; j++) {
+        r.r01[j].re = padd(a.r01[j].re, b.r01[j].re);
+        r.r01[j].im = padd(a.r01[j].im, b.r01[j].im);
+        r.r2[j].re = a.r2[j].re + b.r2[j].re;
+        r.r2[j].im = a.r2[j].im + b.r2[j].im;
+    }
+}
+
+// staple_fwd3: rows 0, 1 of P = A B^+ and of T = P C^+ in row pairs
+__device__ __forceinline__ MR3 staple_fwd3_rows(const G3<float> &ga, const G3<float> &gb, const G3<float> &gc)
 {
     const M3<float> B = expand(gb), C = expand(gc);
     CX2 a[3];
@@ -315,16 +343,108 @@ __device__ __forceinline__ M3<float> staple_fwd3_rows(const G3<float> &ga, const
         const CX2 b[3] = { bcast(B.m[j][0]), bcast(B.m[j][1]), bcast(B.m[j][2]) };
         pr[j] = pdotc3(a, 1, b, 1);
     }
-    M3<float> T;
+    MR3 T;
 #pragma unroll
     for (int j = 0; j < 3; j++) {
         const CX2 c[3] = { bcast(C.m[j][0]), bcast(C.m[j][1]), bcast(C.m[j][2]) };
-        const CX2 t = pdotc3(pr, 1, c, 1);
-        T.m[0][j] = { t.re.x, t.im.x };
-        T.m[1][j] = { t.re.y, t.im.y };
+        T.r01[j] = pdotc3(pr, 1, c, 1);
     }
-    fill_row3(T);
+    M3<float> t = mr_unpack(T);
+    fill_row3(t);
+#pragma unroll
+    for (int j = 0; j < 3; j++) T.r2[j] = t.m[2][j];
     return T;
+}
+
+// staple_bwd3 (T = H^+, H = C^+ R, R = B A): R and H computed with pairs
+// over columns 0, 1 (and H's column 2 with a pair over rows 0, 1), so that
+// the rows 0, 1 of T = H^+ come out as row pairs
+__device__ __forceinline__ MR3 staple_bwd3_rows(const G3<float> &ga, const G3<float> &gb, const G3<float> &gc)
+{
+    const M3<float> A = expand(ga), B = expand(gb), C = expand(gc);
+    // columns 0, 1 of A by rows: ac[k] = (A_k0, A_k1)
+    const CX2 ac[3] = { cpair(A.m[0][0], A.m[0][1]), cpair(A.m[1][0], A.m[1][1]), cpair(A.m[2][0], A.m[2][1]) };
+    M3<float> R;
+    CX2 rc[3];                                       // rc[k] = (R_k0, R_k1)
+#pragma unroll
+    for (int i = 0; i < 2; i++) {
+        const CX2 b[3] = { bcast(B.m[i][0]), bcast(B.m[i][1]), bcast(B.m[i][2]) };
+        rc[i] = pdot3(b, 1, ac, 1);
+        R.m[i][0] = lane0(rc[i]);
+        R.m[i][1] = lane1(rc[i]);
+        R.m[i][2] = dot3(&B.m[i][0], 1, &A.m[0][2], 3);
+    }
+    fill_row3(R);
+    rc[2] = cpair(R.m[2][0], R.m[2][1]);
+    MR3 T;
+    CX2 h[2];                                        // h[i] = (H_i0, H_i1)
+#pragma unroll
+    for (int i = 0; i < 2; i++) {
+        const CX2 c[3] = { bcast(C.m[0][i]), bcast(C.m[1][i]), bcast(C.m[2][i]) };
+        h[i] = pcdot3(c, 1, rc, 1);
+    }
+    // (H_02, H_12): pair over rows, C's columns 0, 1 by rows
+    const CX2 cc[3] = { cpair(C.m[0][0], C.m[0][1]), cpair(C.m[1][0], C.m[1][1]), cpair(C.m[2][0], C.m[2][1]) };
+    const CX2 r2[3] = { bcast(R.m[0][2]), bcast(R.m[1][2]), bcast(R.m[2][2]) };
+    const CX2 h2 = pcdot3(cc, 1, r2, 1);
+    M3<float> H;
+    H.m[0][0] = lane0(h[0]); H.m[0][1] = lane1(h[0]); H.m[0][2] = lane0(h2);
+    H.m[1][0] = lane0(h[1]); H.m[1][1] = lane1(h[1]); H.m[1][2] = lane1(h2);
+    fill_row3(H);
+    // T_ab = conj(H_ba): (T_0b, T_1b) = conj(H_b0, H_b1)
+    T.r01[0] = { h[0].re, pneg(h[0].im) };
+    T.r01[1] = { h[1].re, pneg(h[1].im) };
+    T.r01[2] = { pair(H.m[2][0].re, H.m[2][1].re), pair(-H.m[2][0].im, -H.m[2][1].im) };
+    T.r2[0] = { h2.re.x, -h2.im.x };
+    T.r2[1] = { h2.re.y, -h2.im.y };
+    T.r2[2] = { H.m[2][2].re, -H.m[2][2].im };
+    return T;
+}
+
+// cm3 with OR (unrolled subgroups) with the two rows of each subgroup in
+// pairs: the block's four dot products as two pair dots (rows i, j against
+// one staple column), the rotation of rows i, j as pair FMAs with the
+// block's coefficients paired (u1, v1), (u2, v2) and the old rows
+// broadcast.  Equal to cm3<float, true, Prn, false> bit for bit.
+__device__ __forceinline__ G3<float> cm3_or_rows(const M3<float> &S, const G3<float> &m0, int nhitpar)
+{
+    G3<float> reslt = m0;
+    M3<float> U = expand(m0);
+    for (int n = 0; n < nhitpar; n++) {
+#pragma unroll
+        for (int sg = 0; sg < 3; sg++) {
+            const int i = (sg == 2) ? 1 : 0, j = (sg == 0) ? 1 : 2;
+            CX2 a[3];
+#pragma unroll
+            for (int k = 0; k < 3; k++) a[k] = cpair(U.m[i][k], U.m[j][k]);
+            const CX2 si[3] = { bcast(S.m[0][i]), bcast(S.m[1][i]), bcast(S.m[2][i]) };
+            const CX2 sj[3] = { bcast(S.m[0][j]), bcast(S.m[1][j]), bcast(S.m[2][j]) };
+            const CX2 d1 = pdot3(a, 1, si, 1);        // (u1, v1)
+            const CX2 d2 = pdot3(a, 1, sj, 1);        // (u2, v2)
+            S2<float> r0;
+            r0.u1 = lane0(d1); r0.v1 = lane1(d1); r0.u2 = lane0(d2); r0.v2 = lane1(d2);
+            or_step(r0);
+            const F2 cr1 = pair(r0.u1.re, r0.v1.re), ci1 = pair(r0.u1.im, r0.v1.im);
+            const F2 cr2 = pair(r0.u2.re, r0.v2.re), ci2 = pair(r0.u2.im, r0.v2.im);
+#pragma unroll
+            for (int k = 0; k < 3; k++) {
+                const CX2 x = bcast(U.m[i][k]), y = bcast(U.m[j][k]);
+                F2 re = pmul(cr1, x.re);
+                re = pfma(pneg(ci1), x.im, re);
+                re = pfma(cr2, y.re, re);
+                re = pfma(pneg(ci2), y.im, re);
+                F2 im = pmul(cr1, x.im);
+                im = pfma(ci1, x.re, im);
+                im = pfma(cr2, y.im, im);
+                im = pfma(ci2, y.re, im);
+                U.m[i][k] = { re.x, im.x };
+                U.m[j][k] = { re.y, im.y };
+            }
+        }
+        reslt = gs3<float>(compress(U));
+        U = expand(reslt);
+    }
+    return reslt;
 }
 
 }  // namespace qg

@@ -206,31 +206,31 @@ __device__ __forceinline__ M3<float> staple3_staged(const Field<float> &U, const
     cp_async_commit();
     bwd_copy(nu_of(mu, 0));
     cp_async_commit();
-    M3<float> st, s2;
+    MR3 st, s2;
 #pragma unroll 1
     for (int i = 0; i < 3; i++) {
         const int nu = nu_of(mu, i);
         const int xnp = (nu == 0) ? n.xp : n.x, xnm = (nu == 0) ? n.xm : n.x;
         const int xnmmu = (nu == 0) ? n.xm : xmu;
         cp_async_wait<1>();
-        M3<float> fw = staple_fwd3(get(0, nu, xmu), get(3, mu, xnp), get(6, nu, n.x));
+        MR3 fw = staple_fwd3_rows(get(0, nu, xmu), get(3, mu, xnp), get(6, nu, n.x));
         if (i < 2) fwd_copy(nu_of(mu, i + 1));
         cp_async_commit();
         cp_async_wait<1>();
-        M3<float> bw = staple_bwd3(get(kTermSlots, nu, xnmmu), get(kTermSlots + 3, mu, xnm),
-                                   get(kTermSlots + 6, nu, xnm));
+        MR3 bw = staple_bwd3_rows(get(kTermSlots, nu, xnmmu), get(kTermSlots + 3, mu, xnm),
+                                  get(kTermSlots + 6, nu, xnm));
         if (i < 2) bwd_copy(nu_of(mu, i + 1));
         cp_async_commit();
         if (i == 0) {
-            add3(st, fw, bw);
+            mr_add(st, fw, bw);
         } else {
-            add3(s2, st, fw);
-            add3(st, bw, s2);
+            mr_add(s2, st, fw);
+            mr_add(st, bw, s2);
         }
     }
     cp_async_wait<0>();
     m0 = unstage_link(sb, kOwnSlot);
-    return st;
+    return mr_unpack(st);
 }
 
 // PRN source of thread t (PMODE 0 = RANLUX buffer, 1 = Philox, 2 = gid)
@@ -289,7 +289,11 @@ __device__ __forceinline__ void phase_site(const Field<Real> &U, const Geom &G, 
             st = staple3<mu>(U, G, t, nb, p, tw);
         }
         if (tw.on && mu == 1 && c.x == tw.xlast) m0 = twist3(m0, tw.phi, tw.omega);
-        G3<Real> mU = cm3<Real, OR, decltype(prn), STAGED && !OR>(st, m0, beta, prn, A.nhit, A.nhitpar);
+        G3<Real> mU;
+        if constexpr (STAGED && OR)
+            mU = cm3_or_rows(st, m0, A.nhitpar);
+        else
+            mU = cm3<Real, OR, decltype(prn), STAGED && !OR>(st, m0, beta, prn, A.nhit, A.nhitpar);
         U.st3(mu, e0, mU);
     } else {
         R4<Real> m0 = U.ld2(mu, e0);
