@@ -172,6 +172,33 @@ int qg_measure_wilson(qg_ctx *ctx, int R, int T, double *out);
  * links (traces summed in FP64; about 4x faster, relative error ~1e-6)  */
 int qg_measure_wilson_all(qg_ctx *ctx, int Rmax, int Tmax, int fp64_products, double *out);
 
+/* F_munu: the projections -i Tr(P T_a) of every plaquette P of three planes
+ * onto two group generators, summed over sites (the FMUNU / F0MU variants
+ * of lattice_measurement_plq, sun_measurements_cl.cl:712-1175, with
+ * trace_lambda1..8_double, su3_measurements_cl.cl:355-460, and
+ * trace_sigma1..3_double, su2_measurements_cl.cl:89-124).  field:
+ * QG_FMUNU_H = planes xy, xz, yz (chromomagnetic, key FMUNU), QG_FMUNU_E =
+ * xt, yt, zt (chromoelectric, key F0MU).  T_a = lambda_a / 2 (SU(3),
+ * a = 1..8; the reference offers index1 in {1,2,3,4}, default 3, and
+ * index2 in {5,6,7,8}, default 8) or sigma_a / 2 (SU(2), a = 1..3, real
+ * part only; reference: index1 3 or 1, index2 2).  out[12]: out[2p],
+ * out[2p+1] = Re, Im sum for index1 and plane p; out[6+2p], out[7+2p] for
+ * index2.  Normalise by the number of sites (suncl.cpp:1613-1670).
+ * Allocates its scratch on first use.                                      */
+#define QG_FMUNU_H 0
+#define QG_FMUNU_E 1
+int qg_measure_fmunu(qg_ctx *ctx, int field, int index1, int index2, double *out);
+/* Profiles along coordinate axis (0 x, 1 y, 2 z), out[2 n[axis]]:
+ * action: out[2i], out[2i+1] = sum over the sites with coordinate i of the
+ * spatial and temporal action (beta/N)(3N - ReTr) (lattice_action_diff_
+ * {x,y,z}, sun_measurements_cl.cl:187-615; normalise by 3 V / n[axis],
+ * suncl.cpp:1376-1481); Polyakov: out[2i], out[2i+1] = sum of Re, Im Tr P
+ * over the spatial sites with coordinate i (lattice_polyakov_diff_{x,y,z},
+ * polyakov.cl:142-402; normalise by N n1 n2 n3 / n[axis],
+ * suncl.cpp:1497-1586).  Allocate their scratch on first use.            */
+int qg_measure_action_profile(qg_ctx *ctx, int axis, double *out);
+int qg_measure_polyakov_profile(qg_ctx *ctx, int axis, double *out);
+
 /* buffer_init / buffer_map of the link table (clinterface.cpp:1296-1434):
  * host arrays in the reference layout, Real = float (precision 0) or
  * double (precision 1), qg_info.ref_elems elements.                       */
@@ -316,6 +343,7 @@ int qg_batch_info(qg_batch *b, uint64_t *total_sites, uint64_t *sweeps_done, uin
 #define QG_OBS_S_SPAT       9
 #define QG_OBS_S_TEMP      10
 #define QG_OBS_COUNT       11
+#define QG_FMUNU_COLS      16
 
 typedef struct qg_run_options {
     int iter;              /* ITER: measurements, the first on the start configuration */
@@ -337,6 +365,13 @@ typedef struct qg_run_options {
     int save_every_iter;   /* SAVEEVERY: also after every n-th measured iteration (0 off)*/
     char state_out[512];   /* STATEOUT: .qcg path written (empty: OUTPUTPATH + prefix + */
                            /* the reference's date-stamped name)                       */
+    int fmunu;             /* F_munu every measurement: 0 off (TURNOFFFMUNU), 1 planes   */
+                           /* xy,xz,yz (FMUNU), 2 planes xt,yt,zt (F0MU)               */
+    int fmunu_index1;      /* generator of the first F series: 0 = the reference's     */
+                           /* default 3 (FMUNU1/2/4 keys: 1, 2, 4)                     */
+    int fmunu_index2;      /* second: 0 = default 8 (SU(3), FMUNU5/6/7: 5..7), 2 (SU(2))*/
+    int get_actions_diff;  /* action profiles along x, y, z (ACTIONS_DIFF; the         */
+                           /* reference's get_actions_diff, set in its main())         */
 } qg_run_options;
 
 typedef struct qg_run_result {
@@ -355,6 +390,15 @@ typedef struct qg_run_result {
     double tau_int[QG_OBS_COUNT];
     double error[QG_OBS_COUNT];
     char state_file[640];            /* last .qcg written ("" if none)             */
+    /* F_munu series (when opts.fmunu): the reference's 16 columns in its
+     * order (DM_Fmunu_3 .. DM_Fmunu_abs_8_im, suncl.h:235-252): planes
+     * p0, p1, p2 of generator index1 (Re, Im each), the same for index2,
+     * then |F| = sqrt of the sum of squares over the planes (Re, Im) for
+     * index1 and index2; each normalised by the number of sites          */
+    double fmunu_mean[QG_FMUNU_COLS];
+    double fmunu_variance[QG_FMUNU_COLS];
+    double fmunu_gpu_last[QG_FMUNU_COLS];
+    double fmunu_cpu_last[QG_FMUNU_COLS];
 } qg_run_result;
 
 /* defaults of the reference main() (QCDGPU.cpp:183-205) */
@@ -362,12 +406,13 @@ int qg_default_run_options(qg_run_options *opts);
 /* Host only: read KEY = value lines ('#' starts a comment) and apply the
  * keys onto cfg / opts as lattice_get_init_file does.  Keys: GROUP ND L1..L4
  * LS LT ITER NITER NAV NHIT BETA PHI OMEGA INTS RANDSERIES PRNG OUTPUTPATH
- * GETWILSON GETRETRACE PL_LEVEL WILSONR WILSONT (reference) and PRECISION
+ * GETWILSON GETRETRACE PL_LEVEL WILSONR WILSONT FMUNU F0MU TURNOFFFMUNU
+ * FMUNU1 FMUNU2 FMUNU4 FMUNU5 FMUNU6 FMUNU7 (reference) and PRECISION
  * NHITPAR NOR REUNIT_EVERY REUNIT_FP64 PRNG_INSTANCES ROW_ALIGN INIT
- * STATEFILE SAVESTATE SAVEEVERY STATEOUT (this build; the reference sets
- * INIT and the state file name in main());
- * PLATFORM DEVICE FINISHPATH TURNOFFWAITING REBUILDBINARY and the F_munu
- * keys are accepted and ignored.  Unknown generators are an error.        */
+ * STATEFILE SAVESTATE SAVEEVERY STATEOUT ACTIONS_DIFF (this build; the
+ * reference sets INIT, the state file name and get_actions_diff in main());
+ * PLATFORM DEVICE FINISHPATH TURNOFFWAITING REBUILDBINARY are accepted and
+ * ignored.  Unknown generators are an error.                               */
 int qg_parse_init_file(const char *path, qg_config *cfg, qg_run_options *opts);
 /* lattice_init + lattice_simulate + LatticeCheckCPU + lattice_analysis +
  * lattice_write_results on the current CUDA device.  With opts->init == 0
@@ -408,6 +453,12 @@ typedef struct qg_run_state {
     double *plaquettes;     /* 2 per iteration: ReTr spatial, temporal       */
     double *wilson;         /* 1 per iteration                               */
     double *polyakov;       /* 4 per iteration: Re P, Im P, |P|^2, |P|^4     */
+    int fmunu, fmunu_index1, fmunu_index2, get_actions_diff;   /* as qg_run_options */
+    double *fmunu_series;   /* 12 per iteration: qg_measure_fmunu's out      */
+    /* per iteration: the Polyakov profiles along x, y, z (2 n1 + 2 n2 + 2 n3
+     * doubles, qg_measure_polyakov_profile's out) when pl_level > 2, then
+     * the action profiles (same length) when get_actions_diff            */
+    double *profiles;
 } qg_run_state;
 /* Host only: write a state file from a reference-layout link table
  * (links_bytes = qg_info.ref_elems * sizeof(Real)).                       */

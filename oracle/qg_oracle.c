@@ -218,6 +218,39 @@ static double cd_retr(const cd3 *a, int N)
     return s;
 }
 
+static inline int crd_get(crd o, int d) { return d == 0 ? o.x : d == 1 ? o.y : d == 2 ? o.z : o.t; }
+
+/* -i Tr(P T_a), T_a = lambda_a / 2 for SU(3) (a = 1..8; trace_lambda1..8_double,
+ * su3_measurements_cl.cl:355-460) or sigma_a / 2 for SU(2) (a = 1..3, real
+ * part only; trace_sigma1..3_double, su2_measurements_cl.cl:89-124), from
+ * the entries of P written out per generator; out = {Re, Im} */
+static void gen_proj(const cd3 *P, int N, int a, double out[2])
+{
+    const cdd u1 = P->m[0][0], u2 = P->m[0][1], u3 = P->m[0][2];
+    const cdd v1 = P->m[1][0], v2 = P->m[1][1], v3 = P->m[1][2];
+    const cdd w1 = P->m[2][0], w2 = P->m[2][1], w3 = P->m[2][2];
+    double re = 0, im = 0;
+    if (N == 2) {
+        re = a == 1 ? u2.im : a == 2 ? u2.re : u1.im;
+    } else {
+        switch (a) {
+        case 1: re = u2.im + v1.im; im = -u2.re - v1.re; break;
+        case 2: re = u2.re - v1.re; im = u2.im - v1.im; break;
+        case 3: re = u1.im - v2.im; im = -u1.re + v2.re; break;
+        case 4: re = u3.im + w1.im; im = -u3.re - w1.re; break;
+        case 5: re = u3.re - w1.re; im = u3.im - w1.im; break;
+        case 6: re = v3.im + w2.im; im = -v3.re - w2.re; break;
+        case 7: re = v3.re - w2.re; im = v3.im - w2.im; break;
+        default:
+            re = (u1.im + v2.im - 2.0 * w3.im) * 0.57735026918962576451;
+            im = (-u1.re - v2.re + 2.0 * w3.re) * 0.57735026918962576451;
+            break;
+        }
+        re /= 2; im /= 2;
+    }
+    out[0] = re; out[1] = im;
+}
+
 /* ======================================================= elementary functions */
 /* sin/cos for |x| < 16: Cody-Waite reduction by pi/2 (three-part constant)
  * and Taylor polynomials of degree 17 / 18 on [-pi/4, pi/4], Horner with
@@ -394,6 +427,18 @@ void ol_action(const ol_cfg *c, const void *t, double out[2])
 void ol_polyakov(const ol_cfg *c, const void *t, double out[4])
 {
     DISPATCH(polyakov_f(c, (const float *)t, out), polyakov_d(c, (const double *)t, out));
+}
+void ol_fmunu(const ol_cfg *c, const void *t, int field, int i1, int i2, double out[12])
+{
+    DISPATCH(fmunu_f(c, (const float *)t, field, i1, i2, out), fmunu_d(c, (const double *)t, field, i1, i2, out));
+}
+void ol_action_profile(const ol_cfg *c, const void *t, int axis, double *out)
+{
+    DISPATCH(action_profile_f(c, (const float *)t, axis, out), action_profile_d(c, (const double *)t, axis, out));
+}
+void ol_polyakov_profile(const ol_cfg *c, const void *t, int axis, double *out)
+{
+    DISPATCH(polyakov_profile_f(c, (const float *)t, axis, out), polyakov_profile_d(c, (const double *)t, axis, out));
 }
 double ol_wilson(const ol_cfg *c, const void *t, int R, int T)
 {

@@ -75,6 +75,14 @@ void ol_gramschmidt_fp64(const ol_cfg *c, void *table);   /* FP64 arithmetic */
 void ol_plaquette(const ol_cfg *c, const void *table, double out[2]);
 void ol_action(const ol_cfg *c, const void *table, double out[2]);
 void ol_polyakov(const ol_cfg *c, const void *table, double out[4]);
+/* F_munu projections of the plaquettes (field 0: xy, xz, yz; 1: xt, yt, zt)
+ * on generators i1, i2: out[2p], out[2p+1] = Re, Im sum over sites for i1
+ * and plane p, out[6+2p], out[7+2p] for i2 */
+void ol_fmunu(const ol_cfg *c, const void *table, int field, int i1, int i2, double out[12]);
+/* per slice of coordinate axis (0..2): spatial, temporal action sums */
+void ol_action_profile(const ol_cfg *c, const void *table, int axis, double *out);
+/* per slice of spatial coordinate axis (0..2): Re, Im Polyakov trace sums */
+void ol_polyakov_profile(const ol_cfg *c, const void *table, int axis, double *out);
 double ol_wilson(const ol_cfg *c, const void *table, int R, int T);
 double ol_local_action_link(const ol_cfg *c, const void *table, int gid, int dir);
 

@@ -806,6 +806,39 @@ static void FN(load_d)(const ol_cfg *c, const REAL *tab, const crd *co, int mu, 
     else FN(to_d2)(FN(load2)(c, tab, co, g, mu).uv1, out);
 }
 
+/* the plaquette matrix U_m(x) U_n(x+m) U_m(x+n)^+ U_n(x)^+ in FP64
+ * (lattice_retrace_plaquette3 / _F, su3_measurements_cl.cl:527-586) */
+static void FN(plaq_mat)(const ol_cfg *c, const REAL *tab, crd co, int m, int n, cd3 *w1)
+{
+    crd cm = nb_plus(c, co, m), cn = nb_plus(c, co, n);
+    cd3 a, b, d, e, w2, w3;
+    FN(load_d)(c, tab, &co, m, &a);
+    FN(load_d)(c, tab, &cm, n, &b);
+    FN(load_d)(c, tab, &cn, m, &d);
+    FN(load_d)(c, tab, &co, n, &e);
+    int N = c->group;
+    cd_mul(&a, &b, w1, N);
+    cd_herm(&d, &w2, N);
+    cd_mul(w1, &w2, &w3, N);
+    cd_herm(&e, &w2, N);
+    cd_mul(&w3, &w2, w1, N);
+}
+/* Re Tr of the spatial (xy, xz, yz) and temporal (xt, yt, zt) plaquettes
+ * of one site, summed in the reference order xy, xz, xt, yz, yt, zt
+ * (sun_measurements_cl.cl:1240-1305) */
+static void FN(plaq_site)(const ol_cfg *c, const REAL *tab, crd co, double *rs_out, double *rt_out)
+{
+    static const int pl[6][2] = { {0, 1}, {0, 2}, {0, 3}, {1, 2}, {1, 3}, {2, 3} };
+    double rs = 0, rt = 0;
+    for (int q = 0; q < 6; q++) {
+        cd3 w;
+        FN(plaq_mat)(c, tab, co, pl[q][0], pl[q][1], &w);
+        double tr = cd_retr(&w, c->group);
+        if (pl[q][1] == 3) rt += tr; else rs += tr;
+    }
+    *rs_out = rs; *rt_out = rt;
+}
+
 static void FN(plaquette)(const ol_cfg *c, const REAL *tab, double out[2], double *act_out)
 {
     int V = sites_of(c);
@@ -813,26 +846,8 @@ static void FN(plaquette)(const ol_cfg *c, const REAL *tab, double out[2], doubl
     REAL bet = (REAL)(c->beta / c->group);
     for (int g = 0; g < V; g++) {
         crd co; gid2c(c, g, &co);
-        double rs = 0, rt = 0;
-        /* planes in the reference order: xy, xz, xt, yz, yt, zt (sun_measurements_cl.cl:1240-1305) */
-        static const int pl[6][2] = { {0, 1}, {0, 2}, {0, 3}, {1, 2}, {1, 3}, {2, 3} };
-        for (int q = 0; q < 6; q++) {
-            int m = pl[q][0], n = pl[q][1];
-            crd cm = nb_plus(c, co, m), cn = nb_plus(c, co, n);
-            cd3 a, b, d, e, w1, w2, w3;
-            FN(load_d)(c, tab, &co, m, &a);
-            FN(load_d)(c, tab, &cm, n, &b);
-            FN(load_d)(c, tab, &cn, m, &d);
-            FN(load_d)(c, tab, &co, n, &e);
-            int N = c->group;
-            cd_mul(&a, &b, &w1, N);
-            cd_herm(&d, &w2, N);
-            cd_mul(&w1, &w2, &w3, N);
-            cd_herm(&e, &w2, N);
-            cd_mul(&w3, &w2, &w1, N);
-            double tr = cd_retr(&w1, N);
-            if (n == 3) rt += tr; else rs += tr;
-        }
+        double rs, rt;
+        FN(plaq_site)(c, tab, co, &rs, &rt);
         sp += rs; tp += rt;
         as += (double)bet * (3.0 * c->group - rs);
         at += (double)bet * (3.0 * c->group - rt);
@@ -841,40 +856,106 @@ static void FN(plaquette)(const ol_cfg *c, const REAL *tab, double out[2], doubl
     if (act_out) { act_out[0] = as; act_out[1] = at; }
 }
 
+/* lattice_action_diff_{x,y,z} (sun_measurements_cl.cl:187-615): the
+ * spatial and temporal action (beta/N)(3N - ReTr) summed over the sites of
+ * each slice of coordinate `axis`; out[2 i], out[2 i + 1] for slice i */
+static void FN(action_profile)(const ol_cfg *c, const REAL *tab, int axis, double *out)
+{
+    int V = sites_of(c);
+    REAL bet = (REAL)(c->beta / c->group);
+    memset(out, 0, sizeof(double) * 2 * c->n[axis]);
+    for (int g = 0; g < V; g++) {
+        crd co; gid2c(c, g, &co);
+        double rs, rt;
+        FN(plaq_site)(c, tab, co, &rs, &rt);
+        int k = crd_get(co, axis);
+        out[2 * k] += (double)bet * (3.0 * c->group - rs);
+        out[2 * k + 1] += (double)bet * (3.0 * c->group - rt);
+    }
+}
+
+/* F_munu (FMUNU / F0MU variants of lattice_measurement_plq,
+ * sun_measurements_cl.cl:712-1175): for the planes xy, xz, yz (field 0,
+ * chromomagnetic) or xt, yt, zt (field 1, chromoelectric) the projections
+ * -i Tr(P T_a) of the plaquette matrix P on the generators T = lambda/2
+ * (SU(3), index 1..8) or sigma/2 (SU(2), index 1..3), summed over sites:
+ * out[2 p], out[2 p + 1] = Re, Im for generator i1 and plane p,
+ * out[6 + 2 p], out[7 + 2 p] the same for i2 */
+static void FN(fmunu)(const ol_cfg *c, const REAL *tab, int field, int i1, int i2, double out[12])
+{
+    static const int hp[3][2] = { {0, 1}, {0, 2}, {1, 2} }, ep[3][2] = { {0, 3}, {1, 3}, {2, 3} };
+    int V = sites_of(c);
+    memset(out, 0, sizeof(double) * 12);
+    for (int g = 0; g < V; g++) {
+        crd co; gid2c(c, g, &co);
+        for (int p = 0; p < 3; p++) {
+            const int *pl = field ? ep[p] : hp[p];
+            cd3 w;
+            double f[2];
+            FN(plaq_mat)(c, tab, co, pl[0], pl[1], &w);
+            gen_proj(&w, c->group, i1, f);
+            out[2 * p] += f[0]; out[2 * p + 1] += f[1];
+            gen_proj(&w, c->group, i2, f);
+            out[6 + 2 * p] += f[0]; out[7 + 2 * p] += f[1];
+        }
+    }
+}
+
 /* lattice_polyakov, polyakov.cl:54-140: ordered product of N4 T-links in
  * REAL precision, Re/Im trace to double. */
+static void FN(poly_site)(const ol_cfg *c, const REAL *tab, int x, int y, int z, double *pr_out, double *pi_out)
+{
+    crd co = { x, y, z, 0 };
+    double pr, pi;
+    if (c->group == 3) {
+        M3 v0 = FN(expand)(FN(load3)(c, tab, &co, c2gid(c, co), 3));
+        for (int i = 1; i < c->n[3]; i++) {
+            co = nb_plus(c, co, 3);
+            M3 v1 = FN(expand)(FN(load3)(c, tab, &co, c2gid(c, co), 3));
+            v0 = FN(mul3)(&v0, &v1);
+        }
+        pr = (double)v0.m[0][0].re + (double)v0.m[1][1].re + (double)v0.m[2][2].re;
+        pi = (double)v0.m[0][0].im + (double)v0.m[1][1].im + (double)v0.m[2][2].im;
+    } else {
+        S2 v0 = FN(rec2)(FN(load2)(c, tab, &co, c2gid(c, co), 3).uv1);
+        for (int i = 1; i < c->n[3]; i++) {
+            co = nb_plus(c, co, 3);
+            S2 v1 = FN(rec2)(FN(load2)(c, tab, &co, c2gid(c, co), 3).uv1);
+            v0 = FN(mul2)(&v0, &v1);
+        }
+        pr = (double)v0.u1.re + (double)v0.v2.re;
+        pi = (double)v0.u1.im + (double)v0.v2.im;
+    }
+    *pr_out = pr; *pi_out = pi;
+}
 static void FN(polyakov)(const ol_cfg *c, const REAL *tab, double out[4])
 {
     double re = 0, im = 0, p2 = 0, p4 = 0;
     for (int x = 0; x < c->n[0]; x++)
         for (int z = 0; z < c->n[2]; z++)
             for (int y = 0; y < c->n[1]; y++) {
-                crd co = { x, y, z, 0 };
                 double pr, pi;
-                if (c->group == 3) {
-                    M3 v0 = FN(expand)(FN(load3)(c, tab, &co, c2gid(c, co), 3));
-                    for (int i = 1; i < c->n[3]; i++) {
-                        co = nb_plus(c, co, 3);
-                        M3 v1 = FN(expand)(FN(load3)(c, tab, &co, c2gid(c, co), 3));
-                        v0 = FN(mul3)(&v0, &v1);
-                    }
-                    pr = (double)v0.m[0][0].re + (double)v0.m[1][1].re + (double)v0.m[2][2].re;
-                    pi = (double)v0.m[0][0].im + (double)v0.m[1][1].im + (double)v0.m[2][2].im;
-                } else {
-                    S2 v0 = FN(rec2)(FN(load2)(c, tab, &co, c2gid(c, co), 3).uv1);
-                    for (int i = 1; i < c->n[3]; i++) {
-                        co = nb_plus(c, co, 3);
-                        S2 v1 = FN(rec2)(FN(load2)(c, tab, &co, c2gid(c, co), 3).uv1);
-                        v0 = FN(mul2)(&v0, &v1);
-                    }
-                    pr = (double)v0.u1.re + (double)v0.v2.re;
-                    pi = (double)v0.u1.im + (double)v0.v2.im;
-                }
+                FN(poly_site)(c, tab, x, y, z, &pr, &pi);
                 re += pr; im += pi;
                 double q2 = pr * pr + pi * pi;
                 p2 += q2; p4 += q2 * q2;
             }
     out[0] = re; out[1] = im; out[2] = p2; out[3] = p4;
+}
+/* lattice_polyakov_diff_{x,y,z} (polyakov.cl:142-402): Re, Im Tr of the
+ * Polyakov loop summed over the spatial sites of each slice of coordinate
+ * `axis` (0 x, 1 y, 2 z); out[2 i], out[2 i + 1] for slice i */
+static void FN(polyakov_profile)(const ol_cfg *c, const REAL *tab, int axis, double *out)
+{
+    memset(out, 0, sizeof(double) * 2 * c->n[axis]);
+    for (int x = 0; x < c->n[0]; x++)
+        for (int z = 0; z < c->n[2]; z++)
+            for (int y = 0; y < c->n[1]; y++) {
+                double pr, pi;
+                FN(poly_site)(c, tab, x, y, z, &pr, &pi);
+                int k = axis == 0 ? x : axis == 1 ? y : z;
+                out[2 * k] += pr; out[2 * k + 1] += pi;
+            }
 }
 
 /* lattice_measurement_wilson, wilson_loop.cl:55-454: for every site and

@@ -21,6 +21,8 @@ PRNG_RANLUX, PRNG_PHILOX = 0, 1
 LAYOUT_REFERENCE = 0
 HEATBATH, OVERRELAX = 0, 1
 MEAS_PLAQUETTE, MEAS_ACTION, MEAS_POLYAKOV, MEAS_WILSON = 0, 1, 2, 3
+FMUNU_H, FMUNU_E = 0, 1
+FMUNU_COLS = 16                     # QG_FMUNU_COLS
 TUNE_SHAPES = 6                     # QG_TUNE_SHAPES
 NET_FEATURES, NET_HIDDEN, NET_PARAMS = 8, 32, 1377   # QG_NET_*
 
@@ -34,7 +36,8 @@ EXPORTED_SYMBOLS = (
     "qg_write_state_file", "qg_read_state_file", "qg_save_state", "qg_tau_int",
     "qg_batch_create", "qg_batch_destroy", "qg_batch_init", "qg_batch_set_shape", "qg_batch_run", "qg_batch_sync",
     "qg_batch_get_stream", "qg_batch_series", "qg_batch_links_download", "qg_batch_info",
-    "qg_measure_wilson_all", "qg_net_set", "qg_net_get", "qg_mh_phase", "qg_mh_sweep", "qg_mh_stats", "qg_net_grad", "qg_net_train",
+    "qg_measure_wilson_all", "qg_measure_fmunu", "qg_measure_action_profile", "qg_measure_polyakov_profile",
+    "qg_net_set", "qg_net_get", "qg_mh_phase", "qg_mh_sweep", "qg_mh_stats", "qg_net_grad", "qg_net_train",
 )
 
 
@@ -100,6 +103,10 @@ class RunOptions(ctypes.Structure):
         ("save_state", ctypes.c_int),
         ("save_every_iter", ctypes.c_int),
         ("state_out", ctypes.c_char * 512),
+        ("fmunu", ctypes.c_int),
+        ("fmunu_index1", ctypes.c_int),
+        ("fmunu_index2", ctypes.c_int),
+        ("get_actions_diff", ctypes.c_int),
     ]
 
 
@@ -117,6 +124,10 @@ class RunResult(ctypes.Structure):
         ("tau_int", ctypes.c_double * 11),
         ("error", ctypes.c_double * 11),
         ("state_file", ctypes.c_char * 640),
+        ("fmunu_mean", ctypes.c_double * FMUNU_COLS),
+        ("fmunu_variance", ctypes.c_double * FMUNU_COLS),
+        ("fmunu_gpu_last", ctypes.c_double * FMUNU_COLS),
+        ("fmunu_cpu_last", ctypes.c_double * FMUNU_COLS),
     ]
 
 
@@ -145,6 +156,12 @@ class RunState(ctypes.Structure):
         ("plaquettes", ctypes.POINTER(ctypes.c_double)),
         ("wilson", ctypes.POINTER(ctypes.c_double)),
         ("polyakov", ctypes.POINTER(ctypes.c_double)),
+        ("fmunu", ctypes.c_int),
+        ("fmunu_index1", ctypes.c_int),
+        ("fmunu_index2", ctypes.c_int),
+        ("get_actions_diff", ctypes.c_int),
+        ("fmunu_series", ctypes.POINTER(ctypes.c_double)),
+        ("profiles", ctypes.POINTER(ctypes.c_double)),
     ]
 
 
@@ -184,6 +201,9 @@ def load_library(path=LIB_PATH):
     lib.qg_measure.argtypes = [vp, ctypes.c_int, P(ctypes.c_double)]
     lib.qg_measure_wilson.argtypes = [vp, ctypes.c_int, ctypes.c_int, P(ctypes.c_double)]
     lib.qg_measure_wilson_all.argtypes = [vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, P(ctypes.c_double)]
+    lib.qg_measure_fmunu.argtypes = [vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, P(ctypes.c_double)]
+    lib.qg_measure_action_profile.argtypes = [vp, ctypes.c_int, P(ctypes.c_double)]
+    lib.qg_measure_polyakov_profile.argtypes = [vp, ctypes.c_int, P(ctypes.c_double)]
     lib.qg_links_upload.argtypes = [vp, vp, ctypes.c_int]
     lib.qg_links_download.argtypes = [vp, vp, ctypes.c_int]
     lib.qg_set_phase_counter.argtypes = [vp, ctypes.c_uint64]
@@ -284,6 +304,14 @@ def tau_int(x, c=6.0):
     return t.value, w.value
 
 
+def profile_row(cfg, st):
+    """doubles per iteration of a run state's profile series: Polyakov
+    profiles along x, y, z when pl_level > 2, then the action profiles when
+    get_actions_diff"""
+    plen = 2 * (cfg.size[0] + cfg.size[1] + cfg.size[2])
+    return (plen if st.pl_level > 2 else 0) + (plen if st.get_actions_diff else 0)
+
+
 def read_state_file(path, cfg=None):
     """qg_read_state_file: (config, state, series dict, link table) of a .qcg
     file; the table is the reference layout (float32 / float64).  Host only."""
@@ -295,7 +323,8 @@ def read_state_file(path, cfg=None):
         raise QGError("qg_read_state_file: " + lib.qg_last_error(None).decode())
     n = max(st.iter, 1)
     ser = {"actions": np.zeros(2 * n), "plaquettes": np.zeros(2 * n), "wilson": np.zeros(n),
-           "polyakov": np.zeros(4 * n)}
+           "polyakov": np.zeros(4 * n), "fmunu_series": np.zeros(12 * n),
+           "profiles": np.zeros(profile_row(cfg, st) * n + 1)}
     dp = ctypes.POINTER(ctypes.c_double)
     for k, v in ser.items():
         setattr(st, k, v.ctypes.data_as(dp))
@@ -321,8 +350,9 @@ def write_state_file(path, cfg, st, table, series=None):
     series = dict(series or {})
     keep = {}
     dp = ctypes.POINTER(ctypes.c_double)
-    for k, m in (("actions", 2), ("plaquettes", 2), ("wilson", 1), ("polyakov", 4)):
-        v = np.ascontiguousarray(series.get(k, np.zeros(m * n)), dtype=np.float64)
+    for k, m in (("actions", 2), ("plaquettes", 2), ("wilson", 1), ("polyakov", 4), ("fmunu_series", 12),
+                 ("profiles", profile_row(cfg, st))):
+        v = np.ascontiguousarray(series.get(k, np.zeros(m * n + 1)), dtype=np.float64)
         keep[k] = v
         setattr(st, k, v.ctypes.data_as(dp))
     t = np.ascontiguousarray(table)
@@ -539,6 +569,33 @@ class Lattice:
                                                 out.ctypes.data_as(ctypes.POINTER(ctypes.c_double))),
                  "qg_measure_wilson_all")
         return out.reshape(Rmax, Tmax)
+
+    def fmunu(self, field=0, index1=None, index2=None):
+        """raw F_munu sums (qg_measure_fmunu): array [2 generators][3 planes]
+        [Re, Im]; field FMUNU_H (xy, xz, yz) or FMUNU_E (xt, yt, zt);
+        generators default to the reference's (3, 8) for SU(3), (3, 2) for
+        SU(2)"""
+        i1 = 3 if index1 is None else index1
+        i2 = (8 if self.cfg.group == 3 else 2) if index2 is None else index2
+        out = np.zeros(12)
+        self._ck(self.lib.qg_measure_fmunu(self.ctx, field, i1, i2, out.ctypes.data_as(ctypes.POINTER(ctypes.c_double))),
+                 "qg_measure_fmunu")
+        return out.reshape(2, 3, 2)
+
+    def action_profile(self, axis):
+        """raw per-slice (spatial, temporal) action sums along axis 0..2"""
+        out = np.zeros(2 * self.cfg.size[axis])
+        self._ck(self.lib.qg_measure_action_profile(self.ctx, axis, out.ctypes.data_as(ctypes.POINTER(ctypes.c_double))),
+                 "qg_measure_action_profile")
+        return out.reshape(-1, 2)
+
+    def polyakov_profile(self, axis):
+        """raw per-slice (Re, Im) Polyakov trace sums along axis 0..2"""
+        out = np.zeros(2 * self.cfg.size[axis])
+        self._ck(self.lib.qg_measure_polyakov_profile(self.ctx, axis,
+                                                      out.ctypes.data_as(ctypes.POINTER(ctypes.c_double))),
+                 "qg_measure_polyakov_profile")
+        return out.reshape(-1, 2)
 
     def wilson_sum(self, R=None, T=None):
         out = (ctypes.c_double * 1)()

@@ -44,6 +44,7 @@ struct qg_ctx {
     float *d_grad = nullptr, *d_gpart = nullptr;    // QG_NET_PARAMS + 4 stats; per-block partials
     double *d_wpart = nullptr, *d_wout = nullptr;   // all-loops Wilson measurement (lazy)
     int wpart_rmax = 0;
+    double *d_fpart = nullptr, *d_ppart = nullptr, *d_pout = nullptr;   // F_munu / profiles (lazy)
     unsigned long long *d_mh_acc = nullptr;
     double *d_mh_jump = nullptr;
     double eps_max = 0.0;
@@ -136,6 +137,7 @@ extern "C" int qg_destroy(qg_ctx *c)
     cudaFree(c->d_netw); cudaFree(c->d_master); cudaFree(c->d_adam_m); cudaFree(c->d_adam_v);
     cudaFree(c->d_grad); cudaFree(c->d_gpart); cudaFree(c->d_mh_acc); cudaFree(c->d_mh_jump);
     cudaFree(c->d_wpart); cudaFree(c->d_wout);
+    cudaFree(c->d_fpart); cudaFree(c->d_ppart); cudaFree(c->d_pout);
     if (c->h_results) cudaFreeHost(c->h_results);
     if (c->h_params) cudaFreeHost(c->h_params);
     if (c->stream) cudaStreamDestroy(c->stream);
@@ -822,6 +824,43 @@ extern "C" int qg_measure_wilson_all(qg_ctx *c, int Rmax, int Tmax, int fp64_pro
     QG_CK(cudaStreamSynchronize(c->stream), "wilson sync");
     return QG_OK;
 }
+
+extern "C" int qg_measure_fmunu(qg_ctx *c, int field, int index1, int index2, double *out)
+{
+    if (!c || !out) return QG_ERR_ARG;
+    const qg_config &f = c->cfg;
+    const int na = f.group == 3 ? 8 : 3;
+    if (field != QG_FMUNU_H && field != QG_FMUNU_E) return fail(c, QG_ERR_ARG, "field must be QG_FMUNU_H or QG_FMUNU_E");
+    if (index1 < 1 || index1 > na || index2 < 1 || index2 > na)
+        return fail(c, QG_ERR_ARG, "generator index out of range (1..8 for SU(3), 1..3 for SU(2))");
+    int tw = !(f.phi == 0.0 && f.omega == 0.0);
+    if (!c->d_fpart) QG_CK(cudaMalloc(&c->d_fpart, fmunu_partials(c->G) * sizeof(double)), "fmunu scratch");
+    if (!c->d_pout) QG_CK(cudaMalloc(&c->d_pout, 2 * 4096 * sizeof(double)), "measurement scratch");
+    QG_CK(launch_fmunu(c->G, c->links, f.group, f.precision, c->d_params, tw, field, index1, index2, c->d_fpart,
+                       c->d_pout, c->stream), "fmunu");
+    QG_CK(cudaMemcpyAsync(out, c->d_pout, 12 * sizeof(double), cudaMemcpyDeviceToHost, c->stream), "fmunu copy");
+    QG_CK(cudaStreamSynchronize(c->stream), "fmunu sync");
+    return QG_OK;
+}
+
+static int measure_profile(qg_ctx *c, int kind, int axis, double *out)
+{
+    if (!c || !out) return QG_ERR_ARG;
+    if (axis < 0 || axis > 2) return fail(c, QG_ERR_ARG, "profile axis must be 0 (x), 1 (y) or 2 (z)");
+    if (c->G.n[axis] > 4096) return fail(c, QG_ERR_ARG, "profile longer than 4096 slices");
+    const qg_config &f = c->cfg;
+    int tw = !(f.phi == 0.0 && f.omega == 0.0);
+    if (!c->d_ppart) QG_CK(cudaMalloc(&c->d_ppart, profile_partials(c->G) * sizeof(double)), "profile scratch");
+    if (!c->d_pout) QG_CK(cudaMalloc(&c->d_pout, 2 * 4096 * sizeof(double)), "measurement scratch");
+    QG_CK(launch_profile(c->G, c->links, f.group, f.precision, c->d_params, tw, kind, axis, c->d_ppart, c->d_pout,
+                         c->stream), "profile");
+    QG_CK(cudaMemcpyAsync(out, c->d_pout, 2 * (size_t)c->G.n[axis] * sizeof(double), cudaMemcpyDeviceToHost,
+                          c->stream), "profile copy");
+    QG_CK(cudaStreamSynchronize(c->stream), "profile sync");
+    return QG_OK;
+}
+extern "C" int qg_measure_action_profile(qg_ctx *c, int axis, double *out) { return measure_profile(c, 0, axis, out); }
+extern "C" int qg_measure_polyakov_profile(qg_ctx *c, int axis, double *out) { return measure_profile(c, 1, axis, out); }
 
 extern "C" int qg_measure(qg_ctx *c, int what, double *out)
 {

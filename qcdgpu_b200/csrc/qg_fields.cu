@@ -364,6 +364,118 @@ cudaError_t launch_polyakov(const Geom &G, const void *links, int group, int pre
     return launch_reduce(partials, nb, 4, out, s);
 }
 
+// F_munu (FMUNU / F0MU lattice_measurement_plq, sun_measurements_cl.cl:
+// 712-1175 and reduce_measurement_plq_double2 :1313-1357): 12 sums
+template <int NC, typename Real>
+__global__ void __launch_bounds__(256) k_fmunu(Field<Real> U, Geom G, const double *params, int twist, int field,
+                                                int i1, int i2, double *partials)
+{
+    uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+    double v[12] = { 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0 };
+    if (s < G.V) fmunu_site<NC, Real>(U, G, params, twist, s, field, i1, i2, v);
+    block_sum_store<12>(v, partials);
+}
+
+uint32_t fmunu_partials(const Geom &G) { return plaq_blocks(G) * 12; }
+
+cudaError_t launch_fmunu(const Geom &G, const void *links, int group, int prec, const double *params, int twist,
+                         int field, int i1, int i2, double *partials, double *out, cudaStream_t s)
+{
+    uint32_t nb = plaq_blocks(G);
+    if (prec) {
+        Field<double> U{ (double4 *)links, G.pstride };
+        if (group == 3) k_fmunu<3, double><<<nb, 256, 0, s>>>(U, G, params, twist, field, i1, i2, partials);
+        else k_fmunu<2, double><<<nb, 256, 0, s>>>(U, G, params, twist, field, i1, i2, partials);
+    } else {
+        Field<float> U{ (float4 *)links, G.pstride };
+        if (group == 3) k_fmunu<3, float><<<nb, 256, 0, s>>>(U, G, params, twist, field, i1, i2, partials);
+        else k_fmunu<2, float><<<nb, 256, 0, s>>>(U, G, params, twist, field, i1, i2, partials);
+    }
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    return launch_reduce(partials, nb, 12, out, s);
+}
+
+// Profiles along x, y or z (lattice_action_diff_{x,y,z},
+// sun_measurements_cl.cl:187-615 + reduce_action_diff_*_double2 :629-710;
+// lattice_polyakov_diff_{x,y,z}, polyakov.cl:142-402 + reduce :434-569):
+// block b covers kProfileChunk consecutive sites of slice b / chunks, and
+// the second pass sums each slice's chunks in order (deterministic).
+// KIND 0: spatial and temporal action over all sites of the slice;
+// KIND 1: Re, Im Polyakov trace over the spatial sites of the slice.
+constexpr uint32_t kProfileChunk = 1024;
+
+template <int NC, typename Real, int KIND>
+__global__ void __launch_bounds__(256) k_profile(Field<Real> U, Geom G, const double *params, int twist, int axis,
+                                                  uint32_t per_slice, uint32_t chunks, double *partials)
+{
+    const int k = (int)(blockIdx.x / chunks);
+    const uint32_t j0 = (blockIdx.x % chunks) * kProfileChunk;
+    const uint32_t j1 = min(per_slice, j0 + kProfileChunk);
+    double acc[2] = { 0, 0 };
+    for (uint32_t j = j0 + threadIdx.x; j < j1; j += blockDim.x) {
+        const Crd c = slice_site(G, axis, k, j, KIND == 1);
+        double v[4];
+        if (KIND == 0) {
+            plaq_site_c<NC, Real>(U, G, params, twist, c, v);
+            acc[0] += v[2]; acc[1] += v[3];
+        } else {
+            poly_site_c<NC, Real>(U, G, c, v);
+            acc[0] += v[0]; acc[1] += v[1];
+        }
+    }
+    block_sum_store<2>(acc, partials);
+}
+__global__ void __launch_bounds__(256) k_profile_reduce(const double *partials, uint32_t chunks, double *out)
+{
+    reduce_partials(partials + (size_t)blockIdx.x * chunks * 2, chunks, 2, out + 2 * blockIdx.x);
+}
+
+static uint32_t profile_per_slice(const Geom &G, int axis, int kind)
+{
+    uint32_t n = (uint32_t)G.n[0] * G.n[1] * G.n[2] * (kind == 0 ? G.n[3] : 1);
+    return n / (uint32_t)G.n[axis];
+}
+uint32_t profile_partials(const Geom &G)
+{
+    uint32_t m = 0;
+    for (int axis = 0; axis < 3; axis++)
+        for (int kind = 0; kind < 2; kind++) {
+            uint32_t chunks = (profile_per_slice(G, axis, kind) + kProfileChunk - 1) / kProfileChunk;
+            m = max(m, chunks * (uint32_t)G.n[axis] * 2);
+        }
+    return m;
+}
+
+template <int NC, typename Real>
+static void profile_kernel(int kind, uint32_t nb, const Field<Real> &U, const Geom &G, const double *params,
+                           int twist, int axis, uint32_t per, uint32_t chunks, double *partials, cudaStream_t s)
+{
+    if (kind == 0) k_profile<NC, Real, 0><<<nb, 256, 0, s>>>(U, G, params, twist, axis, per, chunks, partials);
+    else k_profile<NC, Real, 1><<<nb, 256, 0, s>>>(U, G, params, twist, axis, per, chunks, partials);
+}
+
+cudaError_t launch_profile(const Geom &G, const void *links, int group, int prec, const double *params, int twist,
+                           int kind, int axis, double *partials, double *out, cudaStream_t s)
+{
+    const uint32_t per = profile_per_slice(G, axis, kind);
+    const uint32_t chunks = (per + kProfileChunk - 1) / kProfileChunk;
+    const uint32_t nb = chunks * (uint32_t)G.n[axis];
+    if (prec) {
+        Field<double> U{ (double4 *)links, G.pstride };
+        if (group == 3) profile_kernel<3, double>(kind, nb, U, G, params, twist, axis, per, chunks, partials, s);
+        else profile_kernel<2, double>(kind, nb, U, G, params, twist, axis, per, chunks, partials, s);
+    } else {
+        Field<float> U{ (float4 *)links, G.pstride };
+        if (group == 3) profile_kernel<3, float>(kind, nb, U, G, params, twist, axis, per, chunks, partials, s);
+        else profile_kernel<2, float>(kind, nb, U, G, params, twist, axis, per, chunks, partials, s);
+    }
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    k_profile_reduce<<<G.n[axis], 256, 0, s>>>(partials, chunks, out);
+    return cudaGetLastError();
+}
+
 // lattice_measurement_wilson (wilson_loop.cl:55-454): per site and i in
 // {x,y,z}, Re Tr(L_t^T(x) L_i^R(x+T t) L_t^T(x+R i)^+ L_i^R(x)^+) in FP64
 template <int NC, typename Real>

@@ -123,7 +123,44 @@ double retr(const M &a, int N)
 }
 void shift(int x[4], int d, int s, const int n[4]) { x[d] = (x[d] + s + n[d]) % n[d]; }
 
-struct HostObs { double plq_s, plq_t, s_s, s_t, pre, pim, p2, p4, wilson; };
+struct HostObs { double plq_s, plq_t, s_s, s_t, pre, pim, p2, p4, wilson, f[12]; };
+
+// -i Tr(P T_a) with T_a = lambda_a / 2 (SU(3)) or sigma_a / 2 (SU(2))
+// (trace_lambda1..8_double, su3_measurements_cl.cl:355-460;
+// trace_sigma1..3_double, su2_measurements_cl.cl:89-124)
+void gen_proj(const M &P, int N, int a, double &re, double &im)
+{
+    const C u1 = P.m[0][0], u2 = P.m[0][1], u3 = P.m[0][2], v1 = P.m[1][0], v2 = P.m[1][1], v3 = P.m[1][2];
+    const C w1 = P.m[2][0], w2 = P.m[2][1], w3 = P.m[2][2];
+    re = 0; im = 0;
+    if (N == 2) { re = a == 1 ? u2.im : a == 2 ? u2.re : u1.im; return; }
+    switch (a) {
+    case 1: re = u2.im + v1.im; im = -u2.re - v1.re; break;
+    case 2: re = u2.re - v1.re; im = u2.im - v1.im; break;
+    case 3: re = u1.im - v2.im; im = -u1.re + v2.re; break;
+    case 4: re = u3.im + w1.im; im = -u3.re - w1.re; break;
+    case 5: re = u3.re - w1.re; im = u3.im - w1.im; break;
+    case 6: re = v3.im + w2.im; im = -v3.re - w2.re; break;
+    case 7: re = v3.re - w2.re; im = v3.im - w2.im; break;
+    default:
+        re = (u1.im + v2.im - 2.0 * w3.im) * 0.57735026918962576451;
+        im = (-u1.re - v2.re + 2.0 * w3.re) * 0.57735026918962576451;
+    }
+    re /= 2; im /= 2;
+}
+
+// model_lattice_init (suncl.cpp:2212-2230): the F_munu generators
+void fmunu_indices(int N, const qg_run_options &o, int &i1, int &i2)
+{
+    i1 = o.fmunu_index1; i2 = o.fmunu_index2;
+    if (N == 3) {
+        if (i1 != 1 && i1 != 2 && i1 != 4) i1 = 3;
+        if (i2 < 5 || i2 > 7) i2 = 8;
+    } else {
+        if (i1 != 1) i1 = 3;
+        i2 = 2;
+    }
+}
 
 HostObs host_measure(const Table &T, const qg_config &f, const qg_run_options &o)
 {
@@ -148,6 +185,16 @@ HostObs host_measure(const Table &T, const qg_config &f, const qg_run_options &o
                             M p = mul(mul(mul(T.link(x, mu, phi, om), T.link(a, nu, phi, om), N),
                                           dag(T.link(b, mu, phi, om), N), N), dag(T.link(x, nu, phi, om), N), N);
                             (nu == 3 ? rt : rs) += retr(p, N);
+                            if ((o.fmunu == 1 && nu != 3) || (o.fmunu == 2 && nu == 3)) {
+                                int i1, i2;
+                                fmunu_indices(N, o, i1, i2);
+                                const int pl = o.fmunu == 2 ? mu : (mu == 0 ? nu - 1 : 2);
+                                double re, im;
+                                gen_proj(p, N, i1, re, im);
+                                h.f[2 * pl] += re; h.f[2 * pl + 1] += im;
+                                gen_proj(p, N, i2, re, im);
+                                h.f[6 + 2 * pl] += re; h.f[7 + 2 * pl] += im;
+                            }
                         }
                     h.plq_s += rs; h.plq_t += rt;
                     h.s_s += bet * (3.0 * N - rs);
@@ -213,7 +260,7 @@ extern "C" int qg_default_run_options(qg_run_options *o)
     o->iter = 2;
     o->niter = 1;
     o->nav = 0;
-    o->pl_level = 2;
+    o->pl_level = 3;
     o->get_wilson = 0;
     o->get_plaquettes = 1;
     o->get_actions = 1;
@@ -292,11 +339,21 @@ extern "C" int qg_parse_init_file(const char *path, qg_config *cfg, qg_run_optio
         else if (key == "SAVESTATE") o->save_state = (int)iv;
         else if (key == "SAVEEVERY") o->save_every_iter = (int)iv;
         else if (key == "STATEOUT") snprintf(o->state_out, sizeof(o->state_out), "%s", val.c_str());
+        else if (key == "FMUNU") o->fmunu = 1;
+        else if (key == "F0MU") o->fmunu = 2;
+        else if (key == "TURNOFFFMUNU") o->fmunu = 0;
+        else if (key == "FMUNU1") o->fmunu_index1 = 1;
+        else if (key == "FMUNU2") o->fmunu_index1 = 2;
+        else if (key == "FMUNU4") o->fmunu_index1 = 4;
+        else if (key == "FMUNU5") o->fmunu_index2 = 5;
+        else if (key == "FMUNU6") o->fmunu_index2 = 6;
+        else if (key == "FMUNU7") o->fmunu_index2 = 7;
+        else if (key == "ACTIONS_DIFF") o->get_actions_diff = (int)iv;
         else if (key == "PLATFORM" || key == "DEVICE" || key == "FINISHPATH" || key == "TURNOFFWAITING" ||
-                 key == "REBUILDBINARY" || key == "TURNOFFFMUNU" || key == "FMUNU" || key == "F0MU" ||
-                 key.rfind("FMUNU", 0) == 0 || key == "N1") {
-            /* device selection, dispatcher handshake, OpenCL binaries and the
-               F_munu measurements have no role in this build */
+                 key == "REBUILDBINARY" || key.rfind("FMUNU", 0) == 0 || key == "N1") {
+            /* device selection, dispatcher handshake and OpenCL binaries have
+               no role in this build; FMUNU3, FMUNU8, ... select nothing in the
+               reference either */
         }
         else {
             fclose(fp);
@@ -330,6 +387,10 @@ extern "C" int qg_run(const qg_config *cfg_in, const qg_run_options *o_in, qg_ru
         opts.get_actions = rs.get_actions;
         opts.get_plaquettes = rs.get_plaquettes;
         opts.get_wilson = rs.get_wilson;
+        opts.fmunu = rs.fmunu;
+        opts.fmunu_index1 = rs.fmunu_index1;
+        opts.fmunu_index2 = rs.fmunu_index2;
+        opts.get_actions_diff = rs.get_actions_diff;
     }
     if (o->iter < 1 || o->niter < 0 || o->nav < 0) return host_fail(QG_ERR_ARG, "ITER >= 1, NITER >= 0, NAV >= 0");
     // raw lattice sums per measured iteration, the reference's buffers
@@ -339,6 +400,16 @@ extern "C" int qg_run(const qg_config *cfg_in, const qg_run_options *o_in, qg_ru
     rs.plaquettes = s_plq.data();
     rs.wilson = s_wil.data();
     rs.polyakov = s_pol.data();
+    // F_munu sums (12 per iteration) and the profiles along x, y, z
+    const size_t plen = 2 * (size_t)(cfg.size[0] + cfg.size[1] + cfg.size[2]);
+    const size_t poff = o->pl_level > 2 ? plen : 0;                 // action profiles after Polyakov's
+    const size_t prow = poff + (o->get_actions_diff ? plen : 0);
+    std::vector<double> s_f(12 * (size_t)o->iter, 0.0), s_prof(prow * (size_t)o->iter + 1, 0.0);
+    rs.fmunu_series = s_f.data();
+    rs.profiles = s_prof.data();
+    if (o->fmunu < 0 || o->fmunu > 2) return host_fail(QG_ERR_ARG, "fmunu must be 0 (off), 1 (FMUNU) or 2 (F0MU)");
+    int fi1, fi2;
+    fmunu_indices(cfg.group, *o, fi1, fi2);
     qg_ctx *ctx = nullptr;
     rc = qg_create(&cfg, &ctx);
     if (rc) return host_fail(rc, std::string("qg_create: ") + qg_last_error(nullptr));
@@ -384,6 +455,10 @@ extern "C" int qg_run(const qg_config *cfg_in, const qg_run_options *o_in, qg_ru
         rs.get_actions = o->get_actions;
         rs.get_plaquettes = o->get_plaquettes;
         rs.get_wilson = o->get_wilson;
+        rs.fmunu = o->fmunu;
+        rs.fmunu_index1 = fi1;
+        rs.fmunu_index2 = fi2;
+        rs.get_actions_diff = o->get_actions_diff;
     }
     time_t t_start = time(nullptr);
     auto measure = [&](int i) -> int {
@@ -404,6 +479,16 @@ extern "C" int qg_run(const qg_config *cfg_in, const qg_run_options *o_in, qg_ru
         if (o->pl_level > 0) {
             if ((r = qg_measure(ctx, QG_MEAS_POLYAKOV, a))) return r;
             for (int k = 0; k < 4; k++) s_pol[4 * i + k] = a[k];
+        }
+        if (o->fmunu && (r = qg_measure_fmunu(ctx, o->fmunu - 1, fi1, fi2, &s_f[12 * (size_t)i]))) return r;
+        size_t off = prow * (size_t)i;
+        for (int axis = 0; axis < 3 && o->pl_level > 2; axis++) {
+            if ((r = qg_measure_polyakov_profile(ctx, axis, &s_prof[off]))) return r;
+            off += 2 * (size_t)cfg.size[axis];
+        }
+        for (int axis = 0; axis < 3 && o->get_actions_diff; axis++) {
+            if ((r = qg_measure_action_profile(ctx, axis, &s_prof[off]))) return r;
+            off += 2 * (size_t)cfg.size[axis];
         }
         return QG_OK;
     };
@@ -486,6 +571,57 @@ extern "C" int qg_run(const qg_config *cfg_in, const qg_run_options *o_in, qg_ru
         if (n > 1) qg_tau_int(d[k].data() + 1, n, 6.0, &res->tau_int[k], &w);
         res->error[k] = n > 0 ? sqrt(2.0 * res->tau_int[k] * res->variance[k] / n) : 0.0;
     }
+    // the 16 F_munu columns (lattice_make_header2, suncl.cpp:1613-1670):
+    // planes of index1, planes of index2 (Re, Im), then |F| per generator
+    // (data_analysis_joint3: sqrt of the sum of squares over the planes)
+    auto fmunu_row = [&](const double *f, double *row) {
+        for (int k = 0; k < 12; k++) row[k] = f[k] / V;
+        for (int g = 0; g < 2; g++)
+            for (int ri = 0; ri < 2; ri++) {
+                double q = 0;
+                for (int p = 0; p < 3; p++) q += row[6 * g + 2 * p + ri] * row[6 * g + 2 * p + ri];
+                row[12 + 2 * g + ri] = sqrt(q);
+            }
+    };
+    std::vector<double> fd[QG_FMUNU_COLS];
+    if (o->fmunu) {
+        for (int i = 0; i < o->iter; i++) {
+            double row[QG_FMUNU_COLS];
+            fmunu_row(&s_f[12 * (size_t)i], row);
+            for (int k = 0; k < QG_FMUNU_COLS; k++) fd[k].push_back(row[k]);
+        }
+        for (int k = 0; k < QG_FMUNU_COLS; k++) {
+            mean_var(fd[k], res->fmunu_mean[k], res->fmunu_variance[k]);
+            res->fmunu_gpu_last[k] = fd[k].back();
+        }
+    }
+    // profiles (lattice_analysis_PL_diff / _Action_diff and their
+    // normalisations, suncl.cpp:1116-1260,1376-1612): per slice the mean and
+    // variance over samples 1..ITER-1 of the Polyakov loop (Re, Im, per
+    // spatial site / N) and of the total action (per plaquette)
+    struct Slice { double pl, pl_im, pl_var, pl_im_var, s, s_var; };
+    std::vector<Slice> prof[3];
+    for (int axis = 0; axis < 3; axis++) {
+        const int na = cfg.size[axis];
+        prof[axis].assign(na, Slice{ 0, 0, 0, 0, 0, 0 });
+        size_t aoff = 0;
+        for (int b = 0; b < axis; b++) aoff += 2 * (size_t)cfg.size[b];
+        for (int k = 0; k < na; k++) {
+            std::vector<double> re, im, st;
+            for (int i = 0; i < o->iter; i++) {
+                const double *row = &s_prof[prow * (size_t)i];
+                if (o->pl_level > 2) {
+                    re.push_back(row[aoff + 2 * k] / (N * nsp / na));
+                    im.push_back(row[aoff + 2 * k + 1] / (N * nsp / na));
+                }
+                if (o->get_actions_diff)
+                    st.push_back(0.5 * (row[poff + aoff + 2 * k] + row[poff + aoff + 2 * k + 1]) / (3.0 * V / na));
+            }
+            Slice &sl = prof[axis][k];
+            if (!re.empty()) { mean_var(re, sl.pl, sl.pl_var); mean_var(im, sl.pl_im, sl.pl_im_var); }
+            if (!st.empty()) mean_var(st, sl.s, sl.s_var);
+        }
+    }
     // LatticeCheckCPU: FP64 re-measurement of the final configuration
     if (o->verify) {
         std::vector<char> buf(info.ref_elems * (cfg.precision ? 8 : 4));
@@ -508,6 +644,11 @@ extern "C" int qg_run(const qg_config *cfg_in, const qg_run_options *o_in, qg_ru
         bool ok = true;
         for (int k = 0; k < QG_OBS_COUNT; k++)
             if (!d[k].empty()) ok = verify(res->gpu_last[k], res->cpu_last[k], cfg.precision == 0) && ok;
+        if (o->fmunu) {
+            fmunu_row(h.f, res->fmunu_cpu_last);
+            for (int k = 0; k < QG_FMUNU_COLS; k++)
+                ok = verify(res->fmunu_gpu_last[k], res->fmunu_cpu_last[k], cfg.precision == 0) && ok;
+        }
         res->verification_passed = ok ? 1 : 0;
     }
     qg_destroy(ctx);
@@ -542,6 +683,8 @@ extern "C" int qg_run(const qg_config *cfg_in, const qg_run_options *o_in, qg_ru
         fprintf(fp, " ***************************************************\n");
         fprintf(fp, " Wilson loop R               : %d\n", cfg.wilson_r);
         fprintf(fp, " Wilson loop T               : %d\n", cfg.wilson_t);
+        if (o->fmunu == 1) fprintf(fp, " FMUNU(%u, %u)\n", fi1, fi2);
+        if (o->fmunu == 2) fprintf(fp, " F0MU(%u, %u)\n", fi1, fi2);
         fprintf(fp, " BETA                        : %16.13e\n", cfg.beta);
         fprintf(fp, " PHI   (lambda_3)            : %16.13e\n", cfg.phi);
         fprintf(fp, " OMEGA (lambda_8)            : %16.13e\n", cfg.omega);
@@ -563,6 +706,30 @@ extern "C" int qg_run(const qg_config *cfg_in, const qg_run_options *o_in, qg_ru
             fprintf(fp, " Variance %-16s: % 16.13e\n", names[k], res->variance[k]);
         }
         fprintf(fp, " ***************************************************\n");
+        char fnames[QG_FMUNU_COLS][24];
+        {
+            static const char *xyz = "xyz";
+            static const int hp[3][2] = { { 0, 1 }, { 0, 2 }, { 1, 2 } };
+            for (int k = 0; k < 12; k++) {
+                const int p = (k % 6) / 2, idx = k < 6 ? fi1 : fi2;
+                const char *ri = (k & 1) ? "im" : "re";
+                if (o->fmunu == 2) snprintf(fnames[k], 24, "Fmunu_%ct_%u_%s", xyz[p], idx, ri);
+                else snprintf(fnames[k], 24, "Fmunu_%c%c_%u_%s", xyz[hp[p][0]], xyz[hp[p][1]], idx, ri);
+            }
+            for (int k = 12; k < QG_FMUNU_COLS; k++)
+                snprintf(fnames[k], 24, "Fmunu_abs_%1u_%s", k < 14 ? fi1 : fi2, (k & 1) ? "im" : "re");
+        }
+        if (o->fmunu) {
+            for (int k = 0; k < QG_FMUNU_COLS; k++) fprintf(fp, " Mean %-20s: % 16.13e\n", fnames[k], res->fmunu_mean[k]);
+            for (int k = 0; k < QG_FMUNU_COLS; k++)
+                fprintf(fp, " Variance %-16s: % 16.13e\n", fnames[k], res->fmunu_variance[k]);
+            fprintf(fp, " ***************************************************\n");
+            for (int k = 0; k < QG_FMUNU_COLS; k++) {
+                fprintf(fp, " GPU last %-16s: % 16.13e\n", fnames[k], res->fmunu_gpu_last[k]);
+                fprintf(fp, " CPU last %-16s: % 16.13e\n", fnames[k], res->fmunu_cpu_last[k]);
+            }
+            fprintf(fp, " ***************************************************\n");
+        }
         for (int k = 0; k <= QG_OBS_WILSON; k++) {
             fprintf(fp, " Tau_int %-17s: % 16.13e\n", names[k], res->tau_int[k]);
             fprintf(fp, " Error %-19s: % 16.13e\n", names[k], res->error[k]);
@@ -574,6 +741,38 @@ extern "C" int qg_run(const qg_config *cfg_in, const qg_run_options *o_in, qg_ru
         }
         if (res->verification_passed == 1) fprintf(fp, " *** Verification successfully passed! *************\n");
         else if (res->verification_passed == 0) fprintf(fp, " --- Verification failed! --------------------------\n");
+        // profile sections (lattice_write_results, suncl.cpp:1694-1791)
+        static const char *axis_name[3] = { "X", "Y", "Z" };
+        if (o->pl_level > 2) {
+            fprintf(fp, " ***************************************************\n");
+            fprintf(fp, "Differentiated Polyakov loop data (#, PL, PL_im, PL_variance, PL_im_variance):\n");
+            for (int a = 0; a < 3; a++) {
+                fprintf(fp, "\n%s              ", axis_name[a]);
+                for (int k = 0; k < cfg.size[a]; k++) fprintf(fp, "%2u                   ", (unsigned)k);
+                fprintf(fp, "\nPL             ");
+                for (const Slice &q : prof[a]) fprintf(fp, "% 16.13e ", q.pl);
+                fprintf(fp, "\nPL_im          ");
+                for (const Slice &q : prof[a]) fprintf(fp, "% 16.13e ", q.pl_im);
+                fprintf(fp, "\nPL_variance    ");
+                for (const Slice &q : prof[a]) fprintf(fp, "% 16.13e ", q.pl_var);
+                fprintf(fp, "\nPL_im_variance ");
+                for (const Slice &q : prof[a]) fprintf(fp, "% 16.13e ", q.pl_im_var);
+                fprintf(fp, "\n");
+            }
+        }
+        if (o->get_actions_diff) {
+            fprintf(fp, " ***************************************************\n");
+            fprintf(fp, "Differentiated S data (#, S_total, S_variance):\n");
+            for (int a = 0; a < 3; a++) {
+                fprintf(fp, "\n%s              ", axis_name[a]);
+                for (int k = 0; k < cfg.size[a]; k++) fprintf(fp, "%2u                   ", (unsigned)k);
+                fprintf(fp, "\nS             ");
+                for (const Slice &q : prof[a]) fprintf(fp, "% 16.13e ", q.s);
+                fprintf(fp, "\nS_variance    ");
+                for (const Slice &q : prof[a]) fprintf(fp, "% 16.13e ", q.s_var);
+                fprintf(fp, "\n");
+            }
+        }
         fprintf(fp, " ***************************************************\n");
         fprintf(fp, " Data fields:\n    #,  ");
         std::vector<int> cols;
@@ -583,10 +782,14 @@ extern "C" int qg_run(const qg_config *cfg_in, const qg_run_options *o_in, qg_ru
         if (o->pl_level > 0) { cols.push_back(QG_OBS_POLYAKOV); cols.push_back(QG_OBS_POLYAKOV_IM); }
         if (o->pl_level > 1) { cols.push_back(QG_OBS_POLYAKOV_P2); cols.push_back(QG_OBS_POLYAKOV_P4); }
         for (int k : cols) fprintf(fp, "%-21s ", names[k]);
+        if (o->fmunu)
+            for (int k = 0; k < QG_FMUNU_COLS; k++) fprintf(fp, "%-21s ", fnames[k]);
         fprintf(fp, "\n ***************************************************\n");
         for (int i = 0; i < o->iter; i++) {
             fprintf(fp, "%5i", i);
             for (int k : cols) fprintf(fp, " % 16.13e", d[k][i]);
+            if (o->fmunu)
+                for (int k = 0; k < QG_FMUNU_COLS; k++) fprintf(fp, " % 16.13e", fd[k][i]);
             fprintf(fp, "\n");
         }
         fclose(fp);

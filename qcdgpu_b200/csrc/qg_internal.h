@@ -50,6 +50,15 @@ cudaError_t launch_polyakov(const Geom &G, const void *links, int group, int pre
 cudaError_t launch_wilson(const Geom &G, const void *links, int group, int prec, int R, int T, const double *params,
                           int twist, double *partials, double *out, cudaStream_t s);
 cudaError_t launch_reduce(const double *partials, uint32_t nblocks, int ncomp, double *out, cudaStream_t s);
+// F_munu sums (12) of the plaquettes of field 0 (xy,xz,yz) / 1 (xt,yt,zt)
+uint32_t fmunu_partials(const Geom &G);
+cudaError_t launch_fmunu(const Geom &G, const void *links, int group, int prec, const double *params, int twist,
+                         int field, int i1, int i2, double *partials, double *out, cudaStream_t s);
+// per-slice sums along axis 0..2: kind 0 action (spatial, temporal), kind 1
+// Polyakov trace (Re, Im); out holds 2 n[axis] doubles
+uint32_t profile_partials(const Geom &G);
+cudaError_t launch_profile(const Geom &G, const void *links, int group, int prec, const double *params, int twist,
+                           int kind, int axis, double *partials, double *out, cudaStream_t s);
 int wilson_all_blocks(const Geom &G);
 size_t wilson_all_partials(int nbx, int Rmax);
 cudaError_t launch_wilson_all(const Geom &G, const void *links, int group, int prec, int Rmax, int Tmax,

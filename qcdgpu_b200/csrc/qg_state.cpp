@@ -43,6 +43,7 @@ const char *kPrefix = "QCDGPU";
 const char *kVersion = "1.5";                // QCDGPU.cpp:42, the version the reference writes
 const char *kExtTag = "B200";                // marks this build's header words 48-59
 const char *kTailTag = "QGP4";               // tagged |P|^2, |P|^4 block after the table
+const char *kProfTag = "QGPF";               // tagged block of the per-iteration profiles after it
 
 // header word indices (lattice_make_bin_header order)
 enum {
@@ -53,7 +54,7 @@ enum {
     W_FULL_SIZE, W_DOMAIN_SIZE = W_FULL_SIZE + 4,
     // this build
     W_EXT_TAG = 48, W_PRNG_KIND, W_PHASE_LO, W_PHASE_HI, W_SWEEPS_LO, W_SWEEPS_HI, W_NOR, W_REUNIT_EVERY,
-    W_REUNIT_FP64, W_NHITPAR, W_INSTANCES, W_ROW_ALIGN
+    W_REUNIT_FP64, W_NHITPAR, W_INSTANCES, W_ROW_ALIGN, W_FMUNU_KIND, W_ACTIONS_DIFF
 };
 
 // PRNG::convert_generator_to_uint (random.cpp:110-123): RANLUX0..4 = 2..6;
@@ -91,7 +92,7 @@ Sizes sizes_for(const qg_config &c, int iter)
     const uint64_t V = (uint64_t)c.size[0] * c.size[1] * c.size[2] * c.size[3];
     Sizes s;
     s.energies = align_up((uint64_t)(iter > 0 ? iter : 1), a);
-    s.energies_F = s.energies;                 // no F_munu in this build
+    s.energies_F = s.energies * 7;             // MODEL_energies_size: plaquettes + 6 F_munu series
     s.meas_F = align_up((V + 255) / 256, a);
     s.polyakov = s.energies;
     return s;
@@ -144,6 +145,9 @@ extern "C" int qg_write_state_file(const char *path, const qg_config *cfg, const
     h[W_OMEGA_LO] = lo_word(c.omega);
     h[W_OMEGA_HI] = hi_word(c.omega);
     h[W_PL_LEVEL] = (uint32_t)st->pl_level;
+    h[W_FMUNU1] = (uint32_t)st->fmunu_index1;
+    h[W_FMUNU2] = (uint32_t)st->fmunu_index2;
+    h[W_GET_FMUNU] = st->fmunu == 1 ? 1 : 0;
     h[W_GET_ACTIONS] = st->get_actions ? 1 : 0;
     h[W_GET_PLAQUETTES] = st->get_plaquettes ? 1 : 0;
     h[W_GET_WILSON] = st->get_wilson ? 1 : 0;
@@ -166,6 +170,8 @@ extern "C" int qg_write_state_file(const char *path, const qg_config *cfg, const
     h[W_NHITPAR] = (uint32_t)c.nhitpar;
     h[W_INSTANCES] = (uint32_t)c.prng_instances;
     h[W_ROW_ALIGN] = (uint32_t)c.row_align;
+    h[W_FMUNU_KIND] = (uint32_t)st->fmunu;
+    h[W_ACTIONS_DIFF] = (uint32_t)st->get_actions_diff;
 
     // series buffers, in the reference's element order (double2 .x/.y as
     // lattice_analysis reads them: S_spat/S_temp, Plq_spat/Plq_temp, Re/Im)
@@ -173,9 +179,22 @@ extern "C" int qg_write_state_file(const char *path, const qg_config *cfg, const
     std::vector<double> meas(2 * (size_t)z.meas_F, 0.0), en(2 * (size_t)z.energies, 0.0),
         plq(2 * (size_t)z.energies_F, 0.0), wil((size_t)z.energies, 0.0), pol(2 * (size_t)z.polyakov, 0.0),
         p24(2 * (size_t)z.polyakov, 0.0);
+    // the per-iteration profile rows (this build's tail block)
+    const size_t plen = 2 * (size_t)(c.size[0] + c.size[1] + c.size[2]);
+    const size_t prow = (st->pl_level > 2 ? plen : 0) + (st->get_actions_diff ? plen : 0);
+    std::vector<double> prof(prow * (size_t)z.energies, 0.0);   // rows: the series' aligned length
     for (int i = 0; i < n; i++) {
         if (st->actions) { en[2 * i] = st->actions[2 * i]; en[2 * i + 1] = st->actions[2 * i + 1]; }
         if (st->plaquettes) { plq[2 * i] = st->plaquettes[2 * i]; plq[2 * i + 1] = st->plaquettes[2 * i + 1]; }
+        // F_munu in energies_plq blocks 1..6 (reduce_measurement_plq_double2,
+        // sun_measurements_cl.cl:1313-1357): index1 planes, then index2
+        if (st->fmunu && st->fmunu_series)
+            for (int k = 0; k < 6; k++) {
+                plq[2 * ((size_t)(k + 1) * z.energies + i)] = st->fmunu_series[12 * i + 2 * k];
+                plq[2 * ((size_t)(k + 1) * z.energies + i) + 1] = st->fmunu_series[12 * i + 2 * k + 1];
+            }
+        if (prow && st->profiles)
+            for (size_t k = 0; k < prow; k++) prof[prow * i + k] = st->profiles[prow * i + k];
         if (st->wilson) wil[i] = st->wilson[i];
         if (st->polyakov) {
             pol[2 * i] = st->polyakov[4 * i];
@@ -189,7 +208,7 @@ extern "C" int qg_write_state_file(const char *path, const qg_config *cfg, const
     bool ok = fwrite(h, sizeof(uint32_t), QCDGPU_STATE_HEADER_WORDS, fp) == QCDGPU_STATE_HEADER_WORDS;
     ok = ok && fwrite(meas.data(), sizeof(double), meas.size(), fp) == meas.size();
     ok = ok && fwrite(en.data(), sizeof(double), en.size(), fp) == en.size();
-    if (st->get_plaquettes) ok = ok && fwrite(plq.data(), sizeof(double), plq.size(), fp) == plq.size();
+    if (st->get_plaquettes || st->fmunu) ok = ok && fwrite(plq.data(), sizeof(double), plq.size(), fp) == plq.size();
     if (st->get_wilson) ok = ok && fwrite(wil.data(), sizeof(double), wil.size(), fp) == wil.size();
     if (st->pl_level > 0) ok = ok && fwrite(pol.data(), sizeof(double), pol.size(), fp) == pol.size();
     ok = ok && fwrite(links, 1, (size_t)links_bytes, fp) == (size_t)links_bytes;
@@ -197,6 +216,11 @@ extern "C" int qg_write_state_file(const char *path, const qg_config *cfg, const
         const uint32_t tag = str_word(kTailTag, 0);
         ok = ok && fwrite(&tag, sizeof(tag), 1, fp) == 1;
         ok = ok && fwrite(p24.data(), sizeof(double), p24.size(), fp) == p24.size();
+    }
+    if (prow) {
+        const uint32_t tag = str_word(kProfTag, 0);
+        ok = ok && fwrite(&tag, sizeof(tag), 1, fp) == 1;
+        ok = ok && fwrite(prof.data(), sizeof(double), prof.size(), fp) == prof.size();
     }
     if (fclose(fp) != 0) ok = false;
     if (!ok) return st_fail(QG_ERR_IO, std::string("short write to ") + path);
@@ -248,6 +272,10 @@ extern "C" int qg_read_state_file(const char *path, qg_config *cfg, qg_run_state
     st->get_actions = (int)h[W_GET_ACTIONS];
     st->get_plaquettes = (int)h[W_GET_PLAQUETTES];
     st->get_wilson = (int)h[W_GET_WILSON];
+    st->fmunu = h[W_GET_FMUNU] ? 1 : 0;
+    st->fmunu_index1 = (int)h[W_FMUNU1];
+    st->fmunu_index2 = (int)h[W_FMUNU2];
+    st->get_actions_diff = 0;
     st->phase_counter = 0;
     st->sweeps_done = 0;
     const bool ext = h[W_EXT_TAG] == str_word(kExtTag, 0);
@@ -261,6 +289,8 @@ extern "C" int qg_read_state_file(const char *path, qg_config *cfg, qg_run_state
         c.nhitpar = (int)h[W_NHITPAR];
         c.prng_instances = (int)h[W_INSTANCES];
         c.row_align = (int)h[W_ROW_ALIGN];
+        st->fmunu = (int)h[W_FMUNU_KIND];
+        st->get_actions_diff = (int)h[W_ACTIONS_DIFF];
     } else {
         // a file of the reference: every sweep ends with a Gram-Schmidt pass
         c.n_or = 0;
@@ -270,7 +300,8 @@ extern "C" int qg_read_state_file(const char *path, qg_config *cfg, qg_run_state
     }
     const uint32_t meas_F = h[W_MEAS_SIZE_F], en_n = h[W_ENERGIES_SIZE], en_F = h[W_ENERGIES_SIZE_F],
                    pol_n = h[W_POLYAKOV_SIZE];
-    const bool want = links || st->actions || st->plaquettes || st->wilson || st->polyakov;
+    const bool want = links || st->actions || st->plaquettes || st->wilson || st->polyakov || st->fmunu_series ||
+                      st->profiles;
     if (!want) { fclose(fp); return QG_OK; }
     const int n = st->iter_counter < st->iter ? st->iter_counter : st->iter;
     if ((uint32_t)n > en_n || (uint32_t)n > pol_n || (uint32_t)n > en_F) {
@@ -283,7 +314,7 @@ extern "C" int qg_read_state_file(const char *path, qg_config *cfg, qg_run_state
     };
     std::vector<double> meas, en, plq, wil, pol;
     bool ok = rd(meas, 2 * (size_t)meas_F) && rd(en, 2 * (size_t)en_n);
-    if (ok && st->get_plaquettes) ok = rd(plq, 2 * (size_t)en_F);
+    if (ok && (st->get_plaquettes || st->fmunu)) ok = rd(plq, 2 * (size_t)en_F);
     if (ok && st->get_wilson) ok = rd(wil, (size_t)en_n);
     if (ok && st->pl_level > 0) ok = rd(pol, 2 * (size_t)pol_n);
     const size_t real = c.precision ? 8 : 4;
@@ -299,11 +330,16 @@ extern "C" int qg_read_state_file(const char *path, qg_config *cfg, qg_run_state
     } else if (ok) {
         ok = fseek(fp, (long)table_bytes, SEEK_CUR) == 0;
     }
-    std::vector<double> p24;
-    if (ok && st->pl_level > 0) {
-        uint32_t tag = 0;
-        if (fread(&tag, sizeof(tag), 1, fp) == 1 && tag == str_word(kTailTag, 0)) ok = rd(p24, 2 * (size_t)pol_n);
+    std::vector<double> p24, prof;
+    const size_t plen = 2 * (size_t)(c.size[0] + c.size[1] + c.size[2]);
+    const size_t prow = (st->pl_level > 2 ? plen : 0) + (st->get_actions_diff ? plen : 0);
+    uint32_t tag = 0;
+    bool have_tag = ok && fread(&tag, sizeof(tag), 1, fp) == 1;
+    if (have_tag && tag == str_word(kTailTag, 0)) {
+        ok = rd(p24, 2 * (size_t)pol_n);
+        have_tag = ok && fread(&tag, sizeof(tag), 1, fp) == 1;
     }
+    if (have_tag && tag == str_word(kProfTag, 0) && prow) ok = rd(prof, prow * (size_t)en_n);
     fclose(fp);
     if (!ok) return st_fail(QG_ERR_IO, std::string("truncated state file ") + path);
     for (int i = 0; i < n; i++) {
@@ -316,6 +352,13 @@ extern "C" int qg_read_state_file(const char *path, qg_config *cfg, qg_run_state
             st->polyakov[4 * i + 2] = p24.empty() ? 0.0 : p24[2 * i];
             st->polyakov[4 * i + 3] = p24.empty() ? 0.0 : p24[2 * i + 1];
         }
+        if (st->fmunu_series && st->fmunu && (size_t)en_F >= 7 * (size_t)en_n)
+            for (int k = 0; k < 6; k++) {
+                st->fmunu_series[12 * i + 2 * k] = plq[2 * ((size_t)(k + 1) * en_n + i)];
+                st->fmunu_series[12 * i + 2 * k + 1] = plq[2 * ((size_t)(k + 1) * en_n + i) + 1];
+            }
+        if (st->profiles && !prof.empty())
+            for (size_t k = 0; k < prow; k++) st->profiles[prow * i + k] = prof[prow * i + k];
     }
     return QG_OK;
 }

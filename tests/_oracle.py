@@ -66,6 +66,9 @@ def _load():
     lib.ol_action.argtypes = [P(Cfg), ctypes.c_void_p, P(ctypes.c_double)]
     lib.ol_polyakov.argtypes = [P(Cfg), ctypes.c_void_p, P(ctypes.c_double)]
     lib.ol_wilson.argtypes = [P(Cfg), ctypes.c_void_p, ctypes.c_int, ctypes.c_int]
+    lib.ol_fmunu.argtypes = [P(Cfg), ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int, P(ctypes.c_double)]
+    lib.ol_action_profile.argtypes = [P(Cfg), ctypes.c_void_p, ctypes.c_int, P(ctypes.c_double)]
+    lib.ol_polyakov_profile.argtypes = [P(Cfg), ctypes.c_void_p, ctypes.c_int, P(ctypes.c_double)]
     lib.ol_wilson.restype = ctypes.c_double
     lib.ol_local_action_link.argtypes = [P(Cfg), ctypes.c_void_p, ctypes.c_int, ctypes.c_int]
     lib.ol_local_action_link.restype = ctypes.c_double
@@ -186,6 +189,25 @@ def polyakov(c, tab):
 
 def wilson(c, tab, R, T):
     return lib.ol_wilson(ctypes.byref(c), vp(tab), R, T)
+
+
+def fmunu(c, tab, field, i1, i2):
+    """F_munu sums as array [2 generators][3 planes][Re, Im]"""
+    out = (ctypes.c_double * 12)()
+    lib.ol_fmunu(ctypes.byref(c), vp(tab), field, i1, i2, out)
+    return np.array(out[:]).reshape(2, 3, 2)
+
+
+def action_profile(c, tab, axis):
+    out = (ctypes.c_double * (2 * c.n[axis]))()
+    lib.ol_action_profile(ctypes.byref(c), vp(tab), axis, out)
+    return np.array(out[:]).reshape(-1, 2)
+
+
+def polyakov_profile(c, tab, axis):
+    out = (ctypes.c_double * (2 * c.n[axis]))()
+    lib.ol_polyakov_profile(ctypes.byref(c), vp(tab), axis, out)
+    return np.array(out[:]).reshape(-1, 2)
 
 
 def philox(ctr, key):

@@ -413,3 +413,58 @@ def test_wilson_all_loops_match_single_loops_and_oracle(group, precision):
     with pytest.raises(Q.QGError):
         L.wilson_all(4, 17)
     L.close()
+
+
+# ------------------------------------------------ F_munu and profiles
+@pytest.mark.parametrize("group,precision,twist", [(3, 1, False), (3, 0, False), (2, 1, False), (2, 0, False),
+                                                   (3, 1, True)])
+def test_fmunu_and_profiles_match_oracle(group, precision, twist):
+    """qg_measure_fmunu and the action / Polyakov profiles equal the oracle
+    on a thermalising configuration (FP64 sums; tolerances of the plaquette
+    and Polyakov parity), every generator pair and both fields"""
+    phi, omega = (0.3, 0.7) if twist else (0.0, 0.0)
+    dims = (6, 4, 4, 8)
+    L, c = make_pair(group, dims, precision, start=Q.START_HOT, prng=Q.PRNG_RANLUX,
+                     beta=5.8 if group == 3 else 2.3, phi=phi, omega=omega)
+    L.seed(54)
+    L.init(Q.START_HOT)
+    L.sweep(2)
+    t = L.download()
+    V = O.volume(c)
+    pairs = [(1, 5), (2, 6), (3, 8), (4, 7)] if group == 3 else [(3, 2), (1, 2)]
+    for field in (Q.FMUNU_H, Q.FMUNU_E):
+        for i1, i2 in pairs:
+            g, o = L.fmunu(field, i1, i2), O.fmunu(c, t, field, i1, i2)
+            assert np.max(np.abs(g - o)) <= 1e-12 * V, (field, i1, i2, g, o)
+            assert np.any(o != 0)
+    sp = L.action_sums()
+    for axis in range(3):
+        a, oa = L.action_profile(axis), O.action_profile(c, t, axis)
+        assert a.shape == (dims[axis], 2)
+        assert np.allclose(a, oa, rtol=1e-12, atol=1e-12 * V), axis
+        assert abs(a[:, 0].sum() - sp[0]) <= 1e-12 * abs(sp[0])
+        p, op = L.polyakov_profile(axis), O.polyakov_profile(c, t, axis)
+        prel = 1e-12 if precision else 1e-6
+        assert np.max(np.abs(p - op)) <= prel * V / dims[3] * group, axis
+    with pytest.raises(Q.QGError):
+        L.fmunu(2, 3, 8)
+    with pytest.raises(Q.QGError):
+        L.fmunu(0, 0, 8)
+    with pytest.raises(Q.QGError):
+        L.action_profile(3)
+    L.close()
+
+
+def test_fmunu_and_profiles_cold():
+    """cold start: F = 0 exactly, flat profiles (action 0, Polyakov N per site)"""
+    for g in (2, 3):
+        dims = (4, 6, 4, 6)
+        L, c = make_pair(g, dims, 0)
+        L.init(Q.START_COLD)
+        assert np.all(L.fmunu(Q.FMUNU_H) == 0.0) and np.all(L.fmunu(Q.FMUNU_E) == 0.0)
+        for axis in range(3):
+            assert np.all(L.action_profile(axis) == 0.0)
+            p = L.polyakov_profile(axis)
+            per = dims[0] * dims[1] * dims[2] // dims[axis]
+            assert np.all(p[:, 0] == g * per) and np.all(p[:, 1] == 0.0)
+        L.close()

@@ -73,7 +73,8 @@ def test_resume_from_state_file_continues_the_same_chain(tmp_path, prng, start, 
     import struct
     base = dict(group=3, size=(4, 4, 4, 8), precision=precision, start=start, prng=prng, beta=5.9,
                 prng_instances=256, row_align=64, n_or=2, reunit_every=3, wilson_r=2, wilson_t=2)
-    common = dict(niter=2, nav=3, pl_level=2, get_wilson=1, quiet=1, write_results=0, verify=0, save_state=1)
+    common = dict(niter=2, nav=3, pl_level=3, get_wilson=1, quiet=1, write_results=0, verify=0, save_state=1,
+                  fmunu=1, get_actions_diff=1)
     full, half, resumed = (str(tmp_path / n) for n in ("full.qcg", "half.qcg", "resumed.qcg"))
     Q.run(Q.default_config(**base), Q.default_run_options(iter=6, state_out=full, **common))
     Q.run(Q.default_config(**base), Q.default_run_options(iter=3, state_out=half, **common))
@@ -92,3 +93,43 @@ def test_resume_from_state_file_continues_the_same_chain(tmp_path, prng, start, 
     assert np.array_equal(t1, t2)
     for k in ser1:
         assert np.array_equal(ser1[k], ser2[k]), k
+
+
+@pytest.mark.parametrize("group,field", [(3, 1), (3, 2), (2, 1)])
+def test_run_fmunu_and_profiles(tmp_path, group, field):
+    """FMUNU / F0MU with PL_LEVEL 3 and action profiles: the CPU re-check of
+    F passes, the results file carries the FMUNU line, the 16 F columns
+    (|F| = root of the sum of squares of the planes) and the two
+    profile sections with one entry per slice"""
+    dims = (4, 6, 4, 6)
+    cfg = Q.default_config(group=group, size=dims, precision=1, start=Q.START_HOT, prng=Q.PRNG_PHILOX,
+                           beta=5.8 if group == 3 else 2.3, row_align=64, n_or=1)
+    opts = Q.default_run_options(iter=4, niter=1, nav=2, pl_level=3, quiet=1, fmunu=field, get_actions_diff=1,
+                                 fmunu_index1=4 if group == 3 else 1, output_path=str(tmp_path) + "/",
+                                 prefix="su%d-" % group)
+    res = Q.run(cfg, opts)
+    assert res.verification_passed == 1
+    i1, i2 = (4, 8) if group == 3 else (1, 2)
+    last = np.array(res.fmunu_gpu_last[:])
+    assert np.allclose(last, np.array(res.fmunu_cpu_last[:]), rtol=1e-10, atol=1e-13)
+    for g in range(2):
+        for ri in range(2):
+            assert abs(last[12 + 2 * g + ri] - np.sqrt(sum(last[6 * g + 2 * p + ri] ** 2 for p in range(3)))) < 1e-15
+    text = open(res.results_file.decode()).read()
+    assert (" FMUNU(%d, %d)" if field == 1 else " F0MU(%d, %d)") % (i1, i2) in text
+    name = ("Fmunu_xy_%d_re" if field == 1 else "Fmunu_xt_%d_re") % i1
+    assert " Mean %-20s:" % name in text
+    assert "Differentiated Polyakov loop data (#, PL, PL_im, PL_variance, PL_im_variance):" in text
+    assert "Differentiated S data (#, S_total, S_variance):" in text
+    lines = text.split("\n")
+    for a, tag in enumerate(("X", "Y", "Z")):
+        rows = [l for l in lines if l.startswith(tag + "              ")]
+        assert len(rows) == 2 and all(len(r.split()) == 1 + dims[a] for r in rows), tag
+    pl_rows = [l for l in lines if l.startswith("PL             ")]
+    assert len(pl_rows) == 3 and all(len(r.split()) == 1 + dims[a] for a, r in enumerate(pl_rows))
+    rows = [l for l in lines if l[:5].strip().isdigit()]
+    assert len(rows) == 4
+    # #, plaquettes 3, actions 3, Polyakov 2, P2/P4 2, F_munu 16
+    vals = rows[-1].split()
+    assert len(vals) == 1 + 3 + 3 + 2 + 2 + 16
+    assert np.allclose([float(v) for v in vals[-16:]], last, rtol=1e-12, atol=1e-15)

@@ -54,3 +54,17 @@ def test_errors(tmp_path, text, msg):
 def test_missing_file():
     with pytest.raises(Q.QGError, match="cannot open"):
         Q.parse_init_file("/nonexistent/init.dat")
+
+
+def test_fmunu_and_profile_keys(tmp_path):
+    """FMUNU / F0MU / TURNOFFFMUNU and the generator keys FMUNU1/2/4/5/6/7
+    (suncl.cpp:412-452); PL_LEVEL 3 (Polyakov profiles) is the reference
+    main()'s default; ACTIONS_DIFF switches on the action profiles"""
+    d = Q.default_run_options()
+    assert d.pl_level == 3 and d.fmunu == 0 and d.get_actions_diff == 0
+    cfg, o = Q.parse_init_file(write(tmp_path, "FMUNU = 1\nFMUNU4 = 1\nFMUNU6 = 1\nACTIONS_DIFF = 1\n"))
+    assert o.fmunu == 1 and o.fmunu_index1 == 4 and o.fmunu_index2 == 6 and o.get_actions_diff == 1
+    cfg, o = Q.parse_init_file(write(tmp_path, "FMUNU = 1\nF0MU = 1\nFMUNU1 = 1\nFMUNU2 = 1\n"))
+    assert o.fmunu == 2 and o.fmunu_index1 == 2
+    cfg, o = Q.parse_init_file(write(tmp_path, "F0MU = 1\nTURNOFFFMUNU = 1\nFMUNU3 = 1\n"))
+    assert o.fmunu == 0

@@ -29,12 +29,16 @@ def test_state_file_layout_and_roundtrip(tmp_path, group, precision, prng):
     cfg = Q.default_config(group=group, size=(4, 6, 4, 8), precision=precision, prng=prng, beta=5.9, phi=0.25,
                            omega=-0.5, nhit=7, randseries=1234, ranlux_nskip=97, row_align=64, n_or=3,
                            reunit_every=10, reunit_fp64=1, wilson_r=3, wilson_t=2, start=Q.START_HOT)
-    st = Q.RunState(init=1, nav=20, nav_counter=20, niter=5, iter=9, iter_counter=6, pl_level=2, get_actions=1,
+    st = Q.RunState(init=1, nav=20, nav_counter=20, niter=5, iter=9, iter_counter=6, pl_level=3, get_actions=1,
                     get_plaquettes=1, get_wilson=1, prng_counter=331, phase_counter=(1 << 40) + 17,
-                    sweeps_done=45)
+                    sweeps_done=45, fmunu=1, fmunu_index1=3, fmunu_index2=8 if group == 3 else 2,
+                    get_actions_diff=1)
     n = st.iter
+    prow = Q.profile_row(cfg, st)
+    assert prow == 2 * 2 * (4 + 6 + 4)
     series = {"actions": rng.standard_normal(2 * n), "plaquettes": rng.standard_normal(2 * n),
-              "wilson": rng.standard_normal(n), "polyakov": rng.standard_normal(4 * n)}
+              "wilson": rng.standard_normal(n), "polyakov": rng.standard_normal(4 * n),
+              "fmunu_series": rng.standard_normal(12 * n), "profiles": rng.standard_normal(prow * n)}
     table = make_table(cfg, rng)
     path = str(tmp_path / "s.qcg")
     Q.write_state_file(path, cfg, st, table, series)
@@ -49,11 +53,11 @@ def test_state_file_layout_and_roundtrip(tmp_path, group, precision, prng):
     assert np.frombuffer(h[19:21].tobytes(), "<f8")[0] == 5.9
     assert np.frombuffer(h[21:23].tobytes(), "<f8")[0] == 0.25
     assert np.frombuffer(h[23:25].tobytes(), "<f8")[0] == -0.5
-    assert list(h[25:32]) == [2, 0, 0, 0, 1, 1, 1]
+    assert list(h[25:32]) == [3, 3, 8 if group == 3 else 2, 1, 1, 1, 1]
     meas_F, en, en_F, pol = (int(x) for x in h[32:36])
-    assert en == 64 and en_F == 64 and pol == 64
+    assert en == 64 and en_F == 7 * 64 and pol == 64          # MODEL_energies_size = 7
     assert h[36] == group and h[37] == 4 and list(h[38:42]) == [4, 6, 4, 8] and list(h[42:46]) == [4, 6, 4, 8]
-    assert h[48] == word("B200")
+    assert h[48] == word("B200") and h[60] == 1 and h[61] == 1
 
     # buffers in the reference's order: measurement, energies, energies_plq,
     # wilson loop, polyakov loop, link table
@@ -69,10 +73,21 @@ def test_state_file_layout_and_roundtrip(tmp_path, group, precision, prng):
     k = st.iter_counter
     assert np.array_equal(e[:k].ravel(), series["actions"][:2 * k]) and not e[k:].any()
     assert np.array_equal(p[:k].ravel(), series["plaquettes"][:2 * k])
+    # F_munu in energies_plq blocks 1..6: index1 planes xy, xz, yz, then index2
+    f = series["fmunu_series"].reshape(-1, 6, 2)
+    for b in range(6):
+        assert np.array_equal(p[(b + 1) * en:(b + 1) * en + k], f[:k, b]), b
     assert np.array_equal(w[:k], series["wilson"][:k])
     assert np.array_equal(pl[:k], series["polyakov"].reshape(-1, 4)[:k, :2])
     t = np.frombuffer(raw[off:off + table.nbytes], table.dtype)
     assert np.array_equal(t, table)
+    off += table.nbytes
+    assert np.frombuffer(raw[off:off + 4], "<u4")[0] == word("QGP4")
+    off += 4 + 16 * pol
+    assert np.frombuffer(raw[off:off + 4], "<u4")[0] == word("QGPF")
+    prof = np.frombuffer(raw[off + 4:off + 4 + 8 * prow * en], "<f8").reshape(en, prow)
+    assert np.array_equal(prof[:k], series["profiles"].reshape(n, prow)[:k]) and not prof[k:].any()
+    assert len(raw) == off + 4 + 8 * prow * en
 
     cfg2, st2, ser2, table2 = Q.read_state_file(path)
     assert np.array_equal(table2, table)
@@ -84,7 +99,10 @@ def test_state_file_layout_and_roundtrip(tmp_path, group, precision, prng):
     for f in ("init", "nav", "nav_counter", "niter", "iter", "iter_counter", "pl_level", "prng_counter",
               "phase_counter", "sweeps_done"):
         assert getattr(st2, f) == getattr(st, f), f
-    for key, m in (("actions", 2), ("plaquettes", 2), ("wilson", 1), ("polyakov", 4)):
+    for f in ("fmunu", "fmunu_index1", "fmunu_index2", "get_actions_diff"):
+        assert getattr(st2, f) == getattr(st, f), f
+    for key, m in (("actions", 2), ("plaquettes", 2), ("wilson", 1), ("polyakov", 4), ("fmunu_series", 12),
+                   ("profiles", prow)):
         assert np.array_equal(ser2[key][:m * k], series[key][:m * k]), key
 
 
