@@ -537,39 +537,122 @@ cudaError_t launch_wilson(const Geom &G, const void *links, int group, int prec,
 // traces, then k_wilson_all_reduce in a fixed order.
 constexpr int kWilsonMax = 16;
 
+// All planar Wilson loops R x T (R <= Rmax, T <= Tmax) in one launch
+// (lattice_measurement_wilson, wilson_loop.cl:55-454, for every R x T at
+// once), products in precision P, sums in FP64.  One thread per time
+// column: thread (spatial site, i, R) walks t0 = 0 .. N4-1 and keeps the
+// spatial lines S(t) = L_i^R(x + t t) of the last Tmax + 1 time slices in
+// a private ring in shared memory, so each line is built once per column
+// (not once per (t0, T)); the time lines at x and x + R i grow by one
+// product per T, and each term is retr4(L_t^T(x), S(t0+T), L_t^T(x+R i),
+// S(t0)).  The per-thread sums w[T] live in shared memory.  Dynamic shared
+// memory: (Tmax+1) ring entries and Tmax doubles per thread.  A ring entry
+// holds the 2 x 2 block for SU(2); for SU(3) the full line in FP64, or
+// with FP32 products rows 1, 2 only (row 3 rebuilt on reading; rebuilding
+// an FP64 product of FP32 links would move it by their ~1e-7 departure
+// from unitarity, more than FP64 products are meant to carry).
+template <int NC, typename P> constexpr int kRingFloats = NC == 2 ? 8 : (sizeof(P) == 8 ? 18 : 12);
+
 template <int NC, typename Real, typename P>
-__global__ void __launch_bounds__(128) k_wilson_all(Field<Real> U, Geom G, int Tmax, const double *params, int twist,
-                                                     double *partials)
+__global__ void __launch_bounds__(128) k_wilson_cols(Field<Real> U, Geom G, int Tmax, const double *params,
+                                                      int twist, double *partials)
 {
+    extern __shared__ __align__(16) unsigned char wsm[];
+    constexpr int RF = kRingFloats<NC, P>;
+    constexpr int ROWS = RF == 18 ? 3 : 2;        // rows stored
     const int R = blockIdx.y + 1, i = blockIdx.z;
-    double w[kWilsonMax];
+    const int nb = blockDim.x, tid = threadIdx.x, slots = Tmax + 1;
+    double *wsum = reinterpret_cast<double *>(wsm);                          // [Tmax][nb]
+    P *ring = reinterpret_cast<P *>(wsm + sizeof(double) * Tmax * nb);       // [slots][RF][nb]
+    auto put = [&](int slot, const M3<P> &m) {
+        P *q = ring + (size_t)slot * RF * nb + tid;
 #pragma unroll
-    for (int k = 0; k < kWilsonMax; k++) w[k] = 0.0;
-    for (uint32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < G.V; s += gridDim.x * blockDim.x) {
-        const Crd x = lex2crd(G, s);
-        Crd a = x;
-        M3<P> m4 = load_as<NC, Real, P>(U, G, a, i, params, twist);
-        for (int k = 1; k < R; k++) { a = step_plus(G, a, i); m4 = mulf(m4, load_as<NC, Real, P>(U, G, a, i, params, twist)); }
-        Crd cx = x, cy = step_plus(G, a, i);
-        M3<P> mx = load_as<NC, Real, P>(U, G, cx, 3, params, twist);
-        M3<P> my = load_as<NC, Real, P>(U, G, cy, 3, params, twist);
+        for (int a = 0; a < ROWS; a++)
 #pragma unroll
-        for (int T = 1; T <= kWilsonMax; T++) {
-            if (T <= Tmax) {
+            for (int b = 0; b < NC; b++) {
+                q[(2 * (a * NC + b)) * nb] = m.m[a][b].re;
+                q[(2 * (a * NC + b) + 1) * nb] = m.m[a][b].im;
+            }
+    };
+    auto get = [&](int slot) {
+        const P *q = ring + (size_t)slot * RF * nb + tid;
+        M3<P> m;
+#pragma unroll
+        for (int a = 0; a < 3; a++)
+#pragma unroll
+            for (int b = 0; b < 3; b++) m.m[a][b] = { (P)0, (P)0 };
+#pragma unroll
+        for (int a = 0; a < ROWS; a++)
+#pragma unroll
+            for (int b = 0; b < NC; b++) m.m[a][b] = { q[(2 * (a * NC + b)) * nb], q[(2 * (a * NC + b) + 1) * nb] };
+        if (NC == 3 && ROWS == 2) fill_row3(m);
+        return m;
+    };
+    for (int k = 0; k < Tmax; k++) wsum[k * nb + tid] = 0.0;
+    const uint32_t Vs = (uint32_t)G.n[0] * G.n[1] * G.n[2];
+    const int nt = G.n[3];
+    for (uint32_t xs = blockIdx.x * blockDim.x + tid; xs < Vs; xs += gridDim.x * blockDim.x) {
+        Crd c0;
+        c0.y = (int)(xs % (uint32_t)G.n[1]);
+        const uint32_t r = xs / (uint32_t)G.n[1];
+        c0.z = (int)(r % (uint32_t)G.n[2]);
+        c0.x = (int)(r / (uint32_t)G.n[2]);
+        c0.t = 0;
+        auto line = [&](int t) {
+            Crd a = c0;
+            a.t = t;
+            M3<P> m = load_as<NC, Real, P>(U, G, a, i, params, twist);
+            for (int k = 1; k < R; k++) { a = step_plus(G, a, i); m = mulf(m, load_as<NC, Real, P>(U, G, a, i, params, twist)); }
+            return m;
+        };
+        Crd cy0 = c0;
+        for (int k = 0; k < R; k++) cy0 = step_plus(G, cy0, i);     // x + R i
+        for (int t = 0; t < Tmax; t++) put(t, line(t % nt));
+#pragma unroll 1
+        for (int t0 = 0; t0 < nt; t0++) {
+            put((t0 + Tmax) % slots, line((t0 + Tmax) % nt));
+            Crd cx = c0, cy = cy0;
+            cx.t = t0;
+            cy.t = t0;
+            M3<P> mx = load_as<NC, Real, P>(U, G, cx, 3, params, twist);
+            M3<P> my = load_as<NC, Real, P>(U, G, cy, 3, params, twist);
+#pragma unroll 1
+            for (int T = 1; T <= Tmax; T++) {
                 if (T > 1) {
                     cx = step_plus(G, cx, 3);
                     mx = mulf(mx, load_as<NC, Real, P>(U, G, cx, 3, params, twist));
                     cy = step_plus(G, cy, 3);
                     my = mulf(my, load_as<NC, Real, P>(U, G, cy, 3, params, twist));
                 }
-                Crd b = step_plus(G, cx, 3);
-                M3<P> m2 = load_as<NC, Real, P>(U, G, b, i, params, twist);
-                for (int k = 1; k < R; k++) { b = step_plus(G, b, i); m2 = mulf(m2, load_as<NC, Real, P>(U, G, b, i, params, twist)); }
-                w[T - 1] += retr4(mx, m2, my, m4);
+                wsum[(T - 1) * nb + tid] += retr4(mx, get((t0 + T) % slots), my, get(t0 % slots));
             }
         }
     }
+    double w[kWilsonMax];
+#pragma unroll
+    for (int k = 0; k < kWilsonMax; k++) w[k] = k < Tmax ? wsum[k * nb + tid] : 0.0;
     block_sum_store<kWilsonMax>(w, partials, (blockIdx.z * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x);
+}
+
+static size_t wilson_cols_smem(int group, int psize, int Tmax, int nb)
+{
+    const int rf = group == 2 ? 8 : (psize == 8 ? 18 : 12);
+    return (size_t)nb * (sizeof(double) * Tmax + (size_t)psize * rf * (Tmax + 1));
+}
+
+static int wilson_cols_blocks(const Geom &G, int nb);
+
+template <int NC, typename Real, typename P>
+static cudaError_t wilson_cols(const Field<Real> &U, const Geom &G, int Rmax, int Tmax, const double *params,
+                               int twist, double *partials, int &nbx, cudaStream_t s)
+{
+    const int nbk = wilson_cols_smem(NC, sizeof(P), Tmax, 128) <= 80 * 1024 ? 128 : 64;
+    const size_t sm = wilson_cols_smem(NC, sizeof(P), Tmax, nbk);
+    dim3 gc((unsigned)wilson_cols_blocks(G, nbk), Rmax, 3);
+    nbx = (int)gc.x;
+    cudaFuncSetAttribute(k_wilson_cols<NC, Real, P>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    k_wilson_cols<NC, Real, P><<<gc, nbk, sm, s>>>(U, G, Tmax, params, twist, partials);
+    return cudaGetLastError();
 }
 
 // out[(R-1) Tmax + T-1] = sum over i and blocks (in that order)
@@ -585,29 +668,34 @@ __global__ void k_wilson_all_reduce(const double *partials, int nbx, int Rmax, i
 }
 
 int wilson_all_blocks(const Geom &G) { return (int)min((G.V + 127u) / 128u, 296u); }
+// column kernel: spatial sites per (R, i) over blocks of nb threads, at most
+// as many blocks as the site kernel uses (the partials are sized for that)
+static int wilson_cols_blocks(const Geom &G, int nb)
+{
+    const uint32_t Vs = (uint32_t)G.n[0] * G.n[1] * G.n[2];
+    return (int)min((Vs + nb - 1) / (uint32_t)nb, (uint32_t)wilson_all_blocks(G));
+}
 size_t wilson_all_partials(int nbx, int Rmax) { return (size_t)3 * Rmax * nbx * kWilsonMax; }
 
 cudaError_t launch_wilson_all(const Geom &G, const void *links, int group, int prec, int Rmax, int Tmax,
                               int fp64_products, const double *params, int twist, double *partials, double *out,
                               cudaStream_t s)
 {
-    const int nbx = wilson_all_blocks(G);
-    dim3 grid(nbx, Rmax, 3);
+    int nbx = 0;
+    cudaError_t e;
     if (prec) {
         Field<double> U{ (double4 *)links, G.pstride };
-        if (group == 3) k_wilson_all<3, double, double><<<grid, 128, 0, s>>>(U, G, Tmax, params, twist, partials);
-        else k_wilson_all<2, double, double><<<grid, 128, 0, s>>>(U, G, Tmax, params, twist, partials);
+        e = group == 3 ? wilson_cols<3, double, double>(U, G, Rmax, Tmax, params, twist, partials, nbx, s)
+                       : wilson_cols<2, double, double>(U, G, Rmax, Tmax, params, twist, partials, nbx, s);
     } else {
         Field<float> U{ (float4 *)links, G.pstride };
-        if (fp64_products) {
-            if (group == 3) k_wilson_all<3, float, double><<<grid, 128, 0, s>>>(U, G, Tmax, params, twist, partials);
-            else k_wilson_all<2, float, double><<<grid, 128, 0, s>>>(U, G, Tmax, params, twist, partials);
-        } else {
-            if (group == 3) k_wilson_all<3, float, float><<<grid, 128, 0, s>>>(U, G, Tmax, params, twist, partials);
-            else k_wilson_all<2, float, float><<<grid, 128, 0, s>>>(U, G, Tmax, params, twist, partials);
-        }
+        if (fp64_products)
+            e = group == 3 ? wilson_cols<3, float, double>(U, G, Rmax, Tmax, params, twist, partials, nbx, s)
+                           : wilson_cols<2, float, double>(U, G, Rmax, Tmax, params, twist, partials, nbx, s);
+        else
+            e = group == 3 ? wilson_cols<3, float, float>(U, G, Rmax, Tmax, params, twist, partials, nbx, s)
+                           : wilson_cols<2, float, float>(U, G, Rmax, Tmax, params, twist, partials, nbx, s);
     }
-    cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     k_wilson_all_reduce<<<(Rmax * Tmax + 127) / 128, 128, 0, s>>>(partials, nbx, Rmax, Tmax, out);
     return cudaGetLastError();
