@@ -44,6 +44,8 @@ def parse():
     ap.add_argument("--prng", default="philox", choices=["philox", "ranlux"])
     ap.add_argument("--size", type=int, default=SIZE)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--shapes", default=None,
+                    help="HB,OR launch shapes to pin instead of tuning (e.g. for a profiler run)")
     return ap.parse_args()
 
 
@@ -205,7 +207,11 @@ def run_ours(args):
     L.seed()
     L.init()
     L.sweep(2)                                  # leave the cold start before timing
-    tune = L.tune(reps=8)                       # launch shapes for this lattice (field restored)
+    if args.shapes:
+        tune = None
+        L.set_shapes(*(int(x) for x in args.shapes.split(",")))
+    else:
+        tune = L.tune(reps=8)                   # launch shapes for this lattice (field restored)
     stream = torch.cuda.ExternalStream(L.stream())
     V = args.size ** 4
     updates_per_step = 4 * V * (1 + N_OR)
@@ -266,6 +272,7 @@ def run_ours(args):
     e2e = RP.whole_job_rate(world, updates_per_step * e2e_steps, e2e_s)
 
     plq = L.plaquette()
+    L_shapes = L.shapes()
     first = 2 + args.warmup
     reunits = sum(1 for n in range(first + 1, first + args.steps + 1) if n % REUNIT_EVERY == 0)
     launches = args.steps * (8 + 8 * N_OR + (1 if prng == Q.PRNG_PHILOX else 0)) + reunits
@@ -291,6 +298,7 @@ def run_ours(args):
                 "what": "qg_set_params + qg_sweep + plaquette/Polyakov read back, host wall clock"},
         "gpu_launches": launches,
         "tuning_ms_per_launch": tune,
+        "shapes": list(L_shapes),
         "clocks": clk,
         "plaquette": plq[2],
     }
