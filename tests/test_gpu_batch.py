@@ -61,3 +61,23 @@ def test_batch_series_capacity_and_argument_checks():
         Q.Batch(common(3, 0), [((4, 5, 4, 4), 6.0, 1)])
     with pytest.raises(Q.QGError):
         Q.Batch(common(3, 0), [((4, 4, 4, 4), 6.0, 0)])
+
+
+def test_beta_scan_split_over_ranks_gives_the_same_ensembles():
+    """the multi-GPU replica scheduler's shares, run here one after the
+    other on one GPU, reproduce the single-batch run ensemble by ensemble
+    bit for bit (each chain depends only on its RANDSERIES and the sweep
+    count, not on the batch it runs in)"""
+    from types import SimpleNamespace
+
+    from qcdgpu_b200 import betascan as BS
+    ens = [((8, 8, 8, 4), 5.6, 1000), ((6, 6, 6, 4), 5.8, 1001), ((8, 8, 8, 6), 6.0, 1002),
+           ((4, 4, 4, 4), 5.5, 1003), ((6, 6, 6, 6), 5.9, 1004)]
+    a = SimpleNamespace(n_or=2, sweeps=6, warmup=3, measure_every=1, shape=4, barrier=None)
+    whole = BS.run_share(ens, list(range(len(ens))), a)
+    shares = BS.partition(ens, 2, a.n_or)
+    assert all(shares)
+    job = BS.merge([BS.run_share(ens, s, a) for s in shares], len(ens))
+    assert job["plaquette"] == whole["plaquette"]
+    assert job["polyakov_abs"] == whole["polyakov_abs"]
+    assert job["updates"] == whole["updates"] and job["sites"] == whole["sites"]

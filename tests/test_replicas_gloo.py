@@ -53,3 +53,65 @@ def test_single_process_needs_no_group():
     assert RP.init("gloo") is None
     assert RP.max_over_ranks(3.0, None) == 3.0
     assert RP.whole_job_rate(1, 10.0, 2.0) == 5.0
+
+
+# ------------------------------------------- beta-scan replica scheduler
+from types import SimpleNamespace
+
+from qcdgpu_b200 import betascan as BS
+
+
+def _fake_runner(ens, idx, a):
+    """stands in for a GPU batch: deterministic per-ensemble values, a
+    device time proportional to the share's cost"""
+    cost = sum(BS.ensemble_cost(ens[k], a.n_or) for k in idx)
+    return {"idx": list(idx), "plaquette": [1.0 + 0.01 * k for k in idx], "polyakov_abs": [0.1 * k for k in idx],
+            "updates": float(cost * a.sweeps), "ms": cost * 1e-6, "sites": sum(int(sum(ens[k][0])) for k in idx),
+            "field_bytes": 0}
+
+
+def _sched_main(rank, world, port, out):
+    os.environ.update({"MASTER_ADDR": "127.0.0.1", "MASTER_PORT": str(port), "RANK": str(rank),
+                       "WORLD_SIZE": str(world), "LOCAL_RANK": str(rank)})
+    dist = RP.init("gloo", timeout_s=60)
+    a = SimpleNamespace(n_or=4, sweeps=10)
+    ens = BS.workload(13, 54)
+    job = BS.schedule(ens, a, dist, rank, world, runner=_fake_runner)
+    out.put((rank, job))
+    RP.finish(dist)
+
+
+def test_partition_covers_every_ensemble_once_and_balances():
+    ens = BS.workload(64, 54)
+    for world in (1, 2, 3, 8, 70):
+        sh = BS.partition(ens, world)
+        assert sorted(k for s in sh for k in s) == list(range(64))
+        assert sh == BS.partition(ens, world)                       # deterministic
+        loads = [sum(BS.ensemble_cost(ens[k], 4) for k in s) for s in sh]
+        assert max(loads) - min(loads) <= max(BS.ensemble_cost(e, 4) for e in ens)
+    assert sum(1 for s in BS.partition(ens, 70) if not s) == 6      # more ranks than ensembles
+
+
+def test_two_gloo_ranks_run_the_beta_scan_schedule():
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_sched_main, args=(r, 2, port, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    res = dict(q.get(timeout=120) for _ in procs)
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    ens = BS.workload(13, 54)
+    a = SimpleNamespace(n_or=4, sweeps=10)
+    sh = BS.partition(ens, 2)
+    for r in (0, 1):
+        job = res[r]
+        assert job["plaquette"] == [1.0 + 0.01 * k for k in range(13)]      # every ensemble, in order
+        assert job["polyakov_abs"] == [0.1 * k for k in range(13)]
+        parts = [_fake_runner(ens, s, a) for s in sh]
+        assert job["ms"] == max(p["ms"] for p in parts)                       # the slowest rank
+        assert job["updates"] == sum(BS.ensemble_cost(e, 4) for e in ens) * 10
+        assert abs(job["link_updates_per_s"] - job["updates"] / (job["ms"] * 1e-3)) < 1e-6 * job["link_updates_per_s"]
+        assert [x["ensembles"] for x in job["ranks"]] == [len(s) for s in sh]
