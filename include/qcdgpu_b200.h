@@ -163,6 +163,16 @@ int qg_reunitarize(qg_ctx *ctx, int fp64);
  * Results are raw lattice sums (normalise as suncl.cpp:1328-1612 does).
  * Synchronous: out is host memory.                                        */
 int qg_measure(qg_ctx *ctx, int what, double *out);
+/* Asynchronous form (new): qg_measure_enqueue puts qg_measure(what)'s
+ * kernels and the copy of its result into a pinned host slot on the
+ * context's stream and returns at once with a ticket; qg_measure_fetch
+ * waits for that ticket's copy and writes the same values qg_measure gives
+ * (2, 2, 4 or 1 doubles).  A run loop can so read every step's result
+ * without stalling the device between steps.  Up to QG_MEASURE_SLOTS
+ * tickets are kept; an older ticket is an error.                          */
+#define QG_MEASURE_SLOTS 64
+int qg_measure_enqueue(qg_ctx *ctx, int what, uint64_t *ticket);
+int qg_measure_fetch(qg_ctx *ctx, uint64_t ticket, double *out);
 /* same, generalised Wilson loop of extent R x T (config keys WILSONR/T)   */
 int qg_measure_wilson(qg_ctx *ctx, int R, int T, double *out);
 /* all planar Wilson loops R x T for R <= Rmax, T <= Tmax (both <= 16): in
@@ -207,8 +217,9 @@ int qg_links_download(qg_ctx *ctx, void *host, int layout);
 
 /* the per-run parameter block the kernels read from device memory, as
  * the reference's lattice_parameters buffer {BETA/N, PHI, OMEGA}
- * (suncl.cpp:3936-3949): stream-ordered host->device copy from pinned
- * staging; later sweeps and measurements use the new values.            */
+ * (suncl.cpp:3936-3949): stream-ordered host->device copy from one of 8
+ * pinned staging slots (the call does not wait for the stream); later
+ * sweeps and measurements use the new values.                            */
 int qg_set_params(qg_ctx *ctx, double beta, double phi, double omega);
 /* the context's CUDA stream (cudaStream_t), for event timing / interop   */
 int qg_get_stream(qg_ctx *ctx, void **stream);

@@ -23,6 +23,7 @@ HEATBATH, OVERRELAX = 0, 1
 MEAS_PLAQUETTE, MEAS_ACTION, MEAS_POLYAKOV, MEAS_WILSON = 0, 1, 2, 3
 FMUNU_H, FMUNU_E = 0, 1
 FMUNU_COLS = 16                     # QG_FMUNU_COLS
+MEASURE_SLOTS = 64                  # QG_MEASURE_SLOTS
 TUNE_SHAPES = 6                     # QG_TUNE_SHAPES
 NET_FEATURES, NET_HIDDEN, NET_PARAMS = 8, 32, 1377   # QG_NET_*
 
@@ -37,6 +38,7 @@ EXPORTED_SYMBOLS = (
     "qg_batch_create", "qg_batch_destroy", "qg_batch_init", "qg_batch_set_shape", "qg_batch_run", "qg_batch_sync",
     "qg_batch_get_stream", "qg_batch_series", "qg_batch_links_download", "qg_batch_info",
     "qg_measure_wilson_all", "qg_measure_fmunu", "qg_measure_action_profile", "qg_measure_polyakov_profile",
+    "qg_measure_enqueue", "qg_measure_fetch",
     "qg_net_set", "qg_net_get", "qg_mh_phase", "qg_mh_sweep", "qg_mh_stats", "qg_net_grad", "qg_net_train",
 )
 
@@ -202,6 +204,8 @@ def load_library(path=LIB_PATH):
     lib.qg_measure_wilson.argtypes = [vp, ctypes.c_int, ctypes.c_int, P(ctypes.c_double)]
     lib.qg_measure_wilson_all.argtypes = [vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, P(ctypes.c_double)]
     lib.qg_measure_fmunu.argtypes = [vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, P(ctypes.c_double)]
+    lib.qg_measure_enqueue.argtypes = [vp, ctypes.c_int, P(ctypes.c_uint64)]
+    lib.qg_measure_fetch.argtypes = [vp, ctypes.c_uint64, P(ctypes.c_double)]
     lib.qg_measure_action_profile.argtypes = [vp, ctypes.c_int, P(ctypes.c_double)]
     lib.qg_measure_polyakov_profile.argtypes = [vp, ctypes.c_int, P(ctypes.c_double)]
     lib.qg_links_upload.argtypes = [vp, vp, ctypes.c_int]
@@ -569,6 +573,19 @@ class Lattice:
                                                 out.ctypes.data_as(ctypes.POINTER(ctypes.c_double))),
                  "qg_measure_wilson_all")
         return out.reshape(Rmax, Tmax)
+
+    def measure_enqueue(self, what):
+        """qg_measure_enqueue: the measurement's kernels and result copy on
+        the stream, without waiting; returns the ticket for measure_fetch"""
+        t = ctypes.c_uint64()
+        self._ck(self.lib.qg_measure_enqueue(self.ctx, what, ctypes.byref(t)), "qg_measure_enqueue")
+        return t.value
+
+    def measure_fetch(self, ticket):
+        """qg_measure_fetch: the values of an enqueued measurement (waits for them)"""
+        out = (ctypes.c_double * 4)()
+        self._ck(self.lib.qg_measure_fetch(self.ctx, ticket, out), "qg_measure_fetch")
+        return tuple(out)
 
     def fmunu(self, field=0, index1=None, index2=None):
         """raw F_munu sums (qg_measure_fmunu): array [2 generators][3 planes]

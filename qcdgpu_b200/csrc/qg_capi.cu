@@ -28,7 +28,15 @@ struct qg_ctx {
     double *h_results = nullptr;    // pinned
     uint64_t *d_phase = nullptr;
     double *d_params = nullptr;     // {BETA/N, PHI, OMEGA, 0}: lattice_parameters
-    double *h_params = nullptr;     // pinned staging
+    double *h_params = nullptr;     // pinned staging, kParamSlots x 4 doubles
+    cudaEvent_t param_ev[8] = {};   // slot's upload done
+    uint32_t param_next = 0;
+    // asynchronous measurements: pinned result slots, their copy events and tickets
+    double *h_ring = nullptr;       // QG_MEASURE_SLOTS x 8 doubles
+    cudaEvent_t ring_ev[QG_MEASURE_SLOTS] = {};
+    uint64_t ring_ticket[QG_MEASURE_SLOTS] = {};
+    int ring_what[QG_MEASURE_SLOTS] = {};
+    uint64_t ticket_next = 1;
     int twist_built = 0;            // twist flag the cached graphs were built with
     int variant_hb = 0, variant_or = 0;   // phase-kernel launch shapes (qg_tune)
     uint64_t phase_counter = 0;     // host mirror of *d_phase
@@ -140,6 +148,9 @@ extern "C" int qg_destroy(qg_ctx *c)
     cudaFree(c->d_fpart); cudaFree(c->d_ppart); cudaFree(c->d_pout);
     if (c->h_results) cudaFreeHost(c->h_results);
     if (c->h_params) cudaFreeHost(c->h_params);
+    if (c->h_ring) cudaFreeHost(c->h_ring);
+    for (cudaEvent_t ev : c->param_ev) if (ev) cudaEventDestroy(ev);
+    for (cudaEvent_t ev : c->ring_ev) if (ev) cudaEventDestroy(ev);
     if (c->stream) cudaStreamDestroy(c->stream);
     delete c;
     return QG_OK;
@@ -191,7 +202,13 @@ extern "C" int qg_create(const qg_config *cfg, qg_ctx **out)
     if ((e = cudaMalloc(&c->d_phase, sizeof(uint64_t))) != cudaSuccess) return bad("cudaMalloc(phase)");
     if ((e = cudaMemsetAsync(c->d_phase, 0, sizeof(uint64_t), c->stream)) != cudaSuccess) return bad("cudaMemset(phase)");
     if ((e = cudaMalloc(&c->d_params, 4 * sizeof(double))) != cudaSuccess) return bad("cudaMalloc(params)");
-    if ((e = cudaMallocHost(&c->h_params, 4 * sizeof(double))) != cudaSuccess) return bad("cudaMallocHost(params)");
+    if ((e = cudaMallocHost(&c->h_params, 8 * 4 * sizeof(double))) != cudaSuccess) return bad("cudaMallocHost(params)");
+    if ((e = cudaMallocHost(&c->h_ring, (size_t)QG_MEASURE_SLOTS * 8 * sizeof(double))) != cudaSuccess)
+        return bad("cudaMallocHost(results ring)");
+    for (cudaEvent_t &ev : c->param_ev)
+        if ((e = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming)) != cudaSuccess) return bad("cudaEventCreate");
+    for (cudaEvent_t &ev : c->ring_ev)
+        if ((e = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming)) != cudaSuccess) return bad("cudaEventCreate");
     if ((e = cudaStreamSynchronize(c->stream)) != cudaSuccess) return bad("create sync");
     if (qg_set_params(c, cfg->beta, cfg->phi, cfg->omega) != QG_OK) { g_create_err = c->err; qg_destroy(c); return QG_ERR_CUDA; }
     *out = c;
@@ -207,13 +224,18 @@ extern "C" int qg_set_params(qg_ctx *c, double beta, double phi, double omega)
     c->cfg.beta = beta;
     c->cfg.phi = phi;
     c->cfg.omega = omega;
-    QG_CK(cudaStreamSynchronize(c->stream), "params sync");   // staging buffer reuse
-    c->h_params[0] = beta / c->cfg.group;
-    c->h_params[1] = phi;
-    c->h_params[2] = omega;
-    c->h_params[3] = 0.0;
-    QG_CK(cudaMemcpyAsync(c->d_params, c->h_params, 4 * sizeof(double), cudaMemcpyHostToDevice, c->stream),
-          "params upload");
+    // stream-ordered upload from one of 8 pinned staging slots; a slot is
+    // rewritten only after its previous upload has completed, so the call
+    // does not wait for the stream
+    const uint32_t slot = c->param_next++ % 8;
+    QG_CK(cudaEventSynchronize(c->param_ev[slot]), "params slot");
+    double *h = c->h_params + 4 * slot;
+    h[0] = beta / c->cfg.group;
+    h[1] = phi;
+    h[2] = omega;
+    h[3] = 0.0;
+    QG_CK(cudaMemcpyAsync(c->d_params, h, 4 * sizeof(double), cudaMemcpyHostToDevice, c->stream), "params upload");
+    QG_CK(cudaEventRecord(c->param_ev[slot], c->stream), "params event");
     if (twist_of(c->cfg) != c->twist_built) destroy_graphs(c);
     return QG_OK;
 }
@@ -887,6 +909,69 @@ extern "C" int qg_measure(qg_ctx *c, int what, double *out)
     default:
         return fail(c, QG_ERR_ARG, "unknown measurement");
     }
+}
+
+// the measurement kernels of `what` into d_results; ncomp values there
+static int measure_launch(qg_ctx *c, int what, int &ncomp, int &first)
+{
+    const qg_config &f = c->cfg;
+    int tw = !(f.phi == 0.0 && f.omega == 0.0);
+    switch (what) {
+    case QG_MEAS_PLAQUETTE:
+    case QG_MEAS_ACTION:
+        QG_CK(launch_plaquette(c->G, c->links, f.group, f.precision, c->d_params, tw, c->partials, c->d_results,
+                               c->stream), "plaquette");
+        ncomp = 2;
+        first = what == QG_MEAS_PLAQUETTE ? 0 : 2;
+        return QG_OK;
+    case QG_MEAS_POLYAKOV:
+        QG_CK(launch_polyakov(c->G, c->links, f.group, f.precision, c->partials, c->d_results, c->stream), "polyakov");
+        ncomp = 4;
+        first = 0;
+        return QG_OK;
+    case QG_MEAS_WILSON:
+        if (f.wilson_r < 1 || f.wilson_t < 1 || f.wilson_r > c->G.n[0] || f.wilson_t > c->G.n[3])
+            return fail(c, QG_ERR_ARG, "Wilson loop extent out of range");
+        QG_CK(launch_wilson(c->G, c->links, f.group, f.precision, f.wilson_r, f.wilson_t, c->d_params, tw, c->partials,
+                            c->d_results, c->stream), "wilson");
+        ncomp = 1;
+        first = 0;
+        return QG_OK;
+    default:
+        return fail(c, QG_ERR_ARG, "unknown measurement");
+    }
+}
+
+extern "C" int qg_measure_enqueue(qg_ctx *c, int what, uint64_t *ticket)
+{
+    if (!c || !ticket) return QG_ERR_ARG;
+    const uint64_t t = c->ticket_next;
+    const int slot = (int)(t % QG_MEASURE_SLOTS);
+    // the slot's previous copy must have landed before it is reused
+    QG_CK(cudaEventSynchronize(c->ring_ev[slot]), "measure slot");
+    int ncomp = 0, first = 0;
+    int r = measure_launch(c, what, ncomp, first);
+    if (r) return r;
+    QG_CK(cudaMemcpyAsync(c->h_ring + 8 * slot, c->d_results + first, ncomp * sizeof(double), cudaMemcpyDeviceToHost,
+                          c->stream), "measure copy");
+    QG_CK(cudaEventRecord(c->ring_ev[slot], c->stream), "measure event");
+    c->ring_ticket[slot] = t;
+    c->ring_what[slot] = what;
+    c->ticket_next++;
+    *ticket = t;
+    return QG_OK;
+}
+
+extern "C" int qg_measure_fetch(qg_ctx *c, uint64_t ticket, double *out)
+{
+    if (!c || !out) return QG_ERR_ARG;
+    const int slot = (int)(ticket % QG_MEASURE_SLOTS);
+    if (ticket == 0 || c->ring_ticket[slot] != ticket)
+        return fail(c, QG_ERR_ARG, "unknown measurement ticket (never issued, or more than QG_MEASURE_SLOTS ago)");
+    QG_CK(cudaEventSynchronize(c->ring_ev[slot]), "measure fetch");
+    const int n = c->ring_what[slot] == QG_MEAS_POLYAKOV ? 4 : c->ring_what[slot] == QG_MEAS_WILSON ? 1 : 2;
+    for (int i = 0; i < n; i++) out[i] = c->h_ring[8 * slot + i];
+    return QG_OK;
 }
 
 extern "C" int qg_links_upload(qg_ctx *c, const void *host, int layout)

@@ -468,3 +468,36 @@ def test_fmunu_and_profiles_cold():
             per = dims[0] * dims[1] * dims[2] // dims[axis]
             assert np.all(p[:, 0] == g * per) and np.all(p[:, 1] == 0.0)
         L.close()
+
+
+def test_async_measurements_and_parameter_staging():
+    """qg_measure_enqueue / _fetch give qg_measure's values; parameter
+    uploads queued back to back (no stream wait) apply in stream order; old
+    or unknown tickets are errors"""
+    L, c, t = hot_config(3, (4, 6, 4, 8), 1)
+    sp, tp = L.plaquette_sums()
+    assert L.measure_fetch(L.measure_enqueue(Q.MEAS_PLAQUETTE))[:2] == (sp, tp)
+    assert L.measure_fetch(L.measure_enqueue(Q.MEAS_POLYAKOV)) == tuple(L.polyakov_sums())
+    with pytest.raises(Q.QGError):                    # WILSONR = 7 > N1 = 4, as qg_measure_wilson
+        L.measure_enqueue(Q.MEAS_WILSON)
+    with pytest.raises(Q.QGError):
+        L.wilson_sum()
+    assert L.measure_fetch(L.measure_enqueue(Q.MEAS_ACTION))[:2] == tuple(L.action_sums())
+    betas = [5.0 + 0.1 * k for k in range(20)]
+    tickets = []
+    for b in betas:                                   # 20 uploads, more than the 8 staging slots
+        L.set_params(b)
+        tickets.append(L.measure_enqueue(Q.MEAS_ACTION))
+    V = O.volume(c)
+    for b, tk in zip(betas, tickets):
+        a = L.measure_fetch(tk)[:2]
+        assert abs(a[0] - b / 3 * (9 * V - sp)) <= 1e-12 * abs(a[0])
+        assert abs(a[1] - b / 3 * (9 * V - tp)) <= 1e-12 * abs(a[1])
+    first = L.measure_enqueue(Q.MEAS_PLAQUETTE)
+    for _ in range(Q.MEASURE_SLOTS):
+        L.measure_enqueue(Q.MEAS_PLAQUETTE)
+    with pytest.raises(Q.QGError):
+        L.measure_fetch(first)                        # its slot was reused
+    with pytest.raises(Q.QGError):
+        L.measure_fetch(10 ** 9)
+    L.close()
