@@ -208,6 +208,15 @@ int qg_measure_fmunu(qg_ctx *ctx, int field, int index1, int index2, double *out
  * suncl.cpp:1497-1586).  Allocate their scratch on first use.            */
 int qg_measure_action_profile(qg_ctx *ctx, int axis, double *out);
 int qg_measure_polyakov_profile(qg_ctx *ctx, int axis, double *out);
+/* One-pass forms (new): the per-site work once for the totals and the
+ * profiles along all three axes.  out[0..3] = qg_measure's four sums
+ * (plaquette: ReTr spatial, temporal, action spatial, temporal; Polyakov:
+ * Re P, Im P, |P|^2, |P|^4), then 2 n1 + 2 n2 + 2 n3 per-slice sums along
+ * x, y, z (action spatial, temporal; Polyakov Re, Im).  Bit-identical to
+ * qg_measure and qg_measure_*_profile; allocate a 2 V-double site buffer
+ * on first use.                                                            */
+int qg_measure_plaquette_all(qg_ctx *ctx, double *out);
+int qg_measure_polyakov_all(qg_ctx *ctx, double *out);
 
 /* buffer_init / buffer_map of the link table (clinterface.cpp:1296-1434):
  * host arrays in the reference layout, Real = float (precision 0) or
@@ -383,6 +392,9 @@ typedef struct qg_run_options {
     int fmunu_index2;      /* second: 0 = default 8 (SU(3), FMUNU5/6/7: 5..7), 2 (SU(2))*/
     int get_actions_diff;  /* action profiles along x, y, z (ACTIONS_DIFF; the         */
                            /* reference's get_actions_diff, set in its main())         */
+    int tune_shapes;       /* 1 (default): time the phase-kernel launch shapes on this */
+                           /* lattice before the run (qg_tune; all shapes give the     */
+                           /* same chain, so the results do not change)               */
 } qg_run_options;
 
 typedef struct qg_run_result {
@@ -420,7 +432,7 @@ int qg_default_run_options(qg_run_options *opts);
  * GETWILSON GETRETRACE PL_LEVEL WILSONR WILSONT FMUNU F0MU TURNOFFFMUNU
  * FMUNU1 FMUNU2 FMUNU4 FMUNU5 FMUNU6 FMUNU7 (reference) and PRECISION
  * NHITPAR NOR REUNIT_EVERY REUNIT_FP64 PRNG_INSTANCES ROW_ALIGN INIT
- * STATEFILE SAVESTATE SAVEEVERY STATEOUT ACTIONS_DIFF (this build; the
+ * STATEFILE SAVESTATE SAVEEVERY STATEOUT ACTIONS_DIFF TUNE (this build; the
  * reference sets INIT, the state file name and get_actions_diff in main());
  * PLATFORM DEVICE FINISHPATH TURNOFFWAITING REBUILDBINARY are accepted and
  * ignored.  Unknown generators are an error.                               */

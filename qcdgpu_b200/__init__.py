@@ -38,7 +38,7 @@ EXPORTED_SYMBOLS = (
     "qg_batch_create", "qg_batch_destroy", "qg_batch_init", "qg_batch_set_shape", "qg_batch_run", "qg_batch_sync",
     "qg_batch_get_stream", "qg_batch_series", "qg_batch_links_download", "qg_batch_info",
     "qg_measure_wilson_all", "qg_measure_fmunu", "qg_measure_action_profile", "qg_measure_polyakov_profile",
-    "qg_measure_enqueue", "qg_measure_fetch",
+    "qg_measure_enqueue", "qg_measure_fetch", "qg_measure_plaquette_all", "qg_measure_polyakov_all",
     "qg_net_set", "qg_net_get", "qg_mh_phase", "qg_mh_sweep", "qg_mh_stats", "qg_net_grad", "qg_net_train",
 )
 
@@ -109,6 +109,7 @@ class RunOptions(ctypes.Structure):
         ("fmunu_index1", ctypes.c_int),
         ("fmunu_index2", ctypes.c_int),
         ("get_actions_diff", ctypes.c_int),
+        ("tune_shapes", ctypes.c_int),
     ]
 
 
@@ -205,6 +206,8 @@ def load_library(path=LIB_PATH):
     lib.qg_measure_wilson_all.argtypes = [vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, P(ctypes.c_double)]
     lib.qg_measure_fmunu.argtypes = [vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, P(ctypes.c_double)]
     lib.qg_measure_enqueue.argtypes = [vp, ctypes.c_int, P(ctypes.c_uint64)]
+    lib.qg_measure_plaquette_all.argtypes = [vp, P(ctypes.c_double)]
+    lib.qg_measure_polyakov_all.argtypes = [vp, P(ctypes.c_double)]
     lib.qg_measure_fetch.argtypes = [vp, ctypes.c_uint64, P(ctypes.c_double)]
     lib.qg_measure_action_profile.argtypes = [vp, ctypes.c_int, P(ctypes.c_double)]
     lib.qg_measure_polyakov_profile.argtypes = [vp, ctypes.c_int, P(ctypes.c_double)]
@@ -586,6 +589,19 @@ class Lattice:
         out = (ctypes.c_double * 4)()
         self._ck(self.lib.qg_measure_fetch(self.ctx, ticket, out), "qg_measure_fetch")
         return tuple(out)
+
+    def measure_all(self, polyakov=False):
+        """qg_measure_plaquette_all / qg_measure_polyakov_all: (four totals,
+        [profile x, profile y, profile z] each an array [slice][2])"""
+        n = list(self.cfg.size)
+        out = np.zeros(4 + 2 * (n[0] + n[1] + n[2]))
+        fn = self.lib.qg_measure_polyakov_all if polyakov else self.lib.qg_measure_plaquette_all
+        self._ck(fn(self.ctx, out.ctypes.data_as(ctypes.POINTER(ctypes.c_double))), "qg_measure_*_all")
+        prof, o = [], 4
+        for a in range(3):
+            prof.append(out[o:o + 2 * n[a]].reshape(-1, 2))
+            o += 2 * n[a]
+        return tuple(out[:4]), prof
 
     def fmunu(self, field=0, index1=None, index2=None):
         """raw F_munu sums (qg_measure_fmunu): array [2 generators][3 planes]

@@ -53,6 +53,7 @@ struct qg_ctx {
     double *d_wpart = nullptr, *d_wout = nullptr;   // all-loops Wilson measurement (lazy)
     int wpart_rmax = 0;
     double *d_fpart = nullptr, *d_ppart = nullptr, *d_pout = nullptr;   // F_munu / profiles (lazy)
+    double *d_sites = nullptr;      // per-site values of the one-pass measurements (lazy)
     unsigned long long *d_mh_acc = nullptr;
     double *d_mh_jump = nullptr;
     double eps_max = 0.0;
@@ -145,7 +146,7 @@ extern "C" int qg_destroy(qg_ctx *c)
     cudaFree(c->d_netw); cudaFree(c->d_master); cudaFree(c->d_adam_m); cudaFree(c->d_adam_v);
     cudaFree(c->d_grad); cudaFree(c->d_gpart); cudaFree(c->d_mh_acc); cudaFree(c->d_mh_jump);
     cudaFree(c->d_wpart); cudaFree(c->d_wout);
-    cudaFree(c->d_fpart); cudaFree(c->d_ppart); cudaFree(c->d_pout);
+    cudaFree(c->d_fpart); cudaFree(c->d_ppart); cudaFree(c->d_pout); cudaFree(c->d_sites);
     if (c->h_results) cudaFreeHost(c->h_results);
     if (c->h_params) cudaFreeHost(c->h_params);
     if (c->h_ring) cudaFreeHost(c->h_ring);
@@ -881,6 +882,25 @@ static int measure_profile(qg_ctx *c, int kind, int axis, double *out)
     QG_CK(cudaStreamSynchronize(c->stream), "profile sync");
     return QG_OK;
 }
+static int measure_all(qg_ctx *c, int kind, double *out)
+{
+    if (!c || !out) return QG_ERR_ARG;
+    const int nout = 4 + 2 * (c->G.n[0] + c->G.n[1] + c->G.n[2]);
+    if (nout > 2 * 4096) return fail(c, QG_ERR_ARG, "profiles longer than the measurement buffer");
+    const qg_config &f = c->cfg;
+    int tw = !(f.phi == 0.0 && f.omega == 0.0);
+    if (!c->d_ppart) QG_CK(cudaMalloc(&c->d_ppart, profile_partials(c->G) * sizeof(double)), "profile scratch");
+    if (!c->d_pout) QG_CK(cudaMalloc(&c->d_pout, 2 * 4096 * sizeof(double)), "measurement scratch");
+    if (!c->d_sites) QG_CK(cudaMalloc(&c->d_sites, sites_buffer_doubles(c->G) * sizeof(double)), "site buffer");
+    QG_CK(launch_measure_all(c->G, c->links, f.group, f.precision, c->d_params, tw, kind, c->partials, c->d_ppart,
+                             c->d_sites, c->d_pout, c->stream), "one-pass measurement");
+    QG_CK(cudaMemcpyAsync(out, c->d_pout, (size_t)nout * sizeof(double), cudaMemcpyDeviceToHost, c->stream),
+          "measurement copy");
+    QG_CK(cudaStreamSynchronize(c->stream), "measurement sync");
+    return QG_OK;
+}
+extern "C" int qg_measure_plaquette_all(qg_ctx *c, double *out) { return measure_all(c, 0, out); }
+extern "C" int qg_measure_polyakov_all(qg_ctx *c, double *out) { return measure_all(c, 1, out); }
 extern "C" int qg_measure_action_profile(qg_ctx *c, int axis, double *out) { return measure_profile(c, 0, axis, out); }
 extern "C" int qg_measure_polyakov_profile(qg_ctx *c, int axis, double *out) { return measure_profile(c, 1, axis, out); }
 

@@ -364,6 +364,58 @@ cudaError_t launch_polyakov(const Geom &G, const void *links, int group, int pre
     return launch_reduce(partials, nb, 4, out, s);
 }
 
+// One-pass measurements: the per-site work once, the totals exactly as
+// k_plaquette / k_polyakov (same blocks, same reduction), the site values
+// kept in a device buffer, then the per-slice sums of every axis from that
+// buffer in k_profile's order -- so the numbers equal the separate
+// qg_measure / qg_measure_*_profile calls bit for bit.
+template <int NC, typename Real>
+__global__ void __launch_bounds__(256) k_plaq_sites(Field<Real> U, Geom G, const double *params, int twist,
+                                                     double *partials, double *sites)
+{
+    uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+    double v[4] = { 0, 0, 0, 0 };
+    if (s < G.V) {
+        plaq_site<NC, Real>(U, G, params, twist, s, v);
+        sites[s] = v[2];                                 // spatial action of the site
+        sites[(size_t)G.V + s] = v[3];                   // temporal
+    }
+    block_sum_store<4>(v, partials);
+}
+template <int NC, typename Real>
+__global__ void __launch_bounds__(256) k_poly_sites(Field<Real> U, Geom G, double *partials, double *sites)
+{
+    const uint32_t Vs = (uint32_t)G.n[0] * G.n[1] * G.n[2];
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    double v[4] = { 0, 0, 0, 0 };
+    if (i < Vs) {
+        poly_site<NC, Real>(U, G, i, v);
+        sites[i] = v[0];
+        sites[(size_t)Vs + i] = v[1];
+    }
+    block_sum_store<4>(v, partials);
+}
+// k_profile's loop over the stored site values (KIND 0: action per lattice
+// site, lexicographic index; KIND 1: Polyakov trace per spatial site,
+// i = y + N2 (z + N3 x))
+template <int KIND>
+__global__ void __launch_bounds__(256) k_bin_sites(const double *sites, Geom G, int axis, uint32_t per_slice,
+                                                    uint32_t chunks, double *partials)
+{
+    const int k = (int)(blockIdx.x / chunks);
+    const uint32_t j0 = (blockIdx.x % chunks) * 1024u;
+    const uint32_t j1 = min(per_slice, j0 + 1024u);
+    const size_t n = KIND == 0 ? (size_t)G.V : (size_t)G.n[0] * G.n[1] * G.n[2];
+    double acc[2] = { 0, 0 };
+    for (uint32_t j = j0 + threadIdx.x; j < j1; j += blockDim.x) {
+        const Crd c = slice_site(G, axis, k, j, KIND == 1);
+        const size_t s = KIND == 0 ? crd2lex(G, c) : (size_t)c.y + (size_t)G.n[1] * (c.z + (size_t)G.n[2] * c.x);
+        acc[0] += sites[s];
+        acc[1] += sites[n + s];
+    }
+    block_sum_store<2>(acc, partials);
+}
+
 // F_munu (FMUNU / F0MU lattice_measurement_plq, sun_measurements_cl.cl:
 // 712-1175 and reduce_measurement_plq_double2 :1313-1357): 12 sums
 template <int NC, typename Real>
@@ -474,6 +526,42 @@ cudaError_t launch_profile(const Geom &G, const void *links, int group, int prec
     if (e != cudaSuccess) return e;
     k_profile_reduce<<<G.n[axis], 256, 0, s>>>(partials, chunks, out);
     return cudaGetLastError();
+}
+
+size_t sites_buffer_doubles(const Geom &G) { return 2 * (size_t)G.V; }
+
+cudaError_t launch_measure_all(const Geom &G, const void *links, int group, int prec, const double *params, int twist,
+                               int kind, double *partials, double *ppartials, double *sites, double *out,
+                               cudaStream_t s)
+{
+    // totals into out[0..3], site values into `sites`
+    const uint32_t Vs = (uint32_t)G.n[0] * G.n[1] * G.n[2];
+    const uint32_t nb = kind == 0 ? plaq_blocks(G) : (Vs + 255) / 256;
+#define QG_SITES(NC, R)                                                                                 \
+    do {                                                                                                \
+        Field<R> U{ (typename V4<R>::T *)links, G.pstride };                                            \
+        if (kind == 0) k_plaq_sites<NC, R><<<nb, 256, 0, s>>>(U, G, params, twist, partials, sites);   \
+        else k_poly_sites<NC, R><<<nb, 256, 0, s>>>(U, G, partials, sites);                            \
+    } while (0)
+    if (prec) { if (group == 3) QG_SITES(3, double); else QG_SITES(2, double); }
+    else { if (group == 3) QG_SITES(3, float); else QG_SITES(2, float); }
+#undef QG_SITES
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    if ((e = launch_reduce(partials, nb, 4, out, s)) != cudaSuccess) return e;
+    // per-slice sums along x, y, z into out[4 ..]
+    double *o = out + 4;
+    for (int axis = 0; axis < 3; axis++) {
+        const uint32_t per = profile_per_slice(G, axis, kind);
+        const uint32_t chunks = (per + kProfileChunk - 1) / kProfileChunk;
+        const uint32_t nbk = chunks * (uint32_t)G.n[axis];
+        if (kind == 0) k_bin_sites<0><<<nbk, 256, 0, s>>>(sites, G, axis, per, chunks, ppartials);
+        else k_bin_sites<1><<<nbk, 256, 0, s>>>(sites, G, axis, per, chunks, ppartials);
+        k_profile_reduce<<<G.n[axis], 256, 0, s>>>(ppartials, chunks, o);
+        if ((e = cudaGetLastError()) != cudaSuccess) return e;
+        o += 2 * G.n[axis];
+    }
+    return cudaSuccess;
 }
 
 // lattice_measurement_wilson (wilson_loop.cl:55-454): per site and i in

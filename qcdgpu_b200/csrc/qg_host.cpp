@@ -266,6 +266,7 @@ extern "C" int qg_default_run_options(qg_run_options *o)
     o->get_actions = 1;
     o->verify = 1;
     o->write_results = 1;
+    o->tune_shapes = 1;
     o->init = 1;
     snprintf(o->prefix, sizeof(o->prefix), "su3-");
     return QG_OK;
@@ -349,6 +350,7 @@ extern "C" int qg_parse_init_file(const char *path, qg_config *cfg, qg_run_optio
         else if (key == "FMUNU6") o->fmunu_index2 = 6;
         else if (key == "FMUNU7") o->fmunu_index2 = 7;
         else if (key == "ACTIONS_DIFF") o->get_actions_diff = (int)iv;
+        else if (key == "TUNE") o->tune_shapes = (int)iv;
         else if (key == "PLATFORM" || key == "DEVICE" || key == "FINISHPATH" || key == "TURNOFFWAITING" ||
                  key == "REBUILDBINARY" || key.rfind("FMUNU", 0) == 0 || key == "N1") {
             /* device selection, dispatcher handshake and OpenCL binaries have
@@ -460,36 +462,42 @@ extern "C" int qg_run(const qg_config *cfg_in, const qg_run_options *o_in, qg_ru
         rs.fmunu_index2 = fi2;
         rs.get_actions_diff = o->get_actions_diff;
     }
+    // launch shapes for this lattice (field restored, PRN counters untouched)
+    if (o->tune_shapes && (rc = qg_tune(ctx, 4, nullptr))) return bail(rc);
     time_t t_start = time(nullptr);
+    // one measurement per kind of site work: plaquette, action and the
+    // action profiles from one pass (qg_measure_plaquette_all), the Polyakov
+    // loop and its profiles from another -- the same numbers as the separate
+    // qg_measure / qg_measure_*_profile calls
+    std::vector<double> all(4 + plen);
     auto measure = [&](int i) -> int {
         double a[4];
         int r;
-        if (o->get_plaquettes) {
-            if ((r = qg_measure(ctx, QG_MEAS_PLAQUETTE, a))) return r;
-            s_plq[2 * i] = a[0]; s_plq[2 * i + 1] = a[1];
+        const size_t prof_row = prow * (size_t)i;
+        if (o->get_plaquettes || o->get_actions || o->get_actions_diff) {
+            if (o->get_actions || o->get_actions_diff) {
+                if ((r = qg_measure_plaquette_all(ctx, all.data()))) return r;
+                memcpy(a, all.data(), sizeof(a));
+                if (o->get_actions_diff) memcpy(&s_prof[prof_row + poff], all.data() + 4, plen * sizeof(double));
+            } else if ((r = qg_measure(ctx, QG_MEAS_PLAQUETTE, a))) {
+                return r;
+            }
+            if (o->get_plaquettes) { s_plq[2 * i] = a[0]; s_plq[2 * i + 1] = a[1]; }
+            if (o->get_actions) { s_act[2 * i] = a[2]; s_act[2 * i + 1] = a[3]; }
         }
         if (o->get_wilson) {
             if ((r = qg_measure(ctx, QG_MEAS_WILSON, a))) return r;
             s_wil[i] = a[0];
         }
-        if (o->get_actions) {
-            if ((r = qg_measure(ctx, QG_MEAS_ACTION, a))) return r;
-            s_act[2 * i] = a[0]; s_act[2 * i + 1] = a[1];
-        }
-        if (o->pl_level > 0) {
+        if (o->pl_level > 2) {
+            if ((r = qg_measure_polyakov_all(ctx, all.data()))) return r;
+            for (int k = 0; k < 4; k++) s_pol[4 * i + k] = all[k];
+            memcpy(&s_prof[prof_row], all.data() + 4, plen * sizeof(double));
+        } else if (o->pl_level > 0) {
             if ((r = qg_measure(ctx, QG_MEAS_POLYAKOV, a))) return r;
             for (int k = 0; k < 4; k++) s_pol[4 * i + k] = a[k];
         }
         if (o->fmunu && (r = qg_measure_fmunu(ctx, o->fmunu - 1, fi1, fi2, &s_f[12 * (size_t)i]))) return r;
-        size_t off = prow * (size_t)i;
-        for (int axis = 0; axis < 3 && o->pl_level > 2; axis++) {
-            if ((r = qg_measure_polyakov_profile(ctx, axis, &s_prof[off]))) return r;
-            off += 2 * (size_t)cfg.size[axis];
-        }
-        for (int axis = 0; axis < 3 && o->get_actions_diff; axis++) {
-            if ((r = qg_measure_action_profile(ctx, axis, &s_prof[off]))) return r;
-            off += 2 * (size_t)cfg.size[axis];
-        }
         return QG_OK;
     };
     // lattice_save_state: the name the reference gives it, or STATEOUT

@@ -57,6 +57,14 @@ cudaError_t launch_fmunu(const Geom &G, const void *links, int group, int prec, 
 // per-slice sums along axis 0..2: kind 0 action (spatial, temporal), kind 1
 // Polyakov trace (Re, Im); out holds 2 n[axis] doubles
 uint32_t profile_partials(const Geom &G);
+// kind 0: plaquette/action totals (out[0..3] as k_plaquette) and the action
+// profiles along x, y, z; kind 1: Polyakov totals (as k_polyakov) and its
+// profiles; out[4 ..] = 2 n1 + 2 n2 + 2 n3 per-slice sums; sites holds
+// sites_buffer_doubles(G)
+size_t sites_buffer_doubles(const Geom &G);
+cudaError_t launch_measure_all(const Geom &G, const void *links, int group, int prec, const double *params, int twist,
+                               int kind, double *partials, double *ppartials, double *sites, double *out,
+                               cudaStream_t s);
 cudaError_t launch_profile(const Geom &G, const void *links, int group, int prec, const double *params, int twist,
                            int kind, int axis, double *partials, double *out, cudaStream_t s);
 int wilson_all_blocks(const Geom &G);

@@ -501,3 +501,24 @@ def test_async_measurements_and_parameter_staging():
     with pytest.raises(Q.QGError):
         L.measure_fetch(10 ** 9)
     L.close()
+
+
+@pytest.mark.parametrize("group,precision,twist", [(3, 0, False), (3, 1, True), (2, 1, False)])
+def test_one_pass_measurements_equal_the_separate_ones(group, precision, twist):
+    """qg_measure_plaquette_all / _polyakov_all: totals and all three
+    profiles bit-identical to qg_measure and qg_measure_*_profile"""
+    phi, omega = (0.3, 0.7) if twist else (0.0, 0.0)
+    L, c = make_pair(group, (6, 4, 4, 8), precision, start=Q.START_HOT, prng=Q.PRNG_RANLUX,
+                     beta=5.8 if group == 3 else 2.3, phi=phi, omega=omega)
+    L.seed(54)
+    L.init(Q.START_HOT)
+    L.sweep(1)
+    tot, prof = L.measure_all()
+    assert tot[:2] == tuple(L.plaquette_sums()) and tot[2:] == tuple(L.action_sums())
+    for a in range(3):
+        assert np.array_equal(prof[a], L.action_profile(a)), a
+    tot, prof = L.measure_all(polyakov=True)
+    assert tot == tuple(L.polyakov_sums())
+    for a in range(3):
+        assert np.array_equal(prof[a], L.polyakov_profile(a)), a
+    L.close()

@@ -68,3 +68,6 @@ def test_fmunu_and_profile_keys(tmp_path):
     assert o.fmunu == 2 and o.fmunu_index1 == 2
     cfg, o = Q.parse_init_file(write(tmp_path, "F0MU = 1\nTURNOFFFMUNU = 1\nFMUNU3 = 1\n"))
     assert o.fmunu == 0
+    assert d.tune_shapes == 1
+    cfg, o = Q.parse_init_file(write(tmp_path, "TUNE = 0\n"))
+    assert o.tune_shapes == 0
