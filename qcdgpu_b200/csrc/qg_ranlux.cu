@@ -5,7 +5,8 @@
 // borrow arithmetic on multiples of 2^-24 is exact in FP32, and the small-
 // value refinement is one correctly rounded add of an exact product.
 //
-// The 24-word state lives in registers.  Within a block of 24 outputs the
+// The 24-word state lives in registers (as exact integers, rl_step).
+// Within a block of 24 outputs the
 // word indices are compile-time constants (switch on the float4 number
 // 0..5); the luxury skip of NSKIP words is whole 24-step rounds plus
 // NSKIP%24 single steps followed by a register rotation that restores the
@@ -17,58 +18,65 @@ namespace qg {
 #define RL_TWOM24 5.9604644775390625e-8f
 #define RL_TWOM12 2.44140625e-4f
 
-__device__ __forceinline__ float rl_step(float (&s)[24], int i, int j, float &carry)
+// The words are kept as exact 24-bit integers W = word * 2^24 and the
+// borrow as 0/1: one subtract-with-borrow step is W_i = W_j - W_i - c,
+// c = (W_i < 0), W_i += c * 2^24 -- the float recurrence of the reference
+// (u = s[j] - s[i] - carry; u < 0: u += 1, carry = 2^-24) on the same exact
+// values, with an integer add and a shift on the borrow chain in place of
+// float subtract, compare and select.  Outputs and the table are floats.
+__device__ __forceinline__ int32_t rl_step(int32_t (&w)[24], int i, int j, int32_t &c)
 {
-    float u = s[j] - s[i] - carry;
-    if (u < 0.0f) { u += 1.0f; carry = RL_TWOM24; } else { carry = 0.0f; }
-    s[i] = u;
+    int32_t u = w[j] - w[i] - c;
+    c = (int32_t)((uint32_t)u >> 31);
+    u += c << 24;
+    w[i] = u;
     return u;
 }
 
 // q-th output of a block: i24 = 23-q, j24 = (9-q) mod 24; the refinement
 // reads the word at the decremented j24
 template <int Q>
-__device__ __forceinline__ float rl_out(float (&s)[24], float &carry)
+__device__ __forceinline__ float rl_out(int32_t (&w)[24], int32_t &c)
 {
     constexpr int I = 23 - Q;
     constexpr int J = (33 - Q) % 24;
     constexpr int JN = (32 - Q) % 24;
-    float u = rl_step(s, I, J, carry);
+    float u = (float)rl_step(w, I, J, c) * RL_TWOM24;
     if (u < RL_TWOM12) {
-        u = u + RL_TWOM24 * s[JN];
+        u = u + RL_TWOM24 * ((float)w[JN] * RL_TWOM24);
         if (u == 0.0f) u = RL_TWOM24 * RL_TWOM24;
     }
     return u;
 }
 
 template <int M>
-__device__ __forceinline__ float4 rl_quad(float (&s)[24], float &carry)
+__device__ __forceinline__ float4 rl_quad(int32_t (&w)[24], int32_t &c)
 {
     float4 r;
-    r.x = rl_out<4 * M + 0>(s, carry);
-    r.y = rl_out<4 * M + 1>(s, carry);
-    r.z = rl_out<4 * M + 2>(s, carry);
-    r.w = rl_out<4 * M + 3>(s, carry);
+    r.x = rl_out<4 * M + 0>(w, c);
+    r.y = rl_out<4 * M + 1>(w, c);
+    r.z = rl_out<4 * M + 2>(w, c);
+    r.w = rl_out<4 * M + 3>(w, c);
     return r;
 }
 
 template <int NSKIP>
-__device__ __forceinline__ void rl_skip(float (&s)[24], float &carry)
+__device__ __forceinline__ void rl_skip(int32_t (&w)[24], int32_t &c)
 {
 #pragma unroll 1
     for (int r = 0; r < NSKIP / 24; r++) {
 #pragma unroll
-        for (int q = 0; q < 24; q++) rl_step(s, 23 - q, (33 - q) % 24, carry);
+        for (int q = 0; q < 24; q++) rl_step(w, 23 - q, (33 - q) % 24, c);
     }
     constexpr int R = NSKIP % 24;
 #pragma unroll
-    for (int q = 0; q < R; q++) rl_step(s, 23 - q, (33 - q) % 24, carry);
+    for (int q = 0; q < R; q++) rl_step(w, 23 - q, (33 - q) % 24, c);
     if (R) {
-        float t[24];
+        int32_t t[24];
 #pragma unroll
-        for (int k = 0; k < 24; k++) t[(k + R) % 24] = s[k];
+        for (int k = 0; k < 24; k++) t[(k + R) % 24] = w[k];
 #pragma unroll
-        for (int k = 0; k < 24; k++) s[k] = t[k];
+        for (int k = 0; k < 24; k++) w[k] = t[k];
     }
 }
 
@@ -77,33 +85,36 @@ __global__ void __launch_bounds__(128) k_ranlux(float4 *table, float4 *prns, int
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= instances) return;
-    float s[24];
+    int32_t w[24];
 #pragma unroll
     for (int k = 0; k < 6; k++) {
         float4 v = table[(size_t)k * instances + i];
-        s[4 * k] = v.x; s[4 * k + 1] = v.y; s[4 * k + 2] = v.z; s[4 * k + 3] = v.w;
+        w[4 * k] = (int32_t)(v.x * 16777216.0f); w[4 * k + 1] = (int32_t)(v.y * 16777216.0f);
+        w[4 * k + 2] = (int32_t)(v.z * 16777216.0f); w[4 * k + 3] = (int32_t)(v.w * 16777216.0f);
     }
     float4 ci = table[(size_t)6 * instances + i];
     int in24 = (int)ci.z;
-    float carry = ci.w;
+    int32_t c = ci.w != 0.0f ? 1 : 0;
     for (int n = 0; n < samples; n++) {
-        if (in24 >= 6) { rl_skip<NSKIP>(s, carry); in24 = 0; }
+        if (in24 >= 6) { rl_skip<NSKIP>(w, c); in24 = 0; }
         float4 out;
         switch (in24) {
-        case 0: out = rl_quad<0>(s, carry); break;
-        case 1: out = rl_quad<1>(s, carry); break;
-        case 2: out = rl_quad<2>(s, carry); break;
-        case 3: out = rl_quad<3>(s, carry); break;
-        case 4: out = rl_quad<4>(s, carry); break;
-        default: out = rl_quad<5>(s, carry); break;
+        case 0: out = rl_quad<0>(w, c); break;
+        case 1: out = rl_quad<1>(w, c); break;
+        case 2: out = rl_quad<2>(w, c); break;
+        case 3: out = rl_quad<3>(w, c); break;
+        case 4: out = rl_quad<4>(w, c); break;
+        default: out = rl_quad<5>(w, c); break;
         }
         in24++;
         prns[(size_t)n * instances + i] = out;
     }
 #pragma unroll
     for (int k = 0; k < 6; k++)
-        table[(size_t)k * instances + i] = make_float4(s[4 * k], s[4 * k + 1], s[4 * k + 2], s[4 * k + 3]);
-    table[(size_t)6 * instances + i] = make_float4(0.0f, 0.0f, (float)in24, carry);
+        table[(size_t)k * instances + i] =
+            make_float4((float)w[4 * k] * RL_TWOM24, (float)w[4 * k + 1] * RL_TWOM24, (float)w[4 * k + 2] * RL_TWOM24,
+                        (float)w[4 * k + 3] * RL_TWOM24);
+    table[(size_t)6 * instances + i] = make_float4(0.0f, 0.0f, (float)in24, c ? RL_TWOM24 : 0.0f);
 }
 
 // ranlux_init (prngcl_ranlux.cl:137-157): 24 seed words from the
