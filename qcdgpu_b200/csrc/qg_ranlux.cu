@@ -18,65 +18,130 @@ namespace qg {
 #define RL_TWOM24 5.9604644775390625e-8f
 #define RL_TWOM12 2.44140625e-4f
 
-// The words are kept as exact 24-bit integers W = word * 2^24 and the
-// borrow as 0/1: one subtract-with-borrow step is W_i = W_j - W_i - c,
-// c = (W_i < 0), W_i += c * 2^24 -- the float recurrence of the reference
-// (u = s[j] - s[i] - carry; u < 0: u += 1, carry = 2^-24) on the same exact
-// values, with an integer add and a shift on the borrow chain in place of
-// float subtract, compare and select.  Outputs and the table are floats.
-__device__ __forceinline__ int32_t rl_step(int32_t (&w)[24], int i, int j, int32_t &c)
+// The words are kept as exact integers x = (word * 2^24) << 8 (the 24
+// significant bits at the top of a 32-bit register) and the borrow as 0/1:
+// a subtract-with-borrow step is x_i = x_j - x_i - 256 c (mod 2^32), with
+// c = the borrow of that subtraction -- the float recurrence of the
+// reference (u = s[j] - s[i] - carry; u < 0: u += 1, carry = 2^-24) on the
+// same exact values.  Outputs and the table are floats (x * 2^-32, exact).
+__device__ __forceinline__ uint32_t rl_step(uint32_t (&x)[24], int i, int j, uint32_t &c)
 {
-    int32_t u = w[j] - w[i] - c;
-    c = (int32_t)((uint32_t)u >> 31);
-    u += c << 24;
-    w[i] = u;
+    const uint32_t a = x[j], b = x[i];
+    const uint32_t u = a - b - (c << 8);
+    c = (a < b || (a == b && c)) ? 1u : 0u;
+    x[i] = u;
     return u;
+}
+__device__ __forceinline__ float rl_float(uint32_t x) { return __uint2float_rn(x) * 2.3283064365386963e-10f; }
+
+// One round of 24 steps (i24 = 23 .. 0 with j24 = 9 .. 0, 23 .. 10) on
+// words held as x = w << 8 in one asm block: each step one subtraction
+// with borrow-in and borrow-out (the carry flag is the subtract-with-
+// borrow borrow; the 2^24 wrap of a word is the 2^32 wrap of x) and a mask
+// of the low byte, which a borrow-in fills with ones.  and.b32 leaves the
+// flag alone, so the borrow chain is one instruction per step.
+__device__ __forceinline__ void rl_round24(uint32_t (&x)[24], uint32_t &c)
+{
+    asm volatile(
+        "{\n\t"
+        ".reg .u32 z, t;\n\t"
+        "mov.u32 z, 0;\n\t"
+        "sub.cc.u32 t, z, %24;\n\t"
+        "subc.cc.u32 %23, %9, %23;\n\t"
+        "and.b32 %23, %23, 0xffffff00;\n\t"
+        "subc.cc.u32 %22, %8, %22;\n\t"
+        "and.b32 %22, %22, 0xffffff00;\n\t"
+        "subc.cc.u32 %21, %7, %21;\n\t"
+        "and.b32 %21, %21, 0xffffff00;\n\t"
+        "subc.cc.u32 %20, %6, %20;\n\t"
+        "and.b32 %20, %20, 0xffffff00;\n\t"
+        "subc.cc.u32 %19, %5, %19;\n\t"
+        "and.b32 %19, %19, 0xffffff00;\n\t"
+        "subc.cc.u32 %18, %4, %18;\n\t"
+        "and.b32 %18, %18, 0xffffff00;\n\t"
+        "subc.cc.u32 %17, %3, %17;\n\t"
+        "and.b32 %17, %17, 0xffffff00;\n\t"
+        "subc.cc.u32 %16, %2, %16;\n\t"
+        "and.b32 %16, %16, 0xffffff00;\n\t"
+        "subc.cc.u32 %15, %1, %15;\n\t"
+        "and.b32 %15, %15, 0xffffff00;\n\t"
+        "subc.cc.u32 %14, %0, %14;\n\t"
+        "and.b32 %14, %14, 0xffffff00;\n\t"
+        "subc.cc.u32 %13, %23, %13;\n\t"
+        "and.b32 %13, %13, 0xffffff00;\n\t"
+        "subc.cc.u32 %12, %22, %12;\n\t"
+        "and.b32 %12, %12, 0xffffff00;\n\t"
+        "subc.cc.u32 %11, %21, %11;\n\t"
+        "and.b32 %11, %11, 0xffffff00;\n\t"
+        "subc.cc.u32 %10, %20, %10;\n\t"
+        "and.b32 %10, %10, 0xffffff00;\n\t"
+        "subc.cc.u32 %9, %19, %9;\n\t"
+        "and.b32 %9, %9, 0xffffff00;\n\t"
+        "subc.cc.u32 %8, %18, %8;\n\t"
+        "and.b32 %8, %8, 0xffffff00;\n\t"
+        "subc.cc.u32 %7, %17, %7;\n\t"
+        "and.b32 %7, %7, 0xffffff00;\n\t"
+        "subc.cc.u32 %6, %16, %6;\n\t"
+        "and.b32 %6, %6, 0xffffff00;\n\t"
+        "subc.cc.u32 %5, %15, %5;\n\t"
+        "and.b32 %5, %5, 0xffffff00;\n\t"
+        "subc.cc.u32 %4, %14, %4;\n\t"
+        "and.b32 %4, %4, 0xffffff00;\n\t"
+        "subc.cc.u32 %3, %13, %3;\n\t"
+        "and.b32 %3, %3, 0xffffff00;\n\t"
+        "subc.cc.u32 %2, %12, %2;\n\t"
+        "and.b32 %2, %2, 0xffffff00;\n\t"
+        "subc.cc.u32 %1, %11, %1;\n\t"
+        "and.b32 %1, %1, 0xffffff00;\n\t"
+        "subc.cc.u32 %0, %10, %0;\n\t"
+        "and.b32 %0, %0, 0xffffff00;\n\t"
+        "subc.u32 t, z, z;\n\t"
+        "neg.s32 %24, t;\n\t"
+        "}"
+        : "+r"(x[0]), "+r"(x[1]), "+r"(x[2]), "+r"(x[3]), "+r"(x[4]), "+r"(x[5]), "+r"(x[6]), "+r"(x[7]), "+r"(x[8]), "+r"(x[9]), "+r"(x[10]), "+r"(x[11]), "+r"(x[12]), "+r"(x[13]), "+r"(x[14]), "+r"(x[15]), "+r"(x[16]), "+r"(x[17]), "+r"(x[18]), "+r"(x[19]), "+r"(x[20]), "+r"(x[21]), "+r"(x[22]), "+r"(x[23]), "+r"(c));
 }
 
 // q-th output of a block: i24 = 23-q, j24 = (9-q) mod 24; the refinement
 // reads the word at the decremented j24
 template <int Q>
-__device__ __forceinline__ float rl_out(int32_t (&w)[24], int32_t &c)
+__device__ __forceinline__ float rl_out(uint32_t (&x)[24], uint32_t &c)
 {
     constexpr int I = 23 - Q;
     constexpr int J = (33 - Q) % 24;
     constexpr int JN = (32 - Q) % 24;
-    float u = (float)rl_step(w, I, J, c) * RL_TWOM24;
+    float u = rl_float(rl_step(x, I, J, c));
     if (u < RL_TWOM12) {
-        u = u + RL_TWOM24 * ((float)w[JN] * RL_TWOM24);
+        u = u + RL_TWOM24 * rl_float(x[JN]);
         if (u == 0.0f) u = RL_TWOM24 * RL_TWOM24;
     }
     return u;
 }
 
 template <int M>
-__device__ __forceinline__ float4 rl_quad(int32_t (&w)[24], int32_t &c)
+__device__ __forceinline__ float4 rl_quad(uint32_t (&x)[24], uint32_t &c)
 {
     float4 r;
-    r.x = rl_out<4 * M + 0>(w, c);
-    r.y = rl_out<4 * M + 1>(w, c);
-    r.z = rl_out<4 * M + 2>(w, c);
-    r.w = rl_out<4 * M + 3>(w, c);
+    r.x = rl_out<4 * M + 0>(x, c);
+    r.y = rl_out<4 * M + 1>(x, c);
+    r.z = rl_out<4 * M + 2>(x, c);
+    r.w = rl_out<4 * M + 3>(x, c);
     return r;
 }
 
 template <int NSKIP>
-__device__ __forceinline__ void rl_skip(int32_t (&w)[24], int32_t &c)
+__device__ __forceinline__ void rl_skip(uint32_t (&x)[24], uint32_t &c)
 {
 #pragma unroll 1
-    for (int r = 0; r < NSKIP / 24; r++) {
-#pragma unroll
-        for (int q = 0; q < 24; q++) rl_step(w, 23 - q, (33 - q) % 24, c);
-    }
+    for (int r = 0; r < NSKIP / 24; r++) rl_round24(x, c);
     constexpr int R = NSKIP % 24;
 #pragma unroll
-    for (int q = 0; q < R; q++) rl_step(w, 23 - q, (33 - q) % 24, c);
+    for (int q = 0; q < R; q++) rl_step(x, 23 - q, (33 - q) % 24, c);
     if (R) {
-        int32_t t[24];
+        uint32_t t[24];
 #pragma unroll
-        for (int k = 0; k < 24; k++) t[(k + R) % 24] = w[k];
+        for (int k = 0; k < 24; k++) t[(k + R) % 24] = x[k];
 #pragma unroll
-        for (int k = 0; k < 24; k++) w[k] = t[k];
+        for (int k = 0; k < 24; k++) x[k] = t[k];
     }
 }
 
@@ -85,26 +150,26 @@ __global__ void __launch_bounds__(128) k_ranlux(float4 *table, float4 *prns, int
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= instances) return;
-    int32_t w[24];
+    uint32_t x[24];
 #pragma unroll
     for (int k = 0; k < 6; k++) {
         float4 v = table[(size_t)k * instances + i];
-        w[4 * k] = (int32_t)(v.x * 16777216.0f); w[4 * k + 1] = (int32_t)(v.y * 16777216.0f);
-        w[4 * k + 2] = (int32_t)(v.z * 16777216.0f); w[4 * k + 3] = (int32_t)(v.w * 16777216.0f);
+        x[4 * k] = (uint32_t)(v.x * 16777216.0f) << 8; x[4 * k + 1] = (uint32_t)(v.y * 16777216.0f) << 8;
+        x[4 * k + 2] = (uint32_t)(v.z * 16777216.0f) << 8; x[4 * k + 3] = (uint32_t)(v.w * 16777216.0f) << 8;
     }
     float4 ci = table[(size_t)6 * instances + i];
     int in24 = (int)ci.z;
-    int32_t c = ci.w != 0.0f ? 1 : 0;
+    uint32_t c = ci.w != 0.0f ? 1u : 0u;
     for (int n = 0; n < samples; n++) {
-        if (in24 >= 6) { rl_skip<NSKIP>(w, c); in24 = 0; }
+        if (in24 >= 6) { rl_skip<NSKIP>(x, c); in24 = 0; }
         float4 out;
         switch (in24) {
-        case 0: out = rl_quad<0>(w, c); break;
-        case 1: out = rl_quad<1>(w, c); break;
-        case 2: out = rl_quad<2>(w, c); break;
-        case 3: out = rl_quad<3>(w, c); break;
-        case 4: out = rl_quad<4>(w, c); break;
-        default: out = rl_quad<5>(w, c); break;
+        case 0: out = rl_quad<0>(x, c); break;
+        case 1: out = rl_quad<1>(x, c); break;
+        case 2: out = rl_quad<2>(x, c); break;
+        case 3: out = rl_quad<3>(x, c); break;
+        case 4: out = rl_quad<4>(x, c); break;
+        default: out = rl_quad<5>(x, c); break;
         }
         in24++;
         prns[(size_t)n * instances + i] = out;
@@ -112,8 +177,7 @@ __global__ void __launch_bounds__(128) k_ranlux(float4 *table, float4 *prns, int
 #pragma unroll
     for (int k = 0; k < 6; k++)
         table[(size_t)k * instances + i] =
-            make_float4((float)w[4 * k] * RL_TWOM24, (float)w[4 * k + 1] * RL_TWOM24, (float)w[4 * k + 2] * RL_TWOM24,
-                        (float)w[4 * k + 3] * RL_TWOM24);
+            make_float4(rl_float(x[4 * k]), rl_float(x[4 * k + 1]), rl_float(x[4 * k + 2]), rl_float(x[4 * k + 3]));
     table[(size_t)6 * instances + i] = make_float4(0.0f, 0.0f, (float)in24, c ? RL_TWOM24 : 0.0f);
 }
 
