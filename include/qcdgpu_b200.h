@@ -432,7 +432,7 @@ int qg_default_run_options(qg_run_options *opts);
  * GETWILSON GETRETRACE PL_LEVEL WILSONR WILSONT FMUNU F0MU TURNOFFFMUNU
  * FMUNU1 FMUNU2 FMUNU4 FMUNU5 FMUNU6 FMUNU7 (reference) and PRECISION
  * NHITPAR NOR REUNIT_EVERY REUNIT_FP64 PRNG_INSTANCES ROW_ALIGN INIT
- * STATEFILE SAVESTATE SAVEEVERY STATEOUT ACTIONS_DIFF TUNE (this build; the
+ * STATEFILE SAVESTATE SAVEEVERY STATEOUT ACTIONS_DIFF TUNE (this library; the
  * reference sets INIT, the state file name and get_actions_diff in main());
  * PLATFORM DEVICE FINISHPATH TURNOFFWAITING REBUILDBINARY are accepted and
  * ignored.  Unknown generators are an error.                               */
@@ -459,7 +459,7 @@ int qg_run(const qg_config *cfg, const qg_run_options *opts, qg_run_result *res)
  * lattice_polyakov_loop (double2 x header[35]: Re, Im sums) if header[25],
  * then the link table in the reference layout (float4 / double4).  Words
  * 48-59 of the header and a tagged block after the link table (|P|^2,
- * |P|^4 sums) are this build's additions; the reference's loader does not
+ * |P|^4 sums) are this library's additions; the reference's loader does not
  * read them.                                                              */
 #define QCDGPU_STATE_HEADER_WORDS 64
 typedef struct qg_run_state {

@@ -5,7 +5,7 @@
  * TEST INFRASTRUCTURE ONLY.  Included once at the end of qg_oracle.c, after
  * the float instantiation of qg_oracle_impl.h, whose staple terms, algebra
  * and Gram-Schmidt it reuses.  The reference has no such update; this file
- * restates this build's own definition (qcdgpu_b200/csrc/qg_learned.cu) in
+ * restates this library's own definition (qcdgpu_b200/csrc/qg_learned.cu) in
  * the same operation order, so that the Metropolis chain is reproduced bit
  * for bit and the training gradient to FP32 accumulation error:
  *   features  -> staple_features,   network -> mlp_out,

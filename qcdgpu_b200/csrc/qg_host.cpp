@@ -354,7 +354,7 @@ extern "C" int qg_parse_init_file(const char *path, qg_config *cfg, qg_run_optio
         else if (key == "PLATFORM" || key == "DEVICE" || key == "FINISHPATH" || key == "TURNOFFWAITING" ||
                  key == "REBUILDBINARY" || key.rfind("FMUNU", 0) == 0 || key == "N1") {
             /* device selection, dispatcher handshake and OpenCL binaries have
-               no role in this build; FMUNU3, FMUNU8, ... select nothing in the
+               no role in this library; FMUNU3, FMUNU8, ... select nothing in the
                reference either */
         }
         else {

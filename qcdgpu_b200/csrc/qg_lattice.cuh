@@ -4,7 +4,7 @@
 // Site numbering follows the reference (SU(N)/suncl/sun_common.cl:41-66):
 // s = y + N2*z + N2*N3*t + N2*N3*N4*x, y fastest, x slowest.
 //
-// HBM layout of the link field (this build's own): 12 planes (SU(3)) or 4
+// HBM layout of the link field (this library's own): 12 planes (SU(3)) or 4
 // planes (SU(2)) of 4-vectors in the reference's plane order (plane
 // dir + 4*k, k = row part), but inside each plane the sites are
 // checkerboarded: element (parity, s>>1) at parity*cb + (s>>1).  A phase

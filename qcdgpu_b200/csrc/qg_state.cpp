@@ -8,7 +8,7 @@
 // buffers, then the link table in the reference layout.  The word order,
 // the code tables (start, generator, precision) and the buffer order follow
 // the reference so that files interchange; header words 48-59 and a tagged
-// block after the link table carry what this build adds (Philox counter,
+// block after the link table carry what this library adds (Philox counter,
 // overrelaxation and reunitarisation settings, |P|^2 and |P|^4 series).
 #include <math.h>
 #include <stdio.h>
@@ -41,7 +41,7 @@ uint32_t str_word(const char *s, size_t off)
 
 const char *kPrefix = "QCDGPU";
 const char *kVersion = "1.5";                // QCDGPU.cpp:42, the version the reference writes
-const char *kExtTag = "B200";                // marks this build's header words 48-59
+const char *kExtTag = "B200";                // marks this library's header words 48-59
 const char *kTailTag = "QGP4";               // tagged |P|^2, |P|^4 block after the table
 const char *kProfTag = "QGPF";               // tagged block of the per-iteration profiles after it
 
@@ -52,13 +52,13 @@ enum {
     W_OMEGA_LO, W_OMEGA_HI, W_PL_LEVEL, W_FMUNU1, W_FMUNU2, W_GET_FMUNU, W_GET_ACTIONS, W_GET_PLAQUETTES,
     W_GET_WILSON, W_MEAS_SIZE_F, W_ENERGIES_SIZE, W_ENERGIES_SIZE_F, W_POLYAKOV_SIZE, W_GROUP, W_ND,
     W_FULL_SIZE, W_DOMAIN_SIZE = W_FULL_SIZE + 4,
-    // this build
+    // this library
     W_EXT_TAG = 48, W_PRNG_KIND, W_PHASE_LO, W_PHASE_HI, W_SWEEPS_LO, W_SWEEPS_HI, W_NOR, W_REUNIT_EVERY,
     W_REUNIT_FP64, W_NHITPAR, W_INSTANCES, W_ROW_ALIGN, W_FMUNU_KIND, W_ACTIONS_DIFF
 };
 
 // PRNG::convert_generator_to_uint (random.cpp:110-123): RANLUX0..4 = 2..6;
-// the counter-based stream of this build gets 12, a code the reference
+// the counter-based stream of this library gets 12, a code the reference
 // does not use
 uint32_t generator_code(const qg_config &c)
 {
@@ -84,7 +84,7 @@ struct Sizes {
 };
 
 // buffer sizes as lattice_create_buffers computes them (suncl.cpp:2266-2291),
-// with the alignment of this build's ROWSIZE in place of the device's
+// with the alignment of this library's ROWSIZE in place of the device's
 // work-group size
 Sizes sizes_for(const qg_config &c, int iter)
 {
@@ -124,7 +124,7 @@ extern "C" int qg_write_state_file(const char *path, const qg_config *cfg, const
     h[1] = str_word(kPrefix, 4);
     h[2] = str_word(kVersion, 0);
     h[W_INIT] = (uint32_t)st->init;
-    h[W_INTS] = (uint32_t)c.start;            // hot 0, cold 1, gid 2 (Haar 3 is this build's)
+    h[W_INTS] = (uint32_t)c.start;            // hot 0, cold 1, gid 2 (Haar 3 is this library's)
     h[W_SERIES] = c.randseries;
     h[W_GEN] = generator_code(c);
     h[W_NSKIP] = (uint32_t)c.ranlux_nskip;
@@ -179,7 +179,7 @@ extern "C" int qg_write_state_file(const char *path, const qg_config *cfg, const
     std::vector<double> meas(2 * (size_t)z.meas_F, 0.0), en(2 * (size_t)z.energies, 0.0),
         plq(2 * (size_t)z.energies_F, 0.0), wil((size_t)z.energies, 0.0), pol(2 * (size_t)z.polyakov, 0.0),
         p24(2 * (size_t)z.polyakov, 0.0);
-    // the per-iteration profile rows (this build's tail block)
+    // the per-iteration profile rows (this library's tail block)
     const size_t plen = 2 * (size_t)(c.size[0] + c.size[1] + c.size[2]);
     const size_t prow = (st->pl_level > 2 ? plen : 0) + (st->get_actions_diff ? plen : 0);
     std::vector<double> prof(prow * (size_t)z.energies, 0.0);   // rows: the series' aligned length

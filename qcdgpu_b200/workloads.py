@@ -1,5 +1,5 @@
-"""The named run configurations of this build on one GPU, with the
-observables and numbers each one is judged by.
+"""The named run configurations on one GPU, with the observables and
+numbers each one reports.
 
   python -m qcdgpu_b200.workloads --config c1|c2|c2b|c5 [--sweeps N] [--therm N]
 

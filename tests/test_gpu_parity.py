@@ -1,6 +1,6 @@
 """CUDA sweep vs the CPU oracle, through the C-ABI (libqg_sun.so).
 
-Tolerances (north star): link fields after phases/sweeps fed the same PRN
+Tolerances (the parity targets): link fields after phases/sweeps fed the same PRN
 stream: max|dU| <= 1e-12 (FP64 links) / 2e-6 (FP32 links); plaquette and
 Polyakov sums on fixed configurations: 1e-13 / 1e-6 relative; RANLUX and
 Philox streams: bit-exact.

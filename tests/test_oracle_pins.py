@@ -103,7 +103,7 @@ def test_gid_mode_matches_reference_cpu_path(case):
 
 
 def test_cold_start_observables_exact():
-    """Cold start: Plq = N, P = 1 exactly (SURVEY known answer)."""
+    """Cold start: Plq = N, P = 1 exactly (a known answer)."""
     for g in (2, 3):
         c = O.make_cfg(group=g, dims=(4, 4, 4, 6), precision=0)
         t = O.new_table(c)
