@@ -302,7 +302,11 @@ def run_ours(args):
         "roofline": {"bound": "hbm", "kernel": dom + " phase", "achieved": achieved, "peak": peak,
                      "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
                      "algorithmic_bytes_per_launch": alg_bytes, "ms_per_launch": dom_ms,
-                     "ms_per_launch_hb": ms_hb, "ms_per_launch_or": ms_or},
+                     "ms_per_launch_hb": ms_hb, "ms_per_launch_or": ms_or,
+                     # the literature's per-update count with no reuse between sites (19 link reads + 1
+                     # write); above the HBM peak because neighbouring sites share their links in L2
+                     "naive_bytes_per_update": 20 * LINK_BYTES,
+                     "naive_gbs": 20 * LINK_BYTES * (V / 2) / (dom_ms * 1e-3) / 1e9},
         "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": 32, "d2h_bytes_per_step": 16,
                 "what": "qg_set_params + qg_sweep + the step's plaquette sums read back (qg_measure_enqueue / "
                         "_fetch, one step behind), host wall clock"},
