@@ -326,8 +326,18 @@ int qg_batch_destroy(qg_batch *b);
 /* QG_START_COLD / HOT (Philox hot start) / HAAR for every ensemble; resets
  * the phase and measurement counters                                      */
 int qg_batch_init(qg_batch *b, int start);
-/* phase-kernel shape of the batched launches: 0 registers, 4 staged      */
+/* phase-kernel launch shapes of the batched launches, numbered as for
+ * qg_tune (0-4; shape 5 is single-lattice only): set_shape sets both kinds,
+ * set_shapes each; qg_batch_tune (new) times every shape of both kinds on
+ * the live fields (restored; no counter moves), keeps the fastest per kind
+ * and, if times_ms is given (2*QG_BATCH_SHAPES floats), stores per shape v
+ * [2v] heatbath and [2v+1] overrelaxation ms per launch.  All shapes
+ * compute the same operation sequence.                                    */
+#define QG_BATCH_SHAPES 5
 int qg_batch_set_shape(qg_batch *b, int shape);
+int qg_batch_set_shapes(qg_batch *b, int heatbath_shape, int overrelax_shape);
+int qg_batch_get_shapes(qg_batch *b, int *heatbath_shape, int *overrelax_shape);
+int qg_batch_tune(qg_batch *b, int reps, float *times_ms);
 /* nsweeps sweeps of every ensemble (graph replays); after every
  * measure_every-th sweep (0 = never) plaquette, action and Polyakov sums of
  * every ensemble are appended to the device series                         */

@@ -25,6 +25,7 @@ FMUNU_H, FMUNU_E = 0, 1
 FMUNU_COLS = 16                     # QG_FMUNU_COLS
 MEASURE_SLOTS = 64                  # QG_MEASURE_SLOTS
 TUNE_SHAPES = 6                     # QG_TUNE_SHAPES
+BATCH_SHAPES = 5                    # QG_BATCH_SHAPES
 NET_FEATURES, NET_HIDDEN, NET_PARAMS = 8, 32, 1377   # QG_NET_*
 
 EXPORTED_SYMBOLS = (
@@ -37,6 +38,7 @@ EXPORTED_SYMBOLS = (
     "qg_write_state_file", "qg_read_state_file", "qg_save_state", "qg_tau_int",
     "qg_batch_create", "qg_batch_destroy", "qg_batch_init", "qg_batch_set_shape", "qg_batch_run", "qg_batch_sync",
     "qg_batch_get_stream", "qg_batch_series", "qg_batch_links_download", "qg_batch_info",
+    "qg_batch_set_shapes", "qg_batch_get_shapes", "qg_batch_tune",
     "qg_measure_wilson_all", "qg_measure_fmunu", "qg_measure_action_profile", "qg_measure_polyakov_profile",
     "qg_measure_enqueue", "qg_measure_fetch", "qg_measure_plaquette_all", "qg_measure_polyakov_all",
     "qg_net_set", "qg_net_get", "qg_mh_phase", "qg_mh_sweep", "qg_mh_stats", "qg_net_grad", "qg_net_train",
@@ -241,6 +243,9 @@ def load_library(path=LIB_PATH):
     lib.qg_batch_destroy.argtypes = [vp]
     lib.qg_batch_init.argtypes = [vp, ctypes.c_int]
     lib.qg_batch_set_shape.argtypes = [vp, ctypes.c_int]
+    lib.qg_batch_set_shapes.argtypes = [vp, ctypes.c_int, ctypes.c_int]
+    lib.qg_batch_get_shapes.argtypes = [vp, P(ctypes.c_int), P(ctypes.c_int)]
+    lib.qg_batch_tune.argtypes = [vp, ctypes.c_int, P(ctypes.c_float)]
     lib.qg_batch_run.argtypes = [vp, ctypes.c_int, ctypes.c_int]
     lib.qg_batch_sync.argtypes = [vp]
     lib.qg_batch_get_stream.argtypes = [vp, P(vp)]
@@ -718,6 +723,22 @@ class Batch:
 
     def set_shape(self, shape):
         self._ck(self.lib.qg_batch_set_shape(self.b, shape), "qg_batch_set_shape")
+
+    def set_shapes(self, heatbath, overrelax):
+        """Pin the batched phase-launch shapes (0 .. BATCH_SHAPES-1) per kind."""
+        self._ck(self.lib.qg_batch_set_shapes(self.b, heatbath, overrelax), "qg_batch_set_shapes")
+
+    def shapes(self):
+        h, o = ctypes.c_int(), ctypes.c_int()
+        self._ck(self.lib.qg_batch_get_shapes(self.b, ctypes.byref(h), ctypes.byref(o)), "qg_batch_get_shapes")
+        return h.value, o.value
+
+    def tune(self, reps=4):
+        """Pick the fastest batched launch shapes on the live fields (restored);
+        returns the measured ms per launch as [(heatbath, overrelaxation)] per shape."""
+        t = (ctypes.c_float * (2 * BATCH_SHAPES))()
+        self._ck(self.lib.qg_batch_tune(self.b, reps, t), "qg_batch_tune")
+        return [(t[2 * v], t[2 * v + 1]) for v in range(BATCH_SHAPES)]
 
     def run(self, nsweeps, measure_every=0):
         self._ck(self.lib.qg_batch_run(self.b, nsweeps, measure_every), "qg_batch_run")

@@ -4,12 +4,14 @@ the sweep and the measurement captured in one CUDA graph -- on one GPU or
 spread over the GPUs of a node.
 
   python -m qcdgpu_b200.betascan [--ensembles 64] [--sweeps 500] [--n-or 4]
-                                 [--measure-every 1] [--seed 54] [--shape 4]
+                                 [--measure-every 1] [--seed 54] [--shape -1]
   torchrun --nproc-per-node N -m qcdgpu_b200.betascan ...   (one rank per GPU)
 
 Workload: N_t drawn from {4, 6, 8} and N_s from {16, 20, 24, 32} with a
 fixed seed, beta = 5.5 + 0.7 i / (n - 1), cold start, FP32 links, FP64
 reunitarisation every 10 sweeps, Philox stream (RANDSERIES 1000 + i).
+The batched launch shapes are autotuned after the warm-up sweeps
+(qg_batch_tune, fields restored) unless --shape pins one.
 
 Several GPUs (the multi-GPU replica scheduler): the ensembles are
 independent, so they are dealt to the ranks by cost (sites x updates per
@@ -62,16 +64,21 @@ def run_share(ens, idx, a):
     import qcdgpu_b200 as Q
     if not idx:
         return {"idx": [], "plaquette": [], "polyakov_abs": [], "updates": 0.0, "ms": 0.0, "sites": 0,
-                "field_bytes": 0}
+                "field_bytes": 0, "shapes": None}
     sub = [ens[k] for k in idx]
     cfg = Q.default_config(group=3, precision=0, prng=Q.PRNG_PHILOX, n_or=a.n_or, reunit_every=10, reunit_fp64=1,
                            nhit=10, row_align=64)
     nmeas = (a.sweeps + a.warmup) // a.measure_every + 1
     B = Q.Batch(cfg, sub, max_measurements=nmeas)
-    B.set_shape(a.shape)
     B.init(Q.START_COLD)
     stream = torch.cuda.ExternalStream(B.stream())
-    B.run(a.warmup, a.measure_every)                  # graph capture and warm-up, untimed
+    B.run(a.warmup, a.measure_every)                  # warm-up, untimed
+    if a.shape < 0:
+        B.tune()                                      # fields restored: the chains are unchanged
+    else:
+        B.set_shape(a.shape)
+    shapes = list(B.shapes())
+    B.run(1, a.measure_every)                         # graph capture with the chosen shapes, untimed
     B.sync()
     if a.barrier is not None:
         a.barrier()
@@ -91,7 +98,7 @@ def run_share(ens, idx, a):
     B.close()
     return {"idx": list(idx), "plaquette": plaq.mean(axis=0).tolist(), "polyakov_abs": poly.mean(axis=0).tolist(),
             "updates": 4.0 * info["sites"] * (1 + a.n_or) * a.sweeps, "ms": ms, "sites": info["sites"],
-            "field_bytes": info["field_bytes"]}
+            "field_bytes": info["field_bytes"], "shapes": shapes}
 
 
 def merge(parts, n):
@@ -106,7 +113,7 @@ def merge(parts, n):
     return {"plaquette": plaq, "polyakov_abs": poly, "ms": ms, "updates": updates,
             "link_updates_per_s": updates / (ms * 1e-3) if ms > 0 else 0.0,
             "sites": sum(p["sites"] for p in parts), "field_bytes": sum(p["field_bytes"] for p in parts),
-            "ranks": [{"ensembles": len(p["idx"]), "ms": p["ms"]} for p in parts]}
+            "ranks": [{"ensembles": len(p["idx"]), "ms": p["ms"], "shapes": p.get("shapes")} for p in parts]}
 
 
 def schedule(ens, a, dist, rank, world, runner=run_share):
@@ -128,7 +135,7 @@ def main():
     ap.add_argument("--n-or", type=int, default=4)
     ap.add_argument("--measure-every", type=int, default=1)
     ap.add_argument("--seed", type=int, default=54)
-    ap.add_argument("--shape", type=int, default=4)
+    ap.add_argument("--shape", type=int, default=-1, help="batched launch shape; -1 = autotune (qg_batch_tune)")
     ap.add_argument("--warmup", type=int, default=3)
     a = ap.parse_args()
     import torch

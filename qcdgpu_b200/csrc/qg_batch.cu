@@ -156,7 +156,7 @@ struct qg_batch {
     uint64_t measurements = 0, sweeps_done = 0;
     cudaStream_t stream = nullptr;
     cudaGraphExec_t graph[4] = { nullptr, nullptr, nullptr, nullptr };   // [measure * 2 + reunit]
-    int shape = 4;
+    int shape_hb = 4, shape_or = 4;    // phase-kernel launch shapes (qg_batch_tune)
 };
 
 namespace {
@@ -184,18 +184,20 @@ cudaError_t launch_phase_batch(qg_batch *b, int parity, int mu, bool OR, uint32_
     const int g = b->cfg.group, nh = b->cfg.nhit, np = b->cfg.nhitpar;
     constexpr bool F32 = sizeof(Real) == 4;
     cudaStream_t s = b->stream;
-    // shape 4: staple staged through shared memory (SU(3) FP32 only)
-#define QB_L(NC, OR_, MU)                                                                                         \
-    do {                                                                                                          \
-        if constexpr (NC == 3 && F32) {                                                                           \
-            if (b->shape == 4) {                                                                                  \
-                k_phase_batch<NC, Real, OR_, MU, 5, true><<<nb, kPhaseBlock, 0, s>>>(b->d_ens, pre, b->n, parity, \
-                                                                                     b->d_phase, offset, nh, np); \
-                break;                                                                                            \
-            }                                                                                                     \
-        }                                                                                                         \
-        k_phase_batch<NC, Real, OR_, MU, 0, false><<<nb, kPhaseBlock, 0, s>>>(b->d_ens, pre, b->n, parity,        \
-                                                                              b->d_phase, offset, nh, np);        \
+    // the single-lattice launch shapes 0-4 (qg_tune): 0 registers, 1 / 2 the
+    // same held to 5 / 6 blocks per SM, 3 / 4 staple staged through shared
+    // memory (SU(3) FP32; elsewhere shapes 0 / 1)
+    const int shape = OR ? b->shape_or : b->shape_hb;
+#define QB_K(NC, OR_, MU, MB, ST) \
+    k_phase_batch<NC, Real, OR_, MU, MB, ST><<<nb, kPhaseBlock, 0, s>>>(b->d_ens, pre, b->n, parity, b->d_phase, offset, nh, np)
+#define QB_L(NC, OR_, MU)                                          \
+    do {                                                           \
+        constexpr bool kSt = NC == 3 && F32;                       \
+        if (shape == 1) QB_K(NC, OR_, MU, 5, false);               \
+        else if (shape == 2) QB_K(NC, OR_, MU, 6, false);          \
+        else if (shape == 3) QB_K(NC, OR_, MU, 0, kSt);            \
+        else if (shape == 4) QB_K(NC, OR_, MU, 5, kSt);            \
+        else QB_K(NC, OR_, MU, 0, false);                          \
     } while (0)
 #define QB_MU(NC, OR_)                               \
     do {                                             \
@@ -210,6 +212,7 @@ cudaError_t launch_phase_batch(qg_batch *b, int parity, int mu, bool OR, uint32_
     else { if (OR) QB_MU(2, true); else QB_MU(2, false); }
 #undef QB_MU
 #undef QB_L
+#undef QB_K
     return cudaGetLastError();
 }
 
@@ -417,11 +420,85 @@ extern "C" int qg_batch_init(qg_batch *b, int start)
     return QG_OK;
 }
 
-extern "C" int qg_batch_set_shape(qg_batch *b, int shape)
+extern "C" int qg_batch_set_shapes(qg_batch *b, int heatbath_shape, int overrelax_shape)
 {
     if (!b) return QG_ERR_ARG;
-    if (shape != 0 && shape != 4) return bfail("batched phase shapes: 0 (registers) or 4 (staged, SU(3) FP32)");
-    b->shape = shape;
+    if (heatbath_shape < 0 || heatbath_shape >= QG_BATCH_SHAPES || overrelax_shape < 0 ||
+        overrelax_shape >= QG_BATCH_SHAPES)
+        return bfail("batched launch shape out of range [0, QG_BATCH_SHAPES)");
+    b->shape_hb = heatbath_shape;
+    b->shape_or = overrelax_shape;
+    destroy_batch_graphs(b);
+    return QG_OK;
+}
+
+extern "C" int qg_batch_set_shape(qg_batch *b, int shape)
+{
+    return qg_batch_set_shapes(b, shape, shape);
+}
+
+extern "C" int qg_batch_get_shapes(qg_batch *b, int *heatbath_shape, int *overrelax_shape)
+{
+    if (!b || !heatbath_shape || !overrelax_shape) return QG_ERR_ARG;
+    *heatbath_shape = b->shape_hb;
+    *overrelax_shape = b->shape_or;
+    return QG_OK;
+}
+
+// times every launch shape of the batched heatbath and overrelaxation
+// phase launches on the live fields (restored afterwards; the Philox phase
+// counter is only read by the phase kernels) and keeps the fastest per kind
+extern "C" int qg_batch_tune(qg_batch *b, int reps, float *times_ms)
+{
+    if (!b) return QG_ERR_ARG;
+    if (reps < 1) reps = 4;
+    void *backup = nullptr;
+    QB_CK(cudaMallocAsync(&backup, b->field_bytes, b->stream), "tune backup");
+    {
+        cudaError_t eb = cudaMemcpyAsync(backup, b->links, b->field_bytes, cudaMemcpyDeviceToDevice, b->stream);
+        if (eb != cudaSuccess) {
+            cudaFreeAsync(backup, b->stream);
+            return bcuda(eb, "tune backup copy");
+        }
+    }
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    const int keep[2] = { b->shape_hb, b->shape_or };
+    float best[2] = { 1e30f, 1e30f };
+    int arg[2] = { keep[0], keep[1] };
+    cudaError_t e = cudaSuccess;
+    for (int v = 0; v < QG_BATCH_SHAPES && e == cudaSuccess; v++)
+        for (int kind = 0; kind < 2 && e == cudaSuccess; kind++) {
+            b->shape_hb = b->shape_or = v;
+            // one untimed launch, then reps timed ones over the 8 phase classes
+            for (int r = -1; r < reps && e == cudaSuccess; r++) {
+                if (r == 0) cudaEventRecord(e0, b->stream);
+                e = phase_batch(b, (r + 1) & 1, ((r + 1) >> 1) & 3, kind == 1, 0);
+            }
+            if (e != cudaSuccess) break;
+            cudaEventRecord(e1, b->stream);
+            cudaEventSynchronize(e1);
+            float ms = 0;
+            cudaEventElapsedTime(&ms, e0, e1);
+            ms /= reps;
+            if (times_ms) times_ms[2 * v + kind] = ms;
+            if (ms < best[kind]) { best[kind] = ms; arg[kind] = v; }
+        }
+    cudaError_t er = cudaMemcpyAsync(b->links, backup, b->field_bytes, cudaMemcpyDeviceToDevice, b->stream);
+    cudaFreeAsync(backup, b->stream);
+    cudaError_t es = cudaStreamSynchronize(b->stream);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (e != cudaSuccess) {
+        b->shape_hb = keep[0];
+        b->shape_or = keep[1];
+        return bcuda(e, "tune launch");
+    }
+    if (er != cudaSuccess) return bcuda(er, "tune restore");
+    if (es != cudaSuccess) return bcuda(es, "tune sync");
+    b->shape_hb = arg[0];
+    b->shape_or = arg[1];
     destroy_batch_graphs(b);
     return QG_OK;
 }

@@ -48,6 +48,41 @@ def test_batch_equals_single_contexts(group, precision, shape, start):
     B.close()
 
 
+def test_every_batch_shape_and_the_tuner_give_the_same_chain():
+    """the batched launch shapes 0-4 compute the same operation sequence,
+    and qg_batch_tune restores the fields it times on: all runs end with the
+    same links and series, bit for bit"""
+    def run(shapes=None, tune=False):
+        B = Q.Batch(common(3, 0), ENSEMBLES, max_measurements=4)
+        B.init(Q.START_HOT)
+        B.run(2, measure_every=1)
+        if tune:
+            t = B.tune(reps=2)
+            assert len(t) == Q.BATCH_SHAPES and all(a > 0 and b > 0 for a, b in t)
+            assert all(0 <= s < Q.BATCH_SHAPES for s in B.shapes())
+        else:
+            B.set_shapes(*shapes)
+            assert B.shapes() == shapes
+        B.run(2, measure_every=1)
+        out = (B.series(), [B.download(e) for e in range(len(ENSEMBLES))])
+        B.close()
+        return out
+    ref_ser, ref_links = run((0, 0))
+    for shapes in [(1, 2), (2, 1), (3, 4), (4, 3), (4, 4)]:
+        ser, links = run(shapes)
+        assert np.array_equal(ser, ref_ser), shapes
+        assert all(np.array_equal(a, b) for a, b in zip(links, ref_links)), shapes
+    ser, links = run(tune=True)
+    assert np.array_equal(ser, ref_ser)
+    assert all(np.array_equal(a, b) for a, b in zip(links, ref_links))
+    B = Q.Batch(common(3, 0), ENSEMBLES[:1])
+    with pytest.raises(Q.QGError):
+        B.set_shapes(Q.BATCH_SHAPES, 0)
+    with pytest.raises(Q.QGError):
+        B.set_shape(-1)
+    B.close()
+
+
 def test_batch_series_capacity_and_argument_checks():
     B = Q.Batch(common(3, 0), ENSEMBLES[:2], max_measurements=1)
     B.init(Q.START_COLD)
