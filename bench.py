@@ -127,9 +127,20 @@ def run_reference_phases(size, procs, warm, timed):
     return times
 
 
+def cpu_model():
+    try:
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("model name"):
+                return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
 def cpu_baseline_line(size, seconds_target=15.0):
     if not os.path.exists(ref_binary()):
         return None
+    one = run_reference_phases(size, 1, 0, 1)[0][0]   # one process alone: the per-core rate
     procs = cpu_workers(size)
     t = run_reference_phases(size, procs, 0, 1)
     per_phase = max(x[0] for x in t)
@@ -140,7 +151,11 @@ def cpu_baseline_line(size, seconds_target=15.0):
     return {"value": links / wall, "unit": UNIT, "cores": procs, "kind": "reference",
             "sample": "reference CPU path (SU(N)/suncpp heatbath, RANLUX3, NHIT=10; it has no overrelaxation) on "
                       "SU(3) %d^4 beta=%.1f cold start: %d concurrent processes x %d phases of %d link updates, "
-                      "%.1f s wall" % (size, BETA, procs, n, size ** 4 // 2, wall)}
+                      "%.1f s wall" % (size, BETA, procs, n, size ** 4 // 2, wall),
+            "single_process": {"value": (size ** 4 // 2) / one, "unit": UNIT, "cores": 1,
+                               "sample": "one process alone, one phase of %d link updates, %.2f s"
+                                         % (size ** 4 // 2, one)},
+            "cpu_model": cpu_model(), "host_cpus": os.cpu_count()}
 
 
 def run_reference_arm(args):
