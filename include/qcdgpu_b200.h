@@ -120,6 +120,14 @@ int qg_prng_seed(qg_ctx *ctx, uint32_t randseries);
 int qg_glibc_seeds(uint32_t randseries, int n, uint32_t *seeds);
 /* PRNG::produce (random.cpp:278-284): one reference-layout RANLUX batch.  */
 int qg_prng_produce(qg_ctx *ctx);
+/* RANLUX lookahead (new; on by default): qg_sweep generates the next
+ * sweep's 8 batches on a second stream while the current sweep's phases
+ * run (8 more batch buffers, allocated on the first RANLUX sweep when they
+ * leave 1 GiB free).  The batches, and which phase reads which, are
+ * unchanged; qg_prng_produce / qg_prns_upload / qg_prns_download /
+ * qg_prng_seed first return the generator to the last batch consumed, and
+ * qg_prns_download after sweeps returns that batch, as without it.       */
+int qg_set_prng_lookahead(qg_ctx *ctx, int on);
 int qg_prns_upload(qg_ctx *ctx, const float *host_quads, uint64_t nquads);
 int qg_prns_download(qg_ctx *ctx, float *host_quads, uint64_t nquads);
 

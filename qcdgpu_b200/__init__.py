@@ -31,6 +31,7 @@ NET_FEATURES, NET_HIDDEN, NET_PARAMS = 8, 32, 1377   # QG_NET_*
 EXPORTED_SYMBOLS = (
     "qg_default_config", "qg_create", "qg_destroy", "qg_last_error", "qg_get_info", "qg_sync",
     "qg_prng_seed", "qg_prng_produce", "qg_prns_upload", "qg_prns_download", "qg_init_links",
+    "qg_set_prng_lookahead",
     "qg_phase", "qg_sweep", "qg_reunitarize", "qg_measure", "qg_measure_wilson",
     "qg_links_upload", "qg_links_download", "qg_set_phase_counter", "qg_glibc_seeds", "qg_set_params", "qg_get_stream",
     "qg_default_run_options", "qg_parse_init_file", "qg_run", "qg_tune", "qg_plaquette_noalloc",
@@ -197,6 +198,7 @@ def load_library(path=LIB_PATH):
     lib.qg_sync.argtypes = [vp]
     lib.qg_prng_seed.argtypes = [vp, ctypes.c_uint32]
     lib.qg_prng_produce.argtypes = [vp]
+    lib.qg_set_prng_lookahead.argtypes = [vp, ctypes.c_int]
     lib.qg_prns_upload.argtypes = [vp, vp, ctypes.c_uint64]
     lib.qg_prns_download.argtypes = [vp, vp, ctypes.c_uint64]
     lib.qg_init_links.argtypes = [vp, ctypes.c_int]
@@ -472,6 +474,11 @@ class Lattice:
 
     def produce(self):
         self._ck(self.lib.qg_prng_produce(self.ctx), "qg_prng_produce")
+
+    def set_prng_lookahead(self, on):
+        """RANLUX mode: generate the next sweep's batches alongside the current
+        sweep (default on); the stream and its use are the same either way."""
+        self._ck(self.lib.qg_set_prng_lookahead(self.ctx, int(bool(on))), "qg_set_prng_lookahead")
 
     def init(self, start=None):
         self._ck(self.lib.qg_init_links(self.ctx, self.cfg.start if start is None else start), "qg_init_links")

@@ -45,7 +45,24 @@ struct qg_ctx {
     uint2 key = { 0, 0 };
     bool seeded = false;
     cudaStream_t stream = nullptr;
-    cudaGraphExec_t graph[2] = { nullptr, nullptr };  // sweep without / with reunitarisation
+    // sweep graphs: [0] / [1] without / with reunitarisation; with the
+    // RANLUX lookahead [2 + 2 v + reunit] for buffer variant v
+    cudaGraphExec_t graph[6] = {};
+    // RANLUX lookahead: while a sweep runs, a second stream generates the
+    // next sweep's 8 batches.  rl_buf[7] is the reference-layout PRN buffer;
+    // rl_buf[0..6], rl_buf[8] are allocated on the first RANLUX sweep (if
+    // memory allows).  Heatbath phase k of a sweep reads rl_buf[k] (k < 7)
+    // or rl_buf[7 + v]; the next sweep's batch k overwrites rl_buf[k] once
+    // phase k is done, its last batch goes to rl_buf[8 - v].  prns points at
+    // the buffer holding the last batch consumed.
+    float4 *rl_buf[9] = {};
+    float4 *rl_snap = nullptr;      // generator state as of the last batch consumed
+    bool rl_ahead = false;          // the generator has run 8 batches past the consumed ones
+    int rl_var = 0;                 // variant v of the next lookahead sweep
+    int rl_look = -1;               // lookahead: -1 not set up yet, 0 off / unavailable, 1 ready
+    bool rl_look_enabled = true;    // qg_set_prng_lookahead
+    cudaStream_t side = nullptr;
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr, ev_phase[8] = {};
     // learned-proposal Metropolis (qg_net_*, qg_mh_*)
     uint16_t *d_netw = nullptr;     // BF16 weights the kernels read
     float *d_master = nullptr, *d_adam_m = nullptr, *d_adam_v = nullptr;
@@ -132,16 +149,74 @@ static int validate(const qg_config *cfg, std::string &why)
 
 static void destroy_graphs(qg_ctx *c)
 {
-    for (int i = 0; i < 2; i++)
-        if (c->graph[i]) { cudaGraphExecDestroy(c->graph[i]); c->graph[i] = nullptr; }
+    for (auto &g : c->graph)
+        if (g) { cudaGraphExecDestroy(g); g = nullptr; }
 }
+
+static size_t rl_table_bytes(const qg_ctx *c) { return (size_t)7 * c->instances * sizeof(float4); }
+static size_t rl_batch_bytes(const qg_ctx *c) { return (size_t)c->instances * c->samples * sizeof(float4); }
+
+// the generator back at the last batch consumed (drops the lookahead
+// batches; they are generated again when needed)
+static cudaError_t rl_settle(qg_ctx *c)
+{
+    if (!c->rl_ahead) return cudaSuccess;
+    c->rl_ahead = false;
+    return cudaMemcpyAsync(c->rl_table, c->rl_snap, rl_table_bytes(c), cudaMemcpyDeviceToDevice, c->stream);
+}
+
+static void rl_free_lookahead(qg_ctx *c)
+{
+    for (int k = 0; k < 9; k++)
+        if (k != 7 && c->rl_buf[k]) { cudaFree(c->rl_buf[k]); c->rl_buf[k] = nullptr; }
+    if (c->rl_snap) { cudaFree(c->rl_snap); c->rl_snap = nullptr; }
+    for (cudaEvent_t &ev : c->ev_phase) if (ev) { cudaEventDestroy(ev); ev = nullptr; }
+    if (c->ev_fork) { cudaEventDestroy(c->ev_fork); c->ev_fork = nullptr; }
+    if (c->ev_join) { cudaEventDestroy(c->ev_join); c->ev_join = nullptr; }
+    if (c->side) { cudaStreamDestroy(c->side); c->side = nullptr; }
+}
+
+// buffers, stream and events of the lookahead, once; false (and the plain
+// sweep) when disabled or when they would not leave 1 GiB of device memory
+static bool rl_lookahead_ready(qg_ctx *c)
+{
+    if (!c->rl_look_enabled) return false;
+    if (c->rl_look >= 0) return c->rl_look == 1;
+    c->rl_look = 0;
+    size_t free_b = 0, total_b = 0;
+    if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) { cudaGetLastError(); return false; }
+    const size_t need = 8 * rl_batch_bytes(c) + rl_table_bytes(c);
+    if (free_b < need + ((size_t)1 << 30)) return false;
+    bool ok = cudaMalloc(&c->rl_snap, rl_table_bytes(c)) == cudaSuccess &&
+              cudaStreamCreateWithFlags(&c->side, cudaStreamNonBlocking) == cudaSuccess &&
+              cudaEventCreateWithFlags(&c->ev_fork, cudaEventDisableTiming) == cudaSuccess &&
+              cudaEventCreateWithFlags(&c->ev_join, cudaEventDisableTiming) == cudaSuccess;
+    for (int k = 0; k < 8 && ok; k++)
+        ok = cudaEventCreateWithFlags(&c->ev_phase[k], cudaEventDisableTiming) == cudaSuccess;
+    for (int k = 0; k < 9 && ok; k++)
+        if (k != 7) ok = cudaMalloc(&c->rl_buf[k], rl_batch_bytes(c)) == cudaSuccess;
+    if (!ok) {
+        cudaGetLastError();
+        rl_free_lookahead(c);
+        return false;
+    }
+    c->rl_look = 1;
+    return true;
+}
+
+// the buffer heatbath phase k of a lookahead sweep of variant v reads, and
+// the one the next sweep's batch k is written to
+static float4 *rl_in(qg_ctx *c, int v, int k) { return c->rl_buf[k < 7 ? k : 7 + v]; }
+static float4 *rl_out(qg_ctx *c, int v, int k) { return c->rl_buf[k < 7 ? k : 8 - v]; }
 
 extern "C" int qg_destroy(qg_ctx *c)
 {
     if (!c) return QG_OK;
     if (c->stream) cudaStreamSynchronize(c->stream);
     destroy_graphs(c);
-    cudaFree(c->links); cudaFree(c->prns); cudaFree(c->rl_table); cudaFree(c->d_seeds);
+    if (c->side) cudaStreamSynchronize(c->side);
+    rl_free_lookahead(c);
+    cudaFree(c->links); cudaFree(c->rl_buf[7]); cudaFree(c->rl_table); cudaFree(c->d_seeds);
     cudaFree(c->partials); cudaFree(c->d_results); cudaFree(c->d_phase); cudaFree(c->d_params);
     cudaFree(c->d_netw); cudaFree(c->d_master); cudaFree(c->d_adam_m); cudaFree(c->d_adam_v);
     cudaFree(c->d_grad); cudaFree(c->d_gpart); cudaFree(c->d_mh_acc); cudaFree(c->d_mh_jump);
@@ -192,7 +267,8 @@ extern "C" int qg_create(const qg_config *cfg, qg_ctx **out)
     if ((e = cudaMemsetAsync(c->links, 0, c->link_bytes, c->stream)) != cudaSuccess) return bad("cudaMemset(links)");
     if (cfg->prng == QG_PRNG_RANLUX) {
         size_t nq = (size_t)c->instances * c->samples;
-        if ((e = cudaMalloc(&c->prns, nq * sizeof(float4))) != cudaSuccess) return bad("cudaMalloc(prns)");
+        if ((e = cudaMalloc(&c->rl_buf[7], nq * sizeof(float4))) != cudaSuccess) return bad("cudaMalloc(prns)");
+        c->prns = c->rl_buf[7];
         if ((e = cudaMemsetAsync(c->prns, 0, nq * sizeof(float4), c->stream)) != cudaSuccess) return bad("cudaMemset(prns)");
         if ((e = cudaMalloc(&c->rl_table, (size_t)7 * c->instances * sizeof(float4))) != cudaSuccess) return bad("cudaMalloc(table)");
         if ((e = cudaMalloc(&c->d_seeds, (size_t)c->instances * sizeof(uint32_t))) != cudaSuccess) return bad("cudaMalloc(seeds)");
@@ -302,9 +378,19 @@ extern "C" int qg_prng_produce(qg_ctx *c)
     if (!c) return QG_ERR_ARG;
     if (c->cfg.prng != QG_PRNG_RANLUX) return fail(c, QG_ERR_STATE, "qg_prng_produce needs the RANLUX stream");
     if (!c->seeded) return fail(c, QG_ERR_STATE, "PRNG not seeded (qg_prng_seed)");
+    QG_CK(rl_settle(c), "ranlux settle");
     QG_CK(launch_ranlux_produce(c->rl_table, c->prns, c->instances, (int)c->samples, c->cfg.ranlux_nskip, c->stream),
           "ranlux");
     c->prng_counter++;
+    return QG_OK;
+}
+
+extern "C" int qg_set_prng_lookahead(qg_ctx *c, int on)
+{
+    if (!c) return QG_ERR_ARG;
+    QG_CK(rl_settle(c), "ranlux settle");
+    c->rl_look_enabled = on != 0;
+    destroy_graphs(c);
     return QG_OK;
 }
 
@@ -321,6 +407,7 @@ extern "C" int qg_prng_seed(qg_ctx *c, uint32_t series)
                               c->stream), "seed upload");
         QG_CK(launch_ranlux_init(c->d_seeds, c->rl_table, c->instances, c->stream), "ranlux_init");
         QG_CK(cudaStreamSynchronize(c->stream), "seed sync");
+        c->rl_ahead = false;
         c->seeded = true;
         c->prng_counter = 0;
         return qg_prng_produce(c);   // PRNG::initialize ends with one produce()
@@ -361,6 +448,7 @@ extern "C" int qg_prns_upload(qg_ctx *c, const float *h, uint64_t nq)
     if (!c || !h) return QG_ERR_ARG;
     if (!c->prns) return fail(c, QG_ERR_STATE, "no PRN buffer (Philox mode)");
     if (nq > (uint64_t)c->instances * c->samples) return fail(c, QG_ERR_ARG, "too many PRN quads");
+    QG_CK(rl_settle(c), "ranlux settle");
     QG_CK(cudaMemcpyAsync(c->prns, h, nq * sizeof(float4), cudaMemcpyHostToDevice, c->stream), "prns upload");
     QG_CK(cudaStreamSynchronize(c->stream), "prns upload sync");
     return QG_OK;
@@ -572,11 +660,55 @@ static cudaError_t enqueue_sweep(qg_ctx *c, bool reunit)
     return cudaSuccess;
 }
 
+// A RANLUX-mode sweep with the next sweep's batches generated alongside:
+// the heatbath phases read this sweep's batches (generated by the previous
+// sweep or the prologue in qg_sweep) from rl_in(v, k); the second stream
+// first saves the generator state (the state at this sweep's last batch,
+// for rl_settle), then produces the next 8 batches into rl_out(v, k), batch
+// k only after phase k has read its buffer.  The batches and the order in
+// which each is consumed are those of enqueue_sweep.
+static cudaError_t enqueue_sweep_lookahead(qg_ctx *c, bool reunit, int v)
+{
+    const qg_config &f = c->cfg;
+    cudaError_t e;
+    const int par_order[2] = { 1, 0 };
+    if ((e = cudaEventRecord(c->ev_fork, c->stream)) != cudaSuccess) return e;
+    if ((e = cudaStreamWaitEvent(c->side, c->ev_fork, 0)) != cudaSuccess) return e;
+    if ((e = cudaMemcpyAsync(c->rl_snap, c->rl_table, rl_table_bytes(c), cudaMemcpyDeviceToDevice, c->side)) !=
+        cudaSuccess)
+        return e;
+    int k = 0;
+    for (int pi = 0; pi < 2; pi++)
+        for (int mu = 0; mu < 4; mu++, k++) {
+            PhaseArgs a = phase_args(c, par_order[pi], mu, QG_UPDATE_HEATBATH, 0);
+            a.prns = rl_in(c, v, k);
+            if ((e = launch_phase(c, a)) != cudaSuccess) return e;
+            if ((e = cudaEventRecord(c->ev_phase[k], c->stream)) != cudaSuccess) return e;
+            if ((e = cudaStreamWaitEvent(c->side, c->ev_phase[k], 0)) != cudaSuccess) return e;
+            if ((e = launch_ranlux_produce(c->rl_table, rl_out(c, v, k), c->instances, (int)c->samples,
+                                           f.ranlux_nskip, c->side)) != cudaSuccess)
+                return e;
+        }
+    for (int n = 0; n < f.n_or; n++)
+        for (int pi = 0; pi < 2; pi++)
+            for (int mu = 0; mu < 4; mu++) {
+                PhaseArgs a = phase_args(c, par_order[pi], mu, QG_UPDATE_OVERRELAX, 0);
+                if ((e = launch_phase(c, a)) != cudaSuccess) return e;
+            }
+    if (reunit) {
+        if ((e = launch_gramschmidt(c->G, c->links, f.group, f.precision, f.reunit_fp64, c->stream)) != cudaSuccess)
+            return e;
+    }
+    if ((e = cudaEventRecord(c->ev_join, c->side)) != cudaSuccess) return e;
+    return cudaStreamWaitEvent(c->stream, c->ev_join, 0);
+}
+
 static int build_graph(qg_ctx *c, int which)
 {
     cudaGraph_t g = nullptr;
     QG_CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal), "begin capture");
-    cudaError_t e = enqueue_sweep(c, which == 1);
+    cudaError_t e = which >= 2 ? enqueue_sweep_lookahead(c, (which & 1) != 0, (which - 2) >> 1)
+                               : enqueue_sweep(c, which == 1);
     cudaError_t e2 = cudaStreamEndCapture(c->stream, &g);
     if (e != cudaSuccess) { if (g) cudaGraphDestroy(g); return cuda_fail(c, e, "sweep capture"); }
     if (e2 != cudaSuccess) return cuda_fail(c, e2, "end capture");
@@ -595,9 +727,21 @@ extern "C" int qg_sweep(qg_ctx *c, int nsweeps)
     const qg_config &f = c->cfg;
     const bool philox = (f.prng == QG_PRNG_PHILOX && f.start != QG_START_GID);
     const bool ranlux = (f.prng == QG_PRNG_RANLUX && f.start != QG_START_GID);
+    const bool look = ranlux && nsweeps > 0 && rl_lookahead_ready(c);
+    if (look && !c->rl_ahead) {
+        // prologue: this sweep's 8 batches, into the buffers of a variant
+        // that leaves the last batch consumed (prns) in place
+        c->rl_var = (c->prns == c->rl_buf[7]) ? 1 : 0;
+        QG_CK(cudaMemcpyAsync(c->rl_snap, c->rl_table, rl_table_bytes(c), cudaMemcpyDeviceToDevice, c->stream),
+              "ranlux snapshot");
+        for (int k = 0; k < 8; k++)
+            QG_CK(launch_ranlux_produce(c->rl_table, rl_in(c, c->rl_var, k), c->instances, (int)c->samples,
+                                        f.ranlux_nskip, c->stream), "ranlux");
+        c->rl_ahead = true;
+    }
     for (int n = 0; n < nsweeps; n++) {
         const bool reunit = f.reunit_every > 0 && ((c->sweeps_done + 1) % (uint64_t)f.reunit_every) == 0;
-        const int which = reunit ? 1 : 0;
+        const int which = look ? 2 + 2 * c->rl_var + (reunit ? 1 : 0) : (reunit ? 1 : 0);
         if (!c->graph[which]) {
             int r = build_graph(c, which);
             if (r) return r;
@@ -606,6 +750,10 @@ extern "C" int qg_sweep(qg_ctx *c, int nsweeps)
         c->sweeps_done++;
         if (philox) c->phase_counter += 8;
         if (ranlux) c->prng_counter += 8;
+        if (look) {
+            c->prns = c->rl_buf[7 + c->rl_var];   // this sweep's last batch
+            c->rl_var ^= 1;
+        }
     }
     return QG_OK;
 }

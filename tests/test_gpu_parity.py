@@ -153,6 +153,62 @@ def test_sweeps_ranlux_reference_cadence(group, precision):
     assert L.info().prng_counter == 1 + 16
 
 
+def _ranlux_lookahead_chain(look, precision):
+    """3 sweeps in one call, one single heatbath phase, 2 more sweeps, then
+    one produce: the PRN buffer after the sweeps, the links, the buffer after
+    the produce and the batch counter"""
+    L, c = make_pair(3, (4, 4, 4, 4), precision, n_or=1, reunit_every=2, reunit_fp64=1)
+    L.set_prng_lookahead(look)
+    L.seed(54)
+    L.init(Q.START_COLD)
+    L.sweep(3)
+    buf3 = L.prns_download()
+    L.phase(1, 2, Q.HEATBATH)                    # reads the last batch consumed, produces none
+    L.sweep(2)
+    links = L.download()
+    L.produce()
+    nxt = L.prns_download()
+    counter = L.info().prng_counter
+    samples = L.info().prng_samples
+    L.close()
+    return c, samples, buf3, links, nxt, counter
+
+
+@pytest.mark.parametrize("precision", [1, 0])
+def test_ranlux_lookahead_keeps_the_stream(precision):
+    """qg_sweep with the RANLUX lookahead (the next sweep's batches generated
+    on a second stream while the current sweep runs) consumes the same
+    batches in the same order as without it; after sweeps the PRN buffer
+    holds the last batch consumed, a single phase reads it, and produce
+    continues the stream from there -- against the oracle, and bit for bit
+    against the context without the lookahead."""
+    c, S, buf3, links, nxt, counter = _ranlux_lookahead_chain(1, precision)
+    _, _, buf3_0, links_0, nxt_0, counter_0 = _ranlux_lookahead_chain(0, precision)
+    assert np.array_equal(buf3.view(np.uint32), buf3_0.view(np.uint32))
+    assert np.array_equal(links, links_0)
+    assert np.array_equal(nxt.view(np.uint32), nxt_0.view(np.uint32))
+    assert counter == counter_0 == 1 + 5 * 8 + 1
+    R = O.Ranlux(54, INSTANCES)
+    R.batch(S)
+    t = cold_table(c)
+    last = None
+    for s in range(5):
+        for par in (1, 0):
+            for mu in range(4):
+                last = R.batch(S)
+                O.phase_hb(c, t, par, mu, prns=last)
+        for par in (1, 0):
+            for mu in range(4):
+                O.lib.ol_phase_or(ctypes.byref(c), O.vp(t), par, mu)
+        if s % 2 == 1:
+            O.lib.ol_gramschmidt_fp64(ctypes.byref(c), O.vp(t))
+        if s == 2:
+            assert np.array_equal(buf3.view(np.uint32), last.view(np.uint32))
+            O.phase_hb(c, t, 1, 2, prns=last)
+    assert maxdiff(links, t) <= TOL_U[precision] * 5
+    assert np.array_equal(nxt.view(np.uint32), R.batch(S).view(np.uint32))
+
+
 @pytest.mark.parametrize("group,precision", [(3, 1), (3, 0), (2, 1), (2, 0)])
 def test_sweeps_philox(group, precision):
     L, c = make_pair(group, (4, 4, 2, 6), precision, start=Q.START_COLD, prng=Q.PRNG_PHILOX,
