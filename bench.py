@@ -176,8 +176,12 @@ def run_reference_arm(args):
             "warmup": args.warmup, "ms_per_step": 1e3 * total / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (cold start)",
             "impl": "reference",
-            "config": {"workload": "SU(3) %d^4 beta=6.0 heatbath phase (V/2 link updates) per process per step"
-                                   % args.size, "processes": procs},
+            "config": {"workload": "SU(3) %d^4 beta=%.1f, FP32 12-real links, 1 HB + %d OR per sweep, FP64 reunit "
+                                   "every %d" % (args.size, BETA, N_OR, REUNIT_EVERY),
+                       "lattice": [args.size] * 4,
+                       "reference_work": "the reference CPU path has heatbath updates only (no overrelaxation, "
+                                         "FP64 links): per step one heatbath phase of V/2 link updates in each "
+                                         "process", "processes": procs},
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": procs, "kind": "reference",
                              "sample": "%d concurrent processes of the reference CPU path, one phase each per step"
                                        % procs},
