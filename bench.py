@@ -322,6 +322,9 @@ def run_ours(args):
                      "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
                      "algorithmic_bytes_per_launch": alg_bytes, "ms_per_launch": dom_ms,
                      "ms_per_launch_hb": ms_hb, "ms_per_launch_or": ms_or,
+                     "ms_per_launch_how": "CUDA events on the library stream around each of 16 single phase "
+                                          "launches per kind, right after the timed region, same lattice and "
+                                          "shapes",
                      # the literature's per-update count with no reuse between sites (19 link reads + 1
                      # write); above the HBM peak because neighbouring sites share their links in L2
                      "naive_bytes_per_update": 20 * LINK_BYTES,
