@@ -11,7 +11,7 @@ with tau_int from the Madras-Sokal automatic window (c = 6); the case's
 mean is the average over chains and its error the combined chain errors.
 
 Usage: python tests/golden/make_stat_golden.py   (needs oracle/_ref built;
-about a minute on 8 cores)
+about five minutes on 8 cores)
 """
 import json
 import os
@@ -29,6 +29,11 @@ CASES = [
      "sweeps": 6000},
     {"name": "su2_4x4_b2.3", "group": 2, "dims": [4, 4, 4, 4], "beta": 2.3, "chains": 8, "therm": 500,
      "sweeps": 12000},
+    # the lattice and coupling of the SU(2) run configuration (8^4, beta = 2.3), cold start
+    {"name": "su2_8x4_b2.3", "group": 2, "dims": [8, 8, 8, 8], "beta": 2.3, "chains": 8, "therm": 500,
+     "sweeps": 5000},
+    {"name": "su3_8x4_b5.7", "group": 3, "dims": [8, 8, 8, 8], "beta": 5.7, "chains": 8, "therm": 300,
+     "sweeps": 3000},
 ]
 
 

@@ -21,12 +21,16 @@ CASES = {c["name"]: c for c in GOLD["cases"]}
 
 @pytest.mark.parametrize("name,precision,n_or,series", [
     ("su3_4x4_b5.7", 0, 0, 11), ("su3_4x4_b5.7", 0, 4, 12), ("su3_4x4_b5.7", 1, 0, 13),
-    ("su2_4x4_b2.3", 1, 2, 14), ("su2_4x4_b2.3", 0, 0, 15)])
+    ("su2_4x4_b2.3", 1, 2, 14), ("su2_4x4_b2.3", 0, 0, 15),
+    # SU(2) 8^4 beta=2.3 FP64, 1 HB + 2 OR: the SU(2) run configuration (cold start)
+    ("su2_8x4_b2.3", 1, 2, 16), ("su2_8x4_b2.3", 0, 0, 17),
+    ("su3_8x4_b5.7", 0, 4, 18), ("su3_8x4_b5.7", 1, 0, 19)])
 def test_plaquette_average_agrees_with_reference_heatbath(name, precision, n_or, series):
     case = CASES[name]
     cfg = Q.default_config(group=case["group"], size=tuple(case["dims"]), precision=precision, start=Q.START_COLD,
                            prng=Q.PRNG_PHILOX, beta=case["beta"], randseries=series, n_or=n_or, reunit_every=1)
-    opts = Q.default_run_options(iter=30001, niter=1, nav=500, pl_level=0, get_actions=0, get_plaquettes=1,
+    sweeps = 30000 if case["dims"][0] == 4 else 15000
+    opts = Q.default_run_options(iter=sweeps + 1, niter=1, nav=500, pl_level=0, get_actions=0, get_plaquettes=1,
                                  quiet=1, write_results=0, verify=0)
     res = Q.run(cfg, opts)
     k = Q.OBS_NAMES.index("Plq_total")
