@@ -164,6 +164,23 @@ int qg_set_shapes(qg_ctx *ctx, int heatbath_shape, int overrelax_shape);
 int qg_get_shapes(qg_ctx *ctx, int *heatbath_shape, int *overrelax_shape);
 /* lattice_GramSchmidt kernel (suncl.cl:350-396); fp64 != 0 computes in FP64 */
 int qg_reunitarize(qg_ctx *ctx, int fp64);
+/* x-slabs (the BIGLAT decomposition, suncl.cpp:4004-4062, as x-slices of
+ * one lattice): a context created with size[0] = w + 2 becomes slab
+ * [x0, x0 + w) of a lattice with n1_global x-slices; its slices 0 and w+1
+ * are halos (global x0 - 1 and x0 + w).  qg_phase then updates the w
+ * interior slices only, with the whole lattice's parity and Philox thread
+ * indices, so every slab draws the numbers the undecomposed lattice draws.
+ * Philox stream, periodic boundaries, even global N1; starts cold or from
+ * qg_links_upload; qg_sweep is refused (phases need halo exchanges).      */
+int qg_set_slab(qg_ctx *ctx, int x0, int n1_global);
+/* halo exchange of the links of direction dir and global parity p: to_buf
+ * = 1 packs boundary slice x = 1 (side 0) or x = w (side 1) into buf
+ * (device or pinned host memory, qg_slab_halo_bytes bytes: the planes one
+ * after another), to_buf = 0 unpacks buf into halo slice x = 0 (side 0) or
+ * x = w + 1 (side 1).  Side 1 of a slab feeds side 0 of its right
+ * neighbour and vice versa.  Asynchronous on the context's stream.       */
+int qg_slab_halo(qg_ctx *ctx, int dir, int parity, int side, void *buf, int to_buf);
+int qg_slab_halo_bytes(qg_ctx *ctx, uint64_t *bytes);
 
 /* lattice_measurement_plq / lattice_measurement / lattice_polyakov /
  * lattice_measurement_wilson + their reductions (sun_measurements_cl.cl:

@@ -31,7 +31,7 @@ NET_FEATURES, NET_HIDDEN, NET_PARAMS = 8, 32, 1377   # QG_NET_*
 EXPORTED_SYMBOLS = (
     "qg_default_config", "qg_create", "qg_destroy", "qg_last_error", "qg_get_info", "qg_sync",
     "qg_prng_seed", "qg_prng_produce", "qg_prns_upload", "qg_prns_download", "qg_init_links",
-    "qg_set_prng_lookahead",
+    "qg_set_prng_lookahead", "qg_set_slab", "qg_slab_halo", "qg_slab_halo_bytes",
     "qg_phase", "qg_sweep", "qg_reunitarize", "qg_measure", "qg_measure_wilson",
     "qg_links_upload", "qg_links_download", "qg_set_phase_counter", "qg_glibc_seeds", "qg_set_params", "qg_get_stream",
     "qg_default_run_options", "qg_parse_init_file", "qg_run", "qg_tune", "qg_plaquette_noalloc",
@@ -199,6 +199,9 @@ def load_library(path=LIB_PATH):
     lib.qg_prng_seed.argtypes = [vp, ctypes.c_uint32]
     lib.qg_prng_produce.argtypes = [vp]
     lib.qg_set_prng_lookahead.argtypes = [vp, ctypes.c_int]
+    lib.qg_set_slab.argtypes = [vp, ctypes.c_int, ctypes.c_int]
+    lib.qg_slab_halo.argtypes = [vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, vp, ctypes.c_int]
+    lib.qg_slab_halo_bytes.argtypes = [vp, P(ctypes.c_uint64)]
     lib.qg_prns_upload.argtypes = [vp, vp, ctypes.c_uint64]
     lib.qg_prns_download.argtypes = [vp, vp, ctypes.c_uint64]
     lib.qg_init_links.argtypes = [vp, ctypes.c_int]
@@ -474,6 +477,22 @@ class Lattice:
 
     def produce(self):
         self._ck(self.lib.qg_prng_produce(self.ctx), "qg_prng_produce")
+
+    def set_slab(self, x0, n1_global):
+        """Make this lattice (size[0] = w + 2) the x-slab [x0, x0 + w) of a
+        lattice of n1_global x-slices, with halo slices 0 and w + 1."""
+        self._ck(self.lib.qg_set_slab(self.ctx, int(x0), int(n1_global)), "qg_set_slab")
+
+    def slab_halo_bytes(self):
+        n = ctypes.c_uint64()
+        self._ck(self.lib.qg_slab_halo_bytes(self.ctx, ctypes.byref(n)), "qg_slab_halo_bytes")
+        return n.value
+
+    def slab_halo(self, direction, parity, side, ptr, to_buf):
+        """Pack the boundary slice (to_buf) or unpack into the halo slice;
+        ptr is a device (or pinned host) address of slab_halo_bytes() bytes."""
+        self._ck(self.lib.qg_slab_halo(self.ctx, int(direction), int(parity), int(side), ctypes.c_void_p(ptr),
+                                       int(bool(to_buf))), "qg_slab_halo")
 
     def set_prng_lookahead(self, on):
         """RANLUX mode: generate the next sweep's batches alongside the current

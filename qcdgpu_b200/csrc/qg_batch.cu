@@ -64,6 +64,9 @@ k_phase_batch(const EnsDesc *ens, const uint32_t *pre, int n, int parity, const 
     A.phase_base = phase_base;
     A.phase_offset = phase_offset;
     A.variant = 0;
+    A.t_begin = 0;
+    A.t_end = G.half;
+    A.t_prn = 0;
     Field<Real> U;
     U.p = reinterpret_cast<typename V4<Real>::T *>(d.links);
     U.pstride = G.pstride;

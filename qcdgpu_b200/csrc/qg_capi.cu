@@ -61,6 +61,10 @@ struct qg_ctx {
     int rl_var = 0;                 // variant v of the next lookahead sweep
     int rl_look = -1;               // lookahead: -1 not set up yet, 0 off / unavailable, 1 ready
     bool rl_look_enabled = true;    // qg_set_prng_lookahead
+    // x-slab of a larger lattice (qg_set_slab): this context's x-slices 1..w
+    // are the global slices x0 .. x0+w-1, slices 0 and w+1 are halos
+    bool slab = false;
+    int slab_x0 = 0, slab_n1 = 0;
     cudaStream_t side = nullptr;
     cudaEvent_t ev_fork = nullptr, ev_join = nullptr, ev_phase[8] = {};
     // learned-proposal Metropolis (qg_net_*, qg_mh_*)
@@ -468,6 +472,8 @@ extern "C" int qg_init_links(qg_ctx *c, int start)
 {
     if (!c) return QG_ERR_ARG;
     const qg_config &f = c->cfg;
+    if (c->slab && start != QG_START_COLD)
+        return fail(c, QG_ERR_UNSUPPORTED, "a slab starts cold or from qg_links_upload of its part of a lattice");
     cudaError_t e;
     switch (start) {
     case QG_START_COLD:
@@ -521,6 +527,18 @@ static PhaseArgs phase_args(qg_ctx *c, int parity, int dir, int kind, uint32_t o
     a.phase_base = c->d_phase;
     a.phase_offset = offset;
     a.variant = (kind == QG_UPDATE_OVERRELAX) ? c->variant_or : c->variant_hb;
+    a.t_begin = 0;
+    a.t_end = c->G.half;
+    a.t_prn = 0;
+    if (c->slab) {
+        // interior slices 1..w only; the global lattice's thread indices
+        // and parity (global x = local x + x0 - 1)
+        const uint32_t h = c->G.n2n3n4 / 2;
+        a.t_begin = h;
+        a.t_end = (uint32_t)(c->G.n[0] - 1) * h;
+        a.t_prn = (int32_t)(c->slab_x0 - 1) * (int32_t)h;
+        a.parity = parity ^ ((c->slab_x0 - 1) & 1);
+    }
     return a;
 }
 
@@ -719,9 +737,68 @@ static int build_graph(qg_ctx *c, int which)
     return QG_OK;
 }
 
+// ------------------------------------------------------------ x-slabs
+extern "C" int qg_set_slab(qg_ctx *c, int x0, int n1_global)
+{
+    if (!c) return QG_ERR_ARG;
+    const qg_config &f = c->cfg;
+    const int w = f.size[0] - 2;
+    if (w < 1 || n1_global < 2 || x0 < 0 || x0 >= n1_global || w > n1_global)
+        return fail(c, QG_ERR_ARG, "slab: size[0] - 2 interior slices starting at global x0 of n1_global");
+    if (n1_global % 2 || c->G.n2n3n4 % 2)
+        return fail(c, QG_ERR_ARG, "slab: the global N1 and N2*N3*N4 must be even (checkerboard across slabs)");
+    if (f.prng != QG_PRNG_PHILOX || f.start == QG_START_GID)
+        return fail(c, QG_ERR_UNSUPPORTED, "slabs run the Philox stream (its numbers depend on the site only)");
+    if (twist_of(f)) return fail(c, QG_ERR_UNSUPPORTED, "slabs need periodic boundaries (PHI = OMEGA = 0)");
+    c->slab = true;
+    c->slab_x0 = x0;
+    c->slab_n1 = n1_global;
+    destroy_graphs(c);
+    return QG_OK;
+}
+
+static uint32_t slab_planes(const qg_ctx *c) { return c->cfg.group == 3 ? 3u : 1u; }
+static size_t slab_elem(const qg_ctx *c) { return c->cfg.precision ? 32 : 16; }
+
+extern "C" int qg_slab_halo_bytes(qg_ctx *c, uint64_t *bytes)
+{
+    if (!c || !bytes) return QG_ERR_ARG;
+    *bytes = (uint64_t)slab_planes(c) * (c->G.n2n3n4 / 2) * slab_elem(c);
+    return QG_OK;
+}
+
+// the links of direction dir and global parity p of one x-slice, plane by
+// plane: to_buf = 1 copies the boundary slice (x = 1 for side 0, x = w for
+// side 1) into buf, to_buf = 0 copies buf into the halo (x = 0 / x = w+1).
+// In a slice of parity q they are the elements q cb + x h .. + h of each
+// plane, ordered by the site index within the slice -- the same order in
+// every slab, so a boundary packed by one slab unpacks into the halo of its
+// neighbour.
+extern "C" int qg_slab_halo(qg_ctx *c, int dir, int parity, int side, void *buf, int to_buf)
+{
+    if (!c || !buf) return QG_ERR_ARG;
+    if (!c->slab) return fail(c, QG_ERR_STATE, "not a slab (qg_set_slab)");
+    if (dir < 0 || dir > 3 || (parity != 0 && parity != 1) || (side != 0 && side != 1))
+        return fail(c, QG_ERR_ARG, "bad direction / parity / side");
+    const uint32_t h = c->G.n2n3n4 / 2, w = (uint32_t)c->G.n[0] - 2;
+    const uint32_t x = to_buf ? (side ? w : 1) : (side ? w + 1 : 0);
+    const uint32_t q = (uint32_t)(parity ^ ((c->slab_x0 - 1) & 1));
+    const size_t es = slab_elem(c), n = (size_t)h * es;
+    char *base = static_cast<char *>(c->links);
+    char *b = static_cast<char *>(buf);
+    for (uint32_t k = 0; k < slab_planes(c); k++) {
+        const size_t plane = (size_t)dir + 4 * k;
+        char *lk = base + (plane * c->G.pstride + (size_t)q * c->G.cb + (size_t)x * h) * es;
+        char *bk = b + k * n;
+        QG_CK(cudaMemcpyAsync(to_buf ? bk : lk, to_buf ? lk : bk, n, cudaMemcpyDefault, c->stream), "slab halo copy");
+    }
+    return QG_OK;
+}
+
 extern "C" int qg_sweep(qg_ctx *c, int nsweeps)
 {
     if (!c) return QG_ERR_ARG;
+    if (c->slab) return fail(c, QG_ERR_STATE, "a slab sweeps phase by phase with halo exchanges (qcdgpu_b200.slabs)");
     if (nsweeps < 0) return fail(c, QG_ERR_ARG, "negative sweep count");
     if (needs_seed(c, QG_UPDATE_HEATBATH)) return fail(c, QG_ERR_STATE, "heatbath needs a seeded PRNG (qg_prng_seed)");
     const qg_config &f = c->cfg;
@@ -761,6 +838,7 @@ extern "C" int qg_sweep(qg_ctx *c, int nsweeps)
 // ------------------------------------------------- learned-proposal Metropolis
 static int net_check(qg_ctx *c)
 {
+    if (c->slab) return fail(c, QG_ERR_UNSUPPORTED, "the learned proposal runs on whole lattices");
     if (c->cfg.group != 3 || c->cfg.precision != 0 || c->cfg.prng != QG_PRNG_PHILOX)
         return fail(c, QG_ERR_UNSUPPORTED, "the learned proposal runs on SU(3) FP32 links with the Philox stream");
     if (c->cfg.phi != 0.0 || c->cfg.omega != 0.0)

@@ -23,6 +23,9 @@ struct PhaseArgs {
     const uint64_t *phase_base;  // device counter (graph-replayable)
     uint32_t phase_offset;       // added to *phase_base
     int variant;                 // launch shape, 0 .. kPhaseVariants-1 (launch_phase_T)
+    uint32_t t_begin, t_end;     // threads updated: [t_begin, t_end) (a slab: its interior x-slices)
+    int32_t t_prn;               // added to the thread index for the Philox stream (a slab: its
+                                 // threads' indices in the whole lattice)
 };
 constexpr int kPhaseVariants = QG_TUNE_SHAPES;
 

@@ -246,7 +246,8 @@ template <typename Real> struct PrnOf<Real, 1> {
     using T = PrnPhilox<Real>;
     __device__ static T make(const PhaseArgs &A, uint32_t t, uint32_t, uint64_t phase, const Geom &)
     {
-        T p; p.key = A.key; p.t = t; p.k = 0; p.plo = (uint32_t)phase; p.phi = (uint32_t)(phase >> 32); return p;
+        T p; p.key = A.key; p.t = (uint32_t)((int32_t)t + A.t_prn); p.k = 0; p.plo = (uint32_t)phase;
+        p.phi = (uint32_t)(phase >> 32); return p;
     }
 };
 template <typename Real> struct PrnOf<Real, 2> {
@@ -323,8 +324,8 @@ __device__ __forceinline__ void phase_site(const Field<Real> &U, const Geom &G, 
 template <int NC, typename Real, int PMODE, bool OR, int mu, int MINB, bool STAGED>
 __global__ void __launch_bounds__(kPhaseBlock, MINB) k_phase(Field<Real> U, Geom G, PhaseArgs A)
 {
-    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= G.half) return;
+    const uint32_t t = A.t_begin + blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= A.t_end) return;
     phase_site<NC, Real, PMODE, OR, mu, STAGED>(U, G, A, t);
 }
 
@@ -384,15 +385,15 @@ cudaError_t launch_phase_T(const Geom &G, void *links, int group, const PhaseArg
     U.p = reinterpret_cast<typename V4<Real>::T *>(links);
     U.pstride = G.pstride;
     const int bs = kPhaseBlock;
-    const unsigned nb = (G.half + bs - 1) / bs;
+    const unsigned nb = (a.t_end - a.t_begin + bs - 1) / bs;
     const int pm = a.prn_mode;   // -1 selects overrelaxation (no PRNs)
     // shapes 3, 4 stage the staple through shared memory where that form
     // exists (SU(3), FP32 links); elsewhere they run shapes 0, 1
     constexpr bool kStage = sizeof(Real) == 4;
-    // shape 5: overrelaxation two links per thread (SU(3), FP32, periodic);
-    // otherwise it runs shape 4
+    // shape 5: overrelaxation two links per thread (SU(3), FP32, periodic,
+    // the whole lattice); otherwise it runs shape 4
     if constexpr (sizeof(Real) == 4) {
-        if (a.variant == 5 && group == 3 && pm == -1 && !a.twist) {
+        if (a.variant == 5 && group == 3 && pm == -1 && !a.twist && a.t_begin == 0 && a.t_end == G.half) {
             const unsigned nbp = ((G.half + 1) / 2 + bs - 1) / bs;
             switch (a.dir) {
             case 0: k_phase_or_pair<0><<<nbp, bs, 0, s>>>(U, G, a); break;

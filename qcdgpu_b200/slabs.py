@@ -1,0 +1,244 @@
+"""x-slab decomposition of one lattice: the reference's BIGLAT scheme
+(SU(N)/suncl/suncl.cpp:4004-4062, 4804-5210), which cuts the lattice into
+sub-lattices along x and exchanges their boundary links after every update
+kernel, here as x-slabs of the C-ABI's slab contexts (qg_set_slab).
+
+A slab of w x-slices is a context of size (w + 2, N2, N3, N4): slices 1..w
+are its part of the lattice, slices 0 and w + 1 hold copies of the
+neighbours' boundary slices (halos).  qg_phase updates the interior only,
+with the whole lattice's parity and Philox thread indices, so the slabs
+together draw exactly the numbers the undecomposed lattice draws and, with
+the halos refreshed after every phase, follow its chain bit for bit.  After
+phase (mu, p) only the links of direction mu and parity p have changed, so
+the exchange moves one boundary slice of those links to each side:
+3 planes x N2 N3 N4 / 2 links (SU(3)).
+
+  SlabSet   -- several slabs on one GPU (the reference runs BIGLAT's
+               sub-lattices on one device the same way to test it,
+               QCDGPU.cpp:129-134); halos copied through a device buffer.
+  DistSlab  -- one slab per rank (torch.distributed: NCCL between GPUs,
+               gloo for the host-side test of the exchange); halos sent with
+               batched point-to-point operations.
+
+Both run the sweep of qg_sweep: heatbath phases odd X..T, even X..T, n_or
+overrelaxation sweeps in the same order, Gram-Schmidt when due (on every
+slab; a halo link is reunitarised to the same bits as its original, so no
+exchange follows it).
+"""
+import numpy as np
+
+import qcdgpu_b200 as Q
+
+PARITY_ORDER = (1, 0)          # odd first, as lattice_simulate
+
+
+def split(n1, parts):
+    """x-slice widths of `parts` slabs of a lattice of n1 slices, as even as
+    possible, and their first global slices"""
+    if parts < 1 or parts > n1:
+        raise ValueError("between 1 and N1 slabs")
+    w = [n1 // parts + (1 if k < n1 % parts else 0) for k in range(parts)]
+    x0 = [sum(w[:k]) for k in range(parts)]
+    return w, x0
+
+
+def slab_config(cfg, w):
+    """the context config of a slab of w slices of the lattice cfg"""
+    c = Q.default_config()
+    for name, _ in Q.Config._fields_:
+        setattr(c, name, getattr(cfg, name))
+    c.size[0] = w + 2
+    return c
+
+
+def phase_sequence(n_or):
+    """(parity, direction, kind) of one sweep, in qg_sweep's order"""
+    seq = [(p, mu, Q.HEATBATH) for p in PARITY_ORDER for mu in range(4)]
+    for _ in range(n_or):
+        seq += [(p, mu, Q.OVERRELAX) for p in PARITY_ORDER for mu in range(4)]
+    return seq
+
+
+def _rows(cfg):
+    """reference-layout planes, row size and x-slice length of cfg's lattice"""
+    n = list(cfg.size)
+    V = int(np.prod(n))
+    a = cfg.row_align if cfg.row_align > 0 else 64
+    planes = 12 if cfg.group == 3 else 4
+    return planes, (V + a - 1) // a * a, V // n[0]
+
+
+class _Slab:
+    """one slab context and its place in the lattice"""
+
+    def __init__(self, cfg, w, x0):
+        self.w, self.x0 = w, x0
+        self.cfg = slab_config(cfg, w)
+        self.L = Q.Lattice(self.cfg)
+        self.L.set_slab(x0, cfg.size[0])
+        self.nbytes = self.L.slab_halo_bytes()
+
+    def close(self):
+        self.L.close()
+
+
+def _to_slab(table, gcfg, w, x0, scfg):
+    """the slab's reference-layout table (halos included) cut from the
+    lattice's (global slices x0-1 .. x0+w, periodic)"""
+    planes, rows, ns = _rows(gcfg)
+    _, srows, _ = _rows(scfg)
+    g = table.reshape(planes, rows, 4)
+    n1 = gcfg.size[0]
+    s = np.zeros((planes, srows, 4), dtype=table.dtype)
+    for k in range(w + 2):
+        x = (x0 - 1 + k) % n1
+        s[:, k * ns:(k + 1) * ns, :] = g[:, x * ns:(x + 1) * ns, :]
+    return s.reshape(-1)
+
+
+class SlabSet:
+    """Several x-slabs of one lattice on the current GPU."""
+
+    def __init__(self, cfg, parts):
+        import torch
+        self.cfg = cfg
+        self.widths, self.x0s = split(cfg.size[0], parts)
+        self.slabs = [_Slab(cfg, w, x0) for w, x0 in zip(self.widths, self.x0s)]
+        nb = max(s.nbytes for s in self.slabs)
+        self.buf_hi = [torch.empty(nb, dtype=torch.uint8, device="cuda") for _ in self.slabs]
+        self.buf_lo = [torch.empty(nb, dtype=torch.uint8, device="cuda") for _ in self.slabs]
+        self.sweeps_done = 0
+
+    def close(self):
+        for s in self.slabs:
+            s.close()
+        self.slabs = []
+
+    def seed(self, randseries=None):
+        for s in self.slabs:
+            s.L.seed(randseries)
+
+    def upload(self, table):
+        """the lattice's links (reference layout, as Lattice.download gives
+        them) into the slabs, halos included"""
+        for s in self.slabs:
+            s.L.upload(_to_slab(table, self.cfg, s.w, s.x0, s.cfg))
+        self._sync()
+
+    def download(self):
+        """the lattice's links (reference layout) from the slabs' interiors"""
+        planes, rows, ns = _rows(self.cfg)
+        out = None
+        for s in self.slabs:
+            t = s.L.download()
+            _, srows, _ = _rows(s.cfg)
+            if out is None:
+                out = np.zeros((planes, rows, 4), dtype=t.dtype)
+            t = t.reshape(planes, srows, 4)
+            out[:, s.x0 * ns:(s.x0 + s.w) * ns, :] = t[:, ns:(s.w + 1) * ns, :]
+        return out.reshape(-1)
+
+    def _sync(self):
+        for s in self.slabs:
+            s.L.sync()
+
+    def exchange(self, direction, parity):
+        """refresh every halo of the links of (direction, parity)"""
+        K = len(self.slabs)
+        self._sync()                         # the staging buffers are free again
+        for k, s in enumerate(self.slabs):
+            s.L.slab_halo(direction, parity, 1, self.buf_hi[k].data_ptr(), True)
+            s.L.slab_halo(direction, parity, 0, self.buf_lo[k].data_ptr(), True)
+        self._sync()
+        for k in range(K):
+            self.slabs[(k + 1) % K].L.slab_halo(direction, parity, 0, self.buf_hi[k].data_ptr(), False)
+            self.slabs[(k - 1) % K].L.slab_halo(direction, parity, 1, self.buf_lo[k].data_ptr(), False)
+
+    def fill_halos(self):
+        for mu in range(4):
+            for p in (0, 1):
+                self.exchange(mu, p)
+
+    def phase(self, parity, direction, kind=Q.HEATBATH):
+        for s in self.slabs:
+            s.L.phase(parity, direction, kind)
+        self.exchange(direction, parity)
+
+    def sweep(self, n=1):
+        for _ in range(n):
+            for p, mu, kind in phase_sequence(self.cfg.n_or):
+                self.phase(p, mu, kind)
+            self.sweeps_done += 1
+            if self.cfg.reunit_every > 0 and self.sweeps_done % self.cfg.reunit_every == 0:
+                for s in self.slabs:
+                    s.L.reunitarize(self.cfg.reunit_fp64)
+        self._sync()
+
+    def action_sums(self):
+        """(spatial, temporal) sums of (beta/N)(3N - Re Tr U_p) over the
+        lattice: the slabs' x-profiles over their interior slices"""
+        tot = np.zeros(2)
+        for s in self.slabs:
+            tot += s.L.action_profile(0)[1:s.w + 1].sum(axis=0)
+        return tot
+
+    def polyakov_sums(self):
+        """(Re, Im) sums of the Polyakov loop over the spatial sites"""
+        tot = np.zeros(2)
+        for s in self.slabs:
+            tot += s.L.polyakov_profile(0)[1:s.w + 1].sum(axis=0)
+        return tot
+
+
+class DistSlab:
+    """One x-slab per rank of a torch.distributed group (rank k holds slab
+    k of split(N1, world)).  `slab` is a _Slab, or any object with the same
+    w / nbytes / L.slab_halo / L.phase / L.reunitarize / L.sync members (the
+    host-side test passes a stand-in)."""
+
+    def __init__(self, cfg, dist, device, slab=None):
+        import torch
+        self.cfg, self.dist = cfg, dist
+        self.rank, self.world = dist.get_rank(), dist.get_world_size()
+        w, x0 = split(cfg.size[0], self.world)
+        self.slab = slab if slab is not None else _Slab(cfg, w[self.rank], x0[self.rank])
+        nb = self.slab.nbytes
+        self.send_hi, self.send_lo, self.recv_hi, self.recv_lo = (
+            torch.empty(nb, dtype=torch.uint8, device=device) for _ in range(4))
+        self.sweeps_done = 0
+
+    def exchange(self, direction, parity):
+        L = self.slab.L
+        L.slab_halo(direction, parity, 1, self.send_hi.data_ptr(), True)
+        L.slab_halo(direction, parity, 0, self.send_lo.data_ptr(), True)
+        L.sync()
+        if self.world == 1:
+            self.recv_lo.copy_(self.send_hi)
+            self.recv_hi.copy_(self.send_lo)
+        else:
+            right, left = (self.rank + 1) % self.world, (self.rank - 1) % self.world
+            P2P = self.dist.P2POp
+            ops = [P2P(self.dist.isend, self.send_hi, right), P2P(self.dist.irecv, self.recv_lo, left),
+                   P2P(self.dist.isend, self.send_lo, left), P2P(self.dist.irecv, self.recv_hi, right)]
+            for r in self.dist.batch_isend_irecv(ops):
+                r.wait()
+            if self.recv_lo.is_cuda:
+                import torch
+                torch.cuda.synchronize(self.recv_lo.device)
+        L.slab_halo(direction, parity, 0, self.recv_lo.data_ptr(), False)
+        L.slab_halo(direction, parity, 1, self.recv_hi.data_ptr(), False)
+
+    def fill_halos(self):
+        for mu in range(4):
+            for p in (0, 1):
+                self.exchange(mu, p)
+
+    def sweep(self, n=1):
+        for _ in range(n):
+            for p, mu, kind in phase_sequence(self.cfg.n_or):
+                self.slab.L.phase(p, mu, kind)
+                self.exchange(mu, p)
+            self.sweeps_done += 1
+            if self.cfg.reunit_every > 0 and self.sweeps_done % self.cfg.reunit_every == 0:
+                self.slab.L.reunitarize(self.cfg.reunit_fp64)
+        self.slab.L.sync()

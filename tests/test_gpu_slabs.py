@@ -1,0 +1,66 @@
+"""x-slab decomposition (qg_set_slab, qcdgpu_b200.slabs.SlabSet): a lattice
+cut into x-slabs on one GPU -- the way the reference exercises its BIGLAT
+decomposition on a single device -- follows the undecomposed lattice's
+chain bit for bit through heatbath, overrelaxation and Gram-Schmidt, and
+the slabs' interior x-profiles add up to the lattice's action and Polyakov
+sums."""
+import numpy as np
+import pytest
+
+import qcdgpu_b200 as Q
+from qcdgpu_b200.slabs import SlabSet, split
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.parametrize("group,precision,dims,parts", [
+    (3, 0, (8, 4, 4, 6), 2), (3, 0, (8, 4, 4, 6), 3), (3, 1, (6, 4, 2, 4), 2), (3, 0, (4, 4, 4, 4), 3),
+    (2, 1, (8, 4, 4, 4), 4), (2, 0, (6, 2, 4, 4), 1)])
+def test_slabs_follow_the_whole_lattice_bit_for_bit(group, precision, dims, parts):
+    cfg = Q.default_config(group=group, size=dims, precision=precision, start=Q.START_HOT, prng=Q.PRNG_PHILOX,
+                           beta=5.8 if group == 3 else 2.3, n_or=2, reunit_every=2, reunit_fp64=1, randseries=77)
+    G = Q.Lattice(cfg)
+    G.seed()
+    G.init(Q.START_HOT)
+    S = SlabSet(cfg, parts)
+    S.seed()
+    S.upload(G.download())
+    assert np.array_equal(S.download(), G.download())
+    for s in range(3):
+        G.sweep(1)
+        S.sweep(1)
+        assert np.array_equal(S.download(), G.download()), s
+    ga, sa = np.array(G.action_sums()), S.action_sums()
+    assert np.all(np.abs(sa - ga) <= 1e-12 * np.abs(ga)), (sa, ga)
+    gp, sp = np.array(G.polyakov_sums()[:2]), S.polyakov_sums()
+    assert np.all(np.abs(sp - gp) <= 1e-12 * (1 + np.abs(gp))), (sp, gp)
+    S.close()
+    G.close()
+
+
+def test_slab_halo_fill_from_a_cold_start_and_argument_checks():
+    cfg = Q.default_config(group=3, size=(6, 4, 4, 4), precision=0, start=Q.START_COLD, prng=Q.PRNG_PHILOX,
+                           beta=6.0, n_or=1, reunit_every=0, randseries=5)
+    G = Q.Lattice(cfg)
+    G.seed()
+    G.init(Q.START_COLD)
+    S = SlabSet(cfg, 2)
+    S.seed()
+    for s in S.slabs:
+        s.L.init(Q.START_COLD)
+    S.fill_halos()
+    S.sweep(2)
+    G.sweep(2)
+    assert np.array_equal(S.download(), G.download())
+    L = S.slabs[0].L
+    with pytest.raises(Q.QGError):
+        L.sweep(1)                                   # a slab sweeps through the slab driver
+    with pytest.raises(Q.QGError):
+        L.init(Q.START_HOT)                          # hot / Haar starts are whole-lattice
+    S.close()
+    G.close()
+    with pytest.raises(Q.QGError):                   # RANLUX: no slabs
+        Q.Lattice(Q.default_config(group=3, size=(4, 4, 4, 4), prng=Q.PRNG_RANLUX)).set_slab(0, 8)
+    with pytest.raises(Q.QGError):                   # odd global N1
+        Q.Lattice(Q.default_config(group=3, size=(4, 4, 4, 4), prng=Q.PRNG_PHILOX)).set_slab(0, 7)
+    assert split(10, 3) == ([4, 3, 3], [0, 4, 7])
