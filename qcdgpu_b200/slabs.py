@@ -193,7 +193,8 @@ class SlabSet:
 class DistSlab:
     """One x-slab per rank of a torch.distributed group (rank k holds slab
     k of split(N1, world)).  `slab` is a _Slab, or any object with the same
-    w / nbytes / L.slab_halo / L.phase / L.reunitarize / L.sync members (the
+    nbytes / L.slab_halo / L.phase / L.reunitarize / L.sync (and, for device
+    buffers, L.stream) members (the
     host-side test passes a stand-in)."""
 
     def __init__(self, cfg, dist, device, slab=None):
@@ -208,23 +209,32 @@ class DistSlab:
         self.sweeps_done = 0
 
     def exchange(self, direction, parity):
+        """pack both boundary slices, swap them with the neighbours, unpack
+        into the halos.  On GPUs every step is ordered on the slab
+        context's stream (the NCCL operations are issued with it as torch's
+        current stream and waited on by it), so no host round trip."""
+        import contextlib
+
+        import torch
         L = self.slab.L
         L.slab_halo(direction, parity, 1, self.send_hi.data_ptr(), True)
         L.slab_halo(direction, parity, 0, self.send_lo.data_ptr(), True)
-        L.sync()
-        if self.world == 1:
-            self.recv_lo.copy_(self.send_hi)
-            self.recv_hi.copy_(self.send_lo)
+        if self.send_hi.is_cuda:
+            scope = torch.cuda.stream(torch.cuda.ExternalStream(L.stream(), device=self.send_hi.device))
         else:
-            right, left = (self.rank + 1) % self.world, (self.rank - 1) % self.world
-            P2P = self.dist.P2POp
-            ops = [P2P(self.dist.isend, self.send_hi, right), P2P(self.dist.irecv, self.recv_lo, left),
-                   P2P(self.dist.isend, self.send_lo, left), P2P(self.dist.irecv, self.recv_hi, right)]
-            for r in self.dist.batch_isend_irecv(ops):
-                r.wait()
-            if self.recv_lo.is_cuda:
-                import torch
-                torch.cuda.synchronize(self.recv_lo.device)
+            L.sync()
+            scope = contextlib.nullcontext()
+        with scope:
+            if self.world == 1:
+                self.recv_lo.copy_(self.send_hi)
+                self.recv_hi.copy_(self.send_lo)
+            else:
+                right, left = (self.rank + 1) % self.world, (self.rank - 1) % self.world
+                P2P = self.dist.P2POp
+                ops = [P2P(self.dist.isend, self.send_hi, right), P2P(self.dist.irecv, self.recv_lo, left),
+                       P2P(self.dist.isend, self.send_lo, left), P2P(self.dist.irecv, self.recv_hi, right)]
+                for r in self.dist.batch_isend_irecv(ops):
+                    r.wait()
         L.slab_halo(direction, parity, 0, self.recv_lo.data_ptr(), False)
         L.slab_halo(direction, parity, 1, self.recv_hi.data_ptr(), False)
 

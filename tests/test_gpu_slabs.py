@@ -8,7 +8,7 @@ import numpy as np
 import pytest
 
 import qcdgpu_b200 as Q
-from qcdgpu_b200.slabs import SlabSet, split
+from qcdgpu_b200.slabs import DistSlab, SlabSet, _to_slab, split
 
 pytestmark = pytest.mark.gpu
 
@@ -64,3 +64,37 @@ def test_slab_halo_fill_from_a_cold_start_and_argument_checks():
     with pytest.raises(Q.QGError):                   # odd global N1
         Q.Lattice(Q.default_config(group=3, size=(4, 4, 4, 4), prng=Q.PRNG_PHILOX)).set_slab(0, 7)
     assert split(10, 3) == ([4, 3, 3], [0, 4, 7])
+
+
+def test_dist_slab_on_one_rank_follows_the_whole_lattice():
+    """DistSlab's GPU path (pack, exchange and unpack ordered on the slab's
+    stream, device buffers) in a one-rank NCCL group: the slab is the whole
+    lattice with its own boundaries as halos"""
+    import socket
+
+    import torch
+    import torch.distributed as dist
+    sk = socket.socket()
+    sk.bind(("127.0.0.1", 0))
+    port = sk.getsockname()[1]
+    sk.close()
+    dist.init_process_group("nccl", init_method="tcp://127.0.0.1:%d" % port, rank=0, world_size=1)
+    try:
+        cfg = Q.default_config(group=3, size=(6, 4, 4, 4), precision=0, start=Q.START_HOT, prng=Q.PRNG_PHILOX,
+                               beta=5.9, n_or=1, reunit_every=2, reunit_fp64=1, randseries=9)
+        G = Q.Lattice(cfg)
+        G.seed()
+        G.init(Q.START_HOT)
+        D = DistSlab(cfg, dist, torch.device("cuda", 0))
+        D.slab.L.seed()
+        D.slab.L.upload(_to_slab(G.download(), cfg, D.slab.w, D.slab.x0, D.slab.cfg))
+        D.sweep(3)
+        G.sweep(3)
+        t = D.slab.L.download().reshape(12, -1, 4)
+        g = G.download().reshape(12, -1, 4)
+        ns = 4 * 4 * 4
+        assert np.array_equal(t[:, ns:7 * ns, :], g[:, :6 * ns, :])
+        D.slab.close()
+        G.close()
+    finally:
+        dist.destroy_process_group()
