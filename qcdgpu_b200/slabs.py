@@ -252,3 +252,81 @@ class DistSlab:
             if self.cfg.reunit_every > 0 and self.sweeps_done % self.cfg.reunit_every == 0:
                 self.slab.L.reunitarize(self.cfg.reunit_fp64)
         self.slab.L.sync()
+
+
+def main():
+    """torchrun --nproc-per-node N -m qcdgpu_b200.slabs [--size 64] [--sweeps 10]
+    one slab per rank of an SU(3) (or SU(2)) lattice from a cold start; rank 0
+    prints the sweep time (slowest rank, CUDA events on the slab's stream)
+    and the lattice's plaquette and Polyakov loop"""
+    import argparse
+    import json
+
+    import torch
+
+    from qcdgpu_b200 import replicas as RP
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--size", type=int, default=32)
+    ap.add_argument("--group", type=int, default=3)
+    ap.add_argument("--precision", type=int, default=0)
+    ap.add_argument("--beta", type=float, default=6.0)
+    ap.add_argument("--n-or", type=int, default=4)
+    ap.add_argument("--sweeps", type=int, default=10)
+    ap.add_argument("--seed", type=int, default=54)
+    a = ap.parse_args()
+    rank, world, local = RP.dist_env()
+    torch.cuda.set_device(local)
+    import torch.distributed as dist
+    if world > 1:
+        RP.init("nccl", 300, torch.device("cuda", local))
+    else:
+        dist.init_process_group("nccl", init_method="tcp://127.0.0.1:%d" % _free_port(), rank=0, world_size=1)
+    cfg = Q.default_config(group=a.group, size=a.size, precision=a.precision, start=Q.START_COLD,
+                           prng=Q.PRNG_PHILOX, beta=a.beta, n_or=a.n_or, reunit_every=10, reunit_fp64=1,
+                           randseries=a.seed)
+    D = DistSlab(cfg, dist, torch.device("cuda", local))
+    L = D.slab.L
+    L.seed()
+    L.init(Q.START_COLD)
+    D.fill_halos()
+    D.sweep(1)
+    stream = torch.cuda.ExternalStream(L.stream())
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    dist.barrier()
+    e0.record(stream)
+    D.sweep(a.sweeps)
+    e1.record(stream)
+    e1.synchronize()
+    ms = torch.tensor([e0.elapsed_time(e1)], device="cuda")
+    dist.all_reduce(ms, op=dist.ReduceOp.MAX)
+    w = D.slab.w
+    sums = torch.tensor(np.concatenate([L.action_profile(0)[1:w + 1].sum(axis=0),
+                                        L.polyakov_profile(0)[1:w + 1].sum(axis=0)]), device="cuda")
+    dist.all_reduce(sums)
+    V = a.size ** 4
+    N = a.group
+    bet = float(np.float32(a.beta / N)) if a.precision == 0 else a.beta / N
+    s = sums.cpu().numpy()
+    # each plaquette contributes (beta/N)(N - Re Tr): mean Re Tr per plaquette, range [-N, N]
+    plaq = (6 * N * V - (s[0] + s[1]) / bet) / (6 * V)
+    if rank == 0:
+        per = ms.item() / a.sweeps
+        print(json.dumps({"workload": "SU(%d) %d^4 beta=%.2f, 1 HB + %d OR, x-slabs over %d ranks"
+                                      % (N, a.size, a.beta, a.n_or, world),
+                          "ms_per_sweep": per, "link_updates_per_s": 4 * V * (1 + a.n_or) / (per * 1e-3),
+                          "plaquette": plaq, "polyakov_re": s[2] / (V / a.size * N), "slab_widths": split(a.size, world)[0]}))
+    D.slab.close()
+    dist.destroy_process_group()
+
+
+def _free_port():
+    import socket
+    s = socket.socket()
+    s.bind(("127.0.0.1", 0))
+    p = s.getsockname()[1]
+    s.close()
+    return p
+
+
+if __name__ == "__main__":
+    main()
