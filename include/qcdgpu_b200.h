@@ -180,6 +180,9 @@ int qg_set_slab(qg_ctx *ctx, int x0, int n1_global);
  * x = w + 1 (side 1).  Side 1 of a slab feeds side 0 of its right
  * neighbour and vice versa.  Asynchronous on the context's stream.       */
 int qg_slab_halo(qg_ctx *ctx, int dir, int parity, int side, void *buf, int to_buf);
+/* both sides in one kernel launch: buf_lo for side 0, buf_hi for side 1
+ * (device memory, 16-byte aligned, qg_slab_halo_bytes bytes each)        */
+int qg_slab_halo2(qg_ctx *ctx, int dir, int parity, void *buf_lo, void *buf_hi, int to_buf);
 int qg_slab_halo_bytes(qg_ctx *ctx, uint64_t *bytes);
 
 /* lattice_measurement_plq / lattice_measurement / lattice_polyakov /

@@ -795,6 +795,45 @@ extern "C" int qg_slab_halo(qg_ctx *c, int dir, int parity, int side, void *buf,
     return QG_OK;
 }
 
+// both sides in one launch: to_buf = 1 packs boundary slices x = 1 into
+// buf_lo and x = w into buf_hi; to_buf = 0 unpacks buf_lo into halo x = 0
+// and buf_hi into halo x = w+1 (buffers in device memory, 16-byte aligned)
+extern "C" int qg_slab_halo2(qg_ctx *c, int dir, int parity, void *buf_lo, void *buf_hi, int to_buf)
+{
+    if (!c || !buf_lo || !buf_hi) return QG_ERR_ARG;
+    if (!c->slab) return fail(c, QG_ERR_STATE, "not a slab (qg_set_slab)");
+    if (dir < 0 || dir > 3 || (parity != 0 && parity != 1)) return fail(c, QG_ERR_ARG, "bad direction / parity");
+    if (((uintptr_t)buf_lo | (uintptr_t)buf_hi) & 15) return fail(c, QG_ERR_ARG, "halo buffers must be 16-byte aligned");
+    for (void *b : { buf_lo, buf_hi }) {       // the kernel reads and writes them: device memory only
+        cudaPointerAttributes at;
+        if (cudaPointerGetAttributes(&at, b) != cudaSuccess ||
+            (at.type != cudaMemoryTypeDevice && at.type != cudaMemoryTypeManaged)) {
+            cudaGetLastError();
+            return fail(c, QG_ERR_ARG, "qg_slab_halo2 needs device buffers (qg_slab_halo copies from host memory)");
+        }
+    }
+    const uint32_t h = c->G.n2n3n4 / 2, w = (uint32_t)c->G.n[0] - 2;
+    const uint32_t q = (uint32_t)(parity ^ ((c->slab_x0 - 1) & 1));
+    const size_t unit = slab_elem(c) / 16;                       // 16-byte words per element
+    uint4 *base = static_cast<uint4 *>(c->links);
+    SlabCopy cp;
+    cp.n = 0;
+    cp.words = (uint32_t)(h * unit);
+    for (int side = 0; side < 2; side++) {
+        const uint32_t x = to_buf ? (side ? w : 1) : (side ? w + 1 : 0);
+        uint4 *b = static_cast<uint4 *>(side ? buf_hi : buf_lo);
+        for (uint32_t k = 0; k < slab_planes(c); k++) {
+            uint4 *lk = base + ((size_t)(dir + 4 * k) * c->G.pstride + (size_t)q * c->G.cb + (size_t)x * h) * unit;
+            uint4 *bk = b + (size_t)k * h * unit;
+            cp.src[cp.n] = to_buf ? lk : bk;
+            cp.dst[cp.n] = to_buf ? bk : lk;
+            cp.n++;
+        }
+    }
+    QG_CK(launch_slab_copy(cp, c->stream), "slab halo kernel");
+    return QG_OK;
+}
+
 extern "C" int qg_sweep(qg_ctx *c, int nsweeps)
 {
     if (!c) return QG_ERR_ARG;

@@ -805,6 +805,25 @@ __global__ void k_add_u64(uint64_t *p, uint64_t v)
 {
     if (threadIdx.x == 0 && blockIdx.x == 0) *p += v;
 }
+// the copies of a slab halo exchange (qg_slab_halo2): blockIdx.y picks
+// the copy, threads stride over its 16-byte words (coalesced both sides)
+__global__ void k_slab_copy(SlabCopy c)
+{
+    const int k = blockIdx.y;
+    const uint4 *src = c.src[k];
+    uint4 *dst = c.dst[k];
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < c.words; i += gridDim.x * blockDim.x)
+        dst[i] = src[i];
+}
+
+cudaError_t launch_slab_copy(const SlabCopy &c, cudaStream_t s)
+{
+    if (c.n <= 0 || c.n > 6 || c.words == 0) return cudaErrorInvalidValue;
+    const unsigned bx = (unsigned)min((c.words + 255u) / 256u, 148u * 4u);
+    k_slab_copy<<<dim3(bx, (unsigned)c.n), 256, 0, s>>>(c);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_add_u64(uint64_t *p, uint64_t v, cudaStream_t s)
 {
     k_add_u64<<<1, 32, 0, s>>>(p, v);

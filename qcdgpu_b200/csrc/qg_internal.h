@@ -76,6 +76,16 @@ cudaError_t launch_wilson_all(const Geom &G, const void *links, int group, int p
                               int fp64_products, const double *params, int twist, double *partials, double *out,
                               cudaStream_t s);
 cudaError_t launch_add_u64(uint64_t *p, uint64_t v, cudaStream_t s);
+// slab halo exchange: both sides of one (direction, parity) slice in one
+// launch; `unit` = 16-byte words per link-plane element, src / dst offsets
+// in those words
+struct SlabCopy {
+    const uint4 *src[6];
+    uint4 *dst[6];
+    int n;                 // copies (sides x planes)
+    uint32_t words;        // 16-byte words per copy
+};
+cudaError_t launch_slab_copy(const SlabCopy &c, cudaStream_t s);
 
 // RANLUX, reference layout: one generator per instance, seed table of 7
 // float4 per instance (SoA), output prns[s*instances + i]

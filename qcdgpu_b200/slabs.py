@@ -147,12 +147,12 @@ class SlabSet:
         K = len(self.slabs)
         self._sync()                         # the staging buffers are free again
         for k, s in enumerate(self.slabs):
-            s.L.slab_halo(direction, parity, 1, self.buf_hi[k].data_ptr(), True)
-            s.L.slab_halo(direction, parity, 0, self.buf_lo[k].data_ptr(), True)
+            s.L.slab_halo2(direction, parity, self.buf_lo[k].data_ptr(), self.buf_hi[k].data_ptr(), True)
         self._sync()
-        for k in range(K):
-            self.slabs[(k + 1) % K].L.slab_halo(direction, parity, 0, self.buf_hi[k].data_ptr(), False)
-            self.slabs[(k - 1) % K].L.slab_halo(direction, parity, 1, self.buf_lo[k].data_ptr(), False)
+        for k, s in enumerate(self.slabs):
+            # low halo <- left neighbour's high boundary, high halo <- right's low
+            s.L.slab_halo2(direction, parity, self.buf_hi[(k - 1) % K].data_ptr(),
+                           self.buf_lo[(k + 1) % K].data_ptr(), False)
 
     def fill_halos(self):
         for mu in range(4):
@@ -193,7 +193,7 @@ class SlabSet:
 class DistSlab:
     """One x-slab per rank of a torch.distributed group (rank k holds slab
     k of split(N1, world)).  `slab` is a _Slab, or any object with the same
-    nbytes / L.slab_halo / L.phase / L.reunitarize / L.sync (and, for device
+    nbytes / L.slab_halo2 / L.phase / L.reunitarize / L.sync (and, for device
     buffers, L.stream) members (the
     host-side test passes a stand-in)."""
 
@@ -217,8 +217,7 @@ class DistSlab:
 
         import torch
         L = self.slab.L
-        L.slab_halo(direction, parity, 1, self.send_hi.data_ptr(), True)
-        L.slab_halo(direction, parity, 0, self.send_lo.data_ptr(), True)
+        L.slab_halo2(direction, parity, self.send_lo.data_ptr(), self.send_hi.data_ptr(), True)
         if self.send_hi.is_cuda:
             scope = torch.cuda.stream(torch.cuda.ExternalStream(L.stream(), device=self.send_hi.device))
         else:
@@ -235,8 +234,7 @@ class DistSlab:
                        P2P(self.dist.isend, self.send_lo, left), P2P(self.dist.irecv, self.recv_hi, right)]
                 for r in self.dist.batch_isend_irecv(ops):
                     r.wait()
-        L.slab_halo(direction, parity, 0, self.recv_lo.data_ptr(), False)
-        L.slab_halo(direction, parity, 1, self.recv_hi.data_ptr(), False)
+        L.slab_halo2(direction, parity, self.recv_lo.data_ptr(), self.recv_hi.data_ptr(), False)
 
     def fill_halos(self):
         for mu in range(4):
@@ -280,7 +278,8 @@ def main():
     if world > 1:
         RP.init("nccl", 300, torch.device("cuda", local))
     else:
-        dist.init_process_group("nccl", init_method="tcp://127.0.0.1:%d" % _free_port(), rank=0, world_size=1)
+        dist.init_process_group("nccl", init_method="tcp://127.0.0.1:%d" % _free_port(), rank=0, world_size=1,
+                                device_id=torch.device("cuda", local))
     cfg = Q.default_config(group=a.group, size=a.size, precision=a.precision, start=Q.START_COLD,
                            prng=Q.PRNG_PHILOX, beta=a.beta, n_or=a.n_or, reunit_every=10, reunit_fp64=1,
                            randseries=a.seed)

@@ -57,6 +57,9 @@ def test_slab_halo_fill_from_a_cold_start_and_argument_checks():
         L.sweep(1)                                   # a slab sweeps through the slab driver
     with pytest.raises(Q.QGError):
         L.init(Q.START_HOT)                          # hot / Haar starts are whole-lattice
+    host = np.zeros(S.slabs[0].nbytes, dtype=np.uint8)
+    with pytest.raises(Q.QGError):                   # the one-launch form takes device buffers only
+        L.slab_halo2(0, 0, host.ctypes.data, host.ctypes.data, True)
     S.close()
     G.close()
     with pytest.raises(Q.QGError):                   # RANLUX: no slabs

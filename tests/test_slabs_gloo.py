@@ -41,6 +41,10 @@ class _FakeL:
             ctypes.memmove(dst.ctypes.data, ptr, NBYTES)
             self.halo[(direction, parity, side)] = int(dst[0]) if np.all(dst == dst[0]) else -1
 
+    def slab_halo2(self, direction, parity, ptr_lo, ptr_hi, to_buf):
+        self.slab_halo(direction, parity, 0, ptr_lo, to_buf)
+        self.slab_halo(direction, parity, 1, ptr_hi, to_buf)
+
     def phase(self, parity, direction, kind):
         self.log.append(("phase", parity, direction, kind))
 
