@@ -183,6 +183,11 @@ int qg_slab_halo(qg_ctx *ctx, int dir, int parity, int side, void *buf, int to_b
 /* both sides in one kernel launch: buf_lo for side 0, buf_hi for side 1
  * (device memory, 16-byte aligned, qg_slab_halo_bytes bytes each)        */
 int qg_slab_halo2(qg_ctx *ctx, int dir, int parity, void *buf_lo, void *buf_hi, int to_buf);
+/* qg_phase of a slab in two parts, so that the exchange of the boundary
+ * links overlaps the interior update: part 0 updates the boundary slices
+ * x = 1 and x = w, part 1 the slices 2 .. w-1 (and advances the heatbath
+ * PRN counter).  Part 0 then part 1 equals qg_phase bit for bit.          */
+int qg_slab_phase(qg_ctx *ctx, int parity, int dir, int kind, int part);
 int qg_slab_halo_bytes(qg_ctx *ctx, uint64_t *bytes);
 
 /* lattice_measurement_plq / lattice_measurement / lattice_polyakov /

@@ -568,6 +568,44 @@ extern "C" int qg_phase(qg_ctx *c, int parity, int dir, int kind)
     return QG_OK;
 }
 
+// one phase of a slab in parts, so that its halo exchange can overlap the
+// interior: part 0 updates the boundary slices x = 1 and x = w, part 1 the
+// interior slices 2 .. w-1 and then advances the heatbath counter as
+// qg_phase does.  The updates of one phase are independent of each other,
+// so part 0 then part 1 is qg_phase bit for bit.
+extern "C" int qg_slab_phase(qg_ctx *c, int parity, int dir, int kind, int part)
+{
+    if (!c) return QG_ERR_ARG;
+    if (!c->slab) return fail(c, QG_ERR_STATE, "not a slab (qg_set_slab)");
+    if ((parity != 0 && parity != 1) || dir < 0 || dir > 3) return fail(c, QG_ERR_ARG, "bad parity/direction");
+    if (kind != QG_UPDATE_HEATBATH && kind != QG_UPDATE_OVERRELAX) return fail(c, QG_ERR_ARG, "bad update kind");
+    if (part != 0 && part != 1) return fail(c, QG_ERR_ARG, "part: 0 boundary slices, 1 interior slices");
+    if (needs_seed(c, kind)) return fail(c, QG_ERR_STATE, "heatbath needs a seeded PRNG (qg_prng_seed)");
+    PhaseArgs a = phase_args(c, parity, dir, kind, 0);
+    const uint32_t h = c->G.n2n3n4 / 2, w = (uint32_t)c->G.n[0] - 2;
+    if (part == 0) {
+        a.t_begin = h;                                   // slice 1
+        a.t_end = 2 * h;
+        QG_CK(launch_phase(c, a), "phase kernel");
+        if (w > 1) {
+            a.t_begin = w * h;                           // slice w
+            a.t_end = (w + 1) * h;
+            QG_CK(launch_phase(c, a), "phase kernel");
+        }
+        return QG_OK;
+    }
+    if (w > 2) {
+        a.t_begin = 2 * h;                               // slices 2 .. w-1
+        a.t_end = w * h;
+        QG_CK(launch_phase(c, a), "phase kernel");
+    }
+    if (kind == QG_UPDATE_HEATBATH && a.prn_mode == QG_PRNG_PHILOX) {
+        QG_CK(launch_add_u64(c->d_phase, 1, c->stream), "phase counter");
+        c->phase_counter++;
+    }
+    return QG_OK;
+}
+
 // times each launch shape of the heatbath and overrelaxation phase kernels
 // on the live field (restored afterwards, PRN counters untouched) and keeps
 // the fastest per kind

@@ -193,47 +193,81 @@ class SlabSet:
 class DistSlab:
     """One x-slab per rank of a torch.distributed group (rank k holds slab
     k of split(N1, world)).  `slab` is a _Slab, or any object with the same
-    nbytes / L.slab_halo2 / L.phase / L.reunitarize / L.sync (and, for device
-    buffers, L.stream) members (the
+    nbytes / L.slab_halo2 / L.slab_phase (L.phase for one rank) /
+    L.reunitarize / L.sync (and, for device buffers, L.stream) members (the
     host-side test passes a stand-in)."""
 
-    def __init__(self, cfg, dist, device, slab=None):
+    def __init__(self, cfg, dist, device, slab=None, overlap=None):
         import torch
         self.cfg, self.dist = cfg, dist
         self.rank, self.world = dist.get_rank(), dist.get_world_size()
+        # split each phase so the swap overlaps the interior (default: when
+        # there is a neighbour to swap with)
+        self.overlap = self.world > 1 if overlap is None else bool(overlap)
         w, x0 = split(cfg.size[0], self.world)
         self.slab = slab if slab is not None else _Slab(cfg, w[self.rank], x0[self.rank])
         nb = self.slab.nbytes
         self.send_hi, self.send_lo, self.recv_hi, self.recv_lo = (
             torch.empty(nb, dtype=torch.uint8, device=device) for _ in range(4))
+        self.comm = torch.cuda.Stream(device=device) if self.send_hi.is_cuda else None
         self.sweeps_done = 0
 
-    def exchange(self, direction, parity):
-        """pack both boundary slices, swap them with the neighbours, unpack
-        into the halos.  On GPUs every step is ordered on the slab
-        context's stream (the NCCL operations are issued with it as torch's
-        current stream and waited on by it), so no host round trip."""
-        import contextlib
+    def _swap(self):
+        """send the packed boundaries, receive the neighbours' (current
+        stream)"""
+        if self.world == 1:
+            self.recv_lo.copy_(self.send_hi)
+            self.recv_hi.copy_(self.send_lo)
+            return
+        right, left = (self.rank + 1) % self.world, (self.rank - 1) % self.world
+        P2P = self.dist.P2POp
+        ops = [P2P(self.dist.isend, self.send_hi, right), P2P(self.dist.irecv, self.recv_lo, left),
+               P2P(self.dist.isend, self.send_lo, left), P2P(self.dist.irecv, self.recv_hi, right)]
+        for r in self.dist.batch_isend_irecv(ops):
+            r.wait()
 
+    def phase(self, parity, direction, kind):
+        """one phase with its halo exchange overlapping the interior update:
+        boundary slices, pack, then the interior on the slab's stream while
+        the swap runs on a second stream; the halos are unpacked (after the
+        swap) before the next phase reads them.  On the host (gloo) the
+        steps run in turn."""
+        import torch
+        L = self.slab.L
+        if not self.overlap:                 # one launch, then the exchange
+            L.phase(parity, direction, kind)
+            self.exchange(direction, parity)
+            return
+        L.slab_phase(parity, direction, kind, 0)
+        L.slab_halo2(direction, parity, self.send_lo.data_ptr(), self.send_hi.data_ptr(), True)
+        if self.send_hi.is_cuda:
+            ctx = torch.cuda.ExternalStream(L.stream(), device=self.send_hi.device)
+            packed = torch.cuda.Event()
+            packed.record(ctx)
+            L.slab_phase(parity, direction, kind, 1)
+            with torch.cuda.stream(self.comm):
+                self.comm.wait_event(packed)
+                self._swap()
+                swapped = torch.cuda.Event()
+                swapped.record(self.comm)
+            ctx.wait_event(swapped)
+        else:
+            L.sync()
+            L.slab_phase(parity, direction, kind, 1)
+            self._swap()
+        L.slab_halo2(direction, parity, self.recv_lo.data_ptr(), self.recv_hi.data_ptr(), False)
+
+    def exchange(self, direction, parity):
+        """refresh the halos of (direction, parity) without an update"""
         import torch
         L = self.slab.L
         L.slab_halo2(direction, parity, self.send_lo.data_ptr(), self.send_hi.data_ptr(), True)
         if self.send_hi.is_cuda:
-            scope = torch.cuda.stream(torch.cuda.ExternalStream(L.stream(), device=self.send_hi.device))
+            with torch.cuda.stream(torch.cuda.ExternalStream(L.stream(), device=self.send_hi.device)):
+                self._swap()
         else:
             L.sync()
-            scope = contextlib.nullcontext()
-        with scope:
-            if self.world == 1:
-                self.recv_lo.copy_(self.send_hi)
-                self.recv_hi.copy_(self.send_lo)
-            else:
-                right, left = (self.rank + 1) % self.world, (self.rank - 1) % self.world
-                P2P = self.dist.P2POp
-                ops = [P2P(self.dist.isend, self.send_hi, right), P2P(self.dist.irecv, self.recv_lo, left),
-                       P2P(self.dist.isend, self.send_lo, left), P2P(self.dist.irecv, self.recv_hi, right)]
-                for r in self.dist.batch_isend_irecv(ops):
-                    r.wait()
+            self._swap()
         L.slab_halo2(direction, parity, self.recv_lo.data_ptr(), self.recv_hi.data_ptr(), False)
 
     def fill_halos(self):
@@ -244,8 +278,7 @@ class DistSlab:
     def sweep(self, n=1):
         for _ in range(n):
             for p, mu, kind in phase_sequence(self.cfg.n_or):
-                self.slab.L.phase(p, mu, kind)
-                self.exchange(mu, p)
+                self.phase(p, mu, kind)
             self.sweeps_done += 1
             if self.cfg.reunit_every > 0 and self.sweeps_done % self.cfg.reunit_every == 0:
                 self.slab.L.reunitarize(self.cfg.reunit_fp64)

@@ -70,9 +70,11 @@ def test_slab_halo_fill_from_a_cold_start_and_argument_checks():
 
 
 def test_dist_slab_on_one_rank_follows_the_whole_lattice():
-    """DistSlab's GPU path (pack, exchange and unpack ordered on the slab's
-    stream, device buffers) in a one-rank NCCL group: the slab is the whole
-    lattice with its own boundaries as halos"""
+    """DistSlab's GPU path in a one-rank NCCL group -- the slab is the whole
+    lattice with its own boundaries as halos: with the overlapped phases
+    (boundary slices, pack, interior on the slab's stream while the swap
+    runs on a second stream, unpack) and without, both bit-identical to the
+    whole lattice"""
     import socket
 
     import torch
@@ -81,23 +83,29 @@ def test_dist_slab_on_one_rank_follows_the_whole_lattice():
     sk.bind(("127.0.0.1", 0))
     port = sk.getsockname()[1]
     sk.close()
-    dist.init_process_group("nccl", init_method="tcp://127.0.0.1:%d" % port, rank=0, world_size=1)
+    dist.init_process_group("nccl", init_method="tcp://127.0.0.1:%d" % port, rank=0, world_size=1,
+                            device_id=torch.device("cuda", 0))
     try:
         cfg = Q.default_config(group=3, size=(6, 4, 4, 4), precision=0, start=Q.START_HOT, prng=Q.PRNG_PHILOX,
                                beta=5.9, n_or=1, reunit_every=2, reunit_fp64=1, randseries=9)
         G = Q.Lattice(cfg)
         G.seed()
         G.init(Q.START_HOT)
-        D = DistSlab(cfg, dist, torch.device("cuda", 0))
-        D.slab.L.seed()
-        D.slab.L.upload(_to_slab(G.download(), cfg, D.slab.w, D.slab.x0, D.slab.cfg))
-        D.sweep(3)
         G.sweep(3)
-        t = D.slab.L.download().reshape(12, -1, 4)
-        g = G.download().reshape(12, -1, 4)
         ns = 4 * 4 * 4
-        assert np.array_equal(t[:, ns:7 * ns, :], g[:, :6 * ns, :])
-        D.slab.close()
+        g = G.download().reshape(12, -1, 4)
+        start = Q.Lattice(cfg)
+        start.seed()
+        start.init(Q.START_HOT)
+        for overlap in (True, False):
+            D = DistSlab(cfg, dist, torch.device("cuda", 0), overlap=overlap)
+            D.slab.L.seed()
+            D.slab.L.upload(_to_slab(start.download(), cfg, D.slab.w, D.slab.x0, D.slab.cfg))
+            D.sweep(3)
+            t = D.slab.L.download().reshape(12, -1, 4)
+            assert np.array_equal(t[:, ns:7 * ns, :], g[:, :6 * ns, :]), overlap
+            D.slab.close()
+        start.close()
         G.close()
     finally:
         dist.destroy_process_group()

@@ -45,8 +45,8 @@ class _FakeL:
         self.slab_halo(direction, parity, 0, ptr_lo, to_buf)
         self.slab_halo(direction, parity, 1, ptr_hi, to_buf)
 
-    def phase(self, parity, direction, kind):
-        self.log.append(("phase", parity, direction, kind))
+    def slab_phase(self, parity, direction, kind, part):
+        self.log.append(("phase", parity, direction, kind, part))
 
     def reunitarize(self, fp64):
         self.log.append(("gs", int(bool(fp64))))
@@ -73,7 +73,7 @@ def _rank_main(rank, world, port, out):
                            reunit_fp64=1)
     D = DistSlab(cfg, dist, "cpu", slab=_FakeSlab(rank))
     D.sweep(2)
-    seq = [("phase",) + s for s in phase_sequence(1)]
+    seq = [("phase",) + s + (part,) for s in phase_sequence(1) for part in (0, 1)]
     expect = seq + seq + [("gs", 1)]
     out.put((rank, dict(D.slab.L.halo), D.slab.L.log == expect))
     dist.destroy_process_group()
