@@ -632,8 +632,9 @@ constexpr int kWilsonMax = 16;
 // spatial lines S(t) = L_i^R(x + t t) of the last Tmax + 1 time slices in
 // a private ring in shared memory, so each line is built once per column
 // (not once per (t0, T)); the time lines at x and x + R i grow by one
-// product per T, and each term is retr4(L_t^T(x), S(t0+T), L_t^T(x+R i),
-// S(t0)).  The per-thread sums w[T] live in shared memory.  Dynamic shared
+// product per T, and each term Re Tr(L_t^T(x) S(t0+T) L_t^T(x+R i)^+
+// S(t0)^+) is taken as Re Tr(Y S(t0+T) L_t^T(x+R i)^+) with Y = S(t0)^+
+// L_t^T(x).  The per-thread sums w[T] live in shared memory.  Dynamic shared
 // memory: (Tmax+1) ring entries and Tmax doubles per thread.  A ring entry
 // holds the 2 x 2 block for SU(2); for SU(3) the full line in FP64, or
 // with FP32 products rows 1, 2 only (row 3 rebuilt on reading; rebuilding
@@ -696,23 +697,46 @@ __global__ void __launch_bounds__(128) k_wilson_cols(Field<Real> U, Geom G, int 
         Crd cy0 = c0;
         for (int k = 0; k < R; k++) cy0 = step_plus(G, cy0, i);     // x + R i
         for (int t = 0; t < Tmax; t++) put(t, line(t % nt));
+        // Re Tr(L_t^T(x) S(t0+T) L_t^T(x+Ri)^+ S(t0)^+) = Re Tr(Y S(t0+T) my^+)
+        // with Y = S(t0)^+ L_t^T(x) grown one link per T like the time line
+        // itself: per T one product for Y, one for my, one for Y S and a
+        // 9-term trace (the bottom line S(t0) enters once per t0)
+        auto hmul = [](const M3<P> &a, const M3<P> &b) {        // a^+ b
+            M3<P> r;
+#pragma unroll
+            for (int i = 0; i < 3; i++)
+#pragma unroll
+                for (int j = 0; j < 3; j++) r.m[i][j] = cdot3(&a.m[0][i], 3, &b.m[0][j], 3);
+            return r;
+        };
+        auto retr_h = [](const M3<P> &a, const M3<P> &b) {      // Re Tr(a b^+), summed in FP64
+            double tr = 0.0;
+#pragma unroll
+            for (int i = 0; i < 3; i++)
+#pragma unroll
+                for (int j = 0; j < 3; j++) {
+                    tr = fma((double)a.m[i][j].re, (double)b.m[i][j].re, tr);
+                    tr = fma((double)a.m[i][j].im, (double)b.m[i][j].im, tr);
+                }
+            return tr;
+        };
 #pragma unroll 1
         for (int t0 = 0; t0 < nt; t0++) {
-            put((t0 + Tmax) % slots, line((t0 + Tmax) % nt));
+            put((t0 + Tmax) % slots, line((t0 + Tmax) % nt));   // the slot of t0 - 1
             Crd cx = c0, cy = cy0;
             cx.t = t0;
             cy.t = t0;
-            M3<P> mx = load_as<NC, Real, P>(U, G, cx, 3, params, twist);
+            M3<P> y = hmul(get(t0 % slots), load_as<NC, Real, P>(U, G, cx, 3, params, twist));
             M3<P> my = load_as<NC, Real, P>(U, G, cy, 3, params, twist);
 #pragma unroll 1
             for (int T = 1; T <= Tmax; T++) {
                 if (T > 1) {
                     cx = step_plus(G, cx, 3);
-                    mx = mulf(mx, load_as<NC, Real, P>(U, G, cx, 3, params, twist));
+                    y = mulf(y, load_as<NC, Real, P>(U, G, cx, 3, params, twist));
                     cy = step_plus(G, cy, 3);
                     my = mulf(my, load_as<NC, Real, P>(U, G, cy, 3, params, twist));
                 }
-                wsum[(T - 1) * nb + tid] += retr4(mx, get((t0 + T) % slots), my, get(t0 % slots));
+                wsum[(T - 1) * nb + tid] += retr_h(mulf(y, get((t0 + T) % slots)), my);
             }
         }
     }
