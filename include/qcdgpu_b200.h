@@ -34,6 +34,7 @@ extern "C" {
 #define QG_ERR_NOMEM      -4
 #define QG_ERR_IO         -5
 #define QG_ERR_UNSUPPORTED -6
+#define QG_ERR_NUMERIC    -7   /* the field left SU(N) or is not finite (qg_field_check) */
 
 /* start types: the reference's INTS key (0=hot, 1=cold, 2=gid),
  * SU(N)/suncl/suncl.cpp:725-730; QG_START_HAAR is new (Haar-distributed). */
@@ -164,6 +165,11 @@ int qg_set_shapes(qg_ctx *ctx, int heatbath_shape, int overrelax_shape);
 int qg_get_shapes(qg_ctx *ctx, int *heatbath_shape, int *overrelax_shape);
 /* lattice_GramSchmidt kernel (suncl.cl:350-396); fp64 != 0 computes in FP64 */
 int qg_reunitarize(qg_ctx *ctx, int fp64);
+/* new: count the links whose stored rows are not finite, not of unit norm
+ * or not orthogonal to within tol (one pass over the field, synchronous);
+ * qg_run checks its final configuration this way (tol 1e-3 for FP32 links,
+ * 1e-9 for FP64) and returns QG_ERR_NUMERIC if any link fails.           */
+int qg_field_check(qg_ctx *ctx, double tol, uint64_t *bad_links);
 /* x-slabs (the BIGLAT decomposition, suncl.cpp:4004-4062, as x-slices of
  * one lattice): a context created with size[0] = w + 2 becomes slab
  * [x0, x0 + w) of a lattice with n1_global x-slices; its slices 0 and w+1

@@ -32,7 +32,7 @@ EXPORTED_SYMBOLS = (
     "qg_default_config", "qg_create", "qg_destroy", "qg_last_error", "qg_get_info", "qg_sync",
     "qg_prng_seed", "qg_prng_produce", "qg_prns_upload", "qg_prns_download", "qg_init_links",
     "qg_set_prng_lookahead", "qg_set_slab", "qg_slab_halo", "qg_slab_halo_bytes", "qg_slab_halo2",
-    "qg_slab_phase",
+    "qg_slab_phase", "qg_field_check",
     "qg_phase", "qg_sweep", "qg_reunitarize", "qg_measure", "qg_measure_wilson",
     "qg_links_upload", "qg_links_download", "qg_set_phase_counter", "qg_glibc_seeds", "qg_set_params", "qg_get_stream",
     "qg_default_run_options", "qg_parse_init_file", "qg_run", "qg_tune", "qg_plaquette_noalloc",
@@ -205,6 +205,7 @@ def load_library(path=LIB_PATH):
     lib.qg_slab_halo_bytes.argtypes = [vp, P(ctypes.c_uint64)]
     lib.qg_slab_halo2.argtypes = [vp, ctypes.c_int, ctypes.c_int, vp, vp, ctypes.c_int]
     lib.qg_slab_phase.argtypes = [vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int]
+    lib.qg_field_check.argtypes = [vp, ctypes.c_double, P(ctypes.c_uint64)]
     lib.qg_prns_upload.argtypes = [vp, vp, ctypes.c_uint64]
     lib.qg_prns_download.argtypes = [vp, vp, ctypes.c_uint64]
     lib.qg_init_links.argtypes = [vp, ctypes.c_int]
@@ -501,6 +502,15 @@ class Lattice:
         """Both sides of slab_halo in one kernel launch (device buffers)."""
         self._ck(self.lib.qg_slab_halo2(self.ctx, int(direction), int(parity), ctypes.c_void_p(ptr_lo),
                                         ctypes.c_void_p(ptr_hi), int(bool(to_buf))), "qg_slab_halo2")
+
+    def field_check(self, tol=None):
+        """number of links not finite or off SU(N) by more than tol (default
+        1e-3 for FP32 links, 1e-9 for FP64)"""
+        if tol is None:
+            tol = 1e-9 if self.cfg.precision else 1e-3
+        n = ctypes.c_uint64()
+        self._ck(self.lib.qg_field_check(self.ctx, float(tol), ctypes.byref(n)), "qg_field_check")
+        return n.value
 
     def slab_phase(self, parity, direction, kind, part):
         """qg_slab_phase: part 0 the boundary slices, part 1 the interior."""

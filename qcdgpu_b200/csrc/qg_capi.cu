@@ -65,6 +65,7 @@ struct qg_ctx {
     // are the global slices x0 .. x0+w-1, slices 0 and w+1 are halos
     bool slab = false;
     int slab_x0 = 0, slab_n1 = 0;
+    unsigned long long *d_bad = nullptr;   // qg_field_check counter
     cudaStream_t side = nullptr;
     cudaEvent_t ev_fork = nullptr, ev_join = nullptr, ev_phase[8] = {};
     // learned-proposal Metropolis (qg_net_*, qg_mh_*)
@@ -226,6 +227,7 @@ extern "C" int qg_destroy(qg_ctx *c)
     cudaFree(c->d_grad); cudaFree(c->d_gpart); cudaFree(c->d_mh_acc); cudaFree(c->d_mh_jump);
     cudaFree(c->d_wpart); cudaFree(c->d_wout);
     cudaFree(c->d_fpart); cudaFree(c->d_ppart); cudaFree(c->d_pout); cudaFree(c->d_sites);
+    cudaFree(c->d_bad);
     if (c->h_results) cudaFreeHost(c->h_results);
     if (c->h_params) cudaFreeHost(c->h_params);
     if (c->h_ring) cudaFreeHost(c->h_ring);
@@ -772,6 +774,22 @@ static int build_graph(qg_ctx *c, int which)
     e = cudaGraphInstantiate(&c->graph[which], g, 0);
     cudaGraphDestroy(g);
     if (e != cudaSuccess) return cuda_fail(c, e, "graph instantiate");
+    return QG_OK;
+}
+
+// links that are not finite or not in SU(N) to within tol (rows of unit
+// norm, orthogonal); synchronous
+extern "C" int qg_field_check(qg_ctx *c, double tol, uint64_t *bad_links)
+{
+    if (!c || !bad_links || !(tol > 0)) return QG_ERR_ARG;
+    if (!c->d_bad) QG_CK(cudaMalloc(&c->d_bad, sizeof(unsigned long long)), "field check counter");
+    QG_CK(cudaMemsetAsync(c->d_bad, 0, sizeof(unsigned long long), c->stream), "field check reset");
+    QG_CK(launch_field_check(c->G, c->links, c->cfg.group, c->cfg.precision, tol, c->d_bad, c->stream),
+          "field check kernel");
+    unsigned long long n = 0;
+    QG_CK(cudaMemcpyAsync(&n, c->d_bad, sizeof(n), cudaMemcpyDeviceToHost, c->stream), "field check read");
+    QG_CK(cudaStreamSynchronize(c->stream), "field check sync");
+    *bad_links = n;
     return QG_OK;
 }
 

@@ -262,6 +262,58 @@ cudaError_t launch_gramschmidt(const Geom &G, void *links, int group, int prec, 
     return cudaGetLastError();
 }
 
+// ------------------------------------------------------------ field check
+// links (thread = element of both parities, blockIdx.y = direction) whose
+// stored rows are not finite, not of unit norm or not orthogonal to within
+// tol: a counter the host reads (qg_field_check)
+template <int NC, typename Real>
+__global__ void k_field_check(Field<Real> U, Geom G, double tol, unsigned long long *bad)
+{
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int mu = blockIdx.y;
+    if (i >= 2 * G.cb) return;
+    const uint32_t h = (i < G.cb) ? i : i - G.cb;
+    if (h >= G.half) return;
+    bool ok;
+    if (NC == 3) {
+        const G3<Real> m = U.ld3(mu, i);
+        // row 1 = (uv1.x, uv1.y, uv1.z) + i (uv2.x, uv2.y, uv2.z); row 2 =
+        // (uv3.x + i uv3.z, uv3.y + i uv3.w, uv1.w + i uv2.w)
+        const double ar[3] = { m.uv1.x, m.uv1.y, m.uv1.z }, ai[3] = { m.uv2.x, m.uv2.y, m.uv2.z };
+        const double br[3] = { m.uv3.x, m.uv3.y, m.uv1.w }, bi[3] = { m.uv3.z, m.uv3.w, m.uv2.w };
+        double n1 = 0, n2 = 0, ore = 0, oim = 0;
+        for (int k = 0; k < 3; k++) {
+            n1 += ar[k] * ar[k] + ai[k] * ai[k];
+            n2 += br[k] * br[k] + bi[k] * bi[k];
+            ore += ar[k] * br[k] + ai[k] * bi[k];
+            oim += ai[k] * br[k] - ar[k] * bi[k];
+        }
+        ok = isfinite(n1) && isfinite(n2) && isfinite(ore) && isfinite(oim) && fabs(n1 - 1.0) <= tol &&
+             fabs(n2 - 1.0) <= tol && ore * ore + oim * oim <= tol * tol;
+    } else {
+        const R4<Real> q = U.ld2(mu, i);
+        const double n = (double)q.x * q.x + (double)q.y * q.y + (double)q.z * q.z + (double)q.w * q.w;
+        ok = isfinite(n) && fabs(n - 1.0) <= tol;
+    }
+    if (!ok) atomicAdd(bad, 1ull);
+}
+
+cudaError_t launch_field_check(const Geom &G, const void *links, int group, int prec, double tol,
+                               unsigned long long *bad, cudaStream_t s)
+{
+    const dim3 grid((2 * G.cb + 127) / 128, 4);
+    if (prec) {
+        Field<double> U{ (double4 *)links, G.pstride };
+        if (group == 3) k_field_check<3, double><<<grid, 128, 0, s>>>(U, G, tol, bad);
+        else k_field_check<2, double><<<grid, 128, 0, s>>>(U, G, tol, bad);
+    } else {
+        Field<float> U{ (float4 *)links, G.pstride };
+        if (group == 3) k_field_check<3, float><<<grid, 128, 0, s>>>(U, G, tol, bad);
+        else k_field_check<2, float><<<grid, 128, 0, s>>>(U, G, tol, bad);
+    }
+    return cudaGetLastError();
+}
+
 // ---------------------------------------------------------- layout convert
 template <typename V>
 __global__ void k_to_native(Geom G, const V *ref, V *nat, int planes, uint32_t rowsize)

@@ -630,6 +630,16 @@ extern "C" int qg_run(const qg_config *cfg_in, const qg_run_options *o_in, qg_ru
             if (!st.empty()) mean_var(st, sl.s, sl.s_var);
         }
     }
+    {   // the final configuration is finite and in SU(N) (a NaN or a broken
+        // link would otherwise only show as odd averages)
+        uint64_t bad = 0;
+        if ((rc = qg_field_check(ctx, cfg.precision ? 1e-9 : 1e-3, &bad))) return bail(rc);
+        if (bad) {
+            qg_destroy(ctx);
+            return host_fail(QG_ERR_NUMERIC, std::to_string(bad) + " links of the final configuration are not "
+                                             "finite or not in SU(N)");
+        }
+    }
     // LatticeCheckCPU: FP64 re-measurement of the final configuration
     if (o->verify) {
         std::vector<char> buf(info.ref_elems * (cfg.precision ? 8 : 4));

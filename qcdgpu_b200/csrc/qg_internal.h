@@ -86,6 +86,8 @@ struct SlabCopy {
     uint32_t words;        // 16-byte words per copy
 };
 cudaError_t launch_slab_copy(const SlabCopy &c, cudaStream_t s);
+cudaError_t launch_field_check(const Geom &G, const void *links, int group, int prec, double tol,
+                               unsigned long long *bad, cudaStream_t s);
 
 // RANLUX, reference layout: one generator per instance, seed table of 7
 // float4 per instance (SoA), output prns[s*instances + i]

@@ -578,3 +578,51 @@ def test_one_pass_measurements_equal_the_separate_ones(group, precision, twist):
     for a in range(3):
         assert np.array_equal(prof[a], L.polyakov_profile(a)), a
     L.close()
+
+
+# ------------------------------------------------------ write sets
+def _changed_links(before, after, c, planes_per_dir):
+    """gid x direction mask of links whose stored reals changed"""
+    P = 12 if c.group == 3 else 4
+    rows = before.size // (P * 4)
+    b = before.reshape(P, rows, 4)
+    a = after.reshape(P, rows, 4)
+    V = int(np.prod(list(c.n)))
+    out = np.zeros((V, 4), dtype=bool)
+    for mu in range(4):
+        planes = [mu + 4 * k for k in range(planes_per_dir)]
+        out[:, mu] = np.any(a[planes, :V, :] != b[planes, :V, :], axis=(0, 2))
+    return out
+
+
+def _parity(c):
+    n = list(c.n)
+    g = np.arange(int(np.prod(n)))
+    y = g % n[1]
+    z = (g // n[1]) % n[2]
+    t = (g // (n[1] * n[2])) % n[3]
+    x = g // (n[1] * n[2] * n[3])
+    return (x + y + z + t) & 1
+
+
+@pytest.mark.parametrize("group,precision,shape", [(3, 0, 0), (3, 0, 4), (3, 0, 5), (3, 1, 0), (2, 0, 1), (2, 1, 0)])
+def test_each_phase_writes_exactly_its_links(group, precision, shape):
+    """write-set disjointness: one (parity, direction) phase of either kind
+    changes the V/2 links of that parity and direction and nothing else"""
+    L, c = make_pair(group, (4, 6, 4, 6), precision, start=Q.START_HOT, prng=Q.PRNG_PHILOX,
+                     beta=5.8 if group == 3 else 2.3)
+    L.set_shapes(shape, shape)
+    L.seed(54)
+    L.init(Q.START_HOT)
+    par = _parity(c)
+    for kind in (Q.HEATBATH, Q.OVERRELAX):
+        for p in (0, 1):
+            for mu in range(4):
+                before = L.download()
+                L.phase(p, mu, kind)
+                ch = _changed_links(before, L.download(), c, 3 if group == 3 else 1)
+                want = np.zeros_like(ch)
+                want[:, mu] = par == p
+                assert not np.any(ch & ~want), (kind, p, mu)            # nothing outside the phase's links
+                assert ch[want].mean() > 0.99, (kind, p, mu)             # and (almost) all of them updated
+    L.close()

@@ -133,3 +133,51 @@ def test_run_fmunu_and_profiles(tmp_path, group, field):
     vals = rows[-1].split()
     assert len(vals) == 1 + 3 + 3 + 2 + 2 + 16
     assert np.allclose([float(v) for v in vals[-16:]], last, rtol=1e-12, atol=1e-15)
+
+
+@pytest.mark.parametrize("group,precision", [(3, 0), (3, 1), (2, 1)])
+def test_field_check_counts_broken_links(group, precision):
+    """qg_field_check: a hot field passes; one NaN or one stretched link is
+    counted once, and Gram-Schmidt does not hide a NaN"""
+    cfg = Q.default_config(group=group, size=(4, 4, 4, 6), precision=precision, start=Q.START_HOT,
+                           prng=Q.PRNG_PHILOX, beta=5.8, n_or=1)
+    L = Q.Lattice(cfg)
+    L.seed()
+    L.init(Q.START_HOT)
+    L.sweep(2)
+    assert L.field_check() == 0
+    good = L.download()
+    t = good.copy()
+    t[5] = np.nan                                    # plane 0 (direction x), site 1, one real
+    L.upload(t)
+    assert L.field_check() == 1
+    L.reunitarize(True)
+    assert L.field_check() == 1
+    t = good.copy()
+    P = 12 if group == 3 else 4
+    rows = t.size // (P * 4)
+    t.reshape(P, rows, 4)[2, 7, :] *= 1.01           # direction z at site 7: row norms off by ~2 %
+    L.upload(t)
+    assert L.field_check() == 1
+    L.close()
+
+
+def test_run_resumed_from_a_state_file_with_a_nan_link_reports_it(tmp_path):
+    """host-side fault injection: a .qcg whose link table carries one NaN,
+    resumed with INIT = 0, ends with QG_ERR_NUMERIC from the final field
+    check instead of returning averages"""
+    base = dict(group=3, size=(4, 4, 4, 4), precision=0, start=Q.START_COLD, prng=Q.PRNG_PHILOX, beta=5.9,
+                row_align=64, n_or=1, reunit_every=2)
+    good = str(tmp_path / "good.qcg")
+    Q.run(Q.default_config(**base), Q.default_run_options(iter=2, niter=1, nav=1, quiet=1, write_results=0,
+                                                          verify=0, save_state=1, state_out=good))
+    cfg, st, ser, table = Q.read_state_file(good)
+    table = table.copy()
+    table[40] = np.nan
+    bad = str(tmp_path / "bad.qcg")
+    st.iter = 4
+    Q.write_state_file(bad, cfg, st, table, ser)
+    with pytest.raises(Q.QGError) as e:
+        Q.run(Q.default_config(), Q.default_run_options(init=0, state_file=bad, quiet=1, write_results=0,
+                                                        verify=0, save_state=0))
+    assert "not finite or not in SU(N)" in str(e.value)

@@ -8,7 +8,7 @@ import numpy as np
 import pytest
 
 import qcdgpu_b200 as Q
-from qcdgpu_b200.slabs import DistSlab, SlabSet, _to_slab, split
+from qcdgpu_b200.slabs import DistSlab, SlabSet, _Slab, _to_slab, split
 
 pytestmark = pytest.mark.gpu
 
@@ -109,3 +109,39 @@ def test_dist_slab_on_one_rank_follows_the_whole_lattice():
         G.close()
     finally:
         dist.destroy_process_group()
+
+
+def test_a_slab_phase_writes_only_its_interior_links():
+    """write-set of one slab phase: the links of its direction and global
+    parity in slices 1..w, never the halo slices"""
+    cfg = Q.default_config(group=3, size=(8, 4, 4, 6), precision=0, start=Q.START_HOT, prng=Q.PRNG_PHILOX,
+                           beta=5.8, randseries=3)
+    G = Q.Lattice(cfg)
+    G.seed()
+    G.init(Q.START_HOT)
+    table = G.download()
+    w, x0 = 3, 5                                         # slices 5, 6, 7; halos 4 and 0
+    S = _Slab(cfg, w, x0)
+    S.L.seed()
+    S.L.upload(_to_slab(table, cfg, w, x0, S.cfg))
+    ns = 4 * 4 * 6
+    Vs = (w + 2) * ns
+    gl = np.arange(Vs)
+    y, z, t, xl = gl % 4, (gl // 4) % 4, (gl // 16) % 6, gl // ns
+    gpar = (xl + x0 - 1 + y + z + t) & 1                 # global parity of each slab site
+    for kind in (Q.HEATBATH, Q.OVERRELAX):
+        for p in (0, 1):
+            for mu in range(4):
+                before = S.L.download().reshape(12, -1, 4)
+                for part in (0, 1):
+                    S.L.slab_phase(p, mu, kind, part)
+                after = S.L.download().reshape(12, -1, 4)
+                for nu in range(4):
+                    planes = [nu + 4 * k for k in range(3)]
+                    ch = np.any(after[planes, :Vs, :] != before[planes, :Vs, :], axis=(0, 2))
+                    want = (gpar == p) & (xl >= 1) & (xl <= w) & (nu == mu)
+                    assert not np.any(ch & ~want), (kind, p, mu, nu)
+                    if nu == mu:
+                        assert ch[want].mean() > 0.99, (kind, p, mu)
+    S.close()
+    G.close()
