@@ -381,6 +381,7 @@ extern "C" int qg_glibc_seeds(uint32_t series, int n, uint32_t *seeds)
 
 extern "C" int qg_prng_produce(qg_ctx *c)
 {
+    NvtxRange nvtx_range("qg_prng_produce");
     if (!c) return QG_ERR_ARG;
     if (c->cfg.prng != QG_PRNG_RANLUX) return fail(c, QG_ERR_STATE, "qg_prng_produce needs the RANLUX stream");
     if (!c->seeded) return fail(c, QG_ERR_STATE, "PRNG not seeded (qg_prng_seed)");
@@ -472,6 +473,7 @@ extern "C" int qg_prns_download(qg_ctx *c, float *h, uint64_t nq)
 
 extern "C" int qg_init_links(qg_ctx *c, int start)
 {
+    NvtxRange nvtx_range("qg_init_links");
     if (!c) return QG_ERR_ARG;
     const qg_config &f = c->cfg;
     if (c->slab && start != QG_START_COLD)
@@ -557,6 +559,7 @@ static bool needs_seed(const qg_ctx *c, int kind)
 
 extern "C" int qg_phase(qg_ctx *c, int parity, int dir, int kind)
 {
+    NvtxRange nvtx_range("qg_phase");
     if (!c) return QG_ERR_ARG;
     if ((parity != 0 && parity != 1) || dir < 0 || dir > 3) return fail(c, QG_ERR_ARG, "bad parity/direction");
     if (kind != QG_UPDATE_HEATBATH && kind != QG_UPDATE_OVERRELAX) return fail(c, QG_ERR_ARG, "bad update kind");
@@ -577,6 +580,7 @@ extern "C" int qg_phase(qg_ctx *c, int parity, int dir, int kind)
 // so part 0 then part 1 is qg_phase bit for bit.
 extern "C" int qg_slab_phase(qg_ctx *c, int parity, int dir, int kind, int part)
 {
+    NvtxRange nvtx_range("qg_slab_phase");
     if (!c) return QG_ERR_ARG;
     if (!c->slab) return fail(c, QG_ERR_STATE, "not a slab (qg_set_slab)");
     if ((parity != 0 && parity != 1) || dir < 0 || dir > 3) return fail(c, QG_ERR_ARG, "bad parity/direction");
@@ -613,6 +617,7 @@ extern "C" int qg_slab_phase(qg_ctx *c, int parity, int dir, int kind, int part)
 // the fastest per kind
 extern "C" int qg_tune(qg_ctx *c, int reps, float *times_ms)
 {
+    NvtxRange nvtx_range("qg_tune");
     if (!c) return QG_ERR_ARG;
     if (reps < 1) reps = 4;
     if (needs_seed(c, QG_UPDATE_HEATBATH)) return fail(c, QG_ERR_STATE, "tuning needs a seeded PRNG (qg_prng_seed)");
@@ -679,6 +684,7 @@ extern "C" int qg_get_shapes(qg_ctx *c, int *heatbath_shape, int *overrelax_shap
 
 extern "C" int qg_reunitarize(qg_ctx *c, int fp64)
 {
+    NvtxRange nvtx_range("qg_reunitarize");
     if (!c) return QG_ERR_ARG;
     QG_CK(launch_gramschmidt(c->G, c->links, c->cfg.group, c->cfg.precision, fp64, c->stream), "gramschmidt");
     return QG_OK;
@@ -781,6 +787,7 @@ static int build_graph(qg_ctx *c, int which)
 // norm, orthogonal); synchronous
 extern "C" int qg_field_check(qg_ctx *c, double tol, uint64_t *bad_links)
 {
+    NvtxRange nvtx_range("qg_field_check");
     if (!c || !bad_links || !(tol > 0)) return QG_ERR_ARG;
     if (!c->d_bad) QG_CK(cudaMalloc(&c->d_bad, sizeof(unsigned long long)), "field check counter");
     QG_CK(cudaMemsetAsync(c->d_bad, 0, sizeof(unsigned long long), c->stream), "field check reset");
@@ -856,6 +863,7 @@ extern "C" int qg_slab_halo(qg_ctx *c, int dir, int parity, int side, void *buf,
 // and buf_hi into halo x = w+1 (buffers in device memory, 16-byte aligned)
 extern "C" int qg_slab_halo2(qg_ctx *c, int dir, int parity, void *buf_lo, void *buf_hi, int to_buf)
 {
+    NvtxRange nvtx_range("qg_slab_halo2");
     if (!c || !buf_lo || !buf_hi) return QG_ERR_ARG;
     if (!c->slab) return fail(c, QG_ERR_STATE, "not a slab (qg_set_slab)");
     if (dir < 0 || dir > 3 || (parity != 0 && parity != 1)) return fail(c, QG_ERR_ARG, "bad direction / parity");
@@ -892,6 +900,7 @@ extern "C" int qg_slab_halo2(qg_ctx *c, int dir, int parity, void *buf_lo, void 
 
 extern "C" int qg_sweep(qg_ctx *c, int nsweeps)
 {
+    NvtxRange nvtx_range("qg_sweep");
     if (!c) return QG_ERR_ARG;
     if (c->slab) return fail(c, QG_ERR_STATE, "a slab sweeps phase by phase with halo exchanges (qcdgpu_b200.slabs)");
     if (nsweeps < 0) return fail(c, QG_ERR_ARG, "negative sweep count");
@@ -1020,6 +1029,7 @@ extern "C" int qg_mh_phase(qg_ctx *c, int parity, int dir, int nhit)
 // qg_sweep (the sweep counter is shared)
 extern "C" int qg_mh_sweep(qg_ctx *c, int nsweeps, int nhit)
 {
+    NvtxRange nvtx_range("qg_mh_sweep");
     if (!c) return QG_ERR_ARG;
     if (nsweeps < 0 || nhit < 1) return fail(c, QG_ERR_ARG, "bad sweep arguments");
     int r = mh_ready(c);
@@ -1092,6 +1102,7 @@ extern "C" int qg_net_grad(qg_ctx *c, int parity, int dir, float *grad, double *
 // order; stats: the mean over the steps of (loss, ESJD, acceptance, links)
 extern "C" int qg_net_train(qg_ctx *c, int steps, double lr, double *stats)
 {
+    NvtxRange nvtx_range("qg_net_train");
     if (!c) return QG_ERR_ARG;
     if (steps < 0 || !(lr > 0.0)) return fail(c, QG_ERR_ARG, "bad training arguments");
     int r = mh_ready(c);
@@ -1147,6 +1158,7 @@ extern "C" int qg_measure_wilson(qg_ctx *c, int R, int T, double *out)
 
 extern "C" int qg_measure_wilson_all(qg_ctx *c, int Rmax, int Tmax, int fp64_products, double *out)
 {
+    NvtxRange nvtx_range("qg_measure_wilson_all");
     if (!c || !out) return QG_ERR_ARG;
     const int ns = std::min(c->G.n[0], std::min(c->G.n[1], c->G.n[2]));
     if (Rmax < 1 || Tmax < 1 || Rmax > 16 || Tmax > 16 || Rmax > ns || Tmax > c->G.n[3])
@@ -1171,6 +1183,7 @@ extern "C" int qg_measure_wilson_all(qg_ctx *c, int Rmax, int Tmax, int fp64_pro
 
 extern "C" int qg_measure_fmunu(qg_ctx *c, int field, int index1, int index2, double *out)
 {
+    NvtxRange nvtx_range("qg_measure_fmunu");
     if (!c || !out) return QG_ERR_ARG;
     const qg_config &f = c->cfg;
     const int na = f.group == 3 ? 8 : 3;
@@ -1285,6 +1298,7 @@ static int measure_launch(qg_ctx *c, int what, int &ncomp, int &first)
 
 extern "C" int qg_measure_enqueue(qg_ctx *c, int what, uint64_t *ticket)
 {
+    NvtxRange nvtx_range("qg_measure_enqueue");
     if (!c || !ticket) return QG_ERR_ARG;
     const uint64_t t = c->ticket_next;
     const int slot = (int)(t % QG_MEASURE_SLOTS);

@@ -7,6 +7,7 @@
 #include <string>
 
 #include "../../include/qcdgpu_b200.h"
+#include <nvtx3/nvToolsExt.h>
 #include "qg_lattice.cuh"
 
 namespace qg {
@@ -86,6 +87,15 @@ struct SlabCopy {
     uint32_t words;        // 16-byte words per copy
 };
 cudaError_t launch_slab_copy(const SlabCopy &c, cudaStream_t s);
+
+// a named NVTX range for the scope (shows the C-ABI calls on a profiler's
+// timeline; nothing happens without a tool attached)
+struct NvtxRange {
+    explicit NvtxRange(const char *name) { nvtxRangePushA(name); }
+    ~NvtxRange() { nvtxRangePop(); }
+    NvtxRange(const NvtxRange &) = delete;
+    NvtxRange &operator=(const NvtxRange &) = delete;
+};
 cudaError_t launch_field_check(const Geom &G, const void *links, int group, int prec, double tol,
                                unsigned long long *bad, cudaStream_t s);
 
