@@ -170,6 +170,18 @@ int qg_reunitarize(qg_ctx *ctx, int fp64);
  * qg_run checks its final configuration this way (tol 1e-3 for FP32 links,
  * 1e-9 for FP64) and returns QG_ERR_NUMERIC if any link fails.           */
 int qg_field_check(qg_ctx *ctx, double tol, uint64_t *bad_links);
+/* per-kernel device times (the reference's GPU_debug.profiling table,
+ * clinterface.cpp:1254-1266,1626-1668): `reps` launches of each class, each
+ * between two CUDA events, on the live field (restored; no PRN counter
+ * moves); mean and standard deviation in ms per launch, indexed by class */
+#define QG_KERNEL_HEATBATH   0   /* one heatbath phase                          */
+#define QG_KERNEL_OVERRELAX  1   /* one overrelaxation phase                    */
+#define QG_KERNEL_REUNIT     2   /* global Gram-Schmidt                         */
+#define QG_KERNEL_PLAQUETTE  3   /* plaquette / action measurement + reduction  */
+#define QG_KERNEL_POLYAKOV   4   /* Polyakov-loop measurement + reduction       */
+#define QG_KERNEL_WILSON     5   /* one WILSONR x WILSONT loop + reduction      */
+#define QG_KERNEL_CLASSES    6
+int qg_profile_kernels(qg_ctx *ctx, int reps, double *mean_ms, double *sigma_ms);
 /* x-slabs (the BIGLAT decomposition, suncl.cpp:4004-4062, as x-slices of
  * one lattice): a context created with size[0] = w + 2 becomes slab
  * [x0, x0 + w) of a lattice with n1_global x-slices; its slices 0 and w+1
@@ -444,6 +456,9 @@ typedef struct qg_run_options {
     int tune_shapes;       /* 1 (default): time the phase-kernel launch shapes on this */
                            /* lattice before the run (qg_tune; all shapes give the     */
                            /* same chain, so the results do not change)               */
+    int profile;           /* PROFILE: per-kernel time table after the run            */
+                           /* (qg_profile_kernels; printed unless quiet, and in        */
+                           /* qg_run_result.kernel_ms)                                 */
 } qg_run_options;
 
 typedef struct qg_run_result {
@@ -471,6 +486,9 @@ typedef struct qg_run_result {
     double fmunu_variance[QG_FMUNU_COLS];
     double fmunu_gpu_last[QG_FMUNU_COLS];
     double fmunu_cpu_last[QG_FMUNU_COLS];
+    /* opts.profile: ms per launch of each QG_KERNEL_* class, mean and sigma */
+    double kernel_ms[QG_KERNEL_CLASSES];
+    double kernel_ms_sigma[QG_KERNEL_CLASSES];
 } qg_run_result;
 
 /* defaults of the reference main() (QCDGPU.cpp:183-205) */
@@ -481,7 +499,7 @@ int qg_default_run_options(qg_run_options *opts);
  * GETWILSON GETRETRACE PL_LEVEL WILSONR WILSONT FMUNU F0MU TURNOFFFMUNU
  * FMUNU1 FMUNU2 FMUNU4 FMUNU5 FMUNU6 FMUNU7 (reference) and PRECISION
  * NHITPAR NOR REUNIT_EVERY REUNIT_FP64 PRNG_INSTANCES ROW_ALIGN INIT
- * STATEFILE SAVESTATE SAVEEVERY STATEOUT ACTIONS_DIFF TUNE (this library; the
+ * STATEFILE SAVESTATE SAVEEVERY STATEOUT ACTIONS_DIFF TUNE PROFILE (this library; the
  * reference sets INIT, the state file name and get_actions_diff in main());
  * PLATFORM DEVICE FINISHPATH TURNOFFWAITING REBUILDBINARY are accepted and
  * ignored.  Unknown generators are an error.                               */

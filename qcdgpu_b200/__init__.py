@@ -26,13 +26,16 @@ FMUNU_COLS = 16                     # QG_FMUNU_COLS
 MEASURE_SLOTS = 64                  # QG_MEASURE_SLOTS
 TUNE_SHAPES = 6                     # QG_TUNE_SHAPES
 BATCH_SHAPES = 5                    # QG_BATCH_SHAPES
+KERNEL_CLASSES = 6                  # QG_KERNEL_CLASSES
+KERNEL_NAMES = ("heatbath phase", "overrelaxation phase", "Gram-Schmidt", "plaquette + action", "Polyakov loop",
+                "Wilson loop")
 NET_FEATURES, NET_HIDDEN, NET_PARAMS = 8, 32, 1377   # QG_NET_*
 
 EXPORTED_SYMBOLS = (
     "qg_default_config", "qg_create", "qg_destroy", "qg_last_error", "qg_get_info", "qg_sync",
     "qg_prng_seed", "qg_prng_produce", "qg_prns_upload", "qg_prns_download", "qg_init_links",
     "qg_set_prng_lookahead", "qg_set_slab", "qg_slab_halo", "qg_slab_halo_bytes", "qg_slab_halo2",
-    "qg_slab_phase", "qg_field_check",
+    "qg_slab_phase", "qg_field_check", "qg_profile_kernels",
     "qg_phase", "qg_sweep", "qg_reunitarize", "qg_measure", "qg_measure_wilson",
     "qg_links_upload", "qg_links_download", "qg_set_phase_counter", "qg_glibc_seeds", "qg_set_params", "qg_get_stream",
     "qg_default_run_options", "qg_parse_init_file", "qg_run", "qg_tune", "qg_plaquette_noalloc",
@@ -114,6 +117,7 @@ class RunOptions(ctypes.Structure):
         ("fmunu_index2", ctypes.c_int),
         ("get_actions_diff", ctypes.c_int),
         ("tune_shapes", ctypes.c_int),
+        ("profile", ctypes.c_int),
     ]
 
 
@@ -135,6 +139,8 @@ class RunResult(ctypes.Structure):
         ("fmunu_variance", ctypes.c_double * FMUNU_COLS),
         ("fmunu_gpu_last", ctypes.c_double * FMUNU_COLS),
         ("fmunu_cpu_last", ctypes.c_double * FMUNU_COLS),
+        ("kernel_ms", ctypes.c_double * KERNEL_CLASSES),
+        ("kernel_ms_sigma", ctypes.c_double * KERNEL_CLASSES),
     ]
 
 
@@ -206,6 +212,7 @@ def load_library(path=LIB_PATH):
     lib.qg_slab_halo2.argtypes = [vp, ctypes.c_int, ctypes.c_int, vp, vp, ctypes.c_int]
     lib.qg_slab_phase.argtypes = [vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int]
     lib.qg_field_check.argtypes = [vp, ctypes.c_double, P(ctypes.c_uint64)]
+    lib.qg_profile_kernels.argtypes = [vp, ctypes.c_int, P(ctypes.c_double), P(ctypes.c_double)]
     lib.qg_prns_upload.argtypes = [vp, vp, ctypes.c_uint64]
     lib.qg_prns_download.argtypes = [vp, vp, ctypes.c_uint64]
     lib.qg_init_links.argtypes = [vp, ctypes.c_int]
@@ -502,6 +509,13 @@ class Lattice:
         """Both sides of slab_halo in one kernel launch (device buffers)."""
         self._ck(self.lib.qg_slab_halo2(self.ctx, int(direction), int(parity), ctypes.c_void_p(ptr_lo),
                                         ctypes.c_void_p(ptr_hi), int(bool(to_buf))), "qg_slab_halo2")
+
+    def profile_kernels(self, reps=20):
+        """{kernel class: (mean ms, sigma ms) per launch} on the live field
+        (restored afterwards)"""
+        m, sd = (ctypes.c_double * KERNEL_CLASSES)(), (ctypes.c_double * KERNEL_CLASSES)()
+        self._ck(self.lib.qg_profile_kernels(self.ctx, int(reps), m, sd), "qg_profile_kernels")
+        return {KERNEL_NAMES[k]: (m[k], sd[k]) for k in range(KERNEL_CLASSES)}
 
     def field_check(self, tol=None):
         """number of links not finite or off SU(N) by more than tol (default

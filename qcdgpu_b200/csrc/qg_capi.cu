@@ -1,5 +1,6 @@
 // qg_capi.cu -- the C-ABI of include/qcdgpu_b200.h: context, buffers,
 // PRN cadence, sweep graphs and measurements on one CUDA stream.
+#include <math.h>
 #include <stdlib.h>
 #include <string.h>
 
@@ -609,6 +610,70 @@ extern "C" int qg_slab_phase(qg_ctx *c, int parity, int dir, int kind, int part)
         QG_CK(launch_add_u64(c->d_phase, 1, c->stream), "phase counter");
         c->phase_counter++;
     }
+    return QG_OK;
+}
+
+// per-launch device time of each kernel class (the reference's per-kernel
+// profiling table, clinterface.cpp:1254-1266,1626-1668): reps launches of
+// each, every one between two CUDA events, on the live field (restored
+// afterwards; no PRN counter moves)
+extern "C" int qg_profile_kernels(qg_ctx *c, int reps, double *mean_ms, double *sigma_ms)
+{
+    NvtxRange nvtx_range("qg_profile_kernels");
+    if (!c || !mean_ms || !sigma_ms) return QG_ERR_ARG;
+    if (reps < 2) reps = 2;
+    if (needs_seed(c, QG_UPDATE_HEATBATH)) return fail(c, QG_ERR_STATE, "profiling needs a seeded PRNG (qg_prng_seed)");
+    const qg_config &f = c->cfg;
+    const int tw = twist_of(f);
+    void *backup = nullptr;
+    QG_CK(cudaMallocAsync(&backup, c->link_bytes, c->stream), "profile backup");
+    cudaError_t e = cudaMemcpyAsync(backup, c->links, c->link_bytes, cudaMemcpyDeviceToDevice, c->stream);
+    std::vector<cudaEvent_t> ev(2 * (size_t)reps);
+    for (auto &x : ev) cudaEventCreate(&x);
+    for (int k = 0; k < QG_KERNEL_CLASSES && e == cudaSuccess; k++) {
+        for (int r = -1; r < reps && e == cudaSuccess; r++) {     // one untimed launch first
+            if (r >= 0) cudaEventRecord(ev[2 * r], c->stream);
+            const int par = (r + 1) & 1, dir = ((r + 1) >> 1) & 3;
+            switch (k) {
+            case QG_KERNEL_HEATBATH: e = launch_phase(c, phase_args(c, par, dir, QG_UPDATE_HEATBATH, 0)); break;
+            case QG_KERNEL_OVERRELAX: e = launch_phase(c, phase_args(c, par, dir, QG_UPDATE_OVERRELAX, 0)); break;
+            case QG_KERNEL_REUNIT:
+                e = launch_gramschmidt(c->G, c->links, f.group, f.precision, f.reunit_fp64, c->stream);
+                break;
+            case QG_KERNEL_PLAQUETTE:
+                e = launch_plaquette(c->G, c->links, f.group, f.precision, c->d_params, tw, c->partials, c->d_results,
+                                     c->stream);
+                break;
+            case QG_KERNEL_POLYAKOV:
+                e = launch_polyakov(c->G, c->links, f.group, f.precision, c->partials, c->d_results, c->stream);
+                break;
+            default:
+                e = launch_wilson(c->G, c->links, f.group, f.precision, f.wilson_r, f.wilson_t, c->d_params, tw,
+                                  c->partials, c->d_results, c->stream);
+                break;
+            }
+            if (r >= 0) cudaEventRecord(ev[2 * r + 1], c->stream);
+        }
+        if (e != cudaSuccess) break;
+        cudaEventSynchronize(ev[2 * reps - 1]);
+        double m = 0, m2 = 0;
+        for (int r = 0; r < reps; r++) {
+            float ms = 0;
+            cudaEventElapsedTime(&ms, ev[2 * r], ev[2 * r + 1]);
+            m += ms;
+            m2 += (double)ms * ms;
+        }
+        m /= reps;
+        mean_ms[k] = m;
+        sigma_ms[k] = sqrt(fmax(0.0, m2 / reps - m * m) * reps / (reps - 1));
+    }
+    cudaError_t e2 = cudaMemcpyAsync(c->links, backup, c->link_bytes, cudaMemcpyDeviceToDevice, c->stream);
+    cudaFreeAsync(backup, c->stream);
+    cudaError_t e3 = cudaStreamSynchronize(c->stream);
+    for (auto &x : ev) cudaEventDestroy(x);
+    if (e != cudaSuccess) return cuda_fail(c, e, "profile launch");
+    if (e2 != cudaSuccess) return cuda_fail(c, e2, "profile restore");
+    if (e3 != cudaSuccess) return cuda_fail(c, e3, "profile sync");
     return QG_OK;
 }
 

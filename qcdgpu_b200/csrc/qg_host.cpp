@@ -267,6 +267,7 @@ extern "C" int qg_default_run_options(qg_run_options *o)
     o->verify = 1;
     o->write_results = 1;
     o->tune_shapes = 1;
+    o->profile = 0;
     o->init = 1;
     snprintf(o->prefix, sizeof(o->prefix), "su3-");
     return QG_OK;
@@ -351,6 +352,7 @@ extern "C" int qg_parse_init_file(const char *path, qg_config *cfg, qg_run_optio
         else if (key == "FMUNU7") o->fmunu_index2 = 7;
         else if (key == "ACTIONS_DIFF") o->get_actions_diff = (int)iv;
         else if (key == "TUNE") o->tune_shapes = (int)iv;
+        else if (key == "PROFILE") o->profile = (int)iv;
         else if (key == "PLATFORM" || key == "DEVICE" || key == "FINISHPATH" || key == "TURNOFFWAITING" ||
                  key == "REBUILDBINARY" || key.rfind("FMUNU", 0) == 0 || key == "N1") {
             /* device selection, dispatcher handshake and OpenCL binaries have
@@ -628,6 +630,17 @@ extern "C" int qg_run(const qg_config *cfg_in, const qg_run_options *o_in, qg_ru
             Slice &sl = prof[axis][k];
             if (!re.empty()) { mean_var(re, sl.pl, sl.pl_var); mean_var(im, sl.pl_im, sl.pl_im_var); }
             if (!st.empty()) mean_var(st, sl.s, sl.s_var);
+        }
+    }
+    if (o->profile) {   // the per-kernel table (GPU_debug.profiling, print_time_detailed)
+        if ((rc = qg_profile_kernels(ctx, 20, res->kernel_ms, res->kernel_ms_sigma))) return bail(rc);
+        if (!o->quiet) {
+            static const char *names[QG_KERNEL_CLASSES] = { "heatbath phase", "overrelaxation phase",
+                                                            "Gram-Schmidt", "plaquette + action",
+                                                            "Polyakov loop", "Wilson loop" };
+            printf("\n kernel                   ms per launch (20 launches)\n");
+            for (int k = 0; k < QG_KERNEL_CLASSES; k++)
+                printf(" %-22s %10.5f +- %.5f\n", names[k], res->kernel_ms[k], res->kernel_ms_sigma[k]);
         }
     }
     {   // the final configuration is finite and in SU(N) (a NaN or a broken

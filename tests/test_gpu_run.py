@@ -181,3 +181,31 @@ def test_run_resumed_from_a_state_file_with_a_nan_link_reports_it(tmp_path):
         Q.run(Q.default_config(), Q.default_run_options(init=0, state_file=bad, quiet=1, write_results=0,
                                                         verify=0, save_state=0))
     assert "not finite or not in SU(N)" in str(e.value)
+
+
+def test_profile_table_leaves_the_run_unchanged(tmp_path):
+    """PROFILE = 1: every kernel class gets a time per launch, and the run's
+    final table and series equal those of the same run without it (the
+    timing launches work on a copy that is restored)"""
+    base = dict(group=3, size=(4, 4, 4, 8), precision=0, start=Q.START_HOT, prng=Q.PRNG_PHILOX, beta=5.9,
+                row_align=64, n_or=1, reunit_every=2, wilson_r=2, wilson_t=2)
+    outs = []
+    for profile in (0, 1):
+        path = str(tmp_path / ("p%d.qcg" % profile))
+        res = Q.run(Q.default_config(**base), Q.default_run_options(iter=3, niter=2, nav=2, get_wilson=1, quiet=1,
+                                                                    write_results=0, verify=0, save_state=1,
+                                                                    state_out=path, profile=profile))
+        outs.append((res, Q.read_state_file(path)))
+    assert all(x == 0.0 for x in outs[0][0].kernel_ms)
+    assert all(x > 0.0 for x in outs[1][0].kernel_ms)
+    assert np.array_equal(outs[0][1][3], outs[1][1][3])
+    for k in outs[0][1][2]:
+        assert np.array_equal(outs[0][1][2][k], outs[1][1][2][k]), k
+    L = Q.Lattice(Q.default_config(**base))
+    L.seed()
+    L.init(Q.START_HOT)
+    before = L.download()
+    t = L.profile_kernels(reps=3)
+    assert set(t) == set(Q.KERNEL_NAMES) and all(m > 0 for m, _ in t.values())
+    assert np.array_equal(L.download(), before) and L.info().phase_counter == 0
+    L.close()

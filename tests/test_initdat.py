@@ -71,3 +71,6 @@ def test_fmunu_and_profile_keys(tmp_path):
     assert d.tune_shapes == 1
     cfg, o = Q.parse_init_file(write(tmp_path, "TUNE = 0\n"))
     assert o.tune_shapes == 0
+    assert d.profile == 0
+    cfg, o = Q.parse_init_file(write(tmp_path, "PROFILE = 1\n"))
+    assert o.profile == 1
