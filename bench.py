@@ -322,7 +322,9 @@ def run_ours(args):
         "config": {"workload": "SU(3) %d^4 beta=%.1f, FP32 12-real links, 1 HB + %d OR per sweep, FP64 reunit every %d"
                                % (args.size, BETA, N_OR, REUNIT_EVERY),
                    "global_batch": world, "lattice": [args.size] * 4, "prng": args.prng,
-                   "parallelism": "replicas x%d" % world, "l2": "field 201 MB > 126 MB L2, no flush"},
+                   "parallelism": "replicas x%d" % world,
+                   "l2": ("field %.0f MB > 126 MB L2, no flush" if 4 * V * LINK_BYTES > 126e6 else
+                          "field %.0f MB fits the 126 MB L2 (small-lattice run)") % (4 * V * LINK_BYTES / 1e6)},
         "roofline": {"bound": "hbm", "kernel": dom + " phase", "achieved": achieved, "peak": peak,
                      "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
                      "algorithmic_bytes_per_launch": alg_bytes, "ms_per_launch": dom_ms,

@@ -1,0 +1,46 @@
+"""bench.py's output line: the keys the benchmark contract names, on a small
+lattice -- the reference arm on the host (CPU), our arm on the GPU."""
+import json
+import os
+import subprocess
+import sys
+
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def _bench(*args):
+    out = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py")] + list(args), cwd=ROOT,
+                         capture_output=True, text=True, timeout=600)
+    assert out.returncode == 0, out.stderr[-2000:]
+    return json.loads(out.stdout.strip().splitlines()[-1])
+
+
+def test_reference_arm_line():
+    d = _bench("--impl", "reference", "--size", "8", "--steps", "2", "--warmup", "1")
+    assert d["impl"] == "reference"
+    if "unavailable" in d:
+        pytest.skip(d["unavailable"])
+    assert d["value"] > 0 and d["unit"] == "link_updates/s" and d["higher_is_better"] is True
+    assert d["cpu_baseline"]["kind"] == "reference" and d["cpu_baseline"]["cores"] >= 1
+    assert d["e2e"] == {"value": d["value"], "unit": d["unit"], "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}
+    assert d["config"]["lattice"] == [8, 8, 8, 8]
+
+
+@pytest.mark.gpu
+def test_our_arm_line():
+    d = _bench("--size", "16", "--steps", "5", "--warmup", "3", "--no-cpu-baseline")
+    for k in ("metric", "value", "unit", "n_gpus", "steps", "warmup", "ms_per_step", "higher_is_better", "scaling",
+              "vs_baseline", "dtype", "data", "config", "roofline", "e2e", "gpu_launches", "clocks"):
+        assert k in d, k
+    assert d["n_gpus"] == 1 and d["steps"] == 5 and d["warmup"] == 3 and d["value"] > 0
+    assert d["value"] == pytest.approx(4 * 16 ** 4 * 5 / (d["ms_per_step"] * 1e-3), rel=1e-9)
+    r = d["roofline"]
+    assert r["bound"] == "hbm" and r["unit"] == "GB/s" and r["achieved"] > 0 and r["peak"] > 0
+    assert r["frac"] == pytest.approx(r["achieved"] / r["peak"])
+    e = d["e2e"]
+    assert e["value"] > 0 and e["h2d_bytes_per_step"] > 0 and e["d2h_bytes_per_step"] > 0
+    assert d["gpu_launches"] == 5 * (8 + 8 * 4 + 1) + sum(1 for n in range(6, 11) if n % 10 == 0)
+    assert {"sm_mhz", "sm_max_mhz", "reasons"} <= set(d["clocks"])
+    assert "workload" in d["config"] and "fits the 126 MB L2" in d["config"]["l2"]
