@@ -263,7 +263,9 @@ template <typename Real> struct PrnOf<Real, 2> {
 // The update of link U_mu(x) for thread t of a (parity, mu) phase: the
 // body of update_{even,odd}_{X,Y,Z,T}.  STAGED: staple links through
 // shared memory (staple3_staged; SU(3) FP32 links).
-template <int NC, typename Real, int PMODE, bool OR, int mu, bool STAGED>
+// TW: twisted boundaries possible (the launch has A.twist set); without it
+// every twist test folds away at compile time (4 % of the phase's time)
+template <int NC, typename Real, int PMODE, bool OR, int mu, bool STAGED, bool TW = false>
 __device__ __forceinline__ void phase_site(const Field<Real> &U, const Geom &G, const PhaseArgs &A, uint32_t t)
 {
     const int p = A.parity;
@@ -273,7 +275,8 @@ __device__ __forceinline__ void phase_site(const Field<Real> &U, const Geom &G, 
     const uint32_t e0 = (uint32_t)p * G.cb + t;
     const Nbr nb = neighbours(G, c);
     Twist<Real> tw;
-    tw.on = A.twist; tw.xlast = G.n[0] - 1;
+    tw.on = TW ? A.twist : 0;
+    tw.xlast = G.n[0] - 1;
     tw.phi = (Real)(float)A.params[1]; tw.omega = (Real)(float)A.params[2];
     if (sizeof(Real) == 8) { tw.phi = (Real)A.params[1]; tw.omega = (Real)A.params[2]; }
     const Real beta = (Real)A.params[0];            // lattice_parameters[0] = BETA/N
@@ -321,12 +324,12 @@ __device__ __forceinline__ void phase_site(const Field<Real> &U, const Geom &G, 
     }
 }
 
-template <int NC, typename Real, int PMODE, bool OR, int mu, int MINB, bool STAGED>
+template <int NC, typename Real, int PMODE, bool OR, int mu, int MINB, bool STAGED, bool TW>
 __global__ void __launch_bounds__(kPhaseBlock, MINB) k_phase(Field<Real> U, Geom G, PhaseArgs A)
 {
     const uint32_t t = A.t_begin + blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= A.t_end) return;
-    phase_site<NC, Real, PMODE, OR, mu, STAGED>(U, G, A, t);
+    phase_site<NC, Real, PMODE, OR, mu, STAGED, TW>(U, G, A, t);
 }
 
 // Overrelaxation of two links per thread (t and t + ceil(half/2)) with the
@@ -404,10 +407,14 @@ cudaError_t launch_phase_T(const Geom &G, void *links, int group, const PhaseArg
             return cudaGetLastError();
         }
     }
-#define QG_LAUNCH2(NC, PM, OR, MU, MB, ST) k_phase<NC, Real, PM, OR, MU, MB, ST><<<nb, bs, 0, s>>>(U, G, a)
+    // twisted boundaries: shape 0's form with the twist tests compiled in
+    // (any shape computes the same sequence); the others are compiled
+    // without them
+#define QG_LAUNCH2(NC, PM, OR, MU, MB, ST) k_phase<NC, Real, PM, OR, MU, MB, ST, false><<<nb, bs, 0, s>>>(U, G, a)
 #define QG_LAUNCH1(NC, PM, OR, MU)                                                  \
     do {                                                                            \
-        if (a.variant == 1) QG_LAUNCH2(NC, PM, OR, MU, 5, false);                   \
+        if (a.twist) k_phase<NC, Real, PM, OR, MU, 0, false, true><<<nb, bs, 0, s>>>(U, G, a); \
+        else if (a.variant == 1) QG_LAUNCH2(NC, PM, OR, MU, 5, false);              \
         else if (a.variant == 2) QG_LAUNCH2(NC, PM, OR, MU, 6, false);              \
         else if (a.variant == 3) QG_LAUNCH2(NC, PM, OR, MU, 0, NC == 3 && kStage);  \
         else if (a.variant >= 4) QG_LAUNCH2(NC, PM, OR, MU, 5, NC == 3 && kStage);  \
