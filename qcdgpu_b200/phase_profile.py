@@ -2,7 +2,7 @@
 
   python -m qcdgpu_b200.phase_profile [--size 32] [--precision 0] [--group 3]
                                       [--prng philox|ranlux] [--warm 2] [--phases 1]
-                                      [--shape S]
+                                      [--shape S] [--kernel-table REPS]
 
 Cold start, `warm` heatbath sweeps (8 heatbath phase launches each, so a
 profiler skips 8*warm + 1 kernel launches to reach the measured ones), then
@@ -25,6 +25,8 @@ def main():
     ap.add_argument("--warm", type=int, default=2)
     ap.add_argument("--phases", type=int, default=1)
     ap.add_argument("--shape", type=int, default=0)
+    ap.add_argument("--kernel-table", type=int, default=0,
+                    help="after the rest, print qg_profile_kernels' per-launch times (this many launches per class)")
     ap.add_argument("--measure", default="",
                     help="comma list run after the phases: wilson_all (8x8, FP32 products), "
                          "wilson_all64 (FP64 products), fmunu, action_profile, polyakov_profile, plaquette")
@@ -60,6 +62,9 @@ def main():
             raise SystemExit("unknown measurement " + m)
     L.sync()
     print("plaquette", L.plaquette())
+    if a.kernel_table:
+        for name, (m, sd) in L.profile_kernels(a.kernel_table).items():
+            print("%-22s %9.4f ms +- %.4f" % (name, m, sd))
 
 
 if __name__ == "__main__":
