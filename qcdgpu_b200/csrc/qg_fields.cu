@@ -356,13 +356,15 @@ cudaError_t launch_to_ref(const Geom &G, const void *links, void *ref, int group
 // ------------------------------------------------------------ observables
 // lattice_measurement_plq + lattice_measurement (sun_measurements_cl.cl:
 // 55-184,1178-1311): per-site plaquette and action sums, block partials
-template <int NC, typename Real>
+// TW: twisted boundaries possible; without it the per-link twist tests
+// fold away at compile time
+template <int NC, typename Real, bool TW>
 __global__ void __launch_bounds__(256) k_plaquette(Field<Real> U, Geom G, const double *params, int twist,
                                                     double *partials)
 {
     uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
     double v[4] = { 0, 0, 0, 0 };
-    if (s < G.V) plaq_site<NC, Real>(U, G, params, twist, s, v);
+    if (s < G.V) plaq_site<NC, Real>(U, G, params, TW ? twist : 0, s, v);
     block_sum_store<4>(v, partials);
 }
 
@@ -374,13 +376,16 @@ cudaError_t launch_plaquette(const Geom &G, const void *links, int group, int pr
     uint32_t nb = plaq_blocks(G);
     if (prec) {
         Field<double> U{ (double4 *)links, G.pstride };
-        if (group == 3) k_plaquette<3, double><<<nb, 256, 0, s>>>(U, G, params, twist, partials);
-        else k_plaquette<2, double><<<nb, 256, 0, s>>>(U, G, params, twist, partials);
+#define QG_PLQ(NC, R) (twist ? k_plaquette<NC, R, true><<<nb, 256, 0, s>>>(U, G, params, twist, partials) \
+                             : k_plaquette<NC, R, false><<<nb, 256, 0, s>>>(U, G, params, twist, partials))
+        if (group == 3) QG_PLQ(3, double);
+        else QG_PLQ(2, double);
     } else {
         Field<float> U{ (float4 *)links, G.pstride };
-        if (group == 3) k_plaquette<3, float><<<nb, 256, 0, s>>>(U, G, params, twist, partials);
-        else k_plaquette<2, float><<<nb, 256, 0, s>>>(U, G, params, twist, partials);
+        if (group == 3) QG_PLQ(3, float);
+        else QG_PLQ(2, float);
     }
+#undef QG_PLQ
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     return launch_reduce(partials, nb, 4, out, s);
@@ -421,14 +426,14 @@ cudaError_t launch_polyakov(const Geom &G, const void *links, int group, int pre
 // kept in a device buffer, then the per-slice sums of every axis from that
 // buffer in k_profile's order -- so the numbers equal the separate
 // qg_measure / qg_measure_*_profile calls bit for bit.
-template <int NC, typename Real>
+template <int NC, typename Real, bool TW>
 __global__ void __launch_bounds__(256) k_plaq_sites(Field<Real> U, Geom G, const double *params, int twist,
                                                      double *partials, double *sites)
 {
     uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
     double v[4] = { 0, 0, 0, 0 };
     if (s < G.V) {
-        plaq_site<NC, Real>(U, G, params, twist, s, v);
+        plaq_site<NC, Real>(U, G, params, TW ? twist : 0, s, v);
         sites[s] = v[2];                                 // spatial action of the site
         sites[(size_t)G.V + s] = v[3];                   // temporal
     }
@@ -470,10 +475,11 @@ __global__ void __launch_bounds__(256) k_bin_sites(const double *sites, Geom G, 
 
 // F_munu (FMUNU / F0MU lattice_measurement_plq, sun_measurements_cl.cl:
 // 712-1175 and reduce_measurement_plq_double2 :1313-1357): 12 sums
-template <int NC, typename Real>
+template <int NC, typename Real, bool TW>
 __global__ void __launch_bounds__(256) k_fmunu(Field<Real> U, Geom G, const double *params, int twist, int field,
                                                 int i1, int i2, double *partials)
 {
+    if (!TW) twist = 0;                  // untwisted: the twist tests fold away
     uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
     double v[12] = { 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0 };
     if (s < G.V) fmunu_site<NC, Real>(U, G, params, twist, s, field, i1, i2, v);
@@ -488,12 +494,12 @@ cudaError_t launch_fmunu(const Geom &G, const void *links, int group, int prec, 
     uint32_t nb = plaq_blocks(G);
     if (prec) {
         Field<double> U{ (double4 *)links, G.pstride };
-        if (group == 3) k_fmunu<3, double><<<nb, 256, 0, s>>>(U, G, params, twist, field, i1, i2, partials);
-        else k_fmunu<2, double><<<nb, 256, 0, s>>>(U, G, params, twist, field, i1, i2, partials);
+        if (group == 3) (twist ? k_fmunu<3, double, true><<<nb, 256, 0, s>>>(U, G, params, twist, field, i1, i2, partials) : k_fmunu<3, double, false><<<nb, 256, 0, s>>>(U, G, params, twist, field, i1, i2, partials));
+        else (twist ? k_fmunu<2, double, true><<<nb, 256, 0, s>>>(U, G, params, twist, field, i1, i2, partials) : k_fmunu<2, double, false><<<nb, 256, 0, s>>>(U, G, params, twist, field, i1, i2, partials));
     } else {
         Field<float> U{ (float4 *)links, G.pstride };
-        if (group == 3) k_fmunu<3, float><<<nb, 256, 0, s>>>(U, G, params, twist, field, i1, i2, partials);
-        else k_fmunu<2, float><<<nb, 256, 0, s>>>(U, G, params, twist, field, i1, i2, partials);
+        if (group == 3) (twist ? k_fmunu<3, float, true><<<nb, 256, 0, s>>>(U, G, params, twist, field, i1, i2, partials) : k_fmunu<3, float, false><<<nb, 256, 0, s>>>(U, G, params, twist, field, i1, i2, partials));
+        else (twist ? k_fmunu<2, float, true><<<nb, 256, 0, s>>>(U, G, params, twist, field, i1, i2, partials) : k_fmunu<2, float, false><<<nb, 256, 0, s>>>(U, G, params, twist, field, i1, i2, partials));
     }
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
@@ -509,10 +515,11 @@ cudaError_t launch_fmunu(const Geom &G, const void *links, int group, int prec, 
 // KIND 1: Re, Im Polyakov trace over the spatial sites of the slice.
 constexpr uint32_t kProfileChunk = 1024;
 
-template <int NC, typename Real, int KIND>
+template <int NC, typename Real, int KIND, bool TW>
 __global__ void __launch_bounds__(256) k_profile(Field<Real> U, Geom G, const double *params, int twist, int axis,
                                                   uint32_t per_slice, uint32_t chunks, double *partials)
 {
+    if (!TW) twist = 0;                  // untwisted: the twist tests fold away
     const int k = (int)(blockIdx.x / chunks);
     const uint32_t j0 = (blockIdx.x % chunks) * kProfileChunk;
     const uint32_t j1 = min(per_slice, j0 + kProfileChunk);
@@ -555,8 +562,9 @@ template <int NC, typename Real>
 static void profile_kernel(int kind, uint32_t nb, const Field<Real> &U, const Geom &G, const double *params,
                            int twist, int axis, uint32_t per, uint32_t chunks, double *partials, cudaStream_t s)
 {
-    if (kind == 0) k_profile<NC, Real, 0><<<nb, 256, 0, s>>>(U, G, params, twist, axis, per, chunks, partials);
-    else k_profile<NC, Real, 1><<<nb, 256, 0, s>>>(U, G, params, twist, axis, per, chunks, partials);
+    if (kind == 0 && twist) k_profile<NC, Real, 0, true><<<nb, 256, 0, s>>>(U, G, params, twist, axis, per, chunks, partials);
+    else if (kind == 0) k_profile<NC, Real, 0, false><<<nb, 256, 0, s>>>(U, G, params, twist, axis, per, chunks, partials);
+    else k_profile<NC, Real, 1, false><<<nb, 256, 0, s>>>(U, G, params, twist, axis, per, chunks, partials);
 }
 
 cudaError_t launch_profile(const Geom &G, const void *links, int group, int prec, const double *params, int twist,
@@ -592,7 +600,8 @@ cudaError_t launch_measure_all(const Geom &G, const void *links, int group, int 
 #define QG_SITES(NC, R)                                                                                 \
     do {                                                                                                \
         Field<R> U{ (typename V4<R>::T *)links, G.pstride };                                            \
-        if (kind == 0) k_plaq_sites<NC, R><<<nb, 256, 0, s>>>(U, G, params, twist, partials, sites);   \
+        if (kind == 0 && twist) k_plaq_sites<NC, R, true><<<nb, 256, 0, s>>>(U, G, params, twist, partials, sites); \
+        else if (kind == 0) k_plaq_sites<NC, R, false><<<nb, 256, 0, s>>>(U, G, params, twist, partials, sites); \
         else k_poly_sites<NC, R><<<nb, 256, 0, s>>>(U, G, partials, sites);                            \
     } while (0)
     if (prec) { if (group == 3) QG_SITES(3, double); else QG_SITES(2, double); }
@@ -618,10 +627,11 @@ cudaError_t launch_measure_all(const Geom &G, const void *links, int group, int 
 
 // lattice_measurement_wilson (wilson_loop.cl:55-454): per site and i in
 // {x,y,z}, Re Tr(L_t^T(x) L_i^R(x+T t) L_t^T(x+R i)^+ L_i^R(x)^+) in FP64
-template <int NC, typename Real>
+template <int NC, typename Real, bool TW>
 __global__ void __launch_bounds__(128) k_wilson(Field<Real> U, Geom G, int R, int T, const double *params, int twist,
                                                  double *partials)
 {
+    if (!TW) twist = 0;                  // untwisted: the twist tests fold away
     uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
     double v[1] = { 0 };
     if (s < G.V) {
@@ -656,12 +666,12 @@ cudaError_t launch_wilson(const Geom &G, const void *links, int group, int prec,
     uint32_t nb = (G.V + 127) / 128;
     if (prec) {
         Field<double> U{ (double4 *)links, G.pstride };
-        if (group == 3) k_wilson<3, double><<<nb, 128, 0, s>>>(U, G, R, T, params, twist, partials);
-        else k_wilson<2, double><<<nb, 128, 0, s>>>(U, G, R, T, params, twist, partials);
+        if (group == 3) (twist ? k_wilson<3, double, true><<<nb, 128, 0, s>>>(U, G, R, T, params, twist, partials) : k_wilson<3, double, false><<<nb, 128, 0, s>>>(U, G, R, T, params, twist, partials));
+        else (twist ? k_wilson<2, double, true><<<nb, 128, 0, s>>>(U, G, R, T, params, twist, partials) : k_wilson<2, double, false><<<nb, 128, 0, s>>>(U, G, R, T, params, twist, partials));
     } else {
         Field<float> U{ (float4 *)links, G.pstride };
-        if (group == 3) k_wilson<3, float><<<nb, 128, 0, s>>>(U, G, R, T, params, twist, partials);
-        else k_wilson<2, float><<<nb, 128, 0, s>>>(U, G, R, T, params, twist, partials);
+        if (group == 3) (twist ? k_wilson<3, float, true><<<nb, 128, 0, s>>>(U, G, R, T, params, twist, partials) : k_wilson<3, float, false><<<nb, 128, 0, s>>>(U, G, R, T, params, twist, partials));
+        else (twist ? k_wilson<2, float, true><<<nb, 128, 0, s>>>(U, G, R, T, params, twist, partials) : k_wilson<2, float, false><<<nb, 128, 0, s>>>(U, G, R, T, params, twist, partials));
     }
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
@@ -694,10 +704,11 @@ constexpr int kWilsonMax = 16;
 // from unitarity, more than FP64 products are meant to carry).
 template <int NC, typename P> constexpr int kRingFloats = NC == 2 ? 8 : (sizeof(P) == 8 ? 18 : 12);
 
-template <int NC, typename Real, typename P>
+template <int NC, typename Real, typename P, bool TW>
 __global__ void __launch_bounds__(128) k_wilson_cols(Field<Real> U, Geom G, int Tmax, const double *params,
                                                       int twist, double *partials)
 {
+    if (!TW) twist = 0;                  // untwisted: the twist tests fold away
     extern __shared__ __align__(16) unsigned char wsm[];
     constexpr int RF = kRingFloats<NC, P>;
     constexpr int ROWS = RF == 18 ? 3 : 2;        // rows stored
@@ -814,8 +825,13 @@ static cudaError_t wilson_cols(const Field<Real> &U, const Geom &G, int Rmax, in
     const size_t sm = wilson_cols_smem(NC, sizeof(P), Tmax, nbk);
     dim3 gc((unsigned)wilson_cols_blocks(G, nbk), Rmax, 3);
     nbx = (int)gc.x;
-    cudaFuncSetAttribute(k_wilson_cols<NC, Real, P>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-    k_wilson_cols<NC, Real, P><<<gc, nbk, sm, s>>>(U, G, Tmax, params, twist, partials);
+    if (twist) {
+        cudaFuncSetAttribute(k_wilson_cols<NC, Real, P, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+        k_wilson_cols<NC, Real, P, true><<<gc, nbk, sm, s>>>(U, G, Tmax, params, twist, partials);
+    } else {
+        cudaFuncSetAttribute(k_wilson_cols<NC, Real, P, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+        k_wilson_cols<NC, Real, P, false><<<gc, nbk, sm, s>>>(U, G, Tmax, params, twist, partials);
+    }
     return cudaGetLastError();
 }
 
