@@ -441,12 +441,16 @@ def test_set_shapes_rejects_out_of_range():
     L.close()
 
 
-@pytest.mark.parametrize("group,precision", [(3, 0), (3, 1), (2, 1)])
-def test_wilson_all_loops_match_single_loops_and_oracle(group, precision):
+@pytest.mark.parametrize("group,precision,twist", [(3, 0, False), (3, 1, False), (2, 1, False), (3, 0, True),
+                                                   (2, 1, True)])
+def test_wilson_all_loops_match_single_loops_and_oracle(group, precision, twist):
     """qg_measure_wilson_all (every R x T up to Rmax x Tmax in one launch)
     equals qg_measure_wilson loop by loop and the oracle's Wilson loops, to
-    the FP64 summation-order level"""
-    L, c = make_pair(group, (4, 6, 6, 8), precision, start=Q.START_HOT, prng=Q.PRNG_PHILOX, beta=5.8)
+    the FP64 summation-order level; with a twisted boundary both kernels
+    take their twisted form"""
+    phi, omega = (0.3, 0.7) if twist else (0.0, 0.0)
+    L, c = make_pair(group, (4, 6, 6, 8), precision, start=Q.START_HOT, prng=Q.PRNG_PHILOX, beta=5.8,
+                     phi=phi, omega=omega)
     L.seed(54)
     L.init()
     L.sweep(2)
