@@ -26,6 +26,19 @@ def test_reference_arm_line():
     assert d["cpu_baseline"]["kind"] == "reference" and d["cpu_baseline"]["cores"] >= 1
     assert d["e2e"] == {"value": d["value"], "unit": d["unit"], "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}
     assert d["config"]["lattice"] == [8, 8, 8, 8]
+    assert d["steps"] == 2 and d["steps_requested"] == 2
+
+
+def test_reference_arm_caps_its_timed_steps():
+    """one reference step is a whole heatbath phase per process (about a
+    second at 32^4), so a long --steps request is cut to the cap"""
+    sys.path.insert(0, ROOT)
+    import bench
+    d = _bench("--impl", "reference", "--size", "4", "--steps", str(bench.REF_MAX_STEPS + 5), "--warmup", "1")
+    if "unavailable" in d:
+        pytest.skip(d["unavailable"])
+    assert d["steps"] == bench.REF_MAX_STEPS and d["steps_requested"] == bench.REF_MAX_STEPS + 5
+    assert d["value"] > 0
 
 
 @pytest.mark.gpu
