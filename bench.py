@@ -38,7 +38,7 @@ LINK_BYTES = 48          # 12 FP32 reals per stored SU(3) link
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=300)
+    ap.add_argument("--steps", type=int, default=1000)   # about 2.7 s timed: a dozen clock samples
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--prng", default="philox", choices=["philox", "ranlux"])
