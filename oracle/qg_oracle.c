@@ -90,6 +90,8 @@ void ol_ranlux_states(const uint32_t *seeds, int instances, int nskip, ol_ranlux
  * s-th float4 (four consecutive outputs) to prns[s*instances + i]. */
 void ol_ranlux_batch(ol_ranlux *states, int instances, int samples, float *prns)
 {
+    /* every instance runs its own generator: instances in parallel */
+#pragma omp parallel for schedule(static)
     for (int i = 0; i < instances; i++)
         for (int s = 0; s < samples; s++) {
             float *o = prns + ((size_t)s * instances + i) * 4;
@@ -392,6 +394,7 @@ void ol_gramschmidt_fp64(const ol_cfg *c, void *t)
     if (c->precision != 0) { gramschmidt_d(c, (double *)t); return; }
     int V = sites_of(c);
     float *tf = (float *)t;
+#pragma omp parallel for schedule(static)
     for (int g = 0; g < V; g++)
         for (int mu = 0; mu < 4; mu++) {
             if (c->group == 3) {

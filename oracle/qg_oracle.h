@@ -37,21 +37,26 @@ typedef struct ol_cfg {
     int gid_mode;       /* INTS=2 deterministic update formulas          */
 } ol_cfg;
 
-/* PRN source for the heatbath: 0 = reference-layout float4 buffer read at
- * GID + k*PRNGSTEP; 1 = Philox4x32-10 counter stream (fast mode).          */
-typedef struct ol_prn {
-    int mode;
-    const float *prns;        /* mode 0: float4 buffer                      */
-    uint32_t key0, key1;      /* mode 1: Philox key                         */
-    uint64_t phase;           /* mode 1: phase counter                      */
-} ol_prn;
-
 /* ---- PRNG: glibc seeding + RANLUX (random/random.cpp, prngcl_ranlux.cl) */
 typedef struct ol_ranlux {
     float seeds[24];
     int i24, j24, in24, nskip;
     float carry;
 } ol_ranlux;
+
+/* PRN source for the heatbath: 0 = reference-layout float4 buffer read at
+ * GID + k*PRNGSTEP; 1 = Philox4x32-10 counter stream (fast mode);
+ * 2 = one RANLUX stream consumed in order, as the reference's sequential
+ * CPU path draws it (SU(N)/suncpp/su2/update_su2.cpp:81,101: 4 numbers per
+ * Kennedy-Pendleton try, 2 for the direction, no skip after a rejection);
+ * the links of a phase are then visited one after the other.               */
+typedef struct ol_prn {
+    int mode;
+    const float *prns;        /* mode 0: float4 buffer                      */
+    uint32_t key0, key1;      /* mode 1: Philox key                         */
+    uint64_t phase;           /* mode 1: phase counter                      */
+    ol_ranlux *stream;        /* mode 2: the stream (advanced in place)     */
+} ol_prn;
 
 void  ol_glibc_seeds(uint32_t randseries, int instances, uint32_t *seeds);
 void  ol_ranlux_init(ol_ranlux *st, int32_t jseed, int nskip);

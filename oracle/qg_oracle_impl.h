@@ -370,6 +370,11 @@ typedef struct {
 static void FN(prn_next)(FN(prnctx) *p, REAL r[4])
 {
     float q[4];
+    if (p->src->mode == 2) {
+        for (int i = 0; i < 4; i++) r[i] = (REAL)ol_ranlux_next(p->src->stream);
+        p->k++;
+        return;
+    }
     if (p->src->mode == 0) {
         size_t idx = (size_t)p->thread + (size_t)p->k * (size_t)p->cfg->prngstep;
         const float *s = p->src->prns + idx * 4;
@@ -436,6 +441,9 @@ static int FN(kp_step)(S2 *a, REAL beta, FN(prnctx) *p, int su3_path)
             rnd[1] = (REAL)fabs(sin((0.08 -  60.0 / V) * g));
             rnd[2] = (REAL)fabs(cos((0.08 + 150.0 / V) * g));
             rnd[3] = (REAL)fabs(sin((0.08 + 380.0 / V) * g));
+        } else if (p->src->mode == 2) {
+            rnd[0] = (REAL)ol_ranlux_next(p->src->stream);   /* update_su2.cpp:101: 2 numbers */
+            rnd[1] = (REAL)ol_ranlux_next(p->src->stream);
         } else {
             FN(prn_next)(p, rnd);
         }
@@ -456,7 +464,7 @@ static int FN(kp_step)(S2 *a, REAL beta, FN(prnctx) *p, int su3_path)
     if (su3_path) {
         a->u1.re = 1; a->u1.im = 0; a->u2.re = 0; a->u2.im = 0;
         a->v1.re = 0; a->v1.im = 0; a->v2.re = 1; a->v2.im = 0;
-        if (!c->gid_mode) p->k++;
+        if (!c->gid_mode && p->src->mode != 2) p->k++;
     }
     return 0;
 }
@@ -585,11 +593,10 @@ static S2 FN(staple2)(const ol_cfg *c, const REAL *tab, unsigned g, int mu)
 
 /* ----------------------------------------------------------- phase kernel */
 /* update_{even,odd}_{X,Y,Z,T}, SU(N)/suncl/suncl.cl:399-975 */
-static void FN(phase)(const ol_cfg *c, REAL *tab, int parity, int mu, const ol_prn *src, int kind)
+static void FN(phase_link)(const ol_cfg *c, REAL *tab, int parity, int mu, const ol_prn *src, int kind,
+                          REAL beta, unsigned t)
 {
-    unsigned half = (unsigned)(sites_of(c) / 2);
-    REAL beta = (REAL)(c->beta / c->group);
-    for (unsigned t = 0; t < half; t++) {
+    {
         unsigned g = parity ? odd_gid(c, t) : even_gid(c, t);
         crd co;
         gid2c(c, g, &co);
@@ -626,6 +633,21 @@ static void FN(phase)(const ol_cfg *c, REAL *tab, int parity, int mu, const ol_p
             }
         }
     }
+}
+
+static void FN(phase)(const ol_cfg *c, REAL *tab, int parity, int mu, const ol_prn *src, int kind)
+{
+    unsigned half = (unsigned)(sites_of(c) / 2);
+    REAL beta = (REAL)(c->beta / c->group);
+    if (kind == 0 && src && src->mode == 2) {
+        /* one stream consumed link after link: in thread order, serially */
+        for (unsigned t = 0; t < half; t++) FN(phase_link)(c, tab, parity, mu, src, kind, beta, t);
+        return;
+    }
+    /* the links of one (parity, direction) class are updated independently
+     * of one another, so the loop runs in parallel with the same result */
+#pragma omp parallel for schedule(static)
+    for (unsigned t = 0; t < half; t++) FN(phase_link)(c, tab, parity, mu, src, kind, beta, t);
 }
 
 /* --------------------------------------------------------- initialisation */
@@ -696,6 +718,7 @@ static R4 FN(rnd_r4)(const float *prns, size_t idx)
 static void FN(init_hot_dir)(const ol_cfg *c, REAL *tab, int mu, const float *prns)
 {
     int V = sites_of(c);
+#pragma omp parallel for schedule(static)
     for (int g = 0; g < V; g++) {
         if (c->group == 3) {
             R4 r1 = FN(rnd_r4)(prns, (size_t)g);
@@ -766,6 +789,7 @@ static void FN(init_hot_dir)(const ol_cfg *c, REAL *tab, int mu, const float *pr
 static void FN(gramschmidt)(const ol_cfg *c, REAL *tab)
 {
     int V = sites_of(c);
+#pragma omp parallel for schedule(static)
     for (int g = 0; g < V; g++)
         for (int mu = 0; mu < 4; mu++) {
             if (c->group == 3) {

@@ -193,6 +193,9 @@ void ol_mh_phase(const ol_cfg *c, void *table, int parity, int mu, const float *
     src.mode = 1; src.key0 = key0; src.key1 = key1; src.phase = phase;
     uint64_t acc = 0;
     double jump = 0.0;
+    /* links updated independently; the jump sum's order differs with the
+     * thread count (it is a statistic, compared within a tolerance) */
+#pragma omp parallel for schedule(static) reduction(+ : acc, jump)
     for (unsigned t = 0; t < half; t++) {
         unsigned g = parity ? odd_gid(c, t) : even_gid(c, t);
         crd co;

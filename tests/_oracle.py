@@ -38,6 +38,7 @@ class Prn(ctypes.Structure):
         ("key0", ctypes.c_uint32),
         ("key1", ctypes.c_uint32),
         ("phase", ctypes.c_uint64),
+        ("stream", ctypes.c_void_p),
     ]
 
 
@@ -158,9 +159,22 @@ def prn_samples(c, instances, hot=False):
     return 1 + (total - 1) // instances
 
 
-def phase_hb(c, tab, parity, mu, prns=None, philox=None):
+class Stream:
+    """One RANLUX stream consumed in order (PRN source mode 2): the reference
+    sequential CPU path's generator, seeded as PRNG::initialize_CPU does
+    (srand(series), the first rand() mod 2^31-1)."""
+
+    def __init__(self, series, nskip=223):
+        self.state = ctypes.create_string_buffer(lib.ol_sizeof_ranlux())
+        lib.ol_ranlux_init(self.state, int(glibc_seeds(series, 1)[0]), nskip)
+
+
+def phase_hb(c, tab, parity, mu, prns=None, philox=None, stream=None):
     src = Prn()
-    if prns is not None:
+    if stream is not None:
+        src.mode = 2
+        src.stream = ctypes.cast(stream.state, ctypes.c_void_p)
+    elif prns is not None:
         src.mode = 0
         src.prns = prns.ctypes.data
     else:
@@ -254,3 +268,38 @@ def mh_loss(c, tab, parity, mu, w, eps_max, key0, phase, key1=TRAIN_KEY1):
     w = np.ascontiguousarray(w, dtype=np.float64)
     return lib.ol_mh_loss(ctypes.byref(c), vp(tab), parity, mu, w.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
                           eps_max, key0, key1, phase)
+
+
+# ---- the reference's sequential CPU path (oracle/_ref/ref_cpurun "links")
+def table_to_rows(c, tab):
+    """reference-layout table -> per (site, dir) the stored rows as the
+    reference CPU path keeps them: SU(3) u1..u3, v1..v3 (re, im) = 12
+    doubles; SU(2) u1, u2 (re, im) = 4 doubles; site-major, dir fastest"""
+    V = volume(c)
+    planes = 12 if c.group == 3 else 4
+    t = tab.astype(np.float64).reshape(planes, c.rowsize, 4)[:, :V, :]
+    if c.group == 2:
+        a = t[0:4].transpose(1, 0, 2)                      # [site][dir][x y z w]
+        out = np.stack([a[..., 0], a[..., 2], a[..., 1], a[..., 3]], axis=-1)
+        return np.ascontiguousarray(out)
+    p1, p2, p3 = t[0:4].transpose(1, 0, 2), t[4:8].transpose(1, 0, 2), t[8:12].transpose(1, 0, 2)
+    out = np.stack([p1[..., 0], p2[..., 0], p1[..., 1], p2[..., 1], p1[..., 2], p2[..., 2],
+                    p3[..., 0], p3[..., 2], p3[..., 1], p3[..., 3], p1[..., 3], p2[..., 3]], axis=-1)
+    return np.ascontiguousarray(out)
+
+
+def rows_to_table(c, rows):
+    V = volume(c)
+    tab = new_table(c).reshape(-1, c.rowsize, 4)
+    if c.group == 2:
+        r = rows.reshape(V, 4, 4)
+        for d in range(4):
+            tab[d, :V, 0], tab[d, :V, 2], tab[d, :V, 1], tab[d, :V, 3] = r[:, d, 0], r[:, d, 1], r[:, d, 2], r[:, d, 3]
+        return tab.reshape(-1)
+    r = rows.reshape(V, 4, 12)
+    for d in range(4):
+        x = r[:, d, :]
+        tab[d, :V] = np.stack([x[:, 0], x[:, 2], x[:, 4], x[:, 10]], axis=-1)
+        tab[d + 4, :V] = np.stack([x[:, 1], x[:, 3], x[:, 5], x[:, 11]], axis=-1)
+        tab[d + 8, :V] = np.stack([x[:, 6], x[:, 8], x[:, 7], x[:, 9]], axis=-1)
+    return tab.reshape(-1)

@@ -5,6 +5,10 @@
   PRNG::check (random.cpp:339-402) requires GPU instance 0 to equal.
 * glibc seeding: RANDSERIES -> instance seeds as PRNG::initialize does.
 * Philox4x32-10: the published known-answer vectors of the algorithm.
+* Heatbath link by link: fed one RANLUX3 stream in order, the oracle's
+  heatbath phases reproduce the links of the reference's sequential CPU
+  heatbath (SU(N)/suncpp) to 1e-12 -- Kennedy-Pendleton draws with their
+  accept/reject decisions, subgroup embedding and Gram-Schmidt.
 * Deterministic INTS=2 mode: the oracle's restatement of the update kernels
   reproduces the plaquettes of the reference's sequential CPU path
   (SU(N)/suncpp) -- to 1e-14 on the closed-form start and to the ~1e-7
@@ -164,3 +168,78 @@ def test_own_elementary_functions_accuracy():
     for y in ys:
         a, b = lib.ol_logd(float(y)), float(np.log(y))
         assert abs(a - b) <= 2 * np.spacing(abs(b)) + 1e-300, (y, a, b)
+
+
+# ---------------------------------------------- heatbath link by link
+HB_LINKS = np.load(os.path.join(os.path.dirname(__file__), "golden", "reference_heatbath_links.npz"))
+HB_CASES = [("su3_b6.0", 3, (4, 4, 2, 4), 6.0), ("su3_b1.5", 3, (4, 4, 2, 4), 1.5),
+            ("su2_b2.3", 2, (4, 4, 2, 4), 2.3), ("su2_b0.6", 2, (4, 4, 2, 4), 0.6)]
+
+
+def _sequential_phases(c, tab, phases, series=54):
+    """the oracle's heatbath phases drawing one RANLUX3 stream in order, as
+    the reference's sequential CPU path does (PRN source mode 2); returns
+    the number of Kennedy-Pendleton numbers drawn"""
+    st = O.Stream(series)
+    for k in range(phases):
+        O.phase_hb(c, tab, 1 - (k // 4) % 2, k % 4, stream=st)
+    probe = O.Stream(series)
+    n = 0
+    # count the stream's consumption by finding where the two states meet
+    ref = bytes(st.state)
+    while bytes(probe.state) != ref:
+        O.lib.ol_ranlux_next(probe.state)
+        n += 1
+    return n
+
+
+@pytest.mark.parametrize("case", HB_CASES, ids=lambda c: c[0])
+def test_heatbath_links_match_reference_cpu_path(case):
+    """The heatbath arithmetic itself against the reference's executed code:
+    from the same thermalising start and the same RANLUX3 stream drawn in
+    order, one sweep of 8 heatbath phases of the oracle reproduces the links
+    of the reference's sequential CPU heatbath (SU(N)/suncpp/su2/
+    update_su2.cpp:40-126, su3/update_su3.cpp:40-114; golden file made by
+    tests/golden/make_heatbath_links.py) to 1e-12 -- the Kennedy-Pendleton
+    log(1-r) draw, its accept/reject decision (the low-coupling cases reject
+    often), the direction draw, the subgroup embedding and the per-link
+    Gram-Schmidt.  The two sides differ only in rounding order (staple
+    association, matrix products, the log and cos routines): measured
+    max|dU| <= 4e-15, and 3e-13 for SU(3) at beta = 1.5, where cos(alpha) =
+    1 - delta nears -1 and sqrt(1 - cos^2) magnifies last-bit differences."""
+    name, group, dims, beta = case
+    c = O.make_cfg(group=group, dims=dims, precision=1, beta=beta, row_align=64)
+    tab = O.rows_to_table(c, HB_LINKS[name + "_start"])
+    drawn = _sequential_phases(c, tab, 8)
+    ref = O.rows_to_table(c, HB_LINKS[name + "_ref"])
+    d = float(np.max(np.abs(tab - ref)))
+    links = O.volume(c) // 2 * 8
+    tries_per_link = (drawn - 2 * links * (3 if group == 3 else 1)) / 4.0 / (links * (3 if group == 3 else 1))
+    print("%s: max|dU| = %.3g, %.3f Kennedy-Pendleton tries per draw" % (name, d, tries_per_link))
+    assert d <= 1e-12
+    if beta < 2.0:
+        assert tries_per_link > 1.3                  # the rejection path is exercised
+
+
+@pytest.mark.skipif(not os.path.exists(os.path.join(O.REF_DIR, "ref_cpurun")), reason="oracle/_ref not built")
+@pytest.mark.parametrize("group,beta", [(3, 6.0), (2, 2.3)])
+def test_heatbath_links_live_against_reference_binary_8x4(group, beta):
+    """The same comparison at the SU(2) run configuration's lattice size (8^4)
+    over two sweeps, against the reference binary run live"""
+    import tempfile
+    dims = (8, 8, 8, 8)
+    c = O.make_cfg(group=group, dims=dims, precision=1, beta=beta, row_align=64)
+    tab = O.new_table(c)
+    O.lib.ol_init_cold(ctypes.byref(c), O.vp(tab))
+    for ph in range(8):
+        O.phase_hb(c, tab, 1 - (ph // 4) % 2, ph % 4, philox=(9, 0x5D3E1A27, ph))
+    with tempfile.TemporaryDirectory() as d:
+        fin, fout = os.path.join(d, "in.bin"), os.path.join(d, "out.bin")
+        O.table_to_rows(c, tab).tofile(fin)
+        subprocess.check_call([os.path.join(O.REF_DIR, "ref_cpurun"), "links", str(group)] +
+                              [str(x) for x in dims] + [repr(beta), "54", "16", fin, fout])
+        ref = O.rows_to_table(c, np.fromfile(fout, dtype=np.float64))
+    _sequential_phases(c, tab, 16)
+    d = float(np.max(np.abs(tab - ref)))
+    print("SU(%d) 8^4 two sweeps: max|dU| = %.3g" % (group, d))
+    assert d <= 1e-12
