@@ -304,9 +304,13 @@ int qg_set_sweeps_done(qg_ctx *ctx, uint64_t sweeps);
  * present on every GPU that loads it until the process exits, so lattices
  * are limited to 2^24 sites (64^4); larger ones are rejected with
  * QG_ERR_ARG.  The first call on a device looks up that array's device
- * address (cudaGetSymbolAddress); make that first call before any stream
- * capture.  All calls share the array: calls whose kernels may overlap on
- * the GPU race and must be ordered by the caller.  Errors: qg_last_error(NULL). */
+ * address (cudaGetSymbolAddress) and keeps it for the process; make that
+ * first call before any stream capture.  The address belongs to the
+ * device's primary context: after cudaDeviceReset the entry point must not
+ * be called again in that process.  All calls share the array: calls whose
+ * kernels may overlap on the GPU race and must be ordered by the caller.
+ * A CUDA error already pending when the call starts is reported as
+ * QG_ERR_CUDA and left pending.  Errors: qg_last_error(NULL). */
 int qg_plaquette_noalloc(const void *links, int group, int precision, const int size[4], uint32_t rowsize,
                          double beta, double *out, void *stream);
 

@@ -3,14 +3,20 @@
 # from the sources where they lie, into oracle/_ref/ (git-ignored):
 #   _ref/ref_ranlux   -- the reference host RANLUX (random/random.cpp)
 #   _ref/ref_cpurun   -- the reference sequential heatbath (SU(N)/suncpp)
-# Test and baseline infrastructure only.  Usage: build_ref.sh [reference root]
+# Test and baseline infrastructure only.
+# Usage: build_ref.sh [--probe] [reference root]
+#   the root is the argument, else $QCDGPU_REFERENCE, else /root/reference;
+#   --probe only checks that the sources are there (exit 1 if not)
 set -e
 HERE=$(cd "$(dirname "$0")" && pwd)
-REF=${1:-/root/reference}
+PROBE=0
+if [ "$1" = "--probe" ]; then PROBE=1; shift; fi
+REF=${1:-${QCDGPU_REFERENCE:-/root/reference}}
 R="$REF/SU(N)"
 OUT="$HERE/_ref"
 CXX=${CXX:-g++}
 [ -d "$R" ] || { echo "reference sources not found under $REF" >&2; exit 1; }
+[ "$PROBE" = 1 ] && exit 0
 mkdir -p "$OUT"
 $CXX -O2 -D CPU_RUN -I "$R" -o "$OUT/ref_ranlux" "$HERE/ref_ranlux_driver.cpp" "$R/random/random.cpp"
 $CXX -O2 -D CPU_RUN -I "$HERE/ref_stub" -I "$R" -o "$OUT/ref_cpurun" "$HERE/ref_cpurun_driver.cpp" \

@@ -16,6 +16,8 @@ PKG_DIR = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(PKG_DIR, "lib", "libqg_sun.so")
 
 QG_OK = 0
+QG_ERR_ARG, QG_ERR_CUDA, QG_ERR_STATE, QG_ERR_NOMEM, QG_ERR_IO, QG_ERR_UNSUPPORTED, QG_ERR_NUMERIC = \
+    -1, -2, -3, -4, -5, -6, -7
 START_HOT, START_COLD, START_GID, START_HAAR = 0, 1, 2, 3
 PRNG_RANLUX, PRNG_PHILOX = 0, 1
 LAYOUT_REFERENCE = 0

@@ -179,10 +179,20 @@ extern "C" int qg_plaquette_noalloc(const void *links, int group, int precision,
         return QG_ERR_ARG;
     }
     if ((uint64_t)rowsize < V) { qg_set_global_error("rowsize smaller than the number of sites"); return QG_ERR_ARG; }
+    // an error left pending by the caller's earlier work is reported, not
+    // consumed: the launch checks below read the error state
+    cudaError_t e = cudaPeekAtLastError();
+    if (e != cudaSuccess) {
+        qg_set_global_error(std::string("qg_plaquette_noalloc: a CUDA error was pending before the call: ") +
+                            cudaGetErrorString(e));
+        return QG_ERR_CUDA;
+    }
     // set-up, once per device, with that device current: the device
-    // address of the scratch array (the host-side symbol is only a handle)
+    // address of the scratch array (the host-side symbol is only a handle).
+    // The address is kept for the process: it belongs to the device's
+    // primary context and is not valid after cudaDeviceReset.
     int dev = 0;
-    cudaError_t e = cudaGetDevice(&dev);
+    e = cudaGetDevice(&dev);
     if (e != cudaSuccess) { qg_set_global_error(std::string("cudaGetDevice: ") + cudaGetErrorString(e)); return QG_ERR_CUDA; }
     if (dev < 0 || dev >= 64) { qg_set_global_error("device ordinal out of range"); return QG_ERR_ARG; }
     double *scratch;
