@@ -471,20 +471,25 @@ static int FN(kp_step)(S2 *a, REAL beta, FN(prnctx) *p, int su3_path)
 
 /* Microcanonical reflection of the SU(2) block (overrelaxation; absent in
  * the reference, Creutz PRD 36 (1987) 515, Brown-Woch PRL 58 (1987) 2394):
- * with aH the normalised hermitian projection used by the heatbath, the
- * subgroup element aH*aH leaves Re Tr(V W) unchanged and is an involution. */
+ * with aH = h/|h| the normalised hermitian projection used by the heatbath,
+ * the subgroup element aH*aH leaves Re Tr(V W) unchanged and is an
+ * involution.  Written in closed form: aH^2 = (x^2 - y^2 - z^2 - w^2,
+ * 2xy, 2xz, 2xw) / |h|^2 (one reciprocal, no square root). */
 static void FN(or_step)(S2 *a)
 {
-    R4 aH;
-    aH.x =  (a->u1.re + a->v2.re);
-    aH.z = -(a->u1.im - a->v2.im);
-    aH.y = -(a->u2.re - a->v1.re);
-    aH.w = -(a->u2.im + a->v1.im);
-    REAL n2 = aH.x * aH.x;
-    n2 = RFMA(aH.y, aH.y, n2); n2 = RFMA(aH.z, aH.z, n2); n2 = RFMA(aH.w, aH.w, n2);
-    REAL id = (REAL)1 / RSQRT(n2);
-    aH.x *= id; aH.z *= id; aH.y *= id; aH.w *= id;
-    *a = FN(rec2)(FN(times2)(aH, aH));
+    REAL hx =  (a->u1.re + a->v2.re);
+    REAL hz = -(a->u1.im - a->v2.im);
+    REAL hy = -(a->u2.re - a->v1.re);
+    REAL hw = -(a->u2.im + a->v1.im);
+    REAL n2 = hx * hx;
+    n2 = RFMA(hy, hy, n2); n2 = RFMA(hz, hz, n2); n2 = RFMA(hw, hw, n2);
+    REAL v0 = hx * hx;
+    v0 = RFMA(-hy, hy, v0); v0 = RFMA(-hz, hz, v0); v0 = RFMA(-hw, hw, v0);
+    REAL inv = (REAL)1 / n2;
+    REAL t = (hx + hx) * inv;
+    R4 v;
+    v.x = v0 * inv; v.y = hy * t; v.z = hz * t; v.w = hw * t;
+    *a = FN(rec2)(v);
 }
 
 /* rows i, j of U <- V (rows i, j), V = (u1 u2; v1 v2) */
@@ -521,7 +526,10 @@ static G3 FN(cm3)(const M3 *S, G3 m0, REAL beta, FN(prnctx) *p, int nhitpar, int
             if (kind == 0) FN(kp_step)(&r0, beta, p, 1); else FN(or_step)(&r0);
             FN(rotate_rows)(&U, i, j, &r0);
         }
-        reslt = FN(gs3)(FN(compress)(&U));
+        /* Gram-Schmidt after a heatbath update; the reflections keep U
+         * unitary to rounding and an overrelaxed link is stored as it is
+         * (reunitarised by its next heatbath update and the global pass) */
+        reslt = (kind == 0) ? FN(gs3)(FN(compress)(&U)) : FN(compress)(&U);
         U = FN(expand)(reslt);
     }
     return reslt;

@@ -184,27 +184,27 @@ __device__ __forceinline__ void padd3(M32 &r, const M32 &a, const M32 &b)
         }
 }
 
-// per-lane 1 / sqrt(x) as the scalar code computes it ((Real)1 / sqrtf(x))
-__device__ __forceinline__ F2 prsqrt_div(F2 x) { return pair(1.0f / sqrtf(x.x), 1.0f / sqrtf(x.y)); }
+// per-lane 1 / x as the scalar code computes it ((Real)1 / x)
+__device__ __forceinline__ F2 prcp_div(F2 x) { return pair(1.0f / x.x, 1.0f / x.y); }
 
-// the SU(2) reflection of a 2x2 block (or_step, with times2 / rec2)
+// the SU(2) reflection of a 2x2 block (or_step, closed form)
 __device__ __forceinline__ void por_step(S22 &a)
 {
-    F2 hx = padd(a.u1.re, a.v2.re);
-    F2 hz = pneg(psub(a.u1.im, a.v2.im));
-    F2 hy = pneg(psub(a.u2.re, a.v1.re));
-    F2 hw = pneg(padd(a.u2.im, a.v1.im));
+    const F2 hx = padd(a.u1.re, a.v2.re);
+    const F2 hz = pneg(psub(a.u1.im, a.v2.im));
+    const F2 hy = pneg(psub(a.u2.re, a.v1.re));
+    const F2 hw = pneg(padd(a.u2.im, a.v1.im));
     F2 n2 = pmul(hx, hx);
     n2 = pfma(hy, hy, n2);
     n2 = pfma(hz, hz, n2);
     n2 = pfma(hw, hw, n2);
-    const F2 id = prsqrt_div(n2);
-    hx = pmul(hx, id); hz = pmul(hz, id); hy = pmul(hy, id); hw = pmul(hw, id);
-    // times2(aH, aH)
-    F2 ax = pmul(hx, hx); ax = pfma(pneg(hy), hy, ax); ax = pfma(pneg(hz), hz, ax); ax = pfma(pneg(hw), hw, ax);
-    F2 az = pmul(hx, hz); az = pfma(hz, hx, az); az = pfma(hy, hw, az); az = pfma(pneg(hw), hy, az);
-    F2 ay = pmul(hx, hy); ay = pfma(hy, hx, ay); ay = pfma(hw, hz, ay); ay = pfma(pneg(hz), hw, ay);
-    F2 aw = pmul(hx, hw); aw = pfma(hw, hx, aw); aw = pfma(hz, hy, aw); aw = pfma(pneg(hy), hz, aw);
+    F2 v0 = pmul(hx, hx);
+    v0 = pfma(pneg(hy), hy, v0);
+    v0 = pfma(pneg(hz), hz, v0);
+    v0 = pfma(pneg(hw), hw, v0);
+    const F2 inv = prcp_div(n2);
+    const F2 t = pmul(padd(hx, hx), inv);
+    const F2 ax = pmul(v0, inv), ay = pmul(hy, t), az = pmul(hz, t), aw = pmul(hw, t);
     // rec2
     a.u1 = { ax, az }; a.u2 = { ay, aw };
     a.v1 = { pneg(ay), aw }; a.v2 = { ax, pneg(az) };
@@ -229,50 +229,8 @@ __device__ __forceinline__ void protate_rows(M32 &U, int i, int j, const S22 &V)
     }
 }
 
-// Gram-Schmidt of rows 1, 2 in FP32 (gs3<float>)
-__device__ __forceinline__ G32 pgs3(const G32 &g)
-{
-    F2 u[3][2] = { { g.uv1[0], g.uv2[0] }, { g.uv1[1], g.uv2[1] }, { g.uv1[2], g.uv2[2] } };
-    F2 v[3][2] = { { g.uv3[0], g.uv3[2] }, { g.uv3[1], g.uv3[3] }, { g.uv1[3], g.uv2[3] } };
-    F2 n2 = pmul(u[0][0], u[0][0]);
-    n2 = pfma(u[0][1], u[0][1], n2);
-#pragma unroll
-    for (int k = 1; k < 3; k++) { n2 = pfma(u[k][0], u[k][0], n2); n2 = pfma(u[k][1], u[k][1], n2); }
-    const F2 inu = prsqrt_div(n2);
-#pragma unroll
-    for (int k = 0; k < 3; k++) { u[k][0] = pmul(u[k][0], inu); u[k][1] = pmul(u[k][1], inu); }
-    F2 sr = pmul(v[0][0], u[0][0]), si = pmul(v[0][1], u[0][0]);
-    sr = pfma(v[0][1], u[0][1], sr);
-    si = pfma(pneg(v[0][0]), u[0][1], si);
-#pragma unroll
-    for (int k = 1; k < 3; k++) {
-        sr = pfma(v[k][0], u[k][0], sr); sr = pfma(v[k][1], u[k][1], sr);
-        si = pfma(v[k][1], u[k][0], si); si = pfma(pneg(v[k][0]), u[k][1], si);
-    }
-    const F2 nsr = pneg(sr), nsi = pneg(si);
-#pragma unroll
-    for (int k = 0; k < 3; k++) {
-        F2 r = pfma(nsr, u[k][0], v[k][0]);
-        r = pfma(si, u[k][1], r);
-        F2 i = pfma(nsr, u[k][1], v[k][1]);
-        i = pfma(nsi, u[k][0], i);
-        v[k][0] = r; v[k][1] = i;
-    }
-    F2 m2 = pmul(v[0][0], v[0][0]);
-    m2 = pfma(v[0][1], v[0][1], m2);
-#pragma unroll
-    for (int k = 1; k < 3; k++) { m2 = pfma(v[k][0], v[k][0], m2); m2 = pfma(v[k][1], v[k][1], m2); }
-    const F2 inv = prsqrt_div(m2);
-#pragma unroll
-    for (int k = 0; k < 3; k++) { v[k][0] = pmul(v[k][0], inv); v[k][1] = pmul(v[k][1], inv); }
-    G32 r;
-    r.uv1[0] = u[0][0]; r.uv1[1] = u[1][0]; r.uv1[2] = u[2][0]; r.uv1[3] = v[2][0];
-    r.uv2[0] = u[0][1]; r.uv2[1] = u[1][1]; r.uv2[2] = u[2][1]; r.uv2[3] = v[2][1];
-    r.uv3[0] = v[0][0]; r.uv3[1] = v[1][0]; r.uv3[2] = v[0][1]; r.uv3[3] = v[1][1];
-    return r;
-}
-
-// Cabibbo-Marinari overrelaxation of a pair (cm3<float, true>)
+// Cabibbo-Marinari overrelaxation of a pair (cm3<float, true>; no
+// Gram-Schmidt after the reflections, as cm3)
 __device__ __forceinline__ G32 pcm3_or(const M32 &S, const G32 &m0, int nhitpar)
 {
     G32 reslt = m0;
@@ -289,7 +247,7 @@ __device__ __forceinline__ G32 pcm3_or(const M32 &S, const G32 &m0, int nhitpar)
             por_step(r0);
             protate_rows(U, i, j, r0);
         }
-        reslt = pgs3(pcompress(U));
+        reslt = pcompress(U);
         U = pexpand(reslt);
     }
     return reslt;
@@ -441,7 +399,7 @@ __device__ __forceinline__ G3<float> cm3_or_rows(const M3<float> &S, const G3<fl
                 U.m[j][k] = { re.y, im.y };
             }
         }
-        reslt = gs3<float>(compress(U));
+        reslt = compress(U);
         U = expand(reslt);
     }
     return reslt;

@@ -487,21 +487,26 @@ __device__ __forceinline__ bool kp_step(S2<Real> &a, Real beta, Prn &prn, int nh
     return false;
 }
 
-// microcanonical reflection of the block: V = aH*aH (Creutz 1987,
-// Brown & Woch 1987); the reference has no overrelaxation.
+// microcanonical reflection of the block (Creutz 1987, Brown & Woch 1987;
+// the reference has no overrelaxation): V = aH^2 with aH = h / |h| the
+// normalised SU(2) projection h = (x; y, z, w) of the block, written in
+// closed form as V = (x^2 - y^2 - z^2 - w^2, 2xy, 2xz, 2xw) / |h|^2 --
+// one reciprocal, no square root
 template <typename Real>
 __device__ __forceinline__ void or_step(S2<Real> &a)
 {
-    R4<Real> aH;
-    aH.x =  (a.u1.re + a.v2.re);
-    aH.z = -(a.u1.im - a.v2.im);
-    aH.y = -(a.u2.re - a.v1.re);
-    aH.w = -(a.u2.im + a.v1.im);
-    Real n2 = aH.x * aH.x;
-    n2 = FMA(aH.y, aH.y, n2); n2 = FMA(aH.z, aH.z, n2); n2 = FMA(aH.w, aH.w, n2);
-    Real id = (Real)1 / RC<Real>::sq(n2);
-    aH.x *= id; aH.z *= id; aH.y *= id; aH.w *= id;
-    a = rec2(times2(aH, aH));
+    const Real hx =  (a.u1.re + a.v2.re);
+    const Real hz = -(a.u1.im - a.v2.im);
+    const Real hy = -(a.u2.re - a.v1.re);
+    const Real hw = -(a.u2.im + a.v1.im);
+    Real n2 = hx * hx;
+    n2 = FMA(hy, hy, n2); n2 = FMA(hz, hz, n2); n2 = FMA(hw, hw, n2);
+    Real v0 = hx * hx;
+    v0 = FMA(-hy, hy, v0); v0 = FMA(-hz, hz, v0); v0 = FMA(-hw, hw, v0);
+    const Real inv = (Real)1 / n2;
+    const Real t = (hx + hx) * inv;
+    R4<Real> v = { v0 * inv, hy * t, hz * t, hw * t };
+    a = rec2(v);
 }
 
 // rows i, j of U <- V (rows i, j) for the 2x2 block V = (u1 u2; v1 v2)
@@ -523,7 +528,10 @@ __device__ __forceinline__ void rotate_rows(M3<Real> &U, int i, int j, const S2<
 // Cabibbo-Marinari over the SU(2) subgroups (1,2), (1,3), (2,3)
 // (lattice_heatbath3, su3_update_cl.cl:672-779): for each subgroup the 2x2
 // block of W = U staple, a Kennedy-Pendleton draw (or the reflection when
-// OR), and the rotation of the two rows of U; then Gram-Schmidt.
+// OR), and the rotation of the two rows of U; then Gram-Schmidt after a
+// heatbath update.  The reflections keep U unitary to rounding, so an
+// overrelaxation update stores U as it is: every link is reunitarised by
+// its heatbath update once per sweep (and by the global pass).
 // LOOP runs the three subgroups as a runtime loop (rows and columns picked
 // by selects) so that the heatbath draw's code appears once; the
 // arithmetic is the unrolled form's.
@@ -581,7 +589,7 @@ __device__ __forceinline__ G3<Real> cm3(const M3<Real> &S, const G3<Real> &m0, R
                 rotate_rows(U, i, j, r0);
             }
         }
-        reslt = gs3<Real>(compress(U));
+        reslt = OR ? compress(U) : gs3<Real>(compress(U));
         U = expand(reslt);
     }
     return reslt;
