@@ -259,6 +259,36 @@ static void gen_proj(const cd3 *P, int N, int a, double out[2])
  * fma; natural log by y = m 2^e, log m = 2 atanh((m-1)/(m+1)) to s^23.
  * The same operation sequence as the CUDA path's routines, so both sides
  * round identically. */
+/* float sin/cos for |x| < 1024 (qg_sincosf of the kernels): Cody-Waite
+ * reduction by pi/2 with a three-part float constant, Taylor polynomials of
+ * degree 9 / 10 on [-pi/4, pi/4] in Horner form, every step in float */
+static void ol_sincosf(float x, float *s, float *c)
+{
+    const float INV_PIO2 = 0.6366197466850281f;
+    const float P1 = 1.5707963705062866f, P2 = -4.371138828673793e-08f, P3 = -1.7151245100058819e-15f;
+    const float n = rintf(x * INV_PIO2);
+    float f = fmaf(-n, P1, x);
+    f = fmaf(-n, P2, f);
+    f = fmaf(-n, P3, f);
+    const float f2 = f * f;
+    float ps = 2.7557318844628753e-06f;
+    ps = fmaf(ps, f2, -1.9841270113829523e-04f);
+    ps = fmaf(ps, f2, 8.333333767950535e-03f);
+    ps = fmaf(ps, f2, -1.666666716337204e-01f);
+    const float sn = fmaf(ps * f2, f, f);
+    float pc = -2.755731998149713e-07f;
+    pc = fmaf(pc, f2, 2.4801587642286904e-05f);
+    pc = fmaf(pc, f2, -1.3888889225199819e-03f);
+    pc = fmaf(pc, f2, 4.16666679084301e-02f);
+    pc = fmaf(pc, f2, -0.5f);
+    const float cs = fmaf(pc, f2, 1.0f);
+    const int q = ((int)n) & 3;
+    *s = (q == 0) ? sn : (q == 1) ? cs : (q == 2) ? -sn : -cs;
+    *c = (q == 0) ? cs : (q == 1) ? -sn : (q == 2) ? -cs : sn;
+}
+float ol_sinf_own(float x) { float s, c; ol_sincosf(x, &s, &c); return s; }
+float ol_cosf_own(float x) { float s, c; ol_sincosf(x, &s, &c); return c; }
+
 static void ol_sincos(double x, double *s, double *c)
 {
     const double INV_PIO2 = 0.63661977236758134308;

@@ -69,6 +69,10 @@ int   ol_sizeof_ranlux(void);
 void  ol_philox4x32(const uint32_t ctr[4], const uint32_t key[2], uint32_t out[4]);
 void  ol_philox_prn(const ol_prn *src, uint32_t thread, uint32_t k, float out[4]);
 
+/* ---- the float sin / cos of the FP32 update path */
+float ol_sinf_own(float x);
+float ol_cosf_own(float x);
+
 /* ---- lattice kernels (table in reference layout, Real = float|double) */
 void ol_init_cold(const ol_cfg *c, void *table);
 void ol_init_gid(const ol_cfg *c, void *table);

@@ -10,8 +10,9 @@
  *
  * Operation order: every multiply-add is an explicit fma() in a fixed order
  * (the file is compiled with -ffp-contract=off) and sin/cos/log on the
- * update path are the routines ol_sincos / ol_log of qg_oracle.c, so the
- * roundings this restatement performs are fully specified by the source.
+ * update path are the routines ol_sincosf (float links) / ol_sincos (double
+ * links) and ol_log of qg_oracle.c, so the roundings this restatement
+ * performs are fully specified by the source.
  */
 
 #define R4  PASTE(r4,  SFX)
@@ -27,8 +28,8 @@
 #define RPI2  6.283185307179586f
 #define RSQRT sqrtf
 #define RFMA  fmaf
-static float FN(rsin)(float a) { double s, c; ol_sincos((double)a, &s, &c); return (float)s; }
-static float FN(rcos)(float a) { double s, c; ol_sincos((double)a, &s, &c); return (float)c; }
+static float FN(rsin)(float a) { float s, c; ol_sincosf(a, &s, &c); return s; }
+static float FN(rcos)(float a) { float s, c; ol_sincosf(a, &s, &c); return c; }
 #else
 #define RPI   3.1415926535897932384626433832795
 #define RPI2  6.2831853071795864769252867665590

@@ -8,9 +8,10 @@
 //
 // Every multiply-add is an explicit fma in a fixed order and the file is
 // compiled with -fmad=false, and the transcendentals on the update path
-// (sin, cos, log) are this file's own double-precision routines, so a
-// sweep is a fixed sequence of IEEE operations: the CPU oracle that
-// performs the same sequence reproduces it bit for bit.
+// (sin, cos, log) are this file's own routines -- sin and cos in the link
+// precision, log in double as the reference promotes it -- so a sweep is a
+// fixed sequence of IEEE operations: the CPU oracle that performs the same
+// sequence reproduces it bit for bit.
 #pragma once
 #include <cuda_runtime.h>
 #include <stdint.h>
@@ -70,6 +71,36 @@ __device__ __forceinline__ void qg_sincos(double x, double *s, double *c)
     *c = cc;
 }
 
+// sin/cos in float for |x| < 1024 (the FP32 heatbath's float cos and
+// sincos, as the reference's float kernels evaluate them): Cody-Waite
+// reduction by pi/2 with a three-part float constant, Taylor polynomials of
+// degree 9 (sin) / 10 (cos) on [-pi/4, pi/4] in Horner form (truncation
+// below 2e-9, under the float rounding of the result)
+__device__ __forceinline__ void qg_sincosf(float x, float *s, float *c)
+{
+    const float INV_PIO2 = 0.6366197466850281f;
+    const float P1 = 1.5707963705062866f, P2 = -4.371138828673793e-08f, P3 = -1.7151245100058819e-15f;
+    const float n = rintf(x * INV_PIO2);
+    float f = fmaf(-n, P1, x);
+    f = fmaf(-n, P2, f);
+    f = fmaf(-n, P3, f);
+    const float f2 = f * f;
+    float ps = 2.7557318844628753e-06f;                 // 1/9!
+    ps = fmaf(ps, f2, -1.9841270113829523e-04f);         // -1/7!
+    ps = fmaf(ps, f2, 8.333333767950535e-03f);           // 1/5!
+    ps = fmaf(ps, f2, -1.666666716337204e-01f);          // -1/3!
+    const float sn = fmaf(ps * f2, f, f);
+    float pc = -2.755731998149713e-07f;                  // -1/10!
+    pc = fmaf(pc, f2, 2.4801587642286904e-05f);          // 1/8!
+    pc = fmaf(pc, f2, -1.3888889225199819e-03f);         // -1/6!
+    pc = fmaf(pc, f2, 4.16666679084301e-02f);            // 1/4!
+    pc = fmaf(pc, f2, -0.5f);
+    const float cs = fmaf(pc, f2, 1.0f);
+    const int q = ((int)n) & 3;
+    *s = (q == 0) ? sn : (q == 1) ? cs : (q == 2) ? -sn : -cs;
+    *c = (q == 0) ? cs : (q == 1) ? -sn : (q == 2) ? -cs : sn;
+}
+
 // natural log for 0 < y < 2^64: y = m 2^e with m in [sqrt(1/2), sqrt(2)),
 // log m = 2 atanh(s), s = (m-1)/(m+1), odd series to s^23; ln 2 in two parts
 __device__ __forceinline__ double qg_log(double y)
@@ -127,8 +158,8 @@ template <typename Real> struct RC;
 template <> struct RC<float> {
     static constexpr float PI = 3.141592653589793f;
     static constexpr float PI2 = 6.283185307179586f;
-    __device__ static float sn(float a) { double s, c; qg_sincos((double)a, &s, &c); return (float)s; }
-    __device__ static float cs(float a) { double s, c; qg_sincos((double)a, &s, &c); return (float)c; }
+    __device__ static float sn(float a) { float s, c; qg_sincosf(a, &s, &c); return s; }
+    __device__ static float cs(float a) { float s, c; qg_sincosf(a, &s, &c); return c; }
     __device__ static float sq(float a) { return sqrtf(a); }
 };
 template <> struct RC<double> {

@@ -170,6 +170,30 @@ def test_own_elementary_functions_accuracy():
         assert abs(a - b) <= 2 * np.spacing(abs(b)) + 1e-300, (y, a, b)
 
 
+def test_own_float_sincos_accuracy():
+    """The float sin/cos of the FP32 update path (heatbath cos(2 pi r) and
+    direction angles, hot start, twist factors): within 2 float ulp of the
+    exact value (or 1e-7 absolute near a zero), on the heatbath's arguments
+    float(2 pi) * r for r a multiple of 2^-24, on pi * r, and on [-100, 100]"""
+    lib = O.lib
+    for n in ("ol_sinf_own", "ol_cosf_own"):
+        getattr(lib, n).argtypes = [ctypes.c_float]
+        getattr(lib, n).restype = ctypes.c_float
+    rng = np.random.default_rng(1)
+    r = (np.floor(rng.uniform(0, 2 ** 24, 40000)) + 0.5).astype(np.float32) * np.float32(2.0 ** -24)
+    xs = np.concatenate([r * np.float32(6.283185307179586), r * np.float32(3.141592653589793),
+                         rng.uniform(-100, 100, 20000).astype(np.float32)])
+    worst = 0.0
+    for x in xs:
+        xd = float(np.float32(x))
+        for f, g in ((lib.ol_sinf_own, np.sin), (lib.ol_cosf_own, np.cos)):
+            a, b = float(f(xd)), float(g(xd))
+            tol = max(2 * float(np.spacing(np.float32(abs(b)))), 1e-7)
+            worst = max(worst, abs(a - b) / float(np.spacing(np.float32(max(abs(b), 1e-30)))))
+            assert abs(a - b) <= tol, (x, a, b)
+    print("worst float sin/cos error: %.2f ulp" % worst)
+
+
 # ---------------------------------------------- heatbath link by link
 HB_LINKS = np.load(os.path.join(os.path.dirname(__file__), "golden", "reference_heatbath_links.npz"))
 HB_CASES = [("su3_b6.0", 3, (4, 4, 2, 4), 6.0), ("su3_b1.5", 3, (4, 4, 2, 4), 1.5),
