@@ -326,8 +326,12 @@ int qg_plaquette_noalloc(const void *links, int group, int precision, const int 
 /* which no link of the phase changes: the proposal is symmetric and the   */
 /* chain exact for any weights.  Weights are BF16 in the kernels, FP32 for */
 /* the optimiser; the network is trained on the GPU to maximise the        */
-/* expected squared jump distance.  Layout of the QG_NET_PARAMS floats:     */
+/* expected squared jump distance.  Its layers run on the tcgen05 tensor   */
+/* cores (128 links per MMA, BF16 operands, FP32 accumulators in tensor    */
+/* memory), forward and backward.  Layout of the QG_NET_PARAMS floats:      */
 /* W1[32][8], b1[32], W2[32][32], b2[32], w3[32], b3.                       */
+/* The tensor-core waits are bounded: a wait that runs out makes the next  */
+/* qg_net_eps / qg_net_grad / qg_net_train / qg_mh_stats return QG_ERR_CUDA. */
 /* ===================================================================== */
 #define QG_NET_FEATURES 8
 #define QG_NET_HIDDEN 32
@@ -339,6 +343,11 @@ int qg_net_set(qg_ctx *ctx, const float *params, double eps_max);
 int qg_net_get(qg_ctx *ctx, float *master, float *weights_bf16);
 /* one Metropolis phase (parity, dir) with nhit hits per subgroup and link */
 int qg_mh_phase(qg_ctx *ctx, int parity, int dir, int nhit);
+/* the step eps of every link of phase (parity, dir) -- the values the next
+ * qg_mh_phase on the same field and weights uses -- into eps[sites/2], in
+ * the phase's link order (the t-th link of the (parity, dir) class); the
+ * field is not changed                                                     */
+int qg_net_eps(qg_ctx *ctx, int parity, int dir, float *eps);
 /* nsweeps sweeps of Metropolis phases in the heatbath's phase order, with
  * the global reunitarisation on qg_sweep's cadence                         */
 int qg_mh_sweep(qg_ctx *ctx, int nsweeps, int nhit);

@@ -101,8 +101,11 @@ void   ol_mh_features(const ol_cfg *c, const void *table, int gid, int mu, float
 float  ol_mlp_out(const float *w, const float x[8]);
 void   ol_mh_phase(const ol_cfg *c, void *table, int parity, int mu, const float *w, double eps_max, int nhit,
                    uint32_t key0, uint32_t key1, uint64_t phase, uint64_t *acc, double *jump);
+void   ol_mh_phase_eps(const ol_cfg *c, void *table, int parity, int mu, const float *eps, int nhit,
+                       uint32_t key0, uint32_t key1, uint64_t phase, uint64_t *acc, double *jump);
+void   ol_net_eps(const ol_cfg *c, const void *table, int parity, int mu, const float *w, double eps_max, float *eps);
 void   ol_mh_grad(const ol_cfg *c, const void *table, int parity, int mu, const float *w, double eps_max,
-                  uint32_t key0, uint32_t key1, uint64_t phase, double *grad, double stats[4]);
+                  uint32_t key0, uint32_t key1, uint64_t phase, int tc, double *grad, double stats[4]);
 double ol_mh_loss(const ol_cfg *c, const void *table, int parity, int mu, const double *w, double eps_max,
                   uint32_t key0, uint32_t key1, uint64_t phase);
 

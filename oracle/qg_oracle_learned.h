@@ -123,7 +123,46 @@ static void mh_features_f(const ol_cfg *c, const float *tab, unsigned g, int mu,
     x[7] = fmaf(qq[2], qq[2], fmaf(qq[1], qq[1], qq[0] * qq[0])) / 3.0f;
 }
 
-/* forward pass keeping the pre-activations; returns the output o */
+/* BF16 rounding (nearest even) of a finite float, as a float */
+static float bf16r(float f)
+{
+    uint32_t u;
+    memcpy(&u, &f, 4);
+    u += 0x7FFFu + ((u >> 16) & 1u);
+    u &= 0xFFFF0000u;
+    float r;
+    memcpy(&r, &u, 4);
+    return r;
+}
+
+/* forward pass as the tensor-core kernels define it (net_forward of
+ * qg_learned.cu): the features and the first hidden layer enter the
+ * products rounded to BF16, products and sums in FP32 (here summed in
+ * order; the tensor core sums in its own order), the bias added after the
+ * product, the output layer an FP32 dot product from b3 in order */
+static float mlp_fwd_tc_f(const float *w, const float x[NF], float z1[NH], float z2[NH])
+{
+    float xb[NF], h[NH];
+    for (int k = 0; k < NF; k++) xb[k] = bf16r(x[k]);
+    for (int j = 0; j < NH; j++) {
+        float z = 0.0f;
+        for (int k = 0; k < NF; k++) z = fmaf(xb[k], w[P_W1 + j * NF + k], z);
+        z1[j] = z + w[P_B1 + j];
+    }
+    for (int k = 0; k < NH; k++) h[k] = bf16r(z1[k] > 0.0f ? z1[k] : 0.0f);
+    float o = w[P_B3];
+    for (int j = 0; j < NH; j++) {
+        float z = 0.0f;
+        for (int k = 0; k < NH; k++) z = fmaf(h[k], w[P_W2 + j * NH + k], z);
+        z2[j] = z + w[P_B2 + j];
+        o = fmaf(w[P_W3 + j], z2[j] > 0.0f ? z2[j] : 0.0f, o);
+    }
+    return o;
+}
+
+/* the same network without the BF16 operand rounding (FP32 throughout),
+ * whose analytic gradient the finite-difference check compares with the
+ * FP64 loss */
 static float mlp_fwd_f(const float *w, const float x[NF], float z1[NH], float z2[NH])
 {
     for (int j = 0; j < NH; j++) {
@@ -177,13 +216,80 @@ void ol_mh_features(const ol_cfg *c, const void *tab, int gid, int mu, float x[N
 float ol_mlp_out(const float *w, const float x[NF])
 {
     float z1[NH], z2[NH];
-    return mlp_fwd_f(w, x, z1, z2);
+    return mlp_fwd_tc_f(w, x, z1, z2);
+}
+
+/* the step of every link of a phase (the GPU's qg_net_eps) */
+void ol_net_eps(const ol_cfg *c, const void *table, int parity, int mu, const float *w, double eps_max, float *eps)
+{
+    const float *tab = (const float *)table;
+    unsigned half = (unsigned)(sites_of(c) / 2);
+#pragma omp parallel for schedule(static)
+    for (unsigned t = 0; t < half; t++) {
+        unsigned g = parity ? odd_gid(c, t) : even_gid(c, t);
+        m3_f st;
+        float x[NF], z1[NH], z2[NH];
+        mh_features_f(c, tab, g, mu, &st, x);
+        eps[t] = (float)(eps_max * sigmoid_dd(mlp_fwd_tc_f(w, x, z1, z2)));
+    }
+}
+
+/* the Metropolis hits of link t of a phase with step eps (k_mh_phase after
+ * the network) */
+static void mh_link_f(const ol_cfg *c, float *tab, int parity, int mu, unsigned t, float eps, int nhit,
+                      const ol_prn *src, double bn, uint64_t *acc, double *jump)
+{
+    unsigned g = parity ? odd_gid(c, t) : even_gid(c, t);
+    crd co;
+    gid2c(c, g, &co);
+    m3_f st;
+    float x[NF];
+    mh_features_f(c, tab, g, mu, &st, x);
+    m3_f U = expand_f(load3_f(c, tab, &co, g, mu));
+    uint32_t k = 0;
+    for (int h = 0; h < nhit; h++)
+        for (int sg = 0; sg < 3; sg++) {
+            int i = (sg == 2) ? 1 : 0, j = (sg == 0) ? 1 : 2;
+            float q1[4], q2[4];
+            ol_philox_prn(src, t, k++, q1);
+            ol_philox_prn(src, t, k++, q2);
+            double a0, a1, a2;
+            normals3_f(q1, &a0, &a1, &a2);
+            double r = sqrt(fma(a2, a2, fma(a1, a1, a0 * a0)));
+            double th = (double)eps * r, sn, cs;
+            ol_sincos(th, &sn, &cs);
+            double sr = (r > 0.0) ? sn / r : 0.0;
+            float x0 = (float)cs, x1 = (float)(sr * a0), x2 = (float)(sr * a1), x3 = (float)(sr * a2);
+            double cc[4];
+            block_coeffs_f(&U, &st, i, j, cc);
+            double dS = -bn * fma((double)x0 - 1.0, cc[0], fma((double)x1, cc[1], fma((double)x2, cc[2], (double)x3 * cc[3])));
+            if (ol_log((double)q2[0]) <= -dS) {
+                s2_f V;
+                V.u1.re = x0; V.u1.im = x3; V.u2.re = x2; V.u2.im = x1;
+                V.v1.re = -x2; V.v1.im = x1; V.v2.re = x0; V.v2.im = -x3;
+                rotate_rows_f(&U, i, j, &V);
+                (*acc)++;
+                *jump += th * th;
+            }
+        }
+    store3_f(c, tab, g, mu, gs3_f(compress_f(&U)));
 }
 
 /* one learned-proposal Metropolis phase (k_mh_phase); w holds the BF16
- * weights as floats */
+ * weights as floats, the network as the tensor-core kernels define it */
 void ol_mh_phase(const ol_cfg *c, void *table, int parity, int mu, const float *w, double eps_max, int nhit,
                  uint32_t key0, uint32_t key1, uint64_t phase, uint64_t *acc_out, double *jump_out)
+{
+    unsigned half = (unsigned)(sites_of(c) / 2);
+    float *eps = (float *)malloc((size_t)half * sizeof(float));
+    ol_net_eps(c, table, parity, mu, w, eps_max, eps);
+    ol_mh_phase_eps(c, table, parity, mu, eps, nhit, key0, key1, phase, acc_out, jump_out);
+    free(eps);
+}
+
+/* the same phase with the step of link t given as eps[t] */
+void ol_mh_phase_eps(const ol_cfg *c, void *table, int parity, int mu, const float *eps, int nhit, uint32_t key0,
+                     uint32_t key1, uint64_t phase, uint64_t *acc_out, double *jump_out)
 {
     float *tab = (float *)table;
     unsigned half = (unsigned)(sites_of(c) / 2);
@@ -196,43 +302,7 @@ void ol_mh_phase(const ol_cfg *c, void *table, int parity, int mu, const float *
     /* links updated independently; the jump sum's order differs with the
      * thread count (it is a statistic, compared within a tolerance) */
 #pragma omp parallel for schedule(static) reduction(+ : acc, jump)
-    for (unsigned t = 0; t < half; t++) {
-        unsigned g = parity ? odd_gid(c, t) : even_gid(c, t);
-        crd co;
-        gid2c(c, g, &co);
-        m3_f st;
-        float x[NF], z1[NH], z2[NH];
-        mh_features_f(c, tab, g, mu, &st, x);
-        float eps = (float)(eps_max * sigmoid_dd(mlp_fwd_f(w, x, z1, z2)));
-        m3_f U = expand_f(load3_f(c, tab, &co, g, mu));
-        uint32_t k = 0;
-        for (int h = 0; h < nhit; h++)
-            for (int sg = 0; sg < 3; sg++) {
-                int i = (sg == 2) ? 1 : 0, j = (sg == 0) ? 1 : 2;
-                float q1[4], q2[4];
-                ol_philox_prn(&src, t, k++, q1);
-                ol_philox_prn(&src, t, k++, q2);
-                double a0, a1, a2;
-                normals3_f(q1, &a0, &a1, &a2);
-                double r = sqrt(fma(a2, a2, fma(a1, a1, a0 * a0)));
-                double th = (double)eps * r, sn, cs;
-                ol_sincos(th, &sn, &cs);
-                double sr = (r > 0.0) ? sn / r : 0.0;
-                float x0 = (float)cs, x1 = (float)(sr * a0), x2 = (float)(sr * a1), x3 = (float)(sr * a2);
-                double cc[4];
-                block_coeffs_f(&U, &st, i, j, cc);
-                double dS = -bn * fma((double)x0 - 1.0, cc[0], fma((double)x1, cc[1], fma((double)x2, cc[2], (double)x3 * cc[3])));
-                if (ol_log((double)q2[0]) <= -dS) {
-                    s2_f V;
-                    V.u1.re = x0; V.u1.im = x3; V.u2.re = x2; V.u2.im = x1;
-                    V.v1.re = -x2; V.v1.im = x1; V.v2.re = x0; V.v2.im = -x3;
-                    rotate_rows_f(&U, i, j, &V);
-                    acc++;
-                    jump += th * th;
-                }
-            }
-        store3_f(c, tab, g, mu, gs3_f(compress_f(&U)));
-    }
+    for (unsigned t = 0; t < half; t++) mh_link_f(c, tab, parity, mu, t, eps[t], nhit, &src, bn, &acc, &jump);
     if (acc_out) *acc_out = acc;
     if (jump_out) *jump_out = jump;
 }
@@ -240,9 +310,12 @@ void ol_mh_phase(const ol_cfg *c, void *table, int parity, int mu, const float *
 /* the training loss gradient of one phase (k_mh_grad + k_mh_grad_reduce):
  * per-link arithmetic as on the GPU (FP32 network, FP64 acceptance), the
  * sums over links in FP64; grad[NPAR] = mean over links, stats = {loss,
- * ESJD, acceptance} per link and the link count */
+ * ESJD, acceptance} per link and the link count.  tc = 1: the network and
+ * the back-propagated values rounded to BF16 where the tensor-core kernels
+ * round them (the features, h1, h2, dz2, dz1 and dL/do as MMA operands);
+ * tc = 0: FP32 throughout (the analytic gradient of the FP32 network) */
 void ol_mh_grad(const ol_cfg *c, const void *table, int parity, int mu, const float *w, double eps_max,
-                uint32_t key0, uint32_t key1, uint64_t phase, double *grad, double stats[4])
+                uint32_t key0, uint32_t key1, uint64_t phase, int tc, double *grad, double stats[4])
 {
     const float *tab = (const float *)table;
     unsigned half = (unsigned)(sites_of(c) / 2);
@@ -259,7 +332,7 @@ void ol_mh_grad(const ol_cfg *c, const void *table, int parity, int mu, const fl
         m3_f st;
         float x[NF], z1[NH], z2[NH];
         mh_features_f(c, tab, g, mu, &st, x);
-        float o = mlp_fwd_f(w, x, z1, z2);
+        float o = tc ? mlp_fwd_tc_f(w, x, z1, z2) : mlp_fwd_f(w, x, z1, z2);
         double sg = sigmoid_dd(o), eps = eps_max * sg;
         m3_f U = expand_f(load3_f(c, tab, &co, g, mu));
         double geps = 0, es = 0, ac = 0;
@@ -287,23 +360,28 @@ void ol_mh_grad(const ol_cfg *c, const void *table, int parity, int mu, const fl
         se += es;
         sa += ac / 3.0;
         float go = (float)(geps * eps_max * sg * (1.0 - sg));
-        float dz2[NH], h1[NH];
+        float dz2[NH], h1[NH], h2[NH], xo[NF];
         for (int jj = 0; jj < NH; jj++) {
             h1[jj] = z1[jj] > 0.0f ? z1[jj] : 0.0f;
+            h2[jj] = z2[jj] > 0.0f ? z2[jj] : 0.0f;
             dz2[jj] = z2[jj] > 0.0f ? go * w[P_W3 + jj] : 0.0f;
+            if (tc) { h1[jj] = bf16r(h1[jj]); h2[jj] = bf16r(h2[jj]); dz2[jj] = bf16r(dz2[jj]); }
         }
+        for (int m = 0; m < NF; m++) xo[m] = tc ? bf16r(x[m]) : x[m];
+        const float gq = tc ? bf16r(go) : go;
         for (int jj = 0; jj < NH; jj++) {
-            grad[P_W3 + jj] += (double)go * (double)(z2[jj] > 0.0f ? z2[jj] : 0.0f);
+            grad[P_W3 + jj] += (double)gq * (double)h2[jj];
             grad[P_B2 + jj] += (double)dz2[jj];
             for (int k = 0; k < NH; k++) grad[P_W2 + jj * NH + k] += (double)dz2[jj] * (double)h1[k];
         }
-        grad[P_B3] += (double)go;
+        grad[P_B3] += (double)gq;
         for (int k = 0; k < NH; k++) {
             float d = 0.0f;
             for (int jj = 0; jj < NH; jj++) d = fmaf(w[P_W2 + jj * NH + k], dz2[jj], d);
-            float dz1 = h1[k] > 0.0f ? d : 0.0f;
+            float dz1 = z1[k] > 0.0f ? d : 0.0f;
+            if (tc) dz1 = bf16r(dz1);
             grad[P_B1 + k] += (double)dz1;
-            for (int m = 0; m < NF; m++) grad[P_W1 + k * NF + m] += (double)dz1 * (double)x[m];
+            for (int m = 0; m < NF; m++) grad[P_W1 + k * NF + m] += (double)dz1 * (double)xo[m];
         }
     }
     for (int q = 0; q < NPAR; q++) grad[q] /= (double)half;

@@ -48,7 +48,8 @@ EXPORTED_SYMBOLS = (
     "qg_batch_set_shapes", "qg_batch_get_shapes", "qg_batch_tune",
     "qg_measure_wilson_all", "qg_measure_fmunu", "qg_measure_action_profile", "qg_measure_polyakov_profile",
     "qg_measure_enqueue", "qg_measure_fetch", "qg_measure_plaquette_all", "qg_measure_polyakov_all",
-    "qg_net_set", "qg_net_get", "qg_mh_phase", "qg_mh_sweep", "qg_mh_stats", "qg_net_grad", "qg_net_train",
+    "qg_net_set", "qg_net_get", "qg_mh_phase", "qg_net_eps", "qg_mh_sweep", "qg_mh_stats", "qg_net_grad",
+    "qg_net_train",
 )
 
 
@@ -253,6 +254,7 @@ def load_library(path=LIB_PATH):
     lib.qg_net_set.argtypes = [vp, fp, ctypes.c_double]
     lib.qg_net_get.argtypes = [vp, fp, fp]
     lib.qg_mh_phase.argtypes = [vp, ctypes.c_int, ctypes.c_int, ctypes.c_int]
+    lib.qg_net_eps.argtypes = [vp, ctypes.c_int, ctypes.c_int, fp]
     lib.qg_mh_sweep.argtypes = [vp, ctypes.c_int, ctypes.c_int]
     lib.qg_mh_stats.argtypes = [vp, P(ctypes.c_double), P(ctypes.c_double), P(ctypes.c_uint64), ctypes.c_int]
     lib.qg_net_grad.argtypes = [vp, ctypes.c_int, ctypes.c_int, fp, P(ctypes.c_double)]
@@ -585,6 +587,14 @@ class Lattice:
 
     def mh_phase(self, parity, direction, nhit=1):
         self._ck(self.lib.qg_mh_phase(self.ctx, parity, direction, nhit), "qg_mh_phase")
+
+    def net_eps(self, parity, direction):
+        """the step eps of every link of phase (parity, direction) that the
+        next mh_phase uses (the field is not changed)"""
+        e = np.zeros(self.info().sites // 2, dtype=np.float32)
+        self._ck(self.lib.qg_net_eps(self.ctx, parity, direction, e.ctypes.data_as(ctypes.POINTER(ctypes.c_float))),
+                 "qg_net_eps")
+        return e
 
     def mh_sweep(self, n=1, nhit=1):
         self._ck(self.lib.qg_mh_sweep(self.ctx, n, nhit), "qg_mh_sweep")

@@ -79,6 +79,8 @@ struct qg_ctx {
     double *d_sites = nullptr;      // per-site values of the one-pass measurements (lazy)
     unsigned long long *d_mh_acc = nullptr;
     double *d_mh_jump = nullptr;
+    unsigned *d_net_err = nullptr;  // set by the network kernels when a tensor-core wait runs out
+    float *d_eps = nullptr;         // per-link steps of qg_net_eps (lazy)
     double eps_max = 0.0;
     int adam_t = 0;
     uint64_t train_phase = 0, mh_hits = 0;
@@ -226,6 +228,7 @@ extern "C" int qg_destroy(qg_ctx *c)
     cudaFree(c->partials); cudaFree(c->d_results); cudaFree(c->d_phase); cudaFree(c->d_params);
     cudaFree(c->d_netw); cudaFree(c->d_master); cudaFree(c->d_adam_m); cudaFree(c->d_adam_v);
     cudaFree(c->d_grad); cudaFree(c->d_gpart); cudaFree(c->d_mh_acc); cudaFree(c->d_mh_jump);
+    cudaFree(c->d_net_err); cudaFree(c->d_eps);
     cudaFree(c->d_wpart); cudaFree(c->d_wout);
     cudaFree(c->d_fpart); cudaFree(c->d_ppart); cudaFree(c->d_pout); cudaFree(c->d_sites);
     cudaFree(c->d_bad);
@@ -1031,6 +1034,8 @@ extern "C" int qg_net_set(qg_ctx *c, const float *params, double eps_max)
         QG_CK(cudaMalloc(&c->d_gpart, (size_t)mh_grad_blocks(c->G) * (np + 4) * sizeof(float)), "net alloc");
         QG_CK(cudaMalloc(&c->d_mh_acc, sizeof(unsigned long long)), "net alloc");
         QG_CK(cudaMalloc(&c->d_mh_jump, sizeof(double)), "net alloc");
+        QG_CK(cudaMalloc(&c->d_net_err, sizeof(unsigned)), "net alloc");
+        QG_CK(cudaMemsetAsync(c->d_net_err, 0, sizeof(unsigned), c->stream), "net clear");
         QG_CK(cudaMemsetAsync(c->d_mh_acc, 0, sizeof(unsigned long long), c->stream), "net clear");
         QG_CK(cudaMemsetAsync(c->d_mh_jump, 0, sizeof(double), c->stream), "net clear");
     }
@@ -1070,10 +1075,41 @@ static int mh_ready(qg_ctx *c)
     return QG_OK;
 }
 
-static cudaError_t mh_launch(qg_ctx *c, int parity, int dir, int nhit, uint32_t offset)
+static cudaError_t mh_launch(qg_ctx *c, int parity, int dir, int nhit, uint32_t offset, float *eps_out = nullptr)
 {
     PhaseArgs a = phase_args(c, parity, dir, QG_UPDATE_HEATBATH, offset);
-    return launch_mh_phase(c->G, c->links, a, c->d_netw, c->eps_max, nhit, c->d_mh_acc, c->d_mh_jump, c->stream);
+    return launch_mh_phase(c->G, c->links, a, c->d_netw, c->eps_max, nhit, c->d_mh_acc, c->d_mh_jump, eps_out,
+                           c->d_net_err, c->stream);
+}
+
+// the tensor-core waits of the network kernels are bounded; a wait that
+// ran out is reported here (the call that observes it fails, the flag is
+// cleared)
+static int net_err_check(qg_ctx *c)
+{
+    unsigned flag = 0;
+    QG_CK(cudaMemcpyAsync(&flag, c->d_net_err, sizeof(flag), cudaMemcpyDeviceToHost, c->stream), "net flag");
+    QG_CK(cudaStreamSynchronize(c->stream), "net flag sync");
+    if (flag) {
+        QG_CK(cudaMemsetAsync(c->d_net_err, 0, sizeof(unsigned), c->stream), "net flag clear");
+        return fail(c, QG_ERR_CUDA, "a tensor-core wait of the network kernels ran out");
+    }
+    return QG_OK;
+}
+
+// the step eps of every link of phase (parity, dir) as the next qg_mh_phase
+// on the same field and weights computes it (thread order, G.half values)
+extern "C" int qg_net_eps(qg_ctx *c, int parity, int dir, float *eps)
+{
+    if (!c || !eps) return QG_ERR_ARG;
+    if (parity < 0 || parity > 1 || dir < 0 || dir > 3) return fail(c, QG_ERR_ARG, "bad phase");
+    int r = mh_ready(c);
+    if (r) return r;
+    if (!c->d_eps) QG_CK(cudaMalloc(&c->d_eps, (size_t)c->G.half * sizeof(float)), "eps alloc");
+    QG_CK(mh_launch(c, parity, dir, 1, 0, c->d_eps), "net eps");
+    QG_CK(cudaMemcpyAsync(eps, c->d_eps, (size_t)c->G.half * sizeof(float), cudaMemcpyDeviceToHost, c->stream),
+          "eps copy");
+    return net_err_check(c);
 }
 
 extern "C" int qg_mh_phase(qg_ctx *c, int parity, int dir, int nhit)
@@ -1126,6 +1162,10 @@ extern "C" int qg_mh_stats(qg_ctx *c, double *accept_rate, double *jump_per_hit,
         QG_CK(cudaMemcpyAsync(&jump, c->d_mh_jump, sizeof(jump), cudaMemcpyDeviceToHost, c->stream), "stats");
         QG_CK(cudaStreamSynchronize(c->stream), "stats sync");
     }
+    if (c->d_net_err) {
+        int r = net_err_check(c);
+        if (r) return r;
+    }
     const double h = (double)c->mh_hits;
     if (accept_rate) *accept_rate = h > 0 ? (double)acc / h : 0.0;
     if (jump_per_hit) *jump_per_hit = h > 0 ? jump / h : 0.0;
@@ -1147,11 +1187,14 @@ extern "C" int qg_net_grad(qg_ctx *c, int parity, int dir, float *grad, double *
     int r = mh_ready(c);
     if (r) return r;
     QG_CK(launch_mh_grad(c->G, c->links, parity, dir, c->d_params, c->d_netw, c->eps_max,
-                         make_uint2(c->cfg.randseries, kTrainKey), c->train_phase++, c->d_gpart, c->d_grad, c->stream),
+                         make_uint2(c->cfg.randseries, kTrainKey), c->train_phase++, c->d_gpart, c->d_grad,
+                         c->d_net_err, c->stream),
           "net grad");
     std::vector<float> h(QG_NET_PARAMS + 4);
     QG_CK(cudaMemcpyAsync(h.data(), c->d_grad, h.size() * sizeof(float), cudaMemcpyDeviceToHost, c->stream), "grad copy");
     QG_CK(cudaStreamSynchronize(c->stream), "grad sync");
+    r = net_err_check(c);
+    if (r) return r;
     if (grad) memcpy(grad, h.data(), QG_NET_PARAMS * sizeof(float));
     if (stats) {
         const double n = h[QG_NET_PARAMS + 3] > 0 ? h[QG_NET_PARAMS + 3] : 1.0;
@@ -1179,7 +1222,7 @@ extern "C" int qg_net_train(qg_ctx *c, int steps, double lr, double *stats)
         const int k = s % 8;
         QG_CK(launch_mh_grad(c->G, c->links, par_order[k / 4], k % 4, c->d_params, c->d_netw, c->eps_max,
                              make_uint2(c->cfg.randseries, kTrainKey), c->train_phase++, c->d_gpart, c->d_grad,
-                             c->stream), "net grad");
+                             c->d_net_err, c->stream), "net grad");
         c->adam_t++;
         const float b1 = 0.9f, b2 = 0.999f;
         const float c1 = 1.0f - powf(b1, (float)c->adam_t), c2 = 1.0f - powf(b2, (float)c->adam_t);
@@ -1198,7 +1241,7 @@ extern "C" int qg_net_train(qg_ctx *c, int steps, double lr, double *stats)
     }
     if (stats)
         for (int k = 0; k < 4; k++) stats[k] = steps > 0 ? acc[k] / steps : 0.0;
-    return QG_OK;
+    return net_err_check(c);
 }
 
 static int measure_to_host(qg_ctx *c, int ncomp, double *out)

@@ -108,12 +108,15 @@ cudaError_t launch_ranlux_produce(float4 *table, float4 *prns, int instances, in
 Geom make_geom(const int n[4]);
 
 // learned-proposal Metropolis (qg_learned.cu)
+// eps_out non-null: only the per-link step into eps_out (no update); err:
+// set when a tensor-core wait ran out
 cudaError_t launch_mh_phase(const Geom &G, void *links, const PhaseArgs &a, const uint16_t *wq, double eps_max,
-                            int nhit, unsigned long long *acc_count, double *jump_sum, cudaStream_t s);
+                            int nhit, unsigned long long *acc_count, double *jump_sum, float *eps_out, unsigned *err,
+                            cudaStream_t s);
 uint32_t mh_grad_blocks(const Geom &G);
 cudaError_t launch_mh_grad(const Geom &G, const void *links, int parity, int dir, const double *params,
                            const uint16_t *wq, double eps_max, uint2 key, uint64_t phase, float *partials,
-                           float *grad, cudaStream_t s);
+                           float *grad, unsigned *err, cudaStream_t s);
 cudaError_t launch_adam(float *master, float *m, float *v, const float *grad, uint16_t *wq, float lr, float b1,
                         float b2, float c1, float c2, float epsa, cudaStream_t s);
 cudaError_t launch_to_bf16(const float *master, uint16_t *wq, cudaStream_t s);

@@ -17,11 +17,24 @@
 // Training maximises the expected squared jump distance
 // E[min(1, exp(-dS)) (eps |a|)^2] per subgroup proposal from the current
 // link; its derivative in eps is analytic, and the network's backward pass,
-// the block sums of the weight gradients (fixed order, deterministic) and
-// the Adam step are kernels here.  Weights are stored in BF16 for the
-// kernels and in FP32 for the optimiser; all sums accumulate in FP32 (the
-// per-link acceptance arithmetic in FP64).
+// the block sums of the weight gradients and the Adam step are kernels
+// here.  Weights are stored in BF16 for the kernels and in FP32 for the
+// optimiser; the per-link acceptance arithmetic is FP64.
+//
+// Tensor cores.  The network runs on the fifth-generation tensor cores
+// (tcgen05, qg_tc.cuh): a CTA of 128 threads holds 128 links, the MMA's M
+// rows.  Forward: the features (BF16, K = 16 with 8 zero columns) times W1
+// (N = 32) accumulate in FP32 in tensor memory; each thread reads its link's
+// row back (tcgen05.ld), adds the bias, applies the ReLU and stores the
+// hidden layer as BF16 for the second MMA (K = 32, N = 32); the output layer
+// (32 -> 1) is an FP32 dot product in the thread.  Training adds two MMAs:
+// the back-propagated dz1 = W2^T dz2 per link (M = 128 links, N = 32, K = 32)
+// and all weight and bias gradients of the block in one product over the
+// link dimension (M = 128 rows [dz2^T; dz1^T; dL/do], N = 80 columns
+// [h1^T; h2^T; x^T; 1], K = 128 links).  Activations and back-propagated
+// values enter the MMAs rounded to BF16; products and sums are FP32.
 #include "qg_internal.h"
+#include "qg_tc.cuh"
 #include "qg_update.cuh"
 
 namespace qg {
@@ -30,7 +43,6 @@ constexpr int kNF = QG_NET_FEATURES, kNH = QG_NET_HIDDEN;
 constexpr int kW1 = 0, kB1 = kW1 + kNH * kNF, kW2 = kB1 + kNH, kB2 = kW2 + kNH * kNH, kW3 = kB2 + kNH,
               kB3 = kW3 + kNH, kNP = kB3 + 1;
 static_assert(kNP == QG_NET_PARAMS, "parameter count");
-constexpr int kTrainBlock = 64;
 
 __device__ __forceinline__ float bf16_bits_to_float(uint16_t b) { return __uint_as_float((uint32_t)b << 16); }
 // round to nearest even (finite inputs)
@@ -142,25 +154,139 @@ __device__ __forceinline__ void staple_features(const Field<float> &U, const Geo
     x[7] = FMA(qq[2], qq[2], FMA(qq[1], qq[1], qq[0] * qq[0])) / 3.0f;
 }
 
-// the network's output o (weights w in shared memory, FP32)
-__device__ __forceinline__ float mlp_out(const float *w, const float (&x)[kNF])
+constexpr int kMHBlock = 128;                  // links per CTA = the MMA's M
+constexpr uint32_t kWaitPolls = 1u << 22;       // mbarrier polls before a wait gives up
+constexpr uint32_t kIdesc32 = tc::idesc_bf16_f32(128, 32), kIdesc80 = tc::idesc_bf16_f32(128, 80);
+constexpr int kGN = 80;                         // columns of the weight-gradient MMA
+constexpr uint16_t kBF16One = 0x3F80u;
+
+// the network's operands in shared memory (tcgen05 K-major layout)
+struct NetOps {
+    alignas(128) uint8_t a1[kMHBlock * 16 * 2];   // features, BF16, K = 16 (columns 8..15 zero)
+    alignas(128) uint8_t a2[kMHBlock * 32 * 2];   // hidden layer 1 (training: then dz2), BF16, K = 32
+    alignas(128) uint8_t b1[kNH * 16 * 2];        // W1[j][k], K = 16
+    alignas(128) uint8_t b2[kNH * kNH * 2];       // W2[j][k], K = 32
+    float bias1[kNH], bias2[kNH], w3[kNH], b3;
+    uint64_t mbar;
+    uint32_t tmem;
+};
+// the training kernel's extra operands
+struct GradOps {
+    alignas(128) uint8_t b2t[kNH * kNH * 2];      // W2^T: [k][j], K = 32
+    alignas(128) uint8_t ga[128 * kMHBlock * 2];  // rows: dz2^T (0..31), dz1^T (32..63), dL/do (64), 0; K = links
+    alignas(128) uint8_t gb[kGN * kMHBlock * 2];  // rows: h1^T (0..31), h2^T (32..63), x^T (64..71), 1 (72), 0
+    float sst[kMHBlock][4];
+};
+
+__device__ __forceinline__ void st_bf16(uint8_t *base, uint32_t off, uint16_t v)
 {
-    float h1[kNH];
+    *reinterpret_cast<uint16_t *>(base + off) = v;
+}
+// 8 floats as BF16 into one 16-byte chunk (row m, columns c .. c+7)
+__device__ __forceinline__ void st_bf16x8(uint8_t *base, uint32_t off, const float *v)
+{
+    uint4 q;
+    q.x = (uint32_t)float_to_bf16_bits(v[0]) | ((uint32_t)float_to_bf16_bits(v[1]) << 16);
+    q.y = (uint32_t)float_to_bf16_bits(v[2]) | ((uint32_t)float_to_bf16_bits(v[3]) << 16);
+    q.z = (uint32_t)float_to_bf16_bits(v[4]) | ((uint32_t)float_to_bf16_bits(v[5]) << 16);
+    q.w = (uint32_t)float_to_bf16_bits(v[6]) | ((uint32_t)float_to_bf16_bits(v[7]) << 16);
+    *reinterpret_cast<uint4 *>(base + off) = q;
+}
+
+// weights into the operand layout, the mbarrier, ncols TMEM columns
+__device__ __forceinline__ void net_setup(NetOps &S, const uint16_t *wq, uint32_t ncols)
+{
+    for (int i = threadIdx.x; i < kNH * 16; i += blockDim.x) {
+        const int j = i >> 4, k = i & 15;
+        st_bf16(S.b1, tc::kmajor_off(j, k, 16), k < kNF ? wq[kW1 + j * kNF + k] : (uint16_t)0);
+    }
+    for (int i = threadIdx.x; i < kNH * kNH; i += blockDim.x) {
+        const int j = i >> 5, k = i & 31;
+        st_bf16(S.b2, tc::kmajor_off(j, k, 32), wq[kW2 + j * kNH + k]);
+    }
+    for (int i = threadIdx.x; i < kNH; i += blockDim.x) {
+        S.bias1[i] = bf16_bits_to_float(wq[kB1 + i]);
+        S.bias2[i] = bf16_bits_to_float(wq[kB2 + i]);
+        S.w3[i] = bf16_bits_to_float(wq[kW3 + i]);
+    }
+    if (threadIdx.x == 0) {
+        S.b3 = bf16_bits_to_float(wq[kB3]);
+        tc::mbar_init(&S.mbar, 1);
+    }
+    if (threadIdx.x < 32) tc::tmem_alloc(&S.tmem, ncols);
+}
+// all threads: make the generic shared-memory writes visible to the tensor
+// core, order them (and earlier TMEM reads) before the next MMA
+__device__ __forceinline__ void net_sync()
+{
+    tc::fence_async_shared();
+    tc::fence_before_sync();
+    __syncthreads();
+    tc::fence_after_sync();
+}
+// all threads: wait for the committed MMAs; false (block-uniform) if the
+// wait ran out
+__device__ __forceinline__ bool net_wait(NetOps &S, uint32_t &phase)
+{
+    const bool ok = tc::mbar_wait(&S.mbar, phase, kWaitPolls);
+    phase ^= 1u;
+    const int bad = __syncthreads_or(!ok);
+    tc::fence_after_sync();
+    return !bad;
+}
+__device__ __forceinline__ void net_teardown(NetOps &S, uint32_t ncols, bool ok, uint32_t phase)
+{
+    if (!ok) tc::mbar_wait(&S.mbar, phase, kWaitPolls);      // let a late MMA land before the free
+    tc::fence_before_sync();
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        tc::fence_after_sync();
+        tc::tmem_free(S.tmem, ncols);
+    }
+}
+
+// the network for the CTA's 128 links: thread m's features x -> the
+// pre-activations z1, z2 and the output o of its link
+__device__ __forceinline__ bool net_forward(NetOps &S, uint32_t &phase, const float (&x)[kNF], float (&z1)[kNH],
+                                            float (&z2)[kNH], float &o)
+{
+    const int m = threadIdx.x;
+    const float zero8[8] = { 0, 0, 0, 0, 0, 0, 0, 0 };
+    st_bf16x8(S.a1, tc::kmajor_off(m, 0, 16), x);
+    st_bf16x8(S.a1, tc::kmajor_off(m, 8, 16), zero8);
+    net_sync();                                  // also publishes the TMEM address and the mbarrier
+    const uint32_t lane_base = S.tmem + ((uint32_t)(m & ~31) << 16);
+    if (m == 0) {
+        tc::mma_bf16(S.tmem, tc::desc_operand(S.a1, 16, 0), tc::desc_operand(S.b1, 16, 0), kIdesc32, 0);
+        tc::mma_commit(&S.mbar);
+    }
+    if (!net_wait(S, phase)) return false;
+    float acc[32];
+    tc::tmem_ld32(lane_base, acc);
+    float h[kNH];
 #pragma unroll
     for (int j = 0; j < kNH; j++) {
-        float z = w[kB1 + j];
-#pragma unroll
-        for (int k = 0; k < kNF; k++) z = FMA(w[kW1 + j * kNF + k], x[k], z);
-        h1[j] = z > 0.0f ? z : 0.0f;
+        z1[j] = acc[j] + S.bias1[j];
+        h[j] = z1[j] > 0.0f ? z1[j] : 0.0f;
     }
-    float o = w[kB3];
+#pragma unroll
+    for (int c = 0; c < 4; c++) st_bf16x8(S.a2, tc::kmajor_off(m, 8 * c, 32), h + 8 * c);
+    net_sync();
+    if (m == 0) {
+        tc::mma_bf16(S.tmem, tc::desc_operand(S.a2, 32, 0), tc::desc_operand(S.b2, 32, 0), kIdesc32, 0);
+        tc::mma_bf16(S.tmem, tc::desc_operand(S.a2, 32, 16), tc::desc_operand(S.b2, 32, 16), kIdesc32, 1);
+        tc::mma_commit(&S.mbar);
+    }
+    if (!net_wait(S, phase)) return false;
+    tc::tmem_ld32(lane_base, acc);
+    float out = S.b3;
+#pragma unroll
     for (int j = 0; j < kNH; j++) {
-        float z = w[kB2 + j];
-#pragma unroll
-        for (int k = 0; k < kNH; k++) z = FMA(w[kW2 + j * kNH + k], h1[k], z);
-        o = FMA(w[kW3 + j], z > 0.0f ? z : 0.0f, o);
+        z2[j] = acc[j] + S.bias2[j];
+        out = FMA(S.w3[j], z2[j] > 0.0f ? z2[j] : 0.0f, out);
     }
-    return o;
+    o = out;
+    return true;
 }
 
 __device__ __forceinline__ double sigmoid_d(float o) { return 1.0 / (1.0 + qg_exp(-(double)o)); }
@@ -207,32 +333,48 @@ __device__ __forceinline__ S2<float> w_block(const CX<float> (&ri)[3], const CX<
     return w;
 }
 
-template <int mu>
-__global__ void __launch_bounds__(128) k_mh_phase(Field<float> U, Geom G, PhaseArgs A, const uint16_t *wq,
-                                                  double eps_max, int nhit, unsigned long long *acc_count,
-                                                  double *jump_sum)
+// One Metropolis phase; EPS_ONLY: only the step eps of every link of the
+// phase into eps_out[t] (the same arithmetic up to eps, the field untouched)
+template <int mu, bool EPS_ONLY>
+__global__ void __launch_bounds__(kMHBlock) k_mh_phase(Field<float> U, Geom G, PhaseArgs A, const uint16_t *wq,
+                                                       double eps_max, int nhit, unsigned long long *acc_count,
+                                                       double *jump_sum, float *eps_out, unsigned *err)
 {
-    __shared__ float w[kNP];
-    for (int i = threadIdx.x; i < kNP; i += blockDim.x) w[i] = bf16_bits_to_float(wq[i]);
-    __syncthreads();
-    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    __shared__ NetOps S;
+    net_setup(S, wq, 32);
+    const uint32_t t = blockIdx.x * kMHBlock + threadIdx.x;
+    const bool active = t < G.half;
+    const int p = A.parity;
+    Crd c = lex2crd(G, 2 * (active ? t : 0));
+    if (parity_of(c) != p) c.y += 1;
+    const uint32_t e0 = (uint32_t)p * G.cb + t;
+    const Nbr nb = neighbours(G, c);
+    M3<float> st;
+    float x[kNF];
+#pragma unroll
+    for (int k = 0; k < kNF; k++) x[k] = 0.0f;
+    if (active) staple_features<mu>(U, G, t, nb, p, st, x);
+    uint32_t phase = 0;
+    float z1[kNH], z2[kNH], o = 0.0f;
+    const bool ok = net_forward(S, phase, x, z1, z2, o);
+    net_teardown(S, 32, ok, phase);
+    if (!ok) {
+        if (threadIdx.x == 0) atomicOr(err, 1u);
+        return;
+    }
+    const float eps = (float)(eps_max * sigmoid_d(o));
+    if (EPS_ONLY) {
+        if (active) eps_out[t] = eps;
+        return;
+    }
     unsigned acc = 0;
     double jump = 0.0;
-    if (t < G.half) {
-        const int p = A.parity;
-        Crd c = lex2crd(G, 2 * t);
-        if (parity_of(c) != p) c.y += 1;
-        const uint32_t e0 = (uint32_t)p * G.cb + t;
-        const Nbr nb = neighbours(G, c);
+    if (active) {
         const double bn = (double)(float)A.params[0];          // (float)(BETA/N), as the heatbath
-        M3<float> st;
-        float x[kNF];
-        staple_features<mu>(U, G, t, nb, p, st, x);
-        const float eps = (float)(eps_max * sigmoid_d(mlp_out(w, x)));
         M3<float> Um = expand(U.ld3(mu, e0));
-        const uint64_t phase = *A.phase_base + A.phase_offset;
+        const uint64_t ph = *A.phase_base + A.phase_offset;
         PrnPhilox<float> prn;
-        prn.key = A.key; prn.t = t; prn.k = 0; prn.plo = (uint32_t)phase; prn.phi = (uint32_t)(phase >> 32);
+        prn.key = A.key; prn.t = t; prn.k = 0; prn.plo = (uint32_t)ph; prn.phi = (uint32_t)(ph >> 32);
         for (int h = 0; h < nhit; h++) {
 #pragma unroll 1
             for (int sg = 0; sg < 3; sg++) {
@@ -275,9 +417,9 @@ __global__ void __launch_bounds__(128) k_mh_phase(Field<float> U, Geom G, PhaseA
         }
         U.st3(mu, e0, gs3<float>(compress(Um)));
     }
-    for (int o = 16; o > 0; o >>= 1) {
-        acc += __shfl_down_sync(0xffffffffu, acc, o);
-        jump += __shfl_down_sync(0xffffffffu, jump, o);
+    for (int ofs = 16; ofs > 0; ofs >>= 1) {
+        acc += __shfl_down_sync(0xffffffffu, acc, ofs);
+        jump += __shfl_down_sync(0xffffffffu, jump, ofs);
     }
     if ((threadIdx.x & 31) == 0 && acc_count) {
         atomicAdd(acc_count, (unsigned long long)acc);
@@ -288,57 +430,59 @@ __global__ void __launch_bounds__(128) k_mh_phase(Field<float> U, Geom G, PhaseA
 // Gradient of the loss L = -(1/links) sum_links sum_subgroups
 // min(1, exp(-dS)) (eps |a|)^2 over the links of one phase, for proposals
 // drawn from the current links (the field is not changed).  Block b writes
-// its sums of the per-link weight gradients (in thread order) and of
-// (loss, ESJD, acceptance, links) to partials[b][kNP + 4].
+// its sums of the per-link weight gradients and of (loss, ESJD,
+// acceptance, links) to partials[b][kNP + 4]; the weight and bias sums come
+// from one tensor-core product over the block's links (see the file head).
+constexpr size_t kGradSmem = sizeof(NetOps) + sizeof(GradOps) + 128;
+
 template <int mu>
-__global__ void __launch_bounds__(kTrainBlock) k_mh_grad(Field<float> U, Geom G, int parity, const double *params,
-                                                         const uint16_t *wq, double eps_max, uint2 key,
-                                                         uint64_t phase, float *partials)
+__global__ void __launch_bounds__(kMHBlock) k_mh_grad(Field<float> U, Geom G, int parity, const double *params,
+                                                      const uint16_t *wq, double eps_max, uint2 key, uint64_t phase,
+                                                      float *partials, unsigned *err)
 {
-    __shared__ float w[kNP];
-    __shared__ float sx[kTrainBlock][kNF], sh1[kTrainBlock][kNH], sh2[kTrainBlock][kNH], sd1[kTrainBlock][kNH],
-        sd2[kTrainBlock][kNH], sgo[kTrainBlock], sst[kTrainBlock][4];
-    for (int i = threadIdx.x; i < kNP; i += blockDim.x) w[i] = bf16_bits_to_float(wq[i]);
-    __syncthreads();
-    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    extern __shared__ uint8_t smem_raw[];
+    uint8_t *base = (uint8_t *)(((uintptr_t)smem_raw + 127) & ~(uintptr_t)127);
+    NetOps &S = *reinterpret_cast<NetOps *>(base);
+    GradOps &T = *reinterpret_cast<GradOps *>(base + sizeof(NetOps));
+    net_setup(S, wq, 128);
     const int me = threadIdx.x;
-    float x[kNF], z1[kNH], z2[kNH];
+    for (int i = me; i < kNH * kNH; i += kMHBlock) {           // W2^T[k][j] = W2[j][k]
+        const int k = i >> 5, j = i & 31;
+        st_bf16(T.b2t, tc::kmajor_off(k, j, 32), wq[kW2 + j * kNH + k]);
+    }
+    // rows 64..127 of ga (row groups 8..15) and 72..79 of gb (row group 9) start at zero
+    for (int i = me; i < 8 * kMHBlock * 16 / 16; i += kMHBlock)
+        reinterpret_cast<uint4 *>(T.ga + tc::kmajor_off(64, 0, kMHBlock))[i] = make_uint4(0, 0, 0, 0);
+    for (int i = me; i < kMHBlock * 16 / 16; i += kMHBlock)
+        reinterpret_cast<uint4 *>(T.gb + tc::kmajor_off(72, 0, kMHBlock))[i] = make_uint4(0, 0, 0, 0);
+    __syncthreads();
+    st_bf16(T.gb, tc::kmajor_off(72, me, kMHBlock), kBF16One);
+
+    const uint32_t t = blockIdx.x * kMHBlock + me;
+    const bool active = t < G.half;
+    float x[kNF];
 #pragma unroll
     for (int k = 0; k < kNF; k++) x[k] = 0.0f;
-#pragma unroll
-    for (int k = 0; k < kNH; k++) { z1[k] = 0.0f; z2[k] = 0.0f; }
-    float go = 0.0f, loss = 0.0f, esjd = 0.0f, accm = 0.0f, one = 0.0f;
-    if (t < G.half) {
-        Crd c = lex2crd(G, 2 * t);
-        if (parity_of(c) != parity) c.y += 1;
-        const uint32_t e0 = (uint32_t)parity * G.cb + t;
+    M3<float> st;
+    Crd c = lex2crd(G, 2 * (active ? t : 0));
+    if (parity_of(c) != parity) c.y += 1;
+    const uint32_t e0 = (uint32_t)parity * G.cb + t;
+    if (active) {
         const Nbr nb = neighbours(G, c);
-        const double bn = (double)(float)params[0];
-        M3<float> st;
         staple_features<mu>(U, G, t, nb, parity, st, x);
-        // forward, keeping the pre-activations
-#pragma unroll
-        for (int j = 0; j < kNH; j++) {
-            float z = w[kB1 + j];
-#pragma unroll
-            for (int k = 0; k < kNF; k++) z = FMA(w[kW1 + j * kNF + k], x[k], z);
-            z1[j] = z;
-        }
-        float o = w[kB3];
-#pragma unroll
-        for (int j = 0; j < kNH; j++) {
-            float z = w[kB2 + j];
-#pragma unroll
-            for (int k = 0; k < kNH; k++) z = FMA(w[kW2 + j * kNH + k], z1[k] > 0.0f ? z1[k] : 0.0f, z);
-            z2[j] = z;
-            o = FMA(w[kW3 + j], z > 0.0f ? z : 0.0f, o);
-        }
+    }
+    uint32_t mph = 0;
+    float z1[kNH], z2[kNH], o = 0.0f;
+    bool ok = net_forward(S, mph, x, z1, z2, o);
+    float go = 0.0f, loss = 0.0f, esjd = 0.0f, accm = 0.0f, one = 0.0f;
+    if (ok && active) {
+        const double bn = (double)(float)params[0];
         const double sg = sigmoid_d(o);
         const double eps = eps_max * sg;
         const M3<float> Um = expand(U.ld3(mu, e0));
         PrnPhilox<float> prn;
         prn.key = key; prn.t = t; prn.k = 0; prn.plo = (uint32_t)phase; prn.phi = (uint32_t)(phase >> 32);
-        double geps = 0.0, ls = 0.0, es = 0.0, ac = 0.0;
+        double geps = 0.0, es = 0.0, ac = 0.0;
 #pragma unroll 1
         for (int s = 0; s < 3; s++) {
             const int i = (s == 2) ? 1 : 0, j = (s == 0) ? 1 : 2;
@@ -365,57 +509,91 @@ __global__ void __launch_bounds__(kTrainBlock) k_mh_grad(Field<float> U, Geom G,
             ac += a;
             geps -= dade * th * th + a * 2.0 * eps * r * r;
         }
-        ls = -es;
         go = (float)(geps * eps_max * sg * (1.0 - sg));
-        loss = (float)ls;
+        loss = (float)(-es);
         esjd = (float)es;
         accm = (float)(ac / 3.0);
         one = 1.0f;
     }
-    // backward of one link into shared memory
+    if (ok) {
+        // back-propagation through the output layer; dz2 as the A operand
+        // of dz1 = W2^T dz2 (rows = links, K = 32)
+        float dz2[kNH], h[kNH];
 #pragma unroll
-    for (int k = 0; k < kNF; k++) sx[me][k] = x[k];
-    float dz2[kNH];
+        for (int j = 0; j < kNH; j++) dz2[j] = z2[j] > 0.0f ? go * S.w3[j] : 0.0f;
 #pragma unroll
-    for (int j = 0; j < kNH; j++) {
-        sh2[me][j] = z2[j] > 0.0f ? z2[j] : 0.0f;
-        dz2[j] = z2[j] > 0.0f ? go * w[kW3 + j] : 0.0f;
-        sd2[me][j] = dz2[j];
-        sh1[me][j] = z1[j] > 0.0f ? z1[j] : 0.0f;
-    }
-#pragma unroll 1
-    for (int k = 0; k < kNH; k++) {           // dz1[k] = relu'(z1[k]) sum_j W2[j][k] dz2[j]
-        float d = 0.0f;
+        for (int q = 0; q < 4; q++) st_bf16x8(S.a2, tc::kmajor_off(me, 8 * q, 32), dz2 + 8 * q);
+        // the weight-gradient operands of this link (column me)
 #pragma unroll
-        for (int j = 0; j < kNH; j++) d = FMA(w[kW2 + j * kNH + k], dz2[j], d);
-        sd1[me][k] = sh1[me][k] > 0.0f ? d : 0.0f;
-    }
-    sgo[me] = go;
-    sst[me][0] = loss; sst[me][1] = esjd; sst[me][2] = accm; sst[me][3] = one;
-    __syncthreads();
-    // block sums in thread order
-    float *out = partials + (size_t)blockIdx.x * (kNP + 4);
-    for (int q = threadIdx.x; q < kNP + 4; q += blockDim.x) {
-        float acc = 0.0f;
-        if (q < kB1) {                                   // W1[j][k] = sum dz1[j] x[k]
-            const int j = (q - kW1) / kNF, k = (q - kW1) % kNF;
-            for (int u = 0; u < kTrainBlock; u++) acc = FMA(sd1[u][j], sx[u][k], acc);
-        } else if (q < kW2) {                            // b1[j]
-            for (int u = 0; u < kTrainBlock; u++) acc += sd1[u][q - kB1];
-        } else if (q < kB2) {                            // W2[j][k] = sum dz2[j] h1[k]
-            const int j = (q - kW2) / kNH, k = (q - kW2) % kNH;
-            for (int u = 0; u < kTrainBlock; u++) acc = FMA(sd2[u][j], sh1[u][k], acc);
-        } else if (q < kW3) {                            // b2[j]
-            for (int u = 0; u < kTrainBlock; u++) acc += sd2[u][q - kB2];
-        } else if (q < kB3) {                            // w3[k] = sum go h2[k]
-            for (int u = 0; u < kTrainBlock; u++) acc = FMA(sgo[u], sh2[u][q - kW3], acc);
-        } else if (q == kB3) {
-            for (int u = 0; u < kTrainBlock; u++) acc += sgo[u];
-        } else {
-            for (int u = 0; u < kTrainBlock; u++) acc += sst[u][q - kNP];
+        for (int j = 0; j < kNH; j++) {
+            st_bf16(T.ga, tc::kmajor_off(j, me, kMHBlock), float_to_bf16_bits(dz2[j]));
+            h[j] = z1[j] > 0.0f ? z1[j] : 0.0f;
+            st_bf16(T.gb, tc::kmajor_off(j, me, kMHBlock), float_to_bf16_bits(h[j]));
+            st_bf16(T.gb, tc::kmajor_off(32 + j, me, kMHBlock), float_to_bf16_bits(z2[j] > 0.0f ? z2[j] : 0.0f));
         }
-        out[q] = acc;
+#pragma unroll
+        for (int k = 0; k < kNF; k++) st_bf16(T.gb, tc::kmajor_off(64 + k, me, kMHBlock), float_to_bf16_bits(x[k]));
+        st_bf16(T.ga, tc::kmajor_off(64, me, kMHBlock), float_to_bf16_bits(go));
+        net_sync();
+        if (me == 0) {
+            tc::mma_bf16(S.tmem, tc::desc_operand(S.a2, 32, 0), tc::desc_operand(T.b2t, 32, 0), kIdesc32, 0);
+            tc::mma_bf16(S.tmem, tc::desc_operand(S.a2, 32, 16), tc::desc_operand(T.b2t, 32, 16), kIdesc32, 1);
+            tc::mma_commit(&S.mbar);
+        }
+        ok = net_wait(S, mph);
+        if (ok) {
+            float d[32];
+            tc::tmem_ld32(S.tmem + ((uint32_t)(me & ~31) << 16), d);
+#pragma unroll
+            for (int k = 0; k < kNH; k++)
+                st_bf16(T.ga, tc::kmajor_off(32 + k, me, kMHBlock), float_to_bf16_bits(z1[k] > 0.0f ? d[k] : 0.0f));
+            net_sync();
+            if (me == 0) {
+#pragma unroll 1
+                for (int q = 0; q < kMHBlock / 16; q++)
+                    tc::mma_bf16(S.tmem, tc::desc_operand(T.ga, kMHBlock, 16 * q),
+                                 tc::desc_operand(T.gb, kMHBlock, 16 * q), kIdesc80, q > 0 ? 1u : 0u);
+                tc::mma_commit(&S.mbar);
+            }
+            ok = net_wait(S, mph);
+        }
     }
+    T.sst[me][0] = loss; T.sst[me][1] = esjd; T.sst[me][2] = accm; T.sst[me][3] = one;
+    __syncthreads();
+    float *out = partials + (size_t)blockIdx.x * (kNP + 4);
+    if (ok) {
+        const int w = me >> 5, l = me & 31;
+        const uint32_t lanes = S.tmem + ((uint32_t)(w * 32) << 16);
+        float d[32], e[32];
+        if (w == 0) {                                   // rows j: dW2[j][k] (columns 0..31), db2[j] (column 72)
+            tc::tmem_ld32(lanes, d);
+            tc::tmem_ld32(lanes + 64, e);
+#pragma unroll
+            for (int k = 0; k < kNH; k++) out[kW2 + l * kNH + k] = d[k];
+            out[kB2 + l] = e[8];
+        } else if (w == 1) {                            // rows 32 + j: dW1[j][k] (columns 64..71), db1[j] (72)
+            tc::tmem_ld32(lanes + 64, e);
+#pragma unroll
+            for (int k = 0; k < kNF; k++) out[kW1 + l * kNF + k] = e[k];
+            out[kB1 + l] = e[8];
+        } else if (w == 2) {                            // row 64: dw3[j] (columns 32..63), db3 (72)
+            tc::tmem_ld32(lanes + 32, d);
+            tc::tmem_ld32(lanes + 64, e);
+            if (l == 0) {
+#pragma unroll
+                for (int k = 0; k < kNH; k++) out[kW3 + k] = d[k];
+                out[kB3] = e[8];
+            }
+        }
+    } else if (me == 0) {
+        atomicOr(err, 1u);
+    }
+    for (int q = me; q < 4; q += kMHBlock) {            // statistics: FP32 sums in thread order
+        float a = 0.0f;
+        for (int u = 0; u < kMHBlock; u++) a += T.sst[u][q];
+        out[kNP + q] = a;
+    }
+    net_teardown(S, 128, ok, mph);
 }
 
 // grad[q] = (sum over blocks in order) / links, stats = raw sums
@@ -454,34 +632,60 @@ __global__ void k_to_bf16(const float *master, uint16_t *wq)
 
 // ------------------------------------------------------------- launchers
 cudaError_t launch_mh_phase(const Geom &G, void *links, const PhaseArgs &a, const uint16_t *wq, double eps_max,
-                            int nhit, unsigned long long *acc_count, double *jump_sum, cudaStream_t s)
+                            int nhit, unsigned long long *acc_count, double *jump_sum, float *eps_out, unsigned *err,
+                            cudaStream_t s)
 {
     Field<float> U{ (float4 *)links, G.pstride };
-    const unsigned nb = (G.half + 127) / 128;
+    const unsigned nb = (G.half + kMHBlock - 1) / kMHBlock;
+#define QG_MH(MU)                                                                                            \
+    do {                                                                                                     \
+        if (eps_out)                                                                                         \
+            k_mh_phase<MU, true><<<nb, kMHBlock, 0, s>>>(U, G, a, wq, eps_max, nhit, acc_count, jump_sum, eps_out, \
+                                                          err);                                              \
+        else                                                                                                 \
+            k_mh_phase<MU, false><<<nb, kMHBlock, 0, s>>>(U, G, a, wq, eps_max, nhit, acc_count, jump_sum,     \
+                                                           nullptr, err);                                    \
+    } while (0)
     switch (a.dir) {
-    case 0: k_mh_phase<0><<<nb, 128, 0, s>>>(U, G, a, wq, eps_max, nhit, acc_count, jump_sum); break;
-    case 1: k_mh_phase<1><<<nb, 128, 0, s>>>(U, G, a, wq, eps_max, nhit, acc_count, jump_sum); break;
-    case 2: k_mh_phase<2><<<nb, 128, 0, s>>>(U, G, a, wq, eps_max, nhit, acc_count, jump_sum); break;
-    default: k_mh_phase<3><<<nb, 128, 0, s>>>(U, G, a, wq, eps_max, nhit, acc_count, jump_sum); break;
+    case 0: QG_MH(0); break;
+    case 1: QG_MH(1); break;
+    case 2: QG_MH(2); break;
+    default: QG_MH(3); break;
     }
+#undef QG_MH
     return cudaGetLastError();
 }
 
-uint32_t mh_grad_blocks(const Geom &G) { return (G.half + kTrainBlock - 1) / kTrainBlock; }
+uint32_t mh_grad_blocks(const Geom &G) { return (G.half + kMHBlock - 1) / kMHBlock; }
+
+template <int mu>
+static cudaError_t grad_launch(unsigned nb, Field<float> U, const Geom &G, int parity, const double *params,
+                               const uint16_t *wq, double eps_max, uint2 key, uint64_t phase, float *partials,
+                               unsigned *err, cudaStream_t s)
+{
+    static bool attr = false;               // the dynamic shared memory above 48 KB, once per instantiation
+    if (!attr) {
+        cudaError_t e = cudaFuncSetAttribute(k_mh_grad<mu>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kGradSmem);
+        if (e != cudaSuccess) return e;
+        attr = true;
+    }
+    k_mh_grad<mu><<<nb, kMHBlock, kGradSmem, s>>>(U, G, parity, params, wq, eps_max, key, phase, partials, err);
+    return cudaGetLastError();
+}
 
 cudaError_t launch_mh_grad(const Geom &G, const void *links, int parity, int dir, const double *params,
                            const uint16_t *wq, double eps_max, uint2 key, uint64_t phase, float *partials,
-                           float *grad, cudaStream_t s)
+                           float *grad, unsigned *err, cudaStream_t s)
 {
     Field<float> U{ (float4 *)links, G.pstride };
     const unsigned nb = mh_grad_blocks(G);
+    cudaError_t e;
     switch (dir) {
-    case 0: k_mh_grad<0><<<nb, kTrainBlock, 0, s>>>(U, G, parity, params, wq, eps_max, key, phase, partials); break;
-    case 1: k_mh_grad<1><<<nb, kTrainBlock, 0, s>>>(U, G, parity, params, wq, eps_max, key, phase, partials); break;
-    case 2: k_mh_grad<2><<<nb, kTrainBlock, 0, s>>>(U, G, parity, params, wq, eps_max, key, phase, partials); break;
-    default: k_mh_grad<3><<<nb, kTrainBlock, 0, s>>>(U, G, parity, params, wq, eps_max, key, phase, partials); break;
+    case 0: e = grad_launch<0>(nb, U, G, parity, params, wq, eps_max, key, phase, partials, err, s); break;
+    case 1: e = grad_launch<1>(nb, U, G, parity, params, wq, eps_max, key, phase, partials, err, s); break;
+    case 2: e = grad_launch<2>(nb, U, G, parity, params, wq, eps_max, key, phase, partials, err, s); break;
+    default: e = grad_launch<3>(nb, U, G, parity, params, wq, eps_max, key, phase, partials, err, s); break;
     }
-    cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     k_mh_grad_reduce<<<(kNP + 4 + 255) / 256, 256, 0, s>>>(partials, nb, grad);
     return cudaGetLastError();

