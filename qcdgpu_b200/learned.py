@@ -2,7 +2,7 @@
 
   python -m qcdgpu_b200.learned [--size 16] [--beta 5.7] [--train-configs 2000]
                                 [--steps-per-config 2] [--lr 2e-3] [--eps-max 1.5]
-                                [--chain-sweeps 2000] [--nhit 1] [--seed 7]
+                                [--chain-sweeps 2000] [--nhits 1,4,8] [--seed 7]
 
 SU(3) Wilson action, FP32 links, Philox stream.  After cold start and
 heatbath thermalisation:
@@ -13,13 +13,15 @@ heatbath thermalisation:
      `steps-per-config` gradient steps on its links, `train-configs` times;
   3. trained and constant proposals are compared on the same fresh
      heatbath configurations (ESJD, acceptance; paired difference);
-  4. three chains from the same thermalised configuration -- heatbath,
-     constant-step Metropolis, learned Metropolis -- are run
+  4. chains from the same thermalised configuration -- heatbath, and
+     constant-step and learned Metropolis with each hit count in `nhits`
+     (hits per SU(2) subgroup and link; the staple, its features and the
+     network are evaluated once per link whatever the count) -- are run
      `chain-sweeps` sweeps with plaquette and Polyakov loop measured every
      sweep; reported: acceptance, mean plaquette with its tau_int-corrected
-     error, tau_int of Re P and of the plaquette, sweeps/s of the update
+     error, tau_int of the plaquette and of Re P, sweeps/s of the update
      alone (CUDA events) and decorrelated configurations/s
-     = sweeps/s / (2 tau_int(Re P)).
+     = sweeps/s / (2 tau_int) for each of the two observables.
 Prints one JSON line.
 """
 import argparse
@@ -87,7 +89,7 @@ def main():
     ap.add_argument("--eps-max", type=float, default=1.5)
     ap.add_argument("--chain-sweeps", type=int, default=2000)
     ap.add_argument("--therm", type=int, default=200)
-    ap.add_argument("--nhit", type=int, default=1)
+    ap.add_argument("--nhits", default="1,4,8")
     ap.add_argument("--eval-configs", type=int, default=16)
     ap.add_argument("--seed", type=int, default=7)
     a = ap.parse_args()
@@ -129,21 +131,24 @@ def main():
     gain = float(np.mean(e_tr) / np.mean(e_co) - 1.0)
     gain_err = float(np.std(d_esjd) / np.sqrt(len(d_esjd)) / np.mean(e_co))
     # 4. chains from the same thermalised configuration
+    nhits = [int(v) for v in a.nhits.split(",")]
     out = {"workload": "SU(3) %d^4 beta=%g, FP32 links; learned vs constant-step Metropolis vs heatbath"
                        % (a.size, a.beta),
            "train_configs": a.train_configs, "steps_per_config": a.steps_per_config, "lr": a.lr,
-           "eps_max": a.eps_max, "nhit": a.nhit, "constant_step_scan": dict(zip(map(str, grid), scan)),
+           "eps_max": a.eps_max, "nhits": nhits, "constant_step_scan": dict(zip(map(str, grid), scan)),
            "best_constant_step": best, "training_esjd_history": hist,
            "esjd_trained": float(np.mean(e_tr)), "esjd_constant": float(np.mean(e_co)),
            "acceptance_trained": float(np.mean(a_tr)), "acceptance_constant": float(np.mean(a_co)),
            "esjd_gain": gain, "esjd_gain_error": gain_err, "chains": {}}
-    for name, w in (("heatbath", None), ("constant_step", const_w), ("learned", trained_w)):
+    runs = [("heatbath", None, 0)] + [(kind + "_nhit%d" % h, w, h) for h in nhits
+                                      for kind, w in (("constant_step", const_w), ("learned", trained_w))]
+    for name, w, nh in runs:
         L.upload(therm_state)
         if w is None:
             upd = L.sweep
         else:
             L.net_set(w, a.eps_max)
-            upd = lambda n: L.mh_sweep(n, a.nhit)   # noqa: E731
+            upd = lambda n, nh=nh: L.mh_sweep(n, nh)   # noqa: E731
         ms = timed(L, upd, 50)
         L.mh_stats(reset=True) if w is not None else None
         res = chain(L, upd, a.chain_sweeps, V, nsp)
@@ -151,7 +156,8 @@ def main():
             res["acceptance"] = L.mh_stats()[0]
         res["ms_per_sweep"] = ms
         res["sweeps_per_s"] = 1000.0 / ms
-        res["decorrelated_configs_per_s"] = res["sweeps_per_s"] / (2.0 * res["tau_int_polyakov"])
+        res["decorrelated_configs_per_s_polyakov"] = res["sweeps_per_s"] / (2.0 * res["tau_int_polyakov"])
+        res["decorrelated_configs_per_s_plaquette"] = res["sweeps_per_s"] / (2.0 * res["tau_int_plaquette"])
         out["chains"][name] = res
     out["seconds"] = time.time() - t0
     print(json.dumps(out))
