@@ -402,6 +402,19 @@ int qg_batch_set_shape(qg_batch *b, int shape);
 int qg_batch_set_shapes(qg_batch *b, int heatbath_shape, int overrelax_shape);
 int qg_batch_get_shapes(qg_batch *b, int *heatbath_shape, int *overrelax_shape);
 int qg_batch_tune(qg_batch *b, int reps, float *times_ms);
+/* enable != 0: each half-sweep (the four direction phases of one parity) is
+ * ONE persistent launch over all ensembles -- every resident block walks
+ * the batch's tiles direction by direction with a grid barrier between
+ * directions (cooperative launch; the same chains bit for bit).  A barrier
+ * that does not complete within a second sets a device flag and the blocks
+ * return; qg_batch_sync / qg_batch_series then return QG_ERR_CUDA (the
+ * fields are then not consistent) and clear the flag.  Default: off.       */
+int qg_batch_set_persistent(qg_batch *b, int enable);
+/* test of the bounded barrier: one persistent heatbath half-sweep in which
+ * block skip_block leaves out its first arrival; every other block's wait
+ * runs out.  Returns QG_ERR_CUDA (the flag) when the timeout path works; it
+ * changes the fields.                                                      */
+int qg_batch_barrier_test(qg_batch *b, int skip_block);
 /* nsweeps sweeps of every ensemble (graph replays); after every
  * measure_every-th sweep (0 = never) plaquette, action and Polyakov sums of
  * every ensemble are appended to the device series                         */

@@ -45,7 +45,8 @@ EXPORTED_SYMBOLS = (
     "qg_write_state_file", "qg_read_state_file", "qg_save_state", "qg_tau_int",
     "qg_batch_create", "qg_batch_destroy", "qg_batch_init", "qg_batch_set_shape", "qg_batch_run", "qg_batch_sync",
     "qg_batch_get_stream", "qg_batch_series", "qg_batch_links_download", "qg_batch_info",
-    "qg_batch_set_shapes", "qg_batch_get_shapes", "qg_batch_tune",
+    "qg_batch_set_shapes", "qg_batch_get_shapes", "qg_batch_tune", "qg_batch_set_persistent",
+    "qg_batch_barrier_test",
     "qg_measure_wilson_all", "qg_measure_fmunu", "qg_measure_action_profile", "qg_measure_polyakov_profile",
     "qg_measure_enqueue", "qg_measure_fetch", "qg_measure_plaquette_all", "qg_measure_polyakov_all",
     "qg_net_set", "qg_net_get", "qg_mh_phase", "qg_net_eps", "qg_mh_sweep", "qg_mh_stats", "qg_net_grad",
@@ -266,6 +267,8 @@ def load_library(path=LIB_PATH):
     lib.qg_batch_set_shapes.argtypes = [vp, ctypes.c_int, ctypes.c_int]
     lib.qg_batch_get_shapes.argtypes = [vp, P(ctypes.c_int), P(ctypes.c_int)]
     lib.qg_batch_tune.argtypes = [vp, ctypes.c_int, P(ctypes.c_float)]
+    lib.qg_batch_set_persistent.argtypes = [vp, ctypes.c_int]
+    lib.qg_batch_barrier_test.argtypes = [vp, ctypes.c_int]
     lib.qg_batch_run.argtypes = [vp, ctypes.c_int, ctypes.c_int]
     lib.qg_batch_sync.argtypes = [vp]
     lib.qg_batch_get_stream.argtypes = [vp, P(vp)]
@@ -814,6 +817,18 @@ class Batch:
         t = (ctypes.c_float * (2 * BATCH_SHAPES))()
         self._ck(self.lib.qg_batch_tune(self.b, reps, t), "qg_batch_tune")
         return [(t[2 * v], t[2 * v + 1]) for v in range(BATCH_SHAPES)]
+
+    def set_persistent(self, enable=True):
+        """one persistent launch per half-sweep (grid barriers between the
+        directions) instead of one launch per phase"""
+        self._ck(self.lib.qg_batch_set_persistent(self.b, int(enable)), "qg_batch_set_persistent")
+
+    def barrier_test(self, skip_block):
+        """run one persistent half-sweep in which block skip_block skips its
+        first barrier arrival; returns the status code (QG_ERR_CUDA expected)
+        and the error text"""
+        rc = self.lib.qg_batch_barrier_test(self.b, skip_block)
+        return rc, self.lib.qg_last_error(None).decode()
 
     def run(self, nsweeps, measure_every=0):
         self._ck(self.lib.qg_batch_run(self.b, nsweeps, measure_every), "qg_batch_run")

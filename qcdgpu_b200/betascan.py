@@ -4,7 +4,7 @@ the sweep and the measurement captured in one CUDA graph -- on one GPU or
 spread over the GPUs of a node.
 
   python -m qcdgpu_b200.betascan [--ensembles 64] [--sweeps 500] [--n-or 4]
-                                 [--measure-every 1] [--seed 54] [--shape -1]
+                                 [--measure-every 1] [--seed 54] [--shape -1] [--persistent]
   torchrun --nproc-per-node N -m qcdgpu_b200.betascan ...   (one rank per GPU)
 
 Workload: N_t drawn from {4, 6, 8} and N_s from {16, 20, 24, 32} with a
@@ -73,6 +73,8 @@ def run_share(ens, idx, a):
     B.init(Q.START_COLD)
     stream = torch.cuda.ExternalStream(B.stream())
     B.run(a.warmup, a.measure_every)                  # warm-up, untimed
+    if getattr(a, "persistent", False):
+        B.set_persistent(True)                        # one launch per half-sweep (same chains)
     if a.shape < 0:
         B.tune()                                      # fields restored: the chains are unchanged
     else:
@@ -137,6 +139,8 @@ def main():
     ap.add_argument("--seed", type=int, default=54)
     ap.add_argument("--shape", type=int, default=-1, help="batched launch shape; -1 = autotune (qg_batch_tune)")
     ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--persistent", action="store_true",
+                    help="one persistent launch per half-sweep (grid barriers between directions)")
     a = ap.parse_args()
     import torch
 

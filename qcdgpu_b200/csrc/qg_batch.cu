@@ -11,6 +11,7 @@
 // poly_site, gs_site, reduce_partials), so ensemble e's chain is
 // bit-identical to a single context with the same size, coupling and
 // RANDSERIES.
+#include <algorithm>
 #include <string>
 #include <vector>
 
@@ -70,7 +71,131 @@ k_phase_batch(const EnsDesc *ens, const uint32_t *pre, int n, int parity, const 
     Field<Real> U;
     U.p = reinterpret_cast<typename V4<Real>::T *>(d.links);
     U.pstride = G.pstride;
-    phase_site<NC, Real, 1, OR, mu, STAGED>(U, G, A, t);
+    if constexpr (STAGED) {
+        __shared__ __align__(16) StageBuf sb;
+        phase_site<NC, Real, 1, OR, mu, STAGED>(U, G, A, t, &sb);
+    } else {
+        phase_site<NC, Real, 1, OR, mu, STAGED>(U, G, A, t, nullptr);
+    }
+}
+
+// ---------------------------------------------- persistent half-sweep
+// One launch per parity runs the four directions of that parity over all
+// ensembles: every block walks the 128-link tiles of the batch (tile k of
+// the phase's prefix table for k = blockIdx.x, blockIdx.x + gridDim.x, ...)
+// for direction 0, waits at a grid barrier, and so on -- the phases of one
+// parity depend on each other (phase (p, nu) reads the links of parity p
+// and direction mu that phase (p, mu) wrote), so the barrier stands where
+// the per-phase launches had a kernel boundary.  All blocks are resident
+// (cooperative launch sized from the occupancy), and every wait is bounded:
+// a barrier that does not complete within kBarrierNs sets bar->err and the
+// blocks return.  skip_block >= 0 makes that block leave out its arrival at
+// the first barrier (a test of the bounded wait).
+struct GridBarrier {
+    unsigned count, gen, err, pad;
+};
+constexpr unsigned long long kBarrierNs = 1000000000ull;
+
+__device__ __forceinline__ unsigned ld_acquire_u32(const unsigned *p)
+{
+    unsigned v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ unsigned long long global_ns()
+{
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+// all blocks of the grid; false (block-uniform) when the wait ran out
+__device__ bool grid_sync(GridBarrier *bar, bool arrive)
+{
+    __syncthreads();
+    int ok = 1;
+    if (threadIdx.x == 0) {
+        const unsigned g = ld_acquire_u32(&bar->gen);
+        __threadfence();
+        bool last = false;
+        if (arrive && atomicAdd(&bar->count, 1u) + 1u == gridDim.x) {
+            atomicExch(&bar->count, 0u);
+            __threadfence();
+            atomicAdd(&bar->gen, 1u);
+            last = true;
+        }
+        if (!last) {
+            const unsigned long long t0 = global_ns();
+            while (ld_acquire_u32(&bar->gen) == g) {
+                if (global_ns() - t0 > kBarrierNs) {
+                    atomicOr(&bar->err, 1u);
+                    ok = 0;
+                    break;
+                }
+                __nanosleep(256);
+            }
+        }
+        __threadfence();
+    }
+    return __syncthreads_and(ok) != 0;
+}
+
+template <int NC, typename Real, bool OR, bool STAGED>
+__device__ __forceinline__ void half_sweep_body(const EnsDesc *ens, const uint32_t *pre, int n, int parity,
+                                                const uint64_t *phase_base, uint32_t phase_offset0, int nhit,
+                                                int nhitpar, GridBarrier *bar, int skip_block, StageBuf *sb)
+{
+    const uint32_t ntiles = __ldg(pre + n);
+    for (int mu = 0; mu < 4; mu++) {
+        if (mu > 0 && !grid_sync(bar, !(mu == 1 && (int)blockIdx.x == skip_block))) return;
+        for (uint32_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+            const int e = find_ensemble(pre, n, tile);
+            const EnsDesc &d = ens[e];
+            const uint32_t t = (tile - __ldg(pre + e)) * kPhaseBlock + threadIdx.x;
+            const Geom G = d.G;
+            if (t >= G.half) continue;
+            PhaseArgs A;
+            A.parity = parity;
+            A.dir = mu;
+            A.params = d.params;
+            A.twist = 0;
+            A.nhit = nhit;
+            A.nhitpar = nhitpar;
+            A.prn_mode = OR ? -1 : 1;
+            A.prns = nullptr;
+            A.prngstep = 0;
+            A.key = d.key;
+            A.phase_base = phase_base;
+            A.phase_offset = phase_offset0 + (uint32_t)mu;
+            A.variant = 0;
+            A.t_begin = 0;
+            A.t_end = G.half;
+            A.t_prn = 0;
+            Field<Real> U;
+            U.p = reinterpret_cast<typename V4<Real>::T *>(d.links);
+            U.pstride = G.pstride;
+            switch (mu) {
+            case 0: phase_site<NC, Real, 1, OR, 0, STAGED>(U, G, A, t, sb); break;
+            case 1: phase_site<NC, Real, 1, OR, 1, STAGED>(U, G, A, t, sb); break;
+            case 2: phase_site<NC, Real, 1, OR, 2, STAGED>(U, G, A, t, sb); break;
+            default: phase_site<NC, Real, 1, OR, 3, STAGED>(U, G, A, t, sb); break;
+            }
+        }
+    }
+}
+
+template <int NC, typename Real, bool OR, int MINB, bool STAGED>
+__global__ void __launch_bounds__(kPhaseBlock, MINB)
+k_half_sweep_batch(const EnsDesc *ens, const uint32_t *pre, int n, int parity, const uint64_t *phase_base,
+                   uint32_t phase_offset0, int nhit, int nhitpar, GridBarrier *bar, int skip_block)
+{
+    if constexpr (STAGED) {
+        __shared__ __align__(16) StageBuf sb;
+        half_sweep_body<NC, Real, OR, STAGED>(ens, pre, n, parity, phase_base, phase_offset0, nhit, nhitpar, bar,
+                                              skip_block, &sb);
+    } else {
+        half_sweep_body<NC, Real, OR, STAGED>(ens, pre, n, parity, phase_base, phase_offset0, nhit, nhitpar, bar,
+                                              skip_block, nullptr);
+    }
 }
 
 template <int NC, typename Real>
@@ -160,6 +285,8 @@ struct qg_batch {
     cudaStream_t stream = nullptr;
     cudaGraphExec_t graph[4] = { nullptr, nullptr, nullptr, nullptr };   // [measure * 2 + reunit]
     int shape_hb = 4, shape_or = 4;    // phase-kernel launch shapes (qg_batch_tune)
+    bool persistent = false;           // one launch per half-sweep (qg_batch_set_persistent)
+    GridBarrier *d_bar = nullptr;
 };
 
 namespace {
@@ -225,6 +352,64 @@ cudaError_t phase_batch(qg_batch *b, int parity, int mu, bool OR, uint32_t offse
                             : launch_phase_batch<float>(b, parity, mu, OR, offset);
 }
 
+// one cooperative launch of the persistent half-sweep: as many blocks as
+// are resident at once (at most one per tile)
+template <typename KernelT>
+cudaError_t launch_half(qg_batch *b, KernelT kern, int parity, uint32_t offset0, int skip_block)
+{
+    int dev = 0, sms = 0, per_sm = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kPhaseBlock, 0);
+    if (e != cudaSuccess) return e;
+    if (per_sm < 1) return cudaErrorInvalidConfiguration;
+    const unsigned ntiles = b->pre_phase[b->n];
+    const unsigned grid = std::min<unsigned>((unsigned)(sms * per_sm), ntiles);
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(grid);
+    cfg.blockDim = dim3(kPhaseBlock);
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = b->stream;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeCooperative;
+    attr[0].val.cooperative = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, kern, (const EnsDesc *)b->d_ens, (const uint32_t *)b->d_pre, b->n, parity,
+                              (const uint64_t *)b->d_phase, offset0, b->cfg.nhit, b->cfg.nhitpar, b->d_bar,
+                              skip_block);
+}
+
+template <typename Real>
+cudaError_t half_sweep_T(qg_batch *b, int parity, bool OR, uint32_t offset0, int skip_block)
+{
+    constexpr bool F32 = sizeof(Real) == 4;
+    const int shape = OR ? b->shape_or : b->shape_hb;
+    const bool g3 = b->cfg.group == 3;
+    // shapes as in launch_phase_batch: 1 / 2 hold 5 / 6 blocks per SM, 3 / 4
+    // stage the staple (SU(3) FP32)
+#define QB_H(NC, OR_, MB, ST) return launch_half(b, k_half_sweep_batch<NC, Real, OR_, MB, ST>, parity, offset0, skip_block)
+#define QB_HS(NC, OR_)                                                     \
+    do {                                                                   \
+        constexpr bool kSt = NC == 3 && F32;                               \
+        if (shape == 1) QB_H(NC, OR_, 5, false);                           \
+        else if (shape == 2) QB_H(NC, OR_, 6, false);                      \
+        else if (shape == 3) QB_H(NC, OR_, 0, kSt);                        \
+        else if (shape == 4) QB_H(NC, OR_, 5, kSt);                        \
+        else QB_H(NC, OR_, 0, false);                                      \
+    } while (0)
+    if (g3) { if (OR) QB_HS(3, true); else QB_HS(3, false); }
+    else { if (OR) QB_HS(2, true); else QB_HS(2, false); }
+#undef QB_HS
+#undef QB_H
+}
+
+cudaError_t half_sweep(qg_batch *b, int parity, bool OR, uint32_t offset0, int skip_block = -1)
+{
+    return b->cfg.precision ? half_sweep_T<double>(b, parity, OR, offset0, skip_block)
+                            : half_sweep_T<float>(b, parity, OR, offset0, skip_block);
+}
+
 cudaError_t gs_batch(qg_batch *b)
 {
     const unsigned nb = b->pre_gs[b->n];
@@ -283,15 +468,25 @@ cudaError_t enqueue_batch_sweep(qg_batch *b, bool reunit, bool measure)
     cudaError_t e;
     const int par_order[2] = { 1, 0 };
     uint32_t hb = 0;
-    for (int pi = 0; pi < 2; pi++)
-        for (int mu = 0; mu < 4; mu++) {
-            if ((e = phase_batch(b, par_order[pi], mu, false, hb)) != cudaSuccess) return e;
-            hb++;
+    if (b->persistent) {
+        for (int pi = 0; pi < 2; pi++) {
+            if ((e = half_sweep(b, par_order[pi], false, hb)) != cudaSuccess) return e;
+            hb += 4;
         }
-    for (int k = 0; k < b->cfg.n_or; k++)
+        for (int k = 0; k < b->cfg.n_or; k++)
+            for (int pi = 0; pi < 2; pi++)
+                if ((e = half_sweep(b, par_order[pi], true, 0)) != cudaSuccess) return e;
+    } else {
         for (int pi = 0; pi < 2; pi++)
-            for (int mu = 0; mu < 4; mu++)
-                if ((e = phase_batch(b, par_order[pi], mu, true, 0)) != cudaSuccess) return e;
+            for (int mu = 0; mu < 4; mu++) {
+                if ((e = phase_batch(b, par_order[pi], mu, false, hb)) != cudaSuccess) return e;
+                hb++;
+            }
+        for (int k = 0; k < b->cfg.n_or; k++)
+            for (int pi = 0; pi < 2; pi++)
+                for (int mu = 0; mu < 4; mu++)
+                    if ((e = phase_batch(b, par_order[pi], mu, true, 0)) != cudaSuccess) return e;
+    }
     if ((e = launch_add_u64(b->d_phase, hb, b->stream)) != cudaSuccess) return e;
     if (reunit && (e = gs_batch(b)) != cudaSuccess) return e;
     if (measure && (e = measure_batch(b)) != cudaSuccess) return e;
@@ -320,6 +515,7 @@ extern "C" int qg_batch_destroy(qg_batch *b)
     cudaFree(b->d_phase);
     cudaFree(b->d_overflow);
     cudaFree(b->d_series);
+    cudaFree(b->d_bar);
     if (b->stream) cudaStreamDestroy(b->stream);
     delete b;
     return QG_OK;
@@ -380,6 +576,8 @@ extern "C" int qg_batch_create(const qg_config *common, const qg_ensemble *ens, 
     if ((e = cudaMalloc(&b->d_phase, sizeof(uint64_t) * 2)) != cudaSuccess) return fail_free(e, "counters");
     b->d_meas = b->d_phase + 1;
     if ((e = cudaMalloc(&b->d_overflow, sizeof(uint32_t))) != cudaSuccess) return fail_free(e, "overflow");
+    if ((e = cudaMalloc(&b->d_bar, sizeof(GridBarrier))) != cudaSuccess) return fail_free(e, "barrier");
+    if ((e = cudaMemset(b->d_bar, 0, sizeof(GridBarrier))) != cudaSuccess) return fail_free(e, "barrier clear");
     if ((e = cudaMalloc(&b->d_series, sizeof(double) * 8 * n * (b->capacity ? b->capacity : 1))) != cudaSuccess)
         return fail_free(e, "series");
     std::vector<double> params(4 * (size_t)n, 0.0);
@@ -532,11 +730,42 @@ extern "C" int qg_batch_run(qg_batch *b, int nsweeps, int measure_every)
     return QG_OK;
 }
 
+// a grid barrier of the persistent half-sweep that ran out: reported once,
+// the barrier state reset (the fields are not trustworthy afterwards)
+static int barrier_check(qg_batch *b)
+{
+    GridBarrier h;
+    QB_CK(cudaMemcpy(&h, b->d_bar, sizeof(h), cudaMemcpyDeviceToHost), "barrier read");
+    if (h.err) {
+        QB_CK(cudaMemset(b->d_bar, 0, sizeof(GridBarrier)), "barrier reset");
+        return bfail("a grid barrier of the persistent half-sweep ran out (fields not updated consistently)",
+                     QG_ERR_CUDA);
+    }
+    return QG_OK;
+}
+
 extern "C" int qg_batch_sync(qg_batch *b)
 {
     if (!b) return QG_ERR_ARG;
     QB_CK(cudaStreamSynchronize(b->stream), "batch sync");
+    return barrier_check(b);
+}
+
+extern "C" int qg_batch_set_persistent(qg_batch *b, int enable)
+{
+    if (!b) return QG_ERR_ARG;
+    b->persistent = enable != 0;
+    destroy_batch_graphs(b);
     return QG_OK;
+}
+
+extern "C" int qg_batch_barrier_test(qg_batch *b, int skip_block)
+{
+    if (!b || skip_block < 0) return QG_ERR_ARG;
+    QB_CK(cudaStreamSynchronize(b->stream), "batch sync");
+    QB_CK(half_sweep(b, 1, false, 0, skip_block), "half sweep");
+    QB_CK(cudaStreamSynchronize(b->stream), "batch sync");
+    return barrier_check(b);
 }
 
 extern "C" int qg_batch_get_stream(qg_batch *b, void **stream)
@@ -550,6 +779,7 @@ extern "C" int qg_batch_series(qg_batch *b, double *out, uint64_t max_measuremen
 {
     if (!b || !n_measurements) return QG_ERR_ARG;
     QB_CK(cudaStreamSynchronize(b->stream), "batch sync");
+    if (int r = barrier_check(b)) return r;
     uint32_t ovf = 0;
     QB_CK(cudaMemcpy(&ovf, b->d_overflow, sizeof(ovf), cudaMemcpyDeviceToHost), "overflow read");
     const uint64_t have = b->measurements < b->capacity ? b->measurements : b->capacity;

@@ -265,8 +265,11 @@ template <typename Real> struct PrnOf<Real, 2> {
 // shared memory (staple3_staged; SU(3) FP32 links).
 // TW: twisted boundaries possible (the launch has A.twist set); without it
 // every twist test folds away at compile time (4 % of the phase's time)
+// sb: the block's staging buffer (STAGED; declared by the kernel, so that a
+// kernel running several directions holds one)
 template <int NC, typename Real, int PMODE, bool OR, int mu, bool STAGED, bool TW = false>
-__device__ __forceinline__ void phase_site(const Field<Real> &U, const Geom &G, const PhaseArgs &A, uint32_t t)
+__device__ __forceinline__ void phase_site(const Field<Real> &U, const Geom &G, const PhaseArgs &A, uint32_t t,
+                                           StageBuf *sb)
 {
     const int p = A.parity;
     Crd c = lex2crd(G, 2 * t);
@@ -286,8 +289,7 @@ __device__ __forceinline__ void phase_site(const Field<Real> &U, const Geom &G, 
         G3<Real> m0;
         M3<Real> st;
         if constexpr (STAGED) {
-            __shared__ __align__(16) StageBuf sb;
-            st = staple3_staged<mu>(U, G, t, nb, p, tw, sb, m0);
+            st = staple3_staged<mu>(U, G, t, nb, p, tw, *sb, m0);
         } else {
             m0 = U.ld3(mu, e0);
             st = staple3<mu>(U, G, t, nb, p, tw);
@@ -329,7 +331,12 @@ __global__ void __launch_bounds__(kPhaseBlock, MINB) k_phase(Field<Real> U, Geom
 {
     const uint32_t t = A.t_begin + blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= A.t_end) return;
-    phase_site<NC, Real, PMODE, OR, mu, STAGED, TW>(U, G, A, t);
+    if constexpr (STAGED) {
+        __shared__ __align__(16) StageBuf sb;
+        phase_site<NC, Real, PMODE, OR, mu, STAGED, TW>(U, G, A, t, &sb);
+    } else {
+        phase_site<NC, Real, PMODE, OR, mu, STAGED, TW>(U, G, A, t, nullptr);
+    }
 }
 
 // Overrelaxation of two links per thread (t and t + ceil(half/2)) with the

@@ -116,3 +116,46 @@ def test_beta_scan_split_over_ranks_gives_the_same_ensembles():
     assert job["plaquette"] == whole["plaquette"]
     assert job["polyakov_abs"] == whole["polyakov_abs"]
     assert job["updates"] == whole["updates"] and job["sites"] == whole["sites"]
+
+
+@pytest.mark.parametrize("group,precision,shape", [(3, 0, 4), (3, 0, 3), (3, 1, 0), (2, 0, 1)])
+def test_persistent_half_sweeps_give_the_same_chain(group, precision, shape):
+    """one persistent launch per half-sweep (four directions, grid barriers
+    between them) gives, bit for bit, the links and series of the per-phase
+    launches, heatbath and overrelaxation, with the reunitarisation and
+    measurement cadences of the graph"""
+    def run(persistent):
+        B = Q.Batch(common(group, precision), ENSEMBLES, max_measurements=8)
+        B.set_shape(shape)
+        B.set_persistent(persistent)
+        B.init(Q.START_HOT)
+        B.run(5, measure_every=2)
+        out = (B.series(), [B.download(e) for e in range(len(ENSEMBLES))])
+        B.close()
+        return out
+    ser0, links0 = run(False)
+    ser1, links1 = run(True)
+    assert np.array_equal(ser0, ser1)
+    assert all(np.array_equal(a, b) for a, b in zip(links0, links1))
+
+
+def test_persistent_grid_barrier_times_out_and_the_batch_recovers():
+    """the bounded grid barrier: one block leaves out its arrival, every
+    other block's wait runs out after a second, the call reports it, and
+    the batch is usable again (a fresh init and run reproduce a fresh
+    batch)"""
+    B = Q.Batch(common(3, 0), ENSEMBLES, max_measurements=4)
+    B.set_persistent(True)
+    B.init(Q.START_HOT)
+    rc, msg = B.barrier_test(3)
+    assert rc == Q.QG_ERR_CUDA and "grid barrier" in msg, (rc, msg)
+    B.sync()                                            # the flag was cleared by the report
+    B.init(Q.START_HOT)
+    B.run(2, measure_every=1)
+    ser = B.series()
+    R = Q.Batch(common(3, 0), ENSEMBLES, max_measurements=4)
+    R.init(Q.START_HOT)
+    R.run(2, measure_every=1)
+    assert np.array_equal(ser, R.series())
+    B.close()
+    R.close()
