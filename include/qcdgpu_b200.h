@@ -517,6 +517,33 @@ typedef struct qg_run_result {
     double kernel_ms_sigma[QG_KERNEL_CLASSES];
 } qg_run_result;
 
+/* Writes a run's results file in the reference's layout (model::
+ * lattice_write_results with lattice_make_header, model_make_header and
+ * lattice_make_header2, SU(N)/suncl/suncl.cpp:534-615,779-865,1679-1854):
+ * opts->output_path + opts->prefix + the reference's date-stamped name
+ * (from t_end) + ".txt"; the same sections, labels, column widths and
+ * order as the reference's GPU build, its device lines naming the CUDA
+ * platform and device; the F_munu blocks are always present (zero when
+ * F_munu is not measured), as the reference prints them.  What this
+ * library adds -- tau_int and the error of every mean, the overrelaxation
+ * and reunitarisation settings, the update rate -- goes to a companion file
+ * of the same name ending in "-stats.txt".  qg_run calls it; host only.
+ *   series:   [QG_OBS_COUNT][opts->iter] per-measurement values (zero for
+ *             observables not measured)
+ *   fmunu:    [QG_FMUNU_COLS][opts->iter] (opts->fmunu) or NULL
+ *   profiles: for axis 0..2 and each slice 6 values -- PL, PL_im,
+ *             PL_variance, PL_im_variance, S, S_variance (needed when
+ *             opts->pl_level > 2 or opts->get_actions_diff) or NULL
+ *   fmunu_cpu_lattice_variance: the 12 "CPU l.varnc" values or NULL (zero)
+ *   t_start, t_end: wall-clock times of the run (seconds since the epoch)
+ * path (path_len bytes) receives the results file's name.                 */
+int qg_write_results(const qg_config *cfg, const qg_run_options *opts, const qg_run_result *res, int resumed,
+                     const double *series, const double *fmunu, const double *profiles,
+                     const double *fmunu_cpu_lattice_variance, int64_t t_start, int64_t t_end,
+                     const char *platform, const char *device, char *path, size_t path_len);
+/* the CUDA runtime ("CUDA 12.9") and the current device's name            */
+int qg_device_info(char *platform, size_t platform_len, char *device, size_t device_len);
+
 /* defaults of the reference main() (QCDGPU.cpp:183-205) */
 int qg_default_run_options(qg_run_options *opts);
 /* Host only: read KEY = value lines ('#' starts a comment) and apply the

@@ -3,6 +3,7 @@
 # from the sources where they lie, into oracle/_ref/ (git-ignored):
 #   _ref/ref_ranlux   -- the reference host RANLUX (random/random.cpp)
 #   _ref/ref_cpurun   -- the reference sequential heatbath (SU(N)/suncpp)
+#   _ref/ref_qcdgpu   -- the reference main() in its CPU_RUN build (QCDGPU.cpp)
 # Test and baseline infrastructure only.
 # Usage: build_ref.sh [--probe] [reference root]
 #   the root is the argument, else $QCDGPU_REFERENCE, else /root/reference;
@@ -24,4 +25,11 @@ $CXX -O2 -D CPU_RUN -I "$HERE/ref_stub" -I "$R" -o "$OUT/ref_cpurun" "$HERE/ref_
     "$R/suncpp/su2/algebra_su2.cpp" "$R/suncpp/su2/update_su2.cpp" \
     "$R/suncpp/su3/algebra_su3.cpp" "$R/suncpp/su3/update_su3.cpp" \
     "$R/suncpp/Measurements/analysis_cpp.cpp" "$R/suncpp/coord_work/coord_work.cpp" "$R/suncpp/IO/io.cpp"
-echo "built $OUT/ref_ranlux $OUT/ref_cpurun"
+# the reference's own main() (QCDGPU.cpp, -D CPU_RUN): init.dat in, its
+# results file (lattice_write_results) out
+$CXX -O2 -D CPU_RUN -I "$HERE/ref_stub" -I "$R" -o "$OUT/ref_qcdgpu" "$R/QCDGPU.cpp" \
+    "$R/random/random.cpp" "$R/suncl/suncl.cpp" \
+    "$R/suncpp/su2/algebra_su2.cpp" "$R/suncpp/su2/update_su2.cpp" \
+    "$R/suncpp/su3/algebra_su3.cpp" "$R/suncpp/su3/update_su3.cpp" \
+    "$R/suncpp/Measurements/analysis_cpp.cpp" "$R/suncpp/coord_work/coord_work.cpp" "$R/suncpp/IO/io.cpp"
+echo "built $OUT/ref_ranlux $OUT/ref_cpurun $OUT/ref_qcdgpu"

@@ -50,7 +50,7 @@ EXPORTED_SYMBOLS = (
     "qg_measure_wilson_all", "qg_measure_fmunu", "qg_measure_action_profile", "qg_measure_polyakov_profile",
     "qg_measure_enqueue", "qg_measure_fetch", "qg_measure_plaquette_all", "qg_measure_polyakov_all",
     "qg_net_set", "qg_net_get", "qg_mh_phase", "qg_net_eps", "qg_mh_sweep", "qg_mh_stats", "qg_net_grad",
-    "qg_net_train",
+    "qg_net_train", "qg_write_results", "qg_device_info",
 )
 
 
@@ -93,6 +93,9 @@ class Info(ctypes.Structure):
     ]
 
 
+(OBS_S_TOTAL, OBS_PLQ_TOTAL, OBS_POLYAKOV, OBS_POLYAKOV_IM, OBS_POLYAKOV_P2, OBS_POLYAKOV_P4, OBS_WILSON,
+ OBS_PLQ_SPAT, OBS_PLQ_TEMP, OBS_S_SPAT, OBS_S_TEMP) = range(11)          # QG_OBS_*
+OBS_COUNT = 11
 OBS_NAMES = ("S_total", "Plq_total", "Polyakov_loop", "Polyakov_loop_im", "Polyakov_loop_P2",
              "Polyakov_loop_P4", "Wilson_loop", "Plq_spat", "Plq_temp", "S_spat", "S_temp")
 
@@ -266,6 +269,11 @@ def load_library(path=LIB_PATH):
     lib.qg_batch_set_shape.argtypes = [vp, ctypes.c_int]
     lib.qg_batch_set_shapes.argtypes = [vp, ctypes.c_int, ctypes.c_int]
     lib.qg_batch_get_shapes.argtypes = [vp, P(ctypes.c_int), P(ctypes.c_int)]
+    lib.qg_write_results.argtypes = [P(Config), P(RunOptions), P(RunResult), ctypes.c_int, P(ctypes.c_double),
+                                     P(ctypes.c_double), P(ctypes.c_double), P(ctypes.c_double), ctypes.c_int64,
+                                     ctypes.c_int64, ctypes.c_char_p, ctypes.c_char_p, ctypes.c_char_p,
+                                     ctypes.c_size_t]
+    lib.qg_device_info.argtypes = [ctypes.c_char_p, ctypes.c_size_t, ctypes.c_char_p, ctypes.c_size_t]
     lib.qg_batch_tune.argtypes = [vp, ctypes.c_int, P(ctypes.c_float)]
     lib.qg_batch_set_persistent.argtypes = [vp, ctypes.c_int]
     lib.qg_batch_barrier_test.argtypes = [vp, ctypes.c_int]
@@ -438,6 +446,29 @@ def parse_init_file(path, cfg=None, opts=None):
     if rc != QG_OK:
         raise QGError("qg_parse_init_file: %s" % lib.qg_last_error(None).decode())
     return cfg, opts
+
+
+def write_results(cfg, opts, res, series, fmunu=None, profiles=None, fmunu_cpu_lattice_variance=None,
+                  t_start=0, t_end=0, resumed=False, platform="", device=""):
+    """qg_write_results: the reference-layout results file of a finished run
+    (series [QG_OBS_COUNT][iter]); returns the file's path"""
+    lib = load_library()
+    dp = ctypes.POINTER(ctypes.c_double)
+
+    def arr(a):
+        if a is None:
+            return None
+        a = np.ascontiguousarray(a, dtype=np.float64)
+        return a, a.ctypes.data_as(dp)
+    keep = [arr(series), arr(fmunu), arr(profiles), arr(fmunu_cpu_lattice_variance)]
+    ptrs = [k[1] if k is not None else None for k in keep]
+    out = ctypes.create_string_buffer(1024)
+    rc = lib.qg_write_results(ctypes.byref(cfg), ctypes.byref(opts), ctypes.byref(res), int(resumed), ptrs[0],
+                              ptrs[1], ptrs[2], ptrs[3], int(t_start), int(t_end), platform.encode(),
+                              device.encode(), out, len(out))
+    if rc != QG_OK:
+        raise QGError("qg_write_results: %s" % lib.qg_last_error(None).decode())
+    return out.value.decode()
 
 
 def run(cfg, opts):

@@ -28,7 +28,7 @@ NVCC_FLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-fmad=false", "-Xcompile
 CUDA_SOURCES = ["qg_update_f32.cu", "qg_update_f64.cu", "qg_fields.cu", "qg_ranlux.cu", "qg_capi.cu",
                 "qg_noalloc.cu", "qg_batch.cu",
                 "qg_learned.cu"]
-LIB_HOST_SOURCES = ["qg_host.cpp", "qg_state.cpp"]          # C++ host code linked into the library
+LIB_HOST_SOURCES = ["qg_host.cpp", "qg_state.cpp", "qg_results.cpp"]          # C++ host code linked into the library
 CLI_SOURCES = ["qcdgpu_main.cpp"]
 
 

@@ -1469,3 +1469,19 @@ extern "C" int qg_links_download(qg_ctx *c, void *host, int layout)
     QG_CK(cudaStreamSynchronize(c->stream), "download sync");
     return QG_OK;
 }
+
+extern "C" int qg_device_info(char *platform, size_t platform_len, char *device, size_t device_len)
+{
+    int rt = 0, dev = 0;
+    cudaDeviceProp prop;
+    cudaError_t e = cudaRuntimeGetVersion(&rt);
+    if (e == cudaSuccess) e = cudaGetDevice(&dev);
+    if (e == cudaSuccess) e = cudaGetDeviceProperties(&prop, dev);
+    if (e != cudaSuccess) {
+        qg_set_global_error(std::string("qg_device_info: ") + cudaGetErrorString(e));
+        return QG_ERR_CUDA;
+    }
+    if (platform && platform_len) snprintf(platform, platform_len, "CUDA %d.%d", rt / 1000, (rt % 1000) / 10);
+    if (device && device_len) snprintf(device, device_len, "%s", prop.name);
+    return QG_OK;
+}

@@ -123,7 +123,7 @@ double retr(const M &a, int N)
 }
 void shift(int x[4], int d, int s, const int n[4]) { x[d] = (x[d] + s + n[d]) % n[d]; }
 
-struct HostObs { double plq_s, plq_t, s_s, s_t, pre, pim, p2, p4, wilson, f[12]; };
+struct HostObs { double plq_s, plq_t, s_s, s_t, pre, pim, p2, p4, wilson, f[12], f2[12]; };
 
 // -i Tr(P T_a) with T_a = lambda_a / 2 (SU(3)) or sigma_a / 2 (SU(2))
 // (trace_lambda1..8_double, su3_measurements_cl.cl:355-460;
@@ -192,8 +192,10 @@ HostObs host_measure(const Table &T, const qg_config &f, const qg_run_options &o
                                 double re, im;
                                 gen_proj(p, N, i1, re, im);
                                 h.f[2 * pl] += re; h.f[2 * pl + 1] += im;
+                                h.f2[2 * pl] += re * re; h.f2[2 * pl + 1] += im * im;
                                 gen_proj(p, N, i2, re, im);
                                 h.f[6 + 2 * pl] += re; h.f[7 + 2 * pl] += im;
+                                h.f2[6 + 2 * pl] += re * re; h.f2[7 + 2 * pl] += im * im;
                             }
                         }
                     h.plq_s += rs; h.plq_t += rt;
@@ -654,6 +656,9 @@ extern "C" int qg_run(const qg_config *cfg_in, const qg_run_options *o_in, qg_ru
         }
     }
     // LatticeCheckCPU: FP64 re-measurement of the final configuration
+    double f_varnc[12] = { 0 };
+    char platform[64] = "", device[128] = "";
+    if ((rc = qg_device_info(platform, sizeof(platform), device, sizeof(device)))) return bail(rc);
     if (o->verify) {
         std::vector<char> buf(info.ref_elems * (cfg.precision ? 8 : 4));
         if ((rc = qg_links_download(ctx, buf.data(), QG_LAYOUT_REFERENCE))) return bail(rc);
@@ -679,151 +684,32 @@ extern "C" int qg_run(const qg_config *cfg_in, const qg_run_options *o_in, qg_ru
             fmunu_row(h.f, res->fmunu_cpu_last);
             for (int k = 0; k < QG_FMUNU_COLS; k++)
                 ok = verify(res->fmunu_gpu_last[k], res->fmunu_cpu_last[k], cfg.precision == 0) && ok;
+            // the lattice variance of each projection on the final configuration
+            // (the "CPU l.varnc" lines; su3cpu.cpp:1367-1378)
+            for (int k = 0; k < 12; k++) f_varnc[k] = h.f2[k] / V - (h.f[k] / V) * (h.f[k] / V);
         }
         res->verification_passed = ok ? 1 : 0;
     }
     qg_destroy(ctx);
-    // lattice_write_results (suncl.cpp:1679-1854): header, statistics, rows
+    // the results file (lattice_write_results, suncl.cpp:1679-1854) and the
+    // companion statistics file (qg_results.cpp)
     if (o->write_results) {
-        char tbuf[64];
-        snprintf(tbuf, sizeof(tbuf), "%s", ctime(&t_end));
-        char name[96];
-        snprintf(name, sizeof(name), "%.2s-%.3s-%.2s-%.2s-%.2s-%.2s.txt", tbuf + 22, tbuf + 4, tbuf + 8, tbuf + 11,
-                 tbuf + 14, tbuf + 17);
-        snprintf(res->results_file, sizeof(res->results_file), "%s%s%s", o->output_path, o->prefix, name);
-        FILE *fp = fopen(res->results_file, "w");
-        if (!fp) return host_fail(QG_ERR_IO, std::string("cannot write ") + res->results_file);
-        const char *start_name[] = { "0", "1", "2", "3" };
-        fprintf(fp, " B200 SU(%d) simulator (qcdgpu_b200)\n\n", N);
-        fprintf(fp, " Monte Carlo simulation of 4D SU(%d) LGT\n\n", N);
-        fprintf(fp, " ***************************************************\n");
-        fprintf(fp, " lattice size                : %3d x %3d x %3d x %3d\n", cfg.size[0], cfg.size[1], cfg.size[2],
-                cfg.size[3]);
-        fprintf(fp, " init                        : %d\n", resume ? 0 : 1);
-        fprintf(fp, " ints (0=hot, 1=cold, 2=gid) : %s\n", start_name[cfg.start]);
-        fprintf(fp, " random series               : %u\n", cfg.randseries);
-        if (cfg.prng == QG_PRNG_RANLUX) fprintf(fp, " PRN generator (%3d)         : RANLUX\n", cfg.ranlux_nskip);
-        else fprintf(fp, " PRN generator               : PHILOX4x32-10\n");
-        fprintf(fp, " nav                         : %d\n", o->nav);
-        fprintf(fp, " niter                       : %d\n", o->niter);
-        fprintf(fp, " iter (# of samples)         : %d\n", o->iter);
-        fprintf(fp, " nhit                        : %d\n", cfg.nhit);
-        fprintf(fp, " nhitPar                     : %d\n", cfg.nhitpar);
-        fprintf(fp, " overrelaxation sweeps       : %d\n", cfg.n_or);
-        fprintf(fp, " precision                   : %s\n", cfg.precision ? "double" : "single");
-        fprintf(fp, " ***************************************************\n");
-        fprintf(fp, " Wilson loop R               : %d\n", cfg.wilson_r);
-        fprintf(fp, " Wilson loop T               : %d\n", cfg.wilson_t);
-        if (o->fmunu == 1) fprintf(fp, " FMUNU(%u, %u)\n", fi1, fi2);
-        if (o->fmunu == 2) fprintf(fp, " F0MU(%u, %u)\n", fi1, fi2);
-        fprintf(fp, " BETA                        : %16.13e\n", cfg.beta);
-        fprintf(fp, " PHI   (lambda_3)            : %16.13e\n", cfg.phi);
-        fprintf(fp, " OMEGA (lambda_8)            : %16.13e\n", cfg.omega);
-        fprintf(fp, " ***************************************************\n");
-        char ts[64], te[64];
-        snprintf(ts, sizeof(ts), "%s", ctime(&t_start));
-        snprintf(te, sizeof(te), "%s", ctime(&t_end));
-        int el = (int)difftime(t_end, t_start);
-        fprintf(fp, " Start time               : %s", ts);
-        fprintf(fp, " Finish time              : %s", te);
-        fprintf(fp, " Elapsed time             : %d:%2.2d:%2.2d:%2.2d\n", el / 86400, (el / 3600) % 24, (el / 60) % 60,
-                el % 60);
-        fprintf(fp, " ***************************************************\n");
-        static const char *names[QG_OBS_COUNT] = { "S_total", "Plq_total", "Polyakov_loop", "Polyakov_loop_im",
-                                                   "Polyakov_loop_P2", "Polyakov_loop_P4", "Wilson_loop",
-                                                   "Plq_spat", "Plq_temp", "S_spat", "S_temp" };
-        for (int k = 0; k <= QG_OBS_WILSON; k++) {
-            fprintf(fp, " Mean %-20s: % 16.13e\n", names[k], res->mean[k]);
-            fprintf(fp, " Variance %-16s: % 16.13e\n", names[k], res->variance[k]);
-        }
-        fprintf(fp, " ***************************************************\n");
-        char fnames[QG_FMUNU_COLS][24];
-        {
-            static const char *xyz = "xyz";
-            static const int hp[3][2] = { { 0, 1 }, { 0, 2 }, { 1, 2 } };
-            for (int k = 0; k < 12; k++) {
-                const int p = (k % 6) / 2, idx = k < 6 ? fi1 : fi2;
-                const char *ri = (k & 1) ? "im" : "re";
-                if (o->fmunu == 2) snprintf(fnames[k], 24, "Fmunu_%ct_%u_%s", xyz[p], idx, ri);
-                else snprintf(fnames[k], 24, "Fmunu_%c%c_%u_%s", xyz[hp[p][0]], xyz[hp[p][1]], idx, ri);
+        const size_t it = (size_t)o->iter;
+        std::vector<double> ser(QG_OBS_COUNT * it, 0.0), fser(o->fmunu ? QG_FMUNU_COLS * it : 0, 0.0);
+        for (int k = 0; k < QG_OBS_COUNT; k++)
+            for (size_t i = 0; i < d[k].size() && i < it; i++) ser[k * it + i] = d[k][i];
+        for (int k = 0; k < QG_FMUNU_COLS && o->fmunu; k++)
+            for (size_t i = 0; i < fd[k].size() && i < it; i++) fser[k * it + i] = fd[k][i];
+        std::vector<double> pr;
+        for (int a = 0; a < 3; a++)
+            for (const Slice &q : prof[a]) {
+                const double v[6] = { q.pl, q.pl_im, q.pl_var, q.pl_im_var, q.s, q.s_var };
+                pr.insert(pr.end(), v, v + 6);
             }
-            for (int k = 12; k < QG_FMUNU_COLS; k++)
-                snprintf(fnames[k], 24, "Fmunu_abs_%1u_%s", k < 14 ? fi1 : fi2, (k & 1) ? "im" : "re");
-        }
-        if (o->fmunu) {
-            for (int k = 0; k < QG_FMUNU_COLS; k++) fprintf(fp, " Mean %-20s: % 16.13e\n", fnames[k], res->fmunu_mean[k]);
-            for (int k = 0; k < QG_FMUNU_COLS; k++)
-                fprintf(fp, " Variance %-16s: % 16.13e\n", fnames[k], res->fmunu_variance[k]);
-            fprintf(fp, " ***************************************************\n");
-            for (int k = 0; k < QG_FMUNU_COLS; k++) {
-                fprintf(fp, " GPU last %-16s: % 16.13e\n", fnames[k], res->fmunu_gpu_last[k]);
-                fprintf(fp, " CPU last %-16s: % 16.13e\n", fnames[k], res->fmunu_cpu_last[k]);
-            }
-            fprintf(fp, " ***************************************************\n");
-        }
-        for (int k = 0; k <= QG_OBS_WILSON; k++) {
-            fprintf(fp, " Tau_int %-17s: % 16.13e\n", names[k], res->tau_int[k]);
-            fprintf(fp, " Error %-19s: % 16.13e\n", names[k], res->error[k]);
-        }
-        fprintf(fp, " ***************************************************\n");
-        for (int k = 0; k <= QG_OBS_WILSON; k++) {
-            fprintf(fp, " CPU last %-16s: % 16.13e\n", names[k], res->cpu_last[k]);
-            fprintf(fp, " GPU last %-16s: % 16.13e\n", names[k], res->gpu_last[k]);
-        }
-        if (res->verification_passed == 1) fprintf(fp, " *** Verification successfully passed! *************\n");
-        else if (res->verification_passed == 0) fprintf(fp, " --- Verification failed! --------------------------\n");
-        // profile sections (lattice_write_results, suncl.cpp:1694-1791)
-        static const char *axis_name[3] = { "X", "Y", "Z" };
-        if (o->pl_level > 2) {
-            fprintf(fp, " ***************************************************\n");
-            fprintf(fp, "Differentiated Polyakov loop data (#, PL, PL_im, PL_variance, PL_im_variance):\n");
-            for (int a = 0; a < 3; a++) {
-                fprintf(fp, "\n%s              ", axis_name[a]);
-                for (int k = 0; k < cfg.size[a]; k++) fprintf(fp, "%2u                   ", (unsigned)k);
-                fprintf(fp, "\nPL             ");
-                for (const Slice &q : prof[a]) fprintf(fp, "% 16.13e ", q.pl);
-                fprintf(fp, "\nPL_im          ");
-                for (const Slice &q : prof[a]) fprintf(fp, "% 16.13e ", q.pl_im);
-                fprintf(fp, "\nPL_variance    ");
-                for (const Slice &q : prof[a]) fprintf(fp, "% 16.13e ", q.pl_var);
-                fprintf(fp, "\nPL_im_variance ");
-                for (const Slice &q : prof[a]) fprintf(fp, "% 16.13e ", q.pl_im_var);
-                fprintf(fp, "\n");
-            }
-        }
-        if (o->get_actions_diff) {
-            fprintf(fp, " ***************************************************\n");
-            fprintf(fp, "Differentiated S data (#, S_total, S_variance):\n");
-            for (int a = 0; a < 3; a++) {
-                fprintf(fp, "\n%s              ", axis_name[a]);
-                for (int k = 0; k < cfg.size[a]; k++) fprintf(fp, "%2u                   ", (unsigned)k);
-                fprintf(fp, "\nS             ");
-                for (const Slice &q : prof[a]) fprintf(fp, "% 16.13e ", q.s);
-                fprintf(fp, "\nS_variance    ");
-                for (const Slice &q : prof[a]) fprintf(fp, "% 16.13e ", q.s_var);
-                fprintf(fp, "\n");
-            }
-        }
-        fprintf(fp, " ***************************************************\n");
-        fprintf(fp, " Data fields:\n    #,  ");
-        std::vector<int> cols;
-        if (o->get_plaquettes) { cols.push_back(QG_OBS_PLQ_SPAT); cols.push_back(QG_OBS_PLQ_TEMP); cols.push_back(QG_OBS_PLQ_TOTAL); }
-        if (o->get_wilson) cols.push_back(QG_OBS_WILSON);
-        if (o->get_actions) { cols.push_back(QG_OBS_S_SPAT); cols.push_back(QG_OBS_S_TEMP); cols.push_back(QG_OBS_S_TOTAL); }
-        if (o->pl_level > 0) { cols.push_back(QG_OBS_POLYAKOV); cols.push_back(QG_OBS_POLYAKOV_IM); }
-        if (o->pl_level > 1) { cols.push_back(QG_OBS_POLYAKOV_P2); cols.push_back(QG_OBS_POLYAKOV_P4); }
-        for (int k : cols) fprintf(fp, "%-21s ", names[k]);
-        if (o->fmunu)
-            for (int k = 0; k < QG_FMUNU_COLS; k++) fprintf(fp, "%-21s ", fnames[k]);
-        fprintf(fp, "\n ***************************************************\n");
-        for (int i = 0; i < o->iter; i++) {
-            fprintf(fp, "%5i", i);
-            for (int k : cols) fprintf(fp, " % 16.13e", d[k][i]);
-            if (o->fmunu)
-                for (int k = 0; k < QG_FMUNU_COLS; k++) fprintf(fp, " % 16.13e", fd[k][i]);
-            fprintf(fp, "\n");
-        }
-        fclose(fp);
+        if ((rc = qg_write_results(&cfg, o, res, resume ? 1 : 0, ser.data(), o->fmunu ? fser.data() : nullptr,
+                                   pr.data(), o->fmunu && o->verify ? f_varnc : nullptr, (int64_t)t_start,
+                                   (int64_t)t_end, platform, device, res->results_file, sizeof(res->results_file))))
+            return rc;
     }
     if (!o->quiet) {
         printf("\n #        ");

@@ -127,6 +127,9 @@ def test_run_fmunu_and_profiles(tmp_path, group, field):
         assert len(rows) == 2 and all(len(r.split()) == 1 + dims[a] for r in rows), tag
     pl_rows = [l for l in lines if l.startswith("PL             ")]
     assert len(pl_rows) == 3 and all(len(r.split()) == 1 + dims[a] for a, r in enumerate(pl_rows))
+    # the CPU lattice variance of each F projection on the final field
+    varnc = [float(l.split(":")[1]) for l in lines if l.startswith(" CPU l.varnc")]
+    assert len(varnc) == 12 and all(v > 0 for v in varnc), varnc
     rows = [l for l in lines if l[:5].strip().isdigit()]
     assert len(rows) == 4
     # #, plaquettes 3, actions 3, Polyakov 2, P2/P4 2, F_munu 16
@@ -209,3 +212,28 @@ def test_profile_table_leaves_the_run_unchanged(tmp_path):
     assert set(t) == set(Q.KERNEL_NAMES) and all(m > 0 for m, _ in t.values())
     assert np.array_equal(L.download(), before) and L.info().phase_counter == 0
     L.close()
+
+
+@pytest.mark.parametrize("group,beta", [(3, 5.9), (2, 2.3)])
+def test_run_results_file_follows_the_reference_writer(tmp_path, group, beta):
+    """qg_run with the settings of the reference's own results file
+    (tests/golden/reference_results_su{3,2}.txt, written by its CPU_RUN
+    main()): the file it writes has the reference's layout line by line
+    (test_results_file.py's comparison), the cold start's row 0 equals the
+    reference's, and the verification line reports the CPU re-check"""
+    import re
+    import test_results_file as TR
+    ref = open(os.path.join(TR.GOLDEN, "reference_results_su%d.txt" % group)).read().split("\n")
+    cfg = Q.default_config(group=group, size=(4, 4, 4, 6), precision=1, start=Q.START_COLD, prng=Q.PRNG_RANLUX,
+                           beta=beta, randseries=54, nhit=10, ranlux_nskip=223)
+    opts = Q.default_run_options(iter=4, niter=2, nav=2, pl_level=0, get_wilson=0, fmunu=0, get_plaquettes=1,
+                                 get_actions=1, quiet=1, output_path=str(tmp_path) + "/", prefix="su%d-" % group)
+    res = Q.run(cfg, opts)
+    got = open(res.results_file.decode()).read().split("\n")
+    pats = TR.gpu_build_layout(ref)
+    assert len(got) == len(pats)
+    for i, (g, p) in enumerate(zip(got, pats)):
+        assert re.fullmatch(p, g), (i + 1, g, p)
+    row0 = [l for l in got if l[:5].strip() == "0"][0]
+    assert row0.split() == [l for l in ref if l[:5].strip() == "0"][0].split()
+    assert " *** Verification successfully passed! *" in "\n".join(got)
