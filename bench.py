@@ -158,6 +158,73 @@ def cpu_baseline_line(size, seconds_target=15.0):
             "cpu_model": cpu_model(), "host_cpus": os.cpu_count()}
 
 
+def table_rows_fp64(table, size, rowsize):
+    """an FP64 SU(3) reference-layout table (12 planes of rowsize float4s)
+    -> the reference CPU path's stored rows per (site, direction): u1 u2 u3
+    v1 v2 v3 as (re, im), site-major, direction fastest"""
+    import numpy as np
+    V = size ** 4
+    t = table.reshape(12, rowsize, 4)[:, :V, :]
+    p1, p2, p3 = t[0:4].transpose(1, 0, 2), t[4:8].transpose(1, 0, 2), t[8:12].transpose(1, 0, 2)
+    return np.ascontiguousarray(np.stack([p1[..., 0], p2[..., 0], p1[..., 1], p2[..., 1], p1[..., 2], p2[..., 2],
+                                          p3[..., 0], p3[..., 2], p3[..., 1], p3[..., 3], p1[..., 3], p2[..., 3]],
+                                         axis=-1))
+
+
+def like_for_like(Q, torch, size, seconds_target=10.0):
+    """Heatbath-only sweeps in the reference's own arithmetic on both sides:
+    SU(3) size^4 beta=6.0, FP64 links, RANLUX3 batches (one per phase, the
+    reference's lattice_simulate cadence; generated on the GPU inside the
+    timed sweeps), NHIT=10, Gram-Schmidt every sweep.  Ours: CUDA events
+    around 10 sweeps after 20 thermalising ones.  The reference CPU path
+    (SU(N)/suncpp, FP64, RANLUX3, NHIT=10): the same thermalised FP64
+    configuration loaded into each of its concurrent processes, per-phase
+    wall times."""
+    cfg = Q.default_config(group=3, size=size, precision=1, start=Q.START_COLD, prng=Q.PRNG_RANLUX, beta=BETA,
+                           nhit=10, ranlux_nskip=223, n_or=0, reunit_every=1, reunit_fp64=1, randseries=54,
+                           prng_instances=16384)
+    L = Q.Lattice(cfg)
+    L.seed()
+    L.init()
+    L.sweep(20)
+    s = torch.cuda.ExternalStream(L.stream())
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    L.sync()
+    e0.record(s)
+    L.sweep(10)
+    e1.record(s)
+    e1.synchronize()
+    ms_sweep = e0.elapsed_time(e1) / 10
+    V = size ** 4
+    out = {"what": "heatbath-only sweeps in the reference's own arithmetic: SU(3) %d^4 beta=%.1f, FP64 links, RANLUX3 "
+                   "batches generated for every phase, NHIT=10, Gram-Schmidt every sweep, thermalised start (20 "
+                   "sweeps)" % (size, BETA),
+           "ours": {"value": 4 * V / (ms_sweep / 1e3), "unit": UNIT, "ms_per_phase": ms_sweep / 8,
+                    "how": "CUDA events around 10 sweeps (8 RANLUX batches + 8 heatbath phases + Gram-Schmidt each)"}}
+    if os.path.exists(ref_binary()):
+        rows = table_rows_fp64(L.download(), size, L.info().rowsize)
+        with tempfile.TemporaryDirectory() as d:
+            f = os.path.join(d, "thermalised.bin")
+            rows.tofile(f)
+            procs = cpu_workers(size)
+            cmd = [ref_binary(), "phases_from", "3"] + [str(size)] * 4 + [repr(BETA)]
+            ps = [subprocess.Popen(cmd + [str(54 + i), f, "0", "2"], stdout=subprocess.PIPE, text=True)
+                  for i in range(procs)]
+            times = []
+            for p in ps:
+                o, _ = p.communicate()
+                if p.returncode != 0:
+                    raise RuntimeError("reference CPU path failed")
+                times.append([float(x) for x in o.split()[1:]])
+        wall = max(sum(t) for t in times)
+        out["reference"] = {"value": procs * 2 * (V // 2) / wall, "unit": UNIT, "cores": procs,
+                            "ms_per_phase_per_process": 1e3 * wall / 2,
+                            "how": "%d concurrent processes of the reference CPU path, each from the same thermalised "
+                                   "configuration, 2 heatbath phases of %d link updates each" % (procs, V // 2)}
+    L.close()
+    return out
+
+
 REF_MAX_STEPS = 60
 
 
@@ -355,6 +422,7 @@ def run_ours(args):
     }
     if not args.no_cpu_baseline and world == 1:
         line["cpu_baseline"] = cpu_baseline_line(args.size)
+        line["like_for_like"] = like_for_like(Q, torch, args.size)
     print(json.dumps(line))
     return 0
 

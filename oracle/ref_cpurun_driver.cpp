@@ -16,6 +16,8 @@
 //       cold start, <warm> untimed phases, then <timed> phases (the sweep's
 //       odd X..T, even X..T order, V/2 link updates each); prints
 //       "phase_seconds t1 t2 ..."
+//   ref_cpurun phases_from <group> <L1> <L2> <L3> <L4> <beta> <randseries> <in> <warm> <timed>
+//       as "phases", from the start field read from <in> (the "links" format)
 //   ref_cpurun links <group> <L1> <L2> <L3> <L4> <beta> <randseries> <phases> <in|-> <out>
 //       cold start, or the stored rows read from <in> (per site, dir fastest:
 //       SU(3) u1 u2 u3 v1 v2 v3, SU(2) u1 u2, each re im, as doubles; the
@@ -72,7 +74,8 @@ static void get_rows(su_2 &m, const double *r)
 }
 
 template <typename su_n>
-static int links(int group, int *L, double beta, int series, int phases, const char *in, const char *out)
+static int links(int group, int *L, double beta, int series, int phases, const char *in, const char *out,
+                 int timed = 0)
 {
     modelCPU<su_n> *lat = new modelCPU<su_n>;
     lat->lattice_ndCPU = 4;
@@ -103,6 +106,22 @@ static int links(int group, int *L, double beta, int series, int phases, const c
         for (size_t i = 0; i < nlinks; i++) get_rows(lat->lattice_tableCPU[i], rows + i * nrow);
     }
     for (int k = 0; k < phases; k++) phase(lat, prng, k);
+    if (timed > 0) {                          // phases_from: time the next phases, write nothing
+        printf("phase_seconds");
+        for (int k = phases; k < phases + timed; k++) {
+            auto t0 = std::chrono::steady_clock::now();
+            phase(lat, prng, k);
+            auto t1 = std::chrono::steady_clock::now();
+            printf(" %.6f", std::chrono::duration<double>(t1 - t0).count());
+        }
+        printf("\n");
+        free(rows);
+        lat->delete_latticeCPU();
+        free(lat->lattice_size);
+        delete lat;
+        delete prng;
+        return 0;
+    }
     for (size_t i = 0; i < nlinks; i++) put_rows(lat->lattice_tableCPU[i], rows + i * nrow);
     FILE *f = fopen(out, "wb");
     if (!f || fwrite(rows, sizeof(double), nlinks * nrow, f) != nlinks * nrow) {
@@ -175,6 +194,13 @@ static int run(int mode, int group, int *L, double beta, int ints, int series, i
 int main(int argc, char **argv)
 {
     if (argc < 11) { fprintf(stderr, "see source for usage\n"); return 2; }
+    if (strcmp(argv[1], "phases_from") == 0) {
+        if (argc < 12) { fprintf(stderr, "see source for usage\n"); return 2; }
+        int L[4] = { atoi(argv[3]), atoi(argv[4]), atoi(argv[5]), atoi(argv[6]) };
+        return atoi(argv[2]) == 3
+                   ? links<su_3>(3, L, atof(argv[7]), atoi(argv[8]), atoi(argv[10]), argv[9], nullptr, atoi(argv[11]))
+                   : links<su_2>(2, L, atof(argv[7]), atoi(argv[8]), atoi(argv[10]), argv[9], nullptr, atoi(argv[11]));
+    }
     if (strcmp(argv[1], "links") == 0) {
         if (argc < 12) { fprintf(stderr, "see source for usage\n"); return 2; }
         int L[4] = { atoi(argv[3]), atoi(argv[4]), atoi(argv[5]), atoi(argv[6]) };

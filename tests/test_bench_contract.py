@@ -57,3 +57,15 @@ def test_our_arm_line():
     assert d["gpu_launches"] == 5 * (8 + 8 * 4 + 1) + sum(1 for n in range(6, 11) if n % 10 == 0)
     assert {"sm_mhz", "sm_max_mhz", "reasons"} <= set(d["clocks"])
     assert "workload" in d["config"] and "fits the 126 MB L2" in d["config"]["l2"]
+
+
+def test_like_for_like_row_conversion_equals_the_oracles():
+    """bench.py hands the reference CPU path its thermalised start in the
+    reference's stored-row format; the conversion equals the oracle's"""
+    import numpy as np
+
+    import _oracle as O
+    import bench
+    c = O.make_cfg(group=3, dims=(4, 4, 4, 4), precision=1, beta=6.0, row_align=64)
+    t = np.random.default_rng(3).standard_normal(12 * c.rowsize * 4)
+    assert np.array_equal(bench.table_rows_fp64(t, 4, c.rowsize), O.table_to_rows(c, t))
