@@ -59,8 +59,9 @@ def test_cli_runs_init_file(tmp_path):
     out = subprocess.run([exe, p], capture_output=True, text=True, timeout=120)
     assert out.returncode == 0, out.stderr
     assert "Verification successfully passed!" in out.stdout
-    files = [f for f in os.listdir(str(tmp_path)) if f.startswith("su3-") and f.endswith(".txt")]
-    assert len(files) == 1
+    files = sorted(f for f in os.listdir(str(tmp_path)) if f.startswith("su3-") and f.endswith(".txt"))
+    # the results file and its companion with this library's statistics
+    assert len(files) == 2 and files[0][:-4] + "-stats.txt" == files[1], files
 
 
 @pytest.mark.parametrize("prng,start,precision", [(Q.PRNG_PHILOX, Q.START_HOT, 0), (Q.PRNG_RANLUX, Q.START_HOT, 0),
@@ -128,8 +129,12 @@ def test_run_fmunu_and_profiles(tmp_path, group, field):
     pl_rows = [l for l in lines if l.startswith("PL             ")]
     assert len(pl_rows) == 3 and all(len(r.split()) == 1 + dims[a] for a, r in enumerate(pl_rows))
     # the CPU lattice variance of each F projection on the final field
+    # (SU(2): the generator projections are real, their Im columns vanish)
     varnc = [float(l.split(":")[1]) for l in lines if l.startswith(" CPU l.varnc")]
-    assert len(varnc) == 12 and all(v > 0 for v in varnc), varnc
+    assert len(varnc) == 12 and all(v >= 0 for v in varnc), varnc
+    assert all(v > 0 for v in (varnc if group == 3 else varnc[0::2])), varnc
+    if group == 2:
+        assert all(v == 0 for v in varnc[1::2]), varnc
     rows = [l for l in lines if l[:5].strip().isdigit()]
     assert len(rows) == 4
     # #, plaquettes 3, actions 3, Polyakov 2, P2/P4 2, F_munu 16
