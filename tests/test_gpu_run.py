@@ -61,7 +61,8 @@ def test_cli_runs_init_file(tmp_path):
     assert "Verification successfully passed!" in out.stdout
     files = sorted(f for f in os.listdir(str(tmp_path)) if f.startswith("su3-") and f.endswith(".txt"))
     # the results file and its companion with this library's statistics
-    assert len(files) == 2 and files[0][:-4] + "-stats.txt" == files[1], files
+    main = [f for f in files if not f.endswith("-stats.txt")]
+    assert len(files) == 2 and len(main) == 1 and main[0][:-4] + "-stats.txt" in files, files
 
 
 @pytest.mark.parametrize("prng,start,precision", [(Q.PRNG_PHILOX, Q.START_HOT, 0), (Q.PRNG_RANLUX, Q.START_HOT, 0),
