@@ -147,8 +147,10 @@ template <int N>
 __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
 
 // slots of 16 bytes x kPhaseBlock threads: two term buffers of 9 slots
-// (3 links x 3 planes) and 3 slots for the updated link itself
-constexpr int kTermSlots = 9, kOwnSlot = 2 * kTermSlots, kStageSlots = 2 * kTermSlots + 3;
+// (3 links x 3 planes); the updated link itself goes into the forward
+// buffer once the last forward term has been read (36 KB per block, so
+// five blocks fit an SM with room to spare)
+constexpr int kTermSlots = 9, kOwnSlot = 0, kStageSlots = 2 * kTermSlots;
 using StageBuf = float4[kStageSlots][kPhaseBlock];
 
 __device__ __forceinline__ void stage_link(const Field<float> &U, int dir, uint32_t e, StageBuf &sb, int slot)
@@ -176,9 +178,11 @@ __device__ __forceinline__ int32_t pick4(const int32_t (&a)[4], int k)
 // the forward and backward term code, so the kernel's instruction stream
 // stays small); also brings in the updated link U_mu(x).  Term buffer 0
 // holds the forward term of the plane, buffer 1 the backward term; the
-// next plane's copies are issued as soon as a buffer has been read.
-// Every iteration commits one group per buffer (empty on the last plane)
-// so that wait_group 1 always means "this buffer has landed".
+// next plane's copies are issued as soon as a buffer has been read; on the
+// last plane the forward buffer receives U_mu(x) instead, so its copy runs
+// under the last backward term.  Every iteration commits one group per
+// buffer (the last backward group is empty) so that wait_group 1 always
+// means "this buffer has landed".
 template <int mu>
 __device__ __forceinline__ M3<float> staple3_staged(const Field<float> &U, const Geom &G, uint32_t t, const Nbr &n,
                                                    int p, const Twist<float> &tw, StageBuf &sb, G3<float> &m0)
@@ -201,7 +205,6 @@ __device__ __forceinline__ M3<float> staple3_staged(const Field<float> &U, const
         if (tw.on && dir == 1 && xc == tw.xlast) m = twist3(m, tw.phi, tw.omega);
         return m;
     };
-    stage_link(U, mu, own, sb, kOwnSlot);
     fwd_copy(nu_of(mu, 0));
     cp_async_commit();
     bwd_copy(nu_of(mu, 0));
@@ -214,7 +217,10 @@ __device__ __forceinline__ M3<float> staple3_staged(const Field<float> &U, const
         const int xnmmu = (nu == 0) ? n.xm : xmu;
         cp_async_wait<1>();
         MR3 fw = staple_fwd3_rows(get(0, nu, xmu), get(3, mu, xnp), get(6, nu, n.x));
-        if (i < 2) fwd_copy(nu_of(mu, i + 1));
+        if (i < 2)
+            fwd_copy(nu_of(mu, i + 1));
+        else
+            stage_link(U, mu, own, sb, kOwnSlot);
         cp_async_commit();
         cp_async_wait<1>();
         MR3 bw = staple_bwd3_rows(get(kTermSlots, nu, xnmmu), get(kTermSlots + 3, mu, xnm),
