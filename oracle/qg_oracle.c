@@ -322,28 +322,39 @@ static void ol_sincos(double x, double *s, double *c)
     *c = (q == 0) ? cs : (q == 1) ? -sn : (q == 2) ? -cs : sn;
 }
 
+/* natural log of a positive normal y, table-driven (P. T. P. Tang, ACM
+ * TOMS 16 (1990) 378-400): y = 2^e m, m in [1, 2); k = the nearest multiple
+ * of 1/128 to m - 1 from the top 8 mantissa bits; r = fma(m, c_k, -1),
+ * |r| <= 2^-8; log1p(r) by its Taylor terms to r^7; log y = (e ln2_hi +
+ * L_hi) + ((e ln2_lo + L_lo) + log1p(r)) with L = -log c_k.  The table is
+ * the device routine's (qg_logtab.h), the operations qg_log's in order. */
+#include "../qcdgpu_b200/csrc/qg_logtab.h"
+static const double ol_log_c[QG_LOG_TABLE_SIZE] = QG_LOG_C_INIT;
+static const double ol_log_hi[QG_LOG_TABLE_SIZE] = QG_LOG_LHI_INIT;
+static const double ol_log_lo[QG_LOG_TABLE_SIZE] = QG_LOG_LLO_INIT;
+
 static double ol_log(double y)
 {
-    int e;
-    double m = frexp(y, &e);
-    if (m < 0.70710678118654752440) { m = m * 2.0; e -= 1; }
-    double s = (m - 1.0) / (m + 1.0);
-    double s2 = s * s;
-    double p = 1.0 / 23.0;
-    p = fma(p, s2, 1.0 / 21.0);
-    p = fma(p, s2, 1.0 / 19.0);
-    p = fma(p, s2, 1.0 / 17.0);
-    p = fma(p, s2, 1.0 / 15.0);
-    p = fma(p, s2, 1.0 / 13.0);
-    p = fma(p, s2, 1.0 / 11.0);
-    p = fma(p, s2, 1.0 / 9.0);
-    p = fma(p, s2, 1.0 / 7.0);
-    p = fma(p, s2, 1.0 / 5.0);
-    p = fma(p, s2, 1.0 / 3.0);
-    double t = 2.0 * fma(p * s2, s, s);
-    const double LN2_HI = 6.93147180369123816490e-01, LN2_LO = 1.90821492927058770002e-10;
-    double de = (double)e;
-    return fma(de, LN2_HI, fma(de, LN2_LO, t));
+    int64_t b;
+    memcpy(&b, &y, sizeof(b));
+    const int e = (int)(b >> 52) - 1023;
+    const int k = (int)(((b >> 44) & 0xFF) + 1) >> 1;
+    const int64_t mb = (b & 0x000FFFFFFFFFFFFFLL) | 0x3FF0000000000000LL;
+    double m;
+    memcpy(&m, &mb, sizeof(m));
+    const double r = fma(m, ol_log_c[k], -1.0);
+    double q = 1.0 / 7.0;
+    q = fma(q, r, -1.0 / 6.0);
+    q = fma(q, r, 1.0 / 5.0);
+    q = fma(q, r, -0.25);
+    q = fma(q, r, 1.0 / 3.0);
+    q = fma(q, r, -0.5);
+    const double r2 = r * r;
+    const double l1p = fma(r2, q, r);
+    const double de = (double)e;
+    const double hi = fma(de, QG_LN2_HI, ol_log_hi[k]);
+    const double lo = fma(de, QG_LN2_LO, ol_log_lo[k]);
+    return hi + (lo + l1p);
 }
 
 /* exp(x), |x| <= 700: x = k ln2 + r (Cody-Waite, two-part ln 2), Taylor

@@ -101,30 +101,41 @@ __device__ __forceinline__ void qg_sincosf(float x, float *s, float *c)
     *c = (q == 0) ? cs : (q == 1) ? -sn : (q == 2) ? -cs : sn;
 }
 
-// natural log for 0 < y < 2^64: y = m 2^e with m in [sqrt(1/2), sqrt(2)),
-// log m = 2 atanh(s), s = (m-1)/(m+1), odd series to s^23; ln 2 in two parts
+// natural log of a positive normal y, table-driven (P. T. P. Tang, ACM
+// TOMS 16 (1990) 378-400): y = 2^e m, m in [1, 2); k = the nearest multiple
+// of 1/128 to m - 1 (from the top 8 mantissa bits, k in 0..128); with
+// c_k = RN(1/(1 + k/128)) the reduced argument r = fma(m, c_k, -1) has
+// |r| <= 2^-8, so log1p(r) needs the Taylor terms to r^7 only; then
+// log y = (e ln2_hi + L_hi) + ((e ln2_lo + L_lo) + log1p(r)), L = -log c_k.
+// The heads are multiples of 2^-32, so their sum is exact, and for y just
+// below 1 (k = 128, c = 1/2, L = ln 2) heads and tails cancel exactly.  No
+// division.  The table is qg_logtab.h (gen_logtab.py); read through the
+// read-only data cache.
+#include "qg_logtab.h"
+static __device__ const double kLogC[QG_LOG_TABLE_SIZE] = QG_LOG_C_INIT;
+static __device__ const double kLogHi[QG_LOG_TABLE_SIZE] = QG_LOG_LHI_INIT;
+static __device__ const double kLogLo[QG_LOG_TABLE_SIZE] = QG_LOG_LLO_INIT;
+
 __device__ __forceinline__ double qg_log(double y)
 {
-    int e;
-    double m = frexp(y, &e);                             // m in [0.5, 1)
-    if (m < 0.70710678118654752440) { m = m * 2.0; e -= 1; }
-    double s = (m - 1.0) / (m + 1.0);
-    double s2 = s * s;
-    double p = 1.0 / 23.0;
-    p = FMA(p, s2, 1.0 / 21.0);
-    p = FMA(p, s2, 1.0 / 19.0);
-    p = FMA(p, s2, 1.0 / 17.0);
-    p = FMA(p, s2, 1.0 / 15.0);
-    p = FMA(p, s2, 1.0 / 13.0);
-    p = FMA(p, s2, 1.0 / 11.0);
-    p = FMA(p, s2, 1.0 / 9.0);
-    p = FMA(p, s2, 1.0 / 7.0);
-    p = FMA(p, s2, 1.0 / 5.0);
-    p = FMA(p, s2, 1.0 / 3.0);
-    double t = 2.0 * FMA(p * s2, s, s);
-    const double LN2_HI = 6.93147180369123816490e-01, LN2_LO = 1.90821492927058770002e-10;
-    double de = (double)e;
-    return FMA(de, LN2_HI, FMA(de, LN2_LO, t));
+    const long long b = __double_as_longlong(y);
+    const int e = (int)(b >> 52) - 1023;
+    const int k = (int)(((b >> 44) & 0xFF) + 1) >> 1;
+    const double m = __longlong_as_double((b & 0x000FFFFFFFFFFFFFLL) | 0x3FF0000000000000LL);
+    const double c = __ldg(kLogC + k), lh = __ldg(kLogHi + k), ll = __ldg(kLogLo + k);
+    const double r = FMA(m, c, -1.0);
+    double q = 1.0 / 7.0;
+    q = FMA(q, r, -1.0 / 6.0);
+    q = FMA(q, r, 1.0 / 5.0);
+    q = FMA(q, r, -0.25);
+    q = FMA(q, r, 1.0 / 3.0);
+    q = FMA(q, r, -0.5);
+    const double r2 = r * r;
+    const double l1p = FMA(r2, q, r);
+    const double de = (double)e;
+    const double hi = FMA(de, QG_LN2_HI, lh);
+    const double lo = FMA(de, QG_LN2_LO, ll);
+    return hi + (lo + l1p);
 }
 
 // exp(x) for |x| <= 700: x = k ln2 + r (Cody-Waite, ln 2 in two parts),

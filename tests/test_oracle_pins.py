@@ -153,7 +153,9 @@ def site_coords(c, s):
 
 def test_own_elementary_functions_accuracy():
     """The sin/cos/log routines the update path uses (own Cody-Waite +
-    Taylor / atanh-series code) stay within 2 ulp of the C library."""
+    Taylor code; the table-driven log) stay within 2 ulp of the C library:
+    on the heatbath's arguments 1 - r, on a log-uniform sweep of the normal
+    range and just below and above 1 (where the table's heads cancel)."""
     lib = O.lib
     for n in ("ol_sin", "ol_cos", "ol_logd"):
         getattr(lib, n).argtypes = [ctypes.c_double]
@@ -164,10 +166,17 @@ def test_own_elementary_functions_accuracy():
         for f, g in ((lib.ol_sin, np.sin), (lib.ol_cos, np.cos)):
             a, b = f(float(x)), float(g(x))
             assert abs(a - b) <= 2 * np.spacing(max(abs(b), 1e-300)) + 1e-17, (x, a, b)
-    ys = np.concatenate([1.0 - np.float32(rng.uniform(0, 1, 20000)).astype(np.float64), [2.0 ** -24, 0.5, 1.0]])
+    near1 = np.concatenate([1.0 - np.ldexp(1.0, -np.arange(1, 54)), 1.0 + np.ldexp(1.0, -np.arange(1, 53)),
+                            1.0 + rng.uniform(-2 ** -6, 2 ** -6, 5000)])
+    ys = np.concatenate([1.0 - np.float32(rng.uniform(0, 1, 20000)).astype(np.float64), [2.0 ** -24, 0.5, 1.0],
+                         10.0 ** rng.uniform(-300, 300, 20000), near1])
+    worst = 0.0
     for y in ys:
         a, b = lib.ol_logd(float(y)), float(np.log(y))
         assert abs(a - b) <= 2 * np.spacing(abs(b)) + 1e-300, (y, a, b)
+        if b != 0.0:
+            worst = max(worst, abs(a - b) / float(np.spacing(abs(b))))
+    print("worst log error: %.2f ulp" % worst)
 
 
 def test_own_float_sincos_accuracy():
@@ -267,3 +276,30 @@ def test_heatbath_links_live_against_reference_binary_8x4(group, beta):
     d = float(np.max(np.abs(tab - ref)))
     print("SU(%d) 8^4 two sweeps: max|dU| = %.3g" % (group, d))
     assert d <= 1e-12
+
+
+def test_log_table_is_its_generator_output_and_exact():
+    """qg_logtab.h (shared by the device log and the oracle's) is what
+    gen_logtab.py writes, c_k is the correctly rounded 1/(1 + k/128), the
+    heads are multiples of 2^-32 and head + tail equals -log c_k to within
+    2^-60 (checked with Python's decimal logarithm at 40 digits)"""
+    import importlib.util
+    import tempfile
+    from decimal import Decimal, getcontext
+    csrc = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "qcdgpu_b200", "csrc")
+    spec = importlib.util.spec_from_file_location("gen_logtab", os.path.join(csrc, "gen_logtab.py"))
+    gen = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(gen)
+    with tempfile.TemporaryDirectory() as d:
+        p = os.path.join(d, "qg_logtab.h")
+        gen.emit(p)
+        assert open(p).read() == open(os.path.join(csrc, "qg_logtab.h")).read()
+    ln2_hi, ln2_lo, c, lhi, llo = gen.table()
+    getcontext().prec = 40
+    for k in range(129):
+        assert c[k] == 1.0 / (1.0 + k / 128.0)
+        assert (lhi[k] * 2.0 ** 32).is_integer()
+        err = Decimal(lhi[k]) + Decimal(llo[k]) + Decimal(c[k]).ln()
+        assert abs(err) <= Decimal(2) ** -60, (k, err)
+    assert (ln2_hi * 2.0 ** 32).is_integer()
+    assert abs(Decimal(ln2_hi) + Decimal(ln2_lo) - Decimal(2).ln()) <= Decimal(2) ** -60
