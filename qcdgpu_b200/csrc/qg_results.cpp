@@ -68,9 +68,8 @@ extern "C" int qg_write_results(const qg_config *cfgp, const qg_run_options *op,
     // the file name of lattice_write_results: prefix + "YY-Mon-DD-hh-mm-ss.txt"
     // from ctime of the finish time
     const time_t ts = (time_t)t_start, te = (time_t)t_end;
-    char cs[64], ce[64];
-    snprintf(cs, sizeof(cs), "%s", ctime(&ts));
-    snprintf(ce, sizeof(ce), "%s", ctime(&te));
+    char cs[64] = "", ce[64] = "";
+    if (!ctime_r(&ts, cs) || !ctime_r(&te, ce)) return fail(QG_ERR_ARG, "qg_write_results: bad start or end time");
     char stamp[96];
     snprintf(stamp, sizeof(stamp), "%.2s-%.3s-%.2s-%.2s-%.2s-%.2s", ce + 22, ce + 4, ce + 8, ce + 11, ce + 14, ce + 17);
     const std::string name = std::string(o.output_path) + o.prefix + stamp;
@@ -135,7 +134,9 @@ extern "C" int qg_write_results(const qg_config *cfgp, const qg_run_options *op,
     const int el = (int)difftime(te, ts);
     fprintf(fp, " Start time               : %s", cs);
     fprintf(fp, " Finish time              : %s", ce);
-    fprintf(fp, " Elapsed time             : %i:%2.2i:%2.2i:%2.2i\n", el / 86400, (el / 3600) % 3600, (el / 60) % 60,
+    // days:hours:minutes:seconds (hours modulo 24; the reference's formula,
+    // suncl.cpp:805, keeps counting hours past the first day)
+    fprintf(fp, " Elapsed time             : %i:%2.2i:%2.2i:%2.2i\n", el / 86400, (el / 3600) % 24, (el / 60) % 60,
             el % 60);
     fprintf(fp, "%s", kStars);
     for (int k = 0; k <= QG_OBS_WILSON; k++) {

@@ -109,3 +109,15 @@ def test_results_file_name_is_the_reference_stamp(tmp_path):
     c = time.ctime(t)
     assert os.path.basename(path) == "su3-%s-%s-%s-%s-%s-%s.txt" % (c[22:24], c[4:7], c[8:10], c[11:13], c[14:16],
                                                                     c[17:19])
+
+
+def test_results_file_elapsed_time_past_a_day(tmp_path):
+    """days:hours:minutes:seconds with the hours taken modulo 24 (the
+    reference's formula keeps counting hours past the first day)"""
+    cfg = Q.default_config(group=2, size=(4, 4, 4, 4))
+    opts = Q.default_run_options(iter=1, pl_level=0, output_path=str(tmp_path) + "/", prefix="su2-")
+    t0 = 1700000000
+    path = Q.write_results(cfg, opts, Q.RunResult(), np.zeros((Q.OBS_COUNT, 1)), t_start=t0,
+                           t_end=t0 + 2 * 86400 + 5 * 3600 + 7 * 60 + 9)
+    line = [l for l in open(path) if l.startswith(" Elapsed time")][0]
+    assert line.rstrip().endswith(": 2:05:07:09"), line
