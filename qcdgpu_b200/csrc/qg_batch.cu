@@ -139,48 +139,57 @@ __device__ bool grid_sync(GridBarrier *bar, bool arrive)
     return __syncthreads_and(ok) != 0;
 }
 
+// the tiles of direction mu: one loop per direction, so that each loop is
+// compiled with its own register allocation (one loop around a switch over
+// the four directions held 160 registers: 3 blocks per SM instead of 5)
+template <int NC, typename Real, bool OR, int mu, bool STAGED>
+__device__ __forceinline__ void tiles_of_phase(const EnsDesc *ens, const uint32_t *pre, int n, int parity,
+                                               const uint64_t *phase_base, uint32_t phase_offset0, int nhit,
+                                               int nhitpar, StageBuf *sb, uint32_t ntiles)
+{
+    for (uint32_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+        const int e = find_ensemble(pre, n, tile);
+        const EnsDesc &d = ens[e];
+        const uint32_t t = (tile - __ldg(pre + e)) * kPhaseBlock + threadIdx.x;
+        const Geom G = d.G;
+        if (t >= G.half) continue;
+        PhaseArgs A;
+        A.parity = parity;
+        A.dir = mu;
+        A.params = d.params;
+        A.twist = 0;
+        A.nhit = nhit;
+        A.nhitpar = nhitpar;
+        A.prn_mode = OR ? -1 : 1;
+        A.prns = nullptr;
+        A.prngstep = 0;
+        A.key = d.key;
+        A.phase_base = phase_base;
+        A.phase_offset = phase_offset0 + (uint32_t)mu;
+        A.variant = 0;
+        A.t_begin = 0;
+        A.t_end = G.half;
+        A.t_prn = 0;
+        Field<Real> U;
+        U.p = reinterpret_cast<typename V4<Real>::T *>(d.links);
+        U.pstride = G.pstride;
+        phase_site<NC, Real, 1, OR, mu, STAGED>(U, G, A, t, sb);
+    }
+}
+
 template <int NC, typename Real, bool OR, bool STAGED>
 __device__ __forceinline__ void half_sweep_body(const EnsDesc *ens, const uint32_t *pre, int n, int parity,
                                                 const uint64_t *phase_base, uint32_t phase_offset0, int nhit,
                                                 int nhitpar, GridBarrier *bar, int skip_block, StageBuf *sb)
 {
     const uint32_t ntiles = __ldg(pre + n);
-    for (int mu = 0; mu < 4; mu++) {
-        if (mu > 0 && !grid_sync(bar, !(mu == 1 && (int)blockIdx.x == skip_block))) return;
-        for (uint32_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
-            const int e = find_ensemble(pre, n, tile);
-            const EnsDesc &d = ens[e];
-            const uint32_t t = (tile - __ldg(pre + e)) * kPhaseBlock + threadIdx.x;
-            const Geom G = d.G;
-            if (t >= G.half) continue;
-            PhaseArgs A;
-            A.parity = parity;
-            A.dir = mu;
-            A.params = d.params;
-            A.twist = 0;
-            A.nhit = nhit;
-            A.nhitpar = nhitpar;
-            A.prn_mode = OR ? -1 : 1;
-            A.prns = nullptr;
-            A.prngstep = 0;
-            A.key = d.key;
-            A.phase_base = phase_base;
-            A.phase_offset = phase_offset0 + (uint32_t)mu;
-            A.variant = 0;
-            A.t_begin = 0;
-            A.t_end = G.half;
-            A.t_prn = 0;
-            Field<Real> U;
-            U.p = reinterpret_cast<typename V4<Real>::T *>(d.links);
-            U.pstride = G.pstride;
-            switch (mu) {
-            case 0: phase_site<NC, Real, 1, OR, 0, STAGED>(U, G, A, t, sb); break;
-            case 1: phase_site<NC, Real, 1, OR, 1, STAGED>(U, G, A, t, sb); break;
-            case 2: phase_site<NC, Real, 1, OR, 2, STAGED>(U, G, A, t, sb); break;
-            default: phase_site<NC, Real, 1, OR, 3, STAGED>(U, G, A, t, sb); break;
-            }
-        }
-    }
+    tiles_of_phase<NC, Real, OR, 0, STAGED>(ens, pre, n, parity, phase_base, phase_offset0, nhit, nhitpar, sb, ntiles);
+    if (!grid_sync(bar, (int)blockIdx.x != skip_block)) return;
+    tiles_of_phase<NC, Real, OR, 1, STAGED>(ens, pre, n, parity, phase_base, phase_offset0, nhit, nhitpar, sb, ntiles);
+    if (!grid_sync(bar, true)) return;
+    tiles_of_phase<NC, Real, OR, 2, STAGED>(ens, pre, n, parity, phase_base, phase_offset0, nhit, nhitpar, sb, ntiles);
+    if (!grid_sync(bar, true)) return;
+    tiles_of_phase<NC, Real, OR, 3, STAGED>(ens, pre, n, parity, phase_base, phase_offset0, nhit, nhitpar, sb, ntiles);
 }
 
 template <int NC, typename Real, bool OR, int MINB, bool STAGED>
