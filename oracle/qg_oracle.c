@@ -385,6 +385,13 @@ static double ol_exp(double x)
 }
 double ol_expd(double x) { return ol_exp(x); }
 
+/* test-only: when set, the Kennedy-Pendleton step evaluates the reference's
+ * expression for delta unfused, with the C library's cos / sin / log in
+ * place of this build's routines (a measure of how far this build's own
+ * arithmetic moves the chain; not what the device does) */
+int ol_ref_arith = 0;
+void ol_set_reference_arith(int on) { ol_ref_arith = on != 0; }
+
 /* exported for the accuracy tests of the two routines */
 double ol_sin(double x) { double s, c; ol_sincos(x, &s, &c); return s; }
 double ol_cos(double x) { double s, c; ol_sincos(x, &s, &c); return c; }

@@ -69,6 +69,11 @@ int   ol_sizeof_ranlux(void);
 void  ol_philox4x32(const uint32_t ctr[4], const uint32_t key[2], uint32_t out[4]);
 void  ol_philox_prn(const ol_prn *src, uint32_t thread, uint32_t k, float out[4]);
 
+/* ---- test-only: the heatbath's delta as the reference writes it (unfused,
+ *      the C library's cos / sin / log); 0 restores this build's arithmetic */
+void  ol_set_reference_arith(int on);
+extern int ol_ref_arith;
+
 /* ---- the float sin / cos of the FP32 update path */
 float ol_sinf_own(float x);
 float ol_cosf_own(float x);

@@ -429,9 +429,22 @@ static int FN(kp_step)(S2 *a, REAL beta, FN(prnctx) *p, int su3_path)
         } else {
             FN(prn_next)(p, rnd);
         }
-        cosrnd = RCOS(RPI2 * rnd[1]);
-        double lx = ol_log(1.0 - (double)rnd[0]), lz = ol_log(1.0 - (double)rnd[2]);
-        delta = (REAL)(-fma((double)(cosrnd * cosrnd), lz, lx) / (double)bdet);
+        if (ol_ref_arith) {
+            /* the reference's expression as written (su3_update_cl.cl:619-620):
+             * product and sum rounded separately, the C library's cos and log
+             * standing in for the OpenCL runtime's (test-only comparison) */
+#if IS_F
+            cosrnd = cosf(RPI2 * rnd[1]);
+#else
+            cosrnd = cos(RPI2 * rnd[1]);
+#endif
+            double lx = log(1.0 - (double)rnd[0]), lz = log(1.0 - (double)rnd[2]);
+            delta = (REAL)(-(lx + (double)(cosrnd * cosrnd) * lz) / (double)bdet);
+        } else {
+            cosrnd = RCOS(RPI2 * rnd[1]);
+            double lx = ol_log(1.0 - (double)rnd[0]), lz = ol_log(1.0 - (double)rnd[2]);
+            delta = (REAL)(-fma((double)(cosrnd * cosrnd), lz, lx) / (double)bdet);
+        }
         if ((double)(rnd[3] * rnd[3]) <= fma(-0.5, (double)delta, 1.0)) flag = 1;
         if (c->gid_mode) { delta = cosrnd * cosrnd / bdet; flag = 1; }
     }
@@ -454,6 +467,13 @@ static int FN(kp_step)(S2 *a, REAL beta, FN(prnctx) *p, int su3_path)
         REAL sinal = (REAL)sqrt(1.0 - (double)(cosal * cosal));
         REAL phi = RPI2 * rnd[1];
         REAL sinphi = RSIN(phi), cosphi = RCOS(phi);
+        if (ol_ref_arith) {
+#if IS_F
+            sinphi = sinf(phi); cosphi = cosf(phi);
+#else
+            sinphi = sin(phi); cosphi = cos(phi);
+#endif
+        }
         cc.x = cosal;
         cc.z = sinal * costh;
         cc.y = sinal * sinth * sinphi;
