@@ -29,6 +29,23 @@ def test_reference_arm_line():
     assert d["steps"] == 2 and d["steps_requested"] == 2
 
 
+
+def test_reference_arm_reports_a_failing_reference_process(tmp_path, monkeypatch, capsys):
+    """a reference CPU process that exits with an error gives the arm's
+    "unavailable" line and status 0, not a traceback"""
+    sys.path.insert(0, ROOT)
+    import bench
+    fake = tmp_path / "ref_cpurun"
+    fake.write_text("#!/bin/sh\nexit 3\n")
+    fake.chmod(0o755)
+    monkeypatch.setattr(bench, "ref_binary", lambda: str(fake))
+    monkeypatch.setattr(sys, "argv", ["bench.py", "--impl", "reference", "--size", "4", "--steps", "2",
+                                      "--warmup", "1"])
+    args = bench.parse()
+    assert bench.run_reference_arm(args) == 0
+    d = json.loads(capsys.readouterr().out.strip().splitlines()[-1])
+    assert d["impl"] == "reference" and "reference CPU path failed" in d["unavailable"]
+
 def test_reference_arm_caps_its_timed_steps():
     """one reference step is a whole heatbath phase per process (about a
     second at 32^4), so a long --steps request is cut to the cap"""
