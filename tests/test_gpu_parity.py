@@ -630,3 +630,30 @@ def test_each_phase_writes_exactly_its_links(group, precision, shape):
                 assert not np.any(ch & ~want), (kind, p, mu)            # nothing outside the phase's links
                 assert ch[want].mean() > 0.99, (kind, p, mu)             # and (almost) all of them updated
     L.close()
+
+
+@pytest.mark.parametrize("dims", [(2, 2, 2, 2), (2, 4, 2, 6), (4, 2, 6, 2), (2, 6, 4, 2)])
+@pytest.mark.parametrize("group,shape", [(3, 0), (3, 3), (3, 4), (2, 0)])
+def test_extents_of_two_every_shape_bit_exact(dims, group, shape):
+    """Extents of 2, where a link's +1 and -1 neighbours along that
+    direction are the same site (N2 = 2: one y pair per checkerboard row):
+    two heatbath + overrelaxation sweeps of the register form (shape 0) and
+    the staged forms (3, 4) reproduce the oracle bit for bit (FP32, Philox)"""
+    L, c = make_pair(group, dims, 0, start=Q.START_COLD, prng=Q.PRNG_PHILOX,
+                     beta=5.8 if group == 3 else 2.3, n_or=1, reunit_every=3)
+    L.set_shapes(shape, shape)
+    L.seed(54)
+    L.init(Q.START_COLD)
+    t = cold_table(c)
+    ph = 0
+    for s in range(2):
+        L.sweep(1)
+        for par in (1, 0):
+            for mu in range(4):
+                O.phase_hb(c, t, par, mu, philox=(54, 0x5D3E1A27, ph))
+                ph += 1
+        for par in (1, 0):
+            for mu in range(4):
+                O.lib.ol_phase_or(ctypes.byref(c), O.vp(t), par, mu)
+    g = L.download()
+    assert np.array_equal(g, t), "max|dU| = %g" % maxdiff(g, t)
