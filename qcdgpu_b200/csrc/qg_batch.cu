@@ -307,6 +307,7 @@ int bfail(const std::string &m, int code = QG_ERR_ARG)
 }
 int bcuda(cudaError_t e, const char *what)
 {
+    cudaGetLastError();   // reported here; not left pending for the next launch check
     return bfail(std::string(what) + ": " + cudaGetErrorString(e), QG_ERR_CUDA);
 }
 #define QB_CK(x, what)                                   \

@@ -99,6 +99,10 @@ static int fail(qg_ctx *c, int code, const std::string &msg)
 }
 static int cuda_fail(qg_ctx *c, cudaError_t e, const char *where)
 {
+    // the error is reported here: consume it, so that a non-sticky one (a
+    // failed allocation) is not picked up by the next launch check as if
+    // that kernel had failed
+    cudaGetLastError();
     return fail(c, QG_ERR_CUDA, std::string(where) + ": " + cudaGetErrorString(e));
 }
 #define QG_CK(call, where) do { cudaError_t e_ = (call); if (e_ != cudaSuccess) return cuda_fail(c, e_, where); } while (0)

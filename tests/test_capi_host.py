@@ -94,3 +94,26 @@ int main(void) { return 0; }
                         "-L", lib, "-lqg_sun", "-Wl,-rpath," + lib, "-o", str(tmp_path / "example")],
                        capture_output=True, text=True)
     assert r.returncode == 0, r.stderr
+
+
+@pytest.mark.parametrize("kw,why", [
+    (dict(size=(4, 5, 4, 4)), "even"),                           # N2 odd: no checkerboard
+    (dict(size=(1, 4, 4, 4)), "[2, 4096]"),                      # extent below 2
+    (dict(size=(8192, 4, 4, 4)), "[2, 4096]"),                   # extent above 4096
+    (dict(size=(2048, 2048, 2048, 2)), "2^31"),                  # volume above 2^31 sites
+    (dict(group=4), "GROUP"),
+    (dict(precision=2), "precision"),
+    (dict(nhit=0), "NHIT"),
+    (dict(randseries=0), "RANDSERIES 0"),
+])
+def test_create_rejects_invalid_configurations(kw, why):
+    """qg_create refuses configurations the kernels cannot run, before any
+    device work (no GPU needed), with the reason in qg_last_error(NULL)"""
+    base = dict(group=3, size=(4, 4, 4, 4), precision=0)
+    base.update(kw)
+    lib = Q.load_library()
+    cfg = Q.default_config(**base)
+    ctx = ctypes.c_void_p()
+    rc = lib.qg_create(ctypes.byref(cfg), ctypes.byref(ctx))
+    assert rc == Q.QG_ERR_ARG and not ctx.value
+    assert why in lib.qg_last_error(None).decode()

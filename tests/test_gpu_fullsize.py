@@ -81,3 +81,22 @@ def test_24x6_fp32_follows_fp64_for_one_sweep():
     d = np.max(np.abs(res[0][0] - res[1][0]))
     assert d < 1e-4, d
     assert abs(res[0][1] - res[1][1]) < 1e-5
+
+
+def test_lattice_beyond_device_memory_fails_cleanly():
+    """A valid lattice whose links exceed the device memory (160^3 x 256
+    SU(3) FP32: 1.05e9 sites, 201 GB of links against 180 GB of HBM) is
+    refused by qg_create with a CUDA allocation error, not a crash, and
+    the process goes on creating and sweeping lattices"""
+    with pytest.raises(Q.QGError) as e:
+        Q.Lattice(Q.default_config(group=3, size=(160, 160, 160, 256), precision=0, start=Q.START_COLD,
+                                   prng=Q.PRNG_PHILOX))
+    assert "memory" in str(e.value).lower() or "alloc" in str(e.value).lower(), str(e.value)
+    L = Q.Lattice(Q.default_config(group=3, size=(8, 8, 8, 8), precision=0, start=Q.START_COLD,
+                                   prng=Q.PRNG_PHILOX, n_or=1))
+    L.seed(54)
+    L.init()
+    L.sweep(2)
+    sp, tp = L.plaquette_sums()
+    assert 0 < sp < 3 * 8 ** 4 * 3 and 0 < tp < 3 * 8 ** 4 * 3
+    L.close()
