@@ -360,7 +360,8 @@ def run_ours(args):
 
     # end to end through the C-ABI: per step the run parameters go host ->
     # device from pinned staging (qg_set_params), one sweep, and the step's
-    # plaquette sums come back to pinned host memory (qg_measure_enqueue);
+    # plaquette sums -- FP32 products, FP64 sums (QG_MEAS_PLAQUETTE_F32) --
+    # come back to pinned host memory (qg_measure_enqueue);
     # the host reads every step's values (qg_measure_fetch) -- one step
     # behind, so the device does not idle between steps -- and the timed
     # region ends when the last step's values are on the host
@@ -373,7 +374,7 @@ def run_ours(args):
     for _ in range(e2e_steps):
         L.set_params(BETA)
         L.sweep(1)
-        tk = L.measure_enqueue(Q.MEAS_PLAQUETTE)
+        tk = L.measure_enqueue(Q.MEAS_PLAQUETTE_F32)
         if pending is not None:
             e2e_plaq.append(L.measure_fetch(pending))
         pending = tk
@@ -384,6 +385,26 @@ def run_ours(args):
     e2e = RP.whole_job_rate(world, updates_per_step * e2e_steps, e2e_s)
 
     plq = L.plaquette()
+    # the e2e readback's plaquette against the FP64-product one, same field,
+    # and the device time of each (20 queued measurements between two
+    # events, kernels and result copy; median of 3)
+    p64, p32 = L.plaquette_sums(), L.plaquette_sums_f32()
+    plq_dev = max(abs(a - b) for a, b in zip(p32, p64)) / (3 * 3 * V)
+
+    def time_measure(kind, reps=20):
+        runs = []
+        for _ in range(3):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            tks = [L.measure_enqueue(kind) for _ in range(reps)]
+            e1.record(stream)
+            torch.cuda.synchronize()
+            for t in tks:
+                L.measure_fetch(t)
+            runs.append(e0.elapsed_time(e1) / reps)
+        return statistics.median(runs)
+
+    plq_ms = {"fp32_products": time_measure(Q.MEAS_PLAQUETTE_F32), "fp64_products": time_measure(Q.MEAS_PLAQUETTE)}
     L_shapes = L.shapes()
     first = 2 + args.warmup
     reunits = sum(1 for n in range(first + 1, first + args.steps + 1) if n % REUNIT_EVERY == 0)
@@ -417,7 +438,10 @@ def run_ours(args):
                      "naive_gbs": 20 * LINK_BYTES * (V / 2) / (dom_ms * 1e-3) / 1e9},
         "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": 32, "d2h_bytes_per_step": 16,
                 "what": "qg_set_params + qg_sweep + the step's plaquette sums read back (qg_measure_enqueue / "
-                        "_fetch, one step behind), host wall clock"},
+                        "_fetch, one step behind), host wall clock",
+                "plaquette": "FP32 products, FP64 sums (QG_MEAS_PLAQUETTE_F32)",
+                "plaquette_dev_vs_fp64_products": plq_dev,
+                "plaquette_ms": plq_ms},
         "gpu_launches": launches,
         "tuning_ms_per_launch": tune,
         "shapes": list(L_shapes),

@@ -59,6 +59,10 @@ extern "C" {
 #define QG_MEAS_ACTION    1   /* out[0..1] = sum (beta/N)(3N - ReTr) spatial / temporal */
 #define QG_MEAS_POLYAKOV  2   /* out[0..3] = sum Re P, Im P, |P|^2, |P|^4 (traces)      */
 #define QG_MEAS_WILSON    3   /* out[0]    = sum ReTr W(R,T) over sites and x,y,z       */
+/* out[0..1] as QG_MEAS_PLAQUETTE, with the products of each plaquette and its
+ * trace in FP32 on an FP32-link lattice (the site and lattice sums in FP64);
+ * on an FP64-link lattice the same values as QG_MEAS_PLAQUETTE */
+#define QG_MEAS_PLAQUETTE_F32 4
 
 typedef struct qg_ctx qg_ctx;
 

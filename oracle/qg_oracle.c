@@ -470,6 +470,10 @@ void ol_plaquette(const ol_cfg *c, const void *t, double out[2])
 {
     DISPATCH(plaquette_f(c, (const float *)t, out, NULL), plaquette_d(c, (const double *)t, out, NULL));
 }
+void ol_plaquette_f32(const ol_cfg *c, const void *t, double out[2])
+{
+    DISPATCH(plaquette_lp_f(c, (const float *)t, out), plaquette_d(c, (const double *)t, out, NULL));
+}
 void ol_action(const ol_cfg *c, const void *t, double out[2])
 {
     double p[2];

@@ -87,6 +87,8 @@ void ol_phase_or(const ol_cfg *c, void *table, int parity, int dir);
 void ol_gramschmidt(const ol_cfg *c, void *table);        /* Real precision  */
 void ol_gramschmidt_fp64(const ol_cfg *c, void *table);   /* FP64 arithmetic */
 void ol_plaquette(const ol_cfg *c, const void *table, double out[2]);
+/* the plaquette sums with FP32 products and traces (FP32 links; FP64 links: ol_plaquette) */
+void ol_plaquette_f32(const ol_cfg *c, const void *table, double out[2]);
 void ol_action(const ol_cfg *c, const void *table, double out[2]);
 void ol_polyakov(const ol_cfg *c, const void *table, double out[4]);
 /* F_munu projections of the plaquettes (field 0: xy, xz, yz; 1: xt, yt, zt)

@@ -909,6 +909,58 @@ static void FN(plaquette)(const ol_cfg *c, const REAL *tab, double out[2], doubl
     if (act_out) { act_out[0] = as; act_out[1] = at; }
 }
 
+/* The plaquette with the products of each plaquette and its trace in the
+ * link precision (the FP32-product plaquette of FP32-link lattices; the
+ * reference promotes to FP64, su3_measurements_cl.cl:292-319, which
+ * FN(plaquette) follows): Re Tr(a b c^+ d^+) as a b (full product), then
+ * (a b) c^+, then the trace against d, with the same dot products. */
+static REAL FN(retr4_lp)(const M3 *a, const M3 *b, const M3 *c, const M3 *d)
+{
+    M3 ab = FN(mul3)(a, b), abc;
+    for (int i = 0; i < 3; i++)
+        for (int j = 0; j < 3; j++) abc.m[i][j] = FN(dotc3)(&ab.m[i][0], 1, &c->m[j][0], 1);
+    REAL tr = 0;
+    for (int i = 0; i < 3; i++) tr += FN(dotc3)(&abc.m[i][0], 1, &d->m[i][0], 1).re;
+    return tr;
+}
+/* a stored link as a full 3x3 in the link precision; SU(2) in the upper
+ * 2x2 block with a zero third row and column */
+static M3 FN(load_lp)(const ol_cfg *c, const REAL *tab, const crd *co, int mu)
+{
+    unsigned g = c2gid(c, *co);
+    if (c->group == 3) return FN(expand)(FN(load3)(c, tab, co, g, mu));
+    R4 a = FN(load2)(c, tab, co, g, mu).uv1;
+    M3 m;
+    memset(&m, 0, sizeof(m));
+    m.m[0][0].re = a.x;  m.m[0][0].im = a.z;
+    m.m[0][1].re = a.y;  m.m[0][1].im = a.w;
+    m.m[1][0].re = -a.y; m.m[1][0].im = a.w;
+    m.m[1][1].re = a.x;  m.m[1][1].im = -a.z;
+    return m;
+}
+/* spatial / temporal sums; per site the six traces in the order xy, xz,
+ * xt, yz, yt, zt, each converted to FP64 and summed in FP64 */
+static void FN(plaquette_lp)(const ol_cfg *c, const REAL *tab, double out[2])
+{
+    int V = sites_of(c);
+    double sp = 0, tp = 0;
+    for (int g = 0; g < V; g++) {
+        crd co; gid2c(c, g, &co);
+        crd cx = nb_plus(c, co, 0), cy = nb_plus(c, co, 1), cz = nb_plus(c, co, 2), ct = nb_plus(c, co, 3);
+        M3 m1 = FN(load_lp)(c, tab, &co, 0), m4 = FN(load_lp)(c, tab, &co, 1);
+        M3 m5 = FN(load_lp)(c, tab, &co, 2), m6 = FN(load_lp)(c, tab, &co, 3), b, d;
+        double rs, rt;
+        b = FN(load_lp)(c, tab, &cx, 1); d = FN(load_lp)(c, tab, &cy, 0); rs  = (double)FN(retr4_lp)(&m1, &b, &d, &m4);
+        b = FN(load_lp)(c, tab, &cx, 2); d = FN(load_lp)(c, tab, &cz, 0); rs += (double)FN(retr4_lp)(&m1, &b, &d, &m5);
+        b = FN(load_lp)(c, tab, &cx, 3); d = FN(load_lp)(c, tab, &ct, 0); rt  = (double)FN(retr4_lp)(&m1, &b, &d, &m6);
+        b = FN(load_lp)(c, tab, &cy, 2); d = FN(load_lp)(c, tab, &cz, 1); rs += (double)FN(retr4_lp)(&m4, &b, &d, &m5);
+        b = FN(load_lp)(c, tab, &cy, 3); d = FN(load_lp)(c, tab, &ct, 1); rt += (double)FN(retr4_lp)(&m4, &b, &d, &m6);
+        b = FN(load_lp)(c, tab, &cz, 3); d = FN(load_lp)(c, tab, &ct, 2); rt += (double)FN(retr4_lp)(&m5, &b, &d, &m6);
+        sp += rs; tp += rt;
+    }
+    out[0] = sp; out[1] = tp;
+}
+
 /* lattice_action_diff_{x,y,z} (sun_measurements_cl.cl:187-615): the
  * spatial and temporal action (beta/N)(3N - ReTr) summed over the sites of
  * each slice of coordinate `axis`; out[2 i], out[2 i + 1] for slice i */

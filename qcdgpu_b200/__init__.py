@@ -23,6 +23,7 @@ PRNG_RANLUX, PRNG_PHILOX = 0, 1
 LAYOUT_REFERENCE = 0
 HEATBATH, OVERRELAX = 0, 1
 MEAS_PLAQUETTE, MEAS_ACTION, MEAS_POLYAKOV, MEAS_WILSON = 0, 1, 2, 3
+MEAS_PLAQUETTE_F32 = 4             # QG_MEAS_PLAQUETTE_F32
 FMUNU_H, FMUNU_E = 0, 1
 FMUNU_COLS = 16                     # QG_FMUNU_COLS
 MEASURE_SLOTS = 64                  # QG_MEASURE_SLOTS
@@ -676,6 +677,11 @@ class Lattice:
 
     def plaquette_sums(self):
         return self._measure(MEAS_PLAQUETTE, 2)
+
+    def plaquette_sums_f32(self):
+        """plaquette_sums with each plaquette's products and trace in FP32
+        (FP32 links; on FP64 links the same values as plaquette_sums)"""
+        return self._measure(MEAS_PLAQUETTE_F32, 2)
 
     def action_sums(self):
         return self._measure(MEAS_ACTION, 2)

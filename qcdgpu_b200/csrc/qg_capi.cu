@@ -1367,6 +1367,10 @@ extern "C" int qg_measure(qg_ctx *c, int what, double *out)
         else { out[0] = r[2]; out[1] = r[3]; }
         return QG_OK;
     }
+    case QG_MEAS_PLAQUETTE_F32:
+        QG_CK(launch_plaquette_f32(c->G, c->links, f.group, f.precision, c->d_params, tw, c->partials, c->d_results,
+                                   c->stream), "plaquette (FP32 products)");
+        return measure_to_host(c, 2, out);
     case QG_MEAS_POLYAKOV:
         QG_CK(launch_polyakov(c->G, c->links, f.group, f.precision, c->partials, c->d_results, c->stream), "polyakov");
         return measure_to_host(c, 4, out);
@@ -1389,6 +1393,12 @@ static int measure_launch(qg_ctx *c, int what, int &ncomp, int &first)
                                c->stream), "plaquette");
         ncomp = 2;
         first = what == QG_MEAS_PLAQUETTE ? 0 : 2;
+        return QG_OK;
+    case QG_MEAS_PLAQUETTE_F32:
+        QG_CK(launch_plaquette_f32(c->G, c->links, f.group, f.precision, c->d_params, tw, c->partials, c->d_results,
+                                   c->stream), "plaquette (FP32 products)");
+        ncomp = 2;
+        first = 0;
         return QG_OK;
     case QG_MEAS_POLYAKOV:
         QG_CK(launch_polyakov(c->G, c->links, f.group, f.precision, c->partials, c->d_results, c->stream), "polyakov");

@@ -391,6 +391,36 @@ cudaError_t launch_plaquette(const Geom &G, const void *links, int group, int pr
     return launch_reduce(partials, nb, 4, out, s);
 }
 
+// the plaquette with FP32 products (QG_MEAS_PLAQUETTE_F32): same blocks,
+// partials and reduction as k_plaquette; FP64 links take k_plaquette
+template <int NC, bool TW>
+__global__ void __launch_bounds__(256) k_plaquette_f32(Field<float> U, Geom G, const double *params, int twist,
+                                                        double *partials)
+{
+    uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+    double v[4] = { 0, 0, 0, 0 };
+    if (s < G.V) plaq_site_f32<NC>(U, G, params, TW ? twist : 0, lex2crd(G, s), v);
+    block_sum_store<4>(v, partials);
+}
+
+cudaError_t launch_plaquette_f32(const Geom &G, const void *links, int group, int prec, const double *params,
+                                 int twist, double *partials, double *out, cudaStream_t s)
+{
+    if (prec) return launch_plaquette(G, links, group, prec, params, twist, partials, out, s);
+    uint32_t nb = plaq_blocks(G);
+    Field<float> U{ (float4 *)links, G.pstride };
+    if (group == 3) {
+        if (twist) k_plaquette_f32<3, true><<<nb, 256, 0, s>>>(U, G, params, twist, partials);
+        else k_plaquette_f32<3, false><<<nb, 256, 0, s>>>(U, G, params, twist, partials);
+    } else {
+        if (twist) k_plaquette_f32<2, true><<<nb, 256, 0, s>>>(U, G, params, twist, partials);
+        else k_plaquette_f32<2, false><<<nb, 256, 0, s>>>(U, G, params, twist, partials);
+    }
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    return launch_reduce(partials, nb, 4, out, s);
+}
+
 // lattice_polyakov (polyakov.cl:54-140): one thread per spatial site
 template <int NC, typename Real>
 __global__ void __launch_bounds__(256) k_polyakov(Field<Real> U, Geom G, double *partials)

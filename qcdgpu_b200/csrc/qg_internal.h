@@ -48,6 +48,9 @@ cudaError_t launch_to_ref(const Geom &G, const void *links, void *ref, int group
 uint32_t plaq_blocks(const Geom &G);
 cudaError_t launch_plaquette(const Geom &G, const void *links, int group, int prec, const double *params, int twist,
                              double *partials, double *out, cudaStream_t s);
+// the plaquette with FP32 products on FP32 links (as launch_plaquette on FP64 links)
+cudaError_t launch_plaquette_f32(const Geom &G, const void *links, int group, int prec, const double *params,
+                                 int twist, double *partials, double *out, cudaStream_t s);
 uint32_t poly_blocks(const Geom &G);
 cudaError_t launch_polyakov(const Geom &G, const void *links, int group, int prec, double *partials, double *out,
                             cudaStream_t s);

@@ -61,8 +61,9 @@ __device__ __forceinline__ M3<T> mulf(const M3<T> &u, const M3<T> &v)
         for (int j = 0; j < 3; j++) t.m[i][j] = dot3(&u.m[i][0], 1, &v.m[0][j], 3);
     return t;
 }
-// Re Tr(a b c^+ d^+) of FP32 products, the trace summed in FP64
-__device__ __forceinline__ double retr4(const M3<float> &a, const M3<float> &b, const M3<float> &c,
+// Re Tr(a b c^+ d^+) with the products and the trace in FP32: the
+// operations of the FP64 form below, in the link precision
+__device__ __forceinline__ float retr4f(const M3<float> &a, const M3<float> &b, const M3<float> &c,
                                         const M3<float> &d)
 {
     M3<float> ab = mulf(a, b), abc;
@@ -70,12 +71,9 @@ __device__ __forceinline__ double retr4(const M3<float> &a, const M3<float> &b, 
     for (int i = 0; i < 3; i++)
 #pragma unroll
         for (int j = 0; j < 3; j++) abc.m[i][j] = dotc3(&ab.m[i][0], 1, &c.m[j][0], 1);
-    double tr = 0;
+    float tr = 0;
 #pragma unroll
-    for (int i = 0; i < 3; i++)
-#pragma unroll
-        for (int k = 0; k < 3; k++)
-            tr += (double)abc.m[i][k].re * (double)d.m[i][k].re + (double)abc.m[i][k].im * (double)d.m[i][k].im;
+    for (int i = 0; i < 3; i++) tr += dotc3(&abc.m[i][0], 1, &d.m[i][0], 1).re;
     return tr;
 }
 // Re Tr(a b c^+ d^+)  (lattice_retrace_plaquette3, su3_measurements_cl.cl:527-548)
@@ -142,6 +140,29 @@ __device__ __forceinline__ void plaq_site_c(const Field<Real> &U, const Geom &G,
     v[2] = bet * (3.0 * NC - rs);
     v[3] = bet * (3.0 * NC - rt);
 }
+// the same six plaquettes of an FP32-link lattice with FP32 products: each
+// plaquette's trace in FP32, the site and lattice sums in FP64 (the
+// plaquette of QG_MEAS_PLAQUETTE_F32)
+template <int NC>
+__device__ __forceinline__ void plaq_site_f32(const Field<float> &U, const Geom &G, const double *params, int twist,
+                                              const Crd &c, double (&v)[4])
+{
+    const Crd cx = step_plus(G, c, 0), cy = step_plus(G, c, 1), cz = step_plus(G, c, 2), ct = step_plus(G, c, 3);
+    auto ld = [&](const Crd &q, int mu) { return load_as<NC, float, float>(U, G, q, mu, params, twist); };
+    const M3<float> m1 = ld(c, 0), m4 = ld(c, 1), m5 = ld(c, 2), m6 = ld(c, 3);
+    const double bet = (double)param_real<float>(params[0]);
+    double rs, rt;
+    rs  = (double)retr4f(m1, ld(cx, 1), ld(cy, 0), m4);
+    rs += (double)retr4f(m1, ld(cx, 2), ld(cz, 0), m5);
+    rt  = (double)retr4f(m1, ld(cx, 3), ld(ct, 0), m6);
+    rs += (double)retr4f(m4, ld(cy, 2), ld(cz, 1), m5);
+    rt += (double)retr4f(m4, ld(cy, 3), ld(ct, 1), m6);
+    rt += (double)retr4f(m5, ld(cz, 3), ld(ct, 2), m6);
+    v[0] = rs; v[1] = rt;
+    v[2] = bet * (3.0 * NC - rs);
+    v[3] = bet * (3.0 * NC - rt);
+}
+
 template <int NC, typename Real>
 __device__ __forceinline__ void plaq_site(const Field<Real> &U, const Geom &G, const double *params, int twist,
                                           uint32_t s, double (&v)[4])

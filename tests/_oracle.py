@@ -64,6 +64,7 @@ def _load():
     lib.ol_phase_hb.argtypes = [P(Cfg), ctypes.c_void_p, ctypes.c_int, ctypes.c_int, P(Prn)]
     lib.ol_phase_or.argtypes = [P(Cfg), ctypes.c_void_p, ctypes.c_int, ctypes.c_int]
     lib.ol_plaquette.argtypes = [P(Cfg), ctypes.c_void_p, P(ctypes.c_double)]
+    lib.ol_plaquette_f32.argtypes = [P(Cfg), ctypes.c_void_p, P(ctypes.c_double)]
     lib.ol_action.argtypes = [P(Cfg), ctypes.c_void_p, P(ctypes.c_double)]
     lib.ol_polyakov.argtypes = [P(Cfg), ctypes.c_void_p, P(ctypes.c_double)]
     lib.ol_wilson.argtypes = [P(Cfg), ctypes.c_void_p, ctypes.c_int, ctypes.c_int]
@@ -189,6 +190,12 @@ def phase_hb(c, tab, parity, mu, prns=None, philox=None, stream=None):
 def plaquette(c, tab):
     out = (ctypes.c_double * 2)()
     lib.ol_plaquette(ctypes.byref(c), vp(tab), out)
+    return out[0], out[1]
+
+
+def plaquette_f32(c, tab):
+    out = (ctypes.c_double * 2)()
+    lib.ol_plaquette_f32(ctypes.byref(c), vp(tab), out)
     return out[0], out[1]
 
 

@@ -4,8 +4,8 @@ oracle checks the same code paths bit for bit on small lattices):
 * SU(3) 64^4 beta=6.2 FP32, HB + 4 OR (3.2 GB of links): reruns from the
   same seed are bitwise reproducible, the one-pass measurements equal the
   separate ones, all R x T <= 8 x 8 Wilson loops with FP32 products agree
-  with the FP64-product kernel to FP32 accuracy, and W(1,1) equals the
-  temporal plaquette sum (SU(3) rows are checked at 32^4, in
+  with the FP64-product kernel to FP32 accuracy, so does the FP32-product
+  plaquette (within 1e-6), and W(1,1) equals the temporal plaquette sum (SU(3) rows are checked at 32^4, in
   test_gpu_parity.py, where the field fits a host download comfortably).
 * SU(3) 32^4 beta=6.0 FP32 in the reference's RANLUX mode (16384
   instances, 277 MB per batch): the lookahead sweep (next sweep's batches
@@ -46,6 +46,9 @@ def test_64x4_reproducible_and_measurements_consistent():
             # W(1,1) summed over the three spatial directions = the temporal plaquette sum
             assert abs(w64[0, 0] - plq[1]) <= 1e-9 * abs(plq[1])
             assert np.max(np.abs(w32 - w64)) / (3 * 3 * V) < 1e-5
+            # FP32-product plaquette: within 1e-6 of the FP64-product one, normalised
+            p32 = L.plaquette_sums_f32()
+            assert max(abs(a - b) for a, b in zip(p32, plq)) / (3 * 3 * V) < 1e-6, (p32, plq)
         L.close()
     assert sums[0] == sums[1]
     p = (sums[0][0][0] + sums[0][0][1]) / (6 * 64 ** 4)

@@ -340,6 +340,35 @@ def test_plaquette_action_polyakov_wilson(group, precision):
     assert abs(L.wilson_sum(1, 1) - tp) <= 1e-12 * abs(tp)
 
 
+@pytest.mark.parametrize("group,precision,twist", [(3, 0, False), (2, 0, False), (3, 0, True), (2, 0, True),
+                                                   (3, 1, False)])
+def test_plaquette_f32_products_match_oracle_and_fp64(group, precision, twist):
+    """QG_MEAS_PLAQUETTE_F32 (each plaquette's products and trace in FP32,
+    site and lattice sums in FP64): every site's six traces are the
+    oracle's FP32 restatement bit for bit, so the sums agree to the FP64
+    summation-order level; the normalised plaquette is within 1e-6 of the
+    FP64-product plaquette (FP64 links: the same values); the queued form
+    returns the same sums"""
+    phi, omega = (0.3, 0.7) if twist else (0.0, 0.0)
+    L, c = make_pair(group, (4, 6, 6, 8), precision, start=Q.START_HOT, prng=Q.PRNG_PHILOX,
+                     beta=5.8 if group == 3 else 2.3, phi=phi, omega=omega)
+    L.seed(54)
+    L.init()
+    L.sweep(2)
+    tab = L.download()
+    norm = 3 * O.volume(c) * group
+    g32, o32 = L.plaquette_sums_f32(), O.plaquette_f32(c, tab)
+    assert all(abs(a - b) <= 1e-13 * norm for a, b in zip(g32, o32)), (g32, o32)
+    g64 = L.plaquette_sums()
+    if precision:
+        assert g32 == g64
+    else:
+        assert max(abs(a - b) for a, b in zip(g32, g64)) / norm <= 1e-6, (g32, g64)
+    tk = L.measure_enqueue(Q.MEAS_PLAQUETTE_F32)
+    assert L.measure_fetch(tk)[:2] == g32
+    L.close()
+
+
 def test_cold_observables_exact():
     for g in (2, 3):
         L, c = make_pair(g, (4, 4, 4, 6), 0)

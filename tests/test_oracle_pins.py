@@ -119,6 +119,30 @@ def test_cold_start_observables_exact():
         assert re == 4 * 4 * 4 * g and im == 0
 
 
+def test_fp32_product_plaquette_against_fp64_products():
+    """ol_plaquette_f32 (products and traces in FP32, sums in FP64): exact on
+    a cold start; on FP32 links within 1e-6 of the FP64-product plaquette
+    (normalised by 3 V N); on FP64 links the FP64 plaquette itself."""
+    for g in (2, 3):
+        for prec in (0, 1):
+            c = O.make_cfg(group=g, dims=(4, 4, 4, 6), precision=prec, beta=5.7)
+            t = O.new_table(c)
+            O.lib.ol_init_cold(ctypes.byref(c), O.vp(t))
+            V = O.volume(c)
+            assert O.plaquette_f32(c, t) == (3.0 * V * g, 3.0 * V * g)
+            R = O.Ranlux(7, 256)
+            n = O.prn_samples(c, 256, hot=True)
+            R.batch(n)
+            for mu in range(4):
+                O.lib.ol_init_hot_dir(ctypes.byref(c), O.vp(t), mu, O.vp(R.batch(n)))
+            a, b = O.plaquette_f32(c, t), O.plaquette(c, t)
+            if prec:
+                assert a == b
+            else:
+                assert a != b
+                assert max(abs(x - y) for x, y in zip(a, b)) / (3 * V * g) <= 1e-6, (a, b)
+
+
 def test_overrelaxation_preserves_local_action():
     """Microcanonical reflection: Re Tr(U*staple) of each updated link is unchanged."""
     for g in (2, 3):
