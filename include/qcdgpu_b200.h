@@ -414,6 +414,11 @@ int qg_batch_tune(qg_batch *b, int reps, float *times_ms);
  * return; qg_batch_sync / qg_batch_series then return QG_ERR_CUDA (the
  * fields are then not consistent) and clear the flag.  Default: off.       */
 int qg_batch_set_persistent(qg_batch *b, int enable);
+/* (new) the plaquette and action sums of the measurement series with each
+ * plaquette's products and trace in FP32 (FP32 links; the sums of
+ * QG_MEAS_PLAQUETTE_F32), fp32 = 1, or in FP64 as the reference (0, the
+ * default).  The Polyakov sums and FP64-link batches are unchanged.        */
+int qg_batch_set_measure_products(qg_batch *b, int fp32);
 /* test of the bounded barrier: one persistent heatbath half-sweep in which
  * block skip_block leaves out its first arrival; every other block's wait
  * runs out.  Returns QG_ERR_CUDA (the flag) when the timeout path works; it

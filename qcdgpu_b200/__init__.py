@@ -47,6 +47,7 @@ EXPORTED_SYMBOLS = (
     "qg_batch_create", "qg_batch_destroy", "qg_batch_init", "qg_batch_set_shape", "qg_batch_run", "qg_batch_sync",
     "qg_batch_get_stream", "qg_batch_series", "qg_batch_links_download", "qg_batch_info",
     "qg_batch_set_shapes", "qg_batch_get_shapes", "qg_batch_tune", "qg_batch_set_persistent",
+    "qg_batch_set_measure_products",
     "qg_batch_barrier_test",
     "qg_measure_wilson_all", "qg_measure_fmunu", "qg_measure_action_profile", "qg_measure_polyakov_profile",
     "qg_measure_enqueue", "qg_measure_fetch", "qg_measure_plaquette_all", "qg_measure_polyakov_all",
@@ -277,6 +278,7 @@ def load_library(path=LIB_PATH):
     lib.qg_device_info.argtypes = [ctypes.c_char_p, ctypes.c_size_t, ctypes.c_char_p, ctypes.c_size_t]
     lib.qg_batch_tune.argtypes = [vp, ctypes.c_int, P(ctypes.c_float)]
     lib.qg_batch_set_persistent.argtypes = [vp, ctypes.c_int]
+    lib.qg_batch_set_measure_products.argtypes = [vp, ctypes.c_int]
     lib.qg_batch_barrier_test.argtypes = [vp, ctypes.c_int]
     lib.qg_batch_run.argtypes = [vp, ctypes.c_int, ctypes.c_int]
     lib.qg_batch_sync.argtypes = [vp]
@@ -859,6 +861,11 @@ class Batch:
         """one persistent launch per half-sweep (grid barriers between the
         directions) instead of one launch per phase"""
         self._ck(self.lib.qg_batch_set_persistent(self.b, int(enable)), "qg_batch_set_persistent")
+
+    def set_measure_products(self, fp32=True):
+        """plaquette and action series with FP32 products and traces (FP32
+        links) instead of the reference's FP64 products"""
+        self._ck(self.lib.qg_batch_set_measure_products(self.b, int(fp32)), "qg_batch_set_measure_products")
 
     def barrier_test(self, skip_block):
         """run one persistent half-sweep in which block skip_block skips its

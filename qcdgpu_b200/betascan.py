@@ -70,6 +70,8 @@ def run_share(ens, idx, a):
                            nhit=10, row_align=64)
     nmeas = (a.sweeps + a.warmup) // a.measure_every + 1
     B = Q.Batch(cfg, sub, max_measurements=nmeas)
+    if getattr(a, "plaquette_fp32", False):
+        B.set_measure_products(True)                  # FP32 products and traces, FP64 sums
     B.init(Q.START_COLD)
     stream = torch.cuda.ExternalStream(B.stream())
     B.run(a.warmup, a.measure_every)                  # warm-up, untimed
@@ -141,6 +143,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--persistent", action="store_true",
                     help="one persistent launch per half-sweep (grid barriers between directions)")
+    ap.add_argument("--plaquette-fp32", action="store_true",
+                    help="measure the plaquette with FP32 products (FP64 sums) instead of FP64 products")
     a = ap.parse_args()
     import torch
 
@@ -159,7 +163,8 @@ def main():
         "workload": "beta scan, %d SU(3) ensembles, N_s in {16,20,24,32}, N_t in {4,6,8}, beta 5.5..6.2, "
                     "1 HB + %d OR per sweep, FP32 links" % (a.ensembles, a.n_or),
         "gpus": world, "sites": job["sites"], "field_bytes": job["field_bytes"], "sweeps": a.sweeps,
-        "measure_every": a.measure_every, "ms": job["ms"], "ms_per_sweep": job["ms"] / a.sweeps,
+        "measure_every": a.measure_every, "plaquette_products": "fp32" if a.plaquette_fp32 else "fp64",
+        "ms": job["ms"], "ms_per_sweep": job["ms"] / a.sweeps,
         "link_updates_per_s": job["link_updates_per_s"], "ranks": job["ranks"],
         "beta": [b for _, b, _ in ens], "extents": [list(s) for s, _, _ in ens],
         "plaquette": job["plaquette"], "polyakov_abs": job["polyakov_abs"]}))

@@ -222,6 +222,23 @@ __global__ void __launch_bounds__(256) k_plaq_batch(const EnsDesc *ens, const ui
     block_sum_store<4>(v, partials, blockIdx.x);
 }
 
+// k_plaq_batch with FP32 products (FP32 links): the sums of k_plaquette_f32
+template <int NC>
+__global__ void __launch_bounds__(256) k_plaq_batch_f32(const EnsDesc *ens, const uint32_t *pre, int n,
+                                                         double *partials)
+{
+    const int e = find_ensemble(pre, n, blockIdx.x);
+    const EnsDesc &d = ens[e];
+    const Geom G = d.G;
+    const uint32_t s = (blockIdx.x - __ldg(pre + e)) * 256 + threadIdx.x;
+    Field<float> U;
+    U.p = reinterpret_cast<float4 *>(d.links);
+    U.pstride = G.pstride;
+    double v[4] = { 0, 0, 0, 0 };
+    if (s < G.V) plaq_site_f32<NC>(U, G, d.params, 0, lex2crd(G, s), v);
+    block_sum_store<4>(v, partials, blockIdx.x);
+}
+
 template <int NC, typename Real>
 __global__ void __launch_bounds__(256) k_poly_batch(const EnsDesc *ens, const uint32_t *pre, int n, double *partials)
 {
@@ -295,6 +312,7 @@ struct qg_batch {
     cudaGraphExec_t graph[4] = { nullptr, nullptr, nullptr, nullptr };   // [measure * 2 + reunit]
     int shape_hb = 4, shape_or = 4;    // phase-kernel launch shapes (qg_batch_tune)
     bool persistent = false;           // one launch per half-sweep (qg_batch_set_persistent)
+    bool plaq_fp32 = false;            // FP32-product plaquette (qg_batch_set_measure_products)
     GridBarrier *d_bar = nullptr;
 };
 
@@ -455,10 +473,12 @@ cudaError_t measure_batch(qg_batch *b)
         }
     } else {
         if (g == 3) {
-            k_plaq_batch<3, float><<<npl, 256, 0, s>>>(b->d_ens, pre_pl, b->n, b->d_pl);
+            if (b->plaq_fp32) k_plaq_batch_f32<3><<<npl, 256, 0, s>>>(b->d_ens, pre_pl, b->n, b->d_pl);
+            else k_plaq_batch<3, float><<<npl, 256, 0, s>>>(b->d_ens, pre_pl, b->n, b->d_pl);
             k_poly_batch<3, float><<<npo, 256, 0, s>>>(b->d_ens, pre_po, b->n, b->d_po);
         } else {
-            k_plaq_batch<2, float><<<npl, 256, 0, s>>>(b->d_ens, pre_pl, b->n, b->d_pl);
+            if (b->plaq_fp32) k_plaq_batch_f32<2><<<npl, 256, 0, s>>>(b->d_ens, pre_pl, b->n, b->d_pl);
+            else k_plaq_batch<2, float><<<npl, 256, 0, s>>>(b->d_ens, pre_pl, b->n, b->d_pl);
             k_poly_batch<2, float><<<npo, 256, 0, s>>>(b->d_ens, pre_po, b->n, b->d_po);
         }
     }
@@ -765,6 +785,14 @@ extern "C" int qg_batch_set_persistent(qg_batch *b, int enable)
 {
     if (!b) return QG_ERR_ARG;
     b->persistent = enable != 0;
+    destroy_batch_graphs(b);
+    return QG_OK;
+}
+
+extern "C" int qg_batch_set_measure_products(qg_batch *b, int fp32)
+{
+    if (!b) return QG_ERR_ARG;
+    b->plaq_fp32 = fp32 != 0;
     destroy_batch_graphs(b);
     return QG_OK;
 }

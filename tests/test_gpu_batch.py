@@ -48,6 +48,39 @@ def test_batch_equals_single_contexts(group, precision, shape, start):
     B.close()
 
 
+@pytest.mark.parametrize("group", [3, 2])
+def test_batch_fp32_product_measurements_equal_single_contexts(group):
+    """qg_batch_set_measure_products(1): the series' plaquette sums are the
+    single context's QG_MEAS_PLAQUETTE_F32 sums bit for bit, the Polyakov
+    sums are unchanged, the action follows the FP64-product action to FP32
+    accuracy; switching back gives the FP64-product sums again"""
+    sweeps, every = 4, 2
+    B = Q.Batch(common(group, 0), ENSEMBLES, max_measurements=4)
+    B.init(Q.START_HOT)
+    B.set_measure_products(True)
+    B.run(sweeps, measure_every=every)
+    B.set_measure_products(False)
+    B.run(2, measure_every=2)
+    ser = B.series()
+    assert ser.shape == (3, len(ENSEMBLES), 8)
+    for e, (size, beta, series) in enumerate(ENSEMBLES):
+        L = Q.Lattice(common(group, 0, size=size, beta=beta, randseries=series, start=Q.START_HOT))
+        L.seed(series)
+        L.init(Q.START_HOT)
+        norm = 3 * int(np.prod(size)) * group
+        for m, k in enumerate((2, 4, 6)):
+            L.sweep(2)
+            if k < 6:
+                assert np.array_equal(np.array(L.plaquette_sums_f32()), ser[m, e, :2]), (e, k)
+                assert np.max(np.abs(np.array(L.action_sums()) - ser[m, e, 2:4])) <= 1e-6 * beta / group * norm
+            else:
+                assert np.array_equal(np.array(L.plaquette_sums()), ser[m, e, :2]), (e, k)
+                assert np.array_equal(np.array(L.action_sums()), ser[m, e, 2:4]), (e, k)
+            assert np.array_equal(np.array(L.polyakov_sums()), ser[m, e, 4:]), (e, k)
+        L.close()
+    B.close()
+
+
 def test_every_batch_shape_and_the_tuner_give_the_same_chain():
     """the batched launch shapes 0-4 compute the same operation sequence,
     and qg_batch_tune restores the fields it times on: all runs end with the
