@@ -346,8 +346,29 @@ def run_ours(args):
             runs.append(e0.elapsed_time(e1) / reps)
         return statistics.median(runs)
 
-    ms_hb = time_phases(Q.HEATBATH)
-    ms_or = time_phases(Q.OVERRELAX)
+    ms_hb_alone = time_phases(Q.HEATBATH)
+    ms_or_alone = time_phases(Q.OVERRELAX)
+    # each kernel as it runs in the timed sweeps: its share of the sweep
+    # graph (event nodes before and after every phase launch and around the
+    # graph; 20 sweeps of the chain per call, median of 3 calls) times the
+    # timed region's ms per sweep -- the share, not the absolute, carries
+    # over, because the SM clock under load differs between the timed
+    # region and any later measurement and both kernels follow it.  The
+    # RANLUX mode keeps the back-to-back launches.
+    ms_hb, ms_or, graph_times, how = ms_hb_alone, ms_or_alone, None, (
+        "CUDA events on the library stream around 32 back-to-back phase launches per kind (median of 3), right "
+        "after the timed region, same lattice and shapes")
+    if prng == Q.PRNG_PHILOX:
+        inside = [L.sweep_phase_times(20) for _ in range(3)]
+        g_hb, g_or, g_sw = (statistics.median(t[i] for t in inside) for i in range(3))
+        step_ms = ms / args.steps
+        ms_hb, ms_or = g_hb / g_sw * step_ms, g_or / g_sw * step_ms
+        graph_times = {"ms_per_launch_hb": g_hb, "ms_per_launch_or": g_or, "ms_per_sweep": g_sw,
+                       "share_hb": 8 * g_hb / g_sw, "share_or": 8 * N_OR * g_or / g_sw}
+        how = ("share of the sweep graph x the timed region's ms per sweep: qg_sweep_phase_times (CUDA event nodes "
+               "before and after every phase launch and around the graph, 20 sweeps per call, median of 3 calls, "
+               "right after the timed region, same lattice and shapes) gives each kernel's in-graph duration "
+               "over the graph's ms per sweep (graph_times)")
     share_hb, share_or = 8 * ms_hb, 8 * N_OR * ms_or
     dom, dom_ms = ("heatbath", ms_hb) if share_hb >= share_or else ("overrelaxation", ms_or)
     alg_bytes = 4.5 * V * LINK_BYTES                # per phase launch (compulsory traffic)
@@ -429,9 +450,10 @@ def run_ours(args):
                      "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
                      "algorithmic_bytes_per_launch": alg_bytes, "ms_per_launch": dom_ms,
                      "ms_per_launch_hb": ms_hb, "ms_per_launch_or": ms_or,
-                     "ms_per_launch_how": "CUDA events on the library stream around 32 back-to-back phase "
-                                          "launches per kind (median of 3), right after the timed region, same "
-                                          "lattice and shapes",
+                     "ms_per_launch_how": how,
+                     # the same kernels launched one by one, back to back (the launch gaps the graph hides)
+                     "ms_per_launch_hb_standalone": ms_hb_alone, "ms_per_launch_or_standalone": ms_or_alone,
+                     "graph_times": graph_times,
                      # the literature's per-update count with no reuse between sites (19 link reads + 1
                      # write); above the HBM peak because neighbouring sites share their links in L2
                      "naive_bytes_per_update": 20 * LINK_BYTES,

@@ -150,6 +150,15 @@ int qg_phase(qg_ctx *ctx, int parity, int dir, int kind);
  * global reunitarisation when the sweep count hits cfg.reunit_every.
  * Replayed from a captured CUDA graph.                                    */
 int qg_sweep(qg_ctx *ctx, int nsweeps);
+/* (new) nsweeps (1..256) sweeps of the qg_sweep chain -- the same launches,
+ * Philox stream, reunitarisation cadence and counters, so the chain goes on
+ * exactly as after qg_sweep(ctx, nsweeps) -- replayed from one graph with an
+ * event before and after every phase launch and around the whole;
+ * *ms_heatbath and *ms_overrelax are the mean durations of one heatbath and
+ * one overrelaxation phase inside the sweep graph (0 without
+ * overrelaxation), *ms_sweep that of a whole sweep in it.  Synchronous.
+ * The RANLUX mode returns QG_ERR_UNSUPPORTED.                              */
+int qg_sweep_phase_times(qg_ctx *ctx, int nsweeps, double *ms_heatbath, double *ms_overrelax, double *ms_sweep);
 /* Autotuner (new): times each launch shape of the heatbath and the
  * overrelaxation phase kernels on this context's lattice (`reps` launches
  * each; the field is restored and no PRN counter moves) and keeps the

@@ -39,7 +39,7 @@ EXPORTED_SYMBOLS = (
     "qg_prng_seed", "qg_prng_produce", "qg_prns_upload", "qg_prns_download", "qg_init_links",
     "qg_set_prng_lookahead", "qg_set_slab", "qg_slab_halo", "qg_slab_halo_bytes", "qg_slab_halo2",
     "qg_slab_phase", "qg_field_check", "qg_profile_kernels",
-    "qg_phase", "qg_sweep", "qg_reunitarize", "qg_measure", "qg_measure_wilson",
+    "qg_phase", "qg_sweep", "qg_sweep_phase_times", "qg_reunitarize", "qg_measure", "qg_measure_wilson",
     "qg_links_upload", "qg_links_download", "qg_set_phase_counter", "qg_glibc_seeds", "qg_set_params", "qg_get_stream",
     "qg_default_run_options", "qg_parse_init_file", "qg_run", "qg_tune", "qg_plaquette_noalloc",
     "qg_set_shapes", "qg_get_shapes", "qg_get_config", "qg_set_sweeps_done",
@@ -227,6 +227,8 @@ def load_library(path=LIB_PATH):
     lib.qg_init_links.argtypes = [vp, ctypes.c_int]
     lib.qg_phase.argtypes = [vp, ctypes.c_int, ctypes.c_int, ctypes.c_int]
     lib.qg_sweep.argtypes = [vp, ctypes.c_int]
+    lib.qg_sweep_phase_times.argtypes = [vp, ctypes.c_int, P(ctypes.c_double), P(ctypes.c_double),
+                                         P(ctypes.c_double)]
     lib.qg_reunitarize.argtypes = [vp, ctypes.c_int]
     lib.qg_measure.argtypes = [vp, ctypes.c_int, P(ctypes.c_double)]
     lib.qg_measure_wilson.argtypes = [vp, ctypes.c_int, ctypes.c_int, P(ctypes.c_double)]
@@ -586,6 +588,15 @@ class Lattice:
 
     def sweep(self, n=1):
         self._ck(self.lib.qg_sweep(self.ctx, n), "qg_sweep")
+
+    def sweep_phase_times(self, n=20):
+        """qg_sweep_phase_times: n sweeps of the qg_sweep chain, returning the
+        mean (heatbath phase, overrelaxation phase, whole sweep) durations
+        in ms inside the sweep graph"""
+        hb, orx, sw = ctypes.c_double(), ctypes.c_double(), ctypes.c_double()
+        self._ck(self.lib.qg_sweep_phase_times(self.ctx, n, ctypes.byref(hb), ctypes.byref(orx), ctypes.byref(sw)),
+                 "qg_sweep_phase_times")
+        return hb.value, orx.value, sw.value
 
     def reunitarize(self, fp64=False):
         self._ck(self.lib.qg_reunitarize(self.ctx, 1 if fp64 else 0), "qg_reunitarize")

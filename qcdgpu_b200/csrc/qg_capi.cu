@@ -763,12 +763,25 @@ extern "C" int qg_reunitarize(qg_ctx *c, int fp64)
 }
 
 // one sweep's launches: lattice_simulate's working-cycle body
-// (suncl.cpp:5393-5412) plus the overrelaxation sweeps
-static cudaError_t enqueue_sweep(qg_ctx *c, bool reunit)
+// (suncl.cpp:5393-5412) plus the overrelaxation sweeps.  ev (optional):
+// an event recorded before and after every phase launch, ev[2k] and
+// ev[2k + 1] around the sweep's k-th phase (heatbath phases first)
+static cudaError_t enqueue_sweep(qg_ctx *c, bool reunit, cudaEvent_t *ev = nullptr)
 {
     const qg_config &f = c->cfg;
     cudaError_t e;
     uint32_t hb = 0;
+    int k_ph = 0;
+    auto timed_phase = [&](const PhaseArgs &a) {
+        cudaError_t r;
+        if (ev && (r = cudaEventRecordWithFlags(ev[2 * k_ph], c->stream, cudaEventRecordExternal)) != cudaSuccess)
+            return r;
+        if ((r = launch_phase(c, a)) != cudaSuccess) return r;
+        if (ev && (r = cudaEventRecordWithFlags(ev[2 * k_ph + 1], c->stream, cudaEventRecordExternal)) != cudaSuccess)
+            return r;
+        k_ph++;
+        return cudaSuccess;
+    };
     const int par_order[2] = { 1, 0 };   // odd first, then even
     for (int pi = 0; pi < 2; pi++)
         for (int mu = 0; mu < 4; mu++) {
@@ -777,14 +790,14 @@ static cudaError_t enqueue_sweep(qg_ctx *c, bool reunit)
                 e = launch_ranlux_produce(c->rl_table, c->prns, c->instances, (int)c->samples, f.ranlux_nskip, c->stream);
                 if (e != cudaSuccess) return e;
             }
-            if ((e = launch_phase(c, a)) != cudaSuccess) return e;
+            if ((e = timed_phase(a)) != cudaSuccess) return e;
             if (a.prn_mode == QG_PRNG_PHILOX) hb++;
         }
     for (int k = 0; k < f.n_or; k++)
         for (int pi = 0; pi < 2; pi++)
             for (int mu = 0; mu < 4; mu++) {
                 PhaseArgs a = phase_args(c, par_order[pi], mu, QG_UPDATE_OVERRELAX, 0);
-                if ((e = launch_phase(c, a)) != cudaSuccess) return e;
+                if ((e = timed_phase(a)) != cudaSuccess) return e;
             }
     if (hb) {
         if ((e = launch_add_u64(c->d_phase, hb, c->stream)) != cudaSuccess) return e;
@@ -1008,6 +1021,74 @@ extern "C" int qg_sweep(qg_ctx *c, int nsweeps)
             c->rl_var ^= 1;
         }
     }
+    return QG_OK;
+}
+
+// nsweeps sweeps of the qg_sweep chain (Philox stream, same launches and
+// reunitarisation cadence) captured as one graph with an event node before
+// and after every phase launch and around the whole: the mean duration of a
+// heatbath and of an overrelaxation phase as they run inside the sweep
+// graph, and of a whole sweep in that graph
+extern "C" int qg_sweep_phase_times(qg_ctx *c, int nsweeps, double *ms_heatbath, double *ms_overrelax,
+                                    double *ms_sweep)
+{
+    NvtxRange nvtx_range("qg_sweep_phase_times");
+    if (!c || !ms_heatbath || !ms_overrelax || !ms_sweep) return QG_ERR_ARG;
+    if (c->slab) return fail(c, QG_ERR_STATE, "a slab sweeps phase by phase with halo exchanges (qcdgpu_b200.slabs)");
+    if (nsweeps < 1 || nsweeps > 256) return fail(c, QG_ERR_ARG, "phase timing: nsweeps in [1, 256]");
+    const qg_config &f = c->cfg;
+    if (f.prng != QG_PRNG_PHILOX || f.start == QG_START_GID)
+        return fail(c, QG_ERR_UNSUPPORTED, "phase timing inside the sweep graph runs the Philox stream");
+    if (needs_seed(c, QG_UPDATE_HEATBATH)) return fail(c, QG_ERR_STATE, "heatbath needs a seeded PRNG (qg_prng_seed)");
+    const int nph = 8 * (1 + f.n_or);
+    // the phases' events, then the two around the whole graph
+    std::vector<cudaEvent_t> ev((size_t)2 * nph * nsweeps + 2, nullptr);
+    const size_t all0 = (size_t)2 * nph * nsweeps, all1 = all0 + 1;
+    cudaGraph_t g = nullptr;
+    cudaGraphExec_t gx = nullptr;
+    cudaError_t e = cudaSuccess;
+    const char *where = "event create";
+    for (auto &x : ev)
+        if ((e = cudaEventCreate(&x)) != cudaSuccess) break;
+    if (e == cudaSuccess) {
+        where = "timed sweep capture";
+        e = cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal);
+        if (e == cudaSuccess) {
+            e = cudaEventRecordWithFlags(ev[all0], c->stream, cudaEventRecordExternal);
+            for (int n = 0; n < nsweeps && e == cudaSuccess; n++) {
+                const bool reunit = f.reunit_every > 0 && ((c->sweeps_done + n + 1) % (uint64_t)f.reunit_every) == 0;
+                e = enqueue_sweep(c, reunit, ev.data() + (size_t)2 * nph * n);
+            }
+            if (e == cudaSuccess) e = cudaEventRecordWithFlags(ev[all1], c->stream, cudaEventRecordExternal);
+            cudaError_t e2 = cudaStreamEndCapture(c->stream, &g);
+            if (e == cudaSuccess) e = e2;
+        }
+    }
+    if (e == cudaSuccess) { where = "timed sweep instantiate"; e = cudaGraphInstantiate(&gx, g, 0); }
+    if (e == cudaSuccess) { where = "timed sweep launch"; e = cudaGraphLaunch(gx, c->stream); }
+    if (e == cudaSuccess) { where = "timed sweep sync"; e = cudaStreamSynchronize(c->stream); }
+    double sum_hb = 0, sum_or = 0;
+    float all_ms = 0;
+    if (e == cudaSuccess) {
+        c->sweeps_done += (uint64_t)nsweeps;
+        c->phase_counter += 8 * (uint64_t)nsweeps;
+        where = "phase event time";
+        for (int n = 0; n < nsweeps && e == cudaSuccess; n++)
+            for (int k = 0; k < nph && e == cudaSuccess; k++) {
+                float ms = 0;
+                const size_t i = (size_t)2 * nph * n + 2 * k;
+                if ((e = cudaEventElapsedTime(&ms, ev[i], ev[i + 1])) == cudaSuccess) (k < 8 ? sum_hb : sum_or) += ms;
+            }
+        if (e == cudaSuccess) e = cudaEventElapsedTime(&all_ms, ev[all0], ev[all1]);
+    }
+    if (gx) cudaGraphExecDestroy(gx);
+    if (g) cudaGraphDestroy(g);
+    for (auto &x : ev)
+        if (x) cudaEventDestroy(x);
+    if (e != cudaSuccess) return cuda_fail(c, e, where);
+    *ms_heatbath = sum_hb / (8.0 * nsweeps);
+    *ms_overrelax = f.n_or > 0 ? sum_or / (8.0 * f.n_or * nsweeps) : 0.0;
+    *ms_sweep = (double)all_ms / nsweeps;
     return QG_OK;
 }
 

@@ -313,6 +313,42 @@ def test_twisted_boundary_phase():
     assert np.allclose(a, b, rtol=1e-13, atol=0)
 
 
+def test_sweep_phase_times_continue_the_sweep_chain():
+    """qg_sweep_phase_times runs the qg_sweep chain: after it and further
+    sweeps the links and counters equal, bit for bit, those of qg_sweep over
+    the same number of sweeps (a reunitarisation falls inside the timed
+    sweeps); the in-graph phase durations are positive; the RANLUX mode and
+    out-of-range sweep counts are refused"""
+    out = []
+    for timed in (False, True):
+        L = Q.Lattice(Q.default_config(group=3, size=(8, 8, 8, 8), precision=0, start=Q.START_HOT,
+                                       prng=Q.PRNG_PHILOX, beta=6.0, n_or=2, reunit_every=3, reunit_fp64=1,
+                                       randseries=54))
+        L.seed(54)
+        L.init()
+        L.sweep(2)
+        if timed:
+            hb, orx, sw = L.sweep_phase_times(5)
+            assert hb > 0 and orx > 0 and sw > 8 * hb + 16 * orx, (hb, orx, sw)
+            for bad in (0, 257):
+                with pytest.raises(Q.QGError):
+                    L.sweep_phase_times(bad)
+        else:
+            L.sweep(5)
+        L.sweep(2)
+        info = L.info()
+        out.append((L.download(), info.phase_counter, info.sweeps_done))
+        L.close()
+    assert np.array_equal(out[0][0], out[1][0])
+    assert out[0][1:] == out[1][1:]
+    L, c = make_pair(3, (4, 4, 4, 4), 0, start=Q.START_COLD, prng=Q.PRNG_RANLUX)
+    L.seed(54)
+    L.init(Q.START_COLD)
+    with pytest.raises(Q.QGError):
+        L.sweep_phase_times(2)
+    L.close()
+
+
 # --------------------------------------------------------- observables
 def hot_config(group, dims, precision, sweeps=2):
     L, c = make_pair(group, dims, precision, start=Q.START_HOT, prng=Q.PRNG_RANLUX, beta=5.8 if group == 3 else 2.3)
