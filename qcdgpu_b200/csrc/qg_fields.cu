@@ -723,10 +723,11 @@ constexpr int kWilsonMax = 16;
 // column: thread (spatial site, i, R) walks t0 = 0 .. N4-1 and keeps the
 // spatial lines S(t) = L_i^R(x + t t) of the last Tmax + 1 time slices in
 // a private ring in shared memory, so each line is built once per column
-// (not once per (t0, T)); the time lines at x and x + R i grow by one
-// product per T, and each term Re Tr(L_t^T(x) S(t0+T) L_t^T(x+R i)^+
-// S(t0)^+) is taken as Re Tr(Y S(t0+T) L_t^T(x+R i)^+) with Y = S(t0)^+
-// L_t^T(x).  The per-thread sums w[T] live in shared memory.  Dynamic shared
+// (not once per (t0, T)); each term Re Tr(L_t^T(x) S(t0+T) L_t^T(x+R i)^+
+// S(t0)^+) is taken as Re Tr(S(t0+T) Z_T) with Z_T = L_t^T(x+R i)^+ S(t0)^+
+// L_t^T(x), which grows by one time link on each side per T (two products
+// per T, no product for the term itself).  The per-thread sums w[T] live
+// in shared memory.  Dynamic shared
 // memory: (Tmax+1) ring entries and Tmax doubles per thread.  A ring entry
 // holds the 2 x 2 block for SU(2); for SU(3) the full line in FP64, or
 // with FP32 products rows 1, 2 only (row 3 rebuilt on reading; rebuilding
@@ -790,10 +791,11 @@ __global__ void __launch_bounds__(128) k_wilson_cols(Field<Real> U, Geom G, int 
         Crd cy0 = c0;
         for (int k = 0; k < R; k++) cy0 = step_plus(G, cy0, i);     // x + R i
         for (int t = 0; t < Tmax; t++) put(t, line(t % nt));
-        // Re Tr(L_t^T(x) S(t0+T) L_t^T(x+Ri)^+ S(t0)^+) = Re Tr(Y S(t0+T) my^+)
-        // with Y = S(t0)^+ L_t^T(x) grown one link per T like the time line
-        // itself: per T one product for Y, one for my, one for Y S and a
-        // 9-term trace (the bottom line S(t0) enters once per t0)
+        // Re Tr(L_t^T(x) S(t0+T) L_t^T(x+Ri)^+ S(t0)^+) = Re Tr(S(t0+T) Z_T)
+        // with Z_T = L_t^T(x+Ri)^+ S(t0)^+ L_t^T(x), grown by one link on each
+        // side per T: Z_T = b_T^+ Z_(T-1) a_T, Z_0 = S(t0)^+ (a_T, b_T the T-th
+        // time links of the two columns).  Per T two products and a 9-term
+        // trace; the bottom line S(t0) enters once per t0
         auto hmul = [](const M3<P> &a, const M3<P> &b) {        // a^+ b
             M3<P> r;
 #pragma unroll
@@ -802,14 +804,14 @@ __global__ void __launch_bounds__(128) k_wilson_cols(Field<Real> U, Geom G, int 
                 for (int j = 0; j < 3; j++) r.m[i][j] = cdot3(&a.m[0][i], 3, &b.m[0][j], 3);
             return r;
         };
-        auto retr_h = [](const M3<P> &a, const M3<P> &b) {      // Re Tr(a b^+), summed in FP64
+        auto retr_p = [](const M3<P> &a, const M3<P> &b) {      // Re Tr(a b), summed in FP64
             double tr = 0.0;
 #pragma unroll
-            for (int i = 0; i < 3; i++)
+            for (int k = 0; k < 3; k++)
 #pragma unroll
                 for (int j = 0; j < 3; j++) {
-                    tr = fma((double)a.m[i][j].re, (double)b.m[i][j].re, tr);
-                    tr = fma((double)a.m[i][j].im, (double)b.m[i][j].im, tr);
+                    tr = fma((double)a.m[k][j].re, (double)b.m[j][k].re, tr);
+                    tr = fma(-(double)a.m[k][j].im, (double)b.m[j][k].im, tr);
                 }
             return tr;
         };
@@ -819,17 +821,17 @@ __global__ void __launch_bounds__(128) k_wilson_cols(Field<Real> U, Geom G, int 
             Crd cx = c0, cy = cy0;
             cx.t = t0;
             cy.t = t0;
-            M3<P> y = hmul(get(t0 % slots), load_as<NC, Real, P>(U, G, cx, 3, params, twist));
-            M3<P> my = load_as<NC, Real, P>(U, G, cy, 3, params, twist);
+            M3<P> z = hmul(load_as<NC, Real, P>(U, G, cy, 3, params, twist),
+                           hmul(get(t0 % slots), load_as<NC, Real, P>(U, G, cx, 3, params, twist)));
 #pragma unroll 1
             for (int T = 1; T <= Tmax; T++) {
                 if (T > 1) {
                     cx = step_plus(G, cx, 3);
-                    y = mulf(y, load_as<NC, Real, P>(U, G, cx, 3, params, twist));
                     cy = step_plus(G, cy, 3);
-                    my = mulf(my, load_as<NC, Real, P>(U, G, cy, 3, params, twist));
+                    z = mulf(hmul(load_as<NC, Real, P>(U, G, cy, 3, params, twist), z),
+                             load_as<NC, Real, P>(U, G, cx, 3, params, twist));
                 }
-                wsum[(T - 1) * nb + tid] += retr_h(mulf(y, get((t0 + T) % slots)), my);
+                wsum[(T - 1) * nb + tid] += retr_p(get((t0 + T) % slots), z);
             }
         }
     }
