@@ -69,8 +69,18 @@ def test_our_arm_line():
     r = d["roofline"]
     assert r["bound"] == "hbm" and r["unit"] == "GB/s" and r["achieved"] > 0 and r["peak"] > 0
     assert r["frac"] == pytest.approx(r["achieved"] / r["peak"])
+    # kernel times as they run in the timed sweeps: share of the sweep graph x timed ms per step
+    g = r["graph_times"]
+    for kind in ("hb", "or"):
+        assert r["ms_per_launch_" + kind] == pytest.approx(g["ms_per_launch_" + kind] / g["ms_per_sweep"]
+                                                           * d["ms_per_step"])
+        assert r["ms_per_launch_%s_standalone" % kind] > 0
+    assert g["share_hb"] == pytest.approx(8 * g["ms_per_launch_hb"] / g["ms_per_sweep"])
+    assert 0 < g["share_hb"] + g["share_or"] < 1
     e = d["e2e"]
     assert e["value"] > 0 and e["h2d_bytes_per_step"] > 0 and e["d2h_bytes_per_step"] > 0
+    assert 0 <= e["plaquette_dev_vs_fp64_products"] <= 1e-6
+    assert set(e["plaquette_ms"]) == {"fp32_products", "fp64_products"}
     assert d["gpu_launches"] == 5 * (8 + 8 * 4 + 1) + sum(1 for n in range(6, 11) if n % 10 == 0)
     assert {"sm_mhz", "sm_max_mhz", "reasons"} <= set(d["clocks"])
     assert "workload" in d["config"] and "fits the 126 MB L2" in d["config"]["l2"]

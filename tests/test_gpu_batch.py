@@ -81,6 +81,19 @@ def test_batch_fp32_product_measurements_equal_single_contexts(group):
     B.close()
 
 
+def test_batch_fp32_product_flag_leaves_fp64_batches_unchanged():
+    """FP64-link batches measure with FP64 products whatever the flag"""
+    outs = []
+    for flag in (False, True):
+        B = Q.Batch(common(3, 1), ENSEMBLES[:2], max_measurements=2)
+        B.init(Q.START_HOT)
+        B.set_measure_products(flag)
+        B.run(2, measure_every=1)
+        outs.append(B.series())
+        B.close()
+    assert np.array_equal(outs[0], outs[1])
+
+
 def test_every_batch_shape_and_the_tuner_give_the_same_chain():
     """the batched launch shapes 0-4 compute the same operation sequence,
     and qg_batch_tune restores the fields it times on: all runs end with the
