@@ -81,9 +81,9 @@ k_phase_batch(const EnsDesc *ens, const uint32_t *pre, int n, int parity, const 
 
 // ---------------------------------------------- persistent half-sweep
 // One launch per parity runs the four directions of that parity over all
-// ensembles: every block walks the 128-link tiles of the batch (tile k of
-// the phase's prefix table for k = blockIdx.x, blockIdx.x + gridDim.x, ...)
-// for direction 0, waits at a grid barrier, and so on -- the phases of one
+// ensembles: the blocks take the 128-link tiles of the batch (tile k of the
+// phase's prefix table) from a counter of direction 0 until none is left,
+// wait at a grid barrier, go on with direction 1, and so on -- the phases of one
 // parity depend on each other (phase (p, nu) reads the links of parity p
 // and direction mu that phase (p, mu) wrote), so the barrier stands where
 // the per-phase launches had a kernel boundary.  All blocks are resident
@@ -145,9 +145,26 @@ __device__ bool grid_sync(GridBarrier *bar, bool arrive)
 template <int NC, typename Real, bool OR, int mu, bool STAGED>
 __device__ __forceinline__ void tiles_of_phase(const EnsDesc *ens, const uint32_t *pre, int n, int parity,
                                                const uint64_t *phase_base, uint32_t phase_offset0, int nhit,
-                                               int nhitpar, StageBuf *sb, uint32_t ntiles)
+                                               int nhitpar, StageBuf *sb, uint32_t ntiles, unsigned *tile_ctr)
 {
-    for (uint32_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+    // tiles handed out by a counter (zeroed before the launch), so that a
+    // block that finishes early takes the next tile as a new block of a
+    // per-phase launch would; thread 0 takes the block's next tile when it
+    // starts a tile and publishes it after, so the atomic's round trip runs
+    // under the tile's work
+    __shared__ uint32_t s_tile;
+    if (threadIdx.x == 0) s_tile = atomicAdd(tile_ctr, 1u);
+    __syncthreads();
+    uint32_t tile = s_tile;
+    uint32_t next = 0;
+    auto advance = [&]() {                            // publish the next tile (every path of the body)
+        if (threadIdx.x == 0) s_tile = next;
+        __syncthreads();
+        return s_tile;
+    };
+    for (; tile < ntiles; tile = advance()) {
+        __syncthreads();                              // every thread has read s_tile
+        if (threadIdx.x == 0) next = atomicAdd(tile_ctr, 1u);
         const int e = find_ensemble(pre, n, tile);
         const EnsDesc &d = ens[e];
         const uint32_t t = (tile - __ldg(pre + e)) * kPhaseBlock + threadIdx.x;
@@ -180,30 +197,35 @@ __device__ __forceinline__ void tiles_of_phase(const EnsDesc *ens, const uint32_
 template <int NC, typename Real, bool OR, bool STAGED>
 __device__ __forceinline__ void half_sweep_body(const EnsDesc *ens, const uint32_t *pre, int n, int parity,
                                                 const uint64_t *phase_base, uint32_t phase_offset0, int nhit,
-                                                int nhitpar, GridBarrier *bar, int skip_block, StageBuf *sb)
+                                                int nhitpar, GridBarrier *bar, int skip_block, StageBuf *sb,
+                                                unsigned *tiles)
 {
     const uint32_t ntiles = __ldg(pre + n);
-    tiles_of_phase<NC, Real, OR, 0, STAGED>(ens, pre, n, parity, phase_base, phase_offset0, nhit, nhitpar, sb, ntiles);
+    tiles_of_phase<NC, Real, OR, 0, STAGED>(ens, pre, n, parity, phase_base, phase_offset0, nhit, nhitpar, sb, ntiles,
+                                            tiles + 0);
     if (!grid_sync(bar, (int)blockIdx.x != skip_block)) return;
-    tiles_of_phase<NC, Real, OR, 1, STAGED>(ens, pre, n, parity, phase_base, phase_offset0, nhit, nhitpar, sb, ntiles);
+    tiles_of_phase<NC, Real, OR, 1, STAGED>(ens, pre, n, parity, phase_base, phase_offset0, nhit, nhitpar, sb, ntiles,
+                                            tiles + 1);
     if (!grid_sync(bar, true)) return;
-    tiles_of_phase<NC, Real, OR, 2, STAGED>(ens, pre, n, parity, phase_base, phase_offset0, nhit, nhitpar, sb, ntiles);
+    tiles_of_phase<NC, Real, OR, 2, STAGED>(ens, pre, n, parity, phase_base, phase_offset0, nhit, nhitpar, sb, ntiles,
+                                            tiles + 2);
     if (!grid_sync(bar, true)) return;
-    tiles_of_phase<NC, Real, OR, 3, STAGED>(ens, pre, n, parity, phase_base, phase_offset0, nhit, nhitpar, sb, ntiles);
+    tiles_of_phase<NC, Real, OR, 3, STAGED>(ens, pre, n, parity, phase_base, phase_offset0, nhit, nhitpar, sb, ntiles,
+                                            tiles + 3);
 }
 
 template <int NC, typename Real, bool OR, int MINB, bool STAGED>
 __global__ void __launch_bounds__(kPhaseBlock, MINB)
 k_half_sweep_batch(const EnsDesc *ens, const uint32_t *pre, int n, int parity, const uint64_t *phase_base,
-                   uint32_t phase_offset0, int nhit, int nhitpar, GridBarrier *bar, int skip_block)
+                   uint32_t phase_offset0, int nhit, int nhitpar, GridBarrier *bar, int skip_block, unsigned *tiles)
 {
     if constexpr (STAGED) {
         __shared__ __align__(16) StageBuf sb;
         half_sweep_body<NC, Real, OR, STAGED>(ens, pre, n, parity, phase_base, phase_offset0, nhit, nhitpar, bar,
-                                              skip_block, &sb);
+                                              skip_block, &sb, tiles);
     } else {
         half_sweep_body<NC, Real, OR, STAGED>(ens, pre, n, parity, phase_base, phase_offset0, nhit, nhitpar, bar,
-                                              skip_block, nullptr);
+                                              skip_block, nullptr, tiles);
     }
 }
 
@@ -314,6 +336,7 @@ struct qg_batch {
     bool persistent = false;           // one launch per half-sweep (qg_batch_set_persistent)
     bool plaq_fp32 = false;            // FP32-product plaquette (qg_batch_set_measure_products)
     GridBarrier *d_bar = nullptr;
+    unsigned *d_tiles = nullptr;       // the persistent half-sweep's tile counters, one per direction
 };
 
 namespace {
@@ -403,9 +426,10 @@ cudaError_t launch_half(qg_batch *b, KernelT kern, int parity, uint32_t offset0,
     attr[0].val.cooperative = 1;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
+    if ((e = cudaMemsetAsync(b->d_tiles, 0, 4 * sizeof(unsigned), b->stream)) != cudaSuccess) return e;
     return cudaLaunchKernelEx(&cfg, kern, (const EnsDesc *)b->d_ens, (const uint32_t *)b->d_pre, b->n, parity,
                               (const uint64_t *)b->d_phase, offset0, b->cfg.nhit, b->cfg.nhitpar, b->d_bar,
-                              skip_block);
+                              skip_block, b->d_tiles);
 }
 
 template <typename Real>
@@ -546,6 +570,7 @@ extern "C" int qg_batch_destroy(qg_batch *b)
     cudaFree(b->d_overflow);
     cudaFree(b->d_series);
     cudaFree(b->d_bar);
+    cudaFree(b->d_tiles);
     if (b->stream) cudaStreamDestroy(b->stream);
     delete b;
     return QG_OK;
@@ -608,6 +633,7 @@ extern "C" int qg_batch_create(const qg_config *common, const qg_ensemble *ens, 
     if ((e = cudaMalloc(&b->d_overflow, sizeof(uint32_t))) != cudaSuccess) return fail_free(e, "overflow");
     if ((e = cudaMalloc(&b->d_bar, sizeof(GridBarrier))) != cudaSuccess) return fail_free(e, "barrier");
     if ((e = cudaMemset(b->d_bar, 0, sizeof(GridBarrier))) != cudaSuccess) return fail_free(e, "barrier clear");
+    if ((e = cudaMalloc(&b->d_tiles, 4 * sizeof(unsigned))) != cudaSuccess) return fail_free(e, "tile counters");
     if ((e = cudaMalloc(&b->d_series, sizeof(double) * 8 * n * (b->capacity ? b->capacity : 1))) != cudaSuccess)
         return fail_free(e, "series");
     std::vector<double> params(4 * (size_t)n, 0.0);
