@@ -22,6 +22,7 @@ struct qg_ctx {
     void *links = nullptr;
     float4 *prns = nullptr;
     float4 *rl_table = nullptr;
+    RanluxSplit rl_split = { 1, nullptr, nullptr };   // batches over several threads per generator
     uint32_t *d_seeds = nullptr;
     double *partials = nullptr;
     size_t partials_n = 0;
@@ -229,6 +230,7 @@ extern "C" int qg_destroy(qg_ctx *c)
     if (c->side) cudaStreamSynchronize(c->side);
     rl_free_lookahead(c);
     cudaFree(c->links); cudaFree(c->rl_buf[7]); cudaFree(c->rl_table); cudaFree(c->d_seeds);
+    cudaFree(const_cast<uint32_t *>(c->rl_split.mult)); cudaFree(c->rl_split.seg);
     cudaFree(c->partials); cudaFree(c->d_results); cudaFree(c->d_phase); cudaFree(c->d_params);
     cudaFree(c->d_netw); cudaFree(c->d_master); cudaFree(c->d_adam_m); cudaFree(c->d_adam_v);
     cudaFree(c->d_grad); cudaFree(c->d_gpart); cudaFree(c->d_mh_acc); cudaFree(c->d_mh_jump);
@@ -286,6 +288,24 @@ extern "C" int qg_create(const qg_config *cfg, qg_ctx **out)
         if ((e = cudaMemsetAsync(c->prns, 0, nq * sizeof(float4), c->stream)) != cudaSuccess) return bad("cudaMemset(prns)");
         if ((e = cudaMalloc(&c->rl_table, (size_t)7 * c->instances * sizeof(float4))) != cudaSuccess) return bad("cudaMalloc(table)");
         if ((e = cudaMalloc(&c->d_seeds, (size_t)c->instances * sizeof(uint32_t))) != cudaSuccess) return bad("cudaMalloc(seeds)");
+        // batches of whole luxury blocks: each generator's batch over several
+        // threads (the same outputs); without room for the scratch, one thread
+        const int parts = ranlux_split_parts(c->instances, (int)c->samples);
+        if (parts > 1) {
+            std::vector<uint32_t> mult((size_t)parts * 18);
+            ranlux_split_multipliers((int)c->samples, cfg->ranlux_nskip, parts, mult.data());
+            uint32_t *dm = nullptr;
+            float4 *seg = nullptr;
+            if (cudaMalloc(&dm, mult.size() * sizeof(uint32_t)) == cudaSuccess &&
+                cudaMalloc(&seg, (size_t)parts * 7 * c->instances * sizeof(float4)) == cudaSuccess &&
+                cudaMemcpy(dm, mult.data(), mult.size() * sizeof(uint32_t), cudaMemcpyHostToDevice) == cudaSuccess) {
+                c->rl_split = { parts, dm, seg };
+            } else {
+                cudaGetLastError();
+                cudaFree(dm);
+                cudaFree(seg);
+            }
+        }
     }
     if ((e = cudaMalloc(&c->partials, c->partials_n * sizeof(double))) != cudaSuccess) return bad("cudaMalloc(partials)");
     if ((e = cudaMalloc(&c->d_results, 64 * sizeof(double))) != cudaSuccess) return bad("cudaMalloc(results)");
@@ -394,7 +414,8 @@ extern "C" int qg_prng_produce(qg_ctx *c)
     if (c->cfg.prng != QG_PRNG_RANLUX) return fail(c, QG_ERR_STATE, "qg_prng_produce needs the RANLUX stream");
     if (!c->seeded) return fail(c, QG_ERR_STATE, "PRNG not seeded (qg_prng_seed)");
     QG_CK(rl_settle(c), "ranlux settle");
-    QG_CK(launch_ranlux_produce(c->rl_table, c->prns, c->instances, (int)c->samples, c->cfg.ranlux_nskip, c->stream),
+    QG_CK(launch_ranlux_produce(c->rl_table, c->prns, c->instances, (int)c->samples, c->cfg.ranlux_nskip, c->stream,
+                                &c->rl_split),
           "ranlux");
     c->prng_counter++;
     return QG_OK;
@@ -787,7 +808,8 @@ static cudaError_t enqueue_sweep(qg_ctx *c, bool reunit, cudaEvent_t *ev = nullp
         for (int mu = 0; mu < 4; mu++) {
             PhaseArgs a = phase_args(c, par_order[pi], mu, QG_UPDATE_HEATBATH, hb);
             if (a.prn_mode == QG_PRNG_RANLUX) {
-                e = launch_ranlux_produce(c->rl_table, c->prns, c->instances, (int)c->samples, f.ranlux_nskip, c->stream);
+                e = launch_ranlux_produce(c->rl_table, c->prns, c->instances, (int)c->samples, f.ranlux_nskip, c->stream,
+                                          &c->rl_split);
                 if (e != cudaSuccess) return e;
             }
             if ((e = timed_phase(a)) != cudaSuccess) return e;
@@ -835,7 +857,7 @@ static cudaError_t enqueue_sweep_lookahead(qg_ctx *c, bool reunit, int v)
             if ((e = cudaEventRecord(c->ev_phase[k], c->stream)) != cudaSuccess) return e;
             if ((e = cudaStreamWaitEvent(c->side, c->ev_phase[k], 0)) != cudaSuccess) return e;
             if ((e = launch_ranlux_produce(c->rl_table, rl_out(c, v, k), c->instances, (int)c->samples,
-                                           f.ranlux_nskip, c->side)) != cudaSuccess)
+                                           f.ranlux_nskip, c->side, &c->rl_split)) != cudaSuccess)
                 return e;
         }
     for (int n = 0; n < f.n_or; n++)
@@ -1002,7 +1024,7 @@ extern "C" int qg_sweep(qg_ctx *c, int nsweeps)
               "ranlux snapshot");
         for (int k = 0; k < 8; k++)
             QG_CK(launch_ranlux_produce(c->rl_table, rl_in(c, c->rl_var, k), c->instances, (int)c->samples,
-                                        f.ranlux_nskip, c->stream), "ranlux");
+                                        f.ranlux_nskip, c->stream, &c->rl_split), "ranlux");
         c->rl_ahead = true;
     }
     for (int n = 0; n < nsweeps; n++) {

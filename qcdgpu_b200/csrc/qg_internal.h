@@ -105,8 +105,18 @@ cudaError_t launch_field_check(const Geom &G, const void *links, int group, int 
 // RANLUX, reference layout: one generator per instance, seed table of 7
 // float4 per instance (SoA), output prns[s*instances + i]
 cudaError_t launch_ranlux_init(const uint32_t *seeds, float4 *table, int instances, cudaStream_t s);
-cudaError_t launch_ranlux_produce(float4 *table, float4 *prns, int instances, int samples, int nskip,
-                                  cudaStream_t s);
+// a RANLUX batch split over `parts` threads per generator (qg_ranlux.cu):
+// mult = parts x 18 limbs of the jump multipliers, seg = parts x 7 x
+// instances float4 of segment start states; parts = 1: one thread each
+struct RanluxSplit {
+    int parts;
+    const uint32_t *mult;
+    float4 *seg;
+};
+int ranlux_split_parts(int instances, int samples);
+void ranlux_split_multipliers(int samples, int nskip, int parts, uint32_t *out);
+cudaError_t launch_ranlux_produce(float4 *table, float4 *prns, int instances, int samples, int nskip, cudaStream_t s,
+                                  const RanluxSplit *split = nullptr);
 
 Geom make_geom(const int n[4]);
 

@@ -12,6 +12,7 @@
 // NSKIP%24 single steps followed by a register rotation that restores the
 // block-start indexing (i24 = 23, j24 = 9).
 #include "qg_internal.h"
+#include "qg_rlx576.h"
 
 namespace qg {
 
@@ -181,6 +182,104 @@ __global__ void __launch_bounds__(128) k_ranlux(float4 *table, float4 *prns, int
     table[(size_t)6 * instances + i] = make_float4(0.0f, 0.0f, (float)in24, c ? RL_TWOM24 : 0.0f);
 }
 
+// ---------------------------------------------- one generator, several threads
+// A batch of whole luxury blocks (samples % 6 == 0; every batch then starts
+// at a block boundary, in24 = 6) split over `parts` threads per generator:
+// segment j produces luxury blocks [j B / parts, (j+1) B / parts) of the
+// B = samples / 6.  k_ranlux_jump gives each segment its start state --
+// the batch-start state moved S_j = b0_j (NSKIP + 24) steps ahead by one
+// multiplication by a^S_j modulo 2^576 - 2^240 + 1 (qg_rlx576.h; mult holds
+// a^S_j for every segment, host-computed) -- into seg[j]; k_ranlux_seg
+// runs the serial kernel's steps from there, and the last segment writes
+// the batch-end state back to the table.  The outputs are those of the
+// serial kernel bit for bit.
+
+// the table rows of a state at a block start: x[23 - k] is the k-th oldest word
+__device__ __forceinline__ void rl_load(const float4 *t, int instances, int i, uint32_t (&x)[24], uint32_t &c)
+{
+#pragma unroll
+    for (int k = 0; k < 6; k++) {
+        float4 v = t[(size_t)k * instances + i];
+        x[4 * k] = (uint32_t)(v.x * 16777216.0f) << 8; x[4 * k + 1] = (uint32_t)(v.y * 16777216.0f) << 8;
+        x[4 * k + 2] = (uint32_t)(v.z * 16777216.0f) << 8; x[4 * k + 3] = (uint32_t)(v.w * 16777216.0f) << 8;
+    }
+    c = t[(size_t)6 * instances + i].w != 0.0f ? 1u : 0u;
+}
+__device__ __forceinline__ void rl_store(float4 *t, int instances, int i, const uint32_t (&x)[24], uint32_t c)
+{
+#pragma unroll
+    for (int k = 0; k < 6; k++)
+        t[(size_t)k * instances + i] =
+            make_float4(rl_float(x[4 * k]), rl_float(x[4 * k + 1]), rl_float(x[4 * k + 2]), rl_float(x[4 * k + 3]));
+    t[(size_t)6 * instances + i] = make_float4(0.0f, 0.0f, 6.0f, c ? RL_TWOM24 : 0.0f);
+}
+
+__global__ void __launch_bounds__(128) k_ranlux_jump(const float4 *table, float4 *seg, int instances, int parts,
+                                                      const uint32_t *mult)
+{
+    const int id = blockIdx.x * blockDim.x + threadIdx.x;
+    if (id >= instances * parts) return;
+    const int i = id % instances, j = id / instances;
+    uint32_t x[24], c;
+    rl_load(table, instances, i, x, c);
+    if (j > 0) {
+        uint32_t L[24], E[rlx::kLimbs], M[rlx::kLimbs], J[rlx::kLimbs];
+        for (int k = 0; k < 24; k++) L[k] = x[23 - k] >> 8;
+        rlx::encode(L, c, E);
+        for (int k = 0; k < rlx::kLimbs; k++) M[k] = __ldg(mult + (size_t)j * rlx::kLimbs + k);
+        rlx::mulmod(E, M, J);
+        rlx::decode(J, L, c);
+        for (int k = 0; k < 24; k++) x[23 - k] = L[k] << 8;
+    }
+    rl_store(seg + (size_t)j * 7 * instances, instances, i, x, c);
+}
+
+template <int NSKIP>
+__global__ void __launch_bounds__(128) k_ranlux_seg(float4 *table, const float4 *seg, float4 *prns, int instances,
+                                                    int samples, int parts)
+{
+    const int id = blockIdx.x * blockDim.x + threadIdx.x;
+    if (id >= instances * parts) return;
+    const int i = id % instances, j = id / instances;
+    const int B = samples / 6;
+    const int b0 = (int)((long long)j * B / parts), b1 = (int)((long long)(j + 1) * B / parts);
+    uint32_t x[24], c;
+    rl_load(seg + (size_t)j * 7 * instances, instances, i, x, c);
+#pragma unroll 1
+    for (int bl = b0; bl < b1; bl++) {
+        rl_skip<NSKIP>(x, c);
+        float4 *o = prns + (size_t)6 * bl * instances + i;
+        o[0] = rl_quad<0>(x, c);
+        o[(size_t)instances] = rl_quad<1>(x, c);
+        o[(size_t)2 * instances] = rl_quad<2>(x, c);
+        o[(size_t)3 * instances] = rl_quad<3>(x, c);
+        o[(size_t)4 * instances] = rl_quad<4>(x, c);
+        o[(size_t)5 * instances] = rl_quad<5>(x, c);
+    }
+    if (j == parts - 1) rl_store(table, instances, i, x, c);
+}
+
+int ranlux_split_parts(int instances, int samples)
+{
+    if (samples % 6 != 0 || instances < 1) return 1;
+    const int B = samples / 6;
+    int parts = (1 << 17) / instances;          // about 2^17 threads per batch
+    if (parts > B / 8) parts = B / 8;           // at least 8 blocks per segment
+    if (parts > 16) parts = 16;
+    return parts < 2 ? 1 : parts;
+}
+
+void ranlux_split_multipliers(int samples, int nskip, int parts, uint32_t *out)
+{
+    const int B = samples / 6;
+    for (int j = 0; j < parts; j++) {
+        const uint64_t steps = (uint64_t)((long long)j * B / parts) * (uint64_t)(nskip + 24);
+        uint32_t r[rlx::kLimbs];
+        rlx::binv_pow(steps, r);
+        for (int k = 0; k < rlx::kLimbs; k++) out[(size_t)j * rlx::kLimbs + k] = r[k];
+    }
+}
+
 // ranlux_init (prngcl_ranlux.cl:137-157): 24 seed words from the
 // 40014/53668 LCG started at the instance's glibc seed; in24 = 6 forces the
 // luxury skip before the first output.
@@ -207,8 +306,23 @@ cudaError_t launch_ranlux_init(const uint32_t *seeds, float4 *table, int instanc
     return cudaGetLastError();
 }
 
-cudaError_t launch_ranlux_produce(float4 *table, float4 *prns, int instances, int samples, int nskip, cudaStream_t s)
+cudaError_t launch_ranlux_produce(float4 *table, float4 *prns, int instances, int samples, int nskip, cudaStream_t s,
+                                  const RanluxSplit *split)
 {
+    if (split && split->parts > 1) {
+        const int P = split->parts;
+        const unsigned nbp = (unsigned)(((size_t)instances * P + 127) / 128);
+        k_ranlux_jump<<<nbp, 128, 0, s>>>(table, split->seg, instances, P, split->mult);
+        switch (nskip) {
+        case 24: k_ranlux_seg<24><<<nbp, 128, 0, s>>>(table, split->seg, prns, instances, samples, P); break;
+        case 48: k_ranlux_seg<48><<<nbp, 128, 0, s>>>(table, split->seg, prns, instances, samples, P); break;
+        case 97: k_ranlux_seg<97><<<nbp, 128, 0, s>>>(table, split->seg, prns, instances, samples, P); break;
+        case 223: k_ranlux_seg<223><<<nbp, 128, 0, s>>>(table, split->seg, prns, instances, samples, P); break;
+        case 389: k_ranlux_seg<389><<<nbp, 128, 0, s>>>(table, split->seg, prns, instances, samples, P); break;
+        default: return cudaErrorInvalidValue;
+        }
+        return cudaGetLastError();
+    }
     unsigned nb = (instances + 127) / 128;
     switch (nskip) {
     case 24: k_ranlux<24><<<nb, 128, 0, s>>>(table, prns, instances, samples); break;

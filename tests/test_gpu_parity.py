@@ -66,6 +66,38 @@ def test_ranlux_default_instances_bit_exact():
     assert np.array_equal(L.prns_download().view(np.uint32), R.batch(info.prng_samples).view(np.uint32))
 
 
+def split_parts(instances, samples):
+    """the number of threads per generator the library splits a batch over
+    (ranlux_split_parts in qg_ranlux.cu)"""
+    if samples % 6:
+        return 1
+    parts = min((1 << 17) // instances, samples // 6 // 8, 16)
+    return parts if parts >= 2 else 1
+
+
+@pytest.mark.parametrize("dims,instances,nskip,batches", [((8, 8, 8, 8), 512, 389, 3), ((8, 8, 8, 8), 256, 24, 3),
+                                                          ((16, 16, 16, 16), 2048, 223, 3),
+                                                          ((32, 32, 32, 32), 16384, 223, 1)])
+def test_ranlux_split_batches_bit_exact(dims, instances, nskip, batches):
+    """Batches of whole 24-output luxury blocks are produced with each
+    generator's batch split over several threads, every segment started
+    from the batch-start state jumped ahead modulo 2^576 - 2^240 + 1: the
+    batches equal the oracle's serial stream bit for bit, batch after
+    batch (the last case is the bench workload's generator, 16384
+    instances at 32^4)"""
+    L = Q.Lattice(Q.default_config(group=3, size=dims, precision=0, start=Q.START_COLD, prng=Q.PRNG_RANLUX,
+                                   ranlux_nskip=nskip, prng_instances=instances, randseries=54, row_align=64))
+    S = L.info().prng_samples
+    assert split_parts(instances, S) > 1, S
+    R = O.Ranlux(54, instances, nskip)
+    L.seed(54)
+    for k in range(batches):
+        if k:
+            L.produce()
+        assert np.array_equal(L.prns_download().view(np.uint32), R.batch(S).view(np.uint32)), k
+    L.close()
+
+
 # ------------------------------------------------------- layout / starts
 @pytest.mark.parametrize("group,precision", [(3, 0), (3, 1), (2, 0), (2, 1)])
 def test_layout_roundtrip(group, precision):
