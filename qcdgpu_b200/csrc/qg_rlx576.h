@@ -32,52 +32,55 @@ constexpr int kLimbs = 18;
 // m = 2^576 - 2^240 + 1
 QG_RLX_HD uint32_t m_limb(int k) { return k == 0 ? 1u : k == 7 ? 0xFFFF0000u : k >= 8 ? 0xFFFFFFFFu : 0u; }
 
-// r (n limbs, n >= 18) >= m ?
-QG_RLX_HD bool ge_m(const uint32_t *r, int n)
+// r (N limbs, N >= 18) >= m ?
+template <int N>
+QG_RLX_HD bool ge_m(const uint32_t *r)
 {
-    for (int k = n - 1; k >= kLimbs; k--)
-        if (r[k]) return true;
-    for (int k = kLimbs - 1; k >= 0; k--) {
-        const uint32_t mk = m_limb(k);
-        if (r[k] != mk) return r[k] > mk;
+    bool above = false, decided = false;
+#pragma unroll
+    for (int k = N - 1; k >= 0; k--) {
+        const uint32_t mk = k < kLimbs ? m_limb(k) : 0u;
+        if (!decided && r[k] != mk) { above = r[k] > mk; decided = true; }
     }
-    return true;
+    return decided ? above : true;
 }
-// r (n limbs) -= m
-QG_RLX_HD void sub_m(uint32_t *r, int n)
+// r (N limbs) -= m
+template <int N>
+QG_RLX_HD void sub_m(uint32_t *r)
 {
     uint64_t borrow = 0;
-    for (int k = 0; k < n; k++) {
+#pragma unroll
+    for (int k = 0; k < N; k++) {
         const uint64_t s = (uint64_t)r[k] - (k < kLimbs ? m_limb(k) : 0u) - borrow;
         r[k] = (uint32_t)s;
         borrow = (s >> 63) & 1u;
     }
 }
 
-// t (n limbs, n <= 28) + h * (2^240 - 1) with h of nh limbs into t; the
-// caller sizes t for the sum
-QG_RLX_HD void add_fold(uint32_t *t, int n, const uint32_t *h, int nh)
+// t (N limbs) + h (NH limbs) * (2^240 - 1) into t; the caller sizes t for
+// the sum
+template <int N, int NH>
+QG_RLX_HD void add_fold(uint32_t *t, const uint32_t *h)
 {
     // h << 240: 7 limbs and 16 bits
-    uint32_t sh[28];
-    for (int k = 0; k < n; k++) sh[k] = 0;
-    for (int k = 0; k < nh; k++) {
+    uint32_t sh[N];
+#pragma unroll
+    for (int k = 0; k < N; k++) sh[k] = 0;
+#pragma unroll
+    for (int k = 0; k < NH; k++) {
         const uint64_t v = (uint64_t)h[k] << 16;
-        if (k + 7 < n) sh[k + 7] |= (uint32_t)v;
-        if (k + 8 < n) sh[k + 8] |= (uint32_t)(v >> 32);
+        if (k + 7 < N) sh[k + 7] |= (uint32_t)v;
+        if (k + 8 < N) sh[k + 8] |= (uint32_t)(v >> 32);
     }
-    // sh -= h (sh >= h)
-    uint64_t borrow = 0;
-    for (int k = 0; k < n; k++) {
-        const uint64_t s = (uint64_t)sh[k] - (k < nh ? h[k] : 0u) - borrow;
-        sh[k] = (uint32_t)s;
-        borrow = (s >> 63) & 1u;
-    }
-    uint64_t carry = 0;
-    for (int k = 0; k < n; k++) {
-        const uint64_t s = (uint64_t)t[k] + sh[k] + carry;
-        t[k] = (uint32_t)s;
-        carry = s >> 32;
+    // sh -= h (sh >= h), then t += sh
+    uint64_t borrow = 0, carry = 0;
+#pragma unroll
+    for (int k = 0; k < N; k++) {
+        const uint64_t d = (uint64_t)sh[k] - (k < NH ? h[k] : 0u) - borrow;
+        borrow = (d >> 63) & 1u;
+        const uint64_t s2 = (uint64_t)t[k] + (uint32_t)d + carry;
+        t[k] = (uint32_t)s2;
+        carry = s2 >> 32;
     }
 }
 
@@ -85,9 +88,12 @@ QG_RLX_HD void add_fold(uint32_t *t, int n, const uint32_t *h, int nh)
 QG_RLX_HD void mulmod(const uint32_t (&a)[kLimbs], const uint32_t (&b)[kLimbs], uint32_t (&r)[kLimbs])
 {
     uint32_t p[2 * kLimbs];
+#pragma unroll
     for (int k = 0; k < 2 * kLimbs; k++) p[k] = 0;
+#pragma unroll
     for (int i = 0; i < kLimbs; i++) {
         uint64_t carry = 0;
+#pragma unroll
         for (int j = 0; j < kLimbs; j++) {
             const uint64_t s = (uint64_t)a[i] * b[j] + p[i + j] + carry;
             p[i + j] = (uint32_t)s;
@@ -97,12 +103,15 @@ QG_RLX_HD void mulmod(const uint32_t (&a)[kLimbs], const uint32_t (&b)[kLimbs], 
     }
     // p = H 2^576 + L == L + H (2^240 - 1): 27 limbs, then once more: 19
     uint32_t t[27];
+#pragma unroll
     for (int k = 0; k < 27; k++) t[k] = k < kLimbs ? p[k] : 0u;
-    add_fold(t, 27, p + kLimbs, kLimbs);
+    add_fold<27, kLimbs>(t, p + kLimbs);
     uint32_t u[19];
+#pragma unroll
     for (int k = 0; k < 19; k++) u[k] = k < kLimbs ? t[k] : 0u;
-    add_fold(u, 19, t + kLimbs, 27 - kLimbs);
-    while (ge_m(u, 19)) sub_m(u, 19);
+    add_fold<19, 27 - kLimbs>(u, t + kLimbs);
+    while (ge_m<19>(u)) sub_m<19>(u);
+#pragma unroll
     for (int k = 0; k < kLimbs; k++) r[k] = u[k];
 }
 
@@ -111,8 +120,11 @@ QG_RLX_HD void encode(const uint32_t (&L)[24], uint32_t c, uint32_t (&E)[kLimbs]
 {
     // A = sum L[k] 2^(24k), B = sum_{k<10} L[14+k] 2^(24k); E = A + (m - B) + c
     uint32_t A[19], B[kLimbs];
+#pragma unroll
     for (int k = 0; k < 19; k++) A[k] = 0;
+#pragma unroll
     for (int k = 0; k < kLimbs; k++) B[k] = 0;
+#pragma unroll
     for (int k = 0; k < 24; k++) {
         const int bit = 24 * k, w = bit >> 5, o = bit & 31;
         const uint64_t v = (uint64_t)L[k] << o;
@@ -126,6 +138,7 @@ QG_RLX_HD void encode(const uint32_t (&L)[24], uint32_t c, uint32_t (&E)[kLimbs]
     }
     // A += m - B + c
     uint64_t borrow = 0, carry = c;
+#pragma unroll
     for (int k = 0; k < 19; k++) {
         const uint64_t d = (uint64_t)(k < kLimbs ? m_limb(k) : 0u) - (k < kLimbs ? B[k] : 0u) - borrow;
         borrow = (d >> 63) & 1u;
@@ -133,7 +146,8 @@ QG_RLX_HD void encode(const uint32_t (&L)[24], uint32_t c, uint32_t (&E)[kLimbs]
         A[k] = (uint32_t)s;
         carry = s >> 32;
     }
-    while (ge_m(A, 19)) sub_m(A, 19);
+    while (ge_m<19>(A)) sub_m<19>(A);
+#pragma unroll
     for (int k = 0; k < kLimbs; k++) E[k] = A[k];
 }
 
@@ -141,17 +155,35 @@ QG_RLX_HD void encode(const uint32_t (&L)[24], uint32_t c, uint32_t (&E)[kLimbs]
 QG_RLX_HD void decode(const uint32_t (&E)[kLimbs], uint32_t (&L)[24], uint32_t &c)
 {
     uint32_t e[kLimbs];
+#pragma unroll
     for (int k = 0; k < kLimbs; k++) e[k] = E[k];
+#pragma unroll 1
     for (int step = 1; step <= 24; step++) {
-        // t = e 2^24 = q0 2^576 + lo;  b e = q m + r  with  r = lo + q0 (2^240 - 1) - (q - q0) m
+        // b e = q m + r: with b e = q0 2^576 + lo (q0 = the top 24 bits of e),
+        // r = lo + q0 (2^240 - 1) - (q - q0) m; lo + q0 2^240 - q0 touches
+        // limbs 0 and 7, 8 and their carries only
         uint32_t t[19];
-        t[0] = e[0] << 24;
-        for (int k = 1; k < kLimbs; k++) t[k] = (e[k] << 24) | (e[k - 1] >> 8);
         uint32_t q = e[kLimbs - 1] >> 8;
+#pragma unroll
+        for (int k = kLimbs - 1; k > 0; k--) t[k] = (e[k] << 24) | (e[k - 1] >> 8);
+        t[0] = e[0] << 24;
         t[kLimbs] = 0;
-        const uint32_t h[1] = { q };
-        add_fold(t, 19, h, 1);
-        while (ge_m(t, 19)) { sub_m(t, 19); q++; }
+        uint64_t acc = (uint64_t)t[7] + ((uint64_t)q << 16);
+        t[7] = (uint32_t)acc;
+#pragma unroll
+        for (int k = 8; k <= kLimbs; k++) {
+            acc = (acc >> 32) + t[k];
+            t[k] = (uint32_t)acc;
+        }
+        uint64_t borrow = q;
+#pragma unroll
+        for (int k = 0; k <= kLimbs; k++) {
+            const uint64_t d = (uint64_t)t[k] - borrow;
+            t[k] = (uint32_t)d;
+            borrow = (d >> 63) & 1u;
+        }
+        while (ge_m<19>(t)) { sub_m<19>(t); q++; }
+#pragma unroll
         for (int k = 0; k < kLimbs; k++) e[k] = t[k];
         L[24 - step] = q;                       // x_{n-step}
     }
@@ -161,6 +193,7 @@ QG_RLX_HD void decode(const uint32_t (&E)[kLimbs], uint32_t (&L)[24], uint32_t &
     uint64_t borrow = 0;
     uint32_t d0 = 0;
     uint32_t nz = 0;
+#pragma unroll
     for (int k = 0; k < kLimbs; k++) {
         const uint64_t s = (uint64_t)E[k] - E0[k] - borrow;
         borrow = (s >> 63) & 1u;
