@@ -185,6 +185,30 @@ def test_sweeps_ranlux_reference_cadence(group, precision):
     assert L.info().prng_counter == 1 + 16
 
 
+@pytest.mark.parametrize("precision,look", [(1, 1), (0, 0)])
+def test_sweeps_with_split_ranlux_batches(precision, look):
+    """qg_sweep in RANLUX mode at a size whose batches are whole luxury
+    blocks (8^4, 512 generators: each batch over 2 threads per generator),
+    with and without the lookahead: the links follow the oracle's sweep fed
+    the serial stream"""
+    L, c = make_pair(3, (8, 8, 8, 8), precision, start=Q.START_COLD, beta=6.0)
+    L.set_prng_lookahead(look)
+    S = L.info().prng_samples
+    assert split_parts(INSTANCES, S) > 1, S
+    R = O.Ranlux(54, INSTANCES)
+    L.seed(54)
+    L.init(Q.START_COLD)
+    R.batch(S)
+    t = cold_table(c)
+    for s in range(2):
+        L.sweep(1)
+        oracle_sweep_ranlux(c, t, R, S)
+        O.lib.ol_gramschmidt(ctypes.byref(c), O.vp(t))
+        d = maxdiff(L.download(), t)
+        assert d <= TOL_U[precision] * (1 + s), (s, d)
+    L.close()
+
+
 def _ranlux_lookahead_chain(look, precision):
     """3 sweeps in one call, one single heatbath phase, 2 more sweeps, then
     one produce: the PRN buffer after the sweeps, the links, the buffer after
